@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""Tree-force throughput on B200: particles/s of the all-active grouped walk.
+
+Workload (default ``clustered_16m``): 16,777,216 equal-mass particles of a seeded Soneira-Peebles
+hierarchy in the unit cube (eta=4, lambda=1.9, 12 levels, 10% uniform background, softening 1e-4).
+Protocol (shmem/bench_treeforce.cc:35-58 and shmem/mfm.cc:743-751): build the tree, a first walk
+with Barnes-Hut theta=0.7 and aold=0, aold = alpha*|a|/G, then the timed walks with the relative
+criterion alone (alpha=0.0025).  One step = one walk over every particle (targets = orderbuf) with
+inputs resident in HBM; ``value`` = particles walked / device time.  ``e2e`` repeats the step
+through the C ABI with host buffers: each step copies positions, masses, softenings and aold from
+pinned host memory, rebuilds the tree, walks, and copies the accelerations back.  Force error is
+measured against an FP64 direct sum on a seeded 4096-particle sample.
+
+--impl reference times the reference's own CPU walk (shmem::accel_grouped, batch 0, compiled from
+the reference sources into oracle/_ref) on a bounded sample of whole leaf groups of the same
+workload, with every host thread.
+
+Multi-GPU (--gpus N under torchrun): every rank walks its own independent system of the same
+size (seed + rank); there is no data-path collective, only the barrier and a max over ranks of the
+timed region ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "tree-force particles/s at fixed p99 force error: learned-MAC vs plain walk"
+FLOPS_PER_INTERACTION = 20  # r^2 5, rsqrt 1, r^-3 and m 3, h test 2, acceleration 6, potential 2, select 1
+WORKLOADS = {
+    "clustered_16m": dict(desc="Soneira-Peebles clustered box, N=16,777,216, eta=4, lambda=1.9, "
+                               "12 levels, 10% uniform background, softening 1e-4", alpha=0.0025),
+    "galaxy_4m": dict(desc="Hernquist halo 3,145,728 + exponential disk 1,048,576, softening "
+                           "0.005/0.002", alpha=0.0025),
+    "plummer_65k": dict(desc="Plummer sphere N=65,536, truncated at 20a, softening 0.01", alpha=0.005),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_workload(name, seed_offset=0):
+    from gizmo_shared_memory_b200 import ics
+
+    if name == "clustered_16m":
+        return ics.soneira_peebles(seed=3 + seed_offset)
+    if name == "galaxy_4m":
+        return ics.galaxy(seed=2 + seed_offset)
+    if name == "plummer_65k":
+        return ics.plummer(n=65536, seed=42 + seed_offset)
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU reference walk on a bounded sample
+# ---------------------------------------------------------------------------------------------
+def leaf_group_sample(orderbuf, leaf_of, want, rng):
+    """Whole leaf groups (consecutive orderbuf runs with one leaf), picked at random until the
+    sample holds at least `want` targets; returned in tree order."""
+    L = leaf_of[orderbuf]
+    starts = np.concatenate([[0], np.nonzero(np.diff(L))[0] + 1])
+    ends = np.concatenate([starts[1:], [len(L)]])
+    pick = rng.permutation(len(starts))
+    sizes = (ends - starts)[pick]
+    k = int(np.searchsorted(np.cumsum(sizes), want)) + 1
+    sel = np.sort(pick[:k])
+    return np.concatenate([orderbuf[s:e] for s, e in zip(starts[sel], ends[sel])]).astype(np.uint32)
+
+
+class CpuReference:
+    """oracle/_ref (the reference's own shmem tree) when built, else the oracle restatement."""
+
+    def __init__(self):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import Reference, Restatement, reference_available
+
+        self.kind = "reference" if reference_available() else "port"
+        self.lib = Reference() if self.kind == "reference" else Restatement()
+        self.cores = os.cpu_count() or 1
+        if self.kind == "reference":
+            self.lib.set_threads(self.cores)
+        else:
+            os.environ.setdefault("OMP_NUM_THREADS", str(self.cores))
+
+    def build(self, P):
+        t0 = time.perf_counter()
+        T = self.lib.build(P)
+        return T, time.perf_counter() - t0
+
+    def walk(self, T, targets, aold, theta=0.0):
+        if self.kind == "reference":
+            return T.accel_grouped(targets, theta, 1.0, 0, aold=aold)
+        return T.accel_grouped(targets, theta, 1.0, 0, aold=aold)[:3]
+
+
+def cpu_sample_walk(cpu, T, aold_orig, seconds, rng, alpha=None):
+    """Time one walk over a sample of whole leaf groups sized to about `seconds` of CPU work."""
+    ob, _, leaf = T.order()
+    tg = leaf_group_sample(ob, leaf, 4096, rng)
+
+    def aold_for(t):
+        if aold_orig is not None:
+            return aold_orig[t]
+        a = cpu.walk(T, t, None, theta=0.7)
+        return alpha * np.sqrt(a[0] ** 2 + a[1] ** 2 + a[2] ** 2)
+
+    t0 = time.perf_counter()
+    cpu.walk(T, tg, aold_for(tg))
+    dt = time.perf_counter() - t0
+    want = int(min(len(ob), max(4096, len(tg) * seconds / max(dt, 1e-4))))
+    tg = leaf_group_sample(ob, leaf, want, rng)
+    return tg, aold_for(tg)
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = WORKLOADS[args.workload]
+    P = make_workload(args.workload)
+    cpu = CpuReference()
+    T, tbuild = cpu.build(P)
+    rng = np.random.default_rng(123)
+    tg, aold = cpu_sample_walk(cpu, T, None, args.sample_seconds, rng, alpha=cfg["alpha"])
+    for _ in range(args.warmup):
+        cpu.walk(T, tg, aold)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cpu.walk(T, tg, aold)
+        times.append(time.perf_counter() - t0)
+    t = float(np.mean(times))
+    value = len(tg) / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "particles/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": args.workload, "description": cfg["desc"],
+                                        "n": int(len(P["m"])), "criterion": f"relative alpha={cfg['alpha']}",
+                                        "grouping": "leaf groups (batch 0)"},
+        "cpu_baseline": {"value": value, "unit": "particles/s", "cores": cpu.cores, "kind": cpu.kind,
+                         "sample": f"{len(tg)} targets in whole leaf groups picked at random; "
+                                   f"tree prebuilt ({tbuild:.1f} s build, not timed)"},
+        "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------------------------
+def relerr(a, b):
+    d = np.sqrt(sum((x - y) ** 2 for x, y in zip(a, b)))
+    n = np.sqrt(sum(y ** 2 for y in b))
+    return d / np.where(n > 0, n, 1.0)
+
+
+def read_profile_traffic(workload):
+    """dram bytes per walk launch from the committed ncu summary, if one exists."""
+    p = os.path.join(ROOT, "profiles", f"walk_kernel_{workload}.json")
+    try:
+        return json.load(open(p)).get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+def run_gpu_arm(args):
+    import torch
+
+    import gizmo_shared_memory_b200 as g
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    cfg = WORKLOADS[args.workload]
+    alpha = args.alpha if args.alpha is not None else cfg["alpha"]
+    group_mode = {"leaf": g.GT_GROUP_LEAF, "node": g.GT_GROUP_NODE}[args.group]
+    wopts = dict(group_mode=group_mode, group_max=args.group_max)
+
+    P = make_workload(args.workload, seed_offset=rank)
+    n = len(P["m"])
+    dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
+    ctx = g.Context(local, torch_stream=True)
+    peak32, peak64 = ctx.measure_peaks()
+    T = ctx.build(dev)
+    info = T.info()
+    nl = info["n_live"]
+    out = tuple(torch.empty(nl, dtype=torch.float64, device="cuda") for _ in range(3))
+    # bootstrap walk (theta = 0.7, aold = 0), then aold = alpha |a| / G
+    ctx.accel_grouped(T, None, theta=0.7, outs=out + (None,), **wopts)
+    aold = ctx.form_aold(*out, alpha)
+    # counted walk: interactions as the reference counts them (SHMEM_COUNT_WALK)
+    ctx.accel_grouped(T, None, aold=aold, theta=0.0, outs=out + (None,), count=True, **wopts)
+    st = ctx.stats()
+    inter = st["multipole"] + st["pairs"]
+
+    def step():
+        ctx.accel_grouped(T, None, aold=aold, theta=0.0, outs=out + (None,), async_=True, **wopts)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    stream = torch.cuda.current_stream()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    l0 = ctx.launches()
+    torch.cuda.synchronize()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for a, b in evs:
+        a.record(stream)
+        step()
+        b.record(stream)
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    launches = ctx.launches() - l0
+    clocks = sampler.stop()
+    t_total = e_start.elapsed_time(e_end) / 1e3
+    t_kernel = float(np.mean([a.elapsed_time(b) for a, b in evs])) / 1e3
+    if dist:
+        tt = torch.tensor([t_total, t_kernel], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_total, t_kernel = float(tt[0]), float(tt[1])
+    t_step = t_total / args.steps
+    value = nl * world / t_step
+
+    # accuracy: FP64 direct sum on a seeded 4096-particle sample
+    rng = np.random.default_rng(77 + rank)
+    sample = np.sort(rng.choice(n, size=min(4096, n), replace=False)).astype(np.uint32)
+    full = ctx.accel_grouped(T, None, aold=aold, theta=0.0, out_order=g.GT_OUT_ORIGINAL, **wopts)
+    full = [f.cpu().numpy() for f in full]
+    dref = ctx.direct(P, sample)
+    err = relerr([full[k][sample] for k in range(3)], dref[:3])
+    err_med, err_p99 = float(np.median(err)), float(np.quantile(err, 0.99))
+
+    # end to end through the C ABI with host buffers (pinned), build + walk every step
+    e2e = None
+    if not args.no_e2e:
+        pin = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in P.items()}
+        aold_tree = aold.cpu()
+        aold_h = torch.empty(nl, dtype=torch.float64).pin_memory()
+        aold_h.copy_(aold_tree)
+        aold_h = aold_h.numpy()
+        ho = [torch.empty(nl, dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
+        hctx = g.Context(local)
+        ttimes = []
+        for it in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            T2 = hctx.build(pin)
+            hctx.accel_grouped(T2, None, aold=aold_h, theta=0.0, outs=tuple(ho) + (None,), **wopts)
+            t1 = time.perf_counter()
+            T2.free()
+            if it >= args.warmup:
+                ttimes.append(t1 - t0)
+        te = float(np.mean(ttimes))
+        if dist:
+            tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt[0])
+        e2e = {"value": nl * world / te, "unit": "particles/s", "ms_per_step": 1e3 * te,
+               "h2d_bytes_per_step": int(5 * 8 * n + 8 * nl), "d2h_bytes_per_step": int(3 * 8 * nl),
+               "includes": "H2D of x,y,z,m,soft,aold from pinned memory + tree build + walk + D2H of ax,ay,az"}
+        hctx.close()
+
+    # CPU baseline (rank 0 only, N=1 only): the reference walk on a bounded sample
+    cpu_line = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = CpuReference()
+        Tc, tbuild = cpu.build(P)
+        aold_orig = np.zeros(n)
+        aold_orig[T.download(nodes=False)["orderbuf"]] = aold.cpu().numpy()
+        tg, ao = cpu_sample_walk(cpu, Tc, aold_orig, args.sample_seconds, np.random.default_rng(123))
+        t0 = time.perf_counter()
+        cpu.walk(Tc, tg, ao)
+        tc = time.perf_counter() - t0
+        cpu_line = {"value": len(tg) / tc, "unit": "particles/s", "cores": cpu.cores, "kind": cpu.kind,
+                    "sample": f"{len(tg)} targets in whole leaf groups picked at random, the same aold; "
+                              f"tree prebuilt ({tbuild:.1f} s CPU build, not timed)"}
+
+    achieved = FLOPS_PER_INTERACTION * inter / t_kernel / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded; see config.description)",
+        "config": {"workload": args.workload, "description": cfg["desc"], "n": n,
+                   "criterion": f"plain relative criterion alpha={alpha} after a theta=0.7 bootstrap walk",
+                   "mac": "plain", "grouping": args.group + (f" (group_max {args.group_max})" if args.group == "node" else ""),
+                   "l2": f"inputs larger than L2: {n * 32 / 2**20:.0f} MiB of particles + "
+                         f"{info['n_nodes'] * 64 / 2**20:.0f} MiB of nodes per walk",
+                   "precision": "FP64 positions and group-relative offsets, FP32 interactions, "
+                                "Kahan-compensated FP32 acceleration sums, FP64 potential/final sums"},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
+                     "frac": achieved / peak32, "traffic": read_profile_traffic(args.workload),
+                     "peak_source": "measured FP32 FMA-chain probe on this GPU (gt_measure_peaks), "
+                                    "not in MEASURED_PEAKS.json",
+                     "flops_per_interaction": FLOPS_PER_INTERACTION, "kernel": "walk_kernel",
+                     "kernel_ms": 1e3 * t_kernel, "fp64_peak_tflops": peak64},
+        "cpu_baseline": cpu_line,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "error": {"vs": "FP64 direct sum", "sample": int(len(sample)), "median": err_med, "p99": err_p99},
+        "interactions_per_particle": inter / nl,
+        "interactions_per_s": inter * world / t_step,
+        "walk_stats": {k: st[k] for k in ("groups", "nodes_visited", "multipole", "pairs", "max_stack")},
+        "build_ms": info["build_ms"],
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="clustered_16m")
+    ap.add_argument("--alpha", type=float, default=None)
+    ap.add_argument("--group", choices=["leaf", "node"], default="leaf")
+    ap.add_argument("--group-max", type=int, default=32)
+    ap.add_argument("--sample-seconds", type=float, default=8.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warm-up raised to 3 steps (timing rule)")
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,411 @@
+"""ctypes binding of libgt.so (include/gt.h), the B200 tree-gravity library.
+
+The binding is thin on purpose: every call goes straight to the C ABI that C/C++ callers use.
+Host numpy arrays go through ``GT_MEM_HOST`` (the library copies in and out); torch CUDA tensors go
+through ``GT_MEM_DEVICE`` with the context bound to torch's current stream, so library kernels and
+torch work are ordered on one stream.  There is no CPU fallback: importing this module on a
+machine where ``lib/libgt.so`` was not built raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgt.so")
+
+GT_OK = 0
+GT_MEM_HOST, GT_MEM_DEVICE = 0, 1
+GT_KEY_PEANO, GT_KEY_MORTON = 0, 1
+GT_GROUP_LEAF, GT_GROUP_BATCH, GT_GROUP_NODE, GT_GROUP_SINGLE = 0, 1, 2, 3
+GT_MAC_PLAIN, GT_MAC_LEARNED = 0, 1
+GT_DIRECT_FP64, GT_DIRECT_FP32 = 0, 1
+GT_OUT_TARGETS, GT_OUT_ORIGINAL = 0, 1
+
+STATUS = {0: "GT_OK", 1: "GT_ERR_INVALID", 2: "GT_ERR_CUDA", 3: "GT_ERR_NOMEM",
+          4: "GT_ERR_UNSUPPORTED", 5: "GT_ERR_OVERFLOW", 6: "GT_ERR_TIMEOUT",
+          7: "GT_ERR_NONFINITE", 8: "GT_ERR_DEVICE"}
+
+# exported symbols declared in include/gt.h
+EXPORTS = [
+    "gt_version", "gt_status_string", "gt_build_options_default", "gt_walk_options_default",
+    "gt_context_create", "gt_context_destroy", "gt_last_error", "gt_context_get_stream",
+    "gt_context_set_stream", "gt_synchronize", "gt_launch_count", "gt_build", "gt_tree_free",
+    "gt_tree_info_get", "gt_tree_download", "gt_tree_keys", "gt_accel_grouped", "gt_accel",
+    "gt_potential", "gt_walk_stats_get", "gt_form_aold", "gt_direct", "gt_peano_keys",
+    "gt_measure_peaks",
+]
+
+
+class GTError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class BuildOptions(C.Structure):
+    _fields_ = [("key_mode", C.c_int), ("leaf_max", C.c_int), ("max_level", C.c_int),
+                ("randomize_seed", C.c_longlong), ("nodelta", C.c_int), ("validate", C.c_int),
+                ("shift", C.c_double * 3)]
+
+
+class WalkOptions(C.Structure):
+    _fields_ = [("group_mode", C.c_int), ("group_max", C.c_int), ("mac", C.c_int),
+                ("out_order", C.c_int), ("async_", C.c_int), ("count", C.c_int),
+                ("block_warps", C.c_int), ("list_capacity", C.c_int),
+                ("stack_capacity", C.c_int), ("dtype_out_f32", C.c_int)]
+
+
+class TreeInfo(C.Structure):
+    _fields_ = [("n", C.c_int64), ("n_live", C.c_int64), ("n_nodes", C.c_int64),
+                ("n_levels", C.c_int32), ("root", C.c_int32), ("center", C.c_double * 3),
+                ("side", C.c_double), ("build_ms", C.c_double * 7)]
+
+
+class WalkStats(C.Structure):
+    _fields_ = [("groups", C.c_int64), ("nodes_visited", C.c_int64), ("multipole", C.c_int64),
+                ("pairs", C.c_int64), ("targets", C.c_int64), ("max_stack", C.c_int64),
+                ("list_flushes", C.c_int64), ("walk_ms", C.c_double)]
+
+
+class NodeArrays(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("cx", "cy", "cz", "mass", "size", "delta", "soft", "gcx",
+                                          "gcy", "gcz", "first", "next", "plo", "phi", "parent",
+                                          "level", "w_s", "w_len", "w_soft")]
+
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libgt.so, declaring every entry point; raises if it was not built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with __graft_entry__.build() "
+                           "(there is no CPU fallback)")
+    L = C.CDLL(path)
+    vp, i64, d = C.c_void_p, C.c_int64, C.c_double
+    L.gt_version.restype = C.c_int
+    L.gt_status_string.restype = C.c_char_p
+    L.gt_status_string.argtypes = [C.c_int]
+    L.gt_build_options_default.argtypes = [C.POINTER(BuildOptions)]
+    L.gt_walk_options_default.argtypes = [C.POINTER(WalkOptions)]
+    L.gt_context_create.argtypes = [C.c_int, C.POINTER(vp)]
+    L.gt_context_destroy.argtypes = [vp]
+    L.gt_last_error.restype = C.c_char_p
+    L.gt_last_error.argtypes = [vp]
+    L.gt_context_get_stream.argtypes = [vp, C.POINTER(vp)]
+    L.gt_context_set_stream.argtypes = [vp, vp]
+    L.gt_synchronize.argtypes = [vp]
+    L.gt_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
+    L.gt_build.argtypes = [vp, i64, vp, vp, vp, vp, vp, C.c_int, C.POINTER(BuildOptions), C.POINTER(vp)]
+    L.gt_tree_free.argtypes = [vp]
+    L.gt_tree_info_get.argtypes = [vp, C.POINTER(TreeInfo)]
+    L.gt_tree_download.argtypes = [vp, vp, vp, vp, vp, C.POINTER(NodeArrays)]
+    L.gt_tree_keys.argtypes = [vp, vp, vp]
+    L.gt_accel_grouped.argtypes = [vp, vp, i64, vp, vp, d, d, C.c_int, C.POINTER(WalkOptions),
+                                   C.c_int, vp, vp, vp, vp]
+    L.gt_accel.argtypes = [vp, vp, i64, vp, d, d, vp, C.c_int, vp, vp, vp]
+    L.gt_potential.argtypes = [vp, vp, i64, vp, d, d, vp, C.c_int, vp]
+    L.gt_walk_stats_get.argtypes = [vp, C.POINTER(WalkStats)]
+    L.gt_form_aold.argtypes = [vp, i64, vp, vp, vp, d, d, C.c_int, vp]
+    L.gt_direct.argtypes = [vp, i64, vp, vp, vp, vp, vp, i64, vp, d, C.c_int, C.c_int, vp, vp, vp, vp]
+    L.gt_peano_keys.argtypes = [vp, i64, vp, vp, vp, vp, d, C.c_int, C.c_int, vp, vp, vp, vp]
+    L.gt_measure_peaks.argtypes = [vp, C.POINTER(d), C.POINTER(d)]
+    for name in EXPORTS:
+        fn = getattr(L, name)
+        if fn.restype is C.c_int or fn.restype is None and name not in (
+                "gt_build_options_default", "gt_walk_options_default"):
+            fn.restype = C.c_int
+    L.gt_build_options_default.restype = None
+    L.gt_walk_options_default.restype = None
+    L.gt_last_error.restype = C.c_char_p
+    L.gt_status_string.restype = C.c_char_p
+    _LIB = L
+    return L
+
+
+def _ptr(a):
+    """Address of a numpy array or torch tensor (or None)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor
+
+
+def _is_dev(a):
+    return a is not None and not isinstance(a, np.ndarray) and getattr(a, "is_cuda", False)
+
+
+class Tree:
+    def __init__(self, ctx: "Context", handle):
+        self.ctx = ctx
+        self.h = handle
+
+    def free(self):
+        if self.h:
+            load_library().gt_tree_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        inf = TreeInfo()
+        self.ctx._check(load_library().gt_tree_info_get(self.h, C.byref(inf)))
+        return {"n": inf.n, "n_live": inf.n_live, "n_nodes": inf.n_nodes, "n_levels": inf.n_levels,
+                "center": tuple(inf.center), "side": inf.side,
+                "build_ms": dict(zip(("bbox", "keys", "sort", "structure", "moments", "pack", "total"),
+                                     list(inf.build_ms)))}
+
+    @property
+    def n_live(self):
+        return self.info()["n_live"]
+
+    def download(self, nodes=True):
+        inf = self.info()
+        n, nl, nn = inf["n"], inf["n_live"], inf["n_nodes"]
+        ob = np.empty(nl, np.uint32)
+        rank = np.empty(n, np.uint32)
+        leaf = np.empty(n, np.int32)
+        out = {"orderbuf": ob, "rank": rank, "leaf_of": leaf}
+        na = None
+        if nodes:
+            arr = {}
+            for k in ("cx", "cy", "cz", "mass", "size", "delta", "soft", "gcx", "gcy", "gcz", "w_s"):
+                arr[k] = np.empty(nn)
+            for k in ("first", "next", "plo", "phi", "parent", "level"):
+                arr[k] = np.empty(nn, np.int32)
+            arr["w_len"] = np.empty(nn, np.float32)
+            arr["w_soft"] = np.empty(nn, np.float32)
+            na = NodeArrays(**{k: v.ctypes.data for k, v in arr.items()})
+            out.update(arr)
+        L = load_library()
+        self.ctx._check(L.gt_tree_download(self.ctx.h, self.h, ob.ctypes.data, rank.ctypes.data,
+                                           leaf.ctypes.data, C.byref(na) if na else None))
+        return out
+
+    def keys(self):
+        nl = self.info()["n_live"]
+        k = np.empty(max(nl, 1), np.uint64)
+        self.ctx._check(load_library().gt_tree_keys(self.ctx.h, self.h, k.ctypes.data))
+        return k[:nl]
+
+
+class Context:
+    """One gt_context (device, stream, workspace)."""
+
+    def __init__(self, device: int = 0, torch_stream: bool = False):
+        L = load_library()
+        h = C.c_void_p()
+        st = L.gt_context_create(device, C.byref(h))
+        if st != GT_OK:
+            raise GTError(st, f"gt_context_create(device={device})")
+        self.h = h
+        self.device = device
+        if torch_stream:
+            self.bind_torch_stream()
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().gt_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != GT_OK:
+            msg = load_library().gt_last_error(self.h)
+            raise GTError(st, msg.decode() if msg else "")
+
+    def bind_torch_stream(self):
+        import torch
+
+        s = torch.cuda.current_stream(self.device)
+        self._check(load_library().gt_context_set_stream(self.h, C.c_void_p(s.cuda_stream)))
+
+    def synchronize(self):
+        self._check(load_library().gt_synchronize(self.h))
+
+    def launches(self) -> int:
+        c = C.c_uint64()
+        self._check(load_library().gt_launch_count(self.h, C.byref(c)))
+        return int(c.value)
+
+    def stats(self) -> dict:
+        s = WalkStats()
+        self._check(load_library().gt_walk_stats_get(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in WalkStats._fields_}
+
+    # ---- build -----------------------------------------------------------------------------
+    def build(self, P, key_mode=GT_KEY_PEANO, randomize_seed=-1, nodelta=False, leaf_max=16,
+              max_level=20, validate=True, shift=(0.0, 0.0, 0.0)) -> Tree:
+        o = BuildOptions()
+        load_library().gt_build_options_default(C.byref(o))
+        o.key_mode = key_mode
+        o.randomize_seed = randomize_seed
+        o.nodelta = int(nodelta)
+        o.leaf_max = leaf_max
+        o.max_level = max_level
+        o.validate = int(validate)
+        for k in range(3):
+            o.shift[k] = shift[k]
+        x, y, z, m = P["x"], P["y"], P["z"], P["m"]
+        soft = P.get("soft")
+        dev = _is_dev(x)
+        if not dev:
+            x, y, z, m = (np.ascontiguousarray(a, np.float64) for a in (x, y, z, m))
+            soft = None if soft is None else np.ascontiguousarray(soft, np.float64)
+        h = C.c_void_p()
+        self._check(load_library().gt_build(self.h, len(m), _ptr(x), _ptr(y), _ptr(z), _ptr(m),
+                                             _ptr(soft), GT_MEM_DEVICE if dev else GT_MEM_HOST,
+                                             C.byref(o), C.byref(h)))
+        return Tree(self, h)
+
+    # ---- walks -----------------------------------------------------------------------------
+    def _walk_opts(self, group_mode=GT_GROUP_LEAF, group_max=32, out_order=GT_OUT_TARGETS,
+                   count=False, block_warps=0, async_=False, mac=GT_MAC_PLAIN):
+        o = WalkOptions()
+        load_library().gt_walk_options_default(C.byref(o))
+        o.group_mode = group_mode
+        o.group_max = group_max
+        o.out_order = out_order
+        o.count = int(count)
+        o.block_warps = block_warps
+        o.async_ = int(async_)
+        o.mac = mac
+        return o
+
+    @staticmethod
+    def _targets(targets):
+        if targets is None:
+            return None, 0
+        if _is_dev(targets):
+            return targets, int(targets.numel())
+        t = np.ascontiguousarray(targets, np.uint32)
+        return t, len(t)
+
+    def _outs(self, nout, dev, want_acc=True, want_phi=False, like=None):
+        if dev:
+            import torch
+
+            mk = lambda: torch.empty(nout, dtype=torch.float64, device=like.device if like is not None
+                                     else f"cuda:{self.device}")
+        else:
+            mk = lambda: np.empty(max(nout, 1), np.float64)
+        ax = ay = az = phi = None
+        if want_acc:
+            ax, ay, az = mk(), mk(), mk()
+        if want_phi:
+            phi = mk()
+        return ax, ay, az, phi
+
+    def accel_grouped(self, tree: Tree, targets=None, aold=None, theta=0.0, G=1.0, batch=0,
+                      want_phi=False, device_out=False, outs=None, **opts):
+        t, nt = self._targets(targets)
+        dev = _is_dev(t) or _is_dev(aold) or device_out or (outs is not None and _is_dev(outs[0]))
+        if t is None:
+            nt = tree.info()["n_live"] if opts.get("out_order", 0) == GT_OUT_TARGETS else tree.info()["n"]
+        o = self._walk_opts(**opts)
+        if outs is None:
+            ax, ay, az, phi = self._outs(nt, dev, True, want_phi)
+        else:
+            ax, ay, az, phi = outs
+        if not dev and aold is not None:
+            aold = np.ascontiguousarray(aold, np.float64)
+        self._check(load_library().gt_accel_grouped(
+            self.h, tree.h, nt if targets is not None else 0, _ptr(t), _ptr(aold), theta, G, batch,
+            C.byref(o), GT_MEM_DEVICE if dev else GT_MEM_HOST, _ptr(ax), _ptr(ay), _ptr(az), _ptr(phi)))
+        if not dev:
+            ax, ay, az = ax[:nt], ay[:nt], az[:nt]
+            phi = phi[:nt] if phi is not None else None
+        return (ax, ay, az, phi) if want_phi else (ax, ay, az)
+
+    def accel(self, tree: Tree, targets=None, theta=0.0, G=1.0, aold=None):
+        t, nt = self._targets(targets)
+        if t is None:
+            nt = tree.info()["n_live"]
+        dev = _is_dev(t)
+        ax, ay, az, _ = self._outs(nt, dev)
+        if not dev and aold is not None:
+            aold = np.ascontiguousarray(aold, np.float64)
+        self._check(load_library().gt_accel(self.h, tree.h, nt if targets is not None else 0, _ptr(t),
+                                            theta, G, _ptr(aold), GT_MEM_DEVICE if dev else GT_MEM_HOST,
+                                            _ptr(ax), _ptr(ay), _ptr(az)))
+        return (ax[:nt], ay[:nt], az[:nt]) if not dev else (ax, ay, az)
+
+    def potential(self, tree: Tree, targets=None, theta=0.0, G=1.0, aold=None):
+        t, nt = self._targets(targets)
+        if t is None:
+            nt = tree.info()["n_live"]
+        dev = _is_dev(t)
+        _, _, _, phi = self._outs(nt, dev, False, True)
+        if not dev and aold is not None:
+            aold = np.ascontiguousarray(aold, np.float64)
+        self._check(load_library().gt_potential(self.h, tree.h, nt if targets is not None else 0,
+                                                _ptr(t), theta, G, _ptr(aold),
+                                                GT_MEM_DEVICE if dev else GT_MEM_HOST, _ptr(phi)))
+        return phi[:nt] if not dev else phi
+
+    def form_aold(self, ax, ay, az, alpha, G=1.0):
+        dev = _is_dev(ax)
+        n = int(ax.numel()) if dev else len(ax)
+        if dev:
+            import torch
+
+            out = torch.empty(n, dtype=torch.float64, device=ax.device)
+        else:
+            ax, ay, az = (np.ascontiguousarray(a, np.float64) for a in (ax, ay, az))
+            out = np.empty(max(n, 1))
+        self._check(load_library().gt_form_aold(self.h, n, _ptr(ax), _ptr(ay), _ptr(az), alpha, G,
+                                                GT_MEM_DEVICE if dev else GT_MEM_HOST, _ptr(out)))
+        return out if dev else out[:n]
+
+    def direct(self, P, targets, G=1.0, precision=GT_DIRECT_FP64, want_phi=True):
+        x, y, z, m = P["x"], P["y"], P["z"], P["m"]
+        soft = P.get("soft")
+        dev = _is_dev(x)
+        if not dev:
+            x, y, z, m = (np.ascontiguousarray(a, np.float64) for a in (x, y, z, m))
+            soft = None if soft is None else np.ascontiguousarray(soft, np.float64)
+        t, nt = self._targets(targets)
+        if dev and not _is_dev(t):
+            import torch
+
+            t = torch.as_tensor(np.asarray(t, np.uint32).view(np.int32), device=x.device)
+        ax, ay, az, phi = self._outs(nt, dev, True, want_phi)
+        n = int(m.numel()) if dev else len(m)
+        self._check(load_library().gt_direct(self.h, n, _ptr(x), _ptr(y), _ptr(z), _ptr(m),
+                                             _ptr(soft), nt, _ptr(t), G, precision,
+                                             GT_MEM_DEVICE if dev else GT_MEM_HOST, _ptr(ax),
+                                             _ptr(ay), _ptr(az), _ptr(phi)))
+        if not dev:
+            ax, ay, az = ax[:nt], ay[:nt], az[:nt]
+            phi = phi[:nt] if phi is not None else None
+        return (ax, ay, az, phi) if want_phi else (ax, ay, az)
+
+    def measure_peaks(self):
+        a, b = C.c_double(), C.c_double()
+        self._check(load_library().gt_measure_peaks(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def peano_keys(self, x, y, z, corner, length, bits=42):
+        x, y, z = (np.ascontiguousarray(a, np.float64) for a in (x, y, z))
+        n = len(x)
+        outs = [np.empty(max(n, 1), np.uint64) for _ in range(4)]
+        c = (C.c_double * 3)(*corner)
+        self._check(load_library().gt_peano_keys(self.h, n, _ptr(x), _ptr(y), _ptr(z), c, length,
+                                                 bits, GT_MEM_HOST, *[_ptr(o) for o in outs]))
+        return [o[:n] for o in outs]

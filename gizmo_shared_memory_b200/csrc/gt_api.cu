@@ -1,0 +1,591 @@
+// C ABI of libgt (include/gt.h): argument checking, host<->device staging, error capture.
+//
+// Every entry point runs its body inside guarded(): CUDA errors and allocation failures become a
+// gt_status plus a message on the context, never an exit() (the reference's CUDA entry exits on a
+// launch error, shmem/grav_cuda.cu:239-243).
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "gt_internal.cuh"
+
+namespace gt {
+
+void set_error(gt_context* ctx, int status, const std::string& msg) {
+    if (ctx) ctx->last_error = std::string(gt_status_string(status)) + ": " + msg;
+}
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Fail{e == cudaErrorMemoryAllocation ? GT_ERR_NOMEM : GT_ERR_CUDA,
+                   std::string(what) + ": " + cudaGetErrorString(e)};
+    }
+}
+
+void check_launch(gt_context* ctx, const char* what) {
+    ++ctx->launches;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw Fail{GT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+void* scratch(gt_context* ctx, Slot s, size_t bytes) {
+    if ((int)ctx->scratch.size() < kSlotCount) ctx->scratch.resize(kSlotCount);
+    DevBuf& b = ctx->scratch[s];
+    bytes = std::max<size_t>(bytes, 4096);
+    if (b.bytes >= bytes) return b.ptr;
+    if (b.ptr) {
+        // a smaller buffer may still be read by queued work: wait for the stream before freeing
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(b.ptr);
+        b.ptr = nullptr;
+        b.bytes = 0;
+    }
+    const size_t want = bytes + bytes / 8;
+    const cudaError_t e = cudaMalloc(&b.ptr, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.ptr = nullptr;
+        throw Fail{GT_ERR_NOMEM, "workspace allocation of " + std::to_string(want) + " bytes failed"};
+    }
+    b.bytes = want;
+    return b.ptr;
+}
+
+}  // namespace gt
+
+using namespace gt;
+
+namespace {
+
+template <typename F>
+int guarded(gt_context* ctx, F&& body) {
+    try {
+        body();
+        if (ctx) ctx->last_error.clear();
+        return GT_OK;
+    } catch (const Fail& f) {
+        set_error(ctx, f.status, f.msg);
+        return f.status;
+    } catch (const std::bad_alloc&) {
+        set_error(ctx, GT_ERR_NOMEM, "host allocation failed");
+        return GT_ERR_NOMEM;
+    } catch (...) {
+        set_error(ctx, GT_ERR_CUDA, "unexpected exception");
+        return GT_ERR_CUDA;
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) check_cuda(cudaSetDevice(dev), "cudaSetDevice");
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// Device view of an input array: the pointer itself for GT_MEM_DEVICE, else a staged copy.
+template <typename T>
+const T* stage_in(gt_context* ctx, Slot s, const T* p, int64_t n, int mem) {
+    if (!p) return nullptr;
+    if (mem == GT_MEM_DEVICE) return p;
+    T* d = (T*)scratch(ctx, s, (size_t)std::max<int64_t>(n, 1) * sizeof(T));
+    if (n > 0)
+        check_cuda(cudaMemcpyAsync(d, p, (size_t)n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    return d;
+}
+
+template <typename T>
+T* out_buf(gt_context* ctx, Slot s, T* p, int64_t n, int mem) {
+    if (!p) return nullptr;
+    if (mem == GT_MEM_DEVICE) return p;
+    return (T*)scratch(ctx, s, (size_t)std::max<int64_t>(n, 1) * sizeof(T));
+}
+
+template <typename T>
+void copy_out(gt_context* ctx, T* host, const T* dev, int64_t n, int mem) {
+    if (!host || mem == GT_MEM_DEVICE || n <= 0) return;
+    check_cuda(cudaMemcpyAsync(host, dev, (size_t)n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+}
+
+void check_mem(int mem) {
+    if (mem != GT_MEM_HOST && mem != GT_MEM_DEVICE) throw Fail{GT_ERR_INVALID, "mem must be GT_MEM_HOST or GT_MEM_DEVICE"};
+}
+
+void free_tree_arrays(gt_tree* t) {
+    void* ptrs[] = {t->src, t->ssoft, t->smass, t->order, t->rank, t->leaf_of, t->sleaf, t->skey,
+                    t->nodes, t->parent, t->next, t->level, t->size, t->delta, t->nsoft, t->gc};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (auto& c : t->group_cache)
+        if (c.groups) cudaFree(c.groups);
+    t->group_cache.clear();
+}
+
+void finish(gt_context* ctx, bool sync) {
+    if (sync) check_cuda(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+}
+
+void record_walk_time(gt_context* ctx) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.walk_ms = ms;
+    cudaGetLastError();
+}
+
+void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
+                 const double* aold, double theta, double G, int group_mode, int group_param,
+                 bool leaf_accept, const gt_walk_options* opt, int mem, double* ax, double* ay,
+                 double* az, double* phi) {
+    if (!ctx || !tree) throw Fail{GT_ERR_INVALID, "null context or tree"};
+    check_mem(mem);
+    if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "tree and context are on different devices"};
+    if (n_targets < 0) throw Fail{GT_ERR_INVALID, "n_targets < 0"};
+    gt_walk_options o;
+    gt_walk_options_default(&o);
+    if (opt) o = *opt;
+    if (o.mac != GT_MAC_PLAIN && o.mac != GT_MAC_LEARNED) throw Fail{GT_ERR_INVALID, "unknown mac"};
+    if (o.mac == GT_MAC_LEARNED) throw Fail{GT_ERR_UNSUPPORTED, "no learned criterion is loaded"};
+    if (o.dtype_out_f32 != 0) throw Fail{GT_ERR_INVALID, "dtype_out_f32 is reserved"};
+    if (o.out_order == GT_OUT_ORIGINAL && targets) throw Fail{GT_ERR_INVALID, "GT_OUT_ORIGINAL needs targets == NULL"};
+    DeviceGuard dg(ctx->device);
+    const bool all = targets == nullptr;
+    const int64_t nt = all ? tree->n_live : n_targets;
+    const int64_t nout = (all && o.out_order == GT_OUT_ORIGINAL) ? tree->n : nt;
+    if (!all && nt > 0 && !targets) throw Fail{GT_ERR_INVALID, "targets is null"};
+    if (!all) {
+        // host-side range check of target indices: a bad index would read out of bounds
+        if (mem == GT_MEM_HOST) {
+            for (int64_t k = 0; k < nt; ++k)
+                if ((int64_t)targets[k] >= tree->n) throw Fail{GT_ERR_INVALID, "target index out of range"};
+        }
+    }
+    WalkRequest rq;
+    rq.targets = all ? nullptr : stage_in(ctx, kSlotIn0, targets, nt, mem);
+    rq.n_targets = nt;
+    rq.aold = stage_in(ctx, kSlotIn1, aold, nt, mem);
+    rq.theta = theta;
+    rq.G = G;
+    rq.group_mode = group_mode;
+    rq.group_param = group_param;
+    rq.leaf_accept = leaf_accept;
+    rq.want_acc = ax != nullptr;
+    rq.want_phi = phi != nullptr;
+    rq.out_original = all && o.out_order == GT_OUT_ORIGINAL;
+    rq.mac = o.mac;
+    rq.count = o.count != 0;
+    rq.block_warps = o.block_warps;
+    rq.list_capacity = o.list_capacity;
+    rq.stack_capacity = o.stack_capacity;
+    if ((ax == nullptr) != (ay == nullptr) || (ax == nullptr) != (az == nullptr))
+        throw Fail{GT_ERR_INVALID, "ax, ay, az must all be given or all be null"};
+    if (!ax && !phi) return;
+    rq.ax = out_buf(ctx, kSlotOut0, ax, nout, mem);
+    rq.ay = out_buf(ctx, kSlotOut1, ay, nout, mem);
+    rq.az = out_buf(ctx, kSlotOut2, az, nout, mem);
+    rq.phi = out_buf(ctx, kSlotOut3, phi, nout, mem);
+    if (rq.out_original && nout > nt) {
+        // massless particles are not walked; their outputs are defined as 0
+        for (double* p : {rq.ax, rq.ay, rq.az, rq.phi})
+            if (p) check_cuda(cudaMemsetAsync(p, 0, (size_t)nout * 8, ctx->stream), "memset");
+    }
+    run_walk(ctx, tree, rq);
+    copy_out(ctx, ax, rq.ax, nout, mem);
+    copy_out(ctx, ay, rq.ay, nout, mem);
+    copy_out(ctx, az, rq.az, nout, mem);
+    copy_out(ctx, phi, rq.phi, nout, mem);
+    const bool sync = mem == GT_MEM_HOST || !o.async;
+    finish(ctx, sync);
+    if (sync) record_walk_time(ctx);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gt_version(void) { return GT_VERSION; }
+
+const char* gt_status_string(int s) {
+    switch (s) {
+        case GT_OK: return "GT_OK";
+        case GT_ERR_INVALID: return "GT_ERR_INVALID";
+        case GT_ERR_CUDA: return "GT_ERR_CUDA";
+        case GT_ERR_NOMEM: return "GT_ERR_NOMEM";
+        case GT_ERR_UNSUPPORTED: return "GT_ERR_UNSUPPORTED";
+        case GT_ERR_OVERFLOW: return "GT_ERR_OVERFLOW";
+        case GT_ERR_TIMEOUT: return "GT_ERR_TIMEOUT";
+        case GT_ERR_NONFINITE: return "GT_ERR_NONFINITE";
+        case GT_ERR_DEVICE: return "GT_ERR_DEVICE";
+        default: return "GT_ERR_UNKNOWN";
+    }
+}
+
+void gt_build_options_default(gt_build_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->key_mode = GT_KEY_PEANO;
+    o->leaf_max = 16;
+    o->max_level = 20;
+    o->randomize_seed = -1;
+    o->nodelta = 0;
+    o->validate = 1;
+}
+
+void gt_walk_options_default(gt_walk_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->group_mode = GT_GROUP_LEAF;
+    o->group_max = 32;
+    o->mac = GT_MAC_PLAIN;
+    o->out_order = GT_OUT_TARGETS;
+}
+
+int gt_context_create(int device, gt_context** out) {
+    if (!out) return GT_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return GT_ERR_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return GT_ERR_DEVICE;
+    gt_context* ctx = new gt_context();
+    ctx->device = device;
+    const int st = guarded(ctx, [&] {
+        DeviceGuard dg(device);
+        cudaDeviceProp prop;
+        check_cuda(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+        ctx->num_sms = prop.multiProcessorCount;
+        check_cuda(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ctx->own_stream = true;
+        check_cuda(cudaMallocHost(&ctx->pinned, 4096), "cudaMallocHost");
+        check_cuda(cudaEventCreate(&ctx->ev0), "cudaEventCreate");
+        check_cuda(cudaEventCreate(&ctx->ev1), "cudaEventCreate");
+        ctx->scratch.resize(kSlotCount);
+    });
+    if (st != GT_OK) {
+        gt_context_destroy(ctx);
+        return st;
+    }
+    *out = ctx;
+    return GT_OK;
+}
+
+int gt_context_destroy(gt_context* ctx) {
+    if (!ctx) return GT_ERR_INVALID;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& b : ctx->scratch)
+        if (b.ptr) cudaFree(b.ptr);
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    cudaGetLastError();
+    if (prev >= 0) cudaSetDevice(prev);
+    delete ctx;
+    return GT_OK;
+}
+
+const char* gt_last_error(const gt_context* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int gt_context_get_stream(gt_context* ctx, void** stream) {
+    if (!ctx || !stream) return GT_ERR_INVALID;
+    *stream = (void*)ctx->stream;
+    return GT_OK;
+}
+
+int gt_context_set_stream(gt_context* ctx, void* stream) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        DeviceGuard dg(ctx->device);
+        check_cuda(cudaStreamSynchronize(ctx->stream), "sync");
+        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+        ctx->stream = (cudaStream_t)stream;
+        ctx->own_stream = false;
+    });
+}
+
+int gt_synchronize(gt_context* ctx) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        DeviceGuard dg(ctx->device);
+        check_cuda(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+    });
+}
+
+int gt_launch_count(const gt_context* ctx, uint64_t* count) {
+    if (!ctx || !count) return GT_ERR_INVALID;
+    *count = ctx->launches;
+    return GT_OK;
+}
+
+int gt_build(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
+             const double* m, const double* soft, int mem, const gt_build_options* opt,
+             gt_tree** out) {
+    if (!ctx || !out) return GT_ERR_INVALID;
+    *out = nullptr;
+    gt_tree* t = new gt_tree();
+    const int st = guarded(ctx, [&] {
+        check_mem(mem);
+        if (n < 0) throw Fail{GT_ERR_INVALID, "n < 0"};
+        if (n > 0 && (!x || !y || !z || !m)) throw Fail{GT_ERR_INVALID, "null particle array"};
+        if (n >= (int64_t)INT32_MAX) throw Fail{GT_ERR_INVALID, "n must be below 2^31"};
+        gt_build_options o;
+        gt_build_options_default(&o);
+        if (opt) o = *opt;
+        if (o.key_mode != GT_KEY_PEANO && o.key_mode != GT_KEY_MORTON) throw Fail{GT_ERR_INVALID, "unknown key_mode"};
+        if (o.leaf_max < 1) throw Fail{GT_ERR_INVALID, "leaf_max < 1"};
+        if (o.max_level < 1 || o.max_level > 20) throw Fail{GT_ERR_INVALID, "max_level must be in [1, 20]"};
+        DeviceGuard dg(ctx->device);
+        t->device = ctx->device;
+        t->n = n;
+        t->opt = o;
+        const double* dx = stage_in(ctx, kSlotIn0, x, n, mem);
+        const double* dy = stage_in(ctx, kSlotIn1, y, n, mem);
+        const double* dz = stage_in(ctx, kSlotIn2, z, n, mem);
+        const double* dm = stage_in(ctx, kSlotIn3, m, n, mem);
+        const double* ds = stage_in(ctx, kSlotIn4, soft, n, mem);
+        build_tree(ctx, t, dx, dy, dz, dm, ds);
+        finish(ctx, true);
+    });
+    if (st != GT_OK) {
+        free_tree_arrays(t);
+        delete t;
+        return st;
+    }
+    *out = t;
+    return GT_OK;
+}
+
+int gt_tree_free(gt_tree* t) {
+    if (!t) return GT_ERR_INVALID;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(t->device);
+    cudaDeviceSynchronize();
+    free_tree_arrays(t);
+    cudaGetLastError();
+    if (prev >= 0) cudaSetDevice(prev);
+    delete t;
+    return GT_OK;
+}
+
+int gt_tree_info_get(const gt_tree* t, gt_tree_info* info) {
+    if (!t || !info) return GT_ERR_INVALID;
+    std::memset(info, 0, sizeof(*info));
+    info->n = t->n;
+    info->n_live = t->n_live;
+    info->n_nodes = t->n_nodes;
+    info->n_levels = t->n_levels;
+    info->root = 0;
+    info->center[0] = t->geom.cx;
+    info->center[1] = t->geom.cy;
+    info->center[2] = t->geom.cz;
+    info->side = t->geom.side;
+    for (int k = 0; k < 7; ++k) info->build_ms[k] = t->build_ms[k];
+    return GT_OK;
+}
+
+int gt_tree_download(gt_context* ctx, const gt_tree* t, uint32_t* orderbuf, uint32_t* rank,
+                     int32_t* leaf_of, const gt_node_arrays* nd) {
+    if (!ctx || !t) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        DeviceGuard dg(ctx->device);
+        cudaStream_t st = ctx->stream;
+        const int64_t n = t->n, nl = t->n_live, nn = t->n_nodes;
+        if (orderbuf && nl > 0)
+            check_cuda(cudaMemcpyAsync(orderbuf, t->order, (size_t)nl * 4, cudaMemcpyDeviceToHost, st), "D2H");
+        if (rank && n > 0)
+            check_cuda(cudaMemcpyAsync(rank, t->rank, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "D2H");
+        if (leaf_of && n > 0)
+            check_cuda(cudaMemcpyAsync(leaf_of, t->leaf_of, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "D2H");
+        std::vector<GNode> hn;
+        std::vector<double> hgc;
+        if (nd) {
+            hn.resize((size_t)nn);
+            check_cuda(cudaMemcpyAsync(hn.data(), t->nodes, (size_t)nn * sizeof(GNode), cudaMemcpyDeviceToHost, st), "D2H");
+            auto cp = [&](void* dst, const void* src, size_t bytes) {
+                if (dst) check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st), "D2H");
+            };
+            cp(nd->size, t->size, (size_t)nn * 8);
+            cp(nd->delta, t->delta, (size_t)nn * 8);
+            cp(nd->soft, t->nsoft, (size_t)nn * 8);
+            cp(nd->next, t->next, (size_t)nn * 4);
+            cp(nd->parent, t->parent, (size_t)nn * 4);
+            cp(nd->level, t->level, (size_t)nn * 4);
+            if (nd->gcx || nd->gcy || nd->gcz) {
+                hgc.resize((size_t)nn * 3);
+                check_cuda(cudaMemcpyAsync(hgc.data(), t->gc, (size_t)nn * 24, cudaMemcpyDeviceToHost, st), "D2H");
+            }
+        }
+        check_cuda(cudaStreamSynchronize(st), "sync");
+        if (rank)  // the reference marks massless particles with UINT32_MAX
+            for (int64_t i = 0; i < n; ++i)
+                if ((int64_t)rank[i] >= nl) rank[i] = UINT32_MAX;
+        if (nd) {
+            for (int64_t i = 0; i < nn; ++i) {
+                const GNode& g = hn[(size_t)i];
+                if (nd->cx) nd->cx[i] = g.cx;
+                if (nd->cy) nd->cy[i] = g.cy;
+                if (nd->cz) nd->cz[i] = g.cz;
+                if (nd->mass) nd->mass[i] = g.mass;
+                if (nd->first) nd->first[i] = g.first;
+                if (nd->plo) nd->plo[i] = g.plo;
+                if (nd->phi) nd->phi[i] = g.phi;
+                if (nd->w_s) nd->w_s[i] = g.s;
+                if (nd->w_len) nd->w_len[i] = g.len;
+                if (nd->w_soft) nd->w_soft[i] = g.soft;
+                if (nd->gcx) nd->gcx[i] = hgc[3 * i];
+                if (nd->gcy) nd->gcy[i] = hgc[3 * i + 1];
+                if (nd->gcz) nd->gcz[i] = hgc[3 * i + 2];
+            }
+        }
+    });
+}
+
+int gt_tree_keys(gt_context* ctx, const gt_tree* t, uint64_t* keys) {
+    if (!ctx || !t || !keys) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        DeviceGuard dg(ctx->device);
+        if (t->n_live > 0)
+            check_cuda(cudaMemcpyAsync(keys, t->skey, (size_t)t->n_live * 8, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        finish(ctx, true);
+    });
+}
+
+int gt_accel_grouped(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
+                     const double* aold, double theta, double G, int batch, const gt_walk_options* opt,
+                     int mem, double* ax, double* ay, double* az, double* phi) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        gt_walk_options o;
+        gt_walk_options_default(&o);
+        if (opt) o = *opt;
+        int mode = o.group_mode, param = 0;
+        if (mode == GT_GROUP_LEAF && batch > 0) mode = GT_GROUP_BATCH;
+        if (mode == GT_GROUP_BATCH) param = batch > 0 ? batch : 8;
+        if (mode == GT_GROUP_NODE) param = o.group_max;
+        if (mode < GT_GROUP_LEAF || mode > GT_GROUP_SINGLE) throw Fail{GT_ERR_INVALID, "unknown group_mode"};
+        walk_common(ctx, tree, n_targets, targets, aold, theta, G, mode, param, true, &o, mem, ax, ay, az, phi);
+    });
+}
+
+int gt_accel(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
+             double theta, double G, const double* aold, int mem, double* ax, double* ay, double* az) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        walk_common(ctx, tree, n_targets, targets, aold, theta, G, GT_GROUP_SINGLE, 0, false, nullptr,
+                    mem, ax, ay, az, nullptr);
+    });
+}
+
+int gt_potential(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
+                 double theta, double G, const double* aold, int mem, double* phi) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        if (!phi) throw Fail{GT_ERR_INVALID, "phi is null"};
+        walk_common(ctx, tree, n_targets, targets, aold, theta, G, GT_GROUP_SINGLE, 0, false, nullptr,
+                    mem, nullptr, nullptr, nullptr, phi);
+    });
+}
+
+int gt_walk_stats_get(const gt_context* ctx, gt_walk_stats* s) {
+    if (!ctx || !s) return GT_ERR_INVALID;
+    *s = ctx->stats;
+    return GT_OK;
+}
+
+int gt_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay, const double* az,
+                 double alpha, double G, int mem, double* aold) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (n < 0 || (n > 0 && (!ax || !ay || !az || !aold))) throw Fail{GT_ERR_INVALID, "bad arguments"};
+        if (!(G != 0.0)) throw Fail{GT_ERR_INVALID, "G must be non-zero"};
+        DeviceGuard dg(ctx->device);
+        const double* dx = stage_in(ctx, kSlotIn0, ax, n, mem);
+        const double* dy = stage_in(ctx, kSlotIn1, ay, n, mem);
+        const double* dz = stage_in(ctx, kSlotIn2, az, n, mem);
+        double* o = out_buf(ctx, kSlotOut0, aold, n, mem);
+        run_form_aold(ctx, n, dx, dy, dz, alpha, G, o);
+        copy_out(ctx, aold, (const double*)o, n, mem);
+        finish(ctx, true);
+    });
+}
+
+int gt_direct(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
+              const double* m, const double* soft, int64_t n_targets, const uint32_t* targets,
+              double G, int precision, int mem, double* ax, double* ay, double* az, double* phi) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (n < 0 || n_targets < 0) throw Fail{GT_ERR_INVALID, "negative size"};
+        if (n > 0 && (!x || !y || !z || !m)) throw Fail{GT_ERR_INVALID, "null source array"};
+        if (n_targets > 0 && !targets) throw Fail{GT_ERR_INVALID, "null targets"};
+        if (precision != GT_DIRECT_FP64 && precision != GT_DIRECT_FP32) throw Fail{GT_ERR_INVALID, "unknown precision"};
+        if (mem == GT_MEM_HOST)
+            for (int64_t k = 0; k < n_targets; ++k)
+                if ((int64_t)targets[k] >= n) throw Fail{GT_ERR_INVALID, "target index out of range"};
+        DeviceGuard dg(ctx->device);
+        const double* dx = stage_in(ctx, kSlotIn0, x, n, mem);
+        const double* dy = stage_in(ctx, kSlotIn1, y, n, mem);
+        const double* dz = stage_in(ctx, kSlotIn2, z, n, mem);
+        const double* dm = stage_in(ctx, kSlotIn3, m, n, mem);
+        const double* ds = stage_in(ctx, kSlotIn4, soft, n, mem);
+        const uint32_t* dt = stage_in(ctx, kSlotTargets, targets, n_targets, mem);
+        double* oax = out_buf(ctx, kSlotOut0, ax, n_targets, mem);
+        double* oay = out_buf(ctx, kSlotOut1, ay, n_targets, mem);
+        double* oaz = out_buf(ctx, kSlotOut2, az, n_targets, mem);
+        double* oph = out_buf(ctx, kSlotOut3, phi, n_targets, mem);
+        run_direct(ctx, n, dx, dy, dz, dm, ds, n_targets, dt, G, precision, oax, oay, oaz, oph);
+        copy_out(ctx, ax, (const double*)oax, n_targets, mem);
+        copy_out(ctx, ay, (const double*)oay, n_targets, mem);
+        copy_out(ctx, az, (const double*)oaz, n_targets, mem);
+        copy_out(ctx, phi, (const double*)oph, n_targets, mem);
+        finish(ctx, true);
+    });
+}
+
+int gt_peano_keys(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
+                  const double corner[3], double len, int bits, int mem, uint64_t* ph_hi,
+                  uint64_t* ph_lo, uint64_t* mo_hi, uint64_t* mo_lo) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (n < 0 || !corner || !(len > 0)) throw Fail{GT_ERR_INVALID, "bad arguments"};
+        if (bits < 1 || bits > 42) throw Fail{GT_ERR_INVALID, "bits must be in [1, 42]"};
+        if (n > 0 && (!x || !y || !z)) throw Fail{GT_ERR_INVALID, "null coordinate array"};
+        DeviceGuard dg(ctx->device);
+        const double* dx = stage_in(ctx, kSlotIn0, x, n, mem);
+        const double* dy = stage_in(ctx, kSlotIn1, y, n, mem);
+        const double* dz = stage_in(ctx, kSlotIn2, z, n, mem);
+        uint64_t* a = out_buf(ctx, kSlotOut0, ph_hi, n, mem);
+        uint64_t* b = out_buf(ctx, kSlotOut1, ph_lo, n, mem);
+        uint64_t* c = out_buf(ctx, kSlotOut2, mo_hi, n, mem);
+        uint64_t* d = out_buf(ctx, kSlotOut3, mo_lo, n, mem);
+        run_peano_keys(ctx, n, dx, dy, dz, corner, len, bits, a, b, c, d);
+        copy_out(ctx, ph_hi, (const uint64_t*)a, n, mem);
+        copy_out(ctx, ph_lo, (const uint64_t*)b, n, mem);
+        copy_out(ctx, mo_hi, (const uint64_t*)c, n, mem);
+        copy_out(ctx, mo_lo, (const uint64_t*)d, n, mem);
+        finish(ctx, true);
+    });
+}
+
+int gt_measure_peaks(gt_context* ctx, double* fp32_tflops, double* fp64_tflops) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        DeviceGuard dg(ctx->device);
+        run_peaks(ctx, fp32_tflops, fp64_tflops);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,578 @@
+// Tree build on the device: the replacement for shmem::build (shmem/tree.cc:350-526).
+//
+// Stages (each a handful of kernels on the context stream):
+//   1. bbox       grid-stride min/max over live particles, one block finishes the root cell
+//                 exactly as tree.cc:361-417 does (centre, side*1.0000001, optional randomised or
+//                 shifted root, 20-bit scale).
+//   2. keys       20-bit-per-axis quantisation of tree.cc:409-417, then a Peano-Hilbert key
+//                 (system/peano.cc:297-313 state machine) or the shmem Morton key (tree.h:161-173).
+//                 Massless particles get a key above every live key and sort last.
+//   3. sort       stable LSD radix sort of (key, particle index) (gt_scan.cu).
+//   4. gather     particles into tree order: 32-byte SrcP records (FP64 position, FP32 mass and
+//                 softening) plus FP64 mass/softening for the moments and the opening test.
+//   5. structure  level-synchronous split: one thread per node binary-searches its key range for
+//                 the 8 digit boundaries of the next level (a leaf at <= leaf_max particles or at
+//                 max_level, tree.cc:89); a scan over child counts places every node's children
+//                 contiguously in the next level (BFS order).  Child centres are parent +-
+//                 side/4 by the child's octant bits, as tree.cc:116-118.
+//   6. moments    deepest level first, one warp per node: a leaf reduces its particles, an
+//                 interior node its children, with warp shuffles (mass, mass-weighted position,
+//                 max softening), then COM, delta = |COM - centre| and the packed walk node
+//                 (tree.cc:145-196, 507-523).
+// The next/first threading of the reference (tree.cc:340-348) is produced alongside for the host
+// download; the GPU walk itself only uses the contiguous child ranges.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+
+#include "gt_internal.cuh"
+#include "gt_ph_table.cuh"
+
+namespace gt {
+namespace {
+
+constexpr int kBlk = 256;
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_min_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// ---- 1. bbox ---------------------------------------------------------------------------------
+__global__ void bbox_partial_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                    const double* __restrict__ z, const double* __restrict__ m,
+                                    const double* __restrict__ soft, int64_t n,
+                                    double* __restrict__ part, unsigned long long* __restrict__ cnt) {
+    double lo0 = 1e300, lo1 = 1e300, lo2 = 1e300, hi0 = -1e300, hi1 = -1e300, hi2 = -1e300;
+    unsigned long long live = 0, bad = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double xi = x[i], yi = y[i], zi = z[i], mi = m[i];
+        const double si = soft ? soft[i] : 0.0;
+        if (!isfinite(xi) || !isfinite(yi) || !isfinite(zi) || !isfinite(mi) || !isfinite(si)) ++bad;
+        if (!(mi > 0)) continue;
+        ++live;
+        lo0 = fmin(lo0, xi); hi0 = fmax(hi0, xi);
+        lo1 = fmin(lo1, yi); hi1 = fmax(hi1, yi);
+        lo2 = fmin(lo2, zi); hi2 = fmax(hi2, zi);
+    }
+    lo0 = warp_min_d(lo0); lo1 = warp_min_d(lo1); lo2 = warp_min_d(lo2);
+    hi0 = warp_max_d(hi0); hi1 = warp_max_d(hi1); hi2 = warp_max_d(hi2);
+    __shared__ double sh[8][6];
+    __shared__ unsigned long long sc[8][2];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        live += __shfl_xor_sync(0xffffffffu, live, o);
+        bad += __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if (lane == 0) {
+        sh[w][0] = lo0; sh[w][1] = lo1; sh[w][2] = lo2; sh[w][3] = hi0; sh[w][4] = hi1; sh[w][5] = hi2;
+        sc[w][0] = live; sc[w][1] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+            for (int c = 0; c < 3; ++c) sh[0][c] = fmin(sh[0][c], sh[k][c]);
+            for (int c = 3; c < 6; ++c) sh[0][c] = fmax(sh[0][c], sh[k][c]);
+            sc[0][0] += sc[k][0]; sc[0][1] += sc[k][1];
+        }
+        for (int c = 0; c < 6; ++c) part[blockIdx.x * 6 + c] = sh[0][c];
+        cnt[blockIdx.x * 2 + 0] = sc[0][0];
+        cnt[blockIdx.x * 2 + 1] = sc[0][1];
+    }
+}
+
+// Root cell, tree.cc:361-417.  Runs as one thread: it is a handful of flops.
+__global__ void root_geom_kernel(const double* __restrict__ part, const unsigned long long* __restrict__ cnt,
+                                 int nb, RootGeom* __restrict__ g, unsigned long long* __restrict__ bad_out,
+                                 long long seed, double fx, double fy, double fz, int max_level) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    unsigned long long live = 0, bad = 0;
+    for (int b = 0; b < nb; ++b) {
+        for (int c = 0; c < 3; ++c) {
+            lo[c] = fmin(lo[c], part[b * 6 + c]);
+            hi[c] = fmax(hi[c], part[b * 6 + 3 + c]);
+        }
+        live += cnt[b * 2];
+        bad += cnt[b * 2 + 1];
+    }
+    double cx = 0.5 * (lo[0] + hi[0]), cy = 0.5 * (lo[1] + hi[1]), cz = 0.5 * (lo[2] + hi[2]);
+    double side = fmax(hi[0] - lo[0], fmax(hi[1] - lo[1], hi[2] - lo[2])) * 1.0000001;
+    if (side <= 0) side = 1.0;
+    if (seed >= 0) {  // RANDOMIZE_GRAVTREE, splitmix64 draws of tree.cc:381-393
+        uint64_t s = (uint64_t)seed * 0x9E3779B97F4A7C15ull;
+        double d[3];
+        for (int k = 0; k < 3; ++k) {
+            s += 0x9E3779B97F4A7C15ull;
+            uint64_t v = s;
+            v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ull;
+            v = (v ^ (v >> 27)) * 0x94D049BB133111EBull;
+            d[k] = (double)((v ^ (v >> 31)) >> 11) * (1.0 / 9007199254740992.0);
+        }
+        // the reference's compiler fuses these into FMAs (checked on its x86 build); so do we
+        cx = fma(side, d[0] - 0.5, cx);
+        cy = fma(side, d[1] - 0.5, cy);
+        cz = fma(side, d[2] - 0.5, cz);
+        side *= 2.0;
+    }
+    if (fx != 0.0 || fy != 0.0 || fz != 0.0) {  // SHMEM_TREE_SHIFT, tree.cc:400-407
+        cx = fma(fx, side, cx); cy = fma(fy, side, cy); cz = fma(fz, side, cz);
+        side *= 1.0 + 2.0 * (fabs(fx) + fabs(fy) + fabs(fz));
+    }
+    g->cx = cx; g->cy = cy; g->cz = cz; g->side = side;
+    g->scale = (double)((1u << max_level) - 1) / side;
+    g->corner_x = fma(-0.5, side, cx);  // 0.5*side is exact: fused or not, the same bits
+    g->corner_y = fma(-0.5, side, cy);
+    g->corner_z = fma(-0.5, side, cz);
+    g->n_live = (long long)live;
+    *bad_out = bad;
+}
+
+// ---- 2. keys ---------------------------------------------------------------------------------
+__device__ __forceinline__ void quantise(const RootGeom& g, double x, double y, double z,
+                                         uint32_t& a, uint32_t& b, uint32_t& c) {
+    a = (uint32_t)((x - g.corner_x) * g.scale);
+    b = (uint32_t)((y - g.corner_y) * g.scale);
+    c = (uint32_t)((z - g.corner_z) * g.scale);
+}
+
+__device__ __forceinline__ uint64_t spread3_21(uint64_t v) {
+    v &= 0x1FFFFFull;
+    v = (v | v << 32) & 0x1F00000000FFFFull;
+    v = (v | v << 16) & 0x1F0000FF0000FFull;
+    v = (v | v << 8) & 0x100F00F00F00F00Full;
+    v = (v | v << 4) & 0x10C30C30C30C30C3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+}
+
+__global__ void keys_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                            const double* __restrict__ z, const double* __restrict__ m, int64_t n,
+                            const RootGeom* __restrict__ gp, int key_mode, int levels,
+                            uint64_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+    __shared__ uint16_t tab[48 * 8];
+    for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x) tab[k] = kPhStep[k];
+    __syncthreads();
+    const RootGeom g = *gp;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        idx[i] = (uint32_t)i;
+        if (!(m[i] > 0)) { keys[i] = kDeadKey; continue; }
+        uint32_t a, b, c;
+        quantise(g, x[i], y[i], z[i], a, b, c);
+        uint64_t key;
+        if (key_mode == GT_KEY_MORTON) {
+            key = spread3_21(a) | (spread3_21(b) << 1) | (spread3_21(c) << 2);
+        } else {
+            key = 0;
+            unsigned state = 0;
+            for (int l = levels - 1; l >= 0; --l) {
+                const unsigned pix = ((a >> l) & 1u) << 2 | ((b >> l) & 1u) << 1 | ((c >> l) & 1u);
+                const unsigned step = tab[state * 8 + pix];
+                key = (key << 3) | (step & 7u);
+                state = step >> 3;
+            }
+        }
+        keys[i] = key;
+    }
+}
+
+// ---- 4. gather into tree order ---------------------------------------------------------------
+__global__ void gather_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                              const double* __restrict__ z, const double* __restrict__ m,
+                              const double* __restrict__ soft, const uint32_t* __restrict__ idx,
+                              int64_t n, SrcP* __restrict__ src, double* __restrict__ ssoft,
+                              double* __restrict__ smass, uint32_t* __restrict__ order,
+                              uint32_t* __restrict__ rank, int* __restrict__ leaf_of,
+                              int* __restrict__ sleaf) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = idx[i];
+        SrcP r;
+        r.x = x[p]; r.y = y[p]; r.z = z[p];
+        const double sp = soft ? soft[p] : 0.0;
+        r.m = (float)m[p];
+        r.soft = (float)sp;
+        src[i] = r;
+        ssoft[i] = sp;
+        smass[i] = m[p];
+        order[i] = p;
+        rank[p] = (uint32_t)i;
+        leaf_of[p] = -1;
+        sleaf[i] = -1;
+    }
+}
+
+// ---- 5. structure ----------------------------------------------------------------------------
+__device__ __forceinline__ int lower_bound_digit(const uint64_t* __restrict__ key, int lo, int hi,
+                                                 int shift, unsigned v) {
+    // first index in [lo, hi) whose digit is >= v (digits are non-decreasing over the range)
+    while (lo < hi) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if ((unsigned)((key[mid] >> shift) & 7ull) < v) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void split_kernel(GNode* __restrict__ nodes, const uint64_t* __restrict__ skey,
+                             int64_t a, int64_t b, int level, int max_level, int leaf_max,
+                             int* __restrict__ bnd, uint32_t* __restrict__ nchild) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b - a) return;
+    const GNode& nd = nodes[a + t];
+    const int lo = nd.plo, hi = nd.phi;
+    int cnt = 0;
+    int* B = bnd + t * 9;
+    if (!(hi - lo <= leaf_max || level >= max_level)) {
+        const int shift = 3 * (max_level - level - 1);
+        B[0] = lo;
+        for (unsigned v = 1; v < 8; ++v) B[v] = lower_bound_digit(skey, B[v - 1], hi, shift, v);
+        B[8] = hi;
+        for (int v = 0; v < 8; ++v) cnt += (B[v + 1] > B[v]);
+    }
+    nchild[t] = (uint32_t)cnt;
+}
+
+__global__ void emit_kernel(GNode* __restrict__ nodes, const SrcP* __restrict__ src,
+                            const RootGeom* __restrict__ gp, int64_t a, int64_t b, int level,
+                            int max_level, const int* __restrict__ bnd,
+                            const uint32_t* __restrict__ nchild, const uint32_t* __restrict__ coff,
+                            int* __restrict__ parent, int* __restrict__ next, int* __restrict__ lvl,
+                            double* __restrict__ size, double* __restrict__ gc) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b - a) return;
+    const int64_t i = a + t;
+    const int nc = (int)nchild[t];
+    if (nc == 0) {
+        nodes[i].first = -1;
+        nodes[i].nchild = 0;
+        return;
+    }
+    const RootGeom g = *gp;
+    const int first = (int)(b + coff[t]);
+    nodes[i].first = first;
+    nodes[i].nchild = nc;
+    const int* B = bnd + t * 9;
+    const double sz = size[i], half = sz * 0.5, quarter = sz * 0.25;
+    const double pcx = gc[3 * i], pcy = gc[3 * i + 1], pcz = gc[3 * i + 2];
+    const int pnext = next[i];
+    const int bit = max_level - 1 - level;  // coordinate bit that selects the octant at this level
+    int k = 0;
+    for (int v = 0; v < 8; ++v) {
+        if (B[v + 1] <= B[v]) continue;
+        const int c = first + k;
+        const SrcP& s0 = src[B[v]];
+        uint32_t qa, qb, qc;
+        quantise(g, s0.x, s0.y, s0.z, qa, qb, qc);
+        const int oct = (int)((qa >> bit) & 1u) | (int)(((qb >> bit) & 1u) << 1) | (int)(((qc >> bit) & 1u) << 2);
+        GNode& ch = nodes[c];
+        ch.plo = B[v];
+        ch.phi = B[v + 1];
+        ch.first = -1;
+        ch.nchild = 0;
+        parent[c] = (int)i;
+        lvl[c] = level + 1;
+        size[c] = half;
+        gc[3 * c] = pcx + ((oct & 1) ? quarter : -quarter);
+        gc[3 * c + 1] = pcy + ((oct & 2) ? quarter : -quarter);
+        gc[3 * c + 2] = pcz + ((oct & 4) ? quarter : -quarter);
+        next[c] = (k + 1 < nc) ? c + 1 : pnext;
+        ++k;
+    }
+}
+
+// ---- 6. moments, one warp per node, deepest level first ---------------------------------------
+__global__ void moments_kernel(GNode* __restrict__ nodes, const SrcP* __restrict__ src,
+                               const double* __restrict__ smass, const double* __restrict__ ssoft,
+                               const uint32_t* __restrict__ order, int64_t a, int64_t b,
+                               const double* __restrict__ size, const double* __restrict__ gc,
+                               double* __restrict__ delta, double* __restrict__ nsoft,
+                               int* __restrict__ leaf_of, int* __restrict__ sleaf, int nodelta) {
+    const int lane = threadIdx.x & 31;
+    const int64_t i = a + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    if (i >= b) return;
+    const int first = nodes[i].first, nc = nodes[i].nchild;
+    double M = 0, mx = 0, my = 0, mz = 0, smax = 0;
+    if (first < 0) {
+        const int lo = nodes[i].plo, hi = nodes[i].phi;
+        for (int j = lo + lane; j < hi; j += 32) {
+            const double mj = smass[j];
+            const SrcP s = src[j];
+            M += mj; mx += mj * s.x; my += mj * s.y; mz += mj * s.z;
+            smax = fmax(smax, ssoft[j]);
+            leaf_of[order[j]] = (int)i;
+            sleaf[j] = (int)i;
+        }
+    } else if (lane < nc) {
+        const GNode& ch = nodes[first + lane];
+        M = ch.mass; mx = M * ch.cx; my = M * ch.cy; mz = M * ch.cz;
+        smax = nsoft[first + lane];
+    }
+    M = warp_sum_d(M); mx = warp_sum_d(mx); my = warp_sum_d(my); mz = warp_sum_d(mz);
+    smax = warp_max_d(smax);
+    if (lane == 0) {
+        if (M > 0) { mx /= M; my /= M; mz /= M; }
+        const double dx = mx - gc[3 * i], dy = my - gc[3 * i + 1], dz = mz - gc[3 * i + 2];
+        const double dl = sqrt(dx * dx + dy * dy + dz * dz);
+        GNode& nd = nodes[i];
+        nd.cx = mx; nd.cy = my; nd.cz = mz; nd.mass = M;
+        nd.s = size[i] + (nodelta ? 0.0 : dl);
+        nd.len = (float)size[i];
+        nd.soft = (float)smax;
+        delta[i] = dl;
+        nsoft[i] = smax;
+    }
+}
+
+__global__ void root_init_kernel(GNode* __restrict__ nodes, const RootGeom* __restrict__ gp,
+                                 int* parent, int* next, int* lvl, double* size, double* gc) {
+    const RootGeom g = *gp;
+    GNode& r = nodes[0];
+    r.plo = 0;
+    r.phi = (int)g.n_live;
+    r.first = -1;
+    r.nchild = 0;
+    parent[0] = -1;
+    next[0] = -1;
+    lvl[0] = 0;
+    size[0] = g.side;
+    gc[0] = g.cx; gc[1] = g.cy; gc[2] = g.cz;
+}
+
+// ---- MPI-code keys (domain.cc:2682-2702, peano.cc:297-355) -------------------------------------
+__device__ __forceinline__ uint64_t mantissa_bits(double d, int bits) {
+    const uint64_t u = (uint64_t)__double_as_longlong(d);
+    return (u & 0xFFFFFFFFFFFFFull) >> (52 - bits);
+}
+
+__global__ void peano_keys_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                  const double* __restrict__ z, int64_t n, double c0, double c1,
+                                  double c2, double len, int bits, uint64_t* ph_hi, uint64_t* ph_lo,
+                                  uint64_t* mo_hi, uint64_t* mo_lo) {
+    __shared__ uint16_t tab[48 * 8];
+    for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x) tab[k] = kPhStep[k];
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t xb = mantissa_bits((x[i] - c0) / len + 1.0, bits);
+        const uint64_t yb = mantissa_bits((y[i] - c1) / len + 1.0, bits);
+        const uint64_t zb = mantissa_bits((z[i] - c2) / len + 1.0, bits);
+        uint64_t hh = 0, hl = 0, mh = 0, ml = 0;
+        unsigned state = 0;
+        for (int l = bits - 1; l >= 0; --l) {
+            const unsigned bx = (unsigned)((xb >> l) & 1u), by = (unsigned)((yb >> l) & 1u),
+                           bz = (unsigned)((zb >> l) & 1u);
+            const unsigned step = tab[state * 8 + (bx << 2 | by << 1 | bz)];
+            state = step >> 3;
+            hh = (hh << 3) | (hl >> 61);
+            hl = (hl << 3) | (step & 7u);
+            mh = (mh << 3) | (ml >> 61);
+            ml = (ml << 3) | (bz << 2 | by << 1 | bx);
+        }
+        if (ph_hi) ph_hi[i] = hh;
+        if (ph_lo) ph_lo[i] = hl;
+        if (mo_hi) mo_hi[i] = mh;
+        if (mo_lo) mo_lo[i] = ml;
+    }
+}
+
+__global__ void form_aold_kernel(const double* __restrict__ ax, const double* __restrict__ ay,
+                                 const double* __restrict__ az, int64_t n, double alpha, double G,
+                                 double* __restrict__ aold) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        aold[i] = alpha * sqrt(ax[i] * ax[i] + ay[i] * ay[i] + az[i] * az[i]) / G;
+}
+
+template <typename T>
+T* dalloc(size_t count) {
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, count * sizeof(T) + 16);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Fail{GT_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+    }
+    return (T*)p;
+}
+
+int grid_for(gt_context* ctx, int64_t n, int per_block = kBlk) {
+    const int64_t want = (n + per_block - 1) / per_block;
+    const int64_t cap = (int64_t)ctx->num_sms * 8;
+    return (int)std::max<int64_t>(1, std::min(want, cap));
+}
+
+void grow_nodes(gt_tree* t, int64_t need, cudaStream_t stream) {
+    if (need <= t->node_cap) return;
+    const int64_t cap = std::max<int64_t>(need, t->node_cap * 2);
+    auto grow = [&](auto*& p, size_t per) {
+        using T = std::remove_reference_t<decltype(*p)>;
+        T* q = dalloc<T>((size_t)cap * per);
+        if (p) {
+            check_cuda(cudaMemcpyAsync(q, p, (size_t)t->node_cap * per * sizeof(T), cudaMemcpyDeviceToDevice,
+                                       stream), "grow nodes");
+            check_cuda(cudaStreamSynchronize(stream), "sync");
+            cudaFree(p);
+        }
+        p = q;
+    };
+    grow(t->nodes, 1); grow(t->parent, 1); grow(t->next, 1); grow(t->level, 1);
+    grow(t->size, 1); grow(t->delta, 1); grow(t->nsoft, 1); grow(t->gc, 3);
+    t->node_cap = cap;
+}
+
+}  // namespace
+
+void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, const double* z,
+                const double* m, const double* soft) {
+    cudaStream_t st = ctx->stream;
+    const int64_t n = t->n;
+    const gt_build_options& o = t->opt;
+    cudaEvent_t ev[7];
+    for (auto& e : ev) check_cuda(cudaEventCreate(&e), "event");
+    struct EvGuard {
+        cudaEvent_t* e;
+        ~EvGuard() { for (int k = 0; k < 7; ++k) cudaEventDestroy(e[k]); }
+    } guard{ev};
+    check_cuda(cudaEventRecord(ev[0], st), "event");
+
+    // 1. bbox
+    const int nbb = std::max(1, std::min(ctx->num_sms * 2, div_up(std::max<int64_t>(n, 1), kBlk)));
+    double* part = (double*)scratch(ctx, kSlotPartials, (size_t)nbb * 6 * 8 + (size_t)nbb * 16 + 256);
+    unsigned long long* cnt = (unsigned long long*)(part + (size_t)nbb * 6);
+    RootGeom* gdev = (RootGeom*)scratch(ctx, kSlotCounters, sizeof(RootGeom) + 64);
+    unsigned long long* bad_dev = (unsigned long long*)((char*)gdev + sizeof(RootGeom));
+    bbox_partial_kernel<<<nbb, kBlk, 0, st>>>(x, y, z, m, soft, n, part, cnt);
+    check_launch(ctx, "bbox_partial_kernel");
+    root_geom_kernel<<<1, 1, 0, st>>>(part, cnt, nbb, gdev, bad_dev, o.randomize_seed, o.shift[0],
+                                      o.shift[1], o.shift[2], o.max_level);
+    check_launch(ctx, "root_geom_kernel");
+    {
+        char* pin = (char*)ctx->pinned;
+        check_cuda(cudaMemcpyAsync(pin, gdev, sizeof(RootGeom) + 8, cudaMemcpyDeviceToHost, st), "geom d2h");
+        check_cuda(cudaStreamSynchronize(st), "sync");
+        std::memcpy(&t->geom, pin, sizeof(RootGeom));
+        unsigned long long bad = 0;
+        std::memcpy(&bad, pin + sizeof(RootGeom), 8);
+        if (o.validate && bad > 0)
+            throw Fail{GT_ERR_NONFINITE, "gt_build: " + std::to_string(bad) + " particle(s) with non-finite input"};
+    }
+    t->n_live = t->geom.n_live;
+    check_cuda(cudaEventRecord(ev[1], st), "event");
+
+    // 2. keys
+    uint64_t* keys = (uint64_t*)scratch(ctx, kSlotKeysA, (size_t)std::max<int64_t>(n, 1) * 8);
+    uint32_t* idx = (uint32_t*)scratch(ctx, kSlotValsA, (size_t)std::max<int64_t>(n, 1) * 4);
+    if (n > 0) {
+        keys_kernel<<<grid_for(ctx, n), kBlk, 0, st>>>(x, y, z, m, n, gdev, o.key_mode, o.max_level, keys, idx);
+        check_launch(ctx, "keys_kernel");
+    }
+    check_cuda(cudaEventRecord(ev[2], st), "event");
+
+    // 3. sort: live keys < 2^(3*max_level), the massless sentinel is 2^60
+    radix_sort_pairs(ctx, keys, idx, n, 61);
+    check_cuda(cudaEventRecord(ev[3], st), "event");
+
+    // 4. particle arrays in tree order
+    const int64_t nalloc = std::max<int64_t>(n, 1);
+    t->src = dalloc<SrcP>(nalloc);
+    t->ssoft = dalloc<double>(nalloc);
+    t->smass = dalloc<double>(nalloc);
+    t->order = dalloc<uint32_t>(nalloc);
+    t->rank = dalloc<uint32_t>(nalloc);
+    t->leaf_of = dalloc<int>(nalloc);
+    t->sleaf = dalloc<int>(nalloc);
+    t->skey = dalloc<uint64_t>(nalloc);
+    if (n > 0) {
+        gather_kernel<<<grid_for(ctx, n), kBlk, 0, st>>>(x, y, z, m, soft, idx, n, t->src, t->ssoft,
+                                                         t->smass, t->order, t->rank, t->leaf_of, t->sleaf);
+        check_launch(ctx, "gather_kernel");
+        check_cuda(cudaMemcpyAsync(t->skey, keys, (size_t)n * 8, cudaMemcpyDeviceToDevice, st), "skey");
+    }
+
+    // 5. structure, level by level
+    const int64_t nl = t->n_live;
+    grow_nodes(t, std::max<int64_t>(1024, (2 * nl) / std::max(1, o.leaf_max) * 3 + 1024), st);
+    root_init_kernel<<<1, 1, 0, st>>>(t->nodes, gdev, t->parent, t->next, t->level, t->size, t->gc);
+    check_launch(ctx, "root_init_kernel");
+    t->lvl_off.assign(1, 0);
+    t->lvl_off.push_back(1);
+    uint32_t* total_dev = (uint32_t*)((char*)gdev + sizeof(RootGeom) + 16);
+    for (int L = 0;; ++L) {
+        const int64_t a = t->lvl_off[L], b = t->lvl_off[L + 1];
+        const int64_t cnt_l = b - a;
+        if (cnt_l <= 0) break;
+        int* bnd = (int*)scratch(ctx, kSlotNodeTmp0, (size_t)cnt_l * 9 * 4);
+        uint32_t* nch = (uint32_t*)scratch(ctx, kSlotNodeTmp1, (size_t)cnt_l * 4);
+        uint32_t* coff = (uint32_t*)scratch(ctx, kSlotNodeTmp2, (size_t)cnt_l * 4);
+        split_kernel<<<div_up(cnt_l, kBlk), kBlk, 0, st>>>(t->nodes, t->skey, a, b, L, o.max_level,
+                                                           o.leaf_max, bnd, nch);
+        check_launch(ctx, "split_kernel");
+        scan_exclusive_u32(ctx, nch, coff, cnt_l, total_dev);
+        uint32_t total = 0;
+        check_cuda(cudaMemcpyAsync(ctx->pinned, total_dev, 4, cudaMemcpyDeviceToHost, st), "count d2h");
+        check_cuda(cudaStreamSynchronize(st), "sync");
+        std::memcpy(&total, ctx->pinned, 4);
+        grow_nodes(t, b + (int64_t)total, st);
+        emit_kernel<<<div_up(cnt_l, kBlk), kBlk, 0, st>>>(t->nodes, t->src, gdev, a, b, L, o.max_level,
+                                                          bnd, nch, coff, t->parent, t->next, t->level,
+                                                          t->size, t->gc);
+        check_launch(ctx, "emit_kernel");
+        if (total == 0) break;
+        t->lvl_off.push_back(b + (int64_t)total);
+    }
+    t->n_levels = (int)t->lvl_off.size() - 1;
+    t->n_nodes = t->lvl_off.back();
+    check_cuda(cudaEventRecord(ev[4], st), "event");
+
+    // 6. moments, deepest level first
+    for (int L = t->n_levels - 1; L >= 0; --L) {
+        const int64_t a = t->lvl_off[L], b = t->lvl_off[L + 1];
+        const int64_t warps = b - a;
+        moments_kernel<<<div_up(warps * 32, kBlk), kBlk, 0, st>>>(
+            t->nodes, t->src, t->smass, t->ssoft, t->order, a, b, t->size, t->gc, t->delta,
+            t->nsoft, t->leaf_of, t->sleaf, o.nodelta);
+        check_launch(ctx, "moments_kernel");
+    }
+    check_cuda(cudaEventRecord(ev[5], st), "event");
+    check_cuda(cudaEventRecord(ev[6], st), "event");
+    check_cuda(cudaEventSynchronize(ev[6]), "sync");
+    float ms;
+    for (int k = 0; k < 6; ++k) {
+        check_cuda(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]), "elapsed");
+        t->build_ms[k] = ms;
+    }
+    check_cuda(cudaEventElapsedTime(&ms, ev[0], ev[6]), "elapsed");
+    t->build_ms[6] = ms;
+}
+
+void run_peano_keys(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
+                    const double corner[3], double len, int bits, uint64_t* ph_hi, uint64_t* ph_lo,
+                    uint64_t* mo_hi, uint64_t* mo_lo) {
+    if (n <= 0) return;
+    peano_keys_kernel<<<grid_for(ctx, n), kBlk, 0, ctx->stream>>>(x, y, z, n, corner[0], corner[1],
+                                                                  corner[2], len, bits, ph_hi, ph_lo,
+                                                                  mo_hi, mo_lo);
+    check_launch(ctx, "peano_keys_kernel");
+}
+
+void run_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay,
+                   const double* az, double alpha, double G, double* aold) {
+    if (n <= 0) return;
+    form_aold_kernel<<<grid_for(ctx, n), kBlk, 0, ctx->stream>>>(ax, ay, az, n, alpha, G, aold);
+    check_launch(ctx, "form_aold_kernel");
+}
+
+}  // namespace gt

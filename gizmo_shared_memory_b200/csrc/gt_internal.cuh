@@ -1,0 +1,181 @@
+// Internal declarations of libgt: device layouts, context/tree structs, launch helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "gt.h"
+
+namespace gt {
+
+constexpr int kWarp = 32;
+constexpr uint64_t kDeadKey = 1ull << 60;  // massless particles sort after every live key
+
+// ---------------------------------------------------------------------------------------------
+// Device layouts
+// ---------------------------------------------------------------------------------------------
+
+// Walk node, 64 bytes = two 32-byte sectors, read with four 16-byte loads.  Holds what the
+// opening test and a monopole interaction need (the reference's WNode, shmem/tree.h:195-204)
+// plus the BFS child range: children of a node are contiguous, first .. first+nchild-1.
+struct alignas(16) GNode {
+    double cx, cy;      // centre of mass
+    double cz, mass;
+    double s;           // size + delta: conservative opening radius (size only with nodelta)
+    float len;          // side length (float, as WNode::len)
+    float soft;         // max softening in the node (float, as WNode::soft)
+    int first;          // first child, -1 for a leaf
+    int nchild;         // number of children (0 for a leaf)
+    int plo, phi;       // particle range in tree order
+};
+static_assert(sizeof(GNode) == 64, "GNode must be one 64-byte record");
+
+// Source particle in tree order, 32 bytes: FP64 position (offsets are formed in FP64), FP32 mass
+// and softening (the interaction arithmetic is FP32).
+struct alignas(16) SrcP {
+    double x, y;
+    double z;
+    float m, soft;
+};
+static_assert(sizeof(SrcP) == 32, "SrcP must be 32 bytes");
+
+// Root cell geometry computed on the device (bbox -> centre, side, scale).
+struct RootGeom {
+    double cx, cy, cz, side, scale;
+    double corner_x, corner_y, corner_z;
+    long long n_live;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Host-side structs behind the opaque C handles
+// ---------------------------------------------------------------------------------------------
+
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace gt
+
+struct gt_context {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string last_error;
+    uint64_t launches = 0;
+    gt_walk_stats stats{};
+    std::vector<gt::DevBuf> scratch;  // grow-only workspace slots, indexed by gt::Slot
+    void* pinned = nullptr;           // small pinned host buffer for scalar read-backs
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+struct gt_tree {
+    int device = 0;
+    int64_t n = 0, n_live = 0, n_nodes = 0, node_cap = 0;
+    int n_levels = 0;
+    gt_build_options opt{};
+    gt::RootGeom geom{};
+    std::vector<int64_t> lvl_off;  // node index range of each level: [lvl_off[L], lvl_off[L+1])
+    double build_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+    // device arrays (owned)
+    gt::SrcP* src = nullptr;     // n (live first, in tree order; massless after)
+    double* ssoft = nullptr;     // n, FP64 softening in tree order (targets' opening inputs)
+    double* smass = nullptr;     // n, FP64 mass in tree order
+    uint32_t* order = nullptr;   // n, tree position -> particle index
+    uint32_t* rank = nullptr;    // n, particle index -> tree position (UINT32_MAX: massless)
+    int* leaf_of = nullptr;      // n, particle index -> leaf (-1: massless)
+    int* sleaf = nullptr;        // n, tree position -> leaf (-1: massless)
+    uint64_t* skey = nullptr;    // n, sorted keys
+    gt::GNode* nodes = nullptr;  // node_cap
+    int* parent = nullptr;       // node_cap
+    int* next = nullptr;         // node_cap, reference threading (shmem/tree.cc:340-348)
+    int* level = nullptr;        // node_cap
+    double* size = nullptr;      // node_cap
+    double* delta = nullptr;     // node_cap
+    double* nsoft = nullptr;     // node_cap, FP64 max softening
+    double* gc = nullptr;        // node_cap * 3, geometric centres
+    // cached all-active group lists, keyed by (mode, param)
+    struct GroupCache {
+        int mode = -1, param = 0, kmax = 0;
+        int2* groups = nullptr;
+        int64_t n_groups = 0;
+    };
+    std::vector<GroupCache> group_cache;
+};
+
+namespace gt {
+
+// Scratch slots of the context workspace.
+enum Slot {
+    kSlotIn0 = 0, kSlotIn1, kSlotIn2, kSlotIn3, kSlotIn4,  // staged host inputs
+    kSlotKeysA, kSlotKeysB, kSlotValsA, kSlotValsB,
+    kSlotHist, kSlotScanA, kSlotScanB, kSlotPartials,
+    kSlotNodeTmp0, kSlotNodeTmp1, kSlotNodeTmp2,
+    kSlotTargets, kSlotAold, kSlotGroupKey, kSlotGroupsA, kSlotGroupsB,
+    kSlotOut0, kSlotOut1, kSlotOut2, kSlotOut3,
+    kSlotStack, kSlotCounters, kSlotDirect,
+    kSlotCount
+};
+
+// Error plumbing: every entry point funnels CUDA failures into a gt_status and a message.
+struct Fail {
+    int status;
+    std::string msg;
+};
+
+void set_error(gt_context* ctx, int status, const std::string& msg);
+void* scratch(gt_context* ctx, Slot s, size_t bytes);  // throws Fail on allocation failure
+void check_cuda(cudaError_t e, const char* what);       // throws Fail
+void check_launch(gt_context* ctx, const char* what);   // counts the launch, throws on error
+
+inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// Device-wide helpers (gt_scan.cu).
+// Exclusive scan of n uint32 values into out (may alias in); returns nothing, total written to
+// total_dev[0] when total_dev is non-null.
+void scan_exclusive_u32(gt_context* ctx, const uint32_t* in, uint32_t* out, int64_t n,
+                        uint32_t* total_dev);
+// Stable LSD radix sort of (key, value) pairs over the low `bits` bits of the key.
+void radix_sort_pairs(gt_context* ctx, uint64_t* keys, uint32_t* vals, int64_t n, int bits);
+
+// Build (gt_build.cu)
+void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, const double* z,
+                const double* m, const double* soft);
+
+// Walk (gt_walk.cu)
+struct WalkRequest {
+    const uint32_t* targets = nullptr;  // device, original indices; null = all live in tree order
+    int64_t n_targets = 0;
+    const double* aold = nullptr;       // device, parallel to targets
+    double theta = 0, G = 1;
+    int group_mode = GT_GROUP_LEAF;
+    int group_param = 0;                // batch or group_max
+    bool leaf_accept = true;
+    bool want_acc = true, want_phi = false;
+    bool out_original = false;
+    int mac = GT_MAC_PLAIN;
+    bool count = false;
+    int block_warps = 0, list_capacity = 0, stack_capacity = 0;
+    double *ax = nullptr, *ay = nullptr, *az = nullptr, *phi = nullptr;  // device outputs
+};
+void run_walk(gt_context* ctx, const gt_tree* t, const WalkRequest& rq);
+
+// Direct sum (gt_direct.cu)
+void run_direct(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
+                const double* m, const double* soft, int64_t nt, const uint32_t* targets, double G,
+                int precision, double* ax, double* ay, double* az, double* phi);
+
+// Keys (gt_build.cu)
+void run_peano_keys(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
+                    const double corner[3], double len, int bits, uint64_t* ph_hi, uint64_t* ph_lo,
+                    uint64_t* mo_hi, uint64_t* mo_lo);
+// Peak probe (gt_peak.cu)
+void run_peaks(gt_context* ctx, double* fp32_tflops, double* fp64_tflops);
+void run_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay,
+                   const double* az, double alpha, double G, double* aold);
+
+}  // namespace gt

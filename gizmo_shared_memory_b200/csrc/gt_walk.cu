@@ -1,0 +1,717 @@
+// Group tree walk on the device: the replacement for shmem::accel_grouped (shmem/tree.cc:626-897),
+// shmem::accel (tree.cc:528-582) and shmem::potential (tree.cc:899-944).
+//
+// One warp walks the tree for one group of targets (a leaf's targets, a fixed window, a group
+// node's particles, or a single target) and applies the result to all of them:
+//
+//   * Group reduction (FP64, warp shuffles): bounding box, largest target softening, smallest aold
+//     -- the conservative per-group inputs of the reference's batch walk (tree.cc:682-702).
+//   * Traversal: a per-warp LIFO of node indices.  Each step pops up to 32 nodes, one per lane,
+//     loads each 64-byte node with four 16-byte loads and evaluates the opening test in FP64 on the
+//     group box's nearest point, in the reference's order (shmem/tree.h:109-144; leaves are offered
+//     to the criterion first in the grouped walk, tree.cc:751-779, and always expanded in the
+//     per-target walks).  Opened interior nodes push their contiguous children (a warp prefix sum
+//     gives each lane its slots).  The stack never holds more than 256 entries per tree level: the
+//     blocks of entries pushed by one step have strictly increasing minimum depth from bottom to
+//     top, and one step pushes at most 32*8.
+//   * Interaction list (shared memory, per warp): accepted nodes as monopoles and the particles of
+//     expanded leaves, each stored as its FP64 offset from the group centre cast to FP32, FP32 mass
+//     and softening.  When the list fills it is evaluated against the group's targets.
+//   * Evaluation (FP32): r^2, rsqrt, Newtonian force and potential; the cubic-spline branch only
+//     when r < max(h_target, h_source) (shmem/tree.h:59-80).  r^2 == 0 (the target itself, or a
+//     coincident particle) contributes nothing, as tree.cc:799-802 skips it.  Groups of <= 16
+//     targets split the list across the idle lanes (lane = slice * NT + target) and reduce the
+//     slices at the end.
+//   * Accumulation: each list evaluation sums into FP32 partials, which are added into FP32
+//     Kahan-compensated totals (acceleration) and an FP64 total (potential); the final sums and
+//     the factor G are FP64.
+#include <algorithm>
+#include <cstring>
+
+#include "gt_internal.cuh"
+
+namespace gt {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kMaxWarps = 8;     // warps per block of the walk kernel
+constexpr int kListCap = 256;    // interaction-list entries per warp
+
+struct WalkArgs {
+    const GNode* nodes;
+    const SrcP* src;
+    const double* ssoft;
+    const uint32_t* tpos;       // target -> tree position; null: identity
+    const double* aold;         // per target; null: 0 everywhere
+    const int2* groups;         // [start, end) in target index space
+    int n_groups;
+    double theta2, G;
+    double *ax, *ay, *az, *phi;
+    const uint32_t* out_map;    // null: write at the target index
+    int* stack;
+    int stack_cap;
+    unsigned int* next_group;   // dynamic group counter
+    unsigned long long* stats;  // [nodes, multipole, pairs_structural, zero_r2, flushes, max_stack]
+    int* error;                 // 1: stack overflow
+};
+
+__device__ __forceinline__ int warp_incl_scan_i(int v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+__device__ __forceinline__ double wmin(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+__device__ __forceinline__ double wmax(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+
+struct NodeV {
+    double cx, cy, cz, mass, s;
+    float len, soft;
+    int first, nchild, plo, phi;
+};
+
+__device__ __forceinline__ NodeV load_node(const GNode* __restrict__ p) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    const int4 c = __ldg(reinterpret_cast<const int4*>(p) + 2);
+    const int4 d = __ldg(reinterpret_cast<const int4*>(p) + 3);
+    NodeV v;
+    v.cx = a.x; v.cy = a.y; v.cz = b.x; v.mass = b.y;
+    v.s = __hiloint2double(c.y, c.x);
+    v.len = __int_as_float(c.z);
+    v.soft = __int_as_float(c.w);
+    v.first = d.x; v.nchild = d.y; v.plo = d.z; v.phi = d.w;
+    return v;
+}
+
+__device__ __forceinline__ void load_src(const SrcP* __restrict__ p, double& x, double& y, double& z,
+                                         float& m, float& h) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const int4 b = __ldg(reinterpret_cast<const int4*>(p) + 1);
+    x = a.x; y = a.y;
+    z = __hiloint2double(b.y, b.x);
+    m = __int_as_float(b.z);
+    h = __int_as_float(b.w);
+}
+
+// The opening test of shmem/tree.h:109-144, FP64, same order of arms.
+__device__ __forceinline__ bool open_node(double r2, double len, double l_open, double mass,
+                                          double nsoft, double tsoft, double aold, double theta2,
+                                          double dx, double dy, double dz) {
+    const double rt = tsoft + 0.6 * len, rn = nsoft + 0.6 * len;
+    if (r2 < rt * rt || r2 < rn * rn) return true;
+    if (theta2 > 0.0 && l_open * l_open >= theta2 * r2) return true;
+    if (aold > 0) {
+        if (mass * len * len > r2 * r2 * aold) return true;
+    } else if (theta2 <= 0.0) {
+        return true;
+    }
+    const double lim = 0.6 * len;
+    return dx < lim && dy < lim && dz < lim;
+}
+
+// Softened pair inside the kernel (r < h): force factor and potential of the cubic spline,
+// shmem/tree.h:59-80, in FP32.  r2 == 0 contributes nothing.
+__device__ __noinline__ void spline_pair(float r2, float h, float m, float& f, float& p) {
+    if (!(r2 > 0.0f)) { f = 0.0f; p = 0.0f; return; }
+    const float r = sqrtf(r2);
+    const float hinv = 1.0f / h;
+    const float u = r * hinv;
+    const float hinv3 = hinv * hinv * hinv;
+    if (u < 0.5f) {
+        f = m * hinv3 * (10.666666666666667f + u * u * (32.0f * u - 38.4f));
+        p = m * hinv * (-2.8f + u * u * (5.333333333333333f + u * u * (6.4f * u - 9.6f)));
+    } else {
+        const float u3 = u * u * u;
+        f = m * hinv3 * (21.333333333333332f - 48.0f * u + 38.4f * u * u - 10.666666666666667f * u3 -
+                         0.06666666666666667f / u3);
+        p = m * hinv * (-3.2f + 0.06666666666666667f / u +
+                        u * u * (10.666666666666667f + u * (-16.0f + u * (9.6f - 2.1333333333333333f * u))));
+    }
+}
+
+__device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
+    const float y = x - comp;
+    const float t = sum + y;
+    comp = (t - sum) - y;
+    sum = t;
+}
+
+template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT>
+__global__ void __launch_bounds__(kMaxWarps * 32)
+walk_kernel(const WalkArgs A) {
+    __shared__ float4 s_pm[kMaxWarps][kListCap];
+    __shared__ float s_h[kMaxWarps][kListCap];
+    __shared__ int s_lo[kMaxWarps][32];
+    __shared__ int s_pre[kMaxWarps][32];
+
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + w;
+    int* __restrict__ stk = A.stack + (size_t)gw * A.stack_cap;
+    float4* __restrict__ pm = s_pm[w];
+    float* __restrict__ hs = s_h[w];
+
+    unsigned long long c_nodes = 0, c_multi = 0, c_pairs = 0, c_zero = 0, c_flush = 0;
+    int c_maxtop = 0;
+
+    for (;;) {
+        int g = 0;
+        if (lane == 0) g = (int)atomicAdd(A.next_group, 1u);
+        g = __shfl_sync(kFull, g, 0);
+        if (g >= A.n_groups) break;
+        const int2 gr = A.groups[g];
+        const int t0 = gr.x, nt = gr.y - gr.x;
+        const int nk = (TPL > 1 && nt > 32) ? 2 : 1;  // warp-uniform
+
+        // ---- targets: lane l holds targets l and l+32 --------------------------------------
+        double px[TPL], py[TPL], pz[TPL], ps[TPL];
+        double lx = 1e300, ly = 1e300, lz = 1e300, hx = -1e300, hy = -1e300, hz = -1e300;
+        double emax = 0.0, amin = A.aold ? 1e300 : 0.0;
+#pragma unroll
+        for (int k = 0; k < TPL; ++k) {
+            px[k] = py[k] = pz[k] = 0.0;
+            ps[k] = 0.0;
+            const int i = lane + 32 * k;
+            if (k < nk && i < nt) {
+                const int p = A.tpos ? (int)A.tpos[t0 + i] : t0 + i;
+                float mf, hf;
+                load_src(A.src + p, px[k], py[k], pz[k], mf, hf);
+                ps[k] = A.ssoft[p];
+                lx = fmin(lx, px[k]); hx = fmax(hx, px[k]);
+                ly = fmin(ly, py[k]); hy = fmax(hy, py[k]);
+                lz = fmin(lz, pz[k]); hz = fmax(hz, pz[k]);
+                emax = fmax(emax, ps[k]);
+                if (A.aold) amin = fmin(amin, A.aold[t0 + i]);
+            }
+        }
+        lx = wmin(lx); ly = wmin(ly); lz = wmin(lz);
+        hx = wmax(hx); hy = wmax(hy); hz = wmax(hz);
+        emax = wmax(emax);
+        if (A.aold) amin = wmin(amin);
+        const double gcx = 0.5 * (lx + hx), gcy = 0.5 * (ly + hy), gcz = 0.5 * (lz + hz);
+
+        // ---- evaluation lanes: lane = slice * NT + target ---------------------------------
+        int lg = 5;
+        if (nt <= 16) lg = 32 - __clz(nt - 1);  // NT = next power of two >= nt (nt >= 1)
+        if (nt <= 1) lg = 0;
+        const int NT = 1 << lg, NS = 32 >> lg;
+        const int ti = lane & (NT - 1), slice = lane >> lg;
+        float tx[TPL], ty[TPL], tz[TPL], th[TPL];
+        float sx[TPL], sy[TPL], sz[TPL], cxk[TPL], cyk[TPL], czk[TPL];
+        double pot[TPL];
+#pragma unroll
+        for (int k = 0; k < TPL; ++k) {
+            const double qx = __shfl_sync(kFull, px[k], ti);
+            const double qy = __shfl_sync(kFull, py[k], ti);
+            const double qz = __shfl_sync(kFull, pz[k], ti);
+            const double qs = __shfl_sync(kFull, ps[k], ti);
+            tx[k] = (float)(qx - gcx);
+            ty[k] = (float)(qy - gcy);
+            tz[k] = (float)(qz - gcz);
+            th[k] = (float)qs;
+            sx[k] = sy[k] = sz[k] = cxk[k] = cyk[k] = czk[k] = 0.0f;
+            pot[k] = 0.0;
+        }
+
+        // ---- evaluate the list against the targets ----------------------------------------
+        auto flush = [&](int nlist) {
+            __syncwarp();
+            float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
+#pragma unroll
+            for (int k = 0; k < TPL; ++k) ax_[k] = ay_[k] = az_[k] = ap_[k] = 0.0f;
+            unsigned zero = 0;
+            for (int j = slice; j < nlist; j += NS) {
+                const float4 e = pm[j];
+                const float hj = hs[j];
+#pragma unroll
+                for (int k = 0; k < TPL; ++k) {
+                    if (k < nk) {
+                        const float dx = e.x - tx[k], dy = e.y - ty[k], dz = e.z - tz[k];
+                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float hh = fmaxf(th[k], hj);
+                        float f, p;
+                        if (r2 >= hh * hh && r2 > 0.0f) {
+                            const float ri = rsqrtf(r2);
+                            const float mri = e.w * ri;
+                            f = mri * ri * ri;
+                            p = -mri;
+                        } else {
+                            spline_pair(r2, hh, e.w, f, p);
+                        }
+                        if (COUNT) zero += (r2 == 0.0f);
+                        ax_[k] = fmaf(dx, f, ax_[k]);
+                        ay_[k] = fmaf(dy, f, ay_[k]);
+                        az_[k] = fmaf(dz, f, az_[k]);
+                        if (WANT_POT) ap_[k] += p;
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < TPL; ++k) {
+                kahan_add(sx[k], cxk[k], ax_[k]);
+                kahan_add(sy[k], cyk[k], ay_[k]);
+                kahan_add(sz[k], czk[k], az_[k]);
+                if (WANT_POT) pot[k] += (double)ap_[k];
+            }
+            if (COUNT) {
+                c_zero += zero;
+                c_flush += (lane == 0);
+            }
+            __syncwarp();
+        };
+
+        // ---- traversal ----------------------------------------------------------------------
+        int top = 1;
+        if (lane == 0) stk[0] = 0;
+        __syncwarp();
+        int nlist = 0;
+        bool overflow = false;
+        while (top > 0) {
+            const int npop = min(top, 32);
+            top -= npop;
+            const int node = lane < npop ? stk[top + lane] : -1;
+            __syncwarp();
+            bool accept = false, expand = false, push = false;
+            NodeV nd;
+            nd.first = -1; nd.nchild = 0; nd.plo = nd.phi = 0;
+            nd.cx = nd.cy = nd.cz = nd.mass = nd.s = 0.0; nd.len = nd.soft = 0.0f;
+            if (node >= 0) {
+                nd = load_node(A.nodes + node);
+                const bool leaf = nd.first < 0;
+                const double dx = fmax(0.0, fmax(lx - nd.cx, nd.cx - hx));
+                const double dy = fmax(0.0, fmax(ly - nd.cy, nd.cy - hy));
+                const double dz = fmax(0.0, fmax(lz - nd.cz, nd.cz - hz));
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                bool open = true;
+                if (LEAF_ACCEPT || !leaf)
+                    open = open_node(r2, (double)nd.len, nd.s, nd.mass, (double)nd.soft, emax, amin,
+                                     A.theta2, dx, dy, dz);
+                if (!open) accept = true;
+                else if (leaf) expand = true;
+                else push = true;
+            }
+            if (COUNT && lane == 0) c_nodes += npop;
+
+            // children of opened interior nodes
+            const int nch = push ? nd.nchild : 0;
+            const int incl = warp_incl_scan_i(nch);
+            const int tot = __shfl_sync(kFull, incl, 31);
+            if (top + tot > A.stack_cap) { overflow = true; break; }
+            for (int c = 0; c < nch; ++c) stk[top + incl - nch + c] = nd.first + c;
+            top += tot;
+            __syncwarp();  // pushes are visible to the lanes that pop them
+            if (COUNT) c_maxtop = max(c_maxtop, top);
+
+            // accepted nodes: monopoles
+            const unsigned am = __ballot_sync(kFull, accept);
+            if (am) {
+                const int na = __popc(am);
+                if (nlist + na > kListCap) { flush(nlist); nlist = 0; }
+                if (accept) {
+                    const int pos = nlist + __popc(am & lt_mask);
+                    pm[pos] = make_float4((float)(nd.cx - gcx), (float)(nd.cy - gcy),
+                                          (float)(nd.cz - gcz), (float)nd.mass);
+                    hs[pos] = nd.soft;
+                }
+                nlist += na;
+                if (COUNT && lane == 0) c_multi += (unsigned long long)na * nt;
+            }
+
+            // expanded leaves: their particles
+            const unsigned em = __ballot_sync(kFull, expand);
+            if (em) {
+                const int cnt = expand ? nd.phi - nd.plo : 0;
+                const int inc2 = warp_incl_scan_i(cnt);
+                const int tot2 = __shfl_sync(kFull, inc2, 31);
+                s_lo[w][lane] = nd.plo;
+                s_pre[w][lane] = inc2 - cnt;
+                __syncwarp();
+                if (COUNT && lane == 0) c_pairs += (unsigned long long)tot2 * nt;
+                int done = 0;
+                while (done < tot2) {
+                    if (nlist == kListCap) { flush(nlist); nlist = 0; }
+                    const int chunk = min(tot2 - done, kListCap - nlist);
+                    for (int j = lane; j < chunk; j += 32) {
+                        const int q = done + j;
+                        // owner: the last lane whose exclusive prefix is <= q
+                        int l = 0;
+#pragma unroll
+                        for (int step = 16; step > 0; step >>= 1)
+                            if (s_pre[w][l + step] <= q) l += step;
+                        const int p = s_lo[w][l] + (q - s_pre[w][l]);
+                        double qx, qy, qz;
+                        float qm, qh;
+                        load_src(A.src + p, qx, qy, qz, qm, qh);
+                        pm[nlist + j] = make_float4((float)(qx - gcx), (float)(qy - gcy),
+                                                    (float)(qz - gcz), qm);
+                        hs[nlist + j] = qh;
+                    }
+                    nlist += chunk;
+                    done += chunk;
+                    __syncwarp();
+                }
+            }
+        }
+        if (overflow) {
+            if (lane == 0) atomicExch(A.error, 1);
+            continue;
+        }
+        if (nlist > 0) flush(nlist);
+
+        // ---- combine slices and write -------------------------------------------------------
+#pragma unroll
+        for (int k = 0; k < TPL; ++k) {
+            double vx = (double)sx[k] - (double)cxk[k];
+            double vy = (double)sy[k] - (double)cyk[k];
+            double vz = (double)sz[k] - (double)czk[k];
+            double vp = pot[k];
+            for (int o = NT; o < 32; o <<= 1) {
+                vx += __shfl_xor_sync(kFull, vx, o);
+                vy += __shfl_xor_sync(kFull, vy, o);
+                vz += __shfl_xor_sync(kFull, vz, o);
+                if (WANT_POT) vp += __shfl_xor_sync(kFull, vp, o);
+            }
+            const int i = ti + 32 * k;
+            if (slice == 0 && k < nk && i < nt) {
+                const int idx = t0 + i;
+                const int o = A.out_map ? (int)A.out_map[idx] : idx;
+                if (A.ax) {
+                    A.ax[o] = A.G * vx;
+                    A.ay[o] = A.G * vy;
+                    A.az[o] = A.G * vz;
+                }
+                if (WANT_POT && A.phi) A.phi[o] = A.G * vp;
+            }
+        }
+    }
+    if (COUNT) {
+        if (lane == 0) {
+            atomicAdd(&A.stats[0], c_nodes);
+            atomicAdd(&A.stats[1], c_multi);
+            atomicAdd(&A.stats[2], c_pairs);
+            atomicAdd(&A.stats[4], c_flush);
+            atomicMax(&A.stats[5], (unsigned long long)c_maxtop);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c_zero += __shfl_xor_sync(kFull, c_zero, o);
+        if (lane == 0) atomicAdd(&A.stats[3], c_zero);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Groups
+// ---------------------------------------------------------------------------------------------
+
+// Mark the first tree position of every leaf (mode 0) or group node (mode 1).
+__global__ void mark_group_nodes_kernel(const GNode* __restrict__ nodes, const int* __restrict__ parent,
+                                        int64_t n_nodes, int mode, int gmax, uint32_t* __restrict__ flag) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const GNode& nd = nodes[i];
+        const int cnt = nd.phi - nd.plo;
+        if (cnt <= 0) continue;
+        bool mark;
+        if (mode == 0) {
+            mark = nd.first < 0;
+        } else {
+            const int pa = parent[i];
+            const bool parent_big = pa < 0 || (nodes[pa].phi - nodes[pa].plo) > gmax;
+            mark = (cnt <= gmax && parent_big) || (nd.first < 0 && cnt > gmax);
+        }
+        if (mark) flag[nd.plo] = 1u;
+    }
+}
+
+// Per-tree-position group node id (mode 1), for explicit target lists.
+__global__ void fill_group_id_kernel(const GNode* __restrict__ nodes, const int* __restrict__ parent,
+                                     int64_t n_nodes, int gmax, int* __restrict__ gid) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const GNode& nd = nodes[i];
+        const int cnt = nd.phi - nd.plo;
+        if (cnt <= 0) continue;
+        const int pa = parent[i];
+        const bool parent_big = pa < 0 || (nodes[pa].phi - nodes[pa].plo) > gmax;
+        if ((cnt <= gmax && parent_big) || (nd.first < 0 && cnt > gmax))
+            for (int p = nd.plo; p < nd.phi; ++p) gid[p] = (int)i;
+    }
+}
+
+// Group starts over explicit targets: a new group where the key changes or is negative.
+__global__ void target_flags_kernel(const uint32_t* __restrict__ targets, int64_t nt, int mode,
+                                    int param, const uint32_t* __restrict__ rank,
+                                    const int* __restrict__ leaf_of, const int* __restrict__ gid,
+                                    uint32_t* __restrict__ tpos, uint32_t* __restrict__ flag) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nt;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = targets[k];
+        const uint32_t pos = rank[p];
+        tpos[k] = pos;
+        bool start = (k == 0);
+        if (!start) {
+            if (mode == GT_GROUP_LEAF) {
+                const int a = leaf_of[p], b = leaf_of[targets[k - 1]];
+                start = a != b || a < 0;
+            } else if (mode == GT_GROUP_NODE) {
+                const int a = gid[pos], b = gid[rank[targets[k - 1]]];
+                start = a != b || a < 0;
+            } else if (mode == GT_GROUP_BATCH) {
+                start = (k % param) == 0;
+            } else {
+                start = true;
+            }
+        }
+        flag[k] = start ? 1u : 0u;
+    }
+}
+
+__global__ void compact_starts_kernel(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos,
+                                      int64_t n, int64_t* __restrict__ starts) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        if (flag[i]) starts[pos[i]] = i;
+}
+
+// Split groups longer than kmax into consecutive chunks (each walks with its own, tighter box).
+__global__ void chunk_count_kernel(const int64_t* __restrict__ starts, int64_t ng, int64_t n_end,
+                                   int kmax, uint32_t* __restrict__ nchunk) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ng;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = starts[g], e = (g + 1 < ng) ? starts[g + 1] : n_end;
+        nchunk[g] = (uint32_t)((e - s + kmax - 1) / kmax);
+    }
+}
+
+__global__ void chunk_emit_kernel(const int64_t* __restrict__ starts, int64_t ng, int64_t n_end, int kmax,
+                                  const uint32_t* __restrict__ coff, int2* __restrict__ groups) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ng;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = starts[g], e = (g + 1 < ng) ? starts[g + 1] : n_end;
+        int64_t o = coff[g];
+        for (int64_t a = s; a < e; a += kmax, ++o) groups[o] = make_int2((int)a, (int)std::min<int64_t>(a + kmax, e));
+    }
+}
+
+int grid1d(gt_context* ctx, int64_t n) {
+    const int64_t want = (n + 255) / 256;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->num_sms * 8));
+}
+
+uint32_t read_u32(gt_context* ctx, const uint32_t* dev) {
+    check_cuda(cudaMemcpyAsync(ctx->pinned, dev, 4, cudaMemcpyDeviceToHost, ctx->stream), "d2h");
+    check_cuda(cudaStreamSynchronize(ctx->stream), "sync");
+    uint32_t v;
+    std::memcpy(&v, ctx->pinned, 4);
+    return v;
+}
+
+// Turn group starts (flag array over n items) into chunked [start, end) pairs in `out`.
+// Returns the number of chunks.  `out` is allocated with cudaMalloc when own_out is set.
+int64_t finish_groups(gt_context* ctx, const uint32_t* flag, int64_t n, int kmax, int2** out, bool own_out) {
+    uint32_t* pos = (uint32_t*)scratch(ctx, kSlotScanA, (size_t)n * 4);
+    uint32_t* total = (uint32_t*)scratch(ctx, kSlotCounters, 64);
+    scan_exclusive_u32(ctx, flag, pos, n, total);
+    const int64_t ng = read_u32(ctx, total);
+    int64_t* starts = (int64_t*)scratch(ctx, kSlotGroupsA, (size_t)(ng + 1) * 8);
+    compact_starts_kernel<<<grid1d(ctx, n), 256, 0, ctx->stream>>>(flag, pos, n, starts);
+    check_launch(ctx, "compact_starts_kernel");
+    uint32_t* nchunk = (uint32_t*)scratch(ctx, kSlotNodeTmp1, (size_t)std::max<int64_t>(ng, 1) * 4);
+    uint32_t* coff = (uint32_t*)scratch(ctx, kSlotNodeTmp2, (size_t)std::max<int64_t>(ng, 1) * 4);
+    chunk_count_kernel<<<grid1d(ctx, ng), 256, 0, ctx->stream>>>(starts, ng, n, kmax, nchunk);
+    check_launch(ctx, "chunk_count_kernel");
+    scan_exclusive_u32(ctx, nchunk, coff, ng, total);
+    const int64_t nc = read_u32(ctx, total);
+    int2* groups;
+    if (own_out) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, (size_t)std::max<int64_t>(nc, 1) * sizeof(int2)) != cudaSuccess) {
+            cudaGetLastError();
+            throw Fail{GT_ERR_NOMEM, "cudaMalloc for the group list failed"};
+        }
+        groups = (int2*)p;
+    } else {
+        groups = (int2*)scratch(ctx, kSlotGroupsB, (size_t)std::max<int64_t>(nc, 1) * sizeof(int2));
+    }
+    chunk_emit_kernel<<<grid1d(ctx, ng), 256, 0, ctx->stream>>>(starts, ng, n, kmax, coff, groups);
+    check_launch(ctx, "chunk_emit_kernel");
+    *out = groups;
+    return nc;
+}
+
+template <int TPL, bool LA, bool POT, bool CNT>
+void launch_walk(gt_context* ctx, const WalkArgs& a, int blocks, int warps) {
+    walk_kernel<TPL, LA, POT, CNT><<<blocks, warps * 32, 0, ctx->stream>>>(a);
+    check_launch(ctx, "walk_kernel");
+}
+
+template <int TPL, bool LA, bool POT>
+void dispatch_count(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool cnt) {
+    if (cnt) launch_walk<TPL, LA, POT, true>(ctx, a, blocks, warps);
+    else launch_walk<TPL, LA, POT, false>(ctx, a, blocks, warps);
+}
+
+template <int TPL>
+void dispatch(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la, bool pot, bool cnt) {
+    if (la) {
+        if (pot) dispatch_count<TPL, true, true>(ctx, a, blocks, warps, cnt);
+        else dispatch_count<TPL, true, false>(ctx, a, blocks, warps, cnt);
+    } else {
+        if (pot) dispatch_count<TPL, false, true>(ctx, a, blocks, warps, cnt);
+        else dispatch_count<TPL, false, false>(ctx, a, blocks, warps, cnt);
+    }
+}
+
+template <int TPL, bool LA, bool POT, bool CNT>
+int occupancy_blocks(int warps) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<TPL, LA, POT, CNT>, warps * 32, 0);
+    return std::max(1, nb);
+}
+
+}  // namespace
+
+void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
+    gt_tree* t = const_cast<gt_tree*>(tc);  // only the group cache is mutated
+    cudaStream_t st = ctx->stream;
+    const bool all = rq.targets == nullptr;
+    const int64_t nt = all ? t->n_live : rq.n_targets;
+    ctx->stats = gt_walk_stats{};
+    ctx->stats.targets = nt;
+    if (nt <= 0) return;
+    if (nt > (int64_t)INT32_MAX) throw Fail{GT_ERR_INVALID, "too many targets for one walk"};
+
+    int mode = rq.group_mode;
+    int param = rq.group_param;
+    if (mode == GT_GROUP_NODE && param <= 0) param = 32;
+    if (mode == GT_GROUP_BATCH && param <= 0) mode = GT_GROUP_LEAF;
+    int kmax = 32;
+    if (mode == GT_GROUP_NODE && param > 32) kmax = 64;
+    if (mode == GT_GROUP_BATCH && param > 32) kmax = 64;
+    const int tpl = kmax > 32 ? 2 : 1;
+
+    // ---- groups -------------------------------------------------------------------------------
+    int2* groups = nullptr;
+    int64_t ng = 0;
+    const uint32_t* tpos = nullptr;
+    if (all) {
+        for (auto& c : t->group_cache)
+            if (c.mode == mode && c.param == param && c.kmax == kmax) { groups = c.groups; ng = c.n_groups; }
+        if (!groups) {
+            const int64_t n = t->n_live;
+            uint32_t* flag = (uint32_t*)scratch(ctx, kSlotTargets, (size_t)n * 4);
+            check_cuda(cudaMemsetAsync(flag, 0, (size_t)n * 4, st), "memset");
+            if (mode == GT_GROUP_LEAF || mode == GT_GROUP_NODE) {
+                mark_group_nodes_kernel<<<grid1d(ctx, t->n_nodes), 256, 0, st>>>(
+                    t->nodes, t->parent, t->n_nodes, mode == GT_GROUP_LEAF ? 0 : 1, param, flag);
+                check_launch(ctx, "mark_group_nodes_kernel");
+            } else {
+                // fixed windows (or one group per target) over the tree order
+                target_flags_kernel<<<grid1d(ctx, n), 256, 0, st>>>(
+                    t->order, n, mode == GT_GROUP_BATCH ? GT_GROUP_BATCH : GT_GROUP_SINGLE, param,
+                    t->rank, t->leaf_of, nullptr, (uint32_t*)scratch(ctx, kSlotGroupKey, (size_t)n * 4),
+                    flag);
+                check_launch(ctx, "target_flags_kernel");
+            }
+            ng = finish_groups(ctx, flag, n, kmax, &groups, true);
+            gt_tree::GroupCache c;
+            c.mode = mode; c.param = param; c.kmax = kmax; c.groups = groups; c.n_groups = ng;
+            t->group_cache.push_back(c);
+        }
+    } else {
+        uint32_t* tp = (uint32_t*)scratch(ctx, kSlotGroupKey, (size_t)nt * 4);
+        uint32_t* flag = (uint32_t*)scratch(ctx, kSlotTargets, (size_t)nt * 4);
+        int* gid = nullptr;
+        if (mode == GT_GROUP_NODE) {
+            gid = (int*)scratch(ctx, kSlotNodeTmp0, (size_t)std::max<int64_t>(t->n, 1) * 4);
+            check_cuda(cudaMemsetAsync(gid, 0xff, (size_t)std::max<int64_t>(t->n, 1) * 4, st), "memset");
+            fill_group_id_kernel<<<grid1d(ctx, t->n_nodes), 256, 0, st>>>(t->nodes, t->parent, t->n_nodes,
+                                                                          param, gid);
+            check_launch(ctx, "fill_group_id_kernel");
+        }
+        target_flags_kernel<<<grid1d(ctx, nt), 256, 0, st>>>(rq.targets, nt, mode, param, t->rank,
+                                                             t->leaf_of, gid, tp, flag);
+        check_launch(ctx, "target_flags_kernel");
+        ng = finish_groups(ctx, flag, nt, kmax, &groups, false);
+        tpos = tp;
+    }
+    ctx->stats.groups = ng;
+    if (ng <= 0) return;
+
+    // ---- launch -------------------------------------------------------------------------------
+    const int warps = (rq.block_warps > 0 && rq.block_warps <= kMaxWarps) ? rq.block_warps : kMaxWarps;
+    int per_sm;
+    if (tpl == 1)
+        per_sm = rq.leaf_accept ? occupancy_blocks<1, true, false, false>(warps)
+                                : occupancy_blocks<1, false, false, false>(warps);
+    else
+        per_sm = occupancy_blocks<2, true, false, false>(warps);
+    const int64_t want_blocks = (ng + warps - 1) / warps;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want_blocks, (int64_t)per_sm * ctx->num_sms));
+    int stack_cap = rq.stack_capacity > 0 ? rq.stack_capacity : 256 * std::max(1, t->n_levels) + 32;
+    stack_cap = (stack_cap + 31) & ~31;
+
+    WalkArgs a;
+    a.nodes = t->nodes;
+    a.src = t->src;
+    a.ssoft = t->ssoft;
+    a.tpos = tpos;
+    a.aold = rq.aold;
+    a.groups = groups;
+    a.n_groups = (int)ng;
+    a.theta2 = rq.theta * rq.theta;
+    a.G = rq.G;
+    a.ax = rq.want_acc ? rq.ax : nullptr;
+    a.ay = rq.want_acc ? rq.ay : nullptr;
+    a.az = rq.want_acc ? rq.az : nullptr;
+    a.phi = rq.phi;
+    a.out_map = (all && rq.out_original) ? t->order : nullptr;
+    const int total_warps = blocks * warps;
+    unsigned long long* ctr = (unsigned long long*)scratch(ctx, kSlotCounters, 256);
+    a.next_group = (unsigned int*)(ctr + 8);
+    a.stats = ctr;
+    a.error = (int*)(ctr + 9);
+    const bool want_pot = rq.want_phi && rq.phi;
+
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        a.stack = (int*)scratch(ctx, kSlotStack, (size_t)total_warps * stack_cap * 4);
+        a.stack_cap = stack_cap;
+        check_cuda(cudaMemsetAsync(ctr, 0, 96, st), "memset counters");
+        check_cuda(cudaEventRecord(ctx->ev0, st), "event");
+        if (tpl == 1) dispatch<1>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count);
+        else dispatch<2>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count);
+        check_cuda(cudaEventRecord(ctx->ev1, st), "event");
+        if (!rq.count && attempt == 0 && rq.stack_capacity == 0) {
+            // the default capacity is a proven bound: no read-back needed on the fast path
+            break;
+        }
+        check_cuda(cudaMemcpyAsync(ctx->pinned, ctr, 80, cudaMemcpyDeviceToHost, st), "stats d2h");
+        check_cuda(cudaStreamSynchronize(st), "sync");
+        unsigned long long h[10];
+        std::memcpy(h, ctx->pinned, 80);
+        if ((int)h[9] == 0) {
+            ctx->stats.nodes_visited = (int64_t)h[0];
+            ctx->stats.multipole = (int64_t)h[1];
+            ctx->stats.pairs = (int64_t)h[2] - (int64_t)h[3];
+            ctx->stats.list_flushes = (int64_t)h[4];
+            ctx->stats.max_stack = (int64_t)h[5];
+            break;
+        }
+        if (attempt == 2) throw Fail{GT_ERR_OVERFLOW, "walk stack overflow"};
+        stack_cap *= 2;
+    }
+}
+
+}  // namespace gt

@@ -1,0 +1,220 @@
+/*
+ * gt.h — C ABI of the B200-native tree-gravity library (libgt.so).
+ *
+ * This is the drop-in boundary for GIZMO's shared-memory tree-gravity path.  Each entry point
+ * replaces one function of the reference's call surface, shmem/tree.h:359-451 (cited per entry),
+ * or the reference's only existing C-ABI, shmem_cuda_accel_bruteforce (shmem/grav_cuda.cu:188-192).
+ * The C++ shim in gizmo_shared_memory_b200/shim/ wraps these in the exact shmem:: signatures so
+ * shmem/bench_treeforce.cc and shmem/test_tree.cc compile against it unchanged.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  `mem` says where every array argument of a call lives:
+ *    GT_MEM_HOST (ordinary or pinned host memory; the call copies in and out and returns when the
+ *    results are on the host) or GT_MEM_DEVICE (device pointers on the context's device; the call
+ *    enqueues on the context's stream and returns when the work is complete unless
+ *    gt_walk_options.async is set).
+ *  - Every entry point returns a gt_status; nothing calls exit().  A failing call leaves the
+ *    context usable and records a message for gt_last_error().
+ *  - Outputs are indexed parallel to `targets` and multiplied by G, as in the reference
+ *    (shmem/tree.h:389-394).  targets == NULL means "every live particle in tree order", i.e.
+ *    targets = orderbuf (what shmem/bench_treeforce.cc:41 passes).
+ *  - One context per host thread; one CUDA stream per context.  Trees may be used by any context
+ *    on the same device.
+ *  - Options the GPU path does not implement (adaptive-softening zeta, tidal tensor, jerk, lazy
+ *    drift, sink-direct opening, periodic boxes) are rejected with GT_ERR_UNSUPPORTED; there is
+ *    no CPU fallback.
+ */
+#ifndef GT_H
+#define GT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GT_VERSION 1
+
+#if defined(__GNUC__)
+#define GT_API __attribute__((visibility("default")))
+#else
+#define GT_API
+#endif
+
+typedef enum {
+    GT_OK = 0,
+    GT_ERR_INVALID = 1,     /* bad argument (null pointer, negative size, unknown option) */
+    GT_ERR_CUDA = 2,        /* CUDA runtime error; see gt_last_error() */
+    GT_ERR_NOMEM = 3,       /* device allocation failed */
+    GT_ERR_UNSUPPORTED = 4, /* option of the reference not implemented on the GPU path */
+    GT_ERR_OVERFLOW = 5,    /* a walk stack or list capacity was exceeded and could not be grown */
+    GT_ERR_TIMEOUT = 6,     /* a bounded device-side wait gave up */
+    GT_ERR_NONFINITE = 7,   /* input validation found a NaN or Inf */
+    GT_ERR_DEVICE = 8       /* no usable CUDA device, or the tree belongs to another device */
+} gt_status;
+
+enum { GT_MEM_HOST = 0, GT_MEM_DEVICE = 1 };
+/* Sort keys.  Both quantise each axis to 20 bits exactly as shmem::build (shmem/tree.cc:409-417),
+ * so both give the same cells and the same tree; only the order of children differs. */
+enum { GT_KEY_PEANO = 0, GT_KEY_MORTON = 1 };
+/* Target grouping of the walk. */
+enum {
+    GT_GROUP_LEAF = 0,  /* consecutive targets sharing a leaf: accel_grouped batch <= 0 (tree.cc:656-667) */
+    GT_GROUP_BATCH = 1, /* fixed windows of `batch` consecutive targets: accel_grouped batch > 0 */
+    GT_GROUP_NODE = 2,  /* consecutive targets sharing the deepest ancestor holding <= group_max particles */
+    GT_GROUP_SINGLE = 3 /* one walk per target (accel / potential, tree.cc:528, 899) */
+};
+/* Opening criterion used inside the walk. */
+enum { GT_MAC_PLAIN = 0, GT_MAC_LEARNED = 1 };
+/* Precision of gt_direct. */
+enum { GT_DIRECT_FP64 = 0, GT_DIRECT_FP32 = 1 };
+/* Output order of a walk over targets == NULL. */
+enum { GT_OUT_TARGETS = 0, GT_OUT_ORIGINAL = 1 };
+
+typedef struct gt_context gt_context;
+typedef struct gt_tree gt_tree;
+
+typedef struct {
+    int key_mode;             /* GT_KEY_PEANO (default) or GT_KEY_MORTON */
+    int leaf_max;             /* particles per leaf, default 16 (shmem/tree.h:357) */
+    int max_level;            /* deepest level, default 20 (shmem/tree.h:358) */
+    long long randomize_seed; /* >= 0: RANDOMIZE_GRAVTREE root shift and doubling (tree.cc:381-393) */
+    int nodelta;              /* 1: opening radius = side only (SHMEM_TREE_NODELTA, tree.cc:512-519) */
+    int validate;             /* 1: reject non-finite positions/masses/softenings (default 1) */
+    double shift[3];          /* SHMEM_TREE_SHIFT fractions of a side (tree.cc:400-407); 0 = none */
+} gt_build_options;
+
+typedef struct {
+    int group_mode;      /* GT_GROUP_* ; default GT_GROUP_LEAF */
+    int group_max;       /* GT_GROUP_NODE: most particles per group node (default 32) */
+    int mac;             /* GT_MAC_PLAIN (default) or GT_MAC_LEARNED */
+    int out_order;       /* GT_OUT_TARGETS (default) or GT_OUT_ORIGINAL (targets == NULL only) */
+    int async;           /* GT_MEM_DEVICE only: 1 = return without synchronising the stream */
+    int count;           /* 1 = collect interaction counts (gt_walk_stats); slightly slower */
+    int block_warps;     /* warps per block of the walk kernel; 0 = autotuned default */
+    int list_capacity;   /* interaction-list entries per warp; 0 = default */
+    int stack_capacity;  /* node-stack entries per warp; 0 = default (always sufficient) */
+    int dtype_out_f32;   /* reserved, must be 0 */
+} gt_walk_options;
+
+typedef struct {
+    int64_t n;          /* particles passed to gt_build */
+    int64_t n_live;     /* particles with m > 0 (the tree's) */
+    int64_t n_nodes;
+    int32_t n_levels;
+    int32_t root;       /* always 0 */
+    double center[3];   /* root cell centre */
+    double side;        /* root cell side */
+    double build_ms[7]; /* bbox, keys, sort, structure, moments, pack, total (device time) */
+} gt_tree_info;
+
+typedef struct {
+    int64_t groups, nodes_visited, multipole, pairs, targets;
+    int64_t max_stack, list_flushes;
+    double walk_ms;    /* device time of the walk kernel(s) of the last walk call */
+} gt_walk_stats;
+
+/* Node arrays of gt_tree_download, in the reference's conventions (shmem/tree.h:228-247):
+ * first/next threading, plo/phi index orderbuf, root = 0.  Any pointer may be null. */
+typedef struct {
+    double *cx, *cy, *cz, *mass, *size, *delta, *soft, *gcx, *gcy, *gcz;
+    int32_t *first, *next, *plo, *phi, *parent, *level;
+    double* w_s;   /* WNode::s = size + delta (tree.h:197) */
+    float* w_len;  /* WNode::len */
+    float* w_soft; /* WNode::soft */
+} gt_node_arrays;
+
+/* ---- library / context ------------------------------------------------------------------- */
+GT_API int gt_version(void);
+GT_API const char* gt_status_string(int status);
+GT_API void gt_build_options_default(gt_build_options* opt);
+GT_API void gt_walk_options_default(gt_walk_options* opt);
+
+/* Create a context on `device` with its own non-blocking stream.  No reference counterpart: the
+ * reference's state lives in process globals (grav_cuda.cu:143-153). */
+GT_API int gt_context_create(int device, gt_context** out);
+GT_API int gt_context_destroy(gt_context* ctx);
+/* Message of the last failed call on this context ("" if none). */
+GT_API const char* gt_last_error(const gt_context* ctx);
+/* The context's cudaStream_t (as void*), and a way to replace it (the caller keeps ownership). */
+GT_API int gt_context_get_stream(gt_context* ctx, void** stream);
+GT_API int gt_context_set_stream(gt_context* ctx, void* stream);
+GT_API int gt_synchronize(gt_context* ctx);
+/* Number of kernels this library launched on the context so far. */
+GT_API int gt_launch_count(const gt_context* ctx, uint64_t* count);
+
+/* ---- tree ---------------------------------------------------------------------------------- */
+/* Build the tree of n particles.  Replaces shmem::build (shmem/tree.h:384-385, tree.cc:350-526):
+ * bbox, 20-bit quantisation, key sort, octree with LEAF_MAX / MAX_LEVEL, monopole moments,
+ * next/first threading, rank, leaf_of.  Massless particles (m <= 0) are left out of the tree
+ * (tree.cc:355-359).  soft may be null (all zero).  The tree keeps its own device copy of the
+ * particles, so the input arrays may be freed after the call. */
+GT_API int gt_build(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
+             const double* m, const double* soft, int mem, const gt_build_options* opt,
+             gt_tree** out);
+GT_API int gt_tree_free(gt_tree* tree);
+GT_API int gt_tree_info_get(const gt_tree* tree, gt_tree_info* info);
+/* Copy the tree to host arrays in the reference's layout: orderbuf (n_live), rank (n; UINT32_MAX
+ * for massless particles), leaf_of (n; -1 for massless), nodes (n_nodes each).  Fills the fields
+ * of shmem::Tree that the engine and the benches read (tree.h:228-247).  Any pointer may be null. */
+GT_API int gt_tree_download(gt_context* ctx, const gt_tree* tree, uint32_t* orderbuf, uint32_t* rank,
+                     int32_t* leaf_of, const gt_node_arrays* nodes);
+/* Sorted keys (n_live, u64) of the tree: PH or Morton per the build's key_mode. */
+GT_API int gt_tree_keys(gt_context* ctx, const gt_tree* tree, uint64_t* keys);
+
+/* ---- walks --------------------------------------------------------------------------------- */
+/* Grouped walk.  Replaces shmem::accel_grouped (shmem/tree.h:428-440, tree.cc:626-897) for the
+ * gravity-only case (tidal = jerk = lazy = NULL, sink_direct_radius = 0).  batch <= 0 groups
+ * targets by leaf, batch > 0 in fixed windows, unless opt->group_mode overrides it.
+ * aold (may be NULL) is ErrTolForceAcc*|a_prev|/G per target (tree.h:389-391); theta > 0 adds the
+ * Barnes-Hut test.  phi (may be NULL) receives the potential from the same walk. */
+GT_API int gt_accel_grouped(gt_context* ctx, const gt_tree* tree, int64_t n_targets,
+                     const uint32_t* targets, const double* aold, double theta, double G, int batch,
+                     const gt_walk_options* opt, int mem, double* ax, double* ay, double* az,
+                     double* phi);
+/* Per-target walk (leaves always direct-summed).  Replaces shmem::accel (tree.h:392-394,
+ * tree.cc:528-582). */
+GT_API int gt_accel(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
+             double theta, double G, const double* aold, int mem, double* ax, double* ay,
+             double* az);
+/* Per-target potential walk.  Replaces shmem::potential (tree.h:446-447, tree.cc:899-944). */
+GT_API int gt_potential(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
+                 double theta, double G, const double* aold, int mem, double* phi);
+/* Counts and device time of the last walk on this context (SHMEM_COUNT_WALK, tree.cc:671-677). */
+GT_API int gt_walk_stats_get(const gt_context* ctx, gt_walk_stats* stats);
+
+/* aold[i] = alpha * |a_i| / G, the relative-criterion input the engine forms from the previous
+ * force (shmem/mfm.cc:743-751). */
+GT_API int gt_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay, const double* az,
+                 double alpha, double G, int mem, double* aold);
+
+/* ---- direct sum ---------------------------------------------------------------------------- */
+/* O(n_targets * n) direct summation with the walk's pair rule (kernel of the larger softening,
+ * self and r == 0 skipped).  GT_DIRECT_FP64 replaces shmem::accel_brute (tree.h:450-451,
+ * tree.cc:946-971); GT_DIRECT_FP32 (FP64 pair offset, FP32 arithmetic) replaces
+ * shmem_cuda_accel_bruteforce (grav_cuda.cu:188-247) without zeta terms or periodic wrap.
+ * targets index the n sources; phi may be NULL.  Results include the factor G. */
+GT_API int gt_direct(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
+              const double* m, const double* soft, int64_t n_targets, const uint32_t* targets,
+              double G, int precision, int mem, double* ax, double* ay, double* az, double* phi);
+
+/* ---- keys ---------------------------------------------------------------------------------- */
+/* Peano-Hilbert (and Morton) keys of the MPI code's domain decomposition: each coordinate mapped
+ * to [1,2) as (pos - corner)/len + 1 and its top `bits` mantissa bits taken
+ * (domain/domain.cc:2682-2702), then keyed by the table-driven Hilbert curve
+ * (system/peano.cc:297-355).  bits <= 42; the 126-bit keys come back as hi/lo halves (any output
+ * may be NULL). */
+GT_API int gt_peano_keys(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
+                  const double corner[3], double len, int bits, int mem, uint64_t* ph_hi,
+                  uint64_t* ph_lo, uint64_t* morton_hi, uint64_t* morton_lo);
+
+/* ---- measurement --------------------------------------------------------------------------- */
+/* FP32 and FP64 FMA throughput of this device's CUDA cores in TFLOP/s (independent FMA chains on
+ * every SM), the denominators of the walk's roofline fraction.  No reference counterpart. */
+GT_API int gt_measure_peaks(gt_context* ctx, double* fp32_tflops, double* fp64_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GT_H */

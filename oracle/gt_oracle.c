@@ -1,0 +1,584 @@
+/* ORACLE — test infrastructure only (see gt_oracle.h).
+ *
+ * A CPU restatement of the reference's shared-memory tree-gravity path, written in plain C so it
+ * builds anywhere gcc does and can be loaded by the tests on a GPU box where the reference tree is
+ * absent.  It is NOT part of the product: the CUDA library never links it, and no product code
+ * path calls it.  Every function cites the reference file:line it restates.
+ */
+#define _GNU_SOURCE
+#include "gt_oracle.h"
+
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define OR_LEAF_MAX 16 /* shmem/tree.h:357 */
+#define OR_MAX_LEVEL 20 /* shmem/tree.h:358 */
+
+/* ------------------------------------------------------------------------------------------- */
+/* Scalar kernels                                                                               */
+/* ------------------------------------------------------------------------------------------- */
+
+/* (1/r) dphi/dr of the cubic spline, Newtonian for r >= h.  shmem/tree.h:59-67. */
+double or_spline_force_over_r(double r, double h) {
+    const double hinv = 1.0 / h;
+    const double u = r * hinv;
+    if (u >= 1.0) return 1.0 / (r * r * r);
+    const double hinv3 = hinv * hinv * hinv;
+    if (u < 0.5) return hinv3 * (10.666666666666667 + u * u * (32.0 * u - 38.4));
+    return hinv3 * (21.333333333333332 - 48.0 * u + 38.4 * u * u - 10.666666666666667 * u * u * u -
+                    0.06666666666666667 / (u * u * u));
+}
+
+/* phi(r) of the same spline, -1/r for r >= h.  shmem/tree.h:72-80. */
+double or_spline_potential(double r, double h) {
+    const double hinv = 1.0 / h;
+    const double u = r * hinv;
+    if (u >= 1.0) return -1.0 / r;
+    if (u < 0.5) return hinv * (-2.8 + u * u * (5.333333333333333 + u * u * (6.4 * u - 9.6)));
+    return hinv * (-3.2 + 0.06666666666666667 / u +
+                   u * u * (10.666666666666667 + u * (-16.0 + u * (9.6 - 2.1333333333333333 * u))));
+}
+
+/* Node-opening decision, in the reference's order: softening overlap, Barnes-Hut (theta > 0),
+ * relative criterion M L^2 > r^4 aold (aold > 0; with aold == 0 and no theta: open), then the
+ * inside-node test.  shmem/tree.h:109-144. */
+int or_open_node(double r_sq, double len, double l_open, double node_mass, double node_maxsoft,
+                 double soft_target, double aold, double theta_sq, double adx, double ady, double adz) {
+    const double reach_t = soft_target + 0.6 * len;
+    const double reach_n = node_maxsoft + 0.6 * len;
+    if (r_sq < reach_t * reach_t || r_sq < reach_n * reach_n) return 1;
+    if (theta_sq > 0.0 && l_open * l_open >= theta_sq * r_sq) return 1;
+    if (aold > 0) {
+        if (node_mass * len * len > r_sq * r_sq * aold) return 1;
+    } else if (theta_sq <= 0.0) {
+        return 1;
+    }
+    const double lim = 0.6 * len;
+    return (adx < lim && ady < lim && adz < lim) ? 1 : 0;
+}
+
+/* ------------------------------------------------------------------------------------------- */
+/* Keys                                                                                         */
+/* ------------------------------------------------------------------------------------------- */
+
+/* Morton key of three 21-bit coordinates, x in the lowest bit of each triple.  shmem/tree.h:161-173. */
+static uint64_t spread_bits3(uint64_t v) {
+    uint64_t out = 0;
+    for (int b = 0; b < 21; ++b) out |= ((v >> b) & 1ull) << (3 * b);
+    return out;
+}
+uint64_t or_morton20(uint32_t a, uint32_t b, uint32_t c) {
+    return spread_bits3(a) | (spread_bits3(b) << 1) | (spread_bits3(c) << 2);
+}
+
+/* Peano-Hilbert state machine of system/peano.cc:192-292 (rottable3 / subpix3), stored as one
+ * table: entry = (next_state << 3) | key_digit, indexed [state][pix], pix = 4x + 2y + z. */
+static const uint16_t PH_STEP[48][8] = {
+    {0x120, 0x0e7, 0x0c9, 0x0de, 0x053, 0x054, 0x0ca, 0x0dd},
+    {0x0ef, 0x05c, 0x0c6, 0x0c5, 0x128, 0x05b, 0x0d1, 0x0d2},
+    {0x044, 0x043, 0x0cd, 0x0da, 0x0f7, 0x130, 0x0ce, 0x0d9},
+    {0x04b, 0x138, 0x0c2, 0x0c1, 0x04c, 0x0ff, 0x0d5, 0x0d6},
+    {0x141, 0x0c0, 0x166, 0x107, 0x142, 0x033, 0x165, 0x034},
+    {0x0c8, 0x03b, 0x10f, 0x03c, 0x149, 0x14a, 0x16e, 0x16d},
+    {0x023, 0x152, 0x024, 0x175, 0x0d0, 0x151, 0x117, 0x176},
+    {0x15a, 0x159, 0x17d, 0x17e, 0x02b, 0x0d8, 0x02c, 0x11f},
+    {0x10e, 0x119, 0x127, 0x0e0, 0x10d, 0x11a, 0x014, 0x013},
+    {0x101, 0x102, 0x0e8, 0x01b, 0x116, 0x115, 0x12f, 0x01c},
+    {0x10a, 0x11d, 0x003, 0x004, 0x109, 0x11e, 0x0f0, 0x137},
+    {0x105, 0x106, 0x00c, 0x13f, 0x112, 0x111, 0x00b, 0x0f8},
+    {0x0c7, 0x156, 0x100, 0x171, 0x074, 0x155, 0x073, 0x172},
+    {0x15e, 0x15d, 0x179, 0x17a, 0x0cf, 0x07c, 0x108, 0x07b},
+    {0x145, 0x064, 0x162, 0x063, 0x146, 0x0d7, 0x161, 0x110},
+    {0x06c, 0x0df, 0x06b, 0x118, 0x14d, 0x14e, 0x16a, 0x169},
+    {0x0e6, 0x14f, 0x0e5, 0x0b4, 0x131, 0x158, 0x132, 0x0b3},
+    {0x157, 0x140, 0x0bc, 0x0bb, 0x0ee, 0x139, 0x0ed, 0x13a},
+    {0x148, 0x121, 0x0a3, 0x122, 0x15f, 0x0f6, 0x0a4, 0x0f5},
+    {0x129, 0x0fe, 0x12a, 0x0fd, 0x150, 0x147, 0x0ab, 0x0ac},
+    {0x0e2, 0x093, 0x0e1, 0x168, 0x135, 0x094, 0x136, 0x17f},
+    {0x09b, 0x09c, 0x170, 0x167, 0x0ea, 0x13d, 0x0e9, 0x13e},
+    {0x084, 0x125, 0x16f, 0x126, 0x083, 0x0f2, 0x178, 0x0f1},
+    {0x12d, 0x0fa, 0x12e, 0x0f9, 0x08c, 0x08b, 0x177, 0x160},
+    {0x067, 0x020, 0x00e, 0x019, 0x114, 0x113, 0x00d, 0x01a},
+    {0x028, 0x11b, 0x001, 0x002, 0x06f, 0x11c, 0x016, 0x015},
+    {0x103, 0x104, 0x00a, 0x01d, 0x030, 0x077, 0x009, 0x01e},
+    {0x10c, 0x07f, 0x005, 0x006, 0x10b, 0x038, 0x012, 0x011},
+    {0x086, 0x007, 0x0a1, 0x040, 0x085, 0x0f4, 0x0a2, 0x0f3},
+    {0x00f, 0x0fc, 0x048, 0x0fb, 0x08e, 0x08d, 0x0a9, 0x0aa},
+    {0x0e4, 0x095, 0x0e3, 0x0b2, 0x017, 0x096, 0x050, 0x0b1},
+    {0x09d, 0x09e, 0x0ba, 0x0b9, 0x0ec, 0x01f, 0x0eb, 0x058},
+    {0x049, 0x05e, 0x060, 0x027, 0x04a, 0x05d, 0x0d3, 0x0d4},
+    {0x046, 0x045, 0x02f, 0x0dc, 0x051, 0x052, 0x068, 0x0db},
+    {0x04d, 0x05a, 0x0c4, 0x0c3, 0x04e, 0x059, 0x037, 0x070},
+    {0x042, 0x041, 0x0cb, 0x078, 0x055, 0x056, 0x0cc, 0x03f},
+    {0x000, 0x091, 0x047, 0x0b6, 0x133, 0x092, 0x134, 0x0b5},
+    {0x099, 0x09a, 0x0be, 0x0bd, 0x008, 0x13b, 0x04f, 0x13c},
+    {0x082, 0x123, 0x0a5, 0x124, 0x081, 0x010, 0x0a6, 0x057},
+    {0x12b, 0x018, 0x12c, 0x05f, 0x08a, 0x089, 0x0ad, 0x0ae},
+    {0x021, 0x088, 0x022, 0x173, 0x076, 0x09f, 0x075, 0x174},
+    {0x090, 0x087, 0x17b, 0x17c, 0x029, 0x07e, 0x02a, 0x07d},
+    {0x08f, 0x066, 0x164, 0x065, 0x098, 0x031, 0x163, 0x032},
+    {0x06e, 0x039, 0x06d, 0x03a, 0x097, 0x080, 0x16c, 0x16b},
+    {0x025, 0x154, 0x026, 0x0af, 0x072, 0x153, 0x071, 0x0b8},
+    {0x15c, 0x15b, 0x0b7, 0x0a0, 0x02d, 0x07a, 0x02e, 0x079},
+    {0x143, 0x062, 0x0a8, 0x061, 0x144, 0x035, 0x0bf, 0x036},
+    {0x06a, 0x03d, 0x069, 0x03e, 0x14b, 0x14c, 0x0b0, 0x0a7},
+};
+
+/* Table-driven Hilbert key, most significant level first.  system/peano.cc:297-313. */
+void or_peano_key(uint64_t x, uint64_t y, uint64_t z, int bits, uint64_t* hi, uint64_t* lo) {
+    unsigned __int128 key = 0;
+    unsigned state = 0;
+    for (int b = bits - 1; b >= 0; --b) {
+        const unsigned pix = (unsigned)(((x >> b) & 1) << 2 | ((y >> b) & 1) << 1 | ((z >> b) & 1));
+        const unsigned step = PH_STEP[state][pix];
+        key = (key << 3) | (step & 7u);
+        state = step >> 3;
+    }
+    *hi = (uint64_t)(key >> 64);
+    *lo = (uint64_t)key;
+}
+
+/* Morton key of the MPI code: z in the top bit of each triple.  system/peano.cc:317-329. */
+void or_morton_key(uint64_t x, uint64_t y, uint64_t z, int bits, uint64_t* hi, uint64_t* lo) {
+    unsigned __int128 key = 0;
+    for (int b = bits - 1; b >= 0; --b)
+        key = (key << 3) | (((z >> b) & 1) << 2 | ((y >> b) & 1) << 1 | ((x >> b) & 1));
+    *hi = (uint64_t)(key >> 64);
+    *lo = (uint64_t)key;
+}
+
+/* Mantissa extraction of d in [1,2): the top `bits` fraction bits.  domain/domain.cc:2693-2702. */
+uint64_t or_double_to_int(double d, int bits) {
+    uint64_t u;
+    memcpy(&u, &d, 8);
+    return (u & 0xFFFFFFFFFFFFFull) >> (52 - bits);
+}
+
+/* Root cell of shmem::build: bbox of live particles, centre, side * 1.0000001, optional
+ * randomised root (splitmix64 draw, box doubled).  shmem/tree.cc:355-393. */
+typedef struct {
+    double cx, cy, cz, side, scale;
+} or_geom;
+
+static or_geom root_geometry(int64_t n, const double* x, const double* y, const double* z,
+                             const double* m, long long randomize_seed) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int64_t i = 0; i < n; ++i) {
+        if (!(m[i] > 0)) continue;
+        if (x[i] < lo[0]) lo[0] = x[i];
+        if (x[i] > hi[0]) hi[0] = x[i];
+        if (y[i] < lo[1]) lo[1] = y[i];
+        if (y[i] > hi[1]) hi[1] = y[i];
+        if (z[i] < lo[2]) lo[2] = z[i];
+        if (z[i] > hi[2]) hi[2] = z[i];
+    }
+    or_geom g;
+    g.cx = 0.5 * (lo[0] + hi[0]);
+    g.cy = 0.5 * (lo[1] + hi[1]);
+    g.cz = 0.5 * (lo[2] + hi[2]);
+    double ext = hi[0] - lo[0];
+    if (hi[1] - lo[1] > ext) ext = hi[1] - lo[1];
+    if (hi[2] - lo[2] > ext) ext = hi[2] - lo[2];
+    g.side = ext * 1.0000001;
+    if (g.side <= 0) g.side = 1.0;
+    if (randomize_seed >= 0) {
+        uint64_t s = (uint64_t)randomize_seed * 0x9E3779B97F4A7C15ull;
+        double draw[3];
+        for (int k = 0; k < 3; ++k) {
+            s += 0x9E3779B97F4A7C15ull;
+            uint64_t v = s;
+            v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ull;
+            v = (v ^ (v >> 27)) * 0x94D049BB133111EBull;
+            draw[k] = (double)((v ^ (v >> 31)) >> 11) * (1.0 / 9007199254740992.0);
+        }
+        g.cx += g.side * (draw[0] - 0.5);
+        g.cy += g.side * (draw[1] - 0.5);
+        g.cz += g.side * (draw[2] - 0.5);
+        g.side *= 2.0;
+    }
+    g.scale = (double)((1u << OR_MAX_LEVEL) - 1) / g.side;
+    return g;
+}
+
+/* 20-bit quantisation of shmem/tree.cc:409-418. */
+static void quantise20(const or_geom* g, double x, double y, double z, uint32_t* a, uint32_t* b,
+                       uint32_t* c) {
+    *a = (uint32_t)((x - (g->cx - 0.5 * g->side)) * g->scale);
+    *b = (uint32_t)((y - (g->cy - 0.5 * g->side)) * g->scale);
+    *c = (uint32_t)((z - (g->cz - 0.5 * g->side)) * g->scale);
+}
+
+void or_keys20(int64_t n, const double* x, const double* y, const double* z, const double* m,
+               int key_mode, long long randomize_seed, uint64_t* keys, double* geom_out) {
+    const or_geom g = root_geometry(n, x, y, z, m, randomize_seed);
+    if (geom_out) {
+        geom_out[0] = g.cx; geom_out[1] = g.cy; geom_out[2] = g.cz;
+        geom_out[3] = g.side; geom_out[4] = g.scale;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        if (!(m[i] > 0)) { keys[i] = 1ull << 60; continue; }
+        uint32_t a, b, c;
+        quantise20(&g, x[i], y[i], z[i], &a, &b, &c);
+        if (key_mode == 0) {
+            keys[i] = or_morton20(a, b, c);
+        } else {
+            uint64_t hi, lo;
+            or_peano_key(a, b, c, OR_MAX_LEVEL, &hi, &lo);
+            keys[i] = lo;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------------------------- */
+/* Tree                                                                                         */
+/* ------------------------------------------------------------------------------------------- */
+
+struct or_tree {
+    int64_t n, nlive, nnodes, cap;
+    int root;
+    const double *x, *y, *z, *m, *soft; /* borrowed: the caller keeps them alive */
+    double *cx, *cy, *cz, *mass, *size, *delta, *nsoft, *gcx, *gcy, *gcz, *w_s;
+    float *w_len, *w_soft;
+    int *first, *next, *plo, *phi, *parent, *level;
+    uint32_t* order;
+    uint32_t* rank;
+    int* leaf_of;
+    uint64_t* skey;
+};
+
+typedef struct {
+    uint64_t key;
+    uint32_t idx;
+} key_idx;
+
+static int cmp_key_idx(const void* a, const void* b) {
+    const key_idx* p = (const key_idx*)a;
+    const key_idx* q = (const key_idx*)b;
+    if (p->key != q->key) return p->key < q->key ? -1 : 1;
+    return p->idx < q->idx ? -1 : (p->idx > q->idx);
+}
+
+static int claim_node(or_tree* t) {
+    if (t->nnodes >= t->cap) {
+        t->cap = t->cap * 2 + 1024;
+#define GROW(a, T) t->a = (T*)realloc(t->a, (size_t)t->cap * sizeof(T))
+        GROW(cx, double); GROW(cy, double); GROW(cz, double); GROW(mass, double);
+        GROW(size, double); GROW(delta, double); GROW(nsoft, double); GROW(gcx, double);
+        GROW(gcy, double); GROW(gcz, double); GROW(w_s, double); GROW(w_len, float);
+        GROW(w_soft, float); GROW(first, int); GROW(next, int); GROW(plo, int); GROW(phi, int);
+        GROW(parent, int); GROW(level, int);
+#undef GROW
+    }
+    return (int)t->nnodes++;
+}
+
+/* Recursive octant split of a key-sorted range: leaf at <= LEAF_MAX particles or level 20;
+ * children in octant order; moments from particles (leaf) or from children (interior).
+ * shmem/tree.cc:70-197.  Serial, so node numbering is the preorder the reference produces when
+ * it runs without tasks. */
+static int build_cell(or_tree* t, int lo, int hi, int lvl, double ccx, double ccy, double ccz,
+                      double sz) {
+    const int me = claim_node(t);
+    t->size[me] = sz; t->first[me] = -1; t->next[me] = -1; t->plo[me] = lo; t->phi[me] = hi;
+    t->parent[me] = -1; t->level[me] = lvl;
+    t->gcx[me] = ccx; t->gcy[me] = ccy; t->gcz[me] = ccz;
+    int kids[8], nk = 0;
+    if (!(hi - lo <= OR_LEAF_MAX || lvl >= OR_MAX_LEVEL)) {
+        const int shift = 3 * (OR_MAX_LEVEL - lvl - 1);
+        const double half = sz * 0.5, quarter = sz * 0.25;
+        int at = lo;
+        for (int oct = 0; oct < 8; ++oct) {
+            const int a = at;
+            while (at < hi && (int)((t->skey[at] >> shift) & 7ull) == oct) ++at;
+            if (at == a) continue;
+            const double ox = ccx + ((oct & 1) ? quarter : -quarter);
+            const double oy = ccy + ((oct & 2) ? quarter : -quarter);
+            const double oz = ccz + ((oct & 4) ? quarter : -quarter);
+            kids[nk++] = build_cell(t, a, at, lvl + 1, ox, oy, oz, half);
+        }
+        for (int k = 0; k < nk; ++k) {
+            t->parent[kids[k]] = me;
+            t->next[kids[k]] = (k + 1 < nk) ? kids[k + 1] : -1;
+        }
+        if (nk > 0) t->first[me] = kids[0];
+    }
+    double M = 0, sx = 0, sy = 0, sz_ = 0, smax = 0;
+    if (nk == 0) {
+        for (int i = lo; i < hi; ++i) {
+            const uint32_t p = t->order[i];
+            const double mp = t->m[p];
+            M += mp; sx += mp * t->x[p]; sy += mp * t->y[p]; sz_ += mp * t->z[p];
+            if (t->soft && t->soft[p] > smax) smax = t->soft[p];
+            t->leaf_of[p] = me;
+        }
+    } else {
+        for (int k = 0; k < nk; ++k) {
+            const int c = kids[k];
+            const double mc = t->mass[c];
+            M += mc; sx += mc * t->cx[c]; sy += mc * t->cy[c]; sz_ += mc * t->cz[c];
+            if (t->nsoft[c] > smax) smax = t->nsoft[c];
+        }
+    }
+    if (M > 0) { sx /= M; sy /= M; sz_ /= M; }
+    t->mass[me] = M; t->cx[me] = sx; t->cy[me] = sy; t->cz[me] = sz_; t->nsoft[me] = smax;
+    const double dx = sx - ccx, dy = sy - ccy, dz = sz_ - ccz;
+    t->delta[me] = sqrt(dx * dx + dy * dy + dz * dz);
+    return me;
+}
+
+/* next[] threading: a node's last child falls through to the node's own next.  shmem/tree.cc:340-348. */
+static void thread_walk(or_tree* t, int node, int next_sib) {
+    t->next[node] = next_sib;
+    for (int c = t->first[node]; c >= 0;) {
+        const int sib = t->next[c];
+        thread_walk(t, c, sib >= 0 ? sib : next_sib);
+        c = sib;
+    }
+}
+
+or_tree* or_build(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                  const double* soft, long long randomize_seed, int nodelta) {
+    or_tree* t = (or_tree*)calloc(1, sizeof(or_tree));
+    t->n = n; t->x = x; t->y = y; t->z = z; t->m = m; t->soft = soft;
+    uint64_t* keys = (uint64_t*)malloc((size_t)(n > 0 ? n : 1) * 8);
+    or_keys20(n, x, y, z, m, 0, randomize_seed, keys, NULL);
+    const or_geom g = root_geometry(n, x, y, z, m, randomize_seed);
+    /* live particles (m > 0), sorted by key; ties keep index order */
+    key_idx* ki = (key_idx*)malloc((size_t)(n > 0 ? n : 1) * sizeof(key_idx));
+    int64_t nl = 0;
+    for (int64_t i = 0; i < n; ++i)
+        if (m[i] > 0) { ki[nl].key = keys[i]; ki[nl].idx = (uint32_t)i; ++nl; }
+    qsort(ki, (size_t)nl, sizeof(key_idx), cmp_key_idx);
+    t->nlive = nl;
+    t->order = (uint32_t*)malloc((size_t)(nl > 0 ? nl : 1) * 4);
+    t->skey = (uint64_t*)malloc((size_t)(nl > 0 ? nl : 1) * 8);
+    for (int64_t r = 0; r < nl; ++r) { t->order[r] = ki[r].idx; t->skey[r] = ki[r].key; }
+    free(ki);
+    free(keys);
+    t->leaf_of = (int*)malloc((size_t)(n > 0 ? n : 1) * 4);
+    for (int64_t i = 0; i < n; ++i) t->leaf_of[i] = -1;
+    t->rank = (uint32_t*)malloc((size_t)(n > 0 ? n : 1) * 4);
+    for (int64_t i = 0; i < n; ++i) t->rank[i] = UINT32_MAX;
+    for (int64_t r = 0; r < nl; ++r) t->rank[t->order[r]] = (uint32_t)r;
+    t->cap = 0; t->nnodes = 0;
+    t->root = build_cell(t, 0, (int)nl, 0, g.cx, g.cy, g.cz, g.side);
+    thread_walk(t, t->root, -1);
+    for (int64_t i = 0; i < t->nnodes; ++i) {
+        /* packed walk node, shmem/tree.cc:507-523 (nodelta: SHMEM_TREE_NODELTA, tree.cc:512-519) */
+        t->w_s[i] = t->size[i] + (nodelta ? 0.0 : t->delta[i]);
+        t->w_len[i] = (float)t->size[i];
+        t->w_soft[i] = (float)t->nsoft[i];
+    }
+    return t;
+}
+
+void or_free(or_tree* t) {
+    if (!t) return;
+    free(t->cx); free(t->cy); free(t->cz); free(t->mass); free(t->size); free(t->delta);
+    free(t->nsoft); free(t->gcx); free(t->gcy); free(t->gcz); free(t->w_s); free(t->w_len);
+    free(t->w_soft); free(t->first); free(t->next); free(t->plo); free(t->phi); free(t->parent);
+    free(t->level); free(t->order); free(t->rank); free(t->leaf_of); free(t->skey);
+    free(t);
+}
+
+int64_t or_nnodes(const or_tree* t) { return t->nnodes; }
+int64_t or_nlive(const or_tree* t) { return t->nlive; }
+int or_root(const or_tree* t) { return t->root; }
+
+void or_nodes(const or_tree* t, double* cx, double* cy, double* cz, double* mass, double* size,
+              double* delta, double* soft, double* gcx, double* gcy, double* gcz, int* first,
+              int* next, int* plo, int* phi, int* parent, int* level, double* w_s, float* w_len,
+              float* w_soft) {
+    const size_t nn = (size_t)t->nnodes;
+#define CP(dst, src, sz) if (dst) memcpy(dst, t->src, nn * sz)
+    CP(cx, cx, 8); CP(cy, cy, 8); CP(cz, cz, 8); CP(mass, mass, 8); CP(size, size, 8);
+    CP(delta, delta, 8); CP(soft, nsoft, 8); CP(gcx, gcx, 8); CP(gcy, gcy, 8); CP(gcz, gcz, 8);
+    CP(first, first, 4); CP(next, next, 4); CP(plo, plo, 4); CP(phi, phi, 4);
+    CP(parent, parent, 4); CP(level, level, 4); CP(w_s, w_s, 8); CP(w_len, w_len, 4);
+    CP(w_soft, w_soft, 4);
+#undef CP
+}
+
+void or_order(const or_tree* t, uint32_t* orderbuf, uint32_t* rank, int* leaf_of) {
+    if (orderbuf) memcpy(orderbuf, t->order, (size_t)t->nlive * 4);
+    if (rank) memcpy(rank, t->rank, (size_t)t->n * 4);
+    if (leaf_of) memcpy(leaf_of, t->leaf_of, (size_t)t->n * 4);
+}
+
+/* ------------------------------------------------------------------------------------------- */
+/* Walks                                                                                        */
+/* ------------------------------------------------------------------------------------------- */
+
+/* Leaf groups: a new group wherever leaf_of changes or is -1 (tree.cc:656-667); fixed windows of
+ * `batch` consecutive targets otherwise (tree.cc:668-681). */
+int64_t or_groups(const or_tree* t, int64_t nt, const uint32_t* targets, int batch, int64_t* starts) {
+    int64_t ng = 0;
+    if (nt <= 0) { starts[0] = 0; return 0; }
+    if (batch <= 0) {
+        starts[ng++] = 0;
+        for (int64_t i = 1; i < nt; ++i) {
+            const int li = t->leaf_of[targets[i]], lp = t->leaf_of[targets[i - 1]];
+            if (li != lp || li < 0) starts[ng++] = i;
+        }
+    } else {
+        for (int64_t i = 0; i < nt; i += batch) starts[ng++] = i;
+    }
+    starts[ng] = nt;
+    return ng;
+}
+
+static inline double dmax(double a, double b) { return a > b ? a : b; }
+static inline double dmin(double a, double b) { return a < b ? a : b; }
+
+/* One walk per group over the threaded tree: bbox-nearest-point opening with the group's
+ * largest softening and smallest aold, P-P sums over opened leaves (self and r == 0 skipped,
+ * kernel of the larger softening), P-N monopoles otherwise.  shmem/tree.cc:678-888 (grouped),
+ * tree.cc:538-581 and 905-943 (leaf_accept = 0, the per-target walks). */
+void or_walk_groups(const or_tree* t, int64_t nt, const uint32_t* targets, int64_t ngroups,
+                    const int64_t* starts, double theta, double G, const double* aold,
+                    int leaf_accept, double* ax, double* ay, double* az, double* phi,
+                    int64_t* counters) {
+    const double theta2 = theta * theta;
+    long long c_nodes = 0, c_multi = 0, c_pairs = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : c_nodes, c_multi, c_pairs)
+    for (int64_t g = 0; g < ngroups; ++g) {
+        const int64_t lo = starts[g], hi = starts[g + 1];
+        const int nb = (int)(hi - lo);
+        double b0[3] = {1e300, 1e300, 1e300}, b1[3] = {-1e300, -1e300, -1e300}, emax = 0;
+        double amin = aold ? 1e300 : 0.0;
+        double* tx = (double*)malloc((size_t)nb * 8 * 8);
+        double *ty = tx + nb, *tz = tx + 2 * nb, *te = tx + 3 * nb;
+        double *oax = tx + 4 * nb, *oay = tx + 5 * nb, *oaz = tx + 6 * nb, *oph = tx + 7 * nb;
+        for (int i = 0; i < nb; ++i) {
+            const uint32_t p = targets[lo + i];
+            tx[i] = t->x[p]; ty[i] = t->y[p]; tz[i] = t->z[p];
+            te[i] = t->soft ? t->soft[p] : 0.0;
+            b0[0] = dmin(b0[0], tx[i]); b1[0] = dmax(b1[0], tx[i]);
+            b0[1] = dmin(b0[1], ty[i]); b1[1] = dmax(b1[1], ty[i]);
+            b0[2] = dmin(b0[2], tz[i]); b1[2] = dmax(b1[2], tz[i]);
+            emax = dmax(emax, te[i]);
+            if (aold) amin = dmin(amin, aold[lo + i]);
+            oax[i] = oay[i] = oaz[i] = oph[i] = 0.0;
+        }
+        int node = t->root;
+        while (node >= 0) {
+            ++c_nodes;
+            const double ncx = t->cx[node], ncy = t->cy[node], ncz = t->cz[node];
+            const double dx = dmax(0.0, dmax(b0[0] - ncx, ncx - b1[0]));
+            const double dy = dmax(0.0, dmax(b0[1] - ncy, ncy - b1[1]));
+            const double dz = dmax(0.0, dmax(b0[2] - ncz, ncz - b1[2]));
+            const double rmin2 = dx * dx + dy * dy + dz * dz;
+            const int is_leaf = t->first[node] < 0;
+            int accept;
+            if (leaf_accept || !is_leaf)
+                accept = !or_open_node(rmin2, (double)t->w_len[node], t->w_s[node], t->mass[node],
+                                       (double)t->w_soft[node], emax, amin, theta2, dx, dy, dz);
+            else
+                accept = 0;
+            if (accept) {
+                /* monopole with the softening max(target, node) */
+                c_multi += nb;
+                const double nm = t->mass[node];
+                for (int i = 0; i < nb; ++i) {
+                    const double ox = ncx - tx[i], oy = ncy - ty[i], oz = ncz - tz[i];
+                    const double r2 = ox * ox + oy * oy + oz * oz;
+                    if (r2 <= 0) continue;
+                    const double r = sqrt(r2);
+                    const double e = dmax(dmax(te[i], (double)t->w_soft[node]), 1e-300);
+                    const double f = nm * or_spline_force_over_r(r, e);
+                    oax[i] += ox * f; oay[i] += oy * f; oaz[i] += oz * f;
+                    oph[i] += nm * or_spline_potential(r, e);
+                }
+                node = t->next[node];
+            } else if (is_leaf) {
+                for (int k = t->plo[node]; k < t->phi[node]; ++k) {
+                    const uint32_t q = t->order[k];
+                    const double qx = t->x[q], qy = t->y[q], qz = t->z[q], qm = t->m[q];
+                    const double qs = t->soft ? t->soft[q] : 0.0;
+                    for (int i = 0; i < nb; ++i) {
+                        if (targets[lo + i] == q) continue;
+                        const double ox = qx - tx[i], oy = qy - ty[i], oz = qz - tz[i];
+                        const double r2 = ox * ox + oy * oy + oz * oz;
+                        if (r2 <= 0) continue;
+                        ++c_pairs;
+                        const double r = sqrt(r2);
+                        const double e = dmax(dmax(te[i], qs), 1e-300);
+                        const double f = qm * or_spline_force_over_r(r, e);
+                        oax[i] += ox * f; oay[i] += oy * f; oaz[i] += oz * f;
+                        oph[i] += qm * or_spline_potential(r, e);
+                    }
+                }
+                node = t->next[node];
+            } else {
+                node = t->first[node];
+            }
+        }
+        for (int i = 0; i < nb; ++i) {
+            if (ax) ax[lo + i] = G * oax[i];
+            if (ay) ay[lo + i] = G * oay[i];
+            if (az) az[lo + i] = G * oaz[i];
+            if (phi) phi[lo + i] = G * oph[i];
+        }
+        free(tx);
+    }
+    if (counters) { counters[0] = c_nodes; counters[1] = c_multi; counters[2] = c_pairs; }
+}
+
+void or_accel_grouped(const or_tree* t, int64_t nt, const uint32_t* targets, double theta, double G,
+                      int batch, const double* aold, double* ax, double* ay, double* az,
+                      int64_t* counters) {
+    int64_t* starts = (int64_t*)malloc((size_t)(nt + 1) * 8);
+    const int64_t ng = or_groups(t, nt, targets, batch, starts);
+    or_walk_groups(t, nt, targets, ng, starts, theta, G, aold, 1, ax, ay, az, NULL, counters);
+    free(starts);
+}
+
+static int64_t* singleton_groups(int64_t nt) {
+    int64_t* s = (int64_t*)malloc((size_t)(nt + 1) * 8);
+    for (int64_t i = 0; i <= nt; ++i) s[i] = i;
+    return s;
+}
+
+void or_accel(const or_tree* t, int64_t nt, const uint32_t* targets, double theta, double G,
+              const double* aold, double* ax, double* ay, double* az) {
+    int64_t* s = singleton_groups(nt);
+    or_walk_groups(t, nt, targets, nt, s, theta, G, aold, 0, ax, ay, az, NULL, NULL);
+    free(s);
+}
+
+void or_potential(const or_tree* t, int64_t nt, const uint32_t* targets, double theta, double G,
+                  const double* aold, double* phi) {
+    int64_t* s = singleton_groups(nt);
+    or_walk_groups(t, nt, targets, nt, s, theta, G, aold, 0, NULL, NULL, NULL, phi, NULL);
+    free(s);
+}
+
+/* FP64 direct sum with the walk's pair rule (kernel of max(eps_i, eps_j), self and r == 0
+ * skipped).  shmem/tree.cc:946-971. */
+void or_direct(int64_t n, const double* x, const double* y, const double* z, const double* m,
+               const double* soft, int64_t nt, const uint32_t* targets, double G, double* ax,
+               double* ay, double* az, double* phi) {
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < nt; ++k) {
+        const uint32_t p = targets[k];
+        const double px = x[p], py = y[p], pz = z[p], ep = soft ? soft[p] : 0.0;
+        double sx = 0, sy = 0, sz = 0, sp = 0;
+        for (int64_t q = 0; q < n; ++q) {
+            if (q == (int64_t)p) continue;
+            const double ox = x[q] - px, oy = y[q] - py, oz = z[q] - pz;
+            const double r = sqrt(ox * ox + oy * oy + oz * oz);
+            if (r <= 0) continue;
+            const double e = dmax(dmax(ep, soft ? soft[q] : 0.0), 1e-300);
+            const double f = m[q] * or_spline_force_over_r(r, e);
+            sx += ox * f; sy += oy * f; sz += oz * f;
+            sp += m[q] * or_spline_potential(r, e);
+        }
+        if (ax) ax[k] = G * sx;
+        if (ay) ay[k] = G * sy;
+        if (az) az[k] = G * sz;
+        if (phi) phi[k] = G * sp;
+    }
+}

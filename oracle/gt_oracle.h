@@ -1,0 +1,82 @@
+/* ORACLE — test infrastructure only.
+ *
+ * CPU restatement (plain C, OpenMP over groups) of the reference's shared-memory tree-gravity path:
+ * the shmem build (shmem/tree.cc:350-526), its leaf/batch-grouped walk (shmem/tree.cc:626-897), the
+ * per-target walk and potential (shmem/tree.cc:528-582, 899-944), the FP64 direct sum
+ * (shmem/tree.cc:946-971) and the key functions (shmem/tree.h:161-173, system/peano.cc:192-355,
+ * domain/domain.cc:2693-2702).  Only tests/, bench.py's CPU baseline leg and
+ * __graft_entry__.smoke() may load it, and only as the checker.  It is pinned against the
+ * reference itself (oracle/_ref, compiled from the reference sources) and against the committed
+ * fixtures under tests/golden/.
+ */
+#ifndef GT_ORACLE_H
+#define GT_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_tree or_tree;
+
+/* Scalar kernels (shmem/tree.h:59-80) and the opening test (shmem/tree.h:109-144). */
+double or_spline_force_over_r(double r, double h);
+double or_spline_potential(double r, double h);
+int or_open_node(double r_sq, double len, double l_open, double node_mass, double node_maxsoft,
+                 double soft_target, double aold, double theta_sq, double adx, double ady, double adz);
+
+/* Keys. */
+uint64_t or_morton20(uint32_t a, uint32_t b, uint32_t c);                 /* shmem/tree.h:161-173 */
+void or_peano_key(uint64_t x, uint64_t y, uint64_t z, int bits, uint64_t* hi, uint64_t* lo);
+void or_morton_key(uint64_t x, uint64_t y, uint64_t z, int bits, uint64_t* hi, uint64_t* lo);
+uint64_t or_double_to_int(double d, int bits);                             /* domain.cc:2693-2702 */
+/* 20-bit-per-axis keys of every particle exactly as shmem::build quantises (tree.cc:361-418);
+ * key_mode 0 = Morton (shmem), 1 = Peano-Hilbert over the same integer cells.  Massless particles
+ * get key (1<<60).  geom_out (may be null) receives {cx, cy, cz, side, scale}. */
+void or_keys20(int64_t n, const double* x, const double* y, const double* z, const double* m,
+               int key_mode, long long randomize_seed, uint64_t* keys, double* geom_out);
+
+/* Tree (Morton order, as shmem::build). */
+or_tree* or_build(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                  const double* soft, long long randomize_seed, int nodelta);
+void or_free(or_tree* t);
+int64_t or_nnodes(const or_tree* t);
+int64_t or_nlive(const or_tree* t);
+int or_root(const or_tree* t);
+void or_nodes(const or_tree* t, double* cx, double* cy, double* cz, double* mass, double* size,
+              double* delta, double* soft, double* gcx, double* gcy, double* gcz, int* first,
+              int* next, int* plo, int* phi, int* parent, int* level, double* w_s, float* w_len,
+              float* w_soft);
+void or_order(const or_tree* t, uint32_t* orderbuf, uint32_t* rank, int* leaf_of);
+
+/* Grouping.  Leaf groups (batch <= 0, tree.cc:656-667) or fixed windows (batch > 0).  Returns the
+ * number of groups; starts must hold nt+1 entries. */
+int64_t or_groups(const or_tree* t, int64_t nt, const uint32_t* targets, int batch, int64_t* starts);
+
+/* Walk over explicit groups of `targets` (group g = targets[starts[g] .. starts[g+1])).
+ * leaf_accept = 1: leaves are offered to the criterion first (accel_grouped, tree.cc:751-779);
+ * leaf_accept = 0: leaves are always direct-summed (accel / potential, tree.cc:554-575).
+ * Any of ax/ay/az/phi may be null.  counters (may be null) receives
+ * {nodes_visited, multipole, pairs} as SHMEM_COUNT_WALK counts them (tree.cc:671-677, 746, 803, 841). */
+void or_walk_groups(const or_tree* t, int64_t nt, const uint32_t* targets, int64_t ngroups,
+                    const int64_t* starts, double theta, double G, const double* aold,
+                    int leaf_accept, double* ax, double* ay, double* az, double* phi,
+                    int64_t* counters);
+/* accel_grouped (tree.cc:626-897), gravity only. */
+void or_accel_grouped(const or_tree* t, int64_t nt, const uint32_t* targets, double theta, double G,
+                      int batch, const double* aold, double* ax, double* ay, double* az,
+                      int64_t* counters);
+/* accel (tree.cc:528-582) and potential (tree.cc:899-944): one walk per target. */
+void or_accel(const or_tree* t, int64_t nt, const uint32_t* targets, double theta, double G,
+              const double* aold, double* ax, double* ay, double* az);
+void or_potential(const or_tree* t, int64_t nt, const uint32_t* targets, double theta, double G,
+                  const double* aold, double* phi);
+/* accel_brute (tree.cc:946-971): FP64 direct sum over all n particles.  phi may be null. */
+void or_direct(int64_t n, const double* x, const double* y, const double* z, const double* m,
+               const double* soft, int64_t nt, const uint32_t* targets, double G, double* ax,
+               double* ay, double* az, double* phi);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,416 @@
+"""ORACLE — test infrastructure only.
+
+ctypes bindings for the two CPU checkers of the tree-gravity path:
+
+* ``Restatement`` loads ``oracle/liboracle.so``: the plain-C restatement in ``gt_oracle.c``
+  (each function cites the reference file:line it follows).
+* ``Reference`` loads ``oracle/_ref/libgizmo_ref.so``: the reference's own ``shmem/tree.cc`` and
+  Peano-Hilbert functions, compiled from the reference sources by ``oracle/Makefile`` (target
+  ``ref``).  It is absent wherever the reference sources were not available at build time.
+
+Only ``tests/``, ``bench.py``'s CPU-baseline leg / reference arm and ``__graft_entry__.smoke()``
+import this module, and only as the checker or the timed CPU baseline; the product library never
+calls into it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATEMENT_SO = os.path.join(HERE, "liboracle.so")
+REFERENCE_SO = os.path.join(HERE, "_ref", "libgizmo_ref.so")
+
+_d = C.POINTER(C.c_double)
+_f = C.POINTER(C.c_float)
+_i = C.POINTER(C.c_int)
+_u32 = C.POINTER(C.c_uint32)
+_u64 = C.POINTER(C.c_uint64)
+_i64 = C.POINTER(C.c_int64)
+
+
+def _p(a, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctype)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _targets(t):
+    return np.ascontiguousarray(t, dtype=np.uint32)
+
+
+def build_library():
+    """Compile liboracle.so (and _ref when the reference sources are present)."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    ref_root = os.environ.get("GIZMO_REF", "/root/reference")
+    if os.path.isdir(os.path.join(ref_root, "shmem")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"GIZMO_REF={ref_root}"], check=True)
+
+
+def reference_available() -> bool:
+    return os.path.exists(REFERENCE_SO)
+
+
+class Restatement:
+    """The plain-C restatement (gt_oracle.c)."""
+
+    def __init__(self, path: str = RESTATEMENT_SO):
+        if not os.path.exists(path):
+            build_library()
+        L = C.CDLL(path)
+        self.L = L
+        L.or_spline_force_over_r.restype = C.c_double
+        L.or_spline_force_over_r.argtypes = [C.c_double, C.c_double]
+        L.or_spline_potential.restype = C.c_double
+        L.or_spline_potential.argtypes = [C.c_double, C.c_double]
+        L.or_open_node.restype = C.c_int
+        L.or_open_node.argtypes = [C.c_double] * 11
+        L.or_morton20.restype = C.c_uint64
+        L.or_morton20.argtypes = [C.c_uint32] * 3
+        L.or_peano_key.argtypes = [C.c_uint64] * 3 + [C.c_int, _u64, _u64]
+        L.or_morton_key.argtypes = [C.c_uint64] * 3 + [C.c_int, _u64, _u64]
+        L.or_double_to_int.restype = C.c_uint64
+        L.or_double_to_int.argtypes = [C.c_double, C.c_int]
+        L.or_keys20.argtypes = [C.c_int64, _d, _d, _d, _d, C.c_int, C.c_longlong, _u64, _d]
+        L.or_build.restype = C.c_void_p
+        L.or_build.argtypes = [C.c_int64, _d, _d, _d, _d, _d, C.c_longlong, C.c_int]
+        L.or_free.argtypes = [C.c_void_p]
+        L.or_nnodes.restype = C.c_int64
+        L.or_nnodes.argtypes = [C.c_void_p]
+        L.or_nlive.restype = C.c_int64
+        L.or_nlive.argtypes = [C.c_void_p]
+        L.or_root.restype = C.c_int
+        L.or_root.argtypes = [C.c_void_p]
+        L.or_nodes.argtypes = [C.c_void_p] + [_d] * 10 + [_i] * 6 + [_d, _f, _f]
+        L.or_order.argtypes = [C.c_void_p, _u32, _u32, _i]
+        L.or_groups.restype = C.c_int64
+        L.or_groups.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_int, _i64]
+        L.or_walk_groups.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_int64, _i64, C.c_double,
+                                     C.c_double, _d, C.c_int, _d, _d, _d, _d, _i64]
+        L.or_accel_grouped.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double,
+                                       C.c_int, _d, _d, _d, _d, _i64]
+        L.or_accel.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, _d, _d, _d, _d]
+        L.or_potential.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, _d, _d]
+        L.or_direct.argtypes = [C.c_int64, _d, _d, _d, _d, _d, C.c_int64, _u32, C.c_double,
+                                _d, _d, _d, _d]
+
+    # scalar helpers
+    def spline_force_over_r(self, r, h):
+        return self.L.or_spline_force_over_r(r, h)
+
+    def spline_potential(self, r, h):
+        return self.L.or_spline_potential(r, h)
+
+    def open_node(self, *args):
+        return self.L.or_open_node(*[float(a) for a in args])
+
+    def peano_key(self, x, y, z, bits):
+        hi, lo = C.c_uint64(), C.c_uint64()
+        self.L.or_peano_key(int(x), int(y), int(z), bits, C.byref(hi), C.byref(lo))
+        return (hi.value << 64) | lo.value
+
+    def morton_key(self, x, y, z, bits):
+        hi, lo = C.c_uint64(), C.c_uint64()
+        self.L.or_morton_key(int(x), int(y), int(z), bits, C.byref(hi), C.byref(lo))
+        return (hi.value << 64) | lo.value
+
+    def morton20(self, a, b, c):
+        return self.L.or_morton20(int(a), int(b), int(c))
+
+    def double_to_int(self, d, bits=42):
+        return self.L.or_double_to_int(float(d), bits)
+
+    def keys20(self, P, key_mode=1, randomize_seed=-1):
+        n = len(P["m"])
+        keys = np.empty(n, np.uint64)
+        geom = np.empty(5, np.float64)
+        x, y, z, m = (_f64(P[k]) for k in ("x", "y", "z", "m"))
+        self.L.or_keys20(n, _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), key_mode, randomize_seed,
+                         _p(keys, _u64), _p(geom, _d))
+        return keys, geom
+
+    def build(self, P, randomize_seed=-1, nodelta=False):
+        return OracleTree(self, P, randomize_seed, nodelta)
+
+    def direct(self, P, targets, G=1.0, want_phi=True):
+        t = _targets(targets)
+        nt = len(t)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        phi = np.empty(nt) if want_phi else None
+        x, y, z, m = (_f64(P[k]) for k in ("x", "y", "z", "m"))
+        soft = _f64(P["soft"]) if P.get("soft") is not None else None
+        self.L.or_direct(len(m), _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), _p(soft, _d), nt,
+                         _p(t, _u32), G, _p(ax, _d), _p(ay, _d), _p(az, _d), _p(phi, _d))
+        return (ax, ay, az, phi) if want_phi else (ax, ay, az)
+
+
+class OracleTree:
+    """A restatement tree; keeps the particle arrays it borrows alive."""
+
+    def __init__(self, lib: Restatement, P, randomize_seed=-1, nodelta=False):
+        self.lib = lib
+        self._keep = [_f64(P[k]) for k in ("x", "y", "z", "m")]
+        soft = P.get("soft")
+        self._soft = _f64(soft) if soft is not None else None
+        x, y, z, m = self._keep
+        self.n = len(m)
+        self.h = lib.L.or_build(self.n, _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d),
+                                _p(self._soft, _d), randomize_seed, int(nodelta))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.L.or_free(self.h)
+            self.h = None
+
+    @property
+    def nnodes(self):
+        return self.lib.L.or_nnodes(self.h)
+
+    @property
+    def nlive(self):
+        return self.lib.L.or_nlive(self.h)
+
+    @property
+    def root(self):
+        return self.lib.L.or_root(self.h)
+
+    def nodes(self):
+        nn = self.nnodes
+        out = {k: np.empty(nn) for k in ("cx", "cy", "cz", "mass", "size", "delta", "soft", "gcx",
+                                           "gcy", "gcz")}
+        for k in ("first", "next", "plo", "phi", "parent", "level"):
+            out[k] = np.empty(nn, np.int32)
+        out["w_s"] = np.empty(nn)
+        out["w_len"] = np.empty(nn, np.float32)
+        out["w_soft"] = np.empty(nn, np.float32)
+        L = self.lib.L
+        L.or_nodes(self.h, *[_p(out[k], _d) for k in ("cx", "cy", "cz", "mass", "size", "delta",
+                                                        "soft", "gcx", "gcy", "gcz")],
+                   *[_p(out[k], _i) for k in ("first", "next", "plo", "phi", "parent", "level")],
+                   _p(out["w_s"], _d), _p(out["w_len"], _f), _p(out["w_soft"], _f))
+        return out
+
+    def order(self):
+        ob = np.empty(self.nlive, np.uint32)
+        rank = np.empty(self.n, np.uint32)
+        leaf = np.empty(self.n, np.int32)
+        self.lib.L.or_order(self.h, _p(ob, _u32), _p(rank, _u32), _p(leaf, _i))
+        return ob, rank, leaf
+
+    def groups(self, targets, batch=0):
+        t = _targets(targets)
+        starts = np.empty(len(t) + 1, np.int64)
+        ng = self.lib.L.or_groups(self.h, len(t), _p(t, _u32), batch, _p(starts, _i64))
+        return starts[: ng + 1].copy()
+
+    def walk_groups(self, targets, starts, theta, G=1.0, aold=None, leaf_accept=True,
+                    want_phi=False):
+        t = _targets(targets)
+        nt = len(t)
+        st = np.ascontiguousarray(starts, np.int64)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        phi = np.empty(nt) if want_phi else None
+        cnt = np.zeros(3, np.int64)
+        ao = _f64(aold) if aold is not None else None
+        self.lib.L.or_walk_groups(self.h, nt, _p(t, _u32), len(st) - 1, _p(st, _i64), theta, G,
+                                  _p(ao, _d), int(leaf_accept), _p(ax, _d), _p(ay, _d),
+                                  _p(az, _d), _p(phi, _d), _p(cnt, _i64))
+        return ax, ay, az, phi, cnt
+
+    def accel_grouped(self, targets, theta, G=1.0, batch=0, aold=None):
+        t = _targets(targets)
+        nt = len(t)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        cnt = np.zeros(3, np.int64)
+        ao = _f64(aold) if aold is not None else None
+        self.lib.L.or_accel_grouped(self.h, nt, _p(t, _u32), theta, G, batch, _p(ao, _d),
+                                    _p(ax, _d), _p(ay, _d), _p(az, _d), _p(cnt, _i64))
+        return ax, ay, az, cnt
+
+    def accel(self, targets, theta, G=1.0, aold=None):
+        t = _targets(targets)
+        nt = len(t)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        ao = _f64(aold) if aold is not None else None
+        self.lib.L.or_accel(self.h, nt, _p(t, _u32), theta, G, _p(ao, _d), _p(ax, _d), _p(ay, _d),
+                            _p(az, _d))
+        return ax, ay, az
+
+    def potential(self, targets, theta, G=1.0, aold=None):
+        t = _targets(targets)
+        phi = np.empty(len(t))
+        ao = _f64(aold) if aold is not None else None
+        self.lib.L.or_potential(self.h, len(t), _p(t, _u32), theta, G, _p(ao, _d), _p(phi, _d))
+        return phi
+
+
+class Reference:
+    """The reference's own shmem tree, compiled from its sources into oracle/_ref."""
+
+    def __init__(self, path: str = REFERENCE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (reference sources unavailable)")
+        L = C.CDLL(path)
+        self.L = L
+        L.ref_max_threads.restype = C.c_int
+        L.ref_set_threads.argtypes = [C.c_int]
+        L.ref_build.restype = C.c_void_p
+        L.ref_build.argtypes = [C.c_int64, _d, _d, _d, _d, _d, C.c_longlong, _d]
+        L.ref_free.argtypes = [C.c_void_p]
+        L.ref_tree_nnodes.restype = C.c_int64
+        L.ref_tree_nnodes.argtypes = [C.c_void_p]
+        L.ref_tree_root.restype = C.c_int
+        L.ref_tree_root.argtypes = [C.c_void_p]
+        L.ref_tree_nlive.restype = C.c_int64
+        L.ref_tree_nlive.argtypes = [C.c_void_p]
+        L.ref_tree_nodes.argtypes = [C.c_void_p] + [_d] * 10 + [_i] * 5 + [_d, _f, _f]
+        L.ref_tree_order.argtypes = [C.c_void_p, _u32, _u32, _i]
+        L.ref_accel_grouped.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double,
+                                        C.c_int, _d, _d, _d, _d]
+        L.ref_accel.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, _d, _d, _d, _d]
+        L.ref_potential.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, _d, _d]
+        L.ref_accel_brute.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, _d, _d, _d]
+        L.ref_morton20.restype = C.c_uint64
+        L.ref_morton20.argtypes = [C.c_uint32] * 3
+        L.ref_peano_hilbert_key.argtypes = [C.c_uint64] * 3 + [C.c_int, _u64, _u64]
+        L.ref_morton_key.argtypes = [C.c_uint64] * 3 + [C.c_int, _u64, _u64]
+        L.ref_peano_and_morton_key.argtypes = [C.c_uint64] * 3 + [C.c_int, _u64, _u64, _u64, _u64]
+        L.ref_domain_double_to_int.restype = C.c_uint64
+        L.ref_domain_double_to_int.argtypes = [C.c_double]
+        L.ref_spline_force_over_r.restype = C.c_double
+        L.ref_spline_force_over_r.argtypes = [C.c_double, C.c_double]
+        L.ref_spline_potential.restype = C.c_double
+        L.ref_spline_potential.argtypes = [C.c_double, C.c_double]
+        L.ref_open_node.restype = C.c_int
+        L.ref_open_node.argtypes = [C.c_double] * 11
+
+    def max_threads(self):
+        return self.L.ref_max_threads()
+
+    def set_threads(self, n):
+        self.L.ref_set_threads(int(n))
+
+    def peano_key(self, x, y, z, bits):
+        hi, lo = C.c_uint64(), C.c_uint64()
+        self.L.ref_peano_hilbert_key(int(x), int(y), int(z), bits, C.byref(hi), C.byref(lo))
+        return (hi.value << 64) | lo.value
+
+    def morton_key(self, x, y, z, bits):
+        hi, lo = C.c_uint64(), C.c_uint64()
+        self.L.ref_morton_key(int(x), int(y), int(z), bits, C.byref(hi), C.byref(lo))
+        return (hi.value << 64) | lo.value
+
+    def peano_and_morton_key(self, x, y, z, bits):
+        a, b, c, d = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self.L.ref_peano_and_morton_key(int(x), int(y), int(z), bits, C.byref(a), C.byref(b),
+                                        C.byref(c), C.byref(d))
+        return (a.value << 64) | b.value, (c.value << 64) | d.value
+
+    def morton20(self, a, b, c):
+        return self.L.ref_morton20(int(a), int(b), int(c))
+
+    def double_to_int(self, d):
+        return self.L.ref_domain_double_to_int(float(d))
+
+    def spline_force_over_r(self, r, h):
+        return self.L.ref_spline_force_over_r(r, h)
+
+    def spline_potential(self, r, h):
+        return self.L.ref_spline_potential(r, h)
+
+    def open_node(self, *args):
+        return self.L.ref_open_node(*[float(a) for a in args])
+
+    def build(self, P, randomize_seed=-1):
+        return ReferenceTree(self, P, randomize_seed)
+
+
+class ReferenceTree:
+    def __init__(self, lib: Reference, P, randomize_seed=-1):
+        self.lib = lib
+        x, y, z, m = (_f64(P[k]) for k in ("x", "y", "z", "m"))
+        soft = P.get("soft")
+        soft = _f64(soft) if soft is not None else None
+        self.n = len(m)
+        self.build_times = np.zeros(7)
+        self.h = lib.L.ref_build(self.n, _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), _p(soft, _d),
+                                 randomize_seed, _p(self.build_times, _d))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.L.ref_free(self.h)
+            self.h = None
+
+    @property
+    def nnodes(self):
+        return self.lib.L.ref_tree_nnodes(self.h)
+
+    @property
+    def nlive(self):
+        return self.lib.L.ref_tree_nlive(self.h)
+
+    @property
+    def root(self):
+        return self.lib.L.ref_tree_root(self.h)
+
+    def nodes(self):
+        nn = self.nnodes
+        out = {k: np.empty(nn) for k in ("cx", "cy", "cz", "mass", "size", "delta", "soft", "gcx",
+                                           "gcy", "gcz")}
+        for k in ("first", "next", "plo", "phi", "parent"):
+            out[k] = np.empty(nn, np.int32)
+        out["w_s"] = np.empty(nn)
+        out["w_len"] = np.empty(nn, np.float32)
+        out["w_soft"] = np.empty(nn, np.float32)
+        self.lib.L.ref_tree_nodes(self.h, *[_p(out[k], _d) for k in (
+            "cx", "cy", "cz", "mass", "size", "delta", "soft", "gcx", "gcy", "gcz")],
+            *[_p(out[k], _i) for k in ("first", "next", "plo", "phi", "parent")],
+            _p(out["w_s"], _d), _p(out["w_len"], _f), _p(out["w_soft"], _f))
+        return out
+
+    def order(self):
+        ob = np.empty(self.nlive, np.uint32)
+        rank = np.empty(self.n, np.uint32)
+        leaf = np.empty(self.n, np.int32)
+        self.lib.L.ref_tree_order(self.h, _p(ob, _u32), _p(rank, _u32), _p(leaf, _i))
+        return ob, rank, leaf
+
+    def accel_grouped(self, targets, theta, G=1.0, batch=0, aold=None):
+        t = _targets(targets)
+        nt = len(t)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        ao = _f64(aold) if aold is not None else None
+        self.lib.L.ref_accel_grouped(self.h, nt, _p(t, _u32), theta, G, batch, _p(ao, _d),
+                                     _p(ax, _d), _p(ay, _d), _p(az, _d))
+        return ax, ay, az
+
+    def accel(self, targets, theta, G=1.0, aold=None):
+        t = _targets(targets)
+        nt = len(t)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        ao = _f64(aold) if aold is not None else None
+        self.lib.L.ref_accel(self.h, nt, _p(t, _u32), theta, G, _p(ao, _d), _p(ax, _d),
+                             _p(ay, _d), _p(az, _d))
+        return ax, ay, az
+
+    def potential(self, targets, theta, G=1.0, aold=None):
+        t = _targets(targets)
+        phi = np.empty(len(t))
+        ao = _f64(aold) if aold is not None else None
+        self.lib.L.ref_potential(self.h, len(t), _p(t, _u32), theta, G, _p(ao, _d), _p(phi, _d))
+        return phi
+
+    def accel_brute(self, targets, G=1.0):
+        t = _targets(targets)
+        nt = len(t)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        self.lib.L.ref_accel_brute(self.h, nt, _p(t, _u32), G, _p(ax, _d), _p(ay, _d), _p(az, _d))
+        return ax, ay, az

@@ -1,0 +1,161 @@
+// ORACLE — test infrastructure only; never linked into the product library.
+//
+// Plain C-ABI wrapper around the reference's own shared-memory tree (shmem/tree.h, shmem/tree.cc)
+// and its Peano-Hilbert key functions (system/peano.cc:192-355, domain/domain.cc:2693-2702).
+// The reference sources are NOT copied here: oracle/Makefile.ref compiles them where they lie and
+// links this file against them into oracle/_ref/libgizmo_ref.so.  Only tests/, bench.py's CPU
+// baseline / reference arm and __graft_entry__.smoke() load that library, and only as the checker
+// or the timed CPU baseline.
+#include "tree.h"
+
+#include <cstdint>
+#include <cstring>
+#include <omp.h>
+
+using namespace shmem;
+
+// Extracted at build time from system/peano.cc (typedefs supplied by the recipe's prelude).
+typedef __int128 peanokey;
+typedef unsigned long long peano1D;
+peanokey peano_hilbert_key(peano1D x, peano1D y, peano1D z, int bits);
+peanokey morton_key(peano1D x, peano1D y, peano1D z, int bits);
+peanokey peano_and_morton_key(peano1D x, peano1D y, peano1D z, int bits, peanokey* morton);
+// Extracted at build time from domain/domain.cc (BITS_PER_DIMENSION 42).
+peano1D domain_double_to_int(double d);
+
+namespace {
+struct RefHandle {
+    Particles P;
+    Tree T;
+};
+void split128(peanokey k, uint64_t* hi, uint64_t* lo) {
+    const unsigned __int128 u = (unsigned __int128)k;
+    *hi = (uint64_t)(u >> 64);
+    *lo = (uint64_t)u;
+}
+}  // namespace
+
+extern "C" {
+
+int ref_max_threads() { return omp_get_max_threads(); }
+void ref_set_threads(int n) { omp_set_num_threads(n); }
+
+// shmem::build (tree.cc:350-526).  bt_out, when non-null, receives the 7 BuildTimes fields (ms).
+void* ref_build(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                const double* soft, long long randomize_seed, double* bt_out) {
+    RefHandle* h = new RefHandle();
+    h->P.x.assign(x, x + n); h->P.y.assign(y, y + n); h->P.z.assign(z, z + n);
+    h->P.m.assign(m, m + n);
+    if (soft) h->P.soft.assign(soft, soft + n);
+    BuildTimes bt;
+    h->T = build(h->P, &bt, nullptr, false, randomize_seed);
+    if (bt_out) {
+        bt_out[0] = bt.bbox; bt_out[1] = bt.keys; bt_out[2] = bt.sort; bt_out[3] = bt.recurse;
+        bt_out[4] = bt.links; bt_out[5] = bt.pack; bt_out[6] = bt.total;
+    }
+    return h;
+}
+
+void ref_free(void* p) { delete static_cast<RefHandle*>(p); }
+
+int64_t ref_tree_nnodes(void* p) { return (int64_t)static_cast<RefHandle*>(p)->T.nnodes(); }
+int ref_tree_root(void* p) { return static_cast<RefHandle*>(p)->T.root; }
+int64_t ref_tree_nlive(void* p) { return (int64_t)static_cast<RefHandle*>(p)->T.orderbuf.size(); }
+
+// Node arrays, each nnodes long (any pointer may be null).
+void ref_tree_nodes(void* p, double* cx, double* cy, double* cz, double* mass, double* size,
+                    double* delta, double* soft, double* gcx, double* gcy, double* gcz,
+                    int* first, int* next, int* plo, int* phi, int* parent,
+                    double* w_s, float* w_len, float* w_soft) {
+    const Tree& T = static_cast<RefHandle*>(p)->T;
+    const size_t nn = T.nnodes();
+    auto cpd = [nn](double* dst, const std::vector<double>& src) { if (dst) std::memcpy(dst, src.data(), nn * 8); };
+    auto cpi = [nn](int* dst, const std::vector<int>& src) { if (dst) std::memcpy(dst, src.data(), nn * 4); };
+    cpd(cx, T.cx); cpd(cy, T.cy); cpd(cz, T.cz); cpd(mass, T.mass); cpd(size, T.size);
+    cpd(delta, T.delta); cpd(soft, T.soft); cpd(gcx, T.gcx); cpd(gcy, T.gcy); cpd(gcz, T.gcz);
+    cpi(first, T.first); cpi(next, T.next); cpi(plo, T.plo); cpi(phi, T.phi); cpi(parent, T.parent);
+    for (size_t i = 0; i < nn; ++i) {
+        if (w_s) w_s[i] = T.wn[i].s;
+        if (w_len) w_len[i] = T.wn[i].len;
+        if (w_soft) w_soft[i] = T.wn[i].soft;
+    }
+}
+
+// orderbuf (nlive), rank (n), leaf_of (n).
+void ref_tree_order(void* p, uint32_t* orderbuf, uint32_t* rank, int* leaf_of) {
+    const Tree& T = static_cast<RefHandle*>(p)->T;
+    if (orderbuf) std::memcpy(orderbuf, T.orderbuf.data(), T.orderbuf.size() * 4);
+    if (rank) std::memcpy(rank, T.rank.data(), T.rank.size() * 4);
+    if (leaf_of) std::memcpy(leaf_of, T.leaf_of.data(), T.leaf_of.size() * 4);
+}
+
+// shmem::accel_grouped (tree.cc:626-897), gravity only (no tidal/jerk/lazy/sinks).
+void ref_accel_grouped(void* p, int64_t nt, const uint32_t* targets, double theta, double G,
+                       int batch, const double* aold, double* ax, double* ay, double* az) {
+    RefHandle* h = static_cast<RefHandle*>(p);
+    std::vector<uint32_t> tg(targets, targets + nt);
+    std::vector<double> vx, vy, vz;
+    accel_grouped(h->T, h->P, tg, theta, G, batch, vx, vy, vz, nullptr, aold);
+    std::memcpy(ax, vx.data(), nt * 8); std::memcpy(ay, vy.data(), nt * 8);
+    std::memcpy(az, vz.data(), nt * 8);
+}
+
+// shmem::accel (tree.cc:528-582): one walk per target, leaves always direct-summed.
+void ref_accel(void* p, int64_t nt, const uint32_t* targets, double theta, double G,
+               const double* aold, double* ax, double* ay, double* az) {
+    RefHandle* h = static_cast<RefHandle*>(p);
+    std::vector<uint32_t> tg(targets, targets + nt);
+    std::vector<double> vx, vy, vz;
+    accel(h->T, h->P, tg, theta, G, vx, vy, vz, aold);
+    std::memcpy(ax, vx.data(), nt * 8); std::memcpy(ay, vy.data(), nt * 8);
+    std::memcpy(az, vz.data(), nt * 8);
+}
+
+// shmem::potential (tree.cc:899-944).
+void ref_potential(void* p, int64_t nt, const uint32_t* targets, double theta, double G,
+                   const double* aold, double* phi) {
+    RefHandle* h = static_cast<RefHandle*>(p);
+    std::vector<uint32_t> tg(targets, targets + nt);
+    std::vector<double> out;
+    potential(h->T, h->P, tg, theta, G, out, aold);
+    std::memcpy(phi, out.data(), nt * 8);
+}
+
+// shmem::accel_brute (tree.cc:946-971), FP64 direct sum over every particle of the handle.
+void ref_accel_brute(void* p, int64_t nt, const uint32_t* targets, double G,
+                     double* ax, double* ay, double* az) {
+    RefHandle* h = static_cast<RefHandle*>(p);
+    std::vector<uint32_t> tg(targets, targets + nt);
+    std::vector<double> vx, vy, vz;
+    accel_brute(h->P, tg, G, vx, vy, vz);
+    std::memcpy(ax, vx.data(), nt * 8); std::memcpy(ay, vy.data(), nt * 8);
+    std::memcpy(az, vz.data(), nt * 8);
+}
+
+// Keys.  morton20: shmem::morton (tree.h:161-173).  The 128-bit keys come back as (hi, lo).
+uint64_t ref_morton20(uint32_t a, uint32_t b, uint32_t c) { return morton(a, b, c); }
+void ref_peano_hilbert_key(uint64_t x, uint64_t y, uint64_t z, int bits, uint64_t* hi, uint64_t* lo) {
+    split128(peano_hilbert_key(x, y, z, bits), hi, lo);
+}
+void ref_morton_key(uint64_t x, uint64_t y, uint64_t z, int bits, uint64_t* hi, uint64_t* lo) {
+    split128(morton_key(x, y, z, bits), hi, lo);
+}
+void ref_peano_and_morton_key(uint64_t x, uint64_t y, uint64_t z, int bits, uint64_t* phi_hi,
+                              uint64_t* phi_lo, uint64_t* mo_hi, uint64_t* mo_lo) {
+    peanokey mk = 0;
+    split128(peano_and_morton_key(x, y, z, bits, &mk), phi_hi, phi_lo);
+    split128(mk, mo_hi, mo_lo);
+}
+uint64_t ref_domain_double_to_int(double d) { return domain_double_to_int(d); }
+
+// Scalar kernels of tree.h, for known-answer checks.
+double ref_spline_force_over_r(double r, double h) { return spline_force_over_r(r, h); }
+double ref_spline_potential(double r, double h) { return spline_potential(r, h); }
+int ref_open_node(double r_sq, double len, double l_open, double node_mass, double node_maxsoft,
+                  double soft_target, double aold, double theta_sq, double adx, double ady,
+                  double adz) {
+    return open_node(r_sq, len, l_open, node_mass, node_maxsoft, soft_target, aold, theta_sq,
+                     adx, ady, adz) ? 1 : 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,120 @@
+"""Generate tests/golden/golden.npz from the REFERENCE itself.
+
+Runs the reference's own shmem tree and Peano-Hilbert functions, compiled from the reference
+sources into oracle/_ref/libgizmo_ref.so (``make -C oracle ref``), on small seeded inputs and
+stores their outputs.  The reference ships no golden force vectors (its shmem tests print error
+percentiles without asserting), so these fixtures are what pins the oracle restatement and the GPU
+path to the reference's numbers.  Regenerate with:
+
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from oracle import Reference  # noqa: E402
+
+from gizmo_shared_memory_b200 import ics  # noqa: E402
+
+
+def main():
+    R = Reference()
+    R.set_threads(1)
+    out = {}
+    rng = np.random.default_rng(2024)
+
+    # ---- keys: exhaustive at 1..3 bits per axis, random at 20 and 42 bits (system/peano.cc) ----
+    for bits in (1, 2, 3):
+        g = np.arange(1 << bits, dtype=np.uint64)
+        X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+        X, Y, Z = X.ravel(), Y.ravel(), Z.ravel()
+        ph = [R.peano_key(a, b, c, bits) for a, b, c in zip(X, Y, Z)]
+        mo = [R.morton_key(a, b, c, bits) for a, b, c in zip(X, Y, Z)]
+        out[f"keys{bits}_xyz"] = np.stack([X, Y, Z], 1)
+        out[f"keys{bits}_ph"] = np.array(ph, np.uint64)
+        out[f"keys{bits}_morton"] = np.array(mo, np.uint64)
+    for bits in (20, 42):
+        xyz = rng.integers(0, 1 << bits, size=(2000, 3), dtype=np.uint64)
+        ph, mo = [], []
+        for a, b, c in xyz:
+            p, m = R.peano_and_morton_key(a, b, c, bits)
+            ph.append(p)
+            mo.append(m)
+        out[f"keys{bits}_xyz"] = xyz
+        out[f"keys{bits}_ph_hi"] = np.array([p >> 64 for p in ph], np.uint64)
+        out[f"keys{bits}_ph_lo"] = np.array([p & ((1 << 64) - 1) for p in ph], np.uint64)
+        out[f"keys{bits}_morton_hi"] = np.array([p >> 64 for p in mo], np.uint64)
+        out[f"keys{bits}_morton_lo"] = np.array([p & ((1 << 64) - 1) for p in mo], np.uint64)
+    xyz20 = rng.integers(0, 1 << 20, size=(2000, 3), dtype=np.uint64)
+    out["morton20_xyz"] = xyz20
+    out["morton20"] = np.array([R.morton20(a, b, c) for a, b, c in xyz20], np.uint64)
+    d = rng.uniform(1.0, 2.0, 2000)
+    out["d2i_in"] = d
+    out["d2i_out"] = np.array([R.double_to_int(v) for v in d], np.uint64)
+
+    # ---- kernels (shmem/tree.h:59-80) ----------------------------------------------------------
+    h = 0.01
+    r = np.array([0.25, 0.5, 0.75, 0.999, 1.0, 2.0]) * h
+    out["spline_r"] = r
+    out["spline_h"] = np.full_like(r, h)
+    out["spline_f"] = np.array([R.spline_force_over_r(a, h) for a in r])
+    out["spline_p"] = np.array([R.spline_potential(a, h) for a in r])
+
+    # ---- a Plummer sphere: tree and walks ------------------------------------------------------
+    P = ics.plummer(n=4096, seed=42, soft=0.01)
+    P["m"][::97] = 0.0  # a few massless particles: left out of the tree (tree.cc:355-359)
+    for k in ("x", "y", "z", "m", "soft"):
+        out[f"plummer_{k}"] = P[k]
+    T = R.build(P)
+    nd = T.nodes()
+    ob, rank, leaf = T.order()
+    out["plummer_orderbuf"] = ob
+    out["plummer_rank"] = rank
+    out["plummer_leaf_of"] = leaf
+    for k in ("cx", "cy", "cz", "mass", "size", "delta", "soft", "gcx", "gcy", "gcz", "first",
+              "next", "plo", "phi", "parent", "w_s", "w_len", "w_soft"):
+        out[f"plummer_node_{k}"] = nd[k]
+    tg = ob
+    ax, ay, az = T.accel_grouped(tg, 0.7, 1.0, 0)
+    out["plummer_bh_ax"], out["plummer_bh_ay"], out["plummer_bh_az"] = ax, ay, az
+    aold = 0.005 * np.sqrt(ax * ax + ay * ay + az * az)
+    out["plummer_aold"] = aold
+    bx, by, bz = T.accel_grouped(tg, 0.0, 1.0, 0, aold=aold)
+    out["plummer_rel_ax"], out["plummer_rel_ay"], out["plummer_rel_az"] = bx, by, bz
+    cx, cy, cz = T.accel_grouped(tg, 0.7, 1.0, 8)
+    out["plummer_b8_ax"], out["plummer_b8_ay"], out["plummer_b8_az"] = cx, cy, cz
+    sub = tg[::7].copy()
+    out["plummer_sub"] = sub
+    px, py, pz = T.accel(sub, 0.5)
+    out["plummer_acc_ax"], out["plummer_acc_ay"], out["plummer_acc_az"] = px, py, pz
+    out["plummer_phi"] = T.potential(sub, 0.5)
+    qx, qy, qz = T.accel_brute(sub)
+    out["plummer_direct_ax"], out["plummer_direct_ay"], out["plummer_direct_az"] = qx, qy, qz
+
+    # ---- collocated particles: the level-20 leaf (tree.cc:89) ----------------------------------
+    Q = ics.plummer(n=600, seed=7, soft=0.02)
+    Q["x"][:40] = Q["x"][0]
+    Q["y"][:40] = Q["y"][0]
+    Q["z"][:40] = Q["z"][0]
+    for k in ("x", "y", "z", "m", "soft"):
+        out[f"colloc_{k}"] = Q[k]
+    TQ = R.build(Q)
+    obq, _, _ = TQ.order()
+    out["colloc_nnodes"] = np.array([TQ.nnodes])
+    ex, ey, ez = TQ.accel_grouped(obq, 0.7, 1.0, 0)
+    out["colloc_orderbuf"] = obq
+    out["colloc_ax"], out["colloc_ay"], out["colloc_az"] = ex, ey, ez
+
+    path = os.path.join(HERE, "golden.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path) / 1024:.0f} KiB")
+
+
+if __name__ == "__main__":
+    main()

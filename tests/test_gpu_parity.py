@@ -1,0 +1,405 @@
+"""GPU parity: the sm_100a path, called through the C ABI, against the oracle and the fixtures.
+
+Bars (stated per test):
+  * keys, sort order, tree topology, leaf membership: bit-exact (integer work);
+  * node moments: FP64, relative 1e-12 (the GPU reduces in a different summation order);
+  * walks: FP32 interaction arithmetic on FP64 group-relative offsets, so the acceleration must match
+    the oracle walk with the same opening criterion to a median relative error <= 1e-5; p99 is
+    bounded loosely (a few targets may see an opening decision flip at the threshold);
+  * FP64 direct sum: relative 1e-12.
+"""
+import numpy as np
+import pytest
+
+import gizmo_shared_memory_b200 as g
+from gizmo_shared_memory_b200 import ics
+
+pytestmark = pytest.mark.gpu
+
+MEDIAN_TOL = 1e-5
+
+
+def relerr(ax, ay, az, bx, by, bz):
+    d = np.sqrt((ax - bx) ** 2 + (ay - by) ** 2 + (az - bz) ** 2)
+    n = np.sqrt(bx ** 2 + by ** 2 + bz ** 2)
+    return d / np.where(n > 0, n, 1.0)
+
+
+def stable_order(keys, m):
+    live = np.nonzero(m > 0)[0]
+    return live[np.argsort(keys[live], kind="stable")].astype(np.uint32)
+
+
+@pytest.fixture(scope="module")
+def plummer():
+    return ics.plummer(n=65536, seed=42, soft=0.01)
+
+
+@pytest.fixture(scope="module")
+def plummer_trees(gpu_ctx, oracle, plummer):
+    return gpu_ctx.build(plummer, key_mode=g.GT_KEY_MORTON), oracle.build(plummer)
+
+
+# ---- keys and sort --------------------------------------------------------------------------
+
+@pytest.mark.parametrize("mode", [g.GT_KEY_MORTON, g.GT_KEY_PEANO])
+def test_keys_and_order_bit_exact(gpu_ctx, oracle, plummer, mode):
+    P = dict(plummer)
+    P["m"] = P["m"].copy()
+    P["m"][::101] = 0.0  # massless particles sort last and stay out of the tree
+    T = gpu_ctx.build(P, key_mode=mode)
+    keys, _ = oracle.keys20(P, key_mode=0 if mode == g.GT_KEY_MORTON else 1)
+    want = stable_order(keys, P["m"])
+    d = T.download(nodes=False)
+    assert np.array_equal(d["orderbuf"], want)
+    assert np.array_equal(T.keys(), keys[want])
+    rank = np.full(len(P["m"]), np.iinfo(np.uint32).max, np.uint32)
+    rank[want] = np.arange(len(want), dtype=np.uint32)
+    assert np.array_equal(d["rank"], rank)
+
+
+def test_peano_keys_42bit_golden(gpu_ctx, golden):
+    for bits in (1, 2, 3, 20, 42):
+        xyz = golden[f"keys{bits}_xyz"].astype(np.float64)
+        pos = xyz * 2.0 ** -bits  # (pos - 0)/1 + 1 has exactly these top mantissa bits
+        ph_hi, ph_lo, mo_hi, mo_lo = gpu_ctx.peano_keys(pos[:, 0], pos[:, 1], pos[:, 2], (0, 0, 0), 1.0, bits)
+        if bits <= 3:
+            assert np.array_equal(ph_lo, golden[f"keys{bits}_ph"])
+            assert np.array_equal(mo_lo, golden[f"keys{bits}_morton"])
+        else:
+            assert np.array_equal(ph_hi, golden[f"keys{bits}_ph_hi"])
+            assert np.array_equal(ph_lo, golden[f"keys{bits}_ph_lo"])
+            assert np.array_equal(mo_hi, golden[f"keys{bits}_morton_hi"])
+            assert np.array_equal(mo_lo, golden[f"keys{bits}_morton_lo"])
+
+
+def test_peano_keys_42bit_random(gpu_ctx, oracle):
+    rng = np.random.default_rng(9)
+    x, y, z = rng.uniform(-3, 5, (3, 5000))
+    corner, length = (-3.5, -3.5, -3.5), 9.0
+    ph_hi, ph_lo, _, _ = gpu_ctx.peano_keys(x, y, z, corner, length, 42)
+    for k in range(0, 5000, 7):
+        xb = oracle.double_to_int((x[k] - corner[0]) / length + 1.0, 42)
+        yb = oracle.double_to_int((y[k] - corner[1]) / length + 1.0, 42)
+        zb = oracle.double_to_int((z[k] - corner[2]) / length + 1.0, 42)
+        key = oracle.peano_key(xb, yb, zb, 42)
+        assert (int(ph_hi[k]) << 64) | int(ph_lo[k]) == key
+
+
+# ---- tree -----------------------------------------------------------------------------------
+
+def cell_map(nd):
+    return {(int(l), float(a), float(b), float(c)): i
+            for i, (l, a, b, c) in enumerate(zip(nd["level"], nd["gcx"], nd["gcy"], nd["gcz"]))}
+
+
+@pytest.mark.parametrize("mode", [g.GT_KEY_MORTON, g.GT_KEY_PEANO])
+def test_tree_matches_oracle(gpu_ctx, oracle, plummer, mode):
+    T = gpu_ctx.build(plummer, key_mode=mode)
+    O = oracle.build(plummer)
+    gn, on = T.download(), O.nodes()
+    assert len(gn["mass"]) == len(on["mass"])
+    gm, om = cell_map(gn), cell_map(on)
+    assert gm.keys() == om.keys()  # the same cells, bit-exact centres and levels
+    gi = np.array([gm[k] for k in om])
+    oi = np.array([om[k] for k in om])
+    for k in ("size", "w_len", "w_soft", "soft"):
+        assert np.array_equal(gn[k][gi], on[k][oi]), k
+    np.testing.assert_allclose(gn["mass"][gi], on["mass"][oi], rtol=1e-12)
+    scale = on["size"][oi]
+    for k in ("cx", "cy", "cz"):
+        assert np.all(np.abs(gn[k][gi] - on[k][oi]) <= 1e-12 * scale), k
+    assert np.all(np.abs(gn["w_s"][gi] - on["w_s"][oi]) <= 1e-12 * scale)
+    assert np.array_equal(gn["phi"][gi] - gn["plo"][gi], on["phi"][oi] - on["plo"][oi])
+    assert np.array_equal(gn["first"][gi] < 0, on["first"][oi] < 0)
+    # leaf membership is the same set of particles per cell
+    gob, oob = gn["orderbuf"], O.order()[0]
+    leaves = np.nonzero(on["first"][oi] < 0)[0]
+    for j in leaves[:: max(1, len(leaves) // 500)]:
+        a, b = gi[j], oi[j]
+        assert set(gob[gn["plo"][a]:gn["phi"][a]]) == set(oob[on["plo"][b]:on["phi"][b]])
+    if mode == g.GT_KEY_MORTON:
+        assert np.array_equal(gob, oob)
+
+
+def test_tree_threading_audit(gpu_ctx, plummer):
+    """The reference's audit (tree.cc:986-1015): next-chain children, every particle reached once."""
+    T = gpu_ctx.build(plummer)
+    d = T.download()
+    first, nxt, parent = d["first"], d["next"], d["parent"]
+    seen = np.zeros(len(plummer["m"]), np.int32)
+    stack = [0]
+    assert parent[0] == -1 and nxt[0] == -1
+    visited = 0
+    while stack:
+        X = stack.pop()
+        visited += 1
+        if first[X] < 0:
+            seen[d["orderbuf"][d["plo"][X]:d["phi"][X]]] += 1
+            assert np.all(d["leaf_of"][d["orderbuf"][d["plo"][X]:d["phi"][X]]] == X)
+            continue
+        c = first[X]
+        steps = 0
+        while c != nxt[X]:
+            assert parent[c] == X
+            stack.append(c)
+            c = nxt[c]
+            steps += 1
+            assert steps <= 8
+    assert visited == len(first)
+    assert np.all(seen == 1)
+
+
+# ---- walks ----------------------------------------------------------------------------------
+
+def check(a, b, tol=MEDIAN_TOL, p99=2e-3):
+    e = relerr(*a, *b)
+    assert np.isfinite(e).all()
+    assert np.median(e) <= tol, np.median(e)
+    assert np.quantile(e, 0.99) <= p99, np.quantile(e, 0.99)
+    return e
+
+
+def test_grouped_walk_plummer_65k(gpu_ctx, plummer_trees):
+    T, O = plummer_trees
+    ob = O.order()[0]
+    # first walk: Barnes-Hut theta = 0.7 with aold = 0 (the bootstrap)
+    ax, ay, az = gpu_ctx.accel_grouped(T, ob, theta=0.7)
+    ox, oy, oz, _ = O.accel_grouped(ob, 0.7)
+    check((ax, ay, az), (ox, oy, oz))
+    # then the relative criterion alone with aold = alpha |a| from the oracle's first walk
+    aold = 0.005 * np.sqrt(ox ** 2 + oy ** 2 + oz ** 2)
+    ax, ay, az = gpu_ctx.accel_grouped(T, ob, aold=aold, theta=0.0)
+    ox, oy, oz, _ = O.accel_grouped(ob, 0.0, aold=aold)
+    check((ax, ay, az), (ox, oy, oz))
+
+
+def test_grouped_walk_all_targets_null(gpu_ctx, plummer_trees):
+    """targets == NULL walks every live particle in tree order (= targets = orderbuf)."""
+    T, O = plummer_trees
+    ob = O.order()[0]
+    a = gpu_ctx.accel_grouped(T, None, theta=0.7)
+    b = gpu_ctx.accel_grouped(T, ob, theta=0.7)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
+    c = gpu_ctx.accel_grouped(T, None, theta=0.7, out_order=g.GT_OUT_ORIGINAL)
+    for u, v in zip(c, a):
+        assert np.array_equal(u[ob], v)
+
+
+def test_grouped_walk_golden(gpu_ctx, golden):
+    P = {k: golden[f"plummer_{k}"] for k in ("x", "y", "z", "m", "soft")}
+    T = gpu_ctx.build(P, key_mode=g.GT_KEY_MORTON)
+    tg = golden["plummer_orderbuf"]
+    ref = lambda p: (golden[f"plummer_{p}_ax"], golden[f"plummer_{p}_ay"], golden[f"plummer_{p}_az"])
+    check(gpu_ctx.accel_grouped(T, tg, theta=0.7), ref("bh"))
+    check(gpu_ctx.accel_grouped(T, tg, theta=0.0, aold=golden["plummer_aold"]), ref("rel"))
+    check(gpu_ctx.accel_grouped(T, tg, theta=0.7, batch=8), ref("b8"))
+    sub = golden["plummer_sub"]
+    check(gpu_ctx.accel(T, sub, theta=0.5), ref("acc"))
+    phi = gpu_ctx.potential(T, sub, theta=0.5)
+    e = np.abs(phi - golden["plummer_phi"]) / np.abs(golden["plummer_phi"])
+    assert np.median(e) <= MEDIAN_TOL
+    d = gpu_ctx.direct(P, sub)
+    e = relerr(*d[:3], *ref("direct"))
+    assert e.max() <= 1e-12
+
+
+def test_grouped_walk_peano_tree_same_forces(gpu_ctx, plummer, plummer_trees):
+    """PH and Morton trees hold the same cells: forces agree up to summation order."""
+    Tm, O = plummer_trees
+    Tp = gpu_ctx.build(plummer, key_mode=g.GT_KEY_PEANO)
+    ob = O.order()[0]
+    a = gpu_ctx.accel_grouped(Tp, ob, theta=0.7)
+    b = gpu_ctx.accel_grouped(Tm, ob, theta=0.7)
+    check(a, b, tol=1e-6, p99=1e-4)
+
+
+def test_batch_windows_and_per_target(gpu_ctx, plummer_trees):
+    T, O = plummer_trees
+    ob = O.order()[0]
+    check(gpu_ctx.accel_grouped(T, ob, theta=0.7, batch=8), O.accel_grouped(ob, 0.7, batch=8)[:3])
+    sub = ob[::17].copy()
+    check(gpu_ctx.accel(T, sub, theta=0.5), O.accel(sub, 0.5))
+    phi = gpu_ctx.potential(T, sub, theta=0.5)
+    ophi = O.potential(sub, 0.5)
+    e = np.abs(phi - ophi) / np.abs(ophi)
+    assert np.median(e) <= MEDIAN_TOL
+
+
+def test_grouped_potential_matches_oracle(gpu_ctx, plummer_trees):
+    T, O = plummer_trees
+    ob = O.order()[0]
+    ax, ay, az, phi = gpu_ctx.accel_grouped(T, ob, theta=0.7, want_phi=True)
+    starts = O.groups(ob, 0)
+    ox, oy, oz, ophi, _ = O.walk_groups(ob, starts, 0.7, want_phi=True)
+    check((ax, ay, az), (ox, oy, oz))
+    e = np.abs(phi - ophi) / np.abs(ophi)
+    assert np.median(e) <= MEDIAN_TOL
+
+
+def node_group_starts(O, gmax):
+    """Group starts of GT_GROUP_NODE over the full tree order, from the oracle tree."""
+    nd = O.nodes()
+    cnt = nd["phi"] - nd["plo"]
+    par = nd["parent"]
+    pc = np.where(par >= 0, cnt[np.maximum(par, 0)], np.iinfo(np.int32).max)
+    mark = ((cnt <= gmax) & (pc > gmax)) | ((nd["first"] < 0) & (cnt > gmax))
+    mark &= cnt > 0
+    s = np.sort(nd["plo"][mark]).astype(np.int64)
+    return np.concatenate([s, [O.nlive]])
+
+
+@pytest.mark.parametrize("gmax", [16, 32, 64])
+def test_node_groups_match_oracle(gpu_ctx, plummer_trees, gmax):
+    T, O = plummer_trees
+    ob = O.order()[0]
+    starts = node_group_starts(O, gmax)
+    # chunks of at most the kernel's capacity, as the library splits them
+    kmax = 32 if gmax <= 32 else 64
+    ch = [starts[0]]
+    for a, b in zip(starts[:-1], starts[1:]):
+        x = a
+        while x < b:
+            x = min(x + kmax, b)
+            ch.append(x)
+    ch = np.array(ch, np.int64)
+    aold = 0.0025 * np.ones(len(ob))
+    a = gpu_ctx.accel_grouped(T, None, aold=aold, group_mode=g.GT_GROUP_NODE, group_max=gmax)
+    b = O.walk_groups(ob, ch, 0.0, aold=aold)[:3]
+    check(a, b)
+
+
+def test_interaction_counts_match_oracle(gpu_ctx, plummer_trees):
+    T, O = plummer_trees
+    ob = O.order()[0]
+    gpu_ctx.accel_grouped(T, ob, theta=0.7, count=True)
+    s = gpu_ctx.stats()
+    _, _, _, cnt = O.accel_grouped(ob, 0.7)
+    assert s["nodes_visited"] == pytest.approx(cnt[0], rel=1e-4)
+    assert s["multipole"] == pytest.approx(cnt[1], rel=1e-4)
+    assert s["pairs"] == pytest.approx(cnt[2], rel=1e-4)
+    assert s["groups"] == len(O.groups(ob, 0)) - 1
+
+
+# ---- direct sum -----------------------------------------------------------------------------
+
+def test_direct_fp64_and_fp32(gpu_ctx, oracle, plummer):
+    tg = np.arange(0, 65536, 16, dtype=np.uint32)
+    ox, oy, oz, ophi = oracle.direct(plummer, tg)
+    ax, ay, az, phi = gpu_ctx.direct(plummer, tg)
+    assert relerr(ax, ay, az, ox, oy, oz).max() <= 1e-12
+    np.testing.assert_allclose(phi, ophi, rtol=1e-12)
+    fx, fy, fz, fphi = gpu_ctx.direct(plummer, tg, precision=g.GT_DIRECT_FP32)
+    e = relerr(fx, fy, fz, ox, oy, oz)
+    assert np.median(e) <= 1e-5 and e.max() <= 1e-3
+
+
+# ---- edge cases -----------------------------------------------------------------------------
+
+def test_empty_single_and_pair(gpu_ctx, oracle):
+    for n in (0, 1, 2, 17):
+        P = ics.plummer(n=n, seed=1) if n else {k: np.zeros(0) for k in ("x", "y", "z", "m", "soft")}
+        T = gpu_ctx.build(P)
+        info = T.info()
+        assert info["n_nodes"] >= 1 and info["n_live"] == n
+        if n == 0:
+            ax, ay, az = gpu_ctx.accel_grouped(T, None, theta=0.7)
+            assert len(ax) == 0
+            continue
+        O = oracle.build(P)
+        ob = O.order()[0]
+        a = gpu_ctx.accel_grouped(T, ob, theta=0.7)
+        b = O.accel_grouped(ob, 0.7)[:3]
+        if n == 1:
+            assert np.all(a[0] == 0) and np.all(a[1] == 0) and np.all(a[2] == 0)
+        else:
+            assert relerr(*a, *b).max() <= 1e-5
+
+
+def test_collocated_level20_leaf(gpu_ctx, golden):
+    Q = {k: golden[f"colloc_{k}"] for k in ("x", "y", "z", "m", "soft")}
+    T = gpu_ctx.build(Q, key_mode=g.GT_KEY_MORTON)
+    assert T.info()["n_nodes"] == int(golden["colloc_nnodes"][0])
+    tg = golden["colloc_orderbuf"]
+    a = gpu_ctx.accel_grouped(T, tg, theta=0.7)
+    e = relerr(*a, golden["colloc_ax"], golden["colloc_ay"], golden["colloc_az"])
+    assert np.median(e) <= MEDIAN_TOL and np.isfinite(e).all()
+
+
+def test_ragged_subset_and_massless_targets(gpu_ctx, oracle, plummer):
+    P = dict(plummer)
+    P["m"] = P["m"].copy()
+    P["m"][5::211] = 0.0
+    T = gpu_ctx.build(P, key_mode=g.GT_KEY_MORTON)
+    O = oracle.build(P)
+    _, rank, leaf = O.order()
+    rng = np.random.default_rng(4)
+    act = rng.choice(len(P["m"]), 3000, replace=False).astype(np.uint32)
+    live = act[rank[act] != np.iinfo(np.uint32).max]
+    dead = act[rank[act] == np.iinfo(np.uint32).max]
+    # active set in tree order (mfm.cc:705-711), massless targets appended: each its own group
+    tg = np.concatenate([live[np.argsort(rank[live])], dead]).astype(np.uint32)
+    a = gpu_ctx.accel_grouped(T, tg, theta=0.7)
+    b = O.accel_grouped(tg, 0.7)[:3]
+    check(a, b)
+
+
+def test_host_and_device_paths_identical(gpu_ctx, plummer):
+    import torch
+
+    ctx = g.Context(0, torch_stream=True)
+    T = ctx.build(plummer)
+    dev = {k: torch.as_tensor(v, device="cuda") for k, v in plummer.items()}
+    Td = ctx.build(dev)
+    a = ctx.accel_grouped(T, None, theta=0.7)
+    b = ctx.accel_grouped(Td, None, theta=0.7, device_out=True)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v.cpu().numpy())
+
+
+def test_form_aold(gpu_ctx):
+    rng = np.random.default_rng(3)
+    ax, ay, az = rng.normal(size=(3, 1000))
+    aold = gpu_ctx.form_aold(ax, ay, az, 0.005, G=2.0)
+    np.testing.assert_allclose(aold, 0.005 * np.sqrt(ax ** 2 + ay ** 2 + az ** 2) / 2.0, rtol=1e-15)
+
+
+def test_errors_leave_context_usable(gpu_ctx, plummer):
+    P = dict(plummer)
+    P["x"] = P["x"].copy()
+    P["x"][3] = np.nan
+    with pytest.raises(g.GTError) as e:
+        gpu_ctx.build(P)
+    assert e.value.status == 7  # GT_ERR_NONFINITE
+    T = gpu_ctx.build(plummer)
+    with pytest.raises(g.GTError) as e:
+        gpu_ctx.accel_grouped(T, np.array([10 ** 7], np.uint32), theta=0.7)
+    assert e.value.status == 1  # GT_ERR_INVALID
+    with pytest.raises(g.GTError) as e:
+        gpu_ctx.accel_grouped(T, None, theta=0.7, mac=g.GT_MAC_LEARNED)
+    assert e.value.status == 4  # GT_ERR_UNSUPPORTED (no network loaded)
+    a = gpu_ctx.accel_grouped(T, None, theta=0.7)
+    assert np.isfinite(a[0]).all()
+
+
+# ---- size-independent properties at a large size ----------------------------------------------
+
+def test_properties_galaxy_4m(gpu_ctx):
+    """Full 4M-particle galaxy: G-linearity and mass scaling are exact; permuting the input leaves
+    the tree order, and hence every force, bit-identical."""
+    P = ics.galaxy(seed=2)
+    T = gpu_ctx.build(P)
+    a1 = gpu_ctx.accel_grouped(T, None, theta=0.7, out_order=g.GT_OUT_ORIGINAL)
+    a2 = gpu_ctx.accel_grouped(T, None, theta=0.7, G=2.0, out_order=g.GT_OUT_ORIGINAL)
+    for u, v in zip(a1, a2):
+        assert np.array_equal(2.0 * u, v)
+    perm = np.random.default_rng(0).permutation(len(P["m"]))
+    Pp = {k: v[perm] for k, v in P.items()}
+    Tp = gpu_ctx.build(Pp)
+    ap = gpu_ctx.accel_grouped(Tp, None, theta=0.7, out_order=g.GT_OUT_ORIGINAL)
+    # particles with equal keys may swap, which only reorders sums inside a leaf
+    for u, v in zip(a1, ap):
+        e = np.abs(u[perm] - v) / (np.abs(u[perm]) + 1e-300)
+        assert np.median(e) <= 1e-12 and e.max() < 1e-5
+    assert np.isfinite(a1[0]).all()

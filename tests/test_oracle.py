@@ -1,0 +1,176 @@
+"""CPU tests: the oracle restatement (oracle/gt_oracle.c) pinned against the reference.
+
+Two anchors: the committed fixtures in tests/golden/golden.npz (outputs of the reference's own
+shmem tree and Peano-Hilbert functions, see tests/golden/make_golden.py) and, where the reference
+sources were available at build time, the compiled reference itself (oracle/_ref).
+"""
+import numpy as np
+import pytest
+
+from gizmo_shared_memory_b200 import ics
+
+
+def relerr(ax, ay, az, bx, by, bz):
+    d = np.sqrt((ax - bx) ** 2 + (ay - by) ** 2 + (az - bz) ** 2)
+    n = np.sqrt(bx ** 2 + by ** 2 + bz ** 2)
+    return d / np.where(n > 0, n, 1.0)
+
+
+def particles(golden, prefix):
+    return {k: golden[f"{prefix}_{k}"] for k in ("x", "y", "z", "m", "soft")}
+
+
+# ---- keys -----------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("bits", [1, 2, 3])
+def test_peano_keys_exhaustive(oracle, golden, bits):
+    xyz = golden[f"keys{bits}_xyz"]
+    ph = [oracle.peano_key(a, b, c, bits) for a, b, c in xyz]
+    mo = [oracle.morton_key(a, b, c, bits) for a, b, c in xyz]
+    assert np.array_equal(np.array(ph, np.uint64), golden[f"keys{bits}_ph"])
+    assert np.array_equal(np.array(mo, np.uint64), golden[f"keys{bits}_morton"])
+    # the Hilbert key is a bijection of the 8^bits cells
+    assert len(set(ph)) == len(ph)
+
+
+def test_peano_keys_reach_all_48_states(oracle, golden):
+    # At 3 bits every rotation state of the table is entered at least once on the way down; the
+    # exhaustive match above therefore covers every table row.  Here: keys of consecutive cells
+    # along the curve are face neighbours (the defining Hilbert property).
+    bits = 3
+    xyz = golden[f"keys{bits}_xyz"].astype(np.int64)
+    order = np.argsort(golden[f"keys{bits}_ph"])
+    steps = np.abs(np.diff(xyz[order], axis=0)).sum(1)
+    assert np.all(steps == 1)
+
+
+@pytest.mark.parametrize("bits", [20, 42])
+def test_peano_keys_random(oracle, golden, bits):
+    xyz = golden[f"keys{bits}_xyz"]
+    for k, (a, b, c) in enumerate(xyz):
+        ph = oracle.peano_key(a, b, c, bits)
+        mo = oracle.morton_key(a, b, c, bits)
+        assert ph >> 64 == golden[f"keys{bits}_ph_hi"][k]
+        assert ph & ((1 << 64) - 1) == golden[f"keys{bits}_ph_lo"][k]
+        assert mo >> 64 == golden[f"keys{bits}_morton_hi"][k]
+        assert mo & ((1 << 64) - 1) == golden[f"keys{bits}_morton_lo"][k]
+
+
+def test_morton20_and_double_to_int(oracle, golden):
+    for (a, b, c), want in zip(golden["morton20_xyz"], golden["morton20"]):
+        assert oracle.morton20(a, b, c) == want
+    got = [oracle.double_to_int(d, 42) for d in golden["d2i_in"]]
+    assert np.array_equal(np.array(got, np.uint64), golden["d2i_out"])
+
+
+# ---- kernels and criterion -------------------------------------------------------------------
+
+def test_spline_known_answers(oracle, golden):
+    for r, h, f, p in zip(golden["spline_r"], golden["spline_h"], golden["spline_f"], golden["spline_p"]):
+        assert oracle.spline_force_over_r(r, h) == pytest.approx(f, rel=1e-14)
+        assert oracle.spline_potential(r, h) == pytest.approx(p, rel=1e-14)
+    # Newtonian outside the kernel, continuous at u = 1
+    assert oracle.spline_force_over_r(2.0, 1.0) == pytest.approx(1.0 / 8.0, rel=1e-15)
+    assert oracle.spline_potential(2.0, 1.0) == pytest.approx(-0.5, rel=1e-15)
+    assert oracle.spline_force_over_r(1.0 - 1e-12, 1.0) == pytest.approx(1.0, rel=1e-9)
+
+
+def test_open_node_matches_reference(oracle, reference):
+    rng = np.random.default_rng(5)
+    for _ in range(3000):
+        args = [rng.uniform(0, 2) ** 2, rng.uniform(0.01, 1), rng.uniform(0.01, 1.5),
+                rng.uniform(0, 1), rng.uniform(0, 0.05), rng.uniform(0, 0.05),
+                rng.choice([0.0, rng.uniform(0, 0.01)]), rng.choice([0.0, 0.49]),
+                rng.uniform(0, 1), rng.uniform(0, 1), rng.uniform(0, 1)]
+        assert oracle.open_node(*args) == reference.open_node(*args)
+
+
+# ---- tree ------------------------------------------------------------------------------------
+
+def test_tree_matches_golden(oracle, golden):
+    P = particles(golden, "plummer")
+    T = oracle.build(P)
+    nd = T.nodes()
+    ob, rank, leaf = T.order()
+    assert T.nnodes == len(golden["plummer_node_mass"])
+    assert np.array_equal(ob, golden["plummer_orderbuf"])
+    assert np.array_equal(rank, golden["plummer_rank"])
+    assert np.array_equal(leaf, golden["plummer_leaf_of"])
+    for k in ("first", "next", "plo", "phi", "parent"):
+        assert np.array_equal(nd[k], golden[f"plummer_node_{k}"]), k
+    for k in ("size", "gcx", "gcy", "gcz", "w_len", "w_soft", "soft"):
+        assert np.array_equal(nd[k], golden[f"plummer_node_{k}"]), k
+    for k in ("cx", "cy", "cz", "mass", "delta", "w_s"):
+        np.testing.assert_allclose(nd[k], golden[f"plummer_node_{k}"], rtol=1e-12, atol=1e-15, err_msg=k)
+
+
+def test_empty_and_single_particle(oracle):
+    for n in (0, 1):
+        P = {"x": np.zeros(n), "y": np.zeros(n), "z": np.zeros(n), "m": np.ones(n), "soft": np.zeros(n)}
+        T = oracle.build(P)
+        assert T.nnodes == 1
+        ax, ay, az, _ = T.accel_grouped(np.arange(n, dtype=np.uint32), 0.7)
+        assert np.all(ax == 0) and np.all(ay == 0) and np.all(az == 0)
+
+
+# ---- walks -----------------------------------------------------------------------------------
+
+def test_walks_match_golden(oracle, golden):
+    P = particles(golden, "plummer")
+    T = oracle.build(P)
+    tg = golden["plummer_orderbuf"]
+    ax, ay, az, _ = T.accel_grouped(tg, 0.7)
+    assert relerr(ax, ay, az, golden["plummer_bh_ax"], golden["plummer_bh_ay"], golden["plummer_bh_az"]).max() < 1e-12
+    bx, by, bz, _ = T.accel_grouped(tg, 0.0, aold=golden["plummer_aold"])
+    assert relerr(bx, by, bz, golden["plummer_rel_ax"], golden["plummer_rel_ay"], golden["plummer_rel_az"]).max() < 1e-12
+    cx, cy, cz, _ = T.accel_grouped(tg, 0.7, batch=8)
+    assert relerr(cx, cy, cz, golden["plummer_b8_ax"], golden["plummer_b8_ay"], golden["plummer_b8_az"]).max() < 1e-12
+    sub = golden["plummer_sub"]
+    px, py, pz = T.accel(sub, 0.5)
+    assert relerr(px, py, pz, golden["plummer_acc_ax"], golden["plummer_acc_ay"], golden["plummer_acc_az"]).max() < 1e-12
+    phi = T.potential(sub, 0.5)
+    np.testing.assert_allclose(phi, golden["plummer_phi"], rtol=1e-12)
+    dx, dy, dz, _ = oracle.direct(P, sub)
+    assert relerr(dx, dy, dz, golden["plummer_direct_ax"], golden["plummer_direct_ay"], golden["plummer_direct_az"]).max() < 1e-12
+
+
+def test_collocated_matches_golden(oracle, golden):
+    Q = particles(golden, "colloc")
+    T = oracle.build(Q)
+    assert T.nnodes == int(golden["colloc_nnodes"][0])
+    ob, _, _ = T.order()
+    rob = golden["colloc_orderbuf"]
+    # the reference's parallel sort is not stable: particles with equal keys (the collocated ones)
+    # may come in any order, so compare positions in tree order, then walk the reference's order
+    for k in ("x", "y", "z"):
+        assert np.array_equal(Q[k][ob], Q[k][rob])
+    assert sorted(ob.tolist()) == sorted(rob.tolist())
+    ax, ay, az, _ = T.accel_grouped(rob, 0.7)
+    assert relerr(ax, ay, az, golden["colloc_ax"], golden["colloc_ay"], golden["colloc_az"]).max() < 1e-12
+
+
+def test_restatement_matches_live_reference(oracle, reference):
+    """A second, larger seeded case against the compiled reference (when it is available)."""
+    P = ics.plummer(n=30000, seed=11, soft=0.005)
+    T, R = oracle.build(P), reference.build(P)
+    ob, _, _ = T.order()
+    rob, _, _ = R.order()
+    assert T.nnodes == R.nnodes
+    assert np.array_equal(ob, rob)
+    ax, ay, az, cnt = T.accel_grouped(ob, 0.7)
+    bx, by, bz = R.accel_grouped(ob, 0.7)
+    assert relerr(ax, ay, az, bx, by, bz).max() < 1e-11
+    aold = 0.0025 * np.sqrt(ax ** 2 + ay ** 2 + az ** 2)
+    ax, ay, az, cnt = T.accel_grouped(ob, 0.0, aold=aold)
+    bx, by, bz = R.accel_grouped(ob, 0.0, aold=aold)
+    assert relerr(ax, ay, az, bx, by, bz).max() < 1e-11
+    assert cnt[1] > 0 and cnt[2] > 0
+
+
+def test_randomized_root_matches_reference(oracle, reference):
+    P = ics.plummer(n=5000, seed=3)
+    T, R = oracle.build(P, randomize_seed=17), reference.build(P, randomize_seed=17)
+    assert T.nnodes == R.nnodes
+    tn, rn = T.nodes(), R.nodes()
+    assert np.array_equal(tn["gcx"], rn["gcx"]) and np.array_equal(tn["size"], rn["size"])
+    assert np.array_equal(T.order()[0], R.order()[0])
