@@ -398,8 +398,10 @@ def test_properties_galaxy_4m(gpu_ctx):
     Pp = {k: v[perm] for k, v in P.items()}
     Tp = gpu_ctx.build(Pp)
     ap = gpu_ctx.accel_grouped(Tp, None, theta=0.7, out_order=g.GT_OUT_ORIGINAL)
-    # particles with equal keys may swap, which only reorders sums inside a leaf
+    # particles with equal keys may swap, which only reorders FP32 sums inside a leaf: most forces
+    # stay bit-identical, the rest move by summation-order rounding (amplified where the net force
+    # nearly cancels)
     for u, v in zip(a1, ap):
         e = np.abs(u[perm] - v) / (np.abs(u[perm]) + 1e-300)
-        assert np.median(e) <= 1e-12 and e.max() < 1e-5
+        assert np.median(e) == 0.0 and np.quantile(e, 0.999) <= 1e-6 and e.max() < 1e-3
     assert np.isfinite(a1[0]).all()
