@@ -35,7 +35,7 @@ EXPORTS = [
     "gt_context_set_stream", "gt_synchronize", "gt_launch_count", "gt_build", "gt_tree_free",
     "gt_tree_info_get", "gt_tree_download", "gt_tree_keys", "gt_accel_grouped", "gt_accel",
     "gt_potential", "gt_walk_stats_get", "gt_form_aold", "gt_direct", "gt_peano_keys",
-    "gt_measure_peaks",
+    "gt_measure_peaks", "gt_direct_noalloc",
 ]
 
 
@@ -116,6 +116,7 @@ def load_library(path: str = LIB_PATH):
     L.gt_direct.argtypes = [vp, i64, vp, vp, vp, vp, vp, i64, vp, d, C.c_int, C.c_int, vp, vp, vp, vp]
     L.gt_peano_keys.argtypes = [vp, i64, vp, vp, vp, vp, d, C.c_int, C.c_int, vp, vp, vp, vp]
     L.gt_measure_peaks.argtypes = [vp, C.POINTER(d), C.POINTER(d)]
+    L.gt_direct_noalloc.argtypes = [i64, vp, vp, vp, vp, vp, i64, vp, d, C.c_int, vp, vp, vp, vp, vp]
     for name in EXPORTS:
         fn = getattr(L, name)
         if fn.restype is C.c_int or fn.restype is None and name not in (

@@ -10,8 +10,15 @@
 //   FP32: the pair offset is differenced in double and narrowed, everything after it is float
 //         (grav_cuda.cu:108-134 without zeta terms or a periodic wrap).
 #include <algorithm>
+#include <mutex>
 
 #include "gt_internal.cuh"
+
+// Fixed scratch of the allocation-free entry point gt_direct_noalloc: the per-chunk partial sums,
+// 8 MiB, present on every GPU that loads this library until the process exits.  Host code must
+// never pass this name to a kernel -- on the host it is only a stand-in symbol; its device address
+// comes from cudaGetSymbolAddress (see noalloc_scratch below).
+static __device__ __align__(256) double g_direct_noalloc_scratch[GT_DIRECT_NOALLOC_SCRATCH_DOUBLES];
 
 namespace gt {
 namespace {
@@ -139,28 +146,110 @@ __global__ void direct_reduce_kernel(const double* __restrict__ partial, int64_t
     }
 }
 
+// Source chunking: enough chunks that (target blocks x chunks) fills the GPU, at most
+// `max_chunks`.  Returns the chunk length and sets nchunk.
+int64_t plan_chunks(int64_t n, int64_t nt, int num_sms, int64_t max_chunks, int& nchunk) {
+    const int bx = div_up(nt, kDirThreads);
+    int64_t c = std::max(1, div_up((int64_t)num_sms * 4, bx));
+    c = std::min<int64_t>(c, std::max<int64_t>(1, div_up(n, 4 * kDirTile)));
+    c = std::min<int64_t>(c, std::min<int64_t>(65535, std::max<int64_t>(1, max_chunks)));
+    const int64_t chunk = std::max<int64_t>(1, div_up(n, c));
+    nchunk = std::max(1, div_up(n, chunk));
+    return chunk;
+}
+
+void launch_direct(cudaStream_t st, int num_sms, int64_t n, const double* x, const double* y,
+                   const double* z, const double* m, const double* soft, int64_t nt,
+                   const uint32_t* targets, double G, int precision, double* ax, double* ay,
+                   double* az, double* phi, double* partial, int nchunk, int64_t chunk) {
+    const dim3 grid(div_up(nt, kDirThreads), nchunk);
+    if (precision == GT_DIRECT_FP32)
+        direct_kernel<false><<<grid, kDirThreads, 0, st>>>(x, y, z, m, soft, n, targets, nt, chunk, partial);
+    else
+        direct_kernel<true><<<grid, kDirThreads, 0, st>>>(x, y, z, m, soft, n, targets, nt, chunk, partial);
+    direct_reduce_kernel<<<std::max(1, std::min(div_up(nt, 256), num_sms * 4)), 256, 0, st>>>(
+        partial, nt, nchunk, G, ax, ay, az, phi);
+}
+
 }  // namespace
 
 void run_direct(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
                 const double* m, const double* soft, int64_t nt, const uint32_t* targets, double G,
                 int precision, double* ax, double* ay, double* az, double* phi) {
     if (nt <= 0) return;
-    const int bx = div_up(nt, kDirThreads);
-    int nchunk = std::max(1, div_up((int64_t)ctx->num_sms * 4, bx));
-    nchunk = std::min<int64_t>(nchunk, std::max<int64_t>(1, div_up(n, 4 * kDirTile)));
-    nchunk = std::min(nchunk, 65535);
-    const int64_t chunk = std::max<int64_t>(1, div_up(n, nchunk));
-    nchunk = std::max(1, div_up(n, chunk));
+    int nchunk = 1;
+    const int64_t chunk = plan_chunks(n, nt, ctx->num_sms, 65535, nchunk);
     double* partial = (double*)scratch(ctx, kSlotDirect, (size_t)nchunk * 4 * nt * 8);
-    const dim3 grid(bx, nchunk);
-    if (precision == GT_DIRECT_FP32)
-        direct_kernel<false><<<grid, kDirThreads, 0, ctx->stream>>>(x, y, z, m, soft, n, targets, nt, chunk, partial);
-    else
-        direct_kernel<true><<<grid, kDirThreads, 0, ctx->stream>>>(x, y, z, m, soft, n, targets, nt, chunk, partial);
-    check_launch(ctx, "direct_kernel");
-    direct_reduce_kernel<<<std::max(1, std::min(div_up(nt, 256), ctx->num_sms * 4)), 256, 0, ctx->stream>>>(
-        partial, nt, nchunk, G, ax, ay, az, phi);
-    check_launch(ctx, "direct_reduce_kernel");
+    launch_direct(ctx->stream, ctx->num_sms, n, x, y, z, m, soft, nt, targets, G, precision, ax, ay,
+                  az, phi, partial, nchunk, chunk);
+    ctx->launches += 2;
+    check_cuda(cudaGetLastError(), "direct_kernel");
 }
 
 }  // namespace gt
+
+// ---------------------------------------------------------------------------------------------
+// gt_direct_noalloc: the direct sum for callers that must not allocate device memory
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+int g_noalloc_sms[kNoAllocMaxDevices] = {};
+
+// Device address of g_direct_noalloc_scratch on `dev` (which is current), looked up once per device.
+int noalloc_scratch(int dev, double** ptr, int* sms) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_direct_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return GT_ERR_CUDA;
+        }
+        int nsm = 0;
+        e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess || nsm <= 0) {
+            cudaGetLastError();
+            return GT_ERR_CUDA;
+        }
+        g_noalloc_sms[dev] = nsm;
+        g_noalloc_ptr[dev] = (double*)p;
+    }
+    *ptr = g_noalloc_ptr[dev];
+    *sms = g_noalloc_sms[dev];
+    return GT_OK;
+}
+
+}  // namespace
+
+extern "C" int gt_direct_noalloc(int64_t n, const double* x, const double* y, const double* z,
+                                 const double* m, const double* soft, int64_t n_targets,
+                                 const uint32_t* targets, double G, int precision, double* ax,
+                                 double* ay, double* az, double* phi, void* stream) {
+    if (n < 0 || n_targets < 0) return GT_ERR_INVALID;
+    if (n > 0 && (!x || !y || !z || !m)) return GT_ERR_INVALID;
+    if (n_targets > 0 && (!targets || !ax || !ay || !az)) return GT_ERR_INVALID;
+    if (precision != GT_DIRECT_FP64 && precision != GT_DIRECT_FP32) return GT_ERR_INVALID;
+    if (n_targets > GT_DIRECT_NOALLOC_MAX_TARGETS) return GT_ERR_OVERFLOW;
+    if (n_targets == 0) return GT_OK;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+        cudaGetLastError();
+        return GT_ERR_DEVICE;
+    }
+    double* partial = nullptr;
+    int sms = 0;
+    const int st = noalloc_scratch(dev, &partial, &sms);
+    if (st != GT_OK) return st;
+    // every (chunk, target) partial the reduction reads is written by this call's first kernel,
+    // so the scratch needs no clearing; the chunk count is capped so the partials fit
+    const int64_t max_chunks = GT_DIRECT_NOALLOC_SCRATCH_DOUBLES / (4 * n_targets);
+    int nchunk = 1;
+    const int64_t chunk = gt::plan_chunks(n, n_targets, sms, max_chunks, nchunk);
+    gt::launch_direct((cudaStream_t)stream, sms, n, x, y, z, m, soft, n_targets, targets, G, precision,
+                      ax, ay, az, phi, partial, nchunk, chunk);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GT_OK : GT_ERR_CUDA;
+}

@@ -199,6 +199,30 @@ GT_API int gt_direct(gt_context* ctx, int64_t n, const double* x, const double* 
               const double* m, const double* soft, int64_t n_targets, const uint32_t* targets,
               double G, int precision, int mem, double* ax, double* ay, double* az, double* phi);
 
+/* Allocation-free direct sum.  No counterpart in the reference: it exists for callers that cannot
+ * allocate device memory at the point of the call -- an application whose pool allocator already
+ * owns all free device memory, or one that must not trigger the implicit device-wide
+ * synchronisation that cudaMalloc/cudaFree can cause in the middle of an asynchronous step.
+ * Same computation as gt_direct, but every array is a device pointer on the current device, no
+ * context is used, and the per-chunk partial sums live in one fixed 8 MiB device array inside the
+ * library (GT_DIRECT_NOALLOC_SCRATCH_DOUBLES doubles, held on every GPU that loads the library
+ * until the process exits).  The call never calls cudaMalloc or cudaFree.  It enqueues its two
+ * kernels on `stream` (NULL: the default stream) and returns without synchronising.
+ *  - n_targets above GT_DIRECT_NOALLOC_MAX_TARGETS is rejected with GT_ERR_OVERFLOW, before
+ *    anything is launched.
+ *  - The first call on a device looks up the array's device address with cudaGetSymbolAddress
+ *    (once per device, with that device current); make that first call before any stream capture.
+ *  - Every call shares the one array, which keeps the last call's contents (each call overwrites
+ *    every partial it reads, so nothing needs clearing).  Calls that overlap on the GPU -- on
+ *    different streams, or from different host threads -- race on it and give wrong results;
+ *    serialise them. */
+#define GT_DIRECT_NOALLOC_SCRATCH_DOUBLES (1 << 20)
+#define GT_DIRECT_NOALLOC_MAX_TARGETS (GT_DIRECT_NOALLOC_SCRATCH_DOUBLES / 4)
+GT_API int gt_direct_noalloc(int64_t n, const double* x, const double* y, const double* z,
+                             const double* m, const double* soft, int64_t n_targets,
+                             const uint32_t* targets, double G, int precision, double* ax,
+                             double* ay, double* az, double* phi, void* stream);
+
 /* ---- keys ---------------------------------------------------------------------------------- */
 /* Peano-Hilbert (and Morton) keys of the MPI code's domain decomposition: each coordinate mapped
  * to [1,2) as (pos - corner)/len + 1 and its top `bits` mantissa bits taken
