@@ -246,8 +246,9 @@ def run_gpu_arm(args):
     torch.cuda.set_device(local)
     cfg = WORKLOADS[args.workload]
     alpha = args.alpha if args.alpha is not None else cfg["alpha"]
-    group_mode = {"leaf": g.GT_GROUP_LEAF, "node": g.GT_GROUP_NODE}[args.group]
-    wopts = dict(group_mode=group_mode, group_max=args.group_max)
+    group_mode = {"leaf": g.GT_GROUP_LEAF, "node": g.GT_GROUP_NODE, "batch": g.GT_GROUP_BATCH}[args.group]
+    wopts = dict(group_mode=group_mode, group_max=args.group_max,
+                 batch=args.group_max if args.group == "batch" else 0)
 
     P = make_workload(args.workload, seed_offset=rank)
     n = len(P["m"])
@@ -364,7 +365,9 @@ def run_gpu_arm(args):
         "data": "synthetic (seeded; see config.description)",
         "config": {"workload": args.workload, "description": cfg["desc"], "n": n,
                    "criterion": f"plain relative criterion alpha={alpha} after a theta=0.7 bootstrap walk",
-                   "mac": "plain", "grouping": args.group + (f" (group_max {args.group_max})" if args.group == "node" else ""),
+                   "mac": "plain", "grouping": {"leaf": "leaf groups (accel_grouped batch 0)",
+                                "batch": f"windows of {args.group_max} consecutive targets in Peano-Hilbert tree order (accel_grouped batch {args.group_max})",
+                                "node": f"tree nodes of at most {args.group_max} particles"}[args.group],
                    "l2": f"inputs larger than L2: {n * 32 / 2**20:.0f} MiB of particles + "
                          f"{info['n_nodes'] * 64 / 2**20:.0f} MiB of nodes per walk",
                    "precision": "FP64 positions and group-relative offsets, FP32 interactions, "
@@ -400,7 +403,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="clustered_16m")
     ap.add_argument("--alpha", type=float, default=None)
-    ap.add_argument("--group", choices=["leaf", "node"], default="leaf")
+    ap.add_argument("--group", choices=["leaf", "node", "batch"], default="batch",
+                    help="leaf: accel_grouped batch 0; batch: windows of --group-max consecutive "
+                         "targets in tree order (accel_grouped batch > 0); node: tree nodes of at "
+                         "most --group-max particles")
     ap.add_argument("--group-max", type=int, default=32)
     ap.add_argument("--sample-seconds", type=float, default=8.0)
     ap.add_argument("--no-e2e", action="store_true")

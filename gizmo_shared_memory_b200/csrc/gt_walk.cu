@@ -35,7 +35,8 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxWarps = 8;     // warps per block of the walk kernel
-constexpr int kListCap = 256;    // interaction-list entries per warp
+constexpr int kPnCap = 256;      // monopole-list entries per warp
+constexpr int kPpCap = 128;      // particle-list entries per warp
 
 struct WalkArgs {
     const GNode* nodes;
@@ -106,20 +107,20 @@ __device__ __forceinline__ void load_src(const SrcP* __restrict__ p, double& x, 
     h = __int_as_float(b.w);
 }
 
-// The opening test of shmem/tree.h:109-144, FP64, same order of arms.
+// The opening test of shmem/tree.h:109-144 in FP64.  Every arm of the reference returns "open" as
+// soon as it holds and the last arm decides otherwise, so the test is the OR of the arms: softening
+// overlap, Barnes-Hut (theta > 0), relative criterion (aold > 0; with aold == 0 and no theta it
+// opens), inside-node.  Evaluated without branches so the lanes of a warp do not diverge.
 __device__ __forceinline__ bool open_node(double r2, double len, double l_open, double mass,
                                           double nsoft, double tsoft, double aold, double theta2,
                                           double dx, double dy, double dz) {
     const double rt = tsoft + 0.6 * len, rn = nsoft + 0.6 * len;
-    if (r2 < rt * rt || r2 < rn * rn) return true;
-    if (theta2 > 0.0 && l_open * l_open >= theta2 * r2) return true;
-    if (aold > 0) {
-        if (mass * len * len > r2 * r2 * aold) return true;
-    } else if (theta2 <= 0.0) {
-        return true;
-    }
+    const bool overlap = (r2 < rt * rt) | (r2 < rn * rn);
+    const bool bh = (theta2 > 0.0) & (l_open * l_open >= theta2 * r2);
+    const bool rel = (aold > 0) ? (mass * len * len > r2 * r2 * aold) : (theta2 <= 0.0);
     const double lim = 0.6 * len;
-    return dx < lim && dy < lim && dz < lim;
+    const bool inside = (dx < lim) & (dy < lim) & (dz < lim);
+    return overlap | bh | rel | inside;
 }
 
 // Softened pair inside the kernel (r < h): force factor and potential of the cubic spline,
@@ -149,20 +150,31 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
     sum = t;
 }
 
-template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT>
-__global__ void __launch_bounds__(kMaxWarps * 32)
-walk_kernel(const WalkArgs A) {
-    __shared__ float4 s_pm[kMaxWarps][kListCap];
-    __shared__ float s_h[kMaxWarps][kListCap];
-    __shared__ int s_lo[kMaxWarps][32];
-    __shared__ int s_pre[kMaxWarps][32];
+// Per-warp shared memory: the monopole list (float4: offset, mass), the particle list (float4 +
+// softening) and the leaf-expansion scratch.
+struct WarpSmem {
+    float4 pn[kPnCap];
+    float4 pp[kPpCap];
+    float ph[kPpCap];
+    int lo[32];
+    int pre[32];
+    // the group's FP64 state, read where needed instead of held in registers for the whole walk:
+    // box low/high corners, centre, largest target softening, smallest aold
+    double lo_x, lo_y, lo_z, hi_x, hi_y, hi_z, c_x, c_y, c_z, emax, amin;
+};
 
+template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT>
+__global__ void __launch_bounds__(kMaxWarps * 32, TPL == 1 ? 3 : 2)
+walk_kernel(const WalkArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
     const int gw = blockIdx.x * (blockDim.x >> 5) + w;
     int* __restrict__ stk = A.stack + (size_t)gw * A.stack_cap;
-    float4* __restrict__ pm = s_pm[w];
-    float* __restrict__ hs = s_h[w];
+    WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[w];
+    float4* __restrict__ pn = S.pn;
+    float4* __restrict__ pp = S.pp;
+    float* __restrict__ ph = S.ph;
 
     unsigned long long c_nodes = 0, c_multi = 0, c_pairs = 0, c_zero = 0, c_flush = 0;
     int c_maxtop = 0;
@@ -174,7 +186,7 @@ walk_kernel(const WalkArgs A) {
         if (g >= A.n_groups) break;
         const int2 gr = A.groups[g];
         const int t0 = gr.x, nt = gr.y - gr.x;
-        const int nk = (TPL > 1 && nt > 32) ? 2 : 1;  // warp-uniform
+        const int nk = TPL > 1 ? min(TPL, (nt + 31) >> 5) : 1;  // targets per lane in use (warp-uniform)
 
         // ---- targets: lane l holds targets l and l+32 --------------------------------------
         double px[TPL], py[TPL], pz[TPL], ps[TPL];
@@ -201,7 +213,13 @@ walk_kernel(const WalkArgs A) {
         hx = wmax(hx); hy = wmax(hy); hz = wmax(hz);
         emax = wmax(emax);
         if (A.aold) amin = wmin(amin);
-        const double gcx = 0.5 * (lx + hx), gcy = 0.5 * (ly + hy), gcz = 0.5 * (lz + hz);
+        if (lane == 0) {
+            S.lo_x = lx; S.lo_y = ly; S.lo_z = lz; S.hi_x = hx; S.hi_y = hy; S.hi_z = hz;
+            S.c_x = 0.5 * (lx + hx); S.c_y = 0.5 * (ly + hy); S.c_z = 0.5 * (lz + hz);
+            S.emax = emax; S.amin = amin;
+        }
+        __syncwarp();
+        const double gcx = S.c_x, gcy = S.c_y, gcz = S.c_z;
 
         // ---- evaluation lanes: lane = slice * NT + target ---------------------------------
         int lg = 5;
@@ -226,16 +244,55 @@ walk_kernel(const WalkArgs A) {
             pot[k] = 0.0;
         }
 
-        // ---- evaluate the list against the targets ----------------------------------------
-        auto flush = [&](int nlist) {
+        // ---- evaluate the lists against the targets ---------------------------------------
+        auto accumulate = [&](const float* ax_, const float* ay_, const float* az_, const float* ap_) {
+#pragma unroll
+            for (int k = 0; k < TPL; ++k) {
+                kahan_add(sx[k], cxk[k], ax_[k]);
+                kahan_add(sy[k], cyk[k], ay_[k]);
+                kahan_add(sz[k], czk[k], az_[k]);
+                if (WANT_POT) pot[k] += (double)ap_[k];
+            }
+            if (COUNT) c_flush += (lane == 0);
+        };
+        // Monopoles.  An accepted node passed the softening-overlap test, so every target of the
+        // group is farther than max(h_target, h_node) from it: the interaction is Newtonian.
+        auto flush_pn = [&](int n) {
+            __syncwarp();
+            float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
+#pragma unroll
+            for (int k = 0; k < TPL; ++k) ax_[k] = ay_[k] = az_[k] = ap_[k] = 0.0f;
+#pragma unroll 4
+            for (int j = slice; j < n; j += NS) {
+                const float4 e = pn[j];
+#pragma unroll
+                for (int k = 0; k < TPL; ++k) {
+                    if (k < nk) {
+                        const float dx = e.x - tx[k], dy = e.y - ty[k], dz = e.z - tz[k];
+                        const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-30f);
+                        const float ri = rsqrtf(r2);
+                        const float mri = e.w * ri;
+                        const float f = mri * (ri * ri);
+                        ax_[k] = fmaf(dx, f, ax_[k]);
+                        ay_[k] = fmaf(dy, f, ay_[k]);
+                        az_[k] = fmaf(dz, f, az_[k]);
+                        if (WANT_POT) ap_[k] -= mri;
+                    }
+                }
+            }
+            accumulate(ax_, ay_, az_, ap_);
+            __syncwarp();
+        };
+        // Particles: kernel of the larger softening; r^2 == 0 (the target itself) contributes 0.
+        auto flush_pp = [&](int n) {
             __syncwarp();
             float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
 #pragma unroll
             for (int k = 0; k < TPL; ++k) ax_[k] = ay_[k] = az_[k] = ap_[k] = 0.0f;
             unsigned zero = 0;
-            for (int j = slice; j < nlist; j += NS) {
-                const float4 e = pm[j];
-                const float hj = hs[j];
+            for (int j = slice; j < n; j += NS) {
+                const float4 e = pp[j];
+                const float hj = ph[j];
 #pragma unroll
                 for (int k = 0; k < TPL; ++k) {
                     if (k < nk) {
@@ -259,17 +316,8 @@ walk_kernel(const WalkArgs A) {
                     }
                 }
             }
-#pragma unroll
-            for (int k = 0; k < TPL; ++k) {
-                kahan_add(sx[k], cxk[k], ax_[k]);
-                kahan_add(sy[k], cyk[k], ay_[k]);
-                kahan_add(sz[k], czk[k], az_[k]);
-                if (WANT_POT) pot[k] += (double)ap_[k];
-            }
-            if (COUNT) {
-                c_zero += zero;
-                c_flush += (lane == 0);
-            }
+            accumulate(ax_, ay_, az_, ap_);
+            if (COUNT) c_zero += zero;
             __syncwarp();
         };
 
@@ -277,7 +325,7 @@ walk_kernel(const WalkArgs A) {
         int top = 1;
         if (lane == 0) stk[0] = 0;
         __syncwarp();
-        int nlist = 0;
+        int npn = 0, npp = 0;
         bool overflow = false;
         while (top > 0) {
             const int npop = min(top, 32);
@@ -291,13 +339,13 @@ walk_kernel(const WalkArgs A) {
             if (node >= 0) {
                 nd = load_node(A.nodes + node);
                 const bool leaf = nd.first < 0;
-                const double dx = fmax(0.0, fmax(lx - nd.cx, nd.cx - hx));
-                const double dy = fmax(0.0, fmax(ly - nd.cy, nd.cy - hy));
-                const double dz = fmax(0.0, fmax(lz - nd.cz, nd.cz - hz));
+                const double dx = fmax(0.0, fmax(S.lo_x - nd.cx, nd.cx - S.hi_x));
+                const double dy = fmax(0.0, fmax(S.lo_y - nd.cy, nd.cy - S.hi_y));
+                const double dz = fmax(0.0, fmax(S.lo_z - nd.cz, nd.cz - S.hi_z));
                 const double r2 = dx * dx + dy * dy + dz * dz;
                 bool open = true;
                 if (LEAF_ACCEPT || !leaf)
-                    open = open_node(r2, (double)nd.len, nd.s, nd.mass, (double)nd.soft, emax, amin,
+                    open = open_node(r2, (double)nd.len, nd.s, nd.mass, (double)nd.soft, S.emax, S.amin,
                                      A.theta2, dx, dy, dz);
                 if (!open) accept = true;
                 else if (leaf) expand = true;
@@ -319,14 +367,13 @@ walk_kernel(const WalkArgs A) {
             const unsigned am = __ballot_sync(kFull, accept);
             if (am) {
                 const int na = __popc(am);
-                if (nlist + na > kListCap) { flush(nlist); nlist = 0; }
+                if (npn + na > kPnCap) { flush_pn(npn); npn = 0; }
                 if (accept) {
-                    const int pos = nlist + __popc(am & lt_mask);
-                    pm[pos] = make_float4((float)(nd.cx - gcx), (float)(nd.cy - gcy),
-                                          (float)(nd.cz - gcz), (float)nd.mass);
-                    hs[pos] = nd.soft;
+                    const int pos = npn + __popc(am & lt_mask);
+                    pn[pos] = make_float4((float)(nd.cx - S.c_x), (float)(nd.cy - S.c_y),
+                                          (float)(nd.cz - S.c_z), (float)nd.mass);
                 }
-                nlist += na;
+                npn += na;
                 if (COUNT && lane == 0) c_multi += (unsigned long long)na * nt;
             }
 
@@ -336,31 +383,49 @@ walk_kernel(const WalkArgs A) {
                 const int cnt = expand ? nd.phi - nd.plo : 0;
                 const int inc2 = warp_incl_scan_i(cnt);
                 const int tot2 = __shfl_sync(kFull, inc2, 31);
-                s_lo[w][lane] = nd.plo;
-                s_pre[w][lane] = inc2 - cnt;
+                S.lo[lane] = nd.plo;
+                S.pre[lane] = inc2 - cnt;
                 __syncwarp();
                 if (COUNT && lane == 0) c_pairs += (unsigned long long)tot2 * nt;
-                int done = 0;
-                while (done < tot2) {
-                    if (nlist == kListCap) { flush(nlist); nlist = 0; }
-                    const int chunk = min(tot2 - done, kListCap - nlist);
-                    for (int j = lane; j < chunk; j += 32) {
-                        const int q = done + j;
+                // 32 particles at a time, one per lane.  A particle farther from the group box
+                // than max(largest target softening, its own) is Newtonian for every target
+                // (the reference's spline is exactly 1/r^3 for r >= h): it joins the monopole
+                // list.  The rest -- the group's own particles among them -- need the softened
+                // pair rule and go to the particle list.
+                for (int base = 0; base < tot2; base += 32) {
+                    const int q = base + lane;
+                    const bool live = q < tot2;
+                    double qx = 0, qy = 0, qz = 0;
+                    float qm = 0.0f, qh = 0.0f;
+                    bool far = false;
+                    if (live) {
                         // owner: the last lane whose exclusive prefix is <= q
                         int l = 0;
 #pragma unroll
                         for (int step = 16; step > 0; step >>= 1)
-                            if (s_pre[w][l + step] <= q) l += step;
-                        const int p = s_lo[w][l] + (q - s_pre[w][l]);
-                        double qx, qy, qz;
-                        float qm, qh;
-                        load_src(A.src + p, qx, qy, qz, qm, qh);
-                        pm[nlist + j] = make_float4((float)(qx - gcx), (float)(qy - gcy),
-                                                    (float)(qz - gcz), qm);
-                        hs[nlist + j] = qh;
+                            if (S.pre[l + step] <= q) l += step;
+                        load_src(A.src + S.lo[l] + (q - S.pre[l]), qx, qy, qz, qm, qh);
+                        const double ex = fmax(0.0, fmax(S.lo_x - qx, qx - S.hi_x));
+                        const double ey = fmax(0.0, fmax(S.lo_y - qy, qy - S.hi_y));
+                        const double ez = fmax(0.0, fmax(S.lo_z - qz, qz - S.hi_z));
+                        const double reach = fmax(S.emax, (double)qh);
+                        far = ex * ex + ey * ey + ez * ez > reach * reach;
                     }
-                    nlist += chunk;
-                    done += chunk;
+                    const unsigned fm = __ballot_sync(kFull, live && far);
+                    const unsigned nm = __ballot_sync(kFull, live && !far);
+                    const int nf = __popc(fm), nn = __popc(nm);
+                    if (npn + nf > kPnCap) { flush_pn(npn); npn = 0; }
+                    if (npp + nn > kPpCap) { flush_pp(npp); npp = 0; }
+                    const float4 e = make_float4((float)(qx - S.c_x), (float)(qy - S.c_y), (float)(qz - S.c_z), qm);
+                    if (live && far) {
+                        pn[npn + __popc(fm & lt_mask)] = e;
+                    } else if (live) {
+                        const int pos = npp + __popc(nm & lt_mask);
+                        pp[pos] = e;
+                        ph[pos] = qh;
+                    }
+                    npn += nf;
+                    npp += nn;
                     __syncwarp();
                 }
             }
@@ -369,7 +434,8 @@ walk_kernel(const WalkArgs A) {
             if (lane == 0) atomicExch(A.error, 1);
             continue;
         }
-        if (nlist > 0) flush(nlist);
+        if (npn > 0) flush_pn(npn);
+        if (npp > 0) flush_pp(npp);
 
         // ---- combine slices and write -------------------------------------------------------
 #pragma unroll
@@ -551,9 +617,27 @@ int64_t finish_groups(gt_context* ctx, const uint32_t* flag, int64_t n, int kmax
     return nc;
 }
 
+size_t walk_smem(int warps) { return (size_t)warps * sizeof(WarpSmem); }
+
+// Dynamic shared memory above 48 KB needs a per-kernel opt-in, done once per instantiation.
+template <int TPL, bool LA, bool POT, bool CNT>
+void prepare_walk() {
+    static bool done = false;
+    if (done) return;
+    check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)walk_smem(kMaxWarps)), "cudaFuncSetAttribute");
+    // the lists need 3 blocks x 55 KB per SM: ask for the largest shared-memory carveout
+    check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT>,
+                                    cudaFuncAttributePreferredSharedMemoryCarveout, 100),
+               "cudaFuncSetAttribute");
+    done = true;
+}
+
 template <int TPL, bool LA, bool POT, bool CNT>
 void launch_walk(gt_context* ctx, const WalkArgs& a, int blocks, int warps) {
-    walk_kernel<TPL, LA, POT, CNT><<<blocks, warps * 32, 0, ctx->stream>>>(a);
+    prepare_walk<TPL, LA, POT, CNT>();
+    walk_kernel<TPL, LA, POT, CNT><<<blocks, warps * 32, walk_smem(warps), ctx->stream>>>(a);
     check_launch(ctx, "walk_kernel");
 }
 
@@ -576,8 +660,10 @@ void dispatch(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la
 
 template <int TPL, bool LA, bool POT, bool CNT>
 int occupancy_blocks(int warps) {
+    prepare_walk<TPL, LA, POT, CNT>();
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<TPL, LA, POT, CNT>, warps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<TPL, LA, POT, CNT>, warps * 32,
+                                                  walk_smem(warps));
     return std::max(1, nb);
 }
 
@@ -597,10 +683,10 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     int param = rq.group_param;
     if (mode == GT_GROUP_NODE && param <= 0) param = 32;
     if (mode == GT_GROUP_BATCH && param <= 0) mode = GT_GROUP_LEAF;
+    // a warp holds up to 32, 64 or 128 targets (1, 2 or 4 per lane); longer groups are chunked
     int kmax = 32;
-    if (mode == GT_GROUP_NODE && param > 32) kmax = 64;
-    if (mode == GT_GROUP_BATCH && param > 32) kmax = 64;
-    const int tpl = kmax > 32 ? 2 : 1;
+    if ((mode == GT_GROUP_NODE || mode == GT_GROUP_BATCH) && param > 32) kmax = param > 64 ? 128 : 64;
+    const int tpl = kmax / 32;
 
     // ---- groups -------------------------------------------------------------------------------
     int2* groups = nullptr;
@@ -656,8 +742,10 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     if (tpl == 1)
         per_sm = rq.leaf_accept ? occupancy_blocks<1, true, false, false>(warps)
                                 : occupancy_blocks<1, false, false, false>(warps);
-    else
+    else if (tpl == 2)
         per_sm = occupancy_blocks<2, true, false, false>(warps);
+    else
+        per_sm = occupancy_blocks<4, true, false, false>(warps);
     const int64_t want_blocks = (ng + warps - 1) / warps;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want_blocks, (int64_t)per_sm * ctx->num_sms));
     int stack_cap = rq.stack_capacity > 0 ? rq.stack_capacity : 256 * std::max(1, t->n_levels) + 32;
@@ -691,7 +779,8 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         check_cuda(cudaMemsetAsync(ctr, 0, 96, st), "memset counters");
         check_cuda(cudaEventRecord(ctx->ev0, st), "event");
         if (tpl == 1) dispatch<1>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count);
-        else dispatch<2>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count);
+        else if (tpl == 2) dispatch<2>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count);
+        else dispatch<4>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count);
         check_cuda(cudaEventRecord(ctx->ev1, st), "event");
         if (!rq.count && attempt == 0 && rq.stack_capacity == 0) {
             // the default capacity is a proven bound: no read-back needed on the fast path

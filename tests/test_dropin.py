@@ -1,0 +1,38 @@
+"""Drop-in evidence: the reference's own tree consumers compiled UNCHANGED against the shmem:: shim.
+
+gizmo_shared_memory_b200/shim/Makefile compiles shmem/test_tree.cc and shmem/bench_treeforce.cc from
+the reference sources with gizmo_shared_memory_b200/shim/ on the include path instead of shmem/,
+linking libshmem_gt.so + libgt.so.  The binaries travel with the repository (git-ignored), so these
+tests run them when present and skip otherwise.
+"""
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BUILD = os.path.join(ROOT, "gizmo_shared_memory_b200", "shim", "_build")
+
+
+def binary(name):
+    p = os.path.join(BUILD, name)
+    if not os.path.exists(p):
+        pytest.skip(f"{name} not built (reference consumer sources unavailable at build time)")
+    return p
+
+
+@pytest.mark.gpu
+def test_reference_test_tree_runs_on_the_gpu_tree():
+    """shmem/test_tree.cc: tree vs brute force on a Plummer sphere at four opening angles."""
+    # line-buffered so the output before any failure survives
+    out = subprocess.run(["stdbuf", "-oL", binary("test_tree"), "200000"], capture_output=True,
+                         text=True, timeout=600, env=dict(os.environ, OMP_NUM_THREADS="4"))
+    assert out.returncode == 0, (out.returncode, out.stdout[-3000:], out.stderr[-2000:])
+    rows = re.findall(r"^\s+([0-9.]+)\s+([0-9.e+-]+)\s+([0-9.e+-]+)\s+([0-9.e+-]+)\s*$", out.stdout, re.M)
+    table = {float(t): (float(a), float(b), float(c)) for t, a, b, c in rows}
+    assert set(table) == {0.8, 0.5, 0.35, 0.2}, out.stdout
+    med = [table[t][0] for t in (0.8, 0.5, 0.35, 0.2)]
+    assert all(x > y for x, y in zip(med, med[1:])), med  # error falls with theta
+    assert table[0.5][0] < 2e-3 and table[0.2][0] < 2e-4, table
+    assert "tree:" in out.stdout and "nodes for 200000 particles" in out.stdout

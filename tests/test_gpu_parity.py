@@ -250,13 +250,24 @@ def node_group_starts(O, gmax):
     return np.concatenate([s, [O.nlive]])
 
 
-@pytest.mark.parametrize("gmax", [16, 32, 64])
+@pytest.mark.parametrize("batch", [32, 64, 128])
+def test_wide_windows_match_oracle(gpu_ctx, plummer_trees, batch):
+    """Fixed windows of 32/64/128 consecutive targets: 1, 2 and 4 targets per lane."""
+    T, O = plummer_trees
+    ob = O.order()[0]
+    aold = 0.0025 * np.ones(len(ob))
+    a = gpu_ctx.accel_grouped(T, ob, aold=aold, batch=batch)
+    b = O.accel_grouped(ob, 0.0, batch=batch, aold=aold)[:3]
+    check(a, b)
+
+
+@pytest.mark.parametrize("gmax", [16, 32, 64, 128])
 def test_node_groups_match_oracle(gpu_ctx, plummer_trees, gmax):
     T, O = plummer_trees
     ob = O.order()[0]
     starts = node_group_starts(O, gmax)
     # chunks of at most the kernel's capacity, as the library splits them
-    kmax = 32 if gmax <= 32 else 64
+    kmax = 32 if gmax <= 32 else (64 if gmax <= 64 else 128)
     ch = [starts[0]]
     for a, b in zip(starts[:-1], starts[1:]):
         x = a
