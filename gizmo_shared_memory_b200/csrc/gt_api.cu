@@ -121,8 +121,9 @@ void check_mem(int mem) {
 void free_tree_arrays(gt_tree* t) {
     void* ptrs[] = {t->src, t->ssoft, t->smass, t->order, t->rank, t->leaf_of, t->sleaf, t->skey,
                     t->nodes, t->parent, t->next, t->level, t->size, t->delta, t->nsoft, t->gc};
+    // tree arrays came from the stream-ordered pool: hand them back to it (callers have synchronised)
     for (void* p : ptrs)
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, 0);
     for (auto& c : t->group_cache)
         if (c.groups) cudaFree(c.groups);
     t->group_cache.clear();
@@ -262,6 +263,13 @@ int gt_context_create(int device, gt_context** out) {
         check_cuda(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
         ctx->num_sms = prop.multiProcessorCount;
         check_cuda(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        // keep freed tree memory in this process's default pool of the device, so a tree rebuilt
+        // every step reuses it instead of returning it to the driver at each synchronisation
+        cudaMemPool_t pool;
+        check_cuda(cudaDeviceGetDefaultMemPool(&pool, device), "cudaDeviceGetDefaultMemPool");
+        uint64_t keep = UINT64_MAX;
+        check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep),
+                   "cudaMemPoolSetAttribute");
         ctx->own_stream = true;
         check_cuda(cudaMallocHost(&ctx->pinned, 4096), "cudaMallocHost");
         check_cuda(cudaEventCreate(&ctx->ev0), "cudaEventCreate");
@@ -357,6 +365,8 @@ int gt_build(gt_context* ctx, int64_t n, const double* x, const double* y, const
         finish(ctx, true);
     });
     if (st != GT_OK) {
+        cudaStreamSynchronize(ctx->stream);  // queued build work may still use the arrays
+        cudaGetLastError();
         free_tree_arrays(t);
         delete t;
         return st;

@@ -397,13 +397,15 @@ __global__ void form_aold_kernel(const double* __restrict__ ax, const double* __
         aold[i] = alpha * sqrt(ax[i] * ax[i] + ay[i] * ay[i] + az[i] * az[i]) / G;
 }
 
+// Tree arrays come from the device's stream-ordered pool (the context keeps freed memory in the
+// pool), so rebuilding a tree every step does not pay cudaMalloc/cudaFree and their device syncs.
 template <typename T>
-T* dalloc(size_t count) {
+T* dalloc(size_t count, cudaStream_t stream) {
     void* p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, count * sizeof(T) + 16);
+    const cudaError_t e = cudaMallocAsync(&p, count * sizeof(T) + 16, stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        throw Fail{GT_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+        throw Fail{GT_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e)};
     }
     return (T*)p;
 }
@@ -419,12 +421,11 @@ void grow_nodes(gt_tree* t, int64_t need, cudaStream_t stream) {
     const int64_t cap = std::max<int64_t>(need, t->node_cap * 2);
     auto grow = [&](auto*& p, size_t per) {
         using T = std::remove_reference_t<decltype(*p)>;
-        T* q = dalloc<T>((size_t)cap * per);
+        T* q = dalloc<T>((size_t)cap * per, stream);
         if (p) {
             check_cuda(cudaMemcpyAsync(q, p, (size_t)t->node_cap * per * sizeof(T), cudaMemcpyDeviceToDevice,
                                        stream), "grow nodes");
-            check_cuda(cudaStreamSynchronize(stream), "sync");
-            cudaFree(p);
+            check_cuda(cudaFreeAsync(p, stream), "cudaFreeAsync");
         }
         p = q;
     };
@@ -487,14 +488,14 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
 
     // 4. particle arrays in tree order
     const int64_t nalloc = std::max<int64_t>(n, 1);
-    t->src = dalloc<SrcP>(nalloc);
-    t->ssoft = dalloc<double>(nalloc);
-    t->smass = dalloc<double>(nalloc);
-    t->order = dalloc<uint32_t>(nalloc);
-    t->rank = dalloc<uint32_t>(nalloc);
-    t->leaf_of = dalloc<int>(nalloc);
-    t->sleaf = dalloc<int>(nalloc);
-    t->skey = dalloc<uint64_t>(nalloc);
+    t->src = dalloc<SrcP>(nalloc, st);
+    t->ssoft = dalloc<double>(nalloc, st);
+    t->smass = dalloc<double>(nalloc, st);
+    t->order = dalloc<uint32_t>(nalloc, st);
+    t->rank = dalloc<uint32_t>(nalloc, st);
+    t->leaf_of = dalloc<int>(nalloc, st);
+    t->sleaf = dalloc<int>(nalloc, st);
+    t->skey = dalloc<uint64_t>(nalloc, st);
     if (n > 0) {
         gather_kernel<<<grid_for(ctx, n), kBlk, 0, st>>>(x, y, z, m, soft, idx, n, t->src, t->ssoft,
                                                          t->smass, t->order, t->rank, t->leaf_of, t->sleaf);
@@ -514,9 +515,11 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
         const int64_t a = t->lvl_off[L], b = t->lvl_off[L + 1];
         const int64_t cnt_l = b - a;
         if (cnt_l <= 0) break;
-        int* bnd = (int*)scratch(ctx, kSlotNodeTmp0, (size_t)cnt_l * 9 * 4);
-        uint32_t* nch = (uint32_t*)scratch(ctx, kSlotNodeTmp1, (size_t)cnt_l * 4);
-        uint32_t* coff = (uint32_t*)scratch(ctx, kSlotNodeTmp2, (size_t)cnt_l * 4);
+        // sized for the widest level possible (node_cap), so the workspace never regrows mid-build
+        const int64_t wmax = std::max<int64_t>(cnt_l, t->node_cap);
+        int* bnd = (int*)scratch(ctx, kSlotNodeTmp0, (size_t)wmax * 9 * 4);
+        uint32_t* nch = (uint32_t*)scratch(ctx, kSlotNodeTmp1, (size_t)wmax * 4);
+        uint32_t* coff = (uint32_t*)scratch(ctx, kSlotNodeTmp2, (size_t)wmax * 4);
         split_kernel<<<div_up(cnt_l, kBlk), kBlk, 0, st>>>(t->nodes, t->skey, a, b, L, o.max_level,
                                                            o.leaf_max, bnd, nch);
         check_launch(ctx, "split_kernel");

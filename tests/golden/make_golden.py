@@ -111,6 +111,17 @@ def main():
     out["colloc_orderbuf"] = obq
     out["colloc_ax"], out["colloc_ay"], out["colloc_az"] = ex, ey, ez
 
+    # ---- the reference's own test program (shmem/test_tree.cc), its printed accuracy table ------
+    import re
+    import subprocess
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "test_tree")
+    txt = subprocess.run([exe, "20000"], capture_output=True, text=True, check=True,
+                         env=dict(os.environ, OMP_NUM_THREADS="4")).stdout
+    acc = txt.split("=== build")[0]
+    rows = re.findall(r"^\s+([0-9.]+)\s+([0-9.e+-]+)\s+([0-9.e+-]+)\s+([0-9.e+-]+)\s*$", acc, re.M)
+    out["test_tree_table"] = np.array([[float(v) for v in r] for r in rows])
+
     path = os.path.join(HERE, "golden.npz")
     np.savez_compressed(path, **out)
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path) / 1024:.0f} KiB")
