@@ -67,7 +67,7 @@ class TreeInfo(C.Structure):
 class WalkStats(C.Structure):
     _fields_ = [("groups", C.c_int64), ("nodes_visited", C.c_int64), ("multipole", C.c_int64),
                 ("pairs", C.c_int64), ("targets", C.c_int64), ("max_stack", C.c_int64),
-                ("list_flushes", C.c_int64), ("walk_ms", C.c_double)]
+                ("list_flushes", C.c_int64), ("traversal_steps", C.c_int64), ("walk_ms", C.c_double)]
 
 
 class NodeArrays(C.Structure):

@@ -52,7 +52,7 @@ struct WalkArgs {
     int* stack;
     int stack_cap;
     unsigned int* next_group;   // dynamic group counter
-    unsigned long long* stats;  // [nodes, multipole, pairs_structural, zero_r2, flushes, max_stack]
+    unsigned long long* stats;  // [nodes, multipole, pairs_structural, zero_r2, flushes, max_stack, steps]
     int* error;                 // 1: stack overflow
 };
 
@@ -176,7 +176,7 @@ walk_kernel(const WalkArgs A) {
     float4* __restrict__ pp = S.pp;
     float* __restrict__ ph = S.ph;
 
-    unsigned long long c_nodes = 0, c_multi = 0, c_pairs = 0, c_zero = 0, c_flush = 0;
+    unsigned long long c_nodes = 0, c_multi = 0, c_pairs = 0, c_zero = 0, c_flush = 0, c_steps = 0;
     int c_maxtop = 0;
 
     for (;;) {
@@ -351,7 +351,7 @@ walk_kernel(const WalkArgs A) {
                 else if (leaf) expand = true;
                 else push = true;
             }
-            if (COUNT && lane == 0) c_nodes += npop;
+            if (COUNT && lane == 0) { c_nodes += npop; ++c_steps; }
 
             // children of opened interior nodes
             const int nch = push ? nd.nchild : 0;
@@ -470,6 +470,7 @@ walk_kernel(const WalkArgs A) {
             atomicAdd(&A.stats[2], c_pairs);
             atomicAdd(&A.stats[4], c_flush);
             atomicMax(&A.stats[5], (unsigned long long)c_maxtop);
+            atomicAdd(&A.stats[6], c_steps);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) c_zero += __shfl_xor_sync(kFull, c_zero, o);
@@ -796,6 +797,7 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
             ctx->stats.pairs = (int64_t)h[2] - (int64_t)h[3];
             ctx->stats.list_flushes = (int64_t)h[4];
             ctx->stats.max_stack = (int64_t)h[5];
+            ctx->stats.traversal_steps = (int64_t)h[6];
             break;
         }
         if (attempt == 2) throw Fail{GT_ERR_OVERFLOW, "walk stack overflow"};

@@ -112,6 +112,7 @@ typedef struct {
 typedef struct {
     int64_t groups, nodes_visited, multipole, pairs, targets;
     int64_t max_stack, list_flushes;
+    int64_t traversal_steps; /* warp steps of the traversal (each pops up to 32 nodes) */
     double walk_ms;    /* device time of the walk kernel(s) of the last walk call */
 } gt_walk_stats;
 
