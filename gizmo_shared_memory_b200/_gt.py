@@ -35,7 +35,8 @@ EXPORTS = [
     "gt_context_set_stream", "gt_synchronize", "gt_launch_count", "gt_build", "gt_tree_free",
     "gt_tree_info_get", "gt_tree_download", "gt_tree_keys", "gt_accel_grouped", "gt_accel",
     "gt_potential", "gt_walk_stats_get", "gt_form_aold", "gt_direct", "gt_peano_keys",
-    "gt_measure_peaks", "gt_direct_noalloc",
+    "gt_measure_peaks", "gt_direct_noalloc", "gt_mac_train_options_default", "gt_mac_sample",
+    "gt_mac_train", "gt_mac_predict", "gt_mac_gradient",
 ]
 
 
@@ -55,7 +56,17 @@ class WalkOptions(C.Structure):
     _fields_ = [("group_mode", C.c_int), ("group_max", C.c_int), ("mac", C.c_int),
                 ("out_order", C.c_int), ("async_", C.c_int), ("count", C.c_int),
                 ("block_warps", C.c_int), ("list_capacity", C.c_int),
-                ("stack_capacity", C.c_int), ("dtype_out_f32", C.c_int)]
+                ("stack_capacity", C.c_int), ("dtype_out_f32", C.c_int),
+                ("mac_model", C.c_void_p), ("mac_kappa", C.c_double), ("mac_band", C.c_double * 2)]
+
+
+class MacTrainOptions(C.Structure):
+    _fields_ = [("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_double), ("tau", C.c_double),
+                ("seed", C.c_uint64)]
+
+
+MAC_MODEL_FLOATS = 2 * 8 + 32 * 8 + 32 + 32 * 32 + 32 + 32 + 1
+MAC_PARAM_FLOATS = MAC_MODEL_FLOATS - 16
 
 
 class TreeInfo(C.Structure):
@@ -117,13 +128,15 @@ def load_library(path: str = LIB_PATH):
     L.gt_peano_keys.argtypes = [vp, i64, vp, vp, vp, vp, d, C.c_int, C.c_int, vp, vp, vp, vp]
     L.gt_measure_peaks.argtypes = [vp, C.POINTER(d), C.POINTER(d)]
     L.gt_direct_noalloc.argtypes = [i64, vp, vp, vp, vp, vp, i64, vp, d, C.c_int, vp, vp, vp, vp, vp]
+    L.gt_mac_train_options_default.argtypes = [C.POINTER(MacTrainOptions)]
+    L.gt_mac_sample.argtypes = [vp, vp, vp, d, C.c_int, i64, d, d, i64, C.c_int, vp, vp, vp,
+                                C.POINTER(i64)]
+    L.gt_mac_train.argtypes = [vp, i64, vp, vp, C.POINTER(MacTrainOptions), C.c_int, vp, C.POINTER(d)]
+    L.gt_mac_predict.argtypes = [vp, vp, i64, vp, C.c_int, vp]
+    L.gt_mac_gradient.argtypes = [vp, vp, i64, vp, vp, d, C.c_int, vp, C.POINTER(d)]
+    void_fns = ("gt_build_options_default", "gt_walk_options_default", "gt_mac_train_options_default")
     for name in EXPORTS:
-        fn = getattr(L, name)
-        if fn.restype is C.c_int or fn.restype is None and name not in (
-                "gt_build_options_default", "gt_walk_options_default"):
-            fn.restype = C.c_int
-    L.gt_build_options_default.restype = None
-    L.gt_walk_options_default.restype = None
+        getattr(L, name).restype = None if name in void_fns else C.c_int
     L.gt_last_error.restype = C.c_char_p
     L.gt_status_string.restype = C.c_char_p
     _LIB = L
@@ -277,7 +290,8 @@ class Context:
 
     # ---- walks -----------------------------------------------------------------------------
     def _walk_opts(self, group_mode=GT_GROUP_LEAF, group_max=32, out_order=GT_OUT_TARGETS,
-                   count=False, block_warps=0, async_=False, mac=GT_MAC_PLAIN):
+                   count=False, block_warps=0, async_=False, mac=GT_MAC_PLAIN, mac_model=None,
+                   mac_kappa=1.0, mac_band=(0.0, 0.0)):
         o = WalkOptions()
         load_library().gt_walk_options_default(C.byref(o))
         o.group_mode = group_mode
@@ -287,7 +301,55 @@ class Context:
         o.block_warps = block_warps
         o.async_ = int(async_)
         o.mac = mac
+        if mac_model is not None:
+            self._mac_keep = np.ascontiguousarray(mac_model, np.float32)
+            o.mac = GT_MAC_LEARNED
+            o.mac_model = self._mac_keep.ctypes.data
+            o.mac_kappa = mac_kappa
+            o.mac_band[0], o.mac_band[1] = mac_band
         return o
+
+    # ---- learned criterion ---------------------------------------------------------------------
+    def mac_sample(self, tree: "Tree", amag, alpha, window=32, stride=1, rho_lo=0.02, rho_hi=50.0,
+                   capacity=1 << 20):
+        """Training samples from a plain walk; amag = |a| per live particle in tree order."""
+        amag = np.ascontiguousarray(amag.cpu().numpy() if _is_dev(amag) else amag, np.float64)
+        f = np.empty((capacity, 8), np.float32)
+        lab = np.empty(capacity, np.float32)
+        rho = np.empty(capacity, np.float32)
+        ns = C.c_int64()
+        self._check(load_library().gt_mac_sample(self.h, tree.h, _ptr(amag), alpha, window, stride,
+                                                 rho_lo, rho_hi, capacity, GT_MEM_HOST, _ptr(f),
+                                                 _ptr(lab), _ptr(rho), C.byref(ns)))
+        k = min(ns.value, capacity)
+        return f[:k], lab[:k], rho[:k], ns.value
+
+    def mac_train(self, features, labels, epochs=30, batch=4096, lr=2e-3, tau=0.9, seed=1):
+        o = MacTrainOptions(epochs=epochs, batch=batch, lr=lr, tau=tau, seed=seed)
+        X = np.ascontiguousarray(features, np.float32)
+        Y = np.ascontiguousarray(labels, np.float32)
+        model = np.empty(MAC_MODEL_FLOATS, np.float32)
+        loss = C.c_double()
+        self._check(load_library().gt_mac_train(self.h, len(Y), _ptr(X), _ptr(Y), C.byref(o),
+                                                GT_MEM_HOST, _ptr(model), C.byref(loss)))
+        return model, loss.value
+
+    def mac_predict(self, model, features):
+        X = np.ascontiguousarray(features, np.float32)
+        m = np.ascontiguousarray(model, np.float32)
+        out = np.empty(max(len(X), 1), np.float32)
+        self._check(load_library().gt_mac_predict(self.h, _ptr(m), len(X), _ptr(X), GT_MEM_HOST, _ptr(out)))
+        return out[:len(X)]
+
+    def mac_gradient(self, model, features, labels, tau=0.9):
+        X = np.ascontiguousarray(features, np.float32)
+        Y = np.ascontiguousarray(labels, np.float32)
+        m = np.ascontiguousarray(model, np.float32)
+        g = np.empty(MAC_PARAM_FLOATS, np.float32)
+        loss = C.c_double()
+        self._check(load_library().gt_mac_gradient(self.h, _ptr(m), len(Y), _ptr(X), _ptr(Y), tau,
+                                                   GT_MEM_HOST, _ptr(g), C.byref(loss)))
+        return g, loss.value
 
     @staticmethod
     def _targets(targets):

@@ -120,7 +120,8 @@ void check_mem(int mem) {
 
 void free_tree_arrays(gt_tree* t) {
     void* ptrs[] = {t->src, t->ssoft, t->smass, t->order, t->rank, t->leaf_of, t->sleaf, t->skey,
-                    t->nodes, t->parent, t->next, t->level, t->size, t->delta, t->nsoft, t->gc};
+                    t->nodes, t->parent, t->next, t->level, t->size, t->delta, t->nsoft, t->gc,
+                    t->nq2};
     // tree arrays came from the stream-ordered pool: hand them back to it (callers have synchronised)
     for (void* p : ptrs)
         if (p) cudaFreeAsync(p, 0);
@@ -151,7 +152,10 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     gt_walk_options_default(&o);
     if (opt) o = *opt;
     if (o.mac != GT_MAC_PLAIN && o.mac != GT_MAC_LEARNED) throw Fail{GT_ERR_INVALID, "unknown mac"};
-    if (o.mac == GT_MAC_LEARNED) throw Fail{GT_ERR_UNSUPPORTED, "no learned criterion is loaded"};
+    if (o.mac == GT_MAC_LEARNED && !o.mac_model)
+        throw Fail{GT_ERR_INVALID, "GT_MAC_LEARNED needs gt_walk_options.mac_model"};
+    if (o.mac == GT_MAC_LEARNED && !leaf_accept)
+        throw Fail{GT_ERR_UNSUPPORTED, "the learned criterion applies to the grouped walk"};
     if (o.dtype_out_f32 != 0) throw Fail{GT_ERR_INVALID, "dtype_out_f32 is reserved"};
     if (o.out_order == GT_OUT_ORIGINAL && targets) throw Fail{GT_ERR_INVALID, "GT_OUT_ORIGINAL needs targets == NULL"};
     DeviceGuard dg(ctx->device);
@@ -179,6 +183,13 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     rq.want_phi = phi != nullptr;
     rq.out_original = all && o.out_order == GT_OUT_ORIGINAL;
     rq.mac = o.mac;
+    if (o.mac == GT_MAC_LEARNED) {
+        // the model is a small host array: stage it with the call
+        rq.mac_model = stage_in(ctx, kSlotIn2, o.mac_model, (int64_t)GT_MAC_MODEL_FLOATS, GT_MEM_HOST);
+        rq.mac_kappa = o.mac_kappa;
+        rq.mac_band_lo = o.mac_band[0];
+        rq.mac_band_hi = o.mac_band[1];
+    }
     rq.count = o.count != 0;
     rq.block_warps = o.block_warps;
     rq.list_capacity = o.list_capacity;
@@ -586,6 +597,93 @@ int gt_peano_keys(gt_context* ctx, int64_t n, const double* x, const double* y, 
         copy_out(ctx, ph_lo, (const uint64_t*)b, n, mem);
         copy_out(ctx, mo_hi, (const uint64_t*)c, n, mem);
         copy_out(ctx, mo_lo, (const uint64_t*)d, n, mem);
+        finish(ctx, true);
+    });
+}
+
+void gt_mac_train_options_default(gt_mac_train_options* o) {
+    if (!o) return;
+    o->epochs = 30;
+    o->batch = 4096;
+    o->lr = 2e-3;
+    o->tau = 0.9;
+    o->seed = 1;
+}
+
+int gt_mac_sample(gt_context* ctx, const gt_tree* tree, const double* amag, double alpha, int window,
+                  int64_t group_stride, double rho_lo, double rho_hi, int64_t capacity, int mem,
+                  float* features, float* labels, float* rho, int64_t* n_samples) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (!tree || !amag || !n_samples || capacity < 0) throw Fail{GT_ERR_INVALID, "bad arguments"};
+        if (window < 1 || window > 32) throw Fail{GT_ERR_INVALID, "window must be in [1, 32]"};
+        if (!(alpha > 0) || !(rho_hi >= rho_lo)) throw Fail{GT_ERR_INVALID, "bad alpha or rho window"};
+        if (capacity > 0 && (!features || !labels || !rho)) throw Fail{GT_ERR_INVALID, "null output"};
+        DeviceGuard dg(ctx->device);
+        const double* da = stage_in(ctx, kSlotIn0, amag, tree->n_live, mem);
+        float* f = out_buf(ctx, kSlotOut0, features, capacity * GT_MAC_FEATURES, mem);
+        float* l = out_buf(ctx, kSlotOut1, labels, capacity, mem);
+        float* r = out_buf(ctx, kSlotOut2, rho, capacity, mem);
+        run_mac_sample(ctx, tree, da, alpha, window, group_stride, rho_lo, rho_hi, capacity, f, l, r,
+                       n_samples);
+        const int64_t got = std::min(*n_samples, capacity);
+        copy_out(ctx, features, (const float*)f, got * GT_MAC_FEATURES, mem);
+        copy_out(ctx, labels, (const float*)l, got, mem);
+        copy_out(ctx, rho, (const float*)r, got, mem);
+        finish(ctx, true);
+    });
+}
+
+int gt_mac_train(gt_context* ctx, int64_t n, const float* features, const float* labels,
+                 const gt_mac_train_options* opt, int mem, float* model, double* loss) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (n <= 0 || !features || !labels || !model) throw Fail{GT_ERR_INVALID, "bad arguments"};
+        gt_mac_train_options o;
+        gt_mac_train_options_default(&o);
+        if (opt) o = *opt;
+        if (o.epochs < 1 || o.batch < 1 || !(o.lr > 0) || !(o.tau > 0 && o.tau < 1))
+            throw Fail{GT_ERR_INVALID, "bad training options"};
+        DeviceGuard dg(ctx->device);
+        const float* X = stage_in(ctx, kSlotIn0, features, n * GT_MAC_FEATURES, mem);
+        const float* Y = stage_in(ctx, kSlotIn1, labels, n, mem);
+        run_mac_train(ctx, n, X, Y, o, model, loss);
+    });
+}
+
+int gt_mac_predict(gt_context* ctx, const float* model, int64_t n, const float* features, int mem,
+                   float* out) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (!model || n < 0 || (n > 0 && (!features || !out))) throw Fail{GT_ERR_INVALID, "bad arguments"};
+        DeviceGuard dg(ctx->device);
+        const float* dm = stage_in(ctx, kSlotIn2, model, (int64_t)GT_MAC_MODEL_FLOATS, GT_MEM_HOST);
+        const float* X = stage_in(ctx, kSlotIn0, features, n * GT_MAC_FEATURES, mem);
+        float* o = out_buf(ctx, kSlotOut0, out, n, mem);
+        run_mac_predict(ctx, dm, n, X, o);
+        copy_out(ctx, out, (const float*)o, n, mem);
+        finish(ctx, true);
+    });
+}
+
+int gt_mac_gradient(gt_context* ctx, const float* model, int64_t n, const float* features,
+                    const float* labels, double tau, int mem, float* grad, double* loss) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (!model || n <= 0 || n > (int64_t)INT32_MAX || !features || !labels || !grad)
+            throw Fail{GT_ERR_INVALID, "bad arguments"};
+        if (!(tau > 0 && tau < 1)) throw Fail{GT_ERR_INVALID, "tau must be in (0, 1)"};
+        DeviceGuard dg(ctx->device);
+        const float* dm = stage_in(ctx, kSlotIn2, model, (int64_t)GT_MAC_MODEL_FLOATS, GT_MEM_HOST);
+        const float* X = stage_in(ctx, kSlotIn0, features, n * GT_MAC_FEATURES, mem);
+        const float* Y = stage_in(ctx, kSlotIn1, labels, n, mem);
+        float* g = out_buf(ctx, kSlotOut0, grad, (int64_t)GT_MAC_PARAM_FLOATS, mem);
+        run_mac_grad(ctx, dm, X, Y, nullptr, 0, (int)n, tau, g, loss);
+        copy_out(ctx, grad, (const float*)g, (int64_t)GT_MAC_PARAM_FLOATS, mem);
         finish(ctx, true);
     });
 }

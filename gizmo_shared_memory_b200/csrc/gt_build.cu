@@ -300,14 +300,15 @@ __global__ void moments_kernel(GNode* __restrict__ nodes, const SrcP* __restrict
                                const uint32_t* __restrict__ order, int64_t a, int64_t b,
                                const double* __restrict__ size, const double* __restrict__ gc,
                                double* __restrict__ delta, double* __restrict__ nsoft,
-                               int* __restrict__ leaf_of, int* __restrict__ sleaf, int nodelta) {
+                               float* __restrict__ nq2, int* __restrict__ leaf_of,
+                               int* __restrict__ sleaf, int nodelta) {
     const int lane = threadIdx.x & 31;
     const int64_t i = a + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     if (i >= b) return;
     const int first = nodes[i].first, nc = nodes[i].nchild;
+    const int lo = nodes[i].plo, hi = nodes[i].phi;
     double M = 0, mx = 0, my = 0, mz = 0, smax = 0;
     if (first < 0) {
-        const int lo = nodes[i].plo, hi = nodes[i].phi;
         for (int j = lo + lane; j < hi; j += 32) {
             const double mj = smass[j];
             const SrcP s = src[j];
@@ -323,6 +324,26 @@ __global__ void moments_kernel(GNode* __restrict__ nodes, const SrcP* __restrict
     }
     M = warp_sum_d(M); mx = warp_sum_d(mx); my = warp_sum_d(my); mz = warp_sum_d(mz);
     smax = warp_max_d(smax);
+    // Second mass moment about the COM, sum m |x - com|^2: from the particles in a leaf, from the
+    // children by the parallel-axis rule otherwise.  Not used by the plain criterion; it is an input
+    // of the learned one (the quadrupole error a monopole makes scales with it).
+    {
+        const double ox = M > 0 ? mx / M : 0.0, oy = M > 0 ? my / M : 0.0, oz = M > 0 ? mz / M : 0.0;
+        double q = 0;
+        if (first < 0) {
+            for (int j = lo + lane; j < hi; j += 32) {
+                const SrcP s = src[j];
+                const double ex = s.x - ox, ey = s.y - oy, ez = s.z - oz;
+                q += smass[j] * (ex * ex + ey * ey + ez * ez);
+            }
+        } else if (lane < nc) {
+            const GNode& ch = nodes[first + lane];
+            const double ex = ch.cx - ox, ey = ch.cy - oy, ez = ch.cz - oz;
+            q = (double)nq2[first + lane] + ch.mass * (ex * ex + ey * ey + ez * ez);
+        }
+        q = warp_sum_d(q);
+        if (lane == 0) nq2[i] = (float)q;
+    }
     if (lane == 0) {
         if (M > 0) { mx /= M; my /= M; mz /= M; }
         const double dx = mx - gc[3 * i], dy = my - gc[3 * i + 1], dz = mz - gc[3 * i + 2];
@@ -430,7 +451,7 @@ void grow_nodes(gt_tree* t, int64_t need, cudaStream_t stream) {
         p = q;
     };
     grow(t->nodes, 1); grow(t->parent, 1); grow(t->next, 1); grow(t->level, 1);
-    grow(t->size, 1); grow(t->delta, 1); grow(t->nsoft, 1); grow(t->gc, 3);
+    grow(t->size, 1); grow(t->delta, 1); grow(t->nsoft, 1); grow(t->gc, 3); grow(t->nq2, 1);
     t->node_cap = cap;
 }
 
@@ -546,7 +567,7 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
         const int64_t warps = b - a;
         moments_kernel<<<div_up(warps * 32, kBlk), kBlk, 0, st>>>(
             t->nodes, t->src, t->smass, t->ssoft, t->order, a, b, t->size, t->gc, t->delta,
-            t->nsoft, t->leaf_of, t->sleaf, o.nodelta);
+            t->nsoft, t->nq2, t->leaf_of, t->sleaf, o.nodelta);
         check_launch(ctx, "moments_kernel");
     }
     check_cuda(cudaEventRecord(ev[5], st), "event");

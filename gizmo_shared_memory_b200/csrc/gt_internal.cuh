@@ -97,6 +97,7 @@ struct gt_tree {
     double* size = nullptr;      // node_cap
     double* delta = nullptr;     // node_cap
     double* nsoft = nullptr;     // node_cap, FP64 max softening
+    float* nq2 = nullptr;        // node_cap, second mass moment about the COM (learned criterion)
     double* gc = nullptr;        // node_cap * 3, geometric centres
     // cached all-active group lists, keyed by (mode, param)
     struct GroupCache {
@@ -158,6 +159,8 @@ struct WalkRequest {
     bool want_acc = true, want_phi = false;
     bool out_original = false;
     int mac = GT_MAC_PLAIN;
+    const float* mac_model = nullptr;   // device copy of the network (GT_MAC_LEARNED)
+    double mac_kappa = 1.0, mac_band_lo = 0.0, mac_band_hi = 0.0;
     bool count = false;
     int block_warps = 0, list_capacity = 0, stack_capacity = 0;
     double *ax = nullptr, *ay = nullptr, *az = nullptr, *phi = nullptr;  // device outputs
@@ -173,6 +176,16 @@ void run_direct(gt_context* ctx, int64_t n, const double* x, const double* y, co
 void run_peano_keys(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
                     const double corner[3], double len, int bits, uint64_t* ph_hi, uint64_t* ph_lo,
                     uint64_t* mo_hi, uint64_t* mo_lo);
+// Learned criterion (gt_mac.cu); all arrays are device pointers.
+void run_mac_sample(gt_context* ctx, const gt_tree* t, const double* amag, double alpha, int window,
+                    int64_t stride, double rho_lo, double rho_hi, int64_t cap, float* feat,
+                    float* label, float* rho, int64_t* n_samples);
+void run_mac_train(gt_context* ctx, int64_t n, const float* X, const float* Y,
+                   const gt_mac_train_options& o, float* model_host, double* loss);
+void run_mac_grad(gt_context* ctx, const float* dmodel, const float* X, const float* Y, const int* perm,
+                  int64_t off, int B, double tau, float* dgrad, double* loss);
+void run_mac_predict(gt_context* ctx, const float* dmodel, int64_t n, const float* X, float* out);
+
 // Peak probe (gt_peak.cu)
 void run_peaks(gt_context* ctx, double* fp32_tflops, double* fp64_tflops);
 void run_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay,

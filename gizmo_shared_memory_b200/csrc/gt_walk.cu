@@ -29,6 +29,7 @@
 #include <cstring>
 
 #include "gt_internal.cuh"
+#include "gt_mac.cuh"
 
 namespace gt {
 namespace {
@@ -54,6 +55,10 @@ struct WalkArgs {
     unsigned int* next_group;   // dynamic group counter
     unsigned long long* stats;  // [nodes, multipole, pairs_structural, zero_r2, flushes, max_stack, steps]
     int* error;                 // 1: stack overflow
+    // learned criterion
+    const float* mac_model;     // GT_MAC_MODEL_FLOATS on the device
+    const float* nq2;           // node second moments
+    double mac_band_lo, mac_band_hi, mac_log_kappa;
 };
 
 __device__ __forceinline__ int warp_incl_scan_i(int v) {
@@ -163,7 +168,7 @@ struct WarpSmem {
     double lo_x, lo_y, lo_z, hi_x, hi_y, hi_z, c_x, c_y, c_z, emax, amin;
 };
 
-template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT>
+template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT, bool MAC>
 __global__ void __launch_bounds__(kMaxWarps * 32, TPL == 1 ? 3 : 2)
 walk_kernel(const WalkArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -172,6 +177,12 @@ walk_kernel(const WalkArgs A) {
     const int gw = blockIdx.x * (blockDim.x >> 5) + w;
     int* __restrict__ stk = A.stack + (size_t)gw * A.stack_cap;
     WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[w];
+    // the learned criterion's network, one copy per block after the warps' lists
+    float* __restrict__ mac_w = reinterpret_cast<float*>(smem_raw + sizeof(WarpSmem) * (blockDim.x >> 5));
+    if (MAC) {
+        for (int i = threadIdx.x; i < kMacModel; i += blockDim.x) mac_w[i] = A.mac_model[i];
+        __syncthreads();
+    }
     float4* __restrict__ pn = S.pn;
     float4* __restrict__ pp = S.pp;
     float* __restrict__ ph = S.ph;
@@ -344,9 +355,45 @@ walk_kernel(const WalkArgs A) {
                 const double dz = fmax(0.0, fmax(S.lo_z - nd.cz, nd.cz - S.hi_z));
                 const double r2 = dx * dx + dy * dy + dz * dz;
                 bool open = true;
-                if (LEAF_ACCEPT || !leaf)
-                    open = open_node(r2, (double)nd.len, nd.s, nd.mass, (double)nd.soft, S.emax, S.amin,
-                                     A.theta2, dx, dy, dz);
+                if (!MAC) {
+                    if (LEAF_ACCEPT || !leaf)
+                        open = open_node(r2, (double)nd.len, nd.s, nd.mass, (double)nd.soft, S.emax, S.amin,
+                                         A.theta2, dx, dy, dz);
+                } else if (LEAF_ACCEPT || !leaf) {
+                    // learned criterion: the softening-overlap, inside-node and Barnes-Hut arms
+                    // stay; the relative arm's estimate M L^2 / r^4 is corrected by the network
+                    // inside the band of rho where it may change the decision
+                    const double len = (double)nd.len;
+                    const double rt = S.emax + 0.6 * len, rn = (double)nd.soft + 0.6 * len;
+                    const double lim = 0.6 * len;
+                    const bool hard = (r2 < rt * rt) | (r2 < rn * rn) |
+                                      ((A.theta2 > 0.0) & (nd.s * nd.s >= A.theta2 * r2)) |
+                                      ((dx < lim) & (dy < lim) & (dz < lim));
+                    const double aold = S.amin;
+                    if (hard) {
+                        open = true;
+                    } else if (!(aold > 0)) {
+                        open = A.theta2 <= 0.0;
+                    } else {
+                        const double rho = nd.mass * len * len / (r2 * r2 * aold);
+                        if (rho <= A.mac_band_lo) {
+                            open = false;
+                        } else if (rho > A.mac_band_hi) {
+                            open = true;
+                        } else {
+                            const double ex = fmax(fabs(nd.cx - S.lo_x), fabs(nd.cx - S.hi_x));
+                            const double ey = fmax(fabs(nd.cy - S.lo_y), fabs(nd.cy - S.hi_y));
+                            const double ez = fmax(fabs(nd.cz - S.lo_z), fabs(nd.cz - S.hi_z));
+                            const double gx = S.hi_x - S.lo_x, gy = S.hi_y - S.lo_y, gz = S.hi_z - S.lo_z;
+                            float f[kMacIn];
+                            mac_features(r2, rho, len, nd.s, nd.mass, (double)A.nq2[node], (double)nd.soft,
+                                         S.emax, nd.phi - nd.plo, ex * ex + ey * ey + ez * ez,
+                                         gx * gx + gy * gy + gz * gz, f);
+                            const float c = mac_forward(mac_w, f);
+                            open = f[4] + c > (float)A.mac_log_kappa;  // f[4] = log10(rho)
+                        }
+                    }
+                }
                 if (!open) accept = true;
                 else if (leaf) expand = true;
                 else push = true;
@@ -618,53 +665,60 @@ int64_t finish_groups(gt_context* ctx, const uint32_t* flag, int64_t n, int kmax
     return nc;
 }
 
-size_t walk_smem(int warps) { return (size_t)warps * sizeof(WarpSmem); }
+size_t walk_smem(int warps, bool mac) {
+    return (size_t)warps * sizeof(WarpSmem) + (mac ? kMacModel * sizeof(float) : 0);
+}
 
 // Dynamic shared memory above 48 KB needs a per-kernel opt-in, done once per instantiation.
-template <int TPL, bool LA, bool POT, bool CNT>
+template <int TPL, bool LA, bool POT, bool CNT, bool MAC>
 void prepare_walk() {
     static bool done = false;
     if (done) return;
-    check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT>,
+    check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT, MAC>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)walk_smem(kMaxWarps)), "cudaFuncSetAttribute");
+                                    (int)walk_smem(kMaxWarps, MAC)), "cudaFuncSetAttribute");
     // the lists need 3 blocks x 55 KB per SM: ask for the largest shared-memory carveout
-    check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT>,
+    check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT, MAC>,
                                     cudaFuncAttributePreferredSharedMemoryCarveout, 100),
                "cudaFuncSetAttribute");
     done = true;
 }
 
-template <int TPL, bool LA, bool POT, bool CNT>
+template <int TPL, bool LA, bool POT, bool CNT, bool MAC>
 void launch_walk(gt_context* ctx, const WalkArgs& a, int blocks, int warps) {
-    prepare_walk<TPL, LA, POT, CNT>();
-    walk_kernel<TPL, LA, POT, CNT><<<blocks, warps * 32, walk_smem(warps), ctx->stream>>>(a);
+    prepare_walk<TPL, LA, POT, CNT, MAC>();
+    walk_kernel<TPL, LA, POT, CNT, MAC><<<blocks, warps * 32, walk_smem(warps, MAC), ctx->stream>>>(a);
     check_launch(ctx, "walk_kernel");
 }
 
-template <int TPL, bool LA, bool POT>
+template <int TPL, bool LA, bool POT, bool MAC>
 void dispatch_count(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool cnt) {
-    if (cnt) launch_walk<TPL, LA, POT, true>(ctx, a, blocks, warps);
-    else launch_walk<TPL, LA, POT, false>(ctx, a, blocks, warps);
+    if (cnt) launch_walk<TPL, LA, POT, true, MAC>(ctx, a, blocks, warps);
+    else launch_walk<TPL, LA, POT, false, MAC>(ctx, a, blocks, warps);
 }
 
+// The learned criterion is a grouped-walk option (leaves offered to the criterion).
 template <int TPL>
-void dispatch(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la, bool pot, bool cnt) {
-    if (la) {
-        if (pot) dispatch_count<TPL, true, true>(ctx, a, blocks, warps, cnt);
-        else dispatch_count<TPL, true, false>(ctx, a, blocks, warps, cnt);
+void dispatch(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la, bool pot, bool cnt,
+              bool mac) {
+    if (mac) {
+        if (pot) dispatch_count<TPL, true, true, true>(ctx, a, blocks, warps, cnt);
+        else dispatch_count<TPL, true, false, true>(ctx, a, blocks, warps, cnt);
+    } else if (la) {
+        if (pot) dispatch_count<TPL, true, true, false>(ctx, a, blocks, warps, cnt);
+        else dispatch_count<TPL, true, false, false>(ctx, a, blocks, warps, cnt);
     } else {
-        if (pot) dispatch_count<TPL, false, true>(ctx, a, blocks, warps, cnt);
-        else dispatch_count<TPL, false, false>(ctx, a, blocks, warps, cnt);
+        if (pot) dispatch_count<TPL, false, true, false>(ctx, a, blocks, warps, cnt);
+        else dispatch_count<TPL, false, false, false>(ctx, a, blocks, warps, cnt);
     }
 }
 
-template <int TPL, bool LA, bool POT, bool CNT>
+template <int TPL, bool LA, bool POT, bool CNT, bool MAC>
 int occupancy_blocks(int warps) {
-    prepare_walk<TPL, LA, POT, CNT>();
+    prepare_walk<TPL, LA, POT, CNT, MAC>();
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<TPL, LA, POT, CNT>, warps * 32,
-                                                  walk_smem(warps));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<TPL, LA, POT, CNT, MAC>, warps * 32,
+                                                  walk_smem(warps, MAC));
     return std::max(1, nb);
 }
 
@@ -739,14 +793,18 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
 
     // ---- launch -------------------------------------------------------------------------------
     const int warps = (rq.block_warps > 0 && rq.block_warps <= kMaxWarps) ? rq.block_warps : kMaxWarps;
+    const bool mac = rq.mac == GT_MAC_LEARNED;
     int per_sm;
     if (tpl == 1)
-        per_sm = rq.leaf_accept ? occupancy_blocks<1, true, false, false>(warps)
-                                : occupancy_blocks<1, false, false, false>(warps);
+        per_sm = mac ? occupancy_blocks<1, true, false, false, true>(warps)
+                     : (rq.leaf_accept ? occupancy_blocks<1, true, false, false, false>(warps)
+                                       : occupancy_blocks<1, false, false, false, false>(warps));
     else if (tpl == 2)
-        per_sm = occupancy_blocks<2, true, false, false>(warps);
+        per_sm = mac ? occupancy_blocks<2, true, false, false, true>(warps)
+                     : occupancy_blocks<2, true, false, false, false>(warps);
     else
-        per_sm = occupancy_blocks<4, true, false, false>(warps);
+        per_sm = mac ? occupancy_blocks<4, true, false, false, true>(warps)
+                     : occupancy_blocks<4, true, false, false, false>(warps);
     const int64_t want_blocks = (ng + warps - 1) / warps;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want_blocks, (int64_t)per_sm * ctx->num_sms));
     int stack_cap = rq.stack_capacity > 0 ? rq.stack_capacity : 256 * std::max(1, t->n_levels) + 32;
@@ -773,15 +831,22 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     a.stats = ctr;
     a.error = (int*)(ctr + 9);
     const bool want_pot = rq.want_phi && rq.phi;
+    a.mac_model = rq.mac_model;
+    a.nq2 = t->nq2;
+    a.mac_band_lo = rq.mac_band_lo;
+    a.mac_band_hi = rq.mac_band_hi;
+    a.mac_log_kappa = rq.mac_kappa > 0 ? std::log10(rq.mac_kappa) : -300.0;
+    if (mac && (!rq.mac_model || !rq.leaf_accept))
+        throw Fail{GT_ERR_INVALID, "the learned criterion needs a model and a grouped walk"};
 
     for (int attempt = 0; attempt < 3; ++attempt) {
         a.stack = (int*)scratch(ctx, kSlotStack, (size_t)total_warps * stack_cap * 4);
         a.stack_cap = stack_cap;
         check_cuda(cudaMemsetAsync(ctr, 0, 96, st), "memset counters");
         check_cuda(cudaEventRecord(ctx->ev0, st), "event");
-        if (tpl == 1) dispatch<1>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count);
-        else if (tpl == 2) dispatch<2>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count);
-        else dispatch<4>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count);
+        if (tpl == 1) dispatch<1>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, mac);
+        else if (tpl == 2) dispatch<2>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, mac);
+        else dispatch<4>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, mac);
         check_cuda(cudaEventRecord(ctx->ev1, st), "event");
         if (!rq.count && attempt == 0 && rq.stack_capacity == 0) {
             // the default capacity is a proven bound: no read-back needed on the fast path

@@ -75,6 +75,14 @@ enum { GT_OUT_TARGETS = 0, GT_OUT_ORIGINAL = 1 };
 typedef struct gt_context gt_context;
 typedef struct gt_tree gt_tree;
 
+/* Learned multipole-acceptance criterion: an MLP of 8 geometric features, 2 hidden layers of 32
+ * (ReLU), one output, FP32.  A model is a flat host array of GT_MAC_MODEL_FLOATS floats:
+ * feature mean[8], 1/std[8], W1[32][8], b1[32], W2[32][32], b2[32], W3[32], b3. */
+#define GT_MAC_FEATURES 8
+#define GT_MAC_HIDDEN 32
+#define GT_MAC_MODEL_FLOATS (2 * 8 + 32 * 8 + 32 + 32 * 32 + 32 + 32 + 1)
+#define GT_MAC_PARAM_FLOATS (GT_MAC_MODEL_FLOATS - 2 * 8)
+
 typedef struct {
     int key_mode;             /* GT_KEY_PEANO (default) or GT_KEY_MORTON */
     int leaf_max;             /* particles per leaf, default 16 (shmem/tree.h:357) */
@@ -96,7 +104,22 @@ typedef struct {
     int list_capacity;   /* interaction-list entries per warp; 0 = default */
     int stack_capacity;  /* node-stack entries per warp; 0 = default (always sufficient) */
     int dtype_out_f32;   /* reserved, must be 0 */
+    /* GT_MAC_LEARNED: the model (host array of GT_MAC_MODEL_FLOATS), the acceptance threshold
+     * kappa (accept when rho * 10^prediction <= kappa, rho = M L^2 / (r^4 aold)), and the band of
+     * rho outside which the network is not consulted: rho <= mac_band[0] accepts, rho >
+     * mac_band[1] opens.  The softening-overlap and inside-node arms always apply. */
+    const float* mac_model;
+    double mac_kappa;
+    double mac_band[2];
 } gt_walk_options;
+
+typedef struct {
+    int epochs;      /* passes over the samples (default 30) */
+    int batch;       /* samples per step (default 4096) */
+    double lr;       /* Adam step size (default 2e-3) */
+    double tau;      /* quantile of the pinball loss (default 0.9: a conservative upper quantile) */
+    uint64_t seed;   /* initialisation and shuffling (default 1) */
+} gt_mac_train_options;
 
 typedef struct {
     int64_t n;          /* particles passed to gt_build */
@@ -233,6 +256,33 @@ GT_API int gt_direct_noalloc(int64_t n, const double* x, const double* y, const 
 GT_API int gt_peano_keys(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
                   const double corner[3], double len, int bits, int mem, uint64_t* ph_hi,
                   uint64_t* ph_lo, uint64_t* morton_hi, uint64_t* morton_lo);
+
+/* ---- learned opening criterion ------------------------------------------------------------- */
+/* No reference counterpart: the learned criterion is new.  Training data come from the walk and
+ * an exact per-node sum; the network is trained and evaluated by this library's own kernels. */
+GT_API void gt_mac_train_options_default(gt_mac_train_options* opt);
+/* Walk the tree with the plain relative criterion (aold = alpha * amag, amag = |a| per live
+ * particle in tree order) over every `group_stride`-th window of `window` consecutive targets;
+ * for each node the walk tests that is not opened by the softening or inside-node arms and whose
+ * ratio rho lies in [rho_lo, rho_hi], record its 8 features, rho, and the label
+ * log10(worst over the window of |a_monopole - a_exact| / |a_target|) - log10(alpha * rho),
+ * the exact value summing the node's particles with the walk's pair rule.  At most `capacity`
+ * samples are written; *n_samples receives how many were found (possibly more). */
+GT_API int gt_mac_sample(gt_context* ctx, const gt_tree* tree, const double* amag, double alpha,
+                         int window, int64_t group_stride, double rho_lo, double rho_hi,
+                         int64_t capacity, int mem, float* features, float* labels, float* rho,
+                         int64_t* n_samples);
+/* Train a model on (features, labels) with the pinball loss at quantile tau, Adam, on the GPU.
+ * model (host, GT_MAC_MODEL_FLOATS) receives the trained network; loss the final epoch's mean. */
+GT_API int gt_mac_train(gt_context* ctx, int64_t n, const float* features, const float* labels,
+                        const gt_mac_train_options* opt, int mem, float* model, double* loss);
+/* Network output for n feature rows. */
+GT_API int gt_mac_predict(gt_context* ctx, const float* model, int64_t n, const float* features,
+                          int mem, float* out);
+/* Mean pinball loss at quantile tau and its gradient with respect to the GT_MAC_PARAM_FLOATS
+ * trainable parameters (model without the normalisation), for checking the training kernels. */
+GT_API int gt_mac_gradient(gt_context* ctx, const float* model, int64_t n, const float* features,
+                           const float* labels, double tau, int mem, float* grad, double* loss);
 
 /* ---- measurement --------------------------------------------------------------------------- */
 /* FP32 and FP64 FMA throughput of this device's CUDA cores in TFLOP/s (independent FMA chains on

@@ -389,7 +389,7 @@ def test_errors_leave_context_usable(gpu_ctx, plummer):
     assert e.value.status == 1  # GT_ERR_INVALID
     with pytest.raises(g.GTError) as e:
         gpu_ctx.accel_grouped(T, None, theta=0.7, mac=g.GT_MAC_LEARNED)
-    assert e.value.status == 4  # GT_ERR_UNSUPPORTED (no network loaded)
+    assert e.value.status == 1  # GT_ERR_INVALID: the learned criterion without a model
     a = gpu_ctx.accel_grouped(T, None, theta=0.7)
     assert np.isfinite(a[0]).all()
 
