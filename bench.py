@@ -395,13 +395,136 @@ def run_gpu_arm(args):
         dist.destroy_process_group()
 
 
+def run_batch_arm(args):
+    """256 independent Plummer systems of uneven N in one forest: one build, the launch
+    configuration picked by the autotuner under a sampled p99 target, then the all-active walk of
+    every system captured once as a CUDA graph and replayed.  Also times the same systems walked
+    one launch per system, to show what batching buys."""
+    import torch
+
+    import gizmo_shared_memory_b200 as g
+    from gizmo_shared_memory_b200 import ics
+
+    torch.cuda.set_device(0)
+    alpha = args.alpha if args.alpha is not None else 0.005
+    P, off, meta = ics.plummer_batch(seed=4)
+    S = len(off) - 1
+    n = len(P["m"])
+    dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
+    ctx = g.Context(0, torch_stream=True)
+    peak32, _ = ctx.measure_peaks()
+    F = ctx.build(dev, offsets=off)
+    info = F.info()
+    nl = info["n_live"]
+    out = tuple(torch.empty(nl, dtype=torch.float64, device="cuda") for _ in range(3))
+    ctx.accel_grouped(F, None, theta=0.7, outs=out + (None,), group_mode=g.GT_GROUP_BATCH, batch=32)
+    aold = ctx.form_aold(*out, alpha)
+    # per-system FP64 direct-sum sample, 16 targets per system (4096 in all)
+    rng = np.random.default_rng(77)
+    sample, ref = [], [[], [], []]
+    for s in range(S):
+        loc = np.sort(rng.choice(int(off[s + 1] - off[s]), 16, replace=False)).astype(np.uint32)
+        d = ctx.direct({k: v[off[s]:off[s + 1]] for k, v in P.items()}, loc, want_phi=False)
+        sample.append(loc + np.uint32(off[s]))
+        for k in range(3):
+            ref[k].append(d[k])
+    sample = np.concatenate(sample)
+    ref = [np.concatenate(r) for r in ref]
+    t0 = time.perf_counter()
+    best, entries = ctx.autotune(F, aold, sample=sample, ref=ref, p99_max=5e-3, reps=3)
+    t_tune = time.perf_counter() - t0
+    kw = {k: v for k, v in best.items()}
+    plan = ctx.plan(F, aold, out, **kw)
+    ctx.accel_grouped(F, None, aold=aold, outs=out + (None,), count=True, **kw)
+    st = ctx.stats()
+    inter = st["multipole"] + st["pairs"]
+    for _ in range(max(args.warmup, 3)):
+        plan.launch()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = ctx.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.launch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = ctx.launches() - l0
+    clocks = sampler.stop()
+    t_step = e0.elapsed_time(e1) / 1e3 / args.steps
+    full = ctx.accel_grouped(F, None, aold=aold, out_order=g.GT_OUT_ORIGINAL, **kw)
+    got = np.stack([f.cpu().numpy()[sample] for f in full])
+    err = relerr(list(got), ref)
+    per_sys = err.reshape(S, 16)
+    # one launch per system, same systems, same criterion and options
+    trees, aolds, outs = [], [], []
+    ob = F.download(nodes=False)["orderbuf"]
+    live, _ = F.systems()
+    aold_h = aold.cpu().numpy()
+    for s in range(S):
+        Ts = ctx.build({k: v[int(off[s]):int(off[s + 1])] for k, v in dev.items()})
+        trees.append(Ts)
+        # the forest's aold, restricted to system s, is already in this tree's order
+        aolds.append(torch.as_tensor(aold_h[live[s]:live[s + 1]], device="cuda"))
+        m = int(live[s + 1] - live[s])
+        outs.append(tuple(torch.empty(m, dtype=torch.float64, device="cuda") for _ in range(3)))
+    assert np.array_equal(ob[live[0]:live[1]] - off[0], trees[0].download(nodes=False)["orderbuf"])
+
+    def separate():
+        for s in range(S):
+            ctx.accel_grouped(trees[s], None, aold=aolds[s], outs=outs[s] + (None,), async_=True, **kw)
+
+    separate()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        separate()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_sep = e0.elapsed_time(e1) / 1e3 / args.steps
+    achieved = FLOPS_PER_INTERACTION * inter / t_step / 1e12
+    line = {
+        "metric": METRIC, "value": nl / t_step, "unit": "particles/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Plummer spheres)",
+        "config": {"workload": "plummer_batch_256", "n": n, "systems": S,
+                   "n_per_system": [int(x) for x in meta["n"]],
+                   "description": "256 Plummer spheres, N log-uniform in [1024, 262144] rescaled to ~2^24 "
+                                  "in all, a log-uniform in [0.5, 2], softening 0.01 a",
+                   "criterion": f"plain relative criterion alpha={alpha} after a theta=0.7 bootstrap walk",
+                   "launch": "forest build (one pass for all systems), autotuned options, all-active walk "
+                             "of every system captured as one CUDA graph (gt_plan) and replayed",
+                   "autotuned": {k: v for k, v in best.items() if k != "mac_model"},
+                   "l2": f"inputs larger than L2: {n * 32 / 2**20:.0f} MiB of particles"},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
+                     "frac": achieved / peak32, "traffic": None, "kernel": "walk_kernel"},
+        "gpu_launches": launches, "clocks": clocks,
+        "error": {"vs": "FP64 direct sum per system, 16 targets each", "sample": int(len(sample)),
+                  "median": float(np.median(err)), "p99": float(np.quantile(err, 0.99)),
+                  "worst_system_p99": float(np.max(np.quantile(per_sys, 0.99, axis=1)))},
+        "interactions_per_particle": inter / nl, "interactions_per_s": inter / t_step,
+        "one_launch_per_system": {"ms_per_step": 1e3 * t_sep, "value": nl / t_sep,
+                                  "speedup_of_batching": t_sep / t_step},
+        "autotune": {"seconds": t_tune, "candidates": len(entries),
+                     "entries": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in e.items()}
+                                 for e in entries]},
+        "build_ms": info["build_ms"],
+    }
+    print(json.dumps(line), flush=True)
+    plan.free()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="clustered_16m")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["plummer_batch_256"], default="clustered_16m",
+                    help="plummer_batch_256: the batched many-system case (forest + autotuner + graph)")
     ap.add_argument("--alpha", type=float, default=None)
     ap.add_argument("--group", choices=["leaf", "node", "batch"], default="batch",
                     help="leaf: accel_grouped batch 0; batch: windows of --group-max consecutive "
@@ -417,6 +540,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload == "plummer_batch_256":
+        run_batch_arm(args)
     else:
         run_gpu_arm(args)
 

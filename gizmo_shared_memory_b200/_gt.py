@@ -20,7 +20,8 @@ GT_OK = 0
 GT_MEM_HOST, GT_MEM_DEVICE = 0, 1
 GT_KEY_PEANO, GT_KEY_MORTON = 0, 1
 GT_GROUP_LEAF, GT_GROUP_BATCH, GT_GROUP_NODE, GT_GROUP_SINGLE = 0, 1, 2, 3
-GT_MAC_PLAIN, GT_MAC_LEARNED = 0, 1
+GT_MAC_PLAIN, GT_MAC_LEARNED, GT_MAC_NODE = 0, 1, 2
+GT_MAC_NODE_FEATURES = (1 << 1) | (1 << 2) | (1 << 5)
 GT_DIRECT_FP64, GT_DIRECT_FP32 = 0, 1
 GT_OUT_TARGETS, GT_OUT_ORIGINAL = 0, 1
 
@@ -36,7 +37,8 @@ EXPORTS = [
     "gt_tree_info_get", "gt_tree_download", "gt_tree_keys", "gt_accel_grouped", "gt_accel",
     "gt_potential", "gt_walk_stats_get", "gt_form_aold", "gt_direct", "gt_peano_keys",
     "gt_measure_peaks", "gt_direct_noalloc", "gt_mac_train_options_default", "gt_mac_sample",
-    "gt_mac_train", "gt_mac_predict", "gt_mac_gradient",
+    "gt_mac_train", "gt_mac_predict", "gt_mac_gradient", "gt_build_systems", "gt_tree_systems",
+    "gt_plan_create", "gt_plan_launch", "gt_plan_destroy", "gt_tune_options_default", "gt_autotune",
 ]
 
 
@@ -60,9 +62,22 @@ class WalkOptions(C.Structure):
                 ("mac_model", C.c_void_p), ("mac_kappa", C.c_double), ("mac_band", C.c_double * 2)]
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [("group_mode", C.c_int), ("group_size", C.c_int), ("block_warps", C.c_int),
+                ("list_capacity", C.c_int), ("mac", C.c_int), ("mac_kappa", C.c_double),
+                ("ms", C.c_double), ("p99", C.c_double), ("median", C.c_double), ("accepted", C.c_int)]
+
+
+class TuneOptions(C.Structure):
+    _fields_ = [("reps", C.c_int), ("p99_max", C.c_double), ("n_sample", C.c_int64),
+                ("sample", C.c_void_p), ("ref_ax", C.c_void_p), ("ref_ay", C.c_void_p),
+                ("ref_az", C.c_void_p), ("mac_model", C.c_void_p), ("n_kappa", C.c_int),
+                ("kappa", C.c_void_p), ("mac_band", C.c_double * 2), ("mac_mode", C.c_int)]
+
+
 class MacTrainOptions(C.Structure):
     _fields_ = [("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_double), ("tau", C.c_double),
-                ("seed", C.c_uint64)]
+                ("seed", C.c_uint64), ("feature_mask", C.c_uint32)]
 
 
 MAC_MODEL_FLOATS = 2 * 8 + 32 * 8 + 32 + 32 * 32 + 32 + 32 + 1
@@ -72,7 +87,7 @@ MAC_PARAM_FLOATS = MAC_MODEL_FLOATS - 16
 class TreeInfo(C.Structure):
     _fields_ = [("n", C.c_int64), ("n_live", C.c_int64), ("n_nodes", C.c_int64),
                 ("n_levels", C.c_int32), ("root", C.c_int32), ("center", C.c_double * 3),
-                ("side", C.c_double), ("build_ms", C.c_double * 7)]
+                ("side", C.c_double), ("build_ms", C.c_double * 7), ("n_systems", C.c_int64)]
 
 
 class WalkStats(C.Structure):
@@ -114,6 +129,9 @@ def load_library(path: str = LIB_PATH):
     L.gt_synchronize.argtypes = [vp]
     L.gt_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.gt_build.argtypes = [vp, i64, vp, vp, vp, vp, vp, C.c_int, C.POINTER(BuildOptions), C.POINTER(vp)]
+    L.gt_build_systems.argtypes = [vp, i64, C.c_int32, vp, vp, vp, vp, vp, vp, C.c_int,
+                                   C.POINTER(BuildOptions), C.POINTER(vp)]
+    L.gt_tree_systems.argtypes = [vp, vp, vp]
     L.gt_tree_free.argtypes = [vp]
     L.gt_tree_info_get.argtypes = [vp, C.POINTER(TreeInfo)]
     L.gt_tree_download.argtypes = [vp, vp, vp, vp, vp, C.POINTER(NodeArrays)]
@@ -134,7 +152,15 @@ def load_library(path: str = LIB_PATH):
     L.gt_mac_train.argtypes = [vp, i64, vp, vp, C.POINTER(MacTrainOptions), C.c_int, vp, C.POINTER(d)]
     L.gt_mac_predict.argtypes = [vp, vp, i64, vp, C.c_int, vp]
     L.gt_mac_gradient.argtypes = [vp, vp, i64, vp, vp, d, C.c_int, vp, C.POINTER(d)]
-    void_fns = ("gt_build_options_default", "gt_walk_options_default", "gt_mac_train_options_default")
+    L.gt_plan_create.argtypes = [vp, vp, vp, d, d, C.c_int, C.POINTER(WalkOptions), vp, vp, vp, vp,
+                                 C.POINTER(vp)]
+    L.gt_plan_launch.argtypes = [vp]
+    L.gt_plan_destroy.argtypes = [vp]
+    L.gt_tune_options_default.argtypes = [C.POINTER(TuneOptions)]
+    L.gt_autotune.argtypes = [vp, vp, vp, C.c_int, d, d, C.POINTER(TuneOptions), C.POINTER(WalkOptions),
+                              C.POINTER(C.c_int), vp, C.c_int, C.POINTER(C.c_int)]
+    void_fns = ("gt_build_options_default", "gt_walk_options_default", "gt_mac_train_options_default",
+                "gt_tune_options_default")
     for name in EXPORTS:
         getattr(L, name).restype = None if name in void_fns else C.c_int
     L.gt_last_error.restype = C.c_char_p
@@ -172,11 +198,19 @@ class Tree:
         except Exception:
             pass
 
+    def systems(self):
+        """(live tree-position offsets [n_systems + 1], root cells [n_systems, 4]: centre, side)."""
+        S = self.info()["n_systems"]
+        off = np.zeros(S + 1, np.int64)
+        roots = np.zeros((S, 4), np.float64)
+        self.ctx._check(load_library().gt_tree_systems(self.h, off.ctypes.data, roots.ctypes.data))
+        return off, roots
+
     def info(self) -> dict:
         inf = TreeInfo()
         self.ctx._check(load_library().gt_tree_info_get(self.h, C.byref(inf)))
         return {"n": inf.n, "n_live": inf.n_live, "n_nodes": inf.n_nodes, "n_levels": inf.n_levels,
-                "center": tuple(inf.center), "side": inf.side,
+                "center": tuple(inf.center), "side": inf.side, "n_systems": inf.n_systems,
                 "build_ms": dict(zip(("bbox", "keys", "sort", "structure", "moments", "pack", "total"),
                                      list(inf.build_ms)))}
 
@@ -212,6 +246,29 @@ class Tree:
         k = np.empty(max(nl, 1), np.uint64)
         self.ctx._check(load_library().gt_tree_keys(self.ctx.h, self.h, k.ctypes.data))
         return k[:nl]
+
+
+class Plan:
+    """A captured all-active walk (gt_plan_create); launch() replays it asynchronously."""
+
+    def __init__(self, ctx: "Context", handle, keep):
+        self.ctx = ctx
+        self.h = handle
+        self._keep = keep  # the device arrays the graph points at
+
+    def launch(self):
+        self.ctx._check(load_library().gt_plan_launch(self.h))
+
+    def free(self):
+        if self.h:
+            load_library().gt_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 class Context:
@@ -265,7 +322,9 @@ class Context:
 
     # ---- build -----------------------------------------------------------------------------
     def build(self, P, key_mode=GT_KEY_PEANO, randomize_seed=-1, nodelta=False, leaf_max=16,
-              max_level=20, validate=True, shift=(0.0, 0.0, 0.0)) -> Tree:
+              max_level=20, validate=True, shift=(0.0, 0.0, 0.0), offsets=None) -> Tree:
+        """Build a tree; with `offsets` (n_systems + 1 input offsets) a forest of independent
+        systems in one pass (gt_build_systems)."""
         o = BuildOptions()
         load_library().gt_build_options_default(C.byref(o))
         o.key_mode = key_mode
@@ -283,14 +342,20 @@ class Context:
             x, y, z, m = (np.ascontiguousarray(a, np.float64) for a in (x, y, z, m))
             soft = None if soft is None else np.ascontiguousarray(soft, np.float64)
         h = C.c_void_p()
-        self._check(load_library().gt_build(self.h, len(m), _ptr(x), _ptr(y), _ptr(z), _ptr(m),
-                                             _ptr(soft), GT_MEM_DEVICE if dev else GT_MEM_HOST,
-                                             C.byref(o), C.byref(h)))
+        mem = GT_MEM_DEVICE if dev else GT_MEM_HOST
+        if offsets is None:
+            self._check(load_library().gt_build(self.h, len(m), _ptr(x), _ptr(y), _ptr(z), _ptr(m),
+                                                 _ptr(soft), mem, C.byref(o), C.byref(h)))
+        else:
+            off = np.ascontiguousarray(offsets, np.int64)
+            self._check(load_library().gt_build_systems(self.h, len(m), len(off) - 1, off.ctypes.data,
+                                                         _ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(soft),
+                                                         mem, C.byref(o), C.byref(h)))
         return Tree(self, h)
 
     # ---- walks -----------------------------------------------------------------------------
     def _walk_opts(self, group_mode=GT_GROUP_LEAF, group_max=32, out_order=GT_OUT_TARGETS,
-                   count=False, block_warps=0, async_=False, mac=GT_MAC_PLAIN, mac_model=None,
+                   count=False, block_warps=0, async_=False, mac=GT_MAC_PLAIN, mac_model=None, list_capacity=0,
                    mac_kappa=1.0, mac_band=(0.0, 0.0)):
         o = WalkOptions()
         load_library().gt_walk_options_default(C.byref(o))
@@ -299,15 +364,68 @@ class Context:
         o.out_order = out_order
         o.count = int(count)
         o.block_warps = block_warps
+        o.list_capacity = list_capacity
         o.async_ = int(async_)
         o.mac = mac
         if mac_model is not None:
             self._mac_keep = np.ascontiguousarray(mac_model, np.float32)
-            o.mac = GT_MAC_LEARNED
+            o.mac = mac if mac != GT_MAC_PLAIN else GT_MAC_LEARNED
             o.mac_model = self._mac_keep.ctypes.data
             o.mac_kappa = mac_kappa
             o.mac_band[0], o.mac_band[1] = mac_band
         return o
+
+    # ---- plans and the autotuner ----------------------------------------------------------------
+    def plan(self, tree: Tree, aold, outs, theta=0.0, G=1.0, batch=0, phi=None, **opts) -> Plan:
+        """Capture the all-active walk into a graph; aold and outs = (ax, ay, az) are device
+        tensors (n_live, tree order) whose contents may change between launches."""
+        o = self._walk_opts(**opts)
+        h = C.c_void_p()
+        self._check(load_library().gt_plan_create(self.h, tree.h, _ptr(aold), theta, G, batch, C.byref(o),
+                                                  _ptr(outs[0]), _ptr(outs[1]), _ptr(outs[2]), _ptr(phi),
+                                                  C.byref(h)))
+        return Plan(self, h, (tree, aold, outs, phi, o))
+
+    def autotune(self, tree: Tree, aold, theta=0.0, G=1.0, sample=None, ref=None, p99_max=5e-3, reps=3,
+                 mac_model=None, kappas=(), mac_band=(0.0, 0.0), mac=GT_MAC_LEARNED, max_entries=64):
+        """Measure candidate launch configurations (gt_autotune).  Returns (walk options for
+        accel_grouped as a dict, entries as a list of dicts)."""
+        o = TuneOptions()
+        L = load_library()
+        L.gt_tune_options_default(C.byref(o))
+        o.reps = reps
+        o.p99_max = p99_max
+        keep = []
+        if sample is not None:
+            smp = np.ascontiguousarray(sample, np.uint32)
+            rx, ry, rz = (np.ascontiguousarray(r, np.float64) for r in ref)
+            keep += [smp, rx, ry, rz]
+            o.n_sample = len(smp)
+            o.sample, o.ref_ax, o.ref_ay, o.ref_az = smp.ctypes.data, rx.ctypes.data, ry.ctypes.data, rz.ctypes.data
+        if mac_model is not None:
+            mm = np.ascontiguousarray(mac_model, np.float32)
+            kp = np.ascontiguousarray(kappas, np.float64)
+            keep += [mm, kp]
+            o.mac_model = mm.ctypes.data
+            o.n_kappa = len(kp)
+            o.kappa = kp.ctypes.data
+            o.mac_band[0], o.mac_band[1] = mac_band
+            o.mac_mode = mac
+        dev = _is_dev(aold)
+        if not dev:
+            aold = np.ascontiguousarray(aold, np.float64)
+        best = WalkOptions()
+        bb = C.c_int()
+        ents = (TuneEntry * max_entries)()
+        ne = C.c_int()
+        self._check(L.gt_autotune(self.h, tree.h, _ptr(aold), GT_MEM_DEVICE if dev else GT_MEM_HOST, theta, G,
+                                  C.byref(o), C.byref(best), C.byref(bb), ents, max_entries, C.byref(ne)))
+        entries = [{k: getattr(e, k) for k, _ in TuneEntry._fields_} for e in ents[:ne.value]]
+        opts = {"group_mode": best.group_mode, "group_max": best.group_max, "block_warps": best.block_warps,
+                "list_capacity": best.list_capacity, "batch": bb.value}
+        if best.mac != GT_MAC_PLAIN:
+            opts.update(mac=best.mac, mac_model=mac_model, mac_kappa=best.mac_kappa, mac_band=tuple(mac_band))
+        return opts, entries
 
     # ---- learned criterion ---------------------------------------------------------------------
     def mac_sample(self, tree: "Tree", amag, alpha, window=32, stride=1, rho_lo=0.02, rho_hi=50.0,
@@ -324,8 +442,8 @@ class Context:
         k = min(ns.value, capacity)
         return f[:k], lab[:k], rho[:k], ns.value
 
-    def mac_train(self, features, labels, epochs=30, batch=4096, lr=2e-3, tau=0.9, seed=1):
-        o = MacTrainOptions(epochs=epochs, batch=batch, lr=lr, tau=tau, seed=seed)
+    def mac_train(self, features, labels, epochs=30, batch=4096, lr=2e-3, tau=0.9, seed=1, feature_mask=0xFF):
+        o = MacTrainOptions(epochs=epochs, batch=batch, lr=lr, tau=tau, seed=seed, feature_mask=feature_mask)
         X = np.ascontiguousarray(features, np.float32)
         Y = np.ascontiguousarray(labels, np.float32)
         model = np.empty(MAC_MODEL_FLOATS, np.float32)

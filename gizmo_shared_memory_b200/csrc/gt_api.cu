@@ -121,12 +121,14 @@ void check_mem(int mem) {
 void free_tree_arrays(gt_tree* t) {
     void* ptrs[] = {t->src, t->ssoft, t->smass, t->order, t->rank, t->leaf_of, t->sleaf, t->skey,
                     t->nodes, t->parent, t->next, t->level, t->size, t->delta, t->nsoft, t->gc,
-                    t->nq2};
+                    t->nq2, t->sys_off_dev, t->geom_dev};
     // tree arrays came from the stream-ordered pool: hand them back to it (callers have synchronised)
     for (void* p : ptrs)
         if (p) cudaFreeAsync(p, 0);
-    for (auto& c : t->group_cache)
+    for (auto& c : t->group_cache) {
         if (c.groups) cudaFree(c.groups);
+        if (c.roots) cudaFree(c.roots);
+    }
     t->group_cache.clear();
 }
 
@@ -143,7 +145,7 @@ void record_walk_time(gt_context* ctx) {
 void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
                  const double* aold, double theta, double G, int group_mode, int group_param,
                  bool leaf_accept, const gt_walk_options* opt, int mem, double* ax, double* ay,
-                 double* az, double* phi) {
+                 double* az, double* phi, WalkBuffers* bufs = nullptr, bool capture = false) {
     if (!ctx || !tree) throw Fail{GT_ERR_INVALID, "null context or tree"};
     check_mem(mem);
     if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "tree and context are on different devices"};
@@ -151,11 +153,16 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     gt_walk_options o;
     gt_walk_options_default(&o);
     if (opt) o = *opt;
-    if (o.mac != GT_MAC_PLAIN && o.mac != GT_MAC_LEARNED) throw Fail{GT_ERR_INVALID, "unknown mac"};
-    if (o.mac == GT_MAC_LEARNED && !o.mac_model)
-        throw Fail{GT_ERR_INVALID, "GT_MAC_LEARNED needs gt_walk_options.mac_model"};
-    if (o.mac == GT_MAC_LEARNED && !leaf_accept)
+    if (o.mac != GT_MAC_PLAIN && o.mac != GT_MAC_LEARNED && o.mac != GT_MAC_NODE)
+        throw Fail{GT_ERR_INVALID, "unknown mac"};
+    const bool learned = o.mac == GT_MAC_LEARNED || o.mac == GT_MAC_NODE;
+    if (learned && !o.mac_model) throw Fail{GT_ERR_INVALID, "a learned criterion needs gt_walk_options.mac_model"};
+    if (learned && !leaf_accept)
         throw Fail{GT_ERR_UNSUPPORTED, "the learned criterion applies to the grouped walk"};
+    if (o.mac == GT_MAC_NODE)
+        for (int i = 0; i < GT_MAC_FEATURES; ++i)
+            if (!((GT_MAC_NODE_FEATURES >> i) & 1u) && o.mac_model[GT_MAC_FEATURES + i] != 0.0f)
+                throw Fail{GT_ERR_INVALID, "GT_MAC_NODE needs a model that reads node features only"};
     if (o.dtype_out_f32 != 0) throw Fail{GT_ERR_INVALID, "dtype_out_f32 is reserved"};
     if (o.out_order == GT_OUT_ORIGINAL && targets) throw Fail{GT_ERR_INVALID, "GT_OUT_ORIGINAL needs targets == NULL"};
     DeviceGuard dg(ctx->device);
@@ -183,9 +190,19 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     rq.want_phi = phi != nullptr;
     rq.out_original = all && o.out_order == GT_OUT_ORIGINAL;
     rq.mac = o.mac;
-    if (o.mac == GT_MAC_LEARNED) {
-        // the model is a small host array: stage it with the call
-        rq.mac_model = stage_in(ctx, kSlotIn2, o.mac_model, (int64_t)GT_MAC_MODEL_FLOATS, GT_MEM_HOST);
+    if (learned) {
+        if (bufs) {
+            // a plan keeps its own device copy, made before capture
+            if (!bufs->model) {
+                check_cuda(cudaMalloc(&bufs->model, GT_MAC_MODEL_FLOATS * sizeof(float)), "cudaMalloc");
+                check_cuda(cudaMemcpy(bufs->model, o.mac_model, GT_MAC_MODEL_FLOATS * sizeof(float),
+                                      cudaMemcpyHostToDevice), "model h2d");
+            }
+            rq.mac_model = bufs->model;
+        } else {
+            // the model is a small host array: stage it with the call
+            rq.mac_model = stage_in(ctx, kSlotIn2, o.mac_model, (int64_t)GT_MAC_MODEL_FLOATS, GT_MEM_HOST);
+        }
         rq.mac_kappa = o.mac_kappa;
         rq.mac_band_lo = o.mac_band[0];
         rq.mac_band_hi = o.mac_band[1];
@@ -194,6 +211,8 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     rq.block_warps = o.block_warps;
     rq.list_capacity = o.list_capacity;
     rq.stack_capacity = o.stack_capacity;
+    rq.bufs = bufs;
+    rq.capture = capture;
     if ((ax == nullptr) != (ay == nullptr) || (ax == nullptr) != (az == nullptr))
         throw Fail{GT_ERR_INVALID, "ax, ay, az must all be given or all be null"};
     if (!ax && !phi) return;
@@ -207,6 +226,7 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
             if (p) check_cuda(cudaMemsetAsync(p, 0, (size_t)nout * 8, ctx->stream), "memset");
     }
     run_walk(ctx, tree, rq);
+    if (capture) return;
     copy_out(ctx, ax, rq.ax, nout, mem);
     copy_out(ctx, ay, rq.ay, nout, mem);
     copy_out(ctx, az, rq.az, nout, mem);
@@ -346,9 +366,10 @@ int gt_launch_count(const gt_context* ctx, uint64_t* count) {
     return GT_OK;
 }
 
-int gt_build(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
-             const double* m, const double* soft, int mem, const gt_build_options* opt,
-             gt_tree** out) {
+namespace {
+int build_common(gt_context* ctx, int64_t n, int32_t n_systems, const int64_t* offsets, const double* x,
+                 const double* y, const double* z, const double* m, const double* soft, int mem,
+                 const gt_build_options* opt, gt_tree** out) {
     if (!ctx || !out) return GT_ERR_INVALID;
     *out = nullptr;
     gt_tree* t = new gt_tree();
@@ -357,6 +378,14 @@ int gt_build(gt_context* ctx, int64_t n, const double* x, const double* y, const
         if (n < 0) throw Fail{GT_ERR_INVALID, "n < 0"};
         if (n > 0 && (!x || !y || !z || !m)) throw Fail{GT_ERR_INVALID, "null particle array"};
         if (n >= (int64_t)INT32_MAX) throw Fail{GT_ERR_INVALID, "n must be below 2^31"};
+        if (n_systems < 1 || n_systems > (1 << 24)) throw Fail{GT_ERR_INVALID, "n_systems must be in [1, 2^24]"};
+        if (n_systems > 1) {
+            if (!offsets) throw Fail{GT_ERR_INVALID, "null system offsets"};
+            if (offsets[0] != 0 || offsets[n_systems] != n)
+                throw Fail{GT_ERR_INVALID, "system offsets must start at 0 and end at n"};
+            for (int32_t s = 0; s < n_systems; ++s)
+                if (offsets[s + 1] < offsets[s]) throw Fail{GT_ERR_INVALID, "system offsets must not decrease"};
+        }
         gt_build_options o;
         gt_build_options_default(&o);
         if (opt) o = *opt;
@@ -372,7 +401,7 @@ int gt_build(gt_context* ctx, int64_t n, const double* x, const double* y, const
         const double* dz = stage_in(ctx, kSlotIn2, z, n, mem);
         const double* dm = stage_in(ctx, kSlotIn3, m, n, mem);
         const double* ds = stage_in(ctx, kSlotIn4, soft, n, mem);
-        build_tree(ctx, t, dx, dy, dz, dm, ds);
+        build_tree(ctx, t, dx, dy, dz, dm, ds, n_systems, offsets);
         finish(ctx, true);
     });
     if (st != GT_OK) {
@@ -383,6 +412,32 @@ int gt_build(gt_context* ctx, int64_t n, const double* x, const double* y, const
         return st;
     }
     *out = t;
+    return GT_OK;
+}
+}  // namespace
+
+int gt_build(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
+             const double* m, const double* soft, int mem, const gt_build_options* opt,
+             gt_tree** out) {
+    return build_common(ctx, n, 1, nullptr, x, y, z, m, soft, mem, opt, out);
+}
+
+int gt_build_systems(gt_context* ctx, int64_t n, int32_t n_systems, const int64_t* offsets,
+                     const double* x, const double* y, const double* z, const double* m,
+                     const double* soft, int mem, const gt_build_options* opt, gt_tree** out) {
+    return build_common(ctx, n, n_systems, offsets, x, y, z, m, soft, mem, opt, out);
+}
+
+int gt_tree_systems(const gt_tree* t, int64_t* live_offsets, double* roots) {
+    if (!t) return GT_ERR_INVALID;
+    for (int s = 0; s < t->n_systems; ++s) {
+        if (live_offsets) live_offsets[s] = t->sys_off[s];
+        if (roots) {
+            const gt::RootGeom& g = t->sys_geom[s];
+            roots[4 * s] = g.cx; roots[4 * s + 1] = g.cy; roots[4 * s + 2] = g.cz; roots[4 * s + 3] = g.side;
+        }
+    }
+    if (live_offsets) live_offsets[t->n_systems] = t->sys_off[t->n_systems];
     return GT_OK;
 }
 
@@ -412,6 +467,7 @@ int gt_tree_info_get(const gt_tree* t, gt_tree_info* info) {
     info->center[2] = t->geom.cz;
     info->side = t->geom.side;
     for (int k = 0; k < 7; ++k) info->build_ms[k] = t->build_ms[k];
+    info->n_systems = t->n_systems;
     return GT_OK;
 }
 
@@ -497,6 +553,156 @@ int gt_accel_grouped(gt_context* ctx, const gt_tree* tree, int64_t n_targets, co
         if (mode < GT_GROUP_LEAF || mode > GT_GROUP_SINGLE) throw Fail{GT_ERR_INVALID, "unknown group_mode"};
         walk_common(ctx, tree, n_targets, targets, aold, theta, G, mode, param, true, &o, mem, ax, ay, az, phi);
     });
+}
+
+void gt_tune_options_default(gt_tune_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->reps = 3;
+    o->p99_max = 5e-3;
+}
+
+int gt_autotune(gt_context* ctx, const gt_tree* tree, const double* aold, int mem, double theta, double G,
+                const gt_tune_options* opt, gt_walk_options* best, int* best_batch, gt_tune_entry* entries,
+                int max_entries, int* n_entries) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (!tree || !best) throw Fail{GT_ERR_INVALID, "null tree or output"};
+        if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "tree and context are on different devices"};
+        gt_tune_options o;
+        gt_tune_options_default(&o);
+        if (opt) o = *opt;
+        if (o.n_sample < 0 || (o.n_sample > 0 && (!o.sample || !o.ref_ax || !o.ref_ay || !o.ref_az)))
+            throw Fail{GT_ERR_INVALID, "bad sample"};
+        for (int64_t i = 0; i < o.n_sample; ++i)
+            if ((int64_t)o.sample[i] >= tree->n) throw Fail{GT_ERR_INVALID, "sample index out of range"};
+        if (o.mac_model && (o.n_kappa <= 0 || !o.kappa)) throw Fail{GT_ERR_INVALID, "a model needs kappa values"};
+        DeviceGuard dg(ctx->device);
+        TuneRequest tr;
+        tr.reps = o.reps;
+        tr.p99_max = o.p99_max;
+        tr.n_sample = o.n_sample;
+        tr.sample = o.sample;
+        tr.ref_ax = o.ref_ax; tr.ref_ay = o.ref_ay; tr.ref_az = o.ref_az;
+        if (o.mac_model) {
+            tr.mac_model = stage_in(ctx, kSlotIn2, o.mac_model, (int64_t)GT_MAC_MODEL_FLOATS, GT_MEM_HOST);
+            tr.kappa.assign(o.kappa, o.kappa + o.n_kappa);
+            tr.mac_band[0] = o.mac_band[0];
+            tr.mac_band[1] = o.mac_band[1];
+            tr.mac_mode = o.mac_mode == GT_MAC_NODE ? GT_MAC_NODE : GT_MAC_LEARNED;
+            if (o.mac_mode != 0 && o.mac_mode != GT_MAC_LEARNED && o.mac_mode != GT_MAC_NODE)
+                throw Fail{GT_ERR_INVALID, "unknown mac_mode"};
+        }
+        const double* da = stage_in(ctx, kSlotIn1, aold, tree->n_live, mem);
+        std::vector<gt_tune_entry> all;
+        gt_tune_entry b;
+        run_autotune(ctx, tree, da, theta, G, tr, all, b);
+        gt_walk_options w;
+        gt_walk_options_default(&w);
+        w.group_mode = b.group_mode;
+        if (b.group_mode == GT_GROUP_NODE) w.group_max = b.group_size;
+        w.block_warps = b.block_warps;
+        w.list_capacity = b.list_capacity;
+        w.mac = b.mac;
+        if (b.mac != GT_MAC_PLAIN) {
+            w.mac_model = o.mac_model;
+            w.mac_kappa = b.mac_kappa;
+            w.mac_band[0] = o.mac_band[0];
+            w.mac_band[1] = o.mac_band[1];
+        }
+        *best = w;
+        if (best_batch) *best_batch = b.group_mode == GT_GROUP_BATCH ? b.group_size : 0;
+        const int k = (int)std::min<size_t>(all.size(), (size_t)std::max(0, max_entries));
+        if (entries)
+            for (int i = 0; i < k; ++i) entries[i] = all[i];
+        if (n_entries) *n_entries = entries ? k : (int)all.size();
+    });
+}
+
+int gt_plan_create(gt_context* ctx, const gt_tree* tree, const double* aold, double theta, double G, int batch,
+                   const gt_walk_options* opt, double* ax, double* ay, double* az, double* phi, gt_plan** out) {
+    if (!ctx || !out) return GT_ERR_INVALID;
+    *out = nullptr;
+    gt_plan* p = new gt_plan();
+    p->ctx = ctx;
+    p->tree = tree;
+    bool capturing = false;
+    // capture on a stream of our own: the context stream may be the legacy default stream, which
+    // cannot be captured; replays go to the context stream
+    cudaStream_t saved = ctx->stream, cs = nullptr;
+    const int st = guarded(ctx, [&] {
+        if (!tree) throw Fail{GT_ERR_INVALID, "null tree"};
+        gt_walk_options o;
+        gt_walk_options_default(&o);
+        if (opt) o = *opt;
+        if (o.count) throw Fail{GT_ERR_INVALID, "a plan does not collect counts"};
+        if (o.stack_capacity) throw Fail{GT_ERR_INVALID, "a plan uses the default stack capacity"};
+        o.async = 1;
+        int mode = o.group_mode, param = 0;
+        if (mode == GT_GROUP_LEAF && batch > 0) mode = GT_GROUP_BATCH;
+        if (mode == GT_GROUP_BATCH) param = batch > 0 ? batch : 8;
+        if (mode == GT_GROUP_NODE) param = o.group_max;
+        if (mode < GT_GROUP_LEAF || mode > GT_GROUP_SINGLE) throw Fail{GT_ERR_INVALID, "unknown group_mode"};
+        DeviceGuard dg(ctx->device);
+        // one ordinary walk first: it builds the group list, sizes the plan's buffers and sets
+        // the kernel attributes, so the capture below allocates nothing
+        walk_common(ctx, tree, 0, nullptr, aold, theta, G, mode, param, true, &o, GT_MEM_DEVICE, ax, ay, az,
+                    phi, &p->bufs, false);
+        check_cuda(cudaStreamSynchronize(ctx->stream), "sync");
+        const uint64_t before = ctx->launches;
+        check_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate");
+        ctx->stream = cs;
+        check_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        capturing = true;
+        walk_common(ctx, tree, 0, nullptr, aold, theta, G, mode, param, true, &o, GT_MEM_DEVICE, ax, ay, az,
+                    phi, &p->bufs, true);
+        capturing = false;
+        check_cuda(cudaStreamEndCapture(cs, &p->graph), "cudaStreamEndCapture");
+        ctx->stream = saved;
+        p->kernels = ctx->launches - before;
+        ctx->launches = before;  // captured, not launched
+        check_cuda(cudaGraphInstantiate(&p->exec, p->graph, 0), "cudaGraphInstantiate");
+    });
+    if (capturing) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(cs, &g);
+        if (g) cudaGraphDestroy(g);
+    }
+    ctx->stream = saved;
+    if (cs) cudaStreamDestroy(cs);
+    if (st != GT_OK) {
+        cudaGetLastError();
+        gt_plan_destroy(p);
+        return st;
+    }
+    *out = p;
+    return GT_OK;
+}
+
+int gt_plan_launch(gt_plan* p) {
+    if (!p || !p->exec) return GT_ERR_INVALID;
+    return guarded(p->ctx, [&] {
+        DeviceGuard dg(p->ctx->device);
+        check_cuda(cudaGraphLaunch(p->exec, p->ctx->stream), "cudaGraphLaunch");
+        p->ctx->launches += p->kernels;
+    });
+}
+
+int gt_plan_destroy(gt_plan* p) {
+    if (!p) return GT_ERR_INVALID;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(p->ctx->device);
+    if (p->ctx->stream) cudaStreamSynchronize(p->ctx->stream);
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    for (void* q : {(void*)p->bufs.stack, (void*)p->bufs.ctr, (void*)p->bufs.model})
+        if (q) cudaFree(q);
+    cudaGetLastError();
+    if (prev >= 0) cudaSetDevice(prev);
+    delete p;
+    return GT_OK;
 }
 
 int gt_accel(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
@@ -608,6 +814,7 @@ void gt_mac_train_options_default(gt_mac_train_options* o) {
     o->lr = 2e-3;
     o->tau = 0.9;
     o->seed = 1;
+    o->feature_mask = 0xFFu;
 }
 
 int gt_mac_sample(gt_context* ctx, const gt_tree* tree, const double* amag, double alpha, int window,
@@ -620,6 +827,7 @@ int gt_mac_sample(gt_context* ctx, const gt_tree* tree, const double* amag, doub
         if (window < 1 || window > 32) throw Fail{GT_ERR_INVALID, "window must be in [1, 32]"};
         if (!(alpha > 0) || !(rho_hi >= rho_lo)) throw Fail{GT_ERR_INVALID, "bad alpha or rho window"};
         if (capacity > 0 && (!features || !labels || !rho)) throw Fail{GT_ERR_INVALID, "null output"};
+        if (tree->n_systems > 1) throw Fail{GT_ERR_UNSUPPORTED, "gt_mac_sample takes a single-system tree"};
         DeviceGuard dg(ctx->device);
         const double* da = stage_in(ctx, kSlotIn0, amag, tree->n_live, mem);
         float* f = out_buf(ctx, kSlotOut0, features, capacity * GT_MAC_FEATURES, mem);

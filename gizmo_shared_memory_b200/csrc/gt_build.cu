@@ -95,20 +95,9 @@ __global__ void bbox_partial_kernel(const double* __restrict__ x, const double* 
     }
 }
 
-// Root cell, tree.cc:361-417.  Runs as one thread: it is a handful of flops.
-__global__ void root_geom_kernel(const double* __restrict__ part, const unsigned long long* __restrict__ cnt,
-                                 int nb, RootGeom* __restrict__ g, unsigned long long* __restrict__ bad_out,
-                                 long long seed, double fx, double fy, double fz, int max_level) {
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    unsigned long long live = 0, bad = 0;
-    for (int b = 0; b < nb; ++b) {
-        for (int c = 0; c < 3; ++c) {
-            lo[c] = fmin(lo[c], part[b * 6 + c]);
-            hi[c] = fmax(hi[c], part[b * 6 + 3 + c]);
-        }
-        live += cnt[b * 2];
-        bad += cnt[b * 2 + 1];
-    }
+// Root cell from the live bounding box, tree.cc:361-417.  A handful of flops, one thread.
+__device__ void finish_root(const double* lo, const double* hi, unsigned long long live, RootGeom* __restrict__ g,
+                            long long seed, double fx, double fy, double fz, int max_level) {
     double cx = 0.5 * (lo[0] + hi[0]), cy = 0.5 * (lo[1] + hi[1]), cz = 0.5 * (lo[2] + hi[2]);
     double side = fmax(hi[0] - lo[0], fmax(hi[1] - lo[1], hi[2] - lo[2])) * 1.0000001;
     if (side <= 0) side = 1.0;
@@ -138,7 +127,70 @@ __global__ void root_geom_kernel(const double* __restrict__ part, const unsigned
     g->corner_y = fma(-0.5, side, cy);
     g->corner_z = fma(-0.5, side, cz);
     g->n_live = (long long)live;
+}
+
+__global__ void root_geom_kernel(const double* __restrict__ part, const unsigned long long* __restrict__ cnt,
+                                 int nb, RootGeom* __restrict__ g, unsigned long long* __restrict__ bad_out,
+                                 long long seed, double fx, double fy, double fz, int max_level) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    unsigned long long live = 0, bad = 0;
+    for (int b = 0; b < nb; ++b) {
+        for (int c = 0; c < 3; ++c) {
+            lo[c] = fmin(lo[c], part[b * 6 + c]);
+            hi[c] = fmax(hi[c], part[b * 6 + 3 + c]);
+        }
+        live += cnt[b * 2];
+        bad += cnt[b * 2 + 1];
+    }
+    finish_root(lo, hi, live, g, seed, fx, fy, fz, max_level);
     *bad_out = bad;
+}
+
+// Forest: one block per system reduces its input range and finishes that system's root cell.
+// bad_out accumulates the non-finite count over all systems.
+__global__ void bbox_systems_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                    const double* __restrict__ z, const double* __restrict__ m,
+                                    const double* __restrict__ soft, const int64_t* __restrict__ off,
+                                    RootGeom* __restrict__ geoms, unsigned long long* __restrict__ bad_out,
+                                    long long seed, double fx, double fy, double fz, int max_level) {
+    const int s = blockIdx.x;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    unsigned long long live = 0, bad = 0;
+    for (int64_t i = off[s] + threadIdx.x; i < off[s + 1]; i += blockDim.x) {
+        const double xi = x[i], yi = y[i], zi = z[i], mi = m[i];
+        const double si = soft ? soft[i] : 0.0;
+        if (!isfinite(xi) || !isfinite(yi) || !isfinite(zi) || !isfinite(mi) || !isfinite(si)) ++bad;
+        if (!(mi > 0)) continue;
+        ++live;
+        lo[0] = fmin(lo[0], xi); hi[0] = fmax(hi[0], xi);
+        lo[1] = fmin(lo[1], yi); hi[1] = fmax(hi[1], yi);
+        lo[2] = fmin(lo[2], zi); hi[2] = fmax(hi[2], zi);
+    }
+    for (int c = 0; c < 3; ++c) { lo[c] = warp_min_d(lo[c]); hi[c] = warp_max_d(hi[c]); }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        live += __shfl_xor_sync(0xffffffffu, live, o);
+        bad += __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    __shared__ double sh[8][6];
+    __shared__ unsigned long long sc[8][2];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        for (int c = 0; c < 3; ++c) { sh[w][c] = lo[c]; sh[w][3 + c] = hi[c]; }
+        sc[w][0] = live; sc[w][1] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+            for (int c = 0; c < 3; ++c) {
+                lo[c] = fmin(lo[c], sh[k][c]);
+                hi[c] = fmax(hi[c], sh[k][3 + c]);
+            }
+            live += sc[k][0]; bad += sc[k][1];
+        }
+        finish_root(lo, hi, live, geoms + s, seed, fx, fy, fz, max_level);
+        if (bad) atomicAdd(bad_out, bad);
+    }
 }
 
 // ---- 2. keys ---------------------------------------------------------------------------------
@@ -162,15 +214,21 @@ __device__ __forceinline__ uint64_t spread3_21(uint64_t v) {
 __global__ void keys_kernel(const double* __restrict__ x, const double* __restrict__ y,
                             const double* __restrict__ z, const double* __restrict__ m, int64_t n,
                             const RootGeom* __restrict__ gp, int key_mode, int levels,
-                            uint64_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+                            uint64_t* __restrict__ keys, uint32_t* __restrict__ idx,
+                            const int64_t* __restrict__ sys_in, int n_systems, uint64_t* __restrict__ sys_key) {
     __shared__ uint16_t tab[48 * 8];
     for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x) tab[k] = kPhStep[k];
     __syncthreads();
-    const RootGeom g = *gp;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         idx[i] = (uint32_t)i;
-        if (!(m[i] > 0)) { keys[i] = kDeadKey; continue; }
+        // forest: the particle's own system's root cell; the second sort key is the system
+        // (massless particles of every system go last)
+        const int s = n_systems > 1 ? system_of(sys_in, n_systems, i) : 0;
+        const bool live = m[i] > 0;
+        if (n_systems > 1) sys_key[i] = live ? (uint64_t)s : (uint64_t)n_systems;
+        if (!live) { keys[i] = kDeadKey; continue; }
+        const RootGeom& g = gp[s];
         uint32_t a, b, c;
         quantise(g, x[i], y[i], z[i], a, b, c);
         uint64_t key;
@@ -251,7 +309,8 @@ __global__ void emit_kernel(GNode* __restrict__ nodes, const SrcP* __restrict__ 
                             int max_level, const int* __restrict__ bnd,
                             const uint32_t* __restrict__ nchild, const uint32_t* __restrict__ coff,
                             int* __restrict__ parent, int* __restrict__ next, int* __restrict__ lvl,
-                            double* __restrict__ size, double* __restrict__ gc) {
+                            double* __restrict__ size, double* __restrict__ gc,
+                            const int* __restrict__ sys_off, int n_systems) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= b - a) return;
     const int64_t i = a + t;
@@ -261,7 +320,7 @@ __global__ void emit_kernel(GNode* __restrict__ nodes, const SrcP* __restrict__ 
         nodes[i].nchild = 0;
         return;
     }
-    const RootGeom g = *gp;
+    const RootGeom g = gp[n_systems > 1 ? system_of(sys_off, n_systems, nodes[i].plo) : 0];
     const int first = (int)(b + coff[t]);
     nodes[i].first = first;
     nodes[i].nchild = nc;
@@ -358,19 +417,45 @@ __global__ void moments_kernel(GNode* __restrict__ nodes, const SrcP* __restrict
     }
 }
 
+// Roots: node s is system s's root, covering its live tree positions [sys_off[s], sys_off[s+1]).
+// Each root stands alone in the reference threading (next = -1).
 __global__ void root_init_kernel(GNode* __restrict__ nodes, const RootGeom* __restrict__ gp,
+                                 const int* __restrict__ sys_off, int n_systems,
                                  int* parent, int* next, int* lvl, double* size, double* gc) {
-    const RootGeom g = *gp;
-    GNode& r = nodes[0];
-    r.plo = 0;
-    r.phi = (int)g.n_live;
-    r.first = -1;
-    r.nchild = 0;
-    parent[0] = -1;
-    next[0] = -1;
-    lvl[0] = 0;
-    size[0] = g.side;
-    gc[0] = g.cx; gc[1] = g.cy; gc[2] = g.cz;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_systems; s += gridDim.x * blockDim.x) {
+        const RootGeom& g = gp[s];
+        GNode& r = nodes[s];
+        r.plo = sys_off[s];
+        r.phi = sys_off[s + 1];
+        r.first = -1;
+        r.nchild = 0;
+        parent[s] = -1;
+        next[s] = -1;
+        lvl[s] = 0;
+        size[s] = g.side;
+        gc[3 * s] = g.cx; gc[3 * s + 1] = g.cy; gc[3 * s + 2] = g.cz;
+    }
+}
+
+// Second key of the forest sort: system of each key-sorted particle.
+__global__ void gather_sys_key_kernel(const uint64_t* __restrict__ sys_key, const uint32_t* __restrict__ idx,
+                                      int64_t n, uint64_t* __restrict__ out, uint32_t* __restrict__ pos) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        out[i] = sys_key[idx[i]];
+        pos[i] = (uint32_t)i;
+    }
+}
+
+__global__ void permute_pairs_kernel(const uint64_t* __restrict__ key, const uint32_t* __restrict__ val,
+                                     const uint32_t* __restrict__ pos, int64_t n, uint64_t* __restrict__ key_out,
+                                     uint32_t* __restrict__ val_out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = pos[i];
+        key_out[i] = key[p];
+        val_out[i] = val[p];
+    }
 }
 
 // ---- MPI-code keys (domain.cc:2682-2702, peano.cc:297-355) -------------------------------------
@@ -458,10 +543,12 @@ void grow_nodes(gt_tree* t, int64_t need, cudaStream_t stream) {
 }  // namespace
 
 void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, const double* z,
-                const double* m, const double* soft) {
+                const double* m, const double* soft, int n_systems, const int64_t* in_off) {
     cudaStream_t st = ctx->stream;
     const int64_t n = t->n;
     const gt_build_options& o = t->opt;
+    const int S = std::max(1, n_systems);
+    t->n_systems = S;
     cudaEvent_t ev[7];
     for (auto& e : ev) check_cuda(cudaEventCreate(&e), "event");
     struct EvGuard {
@@ -470,41 +557,88 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
     } guard{ev};
     check_cuda(cudaEventRecord(ev[0], st), "event");
 
-    // 1. bbox
-    const int nbb = std::max(1, std::min(ctx->num_sms * 2, div_up(std::max<int64_t>(n, 1), kBlk)));
-    double* part = (double*)scratch(ctx, kSlotPartials, (size_t)nbb * 6 * 8 + (size_t)nbb * 16 + 256);
-    unsigned long long* cnt = (unsigned long long*)(part + (size_t)nbb * 6);
-    RootGeom* gdev = (RootGeom*)scratch(ctx, kSlotCounters, sizeof(RootGeom) + 64);
-    unsigned long long* bad_dev = (unsigned long long*)((char*)gdev + sizeof(RootGeom));
-    bbox_partial_kernel<<<nbb, kBlk, 0, st>>>(x, y, z, m, soft, n, part, cnt);
-    check_launch(ctx, "bbox_partial_kernel");
-    root_geom_kernel<<<1, 1, 0, st>>>(part, cnt, nbb, gdev, bad_dev, o.randomize_seed, o.shift[0],
-                                      o.shift[1], o.shift[2], o.max_level);
-    check_launch(ctx, "root_geom_kernel");
+    // 1. bbox: per-system root cells (geom_dev), live counts, the non-finite count
+    t->geom_dev = dalloc<RootGeom>((size_t)S, st);
+    t->sys_off_dev = dalloc<int>((size_t)S + 1, st);
+    RootGeom* gdev = t->geom_dev;
+    unsigned long long* bad_dev = (unsigned long long*)scratch(ctx, kSlotCounters, 64);
+    int64_t* in_off_dev = nullptr;
+    if (S == 1) {
+        const int nbb = std::max(1, std::min(ctx->num_sms * 2, div_up(std::max<int64_t>(n, 1), kBlk)));
+        double* part = (double*)scratch(ctx, kSlotPartials, (size_t)nbb * 6 * 8 + (size_t)nbb * 16 + 256);
+        unsigned long long* cnt = (unsigned long long*)(part + (size_t)nbb * 6);
+        bbox_partial_kernel<<<nbb, kBlk, 0, st>>>(x, y, z, m, soft, n, part, cnt);
+        check_launch(ctx, "bbox_partial_kernel");
+        root_geom_kernel<<<1, 1, 0, st>>>(part, cnt, nbb, gdev, bad_dev, o.randomize_seed, o.shift[0],
+                                          o.shift[1], o.shift[2], o.max_level);
+        check_launch(ctx, "root_geom_kernel");
+    } else {
+        in_off_dev = (int64_t*)scratch(ctx, kSlotPartials, (size_t)(S + 1) * 8);
+        // pageable source: the copy is staged before the call returns, in_off may go away after
+        check_cuda(cudaMemcpyAsync(in_off_dev, in_off, (size_t)(S + 1) * 8, cudaMemcpyHostToDevice, st),
+                   "offsets h2d");
+        check_cuda(cudaMemsetAsync(bad_dev, 0, 8, st), "memset");
+        bbox_systems_kernel<<<S, kBlk, 0, st>>>(x, y, z, m, soft, in_off_dev, gdev, bad_dev, o.randomize_seed,
+                                                o.shift[0], o.shift[1], o.shift[2], o.max_level);
+        check_launch(ctx, "bbox_systems_kernel");
+    }
     {
-        char* pin = (char*)ctx->pinned;
-        check_cuda(cudaMemcpyAsync(pin, gdev, sizeof(RootGeom) + 8, cudaMemcpyDeviceToHost, st), "geom d2h");
-        check_cuda(cudaStreamSynchronize(st), "sync");
-        std::memcpy(&t->geom, pin, sizeof(RootGeom));
+        t->sys_geom.resize(S);
         unsigned long long bad = 0;
-        std::memcpy(&bad, pin + sizeof(RootGeom), 8);
+        check_cuda(cudaMemcpyAsync(t->sys_geom.data(), gdev, sizeof(RootGeom) * S, cudaMemcpyDeviceToHost, st),
+                   "geom d2h");
+        check_cuda(cudaMemcpyAsync(ctx->pinned, bad_dev, 8, cudaMemcpyDeviceToHost, st), "d2h");
+        check_cuda(cudaStreamSynchronize(st), "sync");
+        std::memcpy(&bad, ctx->pinned, 8);
         if (o.validate && bad > 0)
             throw Fail{GT_ERR_NONFINITE, "gt_build: " + std::to_string(bad) + " particle(s) with non-finite input"};
     }
-    t->n_live = t->geom.n_live;
+    t->geom = t->sys_geom[0];
+    t->sys_off.assign(1, 0);
+    for (int s = 0; s < S; ++s) t->sys_off.push_back(t->sys_off.back() + t->sys_geom[s].n_live);
+    t->n_live = t->sys_off.back();
+    {
+        std::vector<int> off32(t->sys_off.begin(), t->sys_off.end());
+        check_cuda(cudaMemcpyAsync(t->sys_off_dev, off32.data(), off32.size() * sizeof(int), cudaMemcpyHostToDevice, st),
+                   "offsets h2d");
+        check_cuda(cudaStreamSynchronize(st), "sync");  // off32 is pageable and goes out of scope
+    }
     check_cuda(cudaEventRecord(ev[1], st), "event");
 
-    // 2. keys
+    // 2. keys (and, in a forest, each particle's system as the second sort key)
     uint64_t* keys = (uint64_t*)scratch(ctx, kSlotKeysA, (size_t)std::max<int64_t>(n, 1) * 8);
     uint32_t* idx = (uint32_t*)scratch(ctx, kSlotValsA, (size_t)std::max<int64_t>(n, 1) * 4);
+    uint64_t* sys_key = nullptr;
+    if (S > 1) sys_key = dalloc<uint64_t>((size_t)std::max<int64_t>(n, 1), st);
     if (n > 0) {
-        keys_kernel<<<grid_for(ctx, n), kBlk, 0, st>>>(x, y, z, m, n, gdev, o.key_mode, o.max_level, keys, idx);
+        keys_kernel<<<grid_for(ctx, n), kBlk, 0, st>>>(x, y, z, m, n, gdev, o.key_mode, o.max_level, keys, idx,
+                                                       in_off_dev, S, sys_key);
         check_launch(ctx, "keys_kernel");
     }
     check_cuda(cudaEventRecord(ev[2], st), "event");
 
-    // 3. sort: live keys < 2^(3*max_level), the massless sentinel is 2^60
+    // 3. sort: live keys < 2^(3*max_level), the massless sentinel is 2^60.  A forest then sorts
+    // stably by system (LSD order: key first, system last), which keeps each system's key order
+    // and puts every massless particle after all live ones.
     radix_sort_pairs(ctx, keys, idx, n, 61);
+    if (S > 1 && n > 1) {
+        uint64_t* k2 = dalloc<uint64_t>((size_t)n, st);
+        uint32_t* pos = dalloc<uint32_t>((size_t)n, st);
+        gather_sys_key_kernel<<<grid_for(ctx, n), kBlk, 0, st>>>(sys_key, idx, n, k2, pos);
+        check_launch(ctx, "gather_sys_key_kernel");
+        int bits = 1;
+        while ((1ll << bits) <= (long long)S) ++bits;
+        radix_sort_pairs(ctx, k2, pos, n, bits);
+        // permute (keys, idx) by pos through the sys_key buffer and k2's value array
+        uint32_t* idx2 = (uint32_t*)k2;  // k2 is no longer needed once pos is sorted: reuse as idx
+        permute_pairs_kernel<<<grid_for(ctx, n), kBlk, 0, st>>>(keys, idx, pos, n, sys_key, idx2);
+        check_launch(ctx, "permute_pairs_kernel");
+        check_cuda(cudaMemcpyAsync(keys, sys_key, (size_t)n * 8, cudaMemcpyDeviceToDevice, st), "copy keys");
+        check_cuda(cudaMemcpyAsync(idx, idx2, (size_t)n * 4, cudaMemcpyDeviceToDevice, st), "copy idx");
+        check_cuda(cudaFreeAsync(k2, st), "cudaFreeAsync");
+        check_cuda(cudaFreeAsync(pos, st), "cudaFreeAsync");
+    }
+    if (sys_key) check_cuda(cudaFreeAsync(sys_key, st), "cudaFreeAsync");
     check_cuda(cudaEventRecord(ev[3], st), "event");
 
     // 4. particle arrays in tree order
@@ -526,12 +660,13 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
 
     // 5. structure, level by level
     const int64_t nl = t->n_live;
-    grow_nodes(t, std::max<int64_t>(1024, (2 * nl) / std::max(1, o.leaf_max) * 3 + 1024), st);
-    root_init_kernel<<<1, 1, 0, st>>>(t->nodes, gdev, t->parent, t->next, t->level, t->size, t->gc);
+    grow_nodes(t, std::max<int64_t>(1024, (2 * nl) / std::max(1, o.leaf_max) * 3 + 1024) + S, st);
+    root_init_kernel<<<div_up(S, kBlk), kBlk, 0, st>>>(t->nodes, gdev, t->sys_off_dev, S, t->parent, t->next,
+                                                       t->level, t->size, t->gc);
     check_launch(ctx, "root_init_kernel");
     t->lvl_off.assign(1, 0);
-    t->lvl_off.push_back(1);
-    uint32_t* total_dev = (uint32_t*)((char*)gdev + sizeof(RootGeom) + 16);
+    t->lvl_off.push_back(S);
+    uint32_t* total_dev = (uint32_t*)(bad_dev + 2);
     for (int L = 0;; ++L) {
         const int64_t a = t->lvl_off[L], b = t->lvl_off[L + 1];
         const int64_t cnt_l = b - a;
@@ -552,7 +687,7 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
         grow_nodes(t, b + (int64_t)total, st);
         emit_kernel<<<div_up(cnt_l, kBlk), kBlk, 0, st>>>(t->nodes, t->src, gdev, a, b, L, o.max_level,
                                                           bnd, nch, coff, t->parent, t->next, t->level,
-                                                          t->size, t->gc);
+                                                          t->size, t->gc, t->sys_off_dev, S);
         check_launch(ctx, "emit_kernel");
         if (total == 0) break;
         t->lvl_off.push_back(b + (int64_t)total);

@@ -49,6 +49,18 @@ struct RootGeom {
     long long n_live;
 };
 
+// System of an index in a forest: the last s with off[s] <= i (off has n_systems + 1 entries,
+// non-decreasing; empty systems are skipped because off[s] == off[s+1]).
+template <typename T>
+__device__ __forceinline__ int system_of(const T* __restrict__ off, int n_systems, int64_t i) {
+    int lo = 0, hi = n_systems;  // invariant: off[lo] <= i < off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if ((int64_t)off[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Host-side structs behind the opaque C handles
 // ---------------------------------------------------------------------------------------------
@@ -78,7 +90,14 @@ struct gt_tree {
     int64_t n = 0, n_live = 0, n_nodes = 0, node_cap = 0;
     int n_levels = 0;
     gt_build_options opt{};
-    gt::RootGeom geom{};
+    gt::RootGeom geom{};           // root cell (of system 0 in a forest)
+    // A forest holds n_systems independent trees built in one pass: system s has root node s and
+    // the live tree positions [sys_off[s], sys_off[s+1]).
+    int n_systems = 1;
+    std::vector<gt::RootGeom> sys_geom;  // per-system root cells
+    std::vector<int64_t> sys_off;        // n_systems + 1
+    int* sys_off_dev = nullptr;          // device copy (int32), n_systems + 1
+    gt::RootGeom* geom_dev = nullptr;    // device copy of sys_geom
     std::vector<int64_t> lvl_off;  // node index range of each level: [lvl_off[L], lvl_off[L+1])
     double build_ms[7] = {0, 0, 0, 0, 0, 0, 0};
     // device arrays (owned)
@@ -103,6 +122,7 @@ struct gt_tree {
     struct GroupCache {
         int mode = -1, param = 0, kmax = 0;
         int2* groups = nullptr;
+        int* roots = nullptr;  // forest: root node of each group
         int64_t n_groups = 0;
     };
     std::vector<GroupCache> group_cache;
@@ -118,7 +138,7 @@ enum Slot {
     kSlotNodeTmp0, kSlotNodeTmp1, kSlotNodeTmp2,
     kSlotTargets, kSlotAold, kSlotGroupKey, kSlotGroupsA, kSlotGroupsB,
     kSlotOut0, kSlotOut1, kSlotOut2, kSlotOut3,
-    kSlotStack, kSlotCounters, kSlotDirect,
+    kSlotStack, kSlotCounters, kSlotDirect, kSlotGroupRoot, kSlotMacL2,
     kSlotCount
 };
 
@@ -144,10 +164,22 @@ void scan_exclusive_u32(gt_context* ctx, const uint32_t* in, uint32_t* out, int6
 void radix_sort_pairs(gt_context* ctx, uint64_t* keys, uint32_t* vals, int64_t n, int bits);
 
 // Build (gt_build.cu)
+// n_systems > 1 builds a forest: particles of system s are the input range [in_off[s], in_off[s+1])
+// (host array of n_systems + 1), each system gets its own root cell and tree.
 void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, const double* z,
-                const double* m, const double* soft);
+                const double* m, const double* soft, int n_systems = 1, const int64_t* in_off = nullptr);
 
 // Walk (gt_walk.cu)
+// Stack and counters owned by a walk plan (a captured graph must not point into the workspace).
+struct WalkBuffers {
+    int* stack = nullptr;
+    size_t stack_bytes = 0;
+    unsigned long long* ctr = nullptr;
+    size_t ctr_bytes = 0;
+    float* model = nullptr;  // device copy of the learned criterion's network
+    float* mac_l2 = nullptr; // GT_MAC_NODE per-node scale
+    size_t mac_l2_bytes = 0;
+};
 struct WalkRequest {
     const uint32_t* targets = nullptr;  // device, original indices; null = all live in tree order
     int64_t n_targets = 0;
@@ -163,9 +195,27 @@ struct WalkRequest {
     double mac_kappa = 1.0, mac_band_lo = 0.0, mac_band_hi = 0.0;
     bool count = false;
     int block_warps = 0, list_capacity = 0, stack_capacity = 0;
+    WalkBuffers* bufs = nullptr;  // plan-owned buffers; null: the context workspace
+    bool capture = false;         // being captured into a graph: no events, no read-back
     double *ax = nullptr, *ay = nullptr, *az = nullptr, *phi = nullptr;  // device outputs
 };
 void run_walk(gt_context* ctx, const gt_tree* t, const WalkRequest& rq);
+
+// Autotuner (gt_tune.cu); aold and mac_model are device pointers, the sample arrays host ones
+// except `sample`, which is copied to the device by the tuner.
+struct TuneRequest {
+    int reps = 3;
+    double p99_max = 5e-3;
+    int64_t n_sample = 0;
+    const uint32_t* sample = nullptr;
+    const double *ref_ax = nullptr, *ref_ay = nullptr, *ref_az = nullptr;
+    const float* mac_model = nullptr;
+    std::vector<double> kappa;
+    double mac_band[2] = {0, 0};
+    int mac_mode = GT_MAC_LEARNED;
+};
+void run_autotune(gt_context* ctx, const gt_tree* t, const double* aold, double theta, double G,
+                  const TuneRequest& tr, std::vector<gt_tune_entry>& entries, gt_tune_entry& best);
 
 // Direct sum (gt_direct.cu)
 void run_direct(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
@@ -185,6 +235,8 @@ void run_mac_train(gt_context* ctx, int64_t n, const float* X, const float* Y,
 void run_mac_grad(gt_context* ctx, const float* dmodel, const float* X, const float* Y, const int* perm,
                   int64_t off, int B, double tau, float* dgrad, double* loss);
 void run_mac_predict(gt_context* ctx, const float* dmodel, int64_t n, const float* X, float* out);
+// GT_MAC_NODE: per-node l2 = len^2 10^(c - log10 kappa) (n_nodes floats).
+void run_mac_node_scale(gt_context* ctx, const gt_tree* t, const float* dmodel, double kappa, float* l2);
 
 // Peak probe (gt_peak.cu)
 void run_peaks(gt_context* ctx, double* fp32_tflops, double* fp64_tflops);
@@ -192,3 +244,13 @@ void run_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* a
                    const double* az, double alpha, double G, double* aold);
 
 }  // namespace gt
+
+// A captured all-active walk (gt_plan_create): the graph and the buffers it points at.
+struct gt_plan {
+    gt_context* ctx = nullptr;
+    const gt_tree* tree = nullptr;
+    gt::WalkBuffers bufs;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t kernels = 0;  // kernel launches one replay makes
+};

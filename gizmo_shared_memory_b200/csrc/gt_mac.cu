@@ -436,6 +436,8 @@ void run_mac_train(gt_context* ctx, int64_t n, const float* X, const float* Y,
     check_cuda(cudaMemcpyAsync(hy.data(), Y, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "D2H");
     check_cuda(cudaMemcpyAsync(model_host, dmodel, kMacNorm * 4, cudaMemcpyDeviceToHost, st), "D2H");
     check_cuda(cudaStreamSynchronize(st), "sync");
+    for (int i = 0; i < kMacIn; ++i)
+        if (!((o.feature_mask >> i) & 1u)) { model_host[i] = 0.0f; model_host[kMacIn + i] = 0.0f; }
     std::vector<float> ys = hy;
     std::nth_element(ys.begin(), ys.begin() + (ptrdiff_t)(o.tau * (n - 1)), ys.end());
     init_params(model_host, o.seed, ys[(size_t)(o.tau * (n - 1))]);
@@ -477,6 +479,38 @@ void run_mac_predict(gt_context* ctx, const float* dmodel, int64_t n, const floa
     mlp_predict_kernel<<<std::max(1, std::min(div_up(n, 256), ctx->num_sms * 8)), 256, 0, ctx->stream>>>(
         dmodel, X, n, out);
     check_launch(ctx, "mlp_predict_kernel");
+}
+
+// ---- per-node criterion (GT_MAC_NODE) ---------------------------------------------------------
+namespace {
+
+// l2[i] = len^2 * 10^(c(node) - log10 kappa): the relative arm's M L^2 with the node's learned
+// correction folded in, so the walk tests M * l2 > r^4 aold exactly as the plain criterion does.
+__global__ void mac_node_scale_kernel(const GNode* __restrict__ nodes, const float* __restrict__ nq2,
+                                      int64_t n_nodes, const float* __restrict__ model, float log_kappa,
+                                      float* __restrict__ l2) {
+    __shared__ float m[kMacModel];
+    for (int i = threadIdx.x; i < kMacModel; i += blockDim.x) m[i] = model[i];
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const GNode nd = nodes[i];
+        float f[kMacIn];
+        mac_node_features((double)nd.len, nd.s, nd.mass, (double)nq2[i], nd.phi - nd.plo, f);
+        const float c = mac_forward(m, f);
+        const double len = (double)nd.len;
+        l2[i] = (float)(len * len * (double)exp10f(c - log_kappa));
+    }
+}
+
+}  // namespace
+
+void run_mac_node_scale(gt_context* ctx, const gt_tree* t, const float* dmodel, double kappa, float* l2) {
+    if (t->n_nodes <= 0) return;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(div_up(t->n_nodes, 256), ctx->num_sms * 4));
+    mac_node_scale_kernel<<<blocks, 256, 0, ctx->stream>>>(t->nodes, t->nq2, t->n_nodes, dmodel,
+                                                           (float)std::log10(kappa), l2);
+    check_launch(ctx, "mac_node_scale_kernel");
 }
 
 }  // namespace gt

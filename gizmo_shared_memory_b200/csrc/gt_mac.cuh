@@ -48,6 +48,19 @@ __device__ __forceinline__ void mac_features(double r2, double rho, double len, 
     f[7] = 0.5f * lg10f(ext2 / l2 + 1e-12);
 }
 
+// The node-only features of the per-node criterion (GT_MAC_NODE_FEATURES): the same definitions as
+// mac_features for features 1, 2 and 5; the pair features stay 0 (the model ignores them).
+__device__ __forceinline__ void mac_node_features(double len, double s, double mass, double q2, int count,
+                                                  float* f) {
+    const double l = fmax(len, 1e-300);
+    const double l2 = l * l;
+#pragma unroll
+    for (int i = 0; i < kMacIn; ++i) f[i] = 0.0f;
+    f[1] = lg10f(q2 / fmax(mass * l2, 1e-300) + 1e-12);
+    f[2] = lg10f((s - len) / l + 1e-6);
+    f[5] = lg10f((double)max(count, 1));
+}
+
 // MLP forward in FP32 on normalised features; `m` points at a model in shared or global memory.
 __device__ __forceinline__ float mac_forward(const float* __restrict__ m, const float* x) {
     float xn[kMacIn];

@@ -36,8 +36,8 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxWarps = 8;     // warps per block of the walk kernel
-constexpr int kPnCap = 256;      // monopole-list entries per warp
-constexpr int kPpCap = 128;      // particle-list entries per warp
+constexpr int kPnCapDefault = 256;  // monopole-list entries per warp (gt_walk_options.list_capacity)
+constexpr int kPnCapMax = 1024;     // the particle list holds half as many entries
 
 struct WalkArgs {
     const GNode* nodes;
@@ -55,10 +55,15 @@ struct WalkArgs {
     unsigned int* next_group;   // dynamic group counter
     unsigned long long* stats;  // [nodes, multipole, pairs_structural, zero_r2, flushes, max_stack, steps]
     int* error;                 // 1: stack overflow
+    int pn_cap, pp_cap;         // list capacities per warp (multiples of 32)
+    int warp_bytes;             // shared memory per warp: header + lists
     // learned criterion
     const float* mac_model;     // GT_MAC_MODEL_FLOATS on the device
     const float* nq2;           // node second moments
     double mac_band_lo, mac_band_hi, mac_log_kappa;
+    const float* mac_l2;        // GT_MAC_NODE: per-node L^2 10^(c - log10 kappa)
+    // forest: root node of each group (its system's root); null: node 0
+    const int* group_root;
 };
 
 __device__ __forceinline__ int warp_incl_scan_i(int v) {
@@ -116,13 +121,14 @@ __device__ __forceinline__ void load_src(const SrcP* __restrict__ p, double& x, 
 // soon as it holds and the last arm decides otherwise, so the test is the OR of the arms: softening
 // overlap, Barnes-Hut (theta > 0), relative criterion (aold > 0; with aold == 0 and no theta it
 // opens), inside-node.  Evaluated without branches so the lanes of a warp do not diverge.
-__device__ __forceinline__ bool open_node(double r2, double len, double l_open, double mass,
+// ml2 is the relative arm's M L^2 (with the per-node learned correction folded in, GT_MAC_NODE).
+__device__ __forceinline__ bool open_node(double r2, double len, double l_open, double ml2,
                                           double nsoft, double tsoft, double aold, double theta2,
                                           double dx, double dy, double dz) {
     const double rt = tsoft + 0.6 * len, rn = nsoft + 0.6 * len;
     const bool overlap = (r2 < rt * rt) | (r2 < rn * rn);
     const bool bh = (theta2 > 0.0) & (l_open * l_open >= theta2 * r2);
-    const bool rel = (aold > 0) ? (mass * len * len > r2 * r2 * aold) : (theta2 <= 0.0);
+    const bool rel = (aold > 0) ? (ml2 > r2 * r2 * aold) : (theta2 <= 0.0);
     const double lim = 0.6 * len;
     const bool inside = (dx < lim) & (dy < lim) & (dz < lim);
     return overlap | bh | rel | inside;
@@ -155,20 +161,24 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
     sum = t;
 }
 
-// Per-warp shared memory: the monopole list (float4: offset, mass), the particle list (float4 +
-// softening) and the leaf-expansion scratch.
-struct WarpSmem {
-    float4 pn[kPnCap];
-    float4 pp[kPpCap];
-    float ph[kPpCap];
-    int lo[32];
+// Per-warp shared memory: this header, then the monopole list (pn_cap float4: offset, mass) and
+// the particle list (pp_cap float4 + pp_cap float softenings).  The capacities are a launch
+// parameter (the autotuner trades list length against blocks per SM).
+struct alignas(16) WarpHdr {
+    int lo[32];   // leaf-expansion scratch
     int pre[32];
     // the group's FP64 state, read where needed instead of held in registers for the whole walk:
     // box low/high corners, centre, largest target softening, smallest aold
     double lo_x, lo_y, lo_z, hi_x, hi_y, hi_z, c_x, c_y, c_z, emax, amin;
 };
 
-template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT, bool MAC>
+__host__ __device__ constexpr int warp_smem_bytes(int pn_cap, int pp_cap) {
+    return ((int)sizeof(WarpHdr) + pn_cap * 16 + pp_cap * 20 + 15) & ~15;
+}
+
+// MAC: 0 plain relative criterion, 1 network inside the walk (GT_MAC_LEARNED), 2 per-node
+// learned scale (GT_MAC_NODE).
+template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT, int MAC>
 __global__ void __launch_bounds__(kMaxWarps * 32, TPL == 1 ? 3 : 2)
 walk_kernel(const WalkArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -176,16 +186,17 @@ walk_kernel(const WalkArgs A) {
     const unsigned lt_mask = (1u << lane) - 1u;
     const int gw = blockIdx.x * (blockDim.x >> 5) + w;
     int* __restrict__ stk = A.stack + (size_t)gw * A.stack_cap;
-    WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[w];
+    unsigned char* wbase = smem_raw + (size_t)w * A.warp_bytes;
+    WarpHdr& S = *reinterpret_cast<WarpHdr*>(wbase);
     // the learned criterion's network, one copy per block after the warps' lists
-    float* __restrict__ mac_w = reinterpret_cast<float*>(smem_raw + sizeof(WarpSmem) * (blockDim.x >> 5));
-    if (MAC) {
+    float* __restrict__ mac_w = reinterpret_cast<float*>(smem_raw + (size_t)A.warp_bytes * (blockDim.x >> 5));
+    if (MAC == 1) {
         for (int i = threadIdx.x; i < kMacModel; i += blockDim.x) mac_w[i] = A.mac_model[i];
         __syncthreads();
     }
-    float4* __restrict__ pn = S.pn;
-    float4* __restrict__ pp = S.pp;
-    float* __restrict__ ph = S.ph;
+    float4* __restrict__ pn = reinterpret_cast<float4*>(wbase + sizeof(WarpHdr));
+    float4* __restrict__ pp = pn + A.pn_cap;
+    float* __restrict__ ph = reinterpret_cast<float*>(pp + A.pp_cap);
 
     unsigned long long c_nodes = 0, c_multi = 0, c_pairs = 0, c_zero = 0, c_flush = 0, c_steps = 0;
     int c_maxtop = 0;
@@ -334,7 +345,7 @@ walk_kernel(const WalkArgs A) {
 
         // ---- traversal ----------------------------------------------------------------------
         int top = 1;
-        if (lane == 0) stk[0] = 0;
+        if (lane == 0) stk[0] = A.group_root ? A.group_root[g] : 0;
         __syncwarp();
         int npn = 0, npp = 0;
         bool overflow = false;
@@ -355,10 +366,12 @@ walk_kernel(const WalkArgs A) {
                 const double dz = fmax(0.0, fmax(S.lo_z - nd.cz, nd.cz - S.hi_z));
                 const double r2 = dx * dx + dy * dy + dz * dz;
                 bool open = true;
-                if (!MAC) {
-                    if (LEAF_ACCEPT || !leaf)
-                        open = open_node(r2, (double)nd.len, nd.s, nd.mass, (double)nd.soft, S.emax, S.amin,
-                                         A.theta2, dx, dy, dz);
+                if (MAC != 1) {
+                    if (LEAF_ACCEPT || !leaf) {
+                        const double len = (double)nd.len;
+                        const double ml2 = MAC == 2 ? nd.mass * (double)__ldg(A.mac_l2 + node) : nd.mass * len * len;
+                        open = open_node(r2, len, nd.s, ml2, (double)nd.soft, S.emax, S.amin, A.theta2, dx, dy, dz);
+                    }
                 } else if (LEAF_ACCEPT || !leaf) {
                     // learned criterion: the softening-overlap, inside-node and Barnes-Hut arms
                     // stay; the relative arm's estimate M L^2 / r^4 is corrected by the network
@@ -414,7 +427,7 @@ walk_kernel(const WalkArgs A) {
             const unsigned am = __ballot_sync(kFull, accept);
             if (am) {
                 const int na = __popc(am);
-                if (npn + na > kPnCap) { flush_pn(npn); npn = 0; }
+                if (npn + na > A.pn_cap) { flush_pn(npn); npn = 0; }
                 if (accept) {
                     const int pos = npn + __popc(am & lt_mask);
                     pn[pos] = make_float4((float)(nd.cx - S.c_x), (float)(nd.cy - S.c_y),
@@ -461,8 +474,8 @@ walk_kernel(const WalkArgs A) {
                     const unsigned fm = __ballot_sync(kFull, live && far);
                     const unsigned nm = __ballot_sync(kFull, live && !far);
                     const int nf = __popc(fm), nn = __popc(nm);
-                    if (npn + nf > kPnCap) { flush_pn(npn); npn = 0; }
-                    if (npp + nn > kPpCap) { flush_pp(npp); npp = 0; }
+                    if (npn + nf > A.pn_cap) { flush_pn(npn); npn = 0; }
+                    if (npp + nn > A.pp_cap) { flush_pp(npp); npp = 0; }
                     const float4 e = make_float4((float)(qx - S.c_x), (float)(qy - S.c_y), (float)(qz - S.c_z), qm);
                     if (live && far) {
                         pn[npn + __popc(fm & lt_mask)] = e;
@@ -568,7 +581,8 @@ __global__ void fill_group_id_kernel(const GNode* __restrict__ nodes, const int*
 __global__ void target_flags_kernel(const uint32_t* __restrict__ targets, int64_t nt, int mode,
                                     int param, const uint32_t* __restrict__ rank,
                                     const int* __restrict__ leaf_of, const int* __restrict__ gid,
-                                    uint32_t* __restrict__ tpos, uint32_t* __restrict__ flag) {
+                                    uint32_t* __restrict__ tpos, uint32_t* __restrict__ flag,
+                                    const int* __restrict__ sys_off, int n_systems, int all_live) {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nt;
          k += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t p = targets[k];
@@ -583,7 +597,15 @@ __global__ void target_flags_kernel(const uint32_t* __restrict__ targets, int64_
                 const int a = gid[pos], b = gid[rank[targets[k - 1]]];
                 start = a != b || a < 0;
             } else if (mode == GT_GROUP_BATCH) {
-                start = (k % param) == 0;
+                if (n_systems > 1) {
+                    // a window never spans two systems of a forest; over all live targets the
+                    // windows of each system start at its first particle, as in its own tree
+                    const int s = system_of(sys_off, n_systems, pos);
+                    start = s != system_of(sys_off, n_systems, rank[targets[k - 1]]) ||
+                            (all_live ? ((int64_t)pos - sys_off[s]) % param == 0 : (k % param) == 0);
+                } else {
+                    start = (k % param) == 0;
+                }
             } else {
                 start = true;
             }
@@ -616,6 +638,17 @@ __global__ void chunk_emit_kernel(const int64_t* __restrict__ starts, int64_t ng
         const int64_t s = starts[g], e = (g + 1 < ng) ? starts[g + 1] : n_end;
         int64_t o = coff[g];
         for (int64_t a = s; a < e; a += kmax, ++o) groups[o] = make_int2((int)a, (int)std::min<int64_t>(a + kmax, e));
+    }
+}
+
+// Forest: the root of each group is the root of the system of its first target (roots are
+// nodes 0 .. n_systems-1, groups never span two systems).
+__global__ void group_root_kernel(const int2* __restrict__ groups, int64_t ng, const uint32_t* __restrict__ tpos,
+                                  const int* __restrict__ sys_off, int n_systems, int* __restrict__ root) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ng;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const int t0 = groups[g].x;
+        root[g] = system_of(sys_off, n_systems, tpos ? (int64_t)tpos[t0] : (int64_t)t0);
     }
 }
 
@@ -665,18 +698,18 @@ int64_t finish_groups(gt_context* ctx, const uint32_t* flag, int64_t n, int kmax
     return nc;
 }
 
-size_t walk_smem(int warps, bool mac) {
-    return (size_t)warps * sizeof(WarpSmem) + (mac ? kMacModel * sizeof(float) : 0);
+size_t walk_smem(int warps, bool mac, int pn_cap) {
+    return (size_t)warps * warp_smem_bytes(pn_cap, pn_cap / 2) + (mac ? kMacModel * sizeof(float) : 0);
 }
 
 // Dynamic shared memory above 48 KB needs a per-kernel opt-in, done once per instantiation.
-template <int TPL, bool LA, bool POT, bool CNT, bool MAC>
+template <int TPL, bool LA, bool POT, bool CNT, int MAC>
 void prepare_walk() {
     static bool done = false;
     if (done) return;
     check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT, MAC>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)walk_smem(kMaxWarps, MAC)), "cudaFuncSetAttribute");
+                                    (int)walk_smem(kMaxWarps, MAC == 1, kPnCapMax)), "cudaFuncSetAttribute");
     // the lists need 3 blocks x 55 KB per SM: ask for the largest shared-memory carveout
     check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT, MAC>,
                                     cudaFuncAttributePreferredSharedMemoryCarveout, 100),
@@ -684,41 +717,44 @@ void prepare_walk() {
     done = true;
 }
 
-template <int TPL, bool LA, bool POT, bool CNT, bool MAC>
+template <int TPL, bool LA, bool POT, bool CNT, int MAC>
 void launch_walk(gt_context* ctx, const WalkArgs& a, int blocks, int warps) {
     prepare_walk<TPL, LA, POT, CNT, MAC>();
-    walk_kernel<TPL, LA, POT, CNT, MAC><<<blocks, warps * 32, walk_smem(warps, MAC), ctx->stream>>>(a);
+    walk_kernel<TPL, LA, POT, CNT, MAC><<<blocks, warps * 32, walk_smem(warps, MAC == 1, a.pn_cap), ctx->stream>>>(a);
     check_launch(ctx, "walk_kernel");
 }
 
-template <int TPL, bool LA, bool POT, bool MAC>
+template <int TPL, bool LA, bool POT, int MAC>
 void dispatch_count(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool cnt) {
     if (cnt) launch_walk<TPL, LA, POT, true, MAC>(ctx, a, blocks, warps);
     else launch_walk<TPL, LA, POT, false, MAC>(ctx, a, blocks, warps);
 }
 
-// The learned criterion is a grouped-walk option (leaves offered to the criterion).
+// The learned criteria are grouped-walk options (leaves offered to the criterion).
 template <int TPL>
 void dispatch(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la, bool pot, bool cnt,
-              bool mac) {
-    if (mac) {
-        if (pot) dispatch_count<TPL, true, true, true>(ctx, a, blocks, warps, cnt);
-        else dispatch_count<TPL, true, false, true>(ctx, a, blocks, warps, cnt);
+              int mac) {
+    if (mac == GT_MAC_LEARNED) {
+        if (pot) dispatch_count<TPL, true, true, 1>(ctx, a, blocks, warps, cnt);
+        else dispatch_count<TPL, true, false, 1>(ctx, a, blocks, warps, cnt);
+    } else if (mac == GT_MAC_NODE) {
+        if (pot) dispatch_count<TPL, true, true, 2>(ctx, a, blocks, warps, cnt);
+        else dispatch_count<TPL, true, false, 2>(ctx, a, blocks, warps, cnt);
     } else if (la) {
-        if (pot) dispatch_count<TPL, true, true, false>(ctx, a, blocks, warps, cnt);
-        else dispatch_count<TPL, true, false, false>(ctx, a, blocks, warps, cnt);
+        if (pot) dispatch_count<TPL, true, true, 0>(ctx, a, blocks, warps, cnt);
+        else dispatch_count<TPL, true, false, 0>(ctx, a, blocks, warps, cnt);
     } else {
-        if (pot) dispatch_count<TPL, false, true, false>(ctx, a, blocks, warps, cnt);
-        else dispatch_count<TPL, false, false, false>(ctx, a, blocks, warps, cnt);
+        if (pot) dispatch_count<TPL, false, true, 0>(ctx, a, blocks, warps, cnt);
+        else dispatch_count<TPL, false, false, 0>(ctx, a, blocks, warps, cnt);
     }
 }
 
-template <int TPL, bool LA, bool POT, bool CNT, bool MAC>
-int occupancy_blocks(int warps) {
+template <int TPL, bool LA, bool POT, bool CNT, int MAC>
+int occupancy_blocks(int warps, int pn_cap) {
     prepare_walk<TPL, LA, POT, CNT, MAC>();
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<TPL, LA, POT, CNT, MAC>, warps * 32,
-                                                  walk_smem(warps, MAC));
+                                                  walk_smem(warps, MAC == 1, pn_cap));
     return std::max(1, nb);
 }
 
@@ -745,11 +781,14 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
 
     // ---- groups -------------------------------------------------------------------------------
     int2* groups = nullptr;
+    int* roots = nullptr;
     int64_t ng = 0;
     const uint32_t* tpos = nullptr;
     if (all) {
         for (auto& c : t->group_cache)
-            if (c.mode == mode && c.param == param && c.kmax == kmax) { groups = c.groups; ng = c.n_groups; }
+            if (c.mode == mode && c.param == param && c.kmax == kmax) {
+                groups = c.groups; roots = c.roots; ng = c.n_groups;
+            }
         if (!groups) {
             const int64_t n = t->n_live;
             uint32_t* flag = (uint32_t*)scratch(ctx, kSlotTargets, (size_t)n * 4);
@@ -763,12 +802,24 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                 target_flags_kernel<<<grid1d(ctx, n), 256, 0, st>>>(
                     t->order, n, mode == GT_GROUP_BATCH ? GT_GROUP_BATCH : GT_GROUP_SINGLE, param,
                     t->rank, t->leaf_of, nullptr, (uint32_t*)scratch(ctx, kSlotGroupKey, (size_t)n * 4),
-                    flag);
+                    flag, t->sys_off_dev, t->n_systems, 1);
                 check_launch(ctx, "target_flags_kernel");
             }
             ng = finish_groups(ctx, flag, n, kmax, &groups, true);
+            if (t->n_systems > 1 && ng > 0) {
+                void* p = nullptr;
+                if (cudaMalloc(&p, (size_t)ng * sizeof(int)) != cudaSuccess) {
+                    cudaGetLastError();
+                    cudaFree(groups);
+                    throw Fail{GT_ERR_NOMEM, "cudaMalloc for the group roots failed"};
+                }
+                roots = (int*)p;
+                group_root_kernel<<<grid1d(ctx, ng), 256, 0, st>>>(groups, ng, nullptr, t->sys_off_dev,
+                                                                   t->n_systems, roots);
+                check_launch(ctx, "group_root_kernel");
+            }
             gt_tree::GroupCache c;
-            c.mode = mode; c.param = param; c.kmax = kmax; c.groups = groups; c.n_groups = ng;
+            c.mode = mode; c.param = param; c.kmax = kmax; c.groups = groups; c.roots = roots; c.n_groups = ng;
             t->group_cache.push_back(c);
         }
     } else {
@@ -783,10 +834,17 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
             check_launch(ctx, "fill_group_id_kernel");
         }
         target_flags_kernel<<<grid1d(ctx, nt), 256, 0, st>>>(rq.targets, nt, mode, param, t->rank,
-                                                             t->leaf_of, gid, tp, flag);
+                                                             t->leaf_of, gid, tp, flag, t->sys_off_dev,
+                                                             t->n_systems, 0);
         check_launch(ctx, "target_flags_kernel");
         ng = finish_groups(ctx, flag, nt, kmax, &groups, false);
         tpos = tp;
+        if (t->n_systems > 1 && ng > 0) {
+            roots = (int*)scratch(ctx, kSlotGroupRoot, (size_t)ng * sizeof(int));
+            group_root_kernel<<<grid1d(ctx, ng), 256, 0, st>>>(groups, ng, tpos, t->sys_off_dev, t->n_systems,
+                                                               roots);
+            check_launch(ctx, "group_root_kernel");
+        }
     }
     ctx->stats.groups = ng;
     if (ng <= 0) return;
@@ -794,17 +852,27 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     // ---- launch -------------------------------------------------------------------------------
     const int warps = (rq.block_warps > 0 && rq.block_warps <= kMaxWarps) ? rq.block_warps : kMaxWarps;
     const bool mac = rq.mac == GT_MAC_LEARNED;
+    const bool macn = rq.mac == GT_MAC_NODE;
+    int pn_cap = kPnCapDefault;
+    if (rq.list_capacity != 0) {
+        if (rq.list_capacity < 64 || rq.list_capacity > kPnCapMax || (rq.list_capacity & 31))
+            throw Fail{GT_ERR_INVALID, "list_capacity must be a multiple of 32 in [64, 1024]"};
+        pn_cap = rq.list_capacity;
+    }
     int per_sm;
     if (tpl == 1)
-        per_sm = mac ? occupancy_blocks<1, true, false, false, true>(warps)
-                     : (rq.leaf_accept ? occupancy_blocks<1, true, false, false, false>(warps)
-                                       : occupancy_blocks<1, false, false, false, false>(warps));
+        per_sm = mac ? occupancy_blocks<1, true, false, false, 1>(warps, pn_cap)
+               : macn ? occupancy_blocks<1, true, false, false, 2>(warps, pn_cap)
+                      : (rq.leaf_accept ? occupancy_blocks<1, true, false, false, 0>(warps, pn_cap)
+                                        : occupancy_blocks<1, false, false, false, 0>(warps, pn_cap));
     else if (tpl == 2)
-        per_sm = mac ? occupancy_blocks<2, true, false, false, true>(warps)
-                     : occupancy_blocks<2, true, false, false, false>(warps);
+        per_sm = mac ? occupancy_blocks<2, true, false, false, 1>(warps, pn_cap)
+               : macn ? occupancy_blocks<2, true, false, false, 2>(warps, pn_cap)
+                      : occupancy_blocks<2, true, false, false, 0>(warps, pn_cap);
     else
-        per_sm = mac ? occupancy_blocks<4, true, false, false, true>(warps)
-                     : occupancy_blocks<4, true, false, false, false>(warps);
+        per_sm = mac ? occupancy_blocks<4, true, false, false, 1>(warps, pn_cap)
+               : macn ? occupancy_blocks<4, true, false, false, 2>(warps, pn_cap)
+                      : occupancy_blocks<4, true, false, false, 0>(warps, pn_cap);
     const int64_t want_blocks = (ng + warps - 1) / warps;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want_blocks, (int64_t)per_sm * ctx->num_sms));
     int stack_cap = rq.stack_capacity > 0 ? rq.stack_capacity : 256 * std::max(1, t->n_levels) + 32;
@@ -826,27 +894,68 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     a.phi = rq.phi;
     a.out_map = (all && rq.out_original) ? t->order : nullptr;
     const int total_warps = blocks * warps;
-    unsigned long long* ctr = (unsigned long long*)scratch(ctx, kSlotCounters, 256);
+    a.pn_cap = pn_cap;
+    a.pp_cap = pn_cap / 2;
+    a.warp_bytes = warp_smem_bytes(a.pn_cap, a.pp_cap);
+    // a captured graph keeps its pointers: it runs on buffers its plan owns, not on the workspace
+    WalkBuffers* wb = rq.bufs;
+    auto own = [&](void** p, size_t& have, size_t need) {
+        if (have >= need) return;
+        if (rq.capture) throw Fail{GT_ERR_INVALID, "walk plan buffers changed size during capture"};
+        if (*p) { check_cuda(cudaStreamSynchronize(st), "sync"); cudaFree(*p); *p = nullptr; have = 0; }
+        check_cuda(cudaMalloc(p, need), "cudaMalloc walk plan buffer");
+        have = need;
+    };
+    unsigned long long* ctr;
+    if (wb) {
+        own((void**)&wb->ctr, wb->ctr_bytes, 256);
+        ctr = wb->ctr;
+    } else {
+        ctr = (unsigned long long*)scratch(ctx, kSlotCounters, 256);
+    }
     a.next_group = (unsigned int*)(ctr + 8);
     a.stats = ctr;
     a.error = (int*)(ctr + 9);
     const bool want_pot = rq.want_phi && rq.phi;
     a.mac_model = rq.mac_model;
     a.nq2 = t->nq2;
+    a.group_root = roots;
     a.mac_band_lo = rq.mac_band_lo;
     a.mac_band_hi = rq.mac_band_hi;
     a.mac_log_kappa = rq.mac_kappa > 0 ? std::log10(rq.mac_kappa) : -300.0;
-    if (mac && (!rq.mac_model || !rq.leaf_accept))
+    if ((mac || macn) && (!rq.mac_model || !rq.leaf_accept))
         throw Fail{GT_ERR_INVALID, "the learned criterion needs a model and a grouped walk"};
+    a.mac_l2 = nullptr;
+    if (macn) {
+        // the per-node correction is part of the walk: computed on the stream before it (and
+        // captured with it in a plan)
+        float* l2;
+        const size_t need = (size_t)std::max<int64_t>(t->n_nodes, 1) * sizeof(float);
+        if (wb) {
+            own((void**)&wb->mac_l2, wb->mac_l2_bytes, need);
+            l2 = wb->mac_l2;
+        } else {
+            l2 = (float*)scratch(ctx, kSlotMacL2, need);
+        }
+        run_mac_node_scale(ctx, t, rq.mac_model, rq.mac_kappa > 0 ? rq.mac_kappa : 1.0, l2);
+        a.mac_l2 = l2;
+    }
 
     for (int attempt = 0; attempt < 3; ++attempt) {
-        a.stack = (int*)scratch(ctx, kSlotStack, (size_t)total_warps * stack_cap * 4);
+        const size_t stack_bytes = (size_t)total_warps * stack_cap * 4;
+        if (wb) {
+            own((void**)&wb->stack, wb->stack_bytes, stack_bytes);
+            a.stack = wb->stack;
+        } else {
+            a.stack = (int*)scratch(ctx, kSlotStack, stack_bytes);
+        }
         a.stack_cap = stack_cap;
         check_cuda(cudaMemsetAsync(ctr, 0, 96, st), "memset counters");
-        check_cuda(cudaEventRecord(ctx->ev0, st), "event");
-        if (tpl == 1) dispatch<1>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, mac);
-        else if (tpl == 2) dispatch<2>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, mac);
-        else dispatch<4>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, mac);
+        if (!rq.capture) check_cuda(cudaEventRecord(ctx->ev0, st), "event");
+        if (tpl == 1) dispatch<1>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
+        else if (tpl == 2) dispatch<2>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
+        else dispatch<4>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
+        if (rq.capture) break;  // the default stack capacity is a proven bound
         check_cuda(cudaEventRecord(ctx->ev1, st), "event");
         if (!rq.count && attempt == 0 && rq.stack_capacity == 0) {
             // the default capacity is a proven bound: no read-back needed on the fast path

@@ -65,8 +65,15 @@ enum {
     GT_GROUP_NODE = 2,  /* consecutive targets sharing the deepest ancestor holding <= group_max particles */
     GT_GROUP_SINGLE = 3 /* one walk per target (accel / potential, tree.cc:528, 899) */
 };
-/* Opening criterion used inside the walk. */
-enum { GT_MAC_PLAIN = 0, GT_MAC_LEARNED = 1 };
+/* Opening criterion used inside the walk.
+ * GT_MAC_LEARNED: the network runs inside the walk for every (group, node) pair in the band.
+ * GT_MAC_NODE: the network sees only the node's own features (GT_MAC_NODE_FEATURES; every other
+ * feature must have inv_sd = 0 in the model, as gt_mac_train gives with that feature mask), so
+ * its correction is evaluated once per node before the walk and the walk itself costs what the
+ * plain one does: accept when M L^2 10^c(node) / kappa <= r^4 aold. */
+enum { GT_MAC_PLAIN = 0, GT_MAC_LEARNED = 1, GT_MAC_NODE = 2 };
+/* Features that depend on the node alone: second moment, COM offset, particle count. */
+#define GT_MAC_NODE_FEATURES ((1u << 1) | (1u << 2) | (1u << 5))
 /* Precision of gt_direct. */
 enum { GT_DIRECT_FP64 = 0, GT_DIRECT_FP32 = 1 };
 /* Output order of a walk over targets == NULL. */
@@ -74,6 +81,7 @@ enum { GT_OUT_TARGETS = 0, GT_OUT_ORIGINAL = 1 };
 
 typedef struct gt_context gt_context;
 typedef struct gt_tree gt_tree;
+typedef struct gt_plan gt_plan;
 
 /* Learned multipole-acceptance criterion: an MLP of 8 geometric features, 2 hidden layers of 32
  * (ReLU), one output, FP32.  A model is a flat host array of GT_MAC_MODEL_FLOATS floats:
@@ -104,7 +112,7 @@ typedef struct {
     int list_capacity;   /* interaction-list entries per warp; 0 = default */
     int stack_capacity;  /* node-stack entries per warp; 0 = default (always sufficient) */
     int dtype_out_f32;   /* reserved, must be 0 */
-    /* GT_MAC_LEARNED: the model (host array of GT_MAC_MODEL_FLOATS), the acceptance threshold
+    /* GT_MAC_LEARNED / GT_MAC_NODE: the model (host array of GT_MAC_MODEL_FLOATS), the acceptance threshold
      * kappa (accept when rho * 10^prediction <= kappa, rho = M L^2 / (r^4 aold)), and the band of
      * rho outside which the network is not consulted: rho <= mac_band[0] accepts, rho >
      * mac_band[1] opens.  The softening-overlap and inside-node arms always apply. */
@@ -119,6 +127,8 @@ typedef struct {
     double lr;       /* Adam step size (default 2e-3) */
     double tau;      /* quantile of the pinball loss (default 0.9: a conservative upper quantile) */
     uint64_t seed;   /* initialisation and shuffling (default 1) */
+    uint32_t feature_mask; /* features the network may read (bit i = feature i; default all 8).
+                              Masked features get mean 0 and inv_sd 0 in the model. */
 } gt_mac_train_options;
 
 typedef struct {
@@ -130,6 +140,7 @@ typedef struct {
     double center[3];   /* root cell centre */
     double side;        /* root cell side */
     double build_ms[7]; /* bbox, keys, sort, structure, moments, pack, total (device time) */
+    int64_t n_systems;  /* 1, or the number of systems of a forest (gt_build_systems) */
 } gt_tree_info;
 
 typedef struct {
@@ -177,6 +188,19 @@ GT_API int gt_launch_count(const gt_context* ctx, uint64_t* count);
 GT_API int gt_build(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
              const double* m, const double* soft, int mem, const gt_build_options* opt,
              gt_tree** out);
+/* Forest: n_systems independent systems built in one pass.  System s owns the input particles
+ * [offsets[s], offsets[s+1]) (host array of n_systems + 1; offsets[0] = 0, offsets[n_systems] = n,
+ * non-decreasing).  Each system gets its own root cell and tree exactly as gt_build would give it
+ * alone (same keys, order and cells); its root is node s and its live particles are the tree
+ * positions gt_tree_systems reports.  Walks on a forest keep every group inside one system and
+ * start it at that system's root, so all systems share one persistent walk launch.  No reference
+ * counterpart: shmem::build makes one tree per call (tree.cc:350). */
+GT_API int gt_build_systems(gt_context* ctx, int64_t n, int32_t n_systems, const int64_t* offsets,
+                     const double* x, const double* y, const double* z, const double* m,
+                     const double* soft, int mem, const gt_build_options* opt, gt_tree** out);
+/* Per-system live tree-position offsets (n_systems + 1) and root cells (4 doubles per system:
+ * centre x, y, z, side).  Either pointer may be null. */
+GT_API int gt_tree_systems(const gt_tree* tree, int64_t* live_offsets, double* roots);
 GT_API int gt_tree_free(gt_tree* tree);
 GT_API int gt_tree_info_get(const gt_tree* tree, gt_tree_info* info);
 /* Copy the tree to host arrays in the reference's layout: orderbuf (n_live), rank (n; UINT32_MAX
@@ -197,6 +221,19 @@ GT_API int gt_accel_grouped(gt_context* ctx, const gt_tree* tree, int64_t n_targ
                      const uint32_t* targets, const double* aold, double theta, double G, int batch,
                      const gt_walk_options* opt, int mem, double* ax, double* ay, double* az,
                      double* phi);
+/* Walk plan: the all-active grouped walk of gt_accel_grouped (targets = NULL) captured once as a
+ * CUDA graph and replayed by gt_plan_launch on the context stream, asynchronously.  aold and the
+ * outputs are DEVICE arrays whose addresses are fixed at creation (update their contents between
+ * launches); the plan owns its stack and counters, so other calls on the context cannot move
+ * them.  The tree, the arrays and the context must outlive the plan.  On a forest
+ * (gt_build_systems) one replay walks every system in one persistent launch.  opt->count and
+ * opt->stack_capacity are not allowed.  No reference counterpart (the engine calls
+ * shmem::accel_grouped once per step, mfm.cc:782). */
+GT_API int gt_plan_create(gt_context* ctx, const gt_tree* tree, const double* aold, double theta,
+                   double G, int batch, const gt_walk_options* opt, double* ax, double* ay,
+                   double* az, double* phi, gt_plan** out);
+GT_API int gt_plan_launch(gt_plan* plan);
+GT_API int gt_plan_destroy(gt_plan* plan);
 /* Per-target walk (leaves always direct-summed).  Replaces shmem::accel (tree.h:392-394,
  * tree.cc:528-582). */
 GT_API int gt_accel(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
@@ -207,6 +244,51 @@ GT_API int gt_potential(gt_context* ctx, const gt_tree* tree, int64_t n_targets,
                  double theta, double G, const double* aold, int mem, double* phi);
 /* Counts and device time of the last walk on this context (SHMEM_COUNT_WALK, tree.cc:671-677). */
 GT_API int gt_walk_stats_get(const gt_context* ctx, gt_walk_stats* stats);
+
+/* ---- autotuner ----------------------------------------------------------------------------- */
+/* One candidate launch configuration of the all-active grouped walk and what it measured. */
+typedef struct {
+    int group_mode;     /* GT_GROUP_BATCH, GT_GROUP_NODE or GT_GROUP_LEAF */
+    int group_size;     /* window (batch) or group_max (node groups); 0 for leaf groups */
+    int block_warps;    /* warps per block */
+    int list_capacity;  /* monopole-list entries per warp (the particle list holds half) */
+    int mac;            /* GT_MAC_PLAIN or GT_MAC_LEARNED */
+    double mac_kappa;   /* learned threshold (GT_MAC_LEARNED) */
+    double ms;          /* median device time of the timed walks */
+    double p99;         /* sampled p99 relative force error; -1 without a sample */
+    double median;      /* sampled median relative force error; -1 without a sample */
+    int accepted;       /* p99 <= p99_max (1 without a sample) */
+} gt_tune_entry;
+
+typedef struct {
+    int reps;                 /* timed walks per candidate (default 3) */
+    double p99_max;           /* sampled-error target (default 5e-3) */
+    int64_t n_sample;         /* sampled targets; 0 = no error check */
+    const uint32_t* sample;   /* host, particle indices of the sample */
+    const double* ref_ax;     /* host, FP64 reference accelerations of the sample (gt_direct) */
+    const double* ref_ay;
+    const double* ref_az;
+    const float* mac_model;   /* optional learned criterion to try (host, GT_MAC_MODEL_FLOATS) */
+    int n_kappa;              /* thresholds of the learned criterion to try */
+    const double* kappa;      /* host, n_kappa */
+    double mac_band[2];       /* band of the learned criterion (gt_walk_options.mac_band) */
+    int mac_mode;             /* GT_MAC_LEARNED (0 = default) or GT_MAC_NODE */
+} gt_tune_options;
+
+GT_API void gt_tune_options_default(gt_tune_options* opt);
+/* Pick the launch configuration of the all-active grouped walk of `tree` by measurement: group
+ * shape and size (windows 16-128, node groups, leaf groups), then warps per block and interaction-
+ * list capacity for the two fastest shapes, then -- when a model is given -- the learned criterion
+ * at each kappa on the fastest configuration.  With a sample, a candidate is accepted only if its
+ * sampled p99 error is at most p99_max, so the learned criterion replaces the plain one only
+ * where it is both accepted and faster; the plain criterion stays the fallback.  `best` receives
+ * the fastest accepted candidate as walk options (with *best_batch the window for
+ * gt_accel_grouped), or the most accurate one if none is accepted.  aold is in tree order (as the
+ * all-active walk takes it).  entries (may be NULL) receive up to max_entries measured candidates.
+ * No reference counterpart. */
+GT_API int gt_autotune(gt_context* ctx, const gt_tree* tree, const double* aold, int mem, double theta,
+                double G, const gt_tune_options* opt, gt_walk_options* best, int* best_batch,
+                gt_tune_entry* entries, int max_entries, int* n_entries);
 
 /* aold[i] = alpha * |a_i| / G, the relative-criterion input the engine forms from the previous
  * force (shmem/mfm.cc:743-751). */

@@ -1,0 +1,154 @@
+"""Forests: many independent systems of uneven N built in one pass (gt_build_systems) and walked in
+one launch.  Each system must come out exactly as if it had been built and walked alone with
+gt_build: the same keys, order and cells, and bit-identical accelerations (the walk visits the same
+nodes in the same order, only the node numbering differs), for windowed, leaf and explicit-target
+walks.  Systems include an empty one and one with massless particles."""
+import numpy as np
+import pytest
+
+import gizmo_shared_memory_b200 as g
+from gizmo_shared_memory_b200 import ics
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def batch():
+    P, off, meta = ics.plummer_batch(n_systems=12, n_min=200, n_max=20000, n_total=60000, seed=7,
+                                     spacing=50.0)
+    # make system 3 empty and give system 5 some massless particles
+    ns = np.diff(off)
+    keep = np.ones(len(P["m"]), bool)
+    keep[off[3]:off[4]] = False
+    P = {k: v[keep] for k, v in P.items()}
+    ns[3] = 0
+    off = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
+    P["m"] = P["m"].copy()
+    P["m"][off[5]:off[6]:7] = 0.0
+    return P, off
+
+
+def split(P, off, s):
+    return {k: v[off[s]:off[s + 1]] for k, v in P.items()}
+
+
+@pytest.fixture(scope="module")
+def forest(gpu_ctx, batch):
+    P, off = batch
+    F = gpu_ctx.build(P, key_mode=g.GT_KEY_MORTON, offsets=off)
+    trees = [gpu_ctx.build(split(P, off, s), key_mode=g.GT_KEY_MORTON) for s in range(len(off) - 1)]
+    return F, trees
+
+
+def test_forest_structure_matches_separate_builds(gpu_ctx, batch, forest):
+    P, off = batch
+    F, trees = forest
+    S = len(off) - 1
+    inf = F.info()
+    assert inf["n_systems"] == S
+    live, roots = F.systems()
+    nl = [t.info()["n_live"] for t in trees]
+    assert np.array_equal(np.diff(live), nl)
+    assert inf["n_live"] == sum(nl)
+    assert inf["n_nodes"] == sum(t.info()["n_nodes"] for t in trees)
+    d = F.download(nodes=True)
+    keys = F.keys()
+    for s, t in enumerate(trees):
+        ti = t.info()
+        if ti["n_live"] > 0:
+            assert np.allclose(roots[s, :3], ti["center"], rtol=0, atol=0)
+            assert roots[s, 3] == ti["side"]
+        ds = t.download(nodes=False)
+        seg = d["orderbuf"][live[s]:live[s + 1]].astype(np.int64) - off[s]
+        assert np.array_equal(seg, ds["orderbuf"].astype(np.int64))
+        assert np.array_equal(keys[live[s]:live[s + 1]], t.keys())
+        # root s covers exactly this system's live particles
+        assert d["plo"][s] == live[s] and d["phi"][s] == live[s + 1]
+        assert d["parent"][s] == -1
+
+
+@pytest.mark.parametrize("mode,batch_size", [(g.GT_GROUP_BATCH, 32), (g.GT_GROUP_LEAF, 0),
+                                             (g.GT_GROUP_BATCH, 64)])
+def test_forest_walk_bit_identical(gpu_ctx, batch, forest, mode, batch_size):
+    P, off = batch
+    F, trees = forest
+    live, _ = F.systems()
+    kw = dict(group_mode=mode, batch=batch_size, out_order=g.GT_OUT_ORIGINAL)
+    fx, fy, fz = gpu_ctx.accel_grouped(F, None, theta=0.7, **kw)
+    for s, t in enumerate(trees):
+        if live[s + 1] == live[s]:
+            continue
+        sx, sy, sz = gpu_ctx.accel_grouped(t, None, theta=0.7, **kw)
+        m = P["m"][off[s]:off[s + 1]] > 0
+        for a, b in ((fx, sx), (fy, sy), (fz, sz)):
+            assert np.array_equal(a[off[s]:off[s + 1]][m], b[m])
+
+
+def test_forest_relative_criterion_and_targets(gpu_ctx, batch, forest):
+    """Relative criterion with per-target aold, and an explicit target list that visits the
+    systems out of order (leaf groups): identical to the separate walks."""
+    P, off = batch
+    F, trees = forest
+    S = len(off) - 1
+    rng = np.random.default_rng(3)
+    fx, fy, fz = gpu_ctx.accel_grouped(F, None, theta=0.7, group_mode=g.GT_GROUP_BATCH, batch=32,
+                                       out_order=g.GT_OUT_ORIGINAL)
+    aold_all = gpu_ctx.form_aold(fx, fy, fz, 0.005)
+    order = rng.permutation(S)
+    tl, al, ref = [], [], []
+    for s in order:
+        idx = np.nonzero(P["m"][off[s]:off[s + 1]] > 0)[0]
+        if len(idx) == 0:
+            continue
+        sub = np.sort(rng.choice(idx, size=max(1, len(idx) // 3), replace=False)).astype(np.uint32)
+        a = aold_all[off[s] + sub]
+        r = gpu_ctx.accel_grouped(trees[s], sub, aold=a, group_mode=g.GT_GROUP_LEAF)
+        tl.append(sub + np.uint32(off[s]))
+        al.append(a)
+        ref.append(np.stack(r))
+    got = gpu_ctx.accel_grouped(F, np.concatenate(tl), aold=np.concatenate(al), group_mode=g.GT_GROUP_LEAF)
+    assert np.array_equal(np.stack(got), np.concatenate(ref, axis=1))
+
+
+def test_forest_accuracy_vs_direct(gpu_ctx, batch, forest):
+    P, off = batch
+    F, _ = forest
+    fx, fy, fz = gpu_ctx.accel_grouped(F, None, theta=0.7, group_mode=g.GT_GROUP_BATCH, batch=32,
+                                       out_order=g.GT_OUT_ORIGINAL)
+    aold = gpu_ctx.form_aold(fx, fy, fz, 0.005)
+    m = P["m"] > 0
+    aold = np.where(m, aold, 0.0)
+    live_idx = np.nonzero(m)[0].astype(np.uint32)
+    ax, ay, az = gpu_ctx.accel_grouped(F, live_idx, aold=aold[live_idx], group_mode=g.GT_GROUP_BATCH,
+                                       batch=32)
+    errs = []
+    for s in range(len(off) - 1):
+        sel = live_idx[(live_idx >= off[s]) & (live_idx < off[s + 1])]
+        if len(sel) == 0:
+            continue
+        pos = np.searchsorted(live_idx, sel)
+        sample = sel[:: max(1, len(sel) // 64)]
+        ps = np.searchsorted(live_idx, sample)
+        dx, dy, dz = gpu_ctx.direct(split(P, off, s), (sample - off[s]).astype(np.uint32), want_phi=False)[:3]
+        d = np.sqrt((ax[ps] - dx) ** 2 + (ay[ps] - dy) ** 2 + (az[ps] - dz) ** 2)
+        errs.append(d / np.sqrt(dx * dx + dy * dy + dz * dz))
+        assert len(pos) == len(sel)
+    e = np.concatenate(errs)
+    assert np.median(e) < 5e-3 and np.quantile(e, 0.99) < 2e-2
+
+
+def test_forest_bad_offsets(gpu_ctx, batch):
+    P, off = batch
+    bad = off.copy()
+    bad[-1] -= 1
+    with pytest.raises(g.GTError) as e:
+        gpu_ctx.build(P, offsets=bad)
+    assert e.value.status == 1
+    bad = off.copy()
+    bad[2], bad[3] = bad[3], bad[2]
+    if bad[2] != bad[3]:
+        with pytest.raises(g.GTError):
+            gpu_ctx.build(P, offsets=bad)
+    # the context stays usable
+    T = gpu_ctx.build(split(P, off, 0))
+    assert T.info()["n_live"] > 0
