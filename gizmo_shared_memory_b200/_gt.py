@@ -39,6 +39,7 @@ EXPORTS = [
     "gt_measure_peaks", "gt_direct_noalloc", "gt_mac_train_options_default", "gt_mac_sample",
     "gt_mac_train", "gt_mac_predict", "gt_mac_gradient", "gt_build_systems", "gt_tree_systems",
     "gt_plan_create", "gt_plan_launch", "gt_plan_destroy", "gt_tune_options_default", "gt_autotune",
+    "gt_accel_grouped_ext", "gt_tree_velocities", "gt_tree_velocity_moments",
 ]
 
 
@@ -139,6 +140,10 @@ def load_library(path: str = LIB_PATH):
     L.gt_accel_grouped.argtypes = [vp, vp, i64, vp, vp, d, d, C.c_int, C.POINTER(WalkOptions),
                                    C.c_int, vp, vp, vp, vp]
     L.gt_accel.argtypes = [vp, vp, i64, vp, d, d, vp, C.c_int, vp, vp, vp]
+    L.gt_accel_grouped_ext.argtypes = [vp, vp, i64, vp, vp, d, d, C.c_int, C.POINTER(WalkOptions),
+                                       C.c_int, vp, vp, vp, vp, vp, vp]
+    L.gt_tree_velocities.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_int]
+    L.gt_tree_velocity_moments.argtypes = [vp, vp, vp, vp, vp, vp]
     L.gt_potential.argtypes = [vp, vp, i64, vp, d, d, vp, C.c_int, vp]
     L.gt_walk_stats_get.argtypes = [vp, C.POINTER(WalkStats)]
     L.gt_form_aold.argtypes = [vp, i64, vp, vp, vp, d, d, C.c_int, vp]
@@ -513,6 +518,40 @@ class Context:
             ax, ay, az = ax[:nt], ay[:nt], az[:nt]
             phi = phi[:nt] if phi is not None else None
         return (ax, ay, az, phi) if want_phi else (ax, ay, az)
+
+    def accel_grouped_ext(self, tree: Tree, targets=None, aold=None, theta=0.0, G=1.0, batch=0, tidal=True,
+                          jerk=False, want_phi=False, **opts):
+        """Grouped walk with the tidal tensor ([nt, 6]: xx yy zz xy yz xz, not times G) and the
+        jerk ([nt, 3]); host arrays.  Returns (ax, ay, az, phi, tidal, jerk)."""
+        t, nt = self._targets(targets)
+        if t is None:
+            nt = tree.info()["n_live"] if opts.get("out_order", 0) == GT_OUT_TARGETS else tree.info()["n"]
+        o = self._walk_opts(**opts)
+        ax, ay, az, phi = self._outs(nt, False, True, want_phi)
+        tt = np.empty((max(nt, 1), 6)) if tidal else None
+        jj = np.empty((max(nt, 1), 3)) if jerk else None
+        ao = np.ascontiguousarray(aold, np.float64) if aold is not None else None
+        self._check(load_library().gt_accel_grouped_ext(
+            self.h, tree.h, nt if targets is not None else 0, _ptr(t), _ptr(ao), theta, G, batch, C.byref(o),
+            GT_MEM_HOST, _ptr(ax), _ptr(ay), _ptr(az), _ptr(phi), _ptr(tt), _ptr(jj)))
+        cut = lambda a: None if a is None else a[:nt]
+        return cut(ax), cut(ay), cut(az), cut(phi), cut(tt), cut(jj)
+
+    def tree_velocities(self, tree: Tree, vx, vy, vz, particles_only=False):
+        """Attach velocities (indexed like the build input): node vcom and vmax, for the jerk."""
+        dev = _is_dev(vx)
+        if not dev:
+            vx, vy, vz = (np.ascontiguousarray(a, np.float64) for a in (vx, vy, vz))
+        self._check(load_library().gt_tree_velocities(self.h, tree.h, _ptr(vx), _ptr(vy), _ptr(vz),
+                                                      int(particles_only), GT_MEM_DEVICE if dev else GT_MEM_HOST))
+
+    def velocity_moments(self, tree: Tree):
+        nn = tree.info()["n_nodes"]
+        v = [np.empty(max(nn, 1)) for _ in range(3)]
+        vmax = np.empty(max(nn, 1), np.float32)
+        self._check(load_library().gt_tree_velocity_moments(self.h, tree.h, _ptr(v[0]), _ptr(v[1]), _ptr(v[2]),
+                                                            _ptr(vmax)))
+        return [a[:nn] for a in v], vmax[:nn]
 
     def accel(self, tree: Tree, targets=None, theta=0.0, G=1.0, aold=None):
         t, nt = self._targets(targets)

@@ -121,7 +121,7 @@ void check_mem(int mem) {
 void free_tree_arrays(gt_tree* t) {
     void* ptrs[] = {t->src, t->ssoft, t->smass, t->order, t->rank, t->leaf_of, t->sleaf, t->skey,
                     t->nodes, t->parent, t->next, t->level, t->size, t->delta, t->nsoft, t->gc,
-                    t->nq2, t->sys_off_dev, t->geom_dev};
+                    t->nq2, t->sys_off_dev, t->geom_dev, t->svel, t->nvel, t->vcom, t->vmax};
     // tree arrays came from the stream-ordered pool: hand them back to it (callers have synchronised)
     for (void* p : ptrs)
         if (p) cudaFreeAsync(p, 0);
@@ -145,7 +145,8 @@ void record_walk_time(gt_context* ctx) {
 void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
                  const double* aold, double theta, double G, int group_mode, int group_param,
                  bool leaf_accept, const gt_walk_options* opt, int mem, double* ax, double* ay,
-                 double* az, double* phi, WalkBuffers* bufs = nullptr, bool capture = false) {
+                 double* az, double* phi, WalkBuffers* bufs = nullptr, bool capture = false,
+                 double* tidal = nullptr, double* jerk = nullptr) {
     if (!ctx || !tree) throw Fail{GT_ERR_INVALID, "null context or tree"};
     check_mem(mem);
     if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "tree and context are on different devices"};
@@ -215,15 +216,19 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     rq.capture = capture;
     if ((ax == nullptr) != (ay == nullptr) || (ax == nullptr) != (az == nullptr))
         throw Fail{GT_ERR_INVALID, "ax, ay, az must all be given or all be null"};
-    if (!ax && !phi) return;
+    if (!ax && !phi && !tidal && !jerk) return;
     rq.ax = out_buf(ctx, kSlotOut0, ax, nout, mem);
     rq.ay = out_buf(ctx, kSlotOut1, ay, nout, mem);
     rq.az = out_buf(ctx, kSlotOut2, az, nout, mem);
     rq.phi = out_buf(ctx, kSlotOut3, phi, nout, mem);
+    rq.tidal = out_buf(ctx, kSlotOut4, tidal, nout * 6, mem);
+    rq.jerk = out_buf(ctx, kSlotOut5, jerk, nout * 3, mem);
     if (rq.out_original && nout > nt) {
         // massless particles are not walked; their outputs are defined as 0
         for (double* p : {rq.ax, rq.ay, rq.az, rq.phi})
             if (p) check_cuda(cudaMemsetAsync(p, 0, (size_t)nout * 8, ctx->stream), "memset");
+        if (rq.tidal) check_cuda(cudaMemsetAsync(rq.tidal, 0, (size_t)nout * 48, ctx->stream), "memset");
+        if (rq.jerk) check_cuda(cudaMemsetAsync(rq.jerk, 0, (size_t)nout * 24, ctx->stream), "memset");
     }
     run_walk(ctx, tree, rq);
     if (capture) return;
@@ -231,6 +236,8 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     copy_out(ctx, ay, rq.ay, nout, mem);
     copy_out(ctx, az, rq.az, nout, mem);
     copy_out(ctx, phi, rq.phi, nout, mem);
+    copy_out(ctx, tidal, rq.tidal, nout * 6, mem);
+    copy_out(ctx, jerk, rq.jerk, nout * 3, mem);
     const bool sync = mem == GT_MEM_HOST || !o.async;
     finish(ctx, sync);
     if (sync) record_walk_time(ctx);
@@ -617,6 +624,65 @@ int gt_autotune(gt_context* ctx, const gt_tree* tree, const double* aold, int me
         if (entries)
             for (int i = 0; i < k; ++i) entries[i] = all[i];
         if (n_entries) *n_entries = entries ? k : (int)all.size();
+    });
+}
+
+int gt_accel_grouped_ext(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
+                         const double* aold, double theta, double G, int batch, const gt_walk_options* opt,
+                         int mem, double* ax, double* ay, double* az, double* phi, double* tidal,
+                         double* jerk) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        gt_walk_options o;
+        gt_walk_options_default(&o);
+        if (opt) o = *opt;
+        int mode = o.group_mode, param = 0;
+        if (mode == GT_GROUP_LEAF && batch > 0) mode = GT_GROUP_BATCH;
+        if (mode == GT_GROUP_BATCH) param = batch > 0 ? batch : 8;
+        if (mode == GT_GROUP_NODE) param = o.group_max;
+        if (mode < GT_GROUP_LEAF || mode > GT_GROUP_NODE) throw Fail{GT_ERR_INVALID, "unknown group_mode"};
+        walk_common(ctx, tree, n_targets, targets, aold, theta, G, mode, param, true, &o, mem, ax, ay, az, phi,
+                    nullptr, false, tidal, jerk);
+    });
+}
+
+int gt_tree_velocities(gt_context* ctx, gt_tree* tree, const double* vx, const double* vy, const double* vz,
+                       int particles_only, int mem) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (!tree || (tree->n > 0 && (!vx || !vy || !vz))) throw Fail{GT_ERR_INVALID, "null tree or velocity"};
+        if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "tree and context are on different devices"};
+        DeviceGuard dg(ctx->device);
+        const double* dx = stage_in(ctx, kSlotIn0, vx, tree->n, mem);
+        const double* dy = stage_in(ctx, kSlotIn1, vy, tree->n, mem);
+        const double* dz = stage_in(ctx, kSlotIn2, vz, tree->n, mem);
+        if (particles_only && !tree->svel) throw Fail{GT_ERR_INVALID, "no node velocities to keep yet"};
+        tree_velocities(ctx, tree, dx, dy, dz, particles_only != 0);
+        finish(ctx, true);
+    });
+}
+
+int gt_tree_velocity_moments(gt_context* ctx, const gt_tree* t, double* vcx, double* vcy, double* vcz,
+                             float* vmax) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        if (!t) throw Fail{GT_ERR_INVALID, "null tree"};
+        if (!t->vcom) throw Fail{GT_ERR_INVALID, "no velocities attached (gt_tree_velocities)"};
+        DeviceGuard dg(ctx->device);
+        const int64_t nn = t->n_nodes;
+        std::vector<double> v((size_t)std::max<int64_t>(nn, 1) * 3);
+        if (nn > 0) {
+            check_cuda(cudaMemcpyAsync(v.data(), t->vcom, (size_t)nn * 24, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+            if (vmax)
+                check_cuda(cudaMemcpyAsync(vmax, t->vmax, (size_t)nn * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        }
+        finish(ctx, true);
+        for (int64_t i = 0; i < nn; ++i) {
+            if (vcx) vcx[i] = v[3 * i];
+            if (vcy) vcy[i] = v[3 * i + 1];
+            if (vcz) vcz[i] = v[3 * i + 2];
+        }
     });
 }
 

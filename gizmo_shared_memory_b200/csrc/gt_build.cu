@@ -495,6 +495,52 @@ __global__ void peano_keys_kernel(const double* __restrict__ x, const double* __
     }
 }
 
+// ---- velocities: particle velocities in tree order, node centre-of-mass velocity and speed bound
+// (tree.cc:149-190: leaves from their particles, interior nodes from their children) -------------
+__global__ void gather_vel_kernel(const double* __restrict__ vx, const double* __restrict__ vy,
+                                  const double* __restrict__ vz, const uint32_t* __restrict__ order,
+                                  int64_t n_live, float4* __restrict__ svel) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_live;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = order[i];
+        svel[i] = make_float4((float)vx[p], (float)vy[p], (float)vz[p], 0.0f);
+    }
+}
+
+__global__ void vel_moments_kernel(const GNode* __restrict__ nodes, const double* __restrict__ smass,
+                                   const uint32_t* __restrict__ order, const double* __restrict__ vx,
+                                   const double* __restrict__ vy, const double* __restrict__ vz, int64_t a,
+                                   int64_t b, double* __restrict__ vcom, float4* __restrict__ nvel,
+                                   float* __restrict__ vmax) {
+    const int lane = threadIdx.x & 31;
+    const int64_t i = a + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    if (i >= b) return;
+    const GNode nd = nodes[i];
+    double px = 0, py = 0, pz = 0, vm = 0;
+    if (nd.first < 0) {
+        for (int j = nd.plo + lane; j < nd.phi; j += 32) {
+            const uint32_t p = order[j];
+            const double m = smass[j], ux = vx[p], uy = vy[p], uz = vz[p];
+            px += m * ux; py += m * uy; pz += m * uz;
+            vm = fmax(vm, sqrt(ux * ux + uy * uy + uz * uz));
+        }
+    } else if (lane < nd.nchild) {
+        const int c = nd.first + lane;
+        const double m = nodes[c].mass;
+        px = m * vcom[3 * c]; py = m * vcom[3 * c + 1]; pz = m * vcom[3 * c + 2];
+        vm = (double)vmax[c];
+    }
+    px = warp_sum_d(px); py = warp_sum_d(py); pz = warp_sum_d(pz);
+    vm = warp_max_d(vm);
+    if (lane == 0) {
+        const double M = nd.mass;
+        const double ux = M > 0 ? px / M : 0.0, uy = M > 0 ? py / M : 0.0, uz = M > 0 ? pz / M : 0.0;
+        vcom[3 * i] = ux; vcom[3 * i + 1] = uy; vcom[3 * i + 2] = uz;
+        nvel[i] = make_float4((float)ux, (float)uy, (float)uz, 0.0f);
+        vmax[i] = (float)vm;
+    }
+}
+
 __global__ void form_aold_kernel(const double* __restrict__ ax, const double* __restrict__ ay,
                                  const double* __restrict__ az, int64_t n, double alpha, double G,
                                  double* __restrict__ aold) {
@@ -725,6 +771,28 @@ void run_peano_keys(gt_context* ctx, int64_t n, const double* x, const double* y
                                                                   corner[2], len, bits, ph_hi, ph_lo,
                                                                   mo_hi, mo_lo);
     check_launch(ctx, "peano_keys_kernel");
+}
+
+void tree_velocities(gt_context* ctx, gt_tree* t, const double* vx, const double* vy, const double* vz,
+                     bool particles_only) {
+    cudaStream_t st = ctx->stream;
+    const int64_t nl = std::max<int64_t>(t->n_live, 1), nn = std::max<int64_t>(t->n_nodes, 1);
+    if (!t->svel) {
+        t->svel = dalloc<float4>((size_t)nl, st);
+        t->nvel = dalloc<float4>((size_t)nn, st);
+        t->vcom = dalloc<double>((size_t)nn * 3, st);
+        t->vmax = dalloc<float>((size_t)nn, st);
+    }
+    if (t->n_live > 0) {
+        gather_vel_kernel<<<grid_for(ctx, t->n_live), kBlk, 0, st>>>(vx, vy, vz, t->order, t->n_live, t->svel);
+        check_launch(ctx, "gather_vel_kernel");
+    }
+    for (int L = t->n_levels - 1; L >= 0 && !particles_only; --L) {
+        const int64_t a = t->lvl_off[L], b = t->lvl_off[L + 1];
+        vel_moments_kernel<<<div_up((b - a) * 32, kBlk), kBlk, 0, st>>>(t->nodes, t->smass, t->order, vx, vy, vz, a,
+                                                                       b, t->vcom, t->nvel, t->vmax);
+        check_launch(ctx, "vel_moments_kernel");
+    }
 }
 
 void run_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay,

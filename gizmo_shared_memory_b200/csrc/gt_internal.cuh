@@ -118,6 +118,12 @@ struct gt_tree {
     double* nsoft = nullptr;     // node_cap, FP64 max softening
     float* nq2 = nullptr;        // node_cap, second mass moment about the COM (learned criterion)
     double* gc = nullptr;        // node_cap * 3, geometric centres
+    // velocities (gt_tree_velocities): per particle in tree order, per-node centre-of-mass
+    // velocity (FP64 for download, float4 for the walk's jerk) and speed bound
+    float4* svel = nullptr;      // n_live
+    float4* nvel = nullptr;      // n_nodes
+    double* vcom = nullptr;      // 3 * n_nodes
+    float* vmax = nullptr;       // n_nodes
     // cached all-active group lists, keyed by (mode, param)
     struct GroupCache {
         int mode = -1, param = 0, kmax = 0;
@@ -137,7 +143,7 @@ enum Slot {
     kSlotHist, kSlotScanA, kSlotScanB, kSlotPartials,
     kSlotNodeTmp0, kSlotNodeTmp1, kSlotNodeTmp2,
     kSlotTargets, kSlotAold, kSlotGroupKey, kSlotGroupsA, kSlotGroupsB,
-    kSlotOut0, kSlotOut1, kSlotOut2, kSlotOut3,
+    kSlotOut0, kSlotOut1, kSlotOut2, kSlotOut3, kSlotOut4, kSlotOut5,
     kSlotStack, kSlotCounters, kSlotDirect, kSlotGroupRoot, kSlotMacL2,
     kSlotCount
 };
@@ -198,6 +204,8 @@ struct WalkRequest {
     WalkBuffers* bufs = nullptr;  // plan-owned buffers; null: the context workspace
     bool capture = false;         // being captured into a graph: no events, no read-back
     double *ax = nullptr, *ay = nullptr, *az = nullptr, *phi = nullptr;  // device outputs
+    double* tidal = nullptr;  // 6 per target (xx yy zz xy yz xz), not times G
+    double* jerk = nullptr;   // 3 per target, times G
 };
 void run_walk(gt_context* ctx, const gt_tree* t, const WalkRequest& rq);
 
@@ -240,6 +248,10 @@ void run_mac_node_scale(gt_context* ctx, const gt_tree* t, const float* dmodel, 
 
 // Peak probe (gt_peak.cu)
 void run_peaks(gt_context* ctx, double* fp32_tflops, double* fp64_tflops);
+// Per-particle velocities in tree order and the per-node centre-of-mass velocity and speed bound
+// (gt_tree_velocities); vx, vy, vz are device arrays over the tree's input particles.
+void tree_velocities(gt_context* ctx, gt_tree* t, const double* vx, const double* vy, const double* vz,
+                     bool particles_only = false);
 void run_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay,
                    const double* az, double alpha, double G, double* aold);
 

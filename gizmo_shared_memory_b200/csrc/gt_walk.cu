@@ -62,6 +62,11 @@ struct WalkArgs {
     const float* nq2;           // node second moments
     double mac_band_lo, mac_band_hi, mac_log_kappa;
     const float* mac_l2;        // GT_MAC_NODE: per-node L^2 10^(c - log10 kappa)
+    // tidal tensor (6 per target: xx yy zz xy yz xz, not times G) and jerk (3 per target, times G)
+    double* tidal;
+    double* jerk;
+    const float4* svel;         // particle velocities in tree order (jerk)
+    const float4* nvel;         // node centre-of-mass velocities (jerk)
     // forest: root node of each group (its system's root); null: node 0
     const int* group_root;
 };
@@ -154,6 +159,25 @@ __device__ __noinline__ void spline_pair(float r2, float h, float m, float& f, f
     }
 }
 
+// The same pair inside the kernel plus the second-derivative (tidal) factor g2 of the cubic spline,
+// shmem/tree.h:85-96 (GIZMO's kernel_gravity mode 2), in FP32.  r2 == 0 contributes nothing.
+__device__ __noinline__ void spline_pair_tidal(float r2, float h, float m, float& f, float& p, float& g2) {
+    spline_pair(r2, h, m, f, p);
+    if (!(r2 > 0.0f)) { g2 = 0.0f; return; }
+    const float hinv = 1.0f / h;
+    const float u = sqrtf(r2) * hinv;
+    const float hinv2 = hinv * hinv;
+    const float hinv5 = hinv2 * hinv2 * hinv;
+    float wk;
+    if (u < 0.5f) {
+        wk = 76.8f - 96.0f * u;
+    } else {
+        const float u2 = u * u;
+        wk = -0.2f / (u2 * u2 * u) + 48.0f / u - 76.8f + 32.0f * u;
+    }
+    g2 = m * wk * hinv5;
+}
+
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
     const float y = x - comp;
     const float t = sum + y;
@@ -172,14 +196,15 @@ struct alignas(16) WarpHdr {
     double lo_x, lo_y, lo_z, hi_x, hi_y, hi_z, c_x, c_y, c_z, emax, amin;
 };
 
-__host__ __device__ constexpr int warp_smem_bytes(int pn_cap, int pp_cap) {
-    return ((int)sizeof(WarpHdr) + pn_cap * 16 + pp_cap * 20 + 15) & ~15;
+// xt: the lists also carry each entry's velocity (float4), for the jerk.
+__host__ __device__ constexpr int warp_smem_bytes(int pn_cap, int pp_cap, bool xt = false) {
+    return ((int)sizeof(WarpHdr) + pn_cap * 16 + pp_cap * 20 + (xt ? (pn_cap + pp_cap) * 16 : 0) + 15) & ~15;
 }
 
 // MAC: 0 plain relative criterion, 1 network inside the walk (GT_MAC_LEARNED), 2 per-node
-// learned scale (GT_MAC_NODE).
-template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT, int MAC>
-__global__ void __launch_bounds__(kMaxWarps * 32, TPL == 1 ? 3 : 2)
+// learned scale (GT_MAC_NODE).  XT: also the tidal tensor and/or the jerk (A.tidal, A.jerk).
+template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT, int MAC, bool XT = false>
+__global__ void __launch_bounds__(kMaxWarps * 32, (TPL == 1 && !XT) ? 3 : 2)
 walk_kernel(const WalkArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -197,6 +222,10 @@ walk_kernel(const WalkArgs A) {
     float4* __restrict__ pn = reinterpret_cast<float4*>(wbase + sizeof(WarpHdr));
     float4* __restrict__ pp = pn + A.pn_cap;
     float* __restrict__ ph = reinterpret_cast<float*>(pp + A.pp_cap);
+    float4* __restrict__ pnv = reinterpret_cast<float4*>(ph + A.pp_cap);  // XT only
+    float4* __restrict__ ppv = pnv + A.pn_cap;
+    const bool want_tid = XT && A.tidal != nullptr;
+    const bool want_jerk = XT && A.jerk != nullptr;
 
     unsigned long long c_nodes = 0, c_multi = 0, c_pairs = 0, c_zero = 0, c_flush = 0, c_steps = 0;
     int c_maxtop = 0;
@@ -265,6 +294,42 @@ walk_kernel(const WalkArgs A) {
             sx[k] = sy[k] = sz[k] = cxk[k] = cyk[k] = czk[k] = 0.0f;
             pot[k] = 0.0;
         }
+        // tidal tensor and jerk: FP64 totals (xx yy zz xy yz xz, jx jy jz) and target velocities
+        double xt[9][TPL];
+        float tvx[TPL], tvy[TPL], tvz[TPL];
+        if (XT) {
+#pragma unroll
+            for (int k = 0; k < TPL; ++k) {
+#pragma unroll
+                for (int c = 0; c < 9; ++c) xt[c][k] = 0.0;
+                tvx[k] = tvy[k] = tvz[k] = 0.0f;
+                const int i = ti + 32 * k;
+                if (want_jerk && i < nt) {
+                    const int p = A.tpos ? (int)A.tpos[t0 + i] : t0 + i;
+                    const float4 v = A.svel[p];
+                    tvx[k] = v.x; tvy[k] = v.y; tvz[k] = v.z;
+                }
+            }
+        }
+        // one interaction's tidal and jerk terms: T += -g1 I + g2 d d, J += g1 dv - (dv.d) g2 d
+        // (shmem/tree.cc:811-837, 845-872); d = source - target, dv = v_source - v_target
+        auto xt_add = [&](float (&q)[9], float dx, float dy, float dz, float g1, float g2, float4 ev, int k) {
+            if (want_tid) {
+                q[0] += fmaf(dx * dx, g2, -g1);
+                q[1] += fmaf(dy * dy, g2, -g1);
+                q[2] += fmaf(dz * dz, g2, -g1);
+                q[3] = fmaf(dx * dy, g2, q[3]);
+                q[4] = fmaf(dy * dz, g2, q[4]);
+                q[5] = fmaf(dx * dz, g2, q[5]);
+            }
+            if (want_jerk) {
+                const float dvx = ev.x - tvx[k], dvy = ev.y - tvy[k], dvz = ev.z - tvz[k];
+                const float vg = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz)) * g2;
+                q[6] += fmaf(g1, dvx, -vg * dx);
+                q[7] += fmaf(g1, dvy, -vg * dy);
+                q[8] += fmaf(g1, dvz, -vg * dz);
+            }
+        };
 
         // ---- evaluate the lists against the targets ---------------------------------------
         auto accumulate = [&](const float* ax_, const float* ay_, const float* az_, const float* ap_) {
@@ -282,8 +347,15 @@ walk_kernel(const WalkArgs A) {
         auto flush_pn = [&](int n) {
             __syncwarp();
             float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
+            float xq[XT ? TPL : 1][9];
 #pragma unroll
             for (int k = 0; k < TPL; ++k) ax_[k] = ay_[k] = az_[k] = ap_[k] = 0.0f;
+            if (XT) {
+#pragma unroll
+                for (int k = 0; k < TPL; ++k)
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) xq[XT ? k : 0][c] = 0.0f;
+            }
 #pragma unroll 4
             for (int j = slice; j < n; j += NS) {
                 const float4 e = pn[j];
@@ -299,18 +371,36 @@ walk_kernel(const WalkArgs A) {
                         ay_[k] = fmaf(dy, f, ay_[k]);
                         az_[k] = fmaf(dz, f, az_[k]);
                         if (WANT_POT) ap_[k] -= mri;
+                        if (XT) {
+                            // Newtonian: g2 = 3 m / r^5
+                            const float4 ev = want_jerk ? pnv[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                            xt_add(xq[XT ? k : 0], dx, dy, dz, f, 3.0f * f * (ri * ri), ev, k);
+                        }
                     }
                 }
             }
             accumulate(ax_, ay_, az_, ap_);
+            if (XT) {
+#pragma unroll
+                for (int k = 0; k < TPL; ++k)
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) xt[c][k] += (double)xq[XT ? k : 0][c];
+            }
             __syncwarp();
         };
         // Particles: kernel of the larger softening; r^2 == 0 (the target itself) contributes 0.
         auto flush_pp = [&](int n) {
             __syncwarp();
             float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
+            float xq[XT ? TPL : 1][9];
 #pragma unroll
             for (int k = 0; k < TPL; ++k) ax_[k] = ay_[k] = az_[k] = ap_[k] = 0.0f;
+            if (XT) {
+#pragma unroll
+                for (int k = 0; k < TPL; ++k)
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) xq[XT ? k : 0][c] = 0.0f;
+            }
             unsigned zero = 0;
             for (int j = slice; j < n; j += NS) {
                 const float4 e = pp[j];
@@ -321,12 +411,15 @@ walk_kernel(const WalkArgs A) {
                         const float dx = e.x - tx[k], dy = e.y - ty[k], dz = e.z - tz[k];
                         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                         const float hh = fmaxf(th[k], hj);
-                        float f, p;
+                        float f, p, g2 = 0.0f;
                         if (r2 >= hh * hh && r2 > 0.0f) {
                             const float ri = rsqrtf(r2);
                             const float mri = e.w * ri;
                             f = mri * ri * ri;
                             p = -mri;
+                            if (XT) g2 = 3.0f * f * (ri * ri);
+                        } else if (XT) {
+                            spline_pair_tidal(r2, hh, e.w, f, p, g2);
                         } else {
                             spline_pair(r2, hh, e.w, f, p);
                         }
@@ -335,10 +428,20 @@ walk_kernel(const WalkArgs A) {
                         ay_[k] = fmaf(dy, f, ay_[k]);
                         az_[k] = fmaf(dz, f, az_[k]);
                         if (WANT_POT) ap_[k] += p;
+                        if (XT) {
+                            const float4 ev = want_jerk ? ppv[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                            xt_add(xq[XT ? k : 0], dx, dy, dz, f, g2, ev, k);
+                        }
                     }
                 }
             }
             accumulate(ax_, ay_, az_, ap_);
+            if (XT) {
+#pragma unroll
+                for (int k = 0; k < TPL; ++k)
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) xt[c][k] += (double)xq[XT ? k : 0][c];
+            }
             if (COUNT) c_zero += zero;
             __syncwarp();
         };
@@ -432,6 +535,7 @@ walk_kernel(const WalkArgs A) {
                     const int pos = npn + __popc(am & lt_mask);
                     pn[pos] = make_float4((float)(nd.cx - S.c_x), (float)(nd.cy - S.c_y),
                                           (float)(nd.cz - S.c_z), (float)nd.mass);
+                    if (want_jerk) pnv[pos] = A.nvel[node];  // the node's centre-of-mass velocity
                 }
                 npn += na;
                 if (COUNT && lane == 0) c_multi += (unsigned long long)na * nt;
@@ -458,13 +562,15 @@ walk_kernel(const WalkArgs A) {
                     double qx = 0, qy = 0, qz = 0;
                     float qm = 0.0f, qh = 0.0f;
                     bool far = false;
+                    int qpos = 0;
                     if (live) {
                         // owner: the last lane whose exclusive prefix is <= q
                         int l = 0;
 #pragma unroll
                         for (int step = 16; step > 0; step >>= 1)
                             if (S.pre[l + step] <= q) l += step;
-                        load_src(A.src + S.lo[l] + (q - S.pre[l]), qx, qy, qz, qm, qh);
+                        qpos = S.lo[l] + (q - S.pre[l]);
+                        load_src(A.src + qpos, qx, qy, qz, qm, qh);
                         const double ex = fmax(0.0, fmax(S.lo_x - qx, qx - S.hi_x));
                         const double ey = fmax(0.0, fmax(S.lo_y - qy, qy - S.hi_y));
                         const double ez = fmax(0.0, fmax(S.lo_z - qz, qz - S.hi_z));
@@ -479,10 +585,12 @@ walk_kernel(const WalkArgs A) {
                     const float4 e = make_float4((float)(qx - S.c_x), (float)(qy - S.c_y), (float)(qz - S.c_z), qm);
                     if (live && far) {
                         pn[npn + __popc(fm & lt_mask)] = e;
+                        if (want_jerk) pnv[npn + __popc(fm & lt_mask)] = A.svel[qpos];
                     } else if (live) {
                         const int pos = npp + __popc(nm & lt_mask);
                         pp[pos] = e;
                         ph[pos] = qh;
+                        if (want_jerk) ppv[pos] = A.svel[qpos];
                     }
                     npn += nf;
                     npp += nn;
@@ -510,6 +618,11 @@ walk_kernel(const WalkArgs A) {
                 vz += __shfl_xor_sync(kFull, vz, o);
                 if (WANT_POT) vp += __shfl_xor_sync(kFull, vp, o);
             }
+            if (XT) {
+#pragma unroll
+                for (int c = 0; c < 9; ++c)
+                    for (int o = NT; o < 32; o <<= 1) xt[c][k] += __shfl_xor_sync(kFull, xt[c][k], o);
+            }
             const int i = ti + 32 * k;
             if (slice == 0 && k < nk && i < nt) {
                 const int idx = t0 + i;
@@ -520,6 +633,12 @@ walk_kernel(const WalkArgs A) {
                     A.az[o] = A.G * vz;
                 }
                 if (WANT_POT && A.phi) A.phi[o] = A.G * vp;
+                if (want_tid)
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) A.tidal[6 * (size_t)o + c] = xt[c][k];
+                if (want_jerk)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) A.jerk[3 * (size_t)o + c] = A.G * xt[6 + c][k];
             }
         }
     }
@@ -698,29 +817,33 @@ int64_t finish_groups(gt_context* ctx, const uint32_t* flag, int64_t n, int kmax
     return nc;
 }
 
-size_t walk_smem(int warps, bool mac, int pn_cap) {
-    return (size_t)warps * warp_smem_bytes(pn_cap, pn_cap / 2) + (mac ? kMacModel * sizeof(float) : 0);
+size_t walk_smem(int warps, bool mac, int pn_cap, bool xt = false) {
+    return (size_t)warps * warp_smem_bytes(pn_cap, pn_cap / 2, xt) + (mac ? kMacModel * sizeof(float) : 0);
 }
 
 // Dynamic shared memory above 48 KB needs a per-kernel opt-in, done once per instantiation.
-template <int TPL, bool LA, bool POT, bool CNT, int MAC>
+template <int TPL, bool LA, bool POT, bool CNT, int MAC, bool XT = false>
 void prepare_walk() {
     static bool done = false;
     if (done) return;
-    check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT, MAC>,
+    // the largest request of this instantiation: 8 warps at the largest list capacity (XT lists
+    // carry velocities too, so XT stops at half the capacity)
+    check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT, MAC, XT>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)walk_smem(kMaxWarps, MAC == 1, kPnCapMax)), "cudaFuncSetAttribute");
+                                    (int)walk_smem(kMaxWarps, MAC == 1, XT ? kPnCapMax / 2 : kPnCapMax, XT)),
+               "cudaFuncSetAttribute");
     // the lists need 3 blocks x 55 KB per SM: ask for the largest shared-memory carveout
-    check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT, MAC>,
+    check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT, MAC, XT>,
                                     cudaFuncAttributePreferredSharedMemoryCarveout, 100),
                "cudaFuncSetAttribute");
     done = true;
 }
 
-template <int TPL, bool LA, bool POT, bool CNT, int MAC>
+template <int TPL, bool LA, bool POT, bool CNT, int MAC, bool XT = false>
 void launch_walk(gt_context* ctx, const WalkArgs& a, int blocks, int warps) {
-    prepare_walk<TPL, LA, POT, CNT, MAC>();
-    walk_kernel<TPL, LA, POT, CNT, MAC><<<blocks, warps * 32, walk_smem(warps, MAC == 1, a.pn_cap), ctx->stream>>>(a);
+    prepare_walk<TPL, LA, POT, CNT, MAC, XT>();
+    walk_kernel<TPL, LA, POT, CNT, MAC, XT><<<blocks, warps * 32, walk_smem(warps, MAC == 1, a.pn_cap, XT),
+                                              ctx->stream>>>(a);
     check_launch(ctx, "walk_kernel");
 }
 
@@ -728,6 +851,17 @@ template <int TPL, bool LA, bool POT, int MAC>
 void dispatch_count(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool cnt) {
     if (cnt) launch_walk<TPL, LA, POT, true, MAC>(ctx, a, blocks, warps);
     else launch_walk<TPL, LA, POT, false, MAC>(ctx, a, blocks, warps);
+}
+
+// Tidal tensor / jerk: grouped walk, plain criterion, groups of at most 32 targets.
+void dispatch_xt(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool pot, bool cnt) {
+    if (pot) {
+        if (cnt) launch_walk<1, true, true, true, 0, true>(ctx, a, blocks, warps);
+        else launch_walk<1, true, true, false, 0, true>(ctx, a, blocks, warps);
+    } else {
+        if (cnt) launch_walk<1, true, false, true, 0, true>(ctx, a, blocks, warps);
+        else launch_walk<1, true, false, false, 0, true>(ctx, a, blocks, warps);
+    }
 }
 
 // The learned criteria are grouped-walk options (leaves offered to the criterion).
@@ -749,12 +883,12 @@ void dispatch(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la
     }
 }
 
-template <int TPL, bool LA, bool POT, bool CNT, int MAC>
+template <int TPL, bool LA, bool POT, bool CNT, int MAC, bool XT = false>
 int occupancy_blocks(int warps, int pn_cap) {
-    prepare_walk<TPL, LA, POT, CNT, MAC>();
+    prepare_walk<TPL, LA, POT, CNT, MAC, XT>();
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<TPL, LA, POT, CNT, MAC>, warps * 32,
-                                                  walk_smem(warps, MAC == 1, pn_cap));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<TPL, LA, POT, CNT, MAC, XT>, warps * 32,
+                                                  walk_smem(warps, MAC == 1, pn_cap, XT));
     return std::max(1, nb);
 }
 
@@ -775,8 +909,9 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     if (mode == GT_GROUP_NODE && param <= 0) param = 32;
     if (mode == GT_GROUP_BATCH && param <= 0) mode = GT_GROUP_LEAF;
     // a warp holds up to 32, 64 or 128 targets (1, 2 or 4 per lane); longer groups are chunked
+    const bool xt = rq.tidal != nullptr || rq.jerk != nullptr;
     int kmax = 32;
-    if ((mode == GT_GROUP_NODE || mode == GT_GROUP_BATCH) && param > 32) kmax = param > 64 ? 128 : 64;
+    if (!xt && (mode == GT_GROUP_NODE || mode == GT_GROUP_BATCH) && param > 32) kmax = param > 64 ? 128 : 64;
     const int tpl = kmax / 32;
 
     // ---- groups -------------------------------------------------------------------------------
@@ -859,8 +994,12 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
             throw Fail{GT_ERR_INVALID, "list_capacity must be a multiple of 32 in [64, 1024]"};
         pn_cap = rq.list_capacity;
     }
+    if (xt && pn_cap > kPnCapMax / 2)
+        throw Fail{GT_ERR_INVALID, "list_capacity must be at most 512 with the tidal tensor or the jerk"};
     int per_sm;
-    if (tpl == 1)
+    if (xt)
+        per_sm = occupancy_blocks<1, true, false, false, 0, true>(warps, pn_cap);
+    else if (tpl == 1)
         per_sm = mac ? occupancy_blocks<1, true, false, false, 1>(warps, pn_cap)
                : macn ? occupancy_blocks<1, true, false, false, 2>(warps, pn_cap)
                       : (rq.leaf_accept ? occupancy_blocks<1, true, false, false, 0>(warps, pn_cap)
@@ -896,7 +1035,14 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     const int total_warps = blocks * warps;
     a.pn_cap = pn_cap;
     a.pp_cap = pn_cap / 2;
-    a.warp_bytes = warp_smem_bytes(a.pn_cap, a.pp_cap);
+    a.warp_bytes = warp_smem_bytes(a.pn_cap, a.pp_cap, xt);
+    a.tidal = rq.tidal;
+    a.jerk = rq.jerk;
+    a.svel = t->svel;
+    a.nvel = t->nvel;
+    if (xt && (rq.mac != GT_MAC_PLAIN || !rq.leaf_accept))
+        throw Fail{GT_ERR_UNSUPPORTED, "the tidal tensor and the jerk come from the grouped walk with the plain criterion"};
+    if (rq.jerk && !t->svel) throw Fail{GT_ERR_INVALID, "the jerk needs velocities (gt_tree_velocities)"};
     // a captured graph keeps its pointers: it runs on buffers its plan owns, not on the workspace
     WalkBuffers* wb = rq.bufs;
     auto own = [&](void** p, size_t& have, size_t need) {
@@ -952,7 +1098,8 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         a.stack_cap = stack_cap;
         check_cuda(cudaMemsetAsync(ctr, 0, 96, st), "memset counters");
         if (!rq.capture) check_cuda(cudaEventRecord(ctx->ev0, st), "event");
-        if (tpl == 1) dispatch<1>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
+        if (xt) dispatch_xt(ctx, a, blocks, warps, want_pot, rq.count);
+        else if (tpl == 1) dispatch<1>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
         else if (tpl == 2) dispatch<2>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
         else dispatch<4>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
         if (rq.capture) break;  // the default stack capacity is a proven bound

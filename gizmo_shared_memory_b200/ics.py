@@ -173,3 +173,22 @@ def config(name: str):
     if name == "merger_67m":
         return merger()
     raise KeyError(name)
+
+
+def write_state(path, P, vel):
+    """The flat particle dump shmem/bench_treeforce.cc reads: N (u64), then x, y, z, m, h, vx, vy,
+    vz as contiguous float64 arrays."""
+    n = len(P["m"])
+    with open(path, "wb") as fh:
+        np.array([n], np.uint64).tofile(fh)
+        for a in (P["x"], P["y"], P["z"], P["m"], P["soft"], vel[0], vel[1], vel[2]):
+            np.ascontiguousarray(a, np.float64).tofile(fh)
+
+
+def plummer_state(n=200000, seed=11, sigma=0.5):
+    """A Plummer sphere with seeded Gaussian velocities: a synthetic stand-in for the engine state
+    files bench_treeforce reads."""
+    P = plummer(n=n, seed=seed, soft=0.01)
+    rng = np.random.default_rng(seed + 1)
+    vel = [rng.normal(0.0, sigma, n) for _ in range(3)]
+    return P, vel

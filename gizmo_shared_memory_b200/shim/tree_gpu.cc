@@ -50,7 +50,7 @@ const double* soft_or_null(const Particles& P) { return P.soft.empty() ? nullptr
 
 Tree build(const Particles& P, BuildTimes* bt, const double* const* vel, bool want_vcom,
            long long randomize_seed) {
-    if (vel && want_vcom) unsupported("centre-of-mass velocities (want_vcom)");
+    if (!vel) want_vcom = false;  // no velocities, no centre-of-mass velocity (tree.cc:352)
     const int64_t n = (int64_t)P.size();
     gt_build_options o;
     gt_build_options_default(&o);
@@ -92,6 +92,17 @@ Tree build(const Particles& P, BuildTimes* bt, const double* const* vel, bool wa
     T.nalloc = (int)nn;
     T.vmax.assign(nn, 0.0f);
     T.xpad.assign(nn, 0.0f);
+    if (vel) {
+        // per-node speed bound, and with want_vcom the centre-of-mass velocity the jerk reads
+        check(gt_tree_velocities(ctx, h, vel[0], vel[1], vel[2], 0, GT_MEM_HOST), "gt_tree_velocities");
+        if (want_vcom) {
+            T.vcom_x.resize(nn); T.vcom_y.resize(nn); T.vcom_z.resize(nn);
+        }
+        check(gt_tree_velocity_moments(ctx, h, want_vcom ? T.vcom_x.data() : nullptr,
+                                       want_vcom ? T.vcom_y.data() : nullptr,
+                                       want_vcom ? T.vcom_z.data() : nullptr, T.vmax.data()),
+              "gt_tree_velocity_moments");
+    }
     if (!P.type.empty()) {
         // sinks (type 5) under each node, for the engine's sink bookkeeping (tree.cc:168, 178)
         T.nsink.assign(nn, 0u);
@@ -155,18 +166,33 @@ void accel_grouped(const Tree& T, const Particles& P, const std::vector<uint32_t
                    std::vector<Vec3d>* jerk, const double* const* vel, double sink_direct_radius) {
     need_gpu(T);
     require_gravity_only(P);
-    if (tidal) unsupported("the tidal tensor");
-    if (jerk && vel) unsupported("the jerk");
     if (lazy) unsupported("lazy drift");
     if (sink_direct_radius > 0 && !P.type.empty()) unsupported("sink-direct opening");
+    // the jerk needs source velocities: the walk's `vel` for particles and the build's node
+    // centre-of-mass velocities (tree.cc:638-640); without them it stays zero
+    const bool want_jerk = jerk && vel && !T.vcom_x.empty();
     const size_t nt = targets.size();
     ax.assign(nt, 0.0); ay.assign(nt, 0.0); az.assign(nt, 0.0);
+    if (tidal) tidal->assign(nt, SymTensor3d{0, 0, 0, 0, 0, 0});
     if (jerk) jerk->assign(nt, Vec3d{0, 0, 0});
     if (!nt) return;
     gt_walk_options o;
     gt_walk_options_default(&o);
-    check(gt_accel_grouped(context(), T.gpu.get(), (int64_t)nt, targets.data(), aold, theta, G, batch,
-                           &o, GT_MEM_HOST, ax.data(), ay.data(), az.data(), nullptr), "gt_accel_grouped");
+    if (!tidal && !want_jerk) {
+        check(gt_accel_grouped(context(), T.gpu.get(), (int64_t)nt, targets.data(), aold, theta, G, batch,
+                               &o, GT_MEM_HOST, ax.data(), ay.data(), az.data(), nullptr), "gt_accel_grouped");
+        return;
+    }
+    if (want_jerk)  // the particles' current velocities, the build's node velocities
+        check(gt_tree_velocities(context(), T.gpu.get(), vel[0], vel[1], vel[2], 1, GT_MEM_HOST),
+              "gt_tree_velocities");
+    static_assert(sizeof(SymTensor3d) == 6 * sizeof(double), "SymTensor3d is six doubles");
+    static_assert(sizeof(Vec3d) == 3 * sizeof(double), "Vec3d is three doubles");
+    check(gt_accel_grouped_ext(context(), T.gpu.get(), (int64_t)nt, targets.data(), aold, theta, G, batch,
+                               &o, GT_MEM_HOST, ax.data(), ay.data(), az.data(), nullptr,
+                               tidal ? reinterpret_cast<double*>(tidal->data()) : nullptr,
+                               want_jerk ? reinterpret_cast<double*>(jerk->data()) : nullptr),
+          "gt_accel_grouped_ext");
 }
 
 void potential(const Tree& T, const Particles& P, const std::vector<uint32_t>& targets,

@@ -210,6 +210,17 @@ GT_API int gt_tree_download(gt_context* ctx, const gt_tree* tree, uint32_t* orde
                      int32_t* leaf_of, const gt_node_arrays* nodes);
 /* Sorted keys (n_live, u64) of the tree: PH or Morton per the build's key_mode. */
 GT_API int gt_tree_keys(gt_context* ctx, const gt_tree* tree, uint64_t* keys);
+/* Attach particle velocities (indexed like the build's input) to the tree: the per-node
+ * centre-of-mass velocity and speed bound of shmem::build with vel and want_vcom
+ * (tree.cc:149-190, Tree::vcom and Tree::vmax), which the jerk needs.  particles_only = 1
+ * refreshes only the particles' velocities and keeps the node moments of the earlier call, as the
+ * reference's jerk reads the current particle velocities but the build-time node velocities
+ * (tree.cc:793-797, 862-866). */
+GT_API int gt_tree_velocities(gt_context* ctx, gt_tree* tree, const double* vx, const double* vy,
+                       const double* vz, int particles_only, int mem);
+/* Per-node centre-of-mass velocity (n_nodes each) and speed bound; any pointer may be null. */
+GT_API int gt_tree_velocity_moments(gt_context* ctx, const gt_tree* tree, double* vcx, double* vcy,
+                             double* vcz, float* vmax);
 
 /* ---- walks --------------------------------------------------------------------------------- */
 /* Grouped walk.  Replaces shmem::accel_grouped (shmem/tree.h:428-440, tree.cc:626-897) for the
@@ -221,6 +232,16 @@ GT_API int gt_accel_grouped(gt_context* ctx, const gt_tree* tree, int64_t n_targ
                      const uint32_t* targets, const double* aold, double theta, double G, int batch,
                      const gt_walk_options* opt, int mem, double* ax, double* ay, double* az,
                      double* phi);
+/* The grouped walk with the tidal tensor and the jerk: shmem::accel_grouped's `tidal` and `jerk`
+ * arguments (tree.cc:811-837, 845-880).  tidal (may be NULL) receives 6 values per target in
+ * SymTensor3d storage order xx yy zz xy yz xz, NOT multiplied by G (as the reference stores it);
+ * jerk (may be NULL) receives 3 values per target, multiplied by G, from the source velocities:
+ * particles' own and nodes' centre-of-mass velocities (gt_tree_velocities must have been
+ * called).  Plain criterion only; groups hold at most 32 targets (longer windows are split). */
+GT_API int gt_accel_grouped_ext(gt_context* ctx, const gt_tree* tree, int64_t n_targets,
+                     const uint32_t* targets, const double* aold, double theta, double G, int batch,
+                     const gt_walk_options* opt, int mem, double* ax, double* ay, double* az,
+                     double* phi, double* tidal, double* jerk);
 /* Walk plan: the all-active grouped walk of gt_accel_grouped (targets = NULL) captured once as a
  * CUDA graph and replayed by gt_plan_launch on the context stream, asynchronously.  aold and the
  * outputs are DEVICE arrays whose addresses are fixed at creation (update their contents between

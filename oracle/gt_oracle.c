@@ -41,6 +41,16 @@ double or_spline_potential(double r, double h) {
                    u * u * (10.666666666666667 + u * (-16.0 + u * (9.6 - 2.1333333333333333 * u))));
 }
 
+/* Second-derivative (tidal) factor of the same spline: 3/r^5 for r >= h.  shmem/tree.h:85-96. */
+double or_spline_tidal_factor(double r, double h) {
+    const double hinv = 1.0 / h;
+    const double u = r * hinv;
+    if (u >= 1.0) return 3.0 / (r * r * r * r * r);
+    const double hinv5 = hinv * hinv * hinv * hinv * hinv;
+    const double wk = u < 0.5 ? 76.8 - 96.0 * u : -0.2 / (u * u * u * u * u) + 48.0 / u - 76.8 + 32.0 * u;
+    return wk * hinv5;
+}
+
 /* Node-opening decision, in the reference's order: softening overlap, Barnes-Hut (theta > 0),
  * relative criterion M L^2 > r^4 aold (aold > 0; with aold == 0 and no theta: open), then the
  * inside-node test.  shmem/tree.h:109-144. */
@@ -580,5 +590,135 @@ void or_direct(int64_t n, const double* x, const double* y, const double* z, con
         if (ay) ay[k] = G * sy;
         if (az) az[k] = G * sz;
         if (phi) phi[k] = G * sp;
+    }
+}
+
+/* Per-node centre-of-mass velocity and speed bound, from the particles of a leaf and from the
+ * children of an interior node (shmem/tree.cc:149-190, built when velocities are supplied).
+ * Nodes are numbered in preorder, so every child comes after its parent: one reverse sweep. */
+void or_velocity_moments(const or_tree* t, const double* vx, const double* vy, const double* vz,
+                         double* vcx, double* vcy, double* vcz, float* vmax) {
+    for (int64_t i = t->nnodes - 1; i >= 0; --i) {
+        double M = 0, px = 0, py = 0, pz = 0, vm = 0;
+        if (t->first[i] < 0) {
+            for (int k = t->plo[i]; k < t->phi[i]; ++k) {
+                const uint32_t p = t->order[k];
+                const double m = t->m[p];
+                const double v = sqrt(vx[p] * vx[p] + vy[p] * vy[p] + vz[p] * vz[p]);
+                if (v > vm) vm = v;
+                M += m; px += m * vx[p]; py += m * vy[p]; pz += m * vz[p];
+            }
+        } else {
+            for (int c = t->first[i]; c >= 0 && t->parent[c] == i; c = t->next[c]) {
+                const double m = t->mass[c];
+                if ((double)vmax[c] > vm) vm = (double)vmax[c];
+                M += m; px += m * vcx[c]; py += m * vcy[c]; pz += m * vcz[c];
+            }
+        }
+        vmax[i] = (float)vm;
+        vcx[i] = M > 0 ? px / M : 0.0;
+        vcy[i] = M > 0 ? py / M : 0.0;
+        vcz[i] = M > 0 ? pz / M : 0.0;
+    }
+}
+
+/* The grouped walk of or_walk_groups (leaf_accept = 1) with the tidal tensor and the jerk:
+ * every P-P and P-N interaction adds T += -g1 I + g2 d d and J += g1 dv - (dv.d) g2 d, with g1
+ * the zeta-free force factor and g2 the tidal factor of the same softening, d = source - target
+ * and dv = v_source - v_target (particles' own velocities, nodes' centre-of-mass velocities).
+ * tidal (6 per target, xx yy zz xy yz xz) is not multiplied by G, jerk (3 per target) is.
+ * shmem/tree.cc:811-837, 845-880. */
+void or_walk_groups_ext(const or_tree* t, int64_t nt, const uint32_t* targets, int64_t ngroups,
+                        const int64_t* starts, double theta, double G, const double* aold,
+                        const double* vx, const double* vy, const double* vz, const double* vcx,
+                        const double* vcy, const double* vcz, double* ax, double* ay, double* az,
+                        double* tidal, double* jerk) {
+    const double theta2 = theta * theta;
+    const int wj = jerk != NULL;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t g = 0; g < ngroups; ++g) {
+        const int64_t lo = starts[g], hi = starts[g + 1];
+        const int nb = (int)(hi - lo);
+        double b0[3] = {1e300, 1e300, 1e300}, b1[3] = {-1e300, -1e300, -1e300}, emax = 0;
+        double amin = aold ? 1e300 : 0.0;
+        double* buf = (double*)calloc((size_t)nb * 19, 8);
+        double *tx = buf, *ty = buf + nb, *tz = buf + 2 * nb, *te = buf + 3 * nb;
+        double *tvx = buf + 4 * nb, *tvy = buf + 5 * nb, *tvz = buf + 6 * nb;
+        double *oax = buf + 7 * nb, *oay = buf + 8 * nb, *oaz = buf + 9 * nb;
+        double* ot = buf + 10 * nb; /* 6 * nb */
+        double* oj = buf + 16 * nb; /* 3 * nb */
+        for (int i = 0; i < nb; ++i) {
+            const uint32_t p = targets[lo + i];
+            tx[i] = t->x[p]; ty[i] = t->y[p]; tz[i] = t->z[p];
+            te[i] = t->soft ? t->soft[p] : 0.0;
+            if (wj) { tvx[i] = vx[p]; tvy[i] = vy[p]; tvz[i] = vz[p]; }
+            b0[0] = dmin(b0[0], tx[i]); b1[0] = dmax(b1[0], tx[i]);
+            b0[1] = dmin(b0[1], ty[i]); b1[1] = dmax(b1[1], ty[i]);
+            b0[2] = dmin(b0[2], tz[i]); b1[2] = dmax(b1[2], tz[i]);
+            emax = dmax(emax, te[i]);
+            if (aold) amin = dmin(amin, aold[lo + i]);
+        }
+        int node = t->root;
+        while (node >= 0) {
+            const double ncx = t->cx[node], ncy = t->cy[node], ncz = t->cz[node];
+            const double dx = dmax(0.0, dmax(b0[0] - ncx, ncx - b1[0]));
+            const double dy = dmax(0.0, dmax(b0[1] - ncy, ncy - b1[1]));
+            const double dz = dmax(0.0, dmax(b0[2] - ncz, ncz - b1[2]));
+            const int is_leaf = t->first[node] < 0;
+            const int accept = !or_open_node(dx * dx + dy * dy + dz * dz, (double)t->w_len[node], t->w_s[node],
+                                             t->mass[node], (double)t->w_soft[node], emax, amin, theta2, dx, dy, dz);
+            if (accept || is_leaf) {
+                const int kb = accept ? -1 : t->plo[node], ke = accept ? 0 : t->phi[node];
+                for (int k = kb; k < ke; ++k) {
+                    /* k == -1: the node as a monopole; otherwise the leaf's particle k */
+                    uint32_t q = 0;
+                    double qx, qy, qz, qm, qs, qvx = 0, qvy = 0, qvz = 0;
+                    if (k < 0) {
+                        qx = ncx; qy = ncy; qz = ncz; qm = t->mass[node]; qs = (double)t->w_soft[node];
+                        if (wj) { qvx = vcx[node]; qvy = vcy[node]; qvz = vcz[node]; }
+                    } else {
+                        q = t->order[k];
+                        qx = t->x[q]; qy = t->y[q]; qz = t->z[q]; qm = t->m[q];
+                        qs = t->soft ? t->soft[q] : 0.0;
+                        if (wj) { qvx = vx[q]; qvy = vy[q]; qvz = vz[q]; }
+                    }
+                    for (int i = 0; i < nb; ++i) {
+                        if (k >= 0 && targets[lo + i] == q) continue;
+                        const double ox = qx - tx[i], oy = qy - ty[i], oz = qz - tz[i];
+                        const double r2 = ox * ox + oy * oy + oz * oz;
+                        if (r2 <= 0) continue;
+                        const double r = sqrt(r2);
+                        const double e = dmax(dmax(te[i], qs), 1e-300);
+                        const double g1 = qm * or_spline_force_over_r(r, e);
+                        const double g2 = qm * or_spline_tidal_factor(r, e);
+                        oax[i] += ox * g1; oay[i] += oy * g1; oaz[i] += oz * g1;
+                        if (tidal) {
+                            ot[6 * i + 0] += -g1 + ox * ox * g2;
+                            ot[6 * i + 1] += -g1 + oy * oy * g2;
+                            ot[6 * i + 2] += -g1 + oz * oz * g2;
+                            ot[6 * i + 3] += ox * oy * g2;
+                            ot[6 * i + 4] += oy * oz * g2;
+                            ot[6 * i + 5] += ox * oz * g2;
+                        }
+                        if (wj) {
+                            const double dvx = qvx - tvx[i], dvy = qvy - tvy[i], dvz = qvz - tvz[i];
+                            const double vdr = dvx * ox + dvy * oy + dvz * oz;
+                            oj[3 * i + 0] += g1 * dvx - vdr * g2 * ox;
+                            oj[3 * i + 1] += g1 * dvy - vdr * g2 * oy;
+                            oj[3 * i + 2] += g1 * dvz - vdr * g2 * oz;
+                        }
+                    }
+                }
+                node = t->next[node];
+            } else {
+                node = t->first[node];
+            }
+        }
+        for (int i = 0; i < nb; ++i) {
+            if (ax) { ax[lo + i] = G * oax[i]; ay[lo + i] = G * oay[i]; az[lo + i] = G * oaz[i]; }
+            if (tidal) for (int c = 0; c < 6; ++c) tidal[6 * (lo + i) + c] = ot[6 * i + c];
+            if (wj) for (int c = 0; c < 3; ++c) jerk[3 * (lo + i) + c] = G * oj[3 * i + c];
+        }
+        free(buf);
     }
 }

@@ -22,6 +22,7 @@ typedef struct or_tree or_tree;
 /* Scalar kernels (shmem/tree.h:59-80) and the opening test (shmem/tree.h:109-144). */
 double or_spline_force_over_r(double r, double h);
 double or_spline_potential(double r, double h);
+double or_spline_tidal_factor(double r, double h); /* shmem/tree.h:85-96 */
 int or_open_node(double r_sq, double len, double l_open, double node_mass, double node_maxsoft,
                  double soft_target, double aold, double theta_sq, double adx, double ady, double adz);
 
@@ -62,6 +63,17 @@ void or_walk_groups(const or_tree* t, int64_t nt, const uint32_t* targets, int64
                     const int64_t* starts, double theta, double G, const double* aold,
                     int leaf_accept, double* ax, double* ay, double* az, double* phi,
                     int64_t* counters);
+/* Node centre-of-mass velocity and speed bound (tree.cc:149-190); arrays of nnodes. */
+void or_velocity_moments(const or_tree* t, const double* vx, const double* vy, const double* vz,
+                         double* vcx, double* vcy, double* vcz, float* vmax);
+/* Grouped walk with the tidal tensor (6 per target, xx yy zz xy yz xz, not times G) and the jerk
+ * (3 per target, times G; needs particle velocities and node vcom); either may be null.
+ * tree.cc:811-837, 845-880. */
+void or_walk_groups_ext(const or_tree* t, int64_t nt, const uint32_t* targets, int64_t ngroups,
+                        const int64_t* starts, double theta, double G, const double* aold,
+                        const double* vx, const double* vy, const double* vz, const double* vcx,
+                        const double* vcy, const double* vcz, double* ax, double* ay, double* az,
+                        double* tidal, double* jerk);
 /* accel_grouped (tree.cc:626-897), gravity only. */
 void or_accel_grouped(const or_tree* t, int64_t nt, const uint32_t* targets, double theta, double G,
                       int batch, const double* aold, double* ax, double* ay, double* az,

@@ -99,6 +99,11 @@ class Restatement:
                                        C.c_int, _d, _d, _d, _d, _i64]
         L.or_accel.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, _d, _d, _d, _d]
         L.or_potential.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, _d, _d]
+        L.or_spline_tidal_factor.restype = C.c_double
+        L.or_spline_tidal_factor.argtypes = [C.c_double, C.c_double]
+        L.or_velocity_moments.argtypes = [C.c_void_p, _d, _d, _d, _d, _d, _d, _f]
+        L.or_walk_groups_ext.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_int64, _i64, C.c_double,
+                                         C.c_double, _d] + [_d] * 11
         L.or_direct.argtypes = [C.c_int64, _d, _d, _d, _d, _d, C.c_int64, _u32, C.c_double,
                                 _d, _d, _d, _d]
 
@@ -225,6 +230,35 @@ class OracleTree:
                                   _p(az, _d), _p(phi, _d), _p(cnt, _i64))
         return ax, ay, az, phi, cnt
 
+    def velocity_moments(self, vel):
+        """Node centre-of-mass velocity (3 arrays) and speed bound for velocities vel = (vx, vy, vz)."""
+        v = [_f64(a) for a in vel]
+        nn = self.nnodes
+        vc = [np.zeros(nn) for _ in range(3)]
+        vmax = np.zeros(nn, np.float32)
+        self.lib.L.or_velocity_moments(self.h, _p(v[0], _d), _p(v[1], _d), _p(v[2], _d), _p(vc[0], _d),
+                                       _p(vc[1], _d), _p(vc[2], _d), _p(vmax, _f))
+        return vc, vmax
+
+    def walk_groups_ext(self, targets, starts, theta, G=1.0, aold=None, vel=None, tidal=True):
+        """Grouped walk with the tidal tensor ([nt, 6], not times G) and, given vel, the jerk ([nt, 3])."""
+        t = _targets(targets)
+        nt = len(t)
+        st = np.ascontiguousarray(starts, np.int64)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        tt = np.zeros((nt, 6)) if tidal else None
+        jj = None
+        v = vc = [None, None, None]
+        if vel is not None:
+            v = [_f64(a) for a in vel]
+            vc, _ = self.velocity_moments(v)
+            jj = np.zeros((nt, 3))
+        ao = _f64(aold) if aold is not None else None
+        self.lib.L.or_walk_groups_ext(self.h, nt, _p(t, _u32), len(st) - 1, _p(st, _i64), theta, G, _p(ao, _d),
+                                      *[_p(a, _d) for a in v], *[_p(a, _d) for a in vc], _p(ax, _d), _p(ay, _d),
+                                      _p(az, _d), _p(tt, _d), _p(jj, _d))
+        return ax, ay, az, tt, jj
+
     def accel_grouped(self, targets, theta, G=1.0, batch=0, aold=None):
         t = _targets(targets)
         nt = len(t)
@@ -291,6 +325,11 @@ class Reference:
         L.ref_spline_potential.argtypes = [C.c_double, C.c_double]
         L.ref_open_node.restype = C.c_int
         L.ref_open_node.argtypes = [C.c_double] * 11
+        L.ref_build_vel.restype = C.c_void_p
+        L.ref_build_vel.argtypes = [C.c_int64] + [_d] * 8 + [C.c_longlong]
+        L.ref_tree_vel.argtypes = [C.c_void_p, _d, _d, _d, _f]
+        L.ref_accel_grouped_ext.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double,
+                                            C.c_int, _d, _d, _d, _d, _d, _d]
 
     def max_threads(self):
         return self.L.ref_max_threads()
@@ -329,20 +368,26 @@ class Reference:
     def open_node(self, *args):
         return self.L.ref_open_node(*[float(a) for a in args])
 
-    def build(self, P, randomize_seed=-1):
-        return ReferenceTree(self, P, randomize_seed)
+    def build(self, P, randomize_seed=-1, vel=None):
+        """vel = (vx, vy, vz): build with velocities (per-node vcom and vmax, for the jerk)."""
+        return ReferenceTree(self, P, randomize_seed, vel)
 
 
 class ReferenceTree:
-    def __init__(self, lib: Reference, P, randomize_seed=-1):
+    def __init__(self, lib: Reference, P, randomize_seed=-1, vel=None):
         self.lib = lib
         x, y, z, m = (_f64(P[k]) for k in ("x", "y", "z", "m"))
         soft = P.get("soft")
         soft = _f64(soft) if soft is not None else None
         self.n = len(m)
         self.build_times = np.zeros(7)
-        self.h = lib.L.ref_build(self.n, _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), _p(soft, _d),
-                                 randomize_seed, _p(self.build_times, _d))
+        if vel is None:
+            self.h = lib.L.ref_build(self.n, _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), _p(soft, _d),
+                                     randomize_seed, _p(self.build_times, _d))
+        else:
+            v = [_f64(a) for a in vel]
+            self.h = lib.L.ref_build_vel(self.n, _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), _p(soft, _d),
+                                         _p(v[0], _d), _p(v[1], _d), _p(v[2], _d), randomize_seed)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -391,6 +436,26 @@ class ReferenceTree:
         self.lib.L.ref_accel_grouped(self.h, nt, _p(t, _u32), theta, G, batch, _p(ao, _d),
                                      _p(ax, _d), _p(ay, _d), _p(az, _d))
         return ax, ay, az
+
+    def accel_grouped_ext(self, targets, theta, G=1.0, batch=0, aold=None, tidal=True, jerk=False):
+        """accel_grouped with the tidal tensor ([nt, 6]: xx yy zz xy yz xz, not times G) and the
+        jerk ([nt, 3], times G; the tree must have been built with velocities)."""
+        t = _targets(targets)
+        nt = len(t)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        tt = np.empty((nt, 6)) if tidal else None
+        jj = np.empty((nt, 3)) if jerk else None
+        ao = _f64(aold) if aold is not None else None
+        self.lib.L.ref_accel_grouped_ext(self.h, nt, _p(t, _u32), theta, G, batch, _p(ao, _d), _p(ax, _d),
+                                         _p(ay, _d), _p(az, _d), _p(tt, _d), _p(jj, _d))
+        return ax, ay, az, tt, jj
+
+    def vel_moments(self):
+        nn = self.nnodes
+        v = [np.zeros(nn) for _ in range(3)]
+        vmax = np.zeros(nn, np.float32)
+        self.lib.L.ref_tree_vel(self.h, _p(v[0], _d), _p(v[1], _d), _p(v[2], _d), _p(vmax, _f))
+        return v, vmax
 
     def accel(self, targets, theta, G=1.0, aold=None):
         t = _targets(targets)

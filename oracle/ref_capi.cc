@@ -27,6 +27,8 @@ namespace {
 struct RefHandle {
     Particles P;
     Tree T;
+    std::vector<double> v[3];  // velocities, when the tree was built with them
+    const double* vel[3] = {nullptr, nullptr, nullptr};
 };
 void split128(peanokey k, uint64_t* hi, uint64_t* lo) {
     const unsigned __int128 u = (unsigned __int128)k;
@@ -34,6 +36,8 @@ void split128(peanokey k, uint64_t* hi, uint64_t* lo) {
     *lo = (uint64_t)u;
 }
 }  // namespace
+
+static_assert(sizeof(SymTensor3d) == 6 * sizeof(double), "SymTensor3d is six doubles");
 
 extern "C" {
 
@@ -54,6 +58,51 @@ void* ref_build(int64_t n, const double* x, const double* y, const double* z, co
         bt_out[4] = bt.links; bt_out[5] = bt.pack; bt_out[6] = bt.total;
     }
     return h;
+}
+
+// shmem::build with velocities and want_vcom (tree.cc:350, 149-190): adds the per-node
+// centre-of-mass velocity (Tree::vcom) and speed bound (Tree::vmax) the jerk needs.
+void* ref_build_vel(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                    const double* soft, const double* vx, const double* vy, const double* vz,
+                    long long randomize_seed) {
+    RefHandle* h = new RefHandle();
+    h->P.x.assign(x, x + n); h->P.y.assign(y, y + n); h->P.z.assign(z, z + n);
+    h->P.m.assign(m, m + n);
+    if (soft) h->P.soft.assign(soft, soft + n);
+    h->v[0].assign(vx, vx + n); h->v[1].assign(vy, vy + n); h->v[2].assign(vz, vz + n);
+    for (int k = 0; k < 3; ++k) h->vel[k] = h->v[k].data();
+    h->T = build(h->P, nullptr, h->vel, true, randomize_seed);
+    return h;
+}
+
+// Per-node centre-of-mass velocity and speed bound (nnodes each; any pointer may be null).
+void ref_tree_vel(void* p, double* vcx, double* vcy, double* vcz, float* vmax) {
+    const Tree& T = static_cast<RefHandle*>(p)->T;
+    const size_t nn = T.nnodes();
+    if (vcx && !T.vcom_x.empty()) std::memcpy(vcx, T.vcom_x.data(), nn * 8);
+    if (vcy && !T.vcom_y.empty()) std::memcpy(vcy, T.vcom_y.data(), nn * 8);
+    if (vcz && !T.vcom_z.empty()) std::memcpy(vcz, T.vcom_z.data(), nn * 8);
+    if (vmax) std::memcpy(vmax, T.vmax.data(), nn * 4);
+}
+
+// shmem::accel_grouped with the tidal tensor (6 per target: xx yy zz xy yz xz, not multiplied by
+// G, tree.cc:876-880) and the jerk (3 per target, times G; needs ref_build_vel).  Either output
+// may be null.
+void ref_accel_grouped_ext(void* p, int64_t nt, const uint32_t* targets, double theta, double G,
+                           int batch, const double* aold, double* ax, double* ay, double* az,
+                           double* tidal, double* jerk) {
+    RefHandle* h = static_cast<RefHandle*>(p);
+    std::vector<uint32_t> tg(targets, targets + nt);
+    std::vector<double> vx, vy, vz;
+    std::vector<SymTensor3d> tt;
+    std::vector<Vec3d> jj;
+    accel_grouped(h->T, h->P, tg, theta, G, batch, vx, vy, vz, tidal ? &tt : nullptr, aold, nullptr,
+                  jerk ? &jj : nullptr, jerk ? h->vel : nullptr);
+    std::memcpy(ax, vx.data(), nt * 8); std::memcpy(ay, vy.data(), nt * 8);
+    std::memcpy(az, vz.data(), nt * 8);
+    if (tidal) std::memcpy(tidal, tt.data(), nt * 6 * 8);
+    for (int64_t i = 0; jerk && i < nt; ++i)
+        for (int k = 0; k < 3; ++k) jerk[3 * i + k] = jj[i][k];
 }
 
 void ref_free(void* p) { delete static_cast<RefHandle*>(p); }

@@ -97,6 +97,21 @@ def main():
     qx, qy, qz = T.accel_brute(sub)
     out["plummer_direct_ax"], out["plummer_direct_ay"], out["plummer_direct_az"] = qx, qy, qz
 
+    # ---- tidal tensor and jerk (tree.cc:811-880) on the same sphere with seeded velocities -----
+    vrng = np.random.default_rng(99)
+    vel = [vrng.normal(0.0, 0.5, 4096) for _ in range(3)]
+    for k, v in zip("xyz", vel):
+        out[f"plummer_v{k}"] = v
+    TV = R.build(P, vel=vel)
+    vc, vmax = TV.vel_moments()
+    for k, v in zip("xyz", vc):
+        out[f"plummer_vcom_{k}"] = v
+    out["plummer_vmax"] = vmax
+    for name, theta, batch, ao in (("bh", 0.7, 0, None), ("b8", 0.7, 8, None), ("rel", 0.0, 0, aold)):
+        _, _, _, tt, jj = TV.accel_grouped_ext(tg, theta, 1.0, batch, aold=ao, tidal=True, jerk=True)
+        out[f"plummer_{name}_tidal"] = tt
+        out[f"plummer_{name}_jerk"] = jj
+
     # ---- collocated particles: the level-20 leaf (tree.cc:89) ----------------------------------
     Q = ics.plummer(n=600, seed=7, soft=0.02)
     Q["x"][:40] = Q["x"][0]
@@ -121,6 +136,19 @@ def main():
     acc = txt.split("=== build")[0]
     rows = re.findall(r"^\s+([0-9.]+)\s+([0-9.e+-]+)\s+([0-9.e+-]+)\s+([0-9.e+-]+)\s*$", acc, re.M)
     out["test_tree_table"] = np.array([[float(v) for v in r] for r in rows])
+
+    # ---- the reference's shmem/bench_treeforce.cc on a synthetic state: its printed checksums ----
+    import tempfile
+
+    Ps, vel = ics.plummer_state()
+    with tempfile.TemporaryDirectory() as d:
+        state = os.path.join(d, "state.bin")
+        ics.write_state(state, Ps, vel)
+        exe = os.path.join(ROOT, "oracle", "_ref", "bench_treeforce")
+        txt = subprocess.run([exe, state, "1"], capture_output=True, text=True, check=True,
+                             env=dict(os.environ, OMP_NUM_THREADS="4")).stdout
+    sums = re.findall(r"sum_a=(\S+) sum_t=(\S+) sum_j=(\S+)", txt)
+    out["treeforce_sums"] = np.array([[float(v) for v in r] for r in sums])
 
     path = os.path.join(HERE, "golden.npz")
     np.savez_compressed(path, **out)

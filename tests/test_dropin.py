@@ -46,3 +46,31 @@ def test_reference_test_tree_runs_on_the_gpu_tree():
         assert med_ == pytest.approx(rmed, rel=1e-2)
         assert p99_ == pytest.approx(rp99, rel=1e-2)
         assert max_ == pytest.approx(rmax, rel=5e-2)
+
+
+@pytest.mark.gpu
+def test_reference_bench_treeforce_runs_on_the_gpu_tree(tmp_path):
+    """shmem/bench_treeforce.cc: one all-active walk producing the acceleration, then also the
+    tidal tensor, then also the jerk (batch 8, theta 0.5, node velocities from the build), on a
+    synthetic Plummer state.  Its printed checksums are compared with the same program on the
+    reference's own tree (tests/golden/make_golden.py).  The tidal trace sum is dominated by the
+    softened pairs and must agree to 1e-4; the acceleration and jerk sums are near-cancelling
+    residuals of 200,000 terms, so they are compared against an absolute bound set by FP32
+    interaction arithmetic (per-particle error ~1e-6 of |a| ~ 10)."""
+    from gizmo_shared_memory_b200 import ics
+
+    P, vel = ics.plummer_state()
+    state = tmp_path / "state.bin"
+    ics.write_state(str(state), P, vel)
+    out = subprocess.run(["stdbuf", "-oL", binary("bench_treeforce"), str(state), "2"], capture_output=True,
+                         text=True, timeout=600, env=dict(os.environ, OMP_NUM_THREADS="4"))
+    assert out.returncode == 0, (out.returncode, out.stdout[-3000:], out.stderr[-2000:])
+    sums = np.array([[float(v) for v in r] for r in
+                     re.findall(r"sum_a=(\S+) sum_t=(\S+) sum_j=(\S+)", out.stdout)])
+    assert sums.shape == (3, 3), out.stdout
+    ref = np.load(os.path.join(ROOT, "tests", "golden", "golden.npz"))["treeforce_sums"]
+    assert np.all(sums[0, 1:] == 0) and sums[1, 2] == 0
+    assert sums[1, 1] == pytest.approx(ref[1, 1], rel=1e-4)
+    assert sums[2, 1] == pytest.approx(ref[2, 1], rel=1e-4)
+    assert np.all(np.abs(sums[:, 0] - ref[:, 0]) < 5e-2)
+    assert abs(sums[2, 2] - ref[2, 2]) < 5e-2 * max(1.0, abs(ref[2, 2]))

@@ -134,6 +134,30 @@ def test_walks_match_golden(oracle, golden):
     assert relerr(dx, dy, dz, golden["plummer_direct_ax"], golden["plummer_direct_ay"], golden["plummer_direct_az"]).max() < 1e-12
 
 
+def test_tidal_and_jerk_match_golden(oracle, golden):
+    """The restatement's node velocity moments, tidal tensor and jerk against the reference's
+    (tree.cc:149-190, 811-880), for leaf groups, windows of 8 and the relative criterion."""
+    P = particles(golden, "plummer")
+    T = oracle.build(P)
+    vel = [golden[f"plummer_v{k}"] for k in "xyz"]
+    vc, vmax = T.velocity_moments(vel)
+    for k, v in zip("xyz", vc):
+        np.testing.assert_allclose(v, golden[f"plummer_vcom_{k}"], rtol=1e-12, atol=1e-15)
+    assert np.array_equal(vmax, golden["plummer_vmax"])
+    tg = golden["plummer_orderbuf"]
+    for name, theta, batch, aold in (("bh", 0.7, 0, None), ("b8", 0.7, 8, None),
+                                     ("rel", 0.0, 0, golden["plummer_aold"])):
+        starts = T.groups(tg, batch)
+        _, _, _, tt, jj = T.walk_groups_ext(tg, starts, theta, aold=aold, vel=vel)
+        gt, gj = golden[f"plummer_{name}_tidal"], golden[f"plummer_{name}_jerk"]
+        tn = np.linalg.norm(gt, axis=1)
+        jn = np.linalg.norm(gj, axis=1)
+        assert (np.linalg.norm(tt - gt, axis=1) / tn).max() < 1e-12, name
+        assert (np.linalg.norm(jj - gj, axis=1) / jn).max() < 1e-12, name
+        # far from every softening the Newtonian tidal tensor is trace-free
+        assert np.median(np.abs(gt[:, 0] + gt[:, 1] + gt[:, 2]) / tn) < 1e-3
+
+
 def test_collocated_matches_golden(oracle, golden):
     Q = particles(golden, "colloc")
     T = oracle.build(Q)
