@@ -227,6 +227,72 @@ def read_profile_traffic(workload):
         return None
 
 
+MAC_MODEL = os.path.join(ROOT, "gizmo_shared_memory_b200", "mac_node_model.npy")
+
+
+def learned_at_equal_p99(args, ctx, g, T, aold, wopts, sample, dref, p99_target, nl, world, dist):
+    """The per-node learned criterion (GT_MAC_NODE, model trained on the Plummer and galaxy
+    workloads by gizmo_shared_memory_b200/train_mac.py) at the largest kappa whose sampled p99 on
+    the same 4096 targets does not exceed the plain walk's, timed like the plain walk."""
+    import torch
+
+    if not os.path.exists(MAC_MODEL):
+        return {"unavailable": "no trained model (python -m gizmo_shared_memory_b200.train_mac)"}
+    model = np.load(MAC_MODEL).astype(np.float32)
+    meta_path = os.path.splitext(MAC_MODEL)[0] + ".json"
+    c0 = json.load(open(meta_path))["median_prediction"] if os.path.exists(meta_path) else 0.0
+    smp = torch.as_tensor(sample.astype(np.int64), device="cuda")
+    ref = np.stack(dref[:3])
+
+    def p99_at(kappa):
+        full = ctx.accel_grouped(T, None, aold=aold, out_order=g.GT_OUT_ORIGINAL, mac=g.GT_MAC_NODE,
+                                 mac_model=model, mac_kappa=kappa, **wopts)
+        got = np.stack([f[smp].cpu().numpy() for f in full])
+        e = np.linalg.norm(got - ref, axis=0) / np.linalg.norm(ref, axis=0)
+        return float(np.quantile(e, 0.99)), float(np.median(e))
+
+    # bisection on log kappa: the accepted bracket end is the fastest criterion meeting the target
+    lo, hi = math.log10(0.05) + c0, math.log10(5.0) + c0
+    best = None
+    for _ in range(9):
+        mid = 0.5 * (lo + hi)
+        p99, med = p99_at(10 ** mid)
+        if p99 <= p99_target:
+            best = (10 ** mid, p99, med)
+            lo = mid
+        else:
+            hi = mid
+    if best is None:
+        return {"unavailable": "no kappa in the bracket met the plain walk's p99"}
+    kappa, p99, med = best
+    lw = dict(mac=g.GT_MAC_NODE, mac_model=model, mac_kappa=kappa, **wopts)
+    nl_ = nl
+    out = tuple(torch.empty(nl_, dtype=torch.float64, device="cuda") for _ in range(3))
+    ctx.accel_grouped(T, None, aold=aold, outs=out + (None,), count=True, **lw)
+    st = ctx.stats()
+    for _ in range(3):
+        ctx.accel_grouped(T, None, aold=aold, outs=out + (None,), async_=True, **lw)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.accel_grouped(T, None, aold=aold, outs=out + (None,), async_=True, **lw)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / args.steps
+    if dist:
+        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt[0])
+    return {"criterion": "per-node learned correction (GT_MAC_NODE), node-only features, trained on the "
+                         "Plummer 65k and galaxy 4M workloads", "kappa": kappa, "p99": p99, "median": med,
+            "p99_target": p99_target, "value": nl_ * world / t, "ms_per_step": 1e3 * t,
+            "interactions_per_particle": (st["multipole"] + st["pairs"]) / nl_}
+
+
 def run_gpu_arm(args):
     import torch
 
@@ -312,6 +378,11 @@ def run_gpu_arm(args):
     err = relerr([full[k][sample] for k in range(3)], dref[:3])
     err_med, err_p99 = float(np.median(err)), float(np.quantile(err, 0.99))
 
+    # the learned criterion at the same sampled p99 (the metric's comparison)
+    learned = None
+    if not args.no_learned:
+        learned = learned_at_equal_p99(args, ctx, g, T, aold, wopts, sample, dref, err_p99, nl, world, dist)
+
     # end to end through the C ABI with host buffers (pinned), build + walk every step
     e2e = None
     if not args.no_e2e:
@@ -358,6 +429,8 @@ def run_gpu_arm(args):
                               f"tree prebuilt ({tbuild:.1f} s CPU build, not timed)"}
 
     achieved = FLOPS_PER_INTERACTION * inter / t_kernel / 1e12
+    if learned and "value" in learned:
+        learned["speedup_vs_plain"] = learned["value"] / value
     line = {
         "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_step,
@@ -387,6 +460,7 @@ def run_gpu_arm(args):
         "interactions_per_s": inter * world / t_step,
         "walk_stats": {k: st[k] for k in ("groups", "nodes_visited", "multipole", "pairs", "max_stack")},
         "build_ms": info["build_ms"],
+        "learned": learned,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -534,6 +608,7 @@ def main():
     ap.add_argument("--sample-seconds", type=float, default=8.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-criterion comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warm-up raised to 3 steps (timing rule)")

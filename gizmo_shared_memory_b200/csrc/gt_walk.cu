@@ -294,6 +294,11 @@ walk_kernel(const WalkArgs A) {
             sx[k] = sy[k] = sz[k] = cxk[k] = cyk[k] = czk[k] = 0.0f;
             pot[k] = 0.0;
         }
+        // monopole-list entry pos (paired layout, see flush_pn)
+        auto pn_put = [&](int pos, float x, float y, float z, float m) {
+            float* q = reinterpret_cast<float*>(pn + 2 * (pos >> 1)) + (pos & 1);
+            q[0] = x; q[2] = y; q[4] = z; q[6] = m;
+        };
         // tidal tensor and jerk: FP64 totals (xx yy zz xy yz xz, jx jy jz) and target velocities
         double xt[9][TPL];
         float tvx[TPL], tvy[TPL], tvz[TPL];
@@ -344,37 +349,95 @@ walk_kernel(const WalkArgs A) {
         };
         // Monopoles.  An accepted node passed the softening-overlap test, so every target of the
         // group is farther than max(h_target, h_node) from it: the interaction is Newtonian.
+        // The list pairs its entries: entries 2p and 2p+1 share two float4s, {x0, x1, y0, y1} and
+        // {z0, z1, m0, m1}, so two 16-byte loads put a pair straight into the register pairs of the
+        // sm_100 packed FP32 instructions (FADD2 / FMUL2 / FFMA2): two interactions per
+        // instruction, each with exactly the scalar rounding.  An odd list is padded with a
+        // massless entry, which the r^2 guard turns into an exact zero.
         auto flush_pn = [&](int n) {
+            if ((n & 1) && lane == 0) {
+                pn_put(n, 0.0f, 0.0f, 0.0f, 0.0f);
+                if (want_jerk) pnv[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
             __syncwarp();
+            const int np = (n + 1) >> 1;
             float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
             float xq[XT ? TPL : 1][9];
 #pragma unroll
             for (int k = 0; k < TPL; ++k) ax_[k] = ay_[k] = az_[k] = ap_[k] = 0.0f;
-            if (XT) {
-#pragma unroll
-                for (int k = 0; k < TPL; ++k)
-#pragma unroll
-                    for (int c = 0; c < 9; ++c) xq[XT ? k : 0][c] = 0.0f;
-            }
-#pragma unroll 4
-            for (int j = slice; j < n; j += NS) {
-                const float4 e = pn[j];
+            // packed for full groups; groups of <= 16 targets split the list over lane slices, where
+            // the scalar loop measured faster
+            if (!XT && NS == 1) {
+                float2 ax2[TPL], ay2[TPL], az2[TPL], ap2[TPL];
+                float2 ntx[TPL], nty[TPL], ntz[TPL];
 #pragma unroll
                 for (int k = 0; k < TPL; ++k) {
-                    if (k < nk) {
-                        const float dx = e.x - tx[k], dy = e.y - ty[k], dz = e.z - tz[k];
-                        const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-30f);
-                        const float ri = rsqrtf(r2);
-                        const float mri = e.w * ri;
-                        const float f = mri * (ri * ri);
-                        ax_[k] = fmaf(dx, f, ax_[k]);
-                        ay_[k] = fmaf(dy, f, ay_[k]);
-                        az_[k] = fmaf(dz, f, az_[k]);
-                        if (WANT_POT) ap_[k] -= mri;
-                        if (XT) {
-                            // Newtonian: g2 = 3 m / r^5
-                            const float4 ev = want_jerk ? pnv[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-                            xt_add(xq[XT ? k : 0], dx, dy, dz, f, 3.0f * f * (ri * ri), ev, k);
+                    ax2[k] = ay2[k] = az2[k] = ap2[k] = make_float2(0.0f, 0.0f);
+                    ntx[k] = make_float2(-tx[k], -tx[k]);
+                    nty[k] = make_float2(-ty[k], -ty[k]);
+                    ntz[k] = make_float2(-tz[k], -tz[k]);
+                }
+#pragma unroll 2
+                for (int jp = slice; jp < np; jp += NS) {
+                    const float4 A = pn[2 * jp], B = pn[2 * jp + 1];
+                    const float2 X = make_float2(A.x, A.y), Y = make_float2(A.z, A.w);
+                    const float2 Z = make_float2(B.x, B.y), M = make_float2(B.z, B.w);
+#pragma unroll
+                    for (int k = 0; k < TPL; ++k) {
+                        if (k < nk) {
+                            const float2 dx = __fadd2_rn(X, ntx[k]), dy = __fadd2_rn(Y, nty[k]);
+                            const float2 dz = __fadd2_rn(Z, ntz[k]);
+                            float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+                            r2.x = fmaxf(r2.x, 1e-30f);
+                            r2.y = fmaxf(r2.y, 1e-30f);
+                            const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+                            const float2 mri = __fmul2_rn(M, ri);
+                            const float2 f = __fmul2_rn(mri, __fmul2_rn(ri, ri));
+                            ax2[k] = __ffma2_rn(dx, f, ax2[k]);
+                            ay2[k] = __ffma2_rn(dy, f, ay2[k]);
+                            az2[k] = __ffma2_rn(dz, f, az2[k]);
+                            if (WANT_POT) ap2[k] = __fadd2_rn(ap2[k], mri);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < TPL; ++k) {
+                    ax_[k] = ax2[k].x + ax2[k].y;
+                    ay_[k] = ay2[k].x + ay2[k].y;
+                    az_[k] = az2[k].x + az2[k].y;
+                    ap_[k] = -(ap2[k].x + ap2[k].y);
+                }
+            } else {
+                if (XT) {
+#pragma unroll
+                    for (int k = 0; k < TPL; ++k)
+#pragma unroll
+                        for (int c = 0; c < 9; ++c) xq[XT ? k : 0][c] = 0.0f;
+                }
+                for (int jp = slice; jp < np; jp += NS) {
+                    const float4 A = pn[2 * jp], B = pn[2 * jp + 1];
+#pragma unroll
+                    for (int sl = 0; sl < 2; ++sl) {
+                        const int j = 2 * jp + sl;
+                        const float4 e = sl ? make_float4(A.y, A.w, B.y, B.w) : make_float4(A.x, A.z, B.x, B.z);
+#pragma unroll
+                        for (int k = 0; k < TPL; ++k) {
+                            if (k < nk) {
+                                const float dx = e.x - tx[k], dy = e.y - ty[k], dz = e.z - tz[k];
+                                const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-30f);
+                                const float ri = rsqrtf(r2);
+                                const float mri = e.w * ri;
+                                const float f = mri * (ri * ri);
+                                ax_[k] = fmaf(dx, f, ax_[k]);
+                                ay_[k] = fmaf(dy, f, ay_[k]);
+                                az_[k] = fmaf(dz, f, az_[k]);
+                                if (WANT_POT) ap_[k] -= mri;
+                                if (XT) {
+                                    // Newtonian: g2 = 3 m / r^5
+                                    const float4 ev = want_jerk ? pnv[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                                    xt_add(xq[XT ? k : 0], dx, dy, dz, f, 3.0f * f * (ri * ri), ev, k);
+                                }
+                            }
                         }
                     }
                 }
@@ -533,8 +596,8 @@ walk_kernel(const WalkArgs A) {
                 if (npn + na > A.pn_cap) { flush_pn(npn); npn = 0; }
                 if (accept) {
                     const int pos = npn + __popc(am & lt_mask);
-                    pn[pos] = make_float4((float)(nd.cx - S.c_x), (float)(nd.cy - S.c_y),
-                                          (float)(nd.cz - S.c_z), (float)nd.mass);
+                    pn_put(pos, (float)(nd.cx - S.c_x), (float)(nd.cy - S.c_y), (float)(nd.cz - S.c_z),
+                           (float)nd.mass);
                     if (want_jerk) pnv[pos] = A.nvel[node];  // the node's centre-of-mass velocity
                 }
                 npn += na;
@@ -584,7 +647,7 @@ walk_kernel(const WalkArgs A) {
                     if (npp + nn > A.pp_cap) { flush_pp(npp); npp = 0; }
                     const float4 e = make_float4((float)(qx - S.c_x), (float)(qy - S.c_y), (float)(qz - S.c_z), qm);
                     if (live && far) {
-                        pn[npn + __popc(fm & lt_mask)] = e;
+                        pn_put(npn + __popc(fm & lt_mask), e.x, e.y, e.z, e.w);
                         if (want_jerk) pnv[npn + __popc(fm & lt_mask)] = A.svel[qpos];
                     } else if (live) {
                         const int pos = npp + __popc(nm & lt_mask);
