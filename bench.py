@@ -42,6 +42,8 @@ WORKLOADS = {
     "galaxy_4m": dict(desc="Hernquist halo 3,145,728 + exponential disk 1,048,576, softening "
                            "0.005/0.002", alpha=0.0025),
     "plummer_65k": dict(desc="Plummer sphere N=65,536, truncated at 20a, softening 0.01", alpha=0.005),
+    "merger_67m": dict(desc="two isolated galaxies of 33,554,432 particles each (halo + disk, masses halved), "
+                            "centres 20 scale radii apart, the second rotated at random", alpha=0.0025),
 }
 
 
@@ -58,6 +60,8 @@ def make_workload(name, seed_offset=0):
         return ics.galaxy(seed=2 + seed_offset)
     if name == "plummer_65k":
         return ics.plummer(n=65536, seed=42 + seed_offset)
+    if name == "merger_67m":
+        return ics.merger(seed=5 + seed_offset)
     raise SystemExit(f"unknown workload {name}")
 
 

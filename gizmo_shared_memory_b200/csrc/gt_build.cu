@@ -146,17 +146,18 @@ __global__ void root_geom_kernel(const double* __restrict__ part, const unsigned
     *bad_out = bad;
 }
 
-// Forest: one block per system reduces its input range and finishes that system's root cell.
-// bad_out accumulates the non-finite count over all systems.
+// Forest: `chunks` blocks per system each reduce a slice of that system's input range into a
+// partial box (6 doubles) and counts (live, non-finite); root_systems_kernel combines them.
 __global__ void bbox_systems_kernel(const double* __restrict__ x, const double* __restrict__ y,
                                     const double* __restrict__ z, const double* __restrict__ m,
                                     const double* __restrict__ soft, const int64_t* __restrict__ off,
-                                    RootGeom* __restrict__ geoms, unsigned long long* __restrict__ bad_out,
-                                    long long seed, double fx, double fy, double fz, int max_level) {
-    const int s = blockIdx.x;
+                                    int chunks, double* __restrict__ part, unsigned long long* __restrict__ cnt) {
+    const int s = blockIdx.x / chunks, c0 = blockIdx.x % chunks;
+    const int64_t a = off[s], len = off[s + 1] - off[s];
+    const int64_t lo_i = a + len * c0 / chunks, hi_i = a + len * (c0 + 1) / chunks;
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     unsigned long long live = 0, bad = 0;
-    for (int64_t i = off[s] + threadIdx.x; i < off[s + 1]; i += blockDim.x) {
+    for (int64_t i = lo_i + threadIdx.x; i < hi_i; i += blockDim.x) {
         const double xi = x[i], yi = y[i], zi = z[i], mi = m[i];
         const double si = soft ? soft[i] : 0.0;
         if (!isfinite(xi) || !isfinite(yi) || !isfinite(zi) || !isfinite(mi) || !isfinite(si)) ++bad;
@@ -188,9 +189,32 @@ __global__ void bbox_systems_kernel(const double* __restrict__ x, const double* 
             }
             live += sc[k][0]; bad += sc[k][1];
         }
-        finish_root(lo, hi, live, geoms + s, seed, fx, fy, fz, max_level);
-        if (bad) atomicAdd(bad_out, bad);
+        for (int c = 0; c < 3; ++c) { part[6 * blockIdx.x + c] = lo[c]; part[6 * blockIdx.x + 3 + c] = hi[c]; }
+        cnt[2 * blockIdx.x] = live;
+        cnt[2 * blockIdx.x + 1] = bad;
     }
+}
+
+// One thread per system: combine its chunks and finish its root cell; the non-finite counts add
+// up into bad_out.
+__global__ void root_systems_kernel(const double* __restrict__ part, const unsigned long long* __restrict__ cnt,
+                                    int n_systems, int chunks, RootGeom* __restrict__ geoms,
+                                    unsigned long long* __restrict__ bad_out, long long seed, double fx, double fy,
+                                    double fz, int max_level) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_systems) return;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    unsigned long long live = 0, bad = 0;
+    for (int k = s * chunks; k < (s + 1) * chunks; ++k) {
+        for (int c = 0; c < 3; ++c) {
+            lo[c] = fmin(lo[c], part[6 * k + c]);
+            hi[c] = fmax(hi[c], part[6 * k + 3 + c]);
+        }
+        live += cnt[2 * k];
+        bad += cnt[2 * k + 1];
+    }
+    finish_root(lo, hi, live, geoms + s, seed, fx, fy, fz, max_level);
+    if (bad) atomicAdd(bad_out, bad);
 }
 
 // ---- 2. keys ---------------------------------------------------------------------------------
@@ -619,14 +643,24 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
                                           o.shift[1], o.shift[2], o.max_level);
         check_launch(ctx, "root_geom_kernel");
     } else {
-        in_off_dev = (int64_t*)scratch(ctx, kSlotPartials, (size_t)(S + 1) * 8);
+        // chunks per system: enough blocks that the largest system is not one block's serial work
+        int64_t nmax = 0;
+        for (int s = 0; s < S; ++s) nmax = std::max<int64_t>(nmax, in_off[s + 1] - in_off[s]);
+        const int chunks = (int)std::min<int64_t>(64, std::max<int64_t>(1, (nmax + 8191) / 8192));
+        const size_t nparts = (size_t)S * chunks;
+        char* ws = (char*)scratch(ctx, kSlotPartials, (size_t)(S + 1) * 8 + nparts * 64 + 256);
+        in_off_dev = (int64_t*)ws;
+        double* part = (double*)(ws + (((size_t)(S + 1) * 8 + 15) & ~(size_t)15));
+        unsigned long long* cnt = (unsigned long long*)(part + nparts * 6);
         // pageable source: the copy is staged before the call returns, in_off may go away after
         check_cuda(cudaMemcpyAsync(in_off_dev, in_off, (size_t)(S + 1) * 8, cudaMemcpyHostToDevice, st),
                    "offsets h2d");
         check_cuda(cudaMemsetAsync(bad_dev, 0, 8, st), "memset");
-        bbox_systems_kernel<<<S, kBlk, 0, st>>>(x, y, z, m, soft, in_off_dev, gdev, bad_dev, o.randomize_seed,
-                                                o.shift[0], o.shift[1], o.shift[2], o.max_level);
+        bbox_systems_kernel<<<(int)nparts, kBlk, 0, st>>>(x, y, z, m, soft, in_off_dev, chunks, part, cnt);
         check_launch(ctx, "bbox_systems_kernel");
+        root_systems_kernel<<<div_up(S, 128), 128, 0, st>>>(part, cnt, S, chunks, gdev, bad_dev, o.randomize_seed,
+                                                            o.shift[0], o.shift[1], o.shift[2], o.max_level);
+        check_launch(ctx, "root_systems_kernel");
     }
     {
         t->sys_geom.resize(S);

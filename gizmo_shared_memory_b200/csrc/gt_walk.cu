@@ -295,9 +295,16 @@ walk_kernel(const WalkArgs A) {
             pot[k] = 0.0;
         }
         // monopole-list entry pos (paired layout, see flush_pn)
+        // The monopole list is paired (see flush_pn) for the packed evaluation of full groups
+        // and one float4 per entry otherwise (warp-uniform: the group size decides).
+        const bool paired = !XT && NS == 1;
         auto pn_put = [&](int pos, float x, float y, float z, float m) {
-            float* q = reinterpret_cast<float*>(pn + 2 * (pos >> 1)) + (pos & 1);
-            q[0] = x; q[2] = y; q[4] = z; q[6] = m;
+            if (paired) {
+                float* q = reinterpret_cast<float*>(pn + 2 * (pos >> 1)) + (pos & 1);
+                q[0] = x; q[2] = y; q[4] = z; q[6] = m;
+            } else {
+                pn[pos] = make_float4(x, y, z, m);
+            }
         };
         // tidal tensor and jerk: FP64 totals (xx yy zz xy yz xz, jx jy jz) and target velocities
         double xt[9][TPL];
@@ -355,10 +362,7 @@ walk_kernel(const WalkArgs A) {
         // instruction, each with exactly the scalar rounding.  An odd list is padded with a
         // massless entry, which the r^2 guard turns into an exact zero.
         auto flush_pn = [&](int n) {
-            if ((n & 1) && lane == 0) {
-                pn_put(n, 0.0f, 0.0f, 0.0f, 0.0f);
-                if (want_jerk) pnv[n] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
+            if (paired && (n & 1) && lane == 0) pn_put(n, 0.0f, 0.0f, 0.0f, 0.0f);
             __syncwarp();
             const int np = (n + 1) >> 1;
             float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
@@ -367,7 +371,7 @@ walk_kernel(const WalkArgs A) {
             for (int k = 0; k < TPL; ++k) ax_[k] = ay_[k] = az_[k] = ap_[k] = 0.0f;
             // packed for full groups; groups of <= 16 targets split the list over lane slices, where
             // the scalar loop measured faster
-            if (!XT && NS == 1) {
+            if (paired) {
                 float2 ax2[TPL], ay2[TPL], az2[TPL], ap2[TPL];
                 float2 ntx[TPL], nty[TPL], ntz[TPL];
 #pragma unroll
@@ -414,29 +418,25 @@ walk_kernel(const WalkArgs A) {
 #pragma unroll
                         for (int c = 0; c < 9; ++c) xq[XT ? k : 0][c] = 0.0f;
                 }
-                for (int jp = slice; jp < np; jp += NS) {
-                    const float4 A = pn[2 * jp], B = pn[2 * jp + 1];
+#pragma unroll 4
+                for (int j = slice; j < n; j += NS) {
+                    const float4 e = pn[j];
 #pragma unroll
-                    for (int sl = 0; sl < 2; ++sl) {
-                        const int j = 2 * jp + sl;
-                        const float4 e = sl ? make_float4(A.y, A.w, B.y, B.w) : make_float4(A.x, A.z, B.x, B.z);
-#pragma unroll
-                        for (int k = 0; k < TPL; ++k) {
-                            if (k < nk) {
-                                const float dx = e.x - tx[k], dy = e.y - ty[k], dz = e.z - tz[k];
-                                const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-30f);
-                                const float ri = rsqrtf(r2);
-                                const float mri = e.w * ri;
-                                const float f = mri * (ri * ri);
-                                ax_[k] = fmaf(dx, f, ax_[k]);
-                                ay_[k] = fmaf(dy, f, ay_[k]);
-                                az_[k] = fmaf(dz, f, az_[k]);
-                                if (WANT_POT) ap_[k] -= mri;
-                                if (XT) {
-                                    // Newtonian: g2 = 3 m / r^5
-                                    const float4 ev = want_jerk ? pnv[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-                                    xt_add(xq[XT ? k : 0], dx, dy, dz, f, 3.0f * f * (ri * ri), ev, k);
-                                }
+                    for (int k = 0; k < TPL; ++k) {
+                        if (k < nk) {
+                            const float dx = e.x - tx[k], dy = e.y - ty[k], dz = e.z - tz[k];
+                            const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-30f);
+                            const float ri = rsqrtf(r2);
+                            const float mri = e.w * ri;
+                            const float f = mri * (ri * ri);
+                            ax_[k] = fmaf(dx, f, ax_[k]);
+                            ay_[k] = fmaf(dy, f, ay_[k]);
+                            az_[k] = fmaf(dz, f, az_[k]);
+                            if (WANT_POT) ap_[k] -= mri;
+                            if (XT) {
+                                // Newtonian: g2 = 3 m / r^5
+                                const float4 ev = want_jerk ? pnv[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                                xt_add(xq[XT ? k : 0], dx, dy, dz, f, 3.0f * f * (ri * ri), ev, k);
                             }
                         }
                     }
