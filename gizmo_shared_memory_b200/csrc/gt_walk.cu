@@ -381,7 +381,7 @@ walk_kernel(const WalkArgs A) {
                     nty[k] = make_float2(-ty[k], -ty[k]);
                     ntz[k] = make_float2(-tz[k], -tz[k]);
                 }
-#pragma unroll 2
+#pragma unroll 4
                 for (int jp = slice; jp < np; jp += NS) {
                     const float4 A = pn[2 * jp], B = pn[2 * jp + 1];
                     const float2 X = make_float2(A.x, A.y), Y = make_float2(A.z, A.w);
