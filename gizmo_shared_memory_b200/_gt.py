@@ -39,7 +39,8 @@ EXPORTS = [
     "gt_measure_peaks", "gt_direct_noalloc", "gt_mac_train_options_default", "gt_mac_sample",
     "gt_mac_train", "gt_mac_predict", "gt_mac_gradient", "gt_build_systems", "gt_tree_systems",
     "gt_plan_create", "gt_plan_launch", "gt_plan_destroy", "gt_tune_options_default", "gt_autotune",
-    "gt_accel_grouped_ext", "gt_tree_velocities", "gt_tree_velocity_moments",
+    "gt_accel_grouped_ext", "gt_tree_velocities", "gt_tree_velocity_moments", "gt_tree_events",
+    "gt_tree_refresh", "gt_tree_node_state", "gt_tree_particles",
 ]
 
 
@@ -144,6 +145,10 @@ def load_library(path: str = LIB_PATH):
                                        C.c_int, vp, vp, vp, vp, vp, vp]
     L.gt_tree_velocities.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_int]
     L.gt_tree_velocity_moments.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.gt_tree_events.argtypes = [vp, vp, C.c_int, i64, vp, vp, vp, vp, vp, d, d, C.c_int]
+    L.gt_tree_refresh.argtypes = [vp, vp, d]
+    L.gt_tree_node_state.argtypes = [vp, vp, d, vp, vp, vp, vp, vp]
+    L.gt_tree_particles.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int]
     L.gt_potential.argtypes = [vp, vp, i64, vp, d, d, vp, C.c_int, vp]
     L.gt_walk_stats_get.argtypes = [vp, C.POINTER(WalkStats)]
     L.gt_form_aold.argtypes = [vp, i64, vp, vp, vp, d, d, C.c_int, vp]
@@ -544,6 +549,33 @@ class Context:
             vx, vy, vz = (np.ascontiguousarray(a, np.float64) for a in (vx, vy, vz))
         self._check(load_library().gt_tree_velocities(self.h, tree.h, _ptr(vx), _ptr(vy), _ptr(vz),
                                                       int(particles_only), GT_MEM_DEVICE if dev else GT_MEM_HOST))
+
+    # ---- tree reuse ---------------------------------------------------------------------------
+    def tree_events(self, tree: Tree, kind, leaf, a=None, x=None, v=None, f=None, tau=0.0, box=0.0):
+        """Events of one kind (GT_EVENT_*: 0 kick, 1 shift, 2 vmax, 3 soft, 4 mass, 5 pad) on
+        leaf nodes of this tree, host arrays."""
+        lf = np.ascontiguousarray(leaf, np.int32)
+        cv = lambda q, dt: None if q is None else np.ascontiguousarray(q, dt)
+        a, x, v, f = cv(a, np.float64), cv(x, np.float64), cv(v, np.float64), cv(f, np.float32)
+        self._check(load_library().gt_tree_events(self.h, tree.h, kind, len(lf), _ptr(lf), _ptr(a), _ptr(x),
+                                                  _ptr(v), _ptr(f), tau, box, GT_MEM_HOST))
+
+    def tree_refresh(self, tree: Tree, tau):
+        self._check(load_library().gt_tree_refresh(self.h, tree.h, tau))
+
+    def tree_node_state(self, tree: Tree, tau):
+        nn = max(tree.info()["n_nodes"], 1)
+        out = {"com": np.empty((nn, 3)), "vel": np.empty((nn, 3)), "mass": np.empty(nn),
+               "vmax": np.empty(nn, np.float32), "xpad": np.empty(nn, np.float32)}
+        self._check(load_library().gt_tree_node_state(self.h, tree.h, tau, _ptr(out["com"]), _ptr(out["vel"]),
+                                                      _ptr(out["mass"]), _ptr(out["vmax"]), _ptr(out["xpad"])))
+        return out
+
+    def tree_particles(self, tree: Tree, x=None, y=None, z=None, m=None, soft=None):
+        cv = lambda q: None if q is None else np.ascontiguousarray(q, np.float64)
+        x, y, z, m, soft = (cv(q) for q in (x, y, z, m, soft))
+        self._check(load_library().gt_tree_particles(self.h, tree.h, _ptr(x), _ptr(y), _ptr(z), _ptr(m),
+                                                     _ptr(soft), GT_MEM_HOST))
 
     def velocity_moments(self, tree: Tree):
         nn = tree.info()["n_nodes"]

@@ -121,7 +121,8 @@ void check_mem(int mem) {
 void free_tree_arrays(gt_tree* t) {
     void* ptrs[] = {t->src, t->ssoft, t->smass, t->order, t->rank, t->leaf_of, t->sleaf, t->skey,
                     t->nodes, t->parent, t->next, t->level, t->size, t->delta, t->nsoft, t->gc,
-                    t->nq2, t->sys_off_dev, t->geom_dev, t->svel, t->nvel, t->vcom, t->vmax};
+                    t->nq2, t->sys_off_dev, t->geom_dev, t->svel, t->nvel, t->vcom, t->vmax,
+                    t->m0, t->c0, t->dp, t->dq, t->dmass, t->xpad};
     // tree arrays came from the stream-ordered pool: hand them back to it (callers have synchronised)
     for (void* p : ptrs)
         if (p) cudaFreeAsync(p, 0);
@@ -660,6 +661,80 @@ int gt_tree_velocities(gt_context* ctx, gt_tree* tree, const double* vx, const d
         if (particles_only && !tree->svel) throw Fail{GT_ERR_INVALID, "no node velocities to keep yet"};
         tree_velocities(ctx, tree, dx, dy, dz, particles_only != 0);
         finish(ctx, true);
+    });
+}
+
+int gt_tree_events(gt_context* ctx, gt_tree* tree, int kind, int64_t n, const int32_t* leaf, const double* a,
+                   const double* x, const double* v, const float* f, double tau, double box, int mem) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (!tree || n < 0) throw Fail{GT_ERR_INVALID, "null tree or negative count"};
+        if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "tree and context are on different devices"};
+        if (kind < GT_EVENT_KICK || kind > GT_EVENT_PAD) throw Fail{GT_ERR_INVALID, "unknown event kind"};
+        if (n == 0) return;
+        const bool need_a = kind != GT_EVENT_VMAX, need_x = kind == GT_EVENT_SHIFT || kind == GT_EVENT_MASS;
+        if (!leaf || (need_a && !a) || (need_x && !x) || (kind == GT_EVENT_MASS && !v) ||
+            (kind == GT_EVENT_VMAX && !f))
+            throw Fail{GT_ERR_INVALID, "null event array"};
+        if (mem == GT_MEM_HOST)
+            for (int64_t e = 0; e < n; ++e)
+                if (leaf[e] >= (int64_t)tree->n_nodes) throw Fail{GT_ERR_INVALID, "leaf node out of range"};
+        DeviceGuard dg(ctx->device);
+        const int* dl = stage_in(ctx, kSlotIn0, leaf, n, mem);
+        const double* da = need_a ? stage_in(ctx, kSlotIn1, a, kind == GT_EVENT_KICK ? 3 * n : n, mem) : nullptr;
+        const double* dx = need_x ? stage_in(ctx, kSlotIn2, x, 3 * n, mem) : nullptr;
+        const double* dv = kind == GT_EVENT_MASS ? stage_in(ctx, kSlotIn3, v, 3 * n, mem) : nullptr;
+        const float* df = kind == GT_EVENT_VMAX ? stage_in(ctx, kSlotIn4, f, n, mem) : nullptr;
+        reuse_events(ctx, tree, kind, n, dl, da, dx, dv, df, tau, box);
+        finish(ctx, mem == GT_MEM_HOST);
+    });
+}
+
+int gt_tree_refresh(gt_context* ctx, gt_tree* tree, double tau) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        if (!tree) throw Fail{GT_ERR_INVALID, "null tree"};
+        DeviceGuard dg(ctx->device);
+        reuse_refresh(ctx, tree, tau);
+        finish(ctx, true);
+    });
+}
+
+int gt_tree_node_state(gt_context* ctx, gt_tree* tree, double tau, double* com, double* vel, double* mass,
+                       float* vmax, float* xpad) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        if (!tree) throw Fail{GT_ERR_INVALID, "null tree"};
+        DeviceGuard dg(ctx->device);
+        const int64_t nn = tree->n_nodes;
+        double* dcom = (double*)scratch(ctx, kSlotOut0, (size_t)std::max<int64_t>(nn, 1) * 24);
+        double* dvel = (double*)scratch(ctx, kSlotOut1, (size_t)std::max<int64_t>(nn, 1) * 24);
+        double* dmass = (double*)scratch(ctx, kSlotOut2, (size_t)std::max<int64_t>(nn, 1) * 8);
+        reuse_node_state(ctx, tree, tau, dcom, dvel, dmass);
+        copy_out(ctx, com, (const double*)dcom, 3 * nn, GT_MEM_HOST);
+        copy_out(ctx, vel, (const double*)dvel, 3 * nn, GT_MEM_HOST);
+        copy_out(ctx, mass, (const double*)dmass, nn, GT_MEM_HOST);
+        copy_out(ctx, vmax, (const float*)tree->vmax, nn, GT_MEM_HOST);
+        copy_out(ctx, xpad, (const float*)tree->xpad, nn, GT_MEM_HOST);
+        finish(ctx, true);
+    });
+}
+
+int gt_tree_particles(gt_context* ctx, gt_tree* tree, const double* x, const double* y, const double* z,
+                      const double* m, const double* soft, int mem) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (!tree) throw Fail{GT_ERR_INVALID, "null tree"};
+        if ((x == nullptr) != (y == nullptr) || (x == nullptr) != (z == nullptr))
+            throw Fail{GT_ERR_INVALID, "x, y, z must all be given or all be null"};
+        DeviceGuard dg(ctx->device);
+        const int64_t n = tree->n;
+        tree_particles(ctx, tree, stage_in(ctx, kSlotIn0, x, n, mem), stage_in(ctx, kSlotIn1, y, n, mem),
+                       stage_in(ctx, kSlotIn2, z, n, mem), stage_in(ctx, kSlotIn3, m, n, mem),
+                       stage_in(ctx, kSlotIn4, soft, n, mem));
+        finish(ctx, mem == GT_MEM_HOST);
     });
 }
 

@@ -815,7 +815,7 @@ void tree_velocities(gt_context* ctx, gt_tree* t, const double* vx, const double
         t->svel = dalloc<float4>((size_t)nl, st);
         t->nvel = dalloc<float4>((size_t)nn, st);
         t->vcom = dalloc<double>((size_t)nn * 3, st);
-        t->vmax = dalloc<float>((size_t)nn, st);
+        if (!t->vmax) t->vmax = dalloc<float>((size_t)nn, st);  // tree reuse may have made it
     }
     if (t->n_live > 0) {
         gather_vel_kernel<<<grid_for(ctx, t->n_live), kBlk, 0, st>>>(vx, vy, vz, t->order, t->n_live, t->svel);

@@ -124,6 +124,14 @@ struct gt_tree {
     float4* nvel = nullptr;      // n_nodes
     double* vcom = nullptr;      // 3 * n_nodes
     float* vmax = nullptr;       // n_nodes
+    // tree reuse (gt_tree_refresh and the event calls): build-time node mass and centre of mass,
+    // mass / momentum / first-moment changes since the build, non-ballistic displacement pads
+    double* m0 = nullptr;        // n_nodes
+    double* c0 = nullptr;        // 3 * n_nodes
+    double* dp = nullptr;        // 3 * n_nodes
+    double* dq = nullptr;        // 3 * n_nodes
+    double* dmass = nullptr;     // n_nodes
+    float* xpad = nullptr;       // n_nodes
     // cached all-active group lists, keyed by (mode, param)
     struct GroupCache {
         int mode = -1, param = 0, kmax = 0;
@@ -248,6 +256,17 @@ void run_mac_node_scale(gt_context* ctx, const gt_tree* t, const float* dmodel, 
 
 // Peak probe (gt_peak.cu)
 void run_peaks(gt_context* ctx, double* fp32_tflops, double* fp64_tflops);
+// Tree reuse (gt_reuse.cu).  Event kinds, applied to leaf nodes (device arrays): kick (a = dp, 3
+// per event, at tau), shift (a = m, x = dx 3 per event), speed bound (f), softening bound (a),
+// mass event (a = dm, x, v 3 per event, at tau, box), displacement pad (a = d).
+enum { kReuseKick = 0, kReuseShift, kReuseVmax, kReuseSoft, kReuseMass, kReusePad };
+void reuse_begin(gt_context* ctx, gt_tree* t);
+void reuse_events(gt_context* ctx, gt_tree* t, int kind, int64_t n, const int* leaf, const double* a,
+                  const double* x, const double* v, const float* f, double tau, double box);
+void reuse_refresh(gt_context* ctx, gt_tree* t, double tau);
+void reuse_node_state(gt_context* ctx, gt_tree* t, double tau, double* com, double* vel, double* mass);
+void tree_particles(gt_context* ctx, gt_tree* t, const double* x, const double* y, const double* z,
+                    const double* m, const double* soft);
 // Per-particle velocities in tree order and the per-node centre-of-mass velocity and speed bound
 // (gt_tree_velocities); vx, vy, vz are device arrays over the tree's input particles.
 void tree_velocities(gt_context* ctx, gt_tree* t, const double* vx, const double* vy, const double* vz,

@@ -141,10 +141,16 @@ struct Tree {
     double t_since_build = 0.0;
     // the device tree behind this host copy (shared by copies of the Tree)
     std::shared_ptr<gt_tree> gpu;
+    // tree reuse: events queued for the device tree (shared by copies of the Tree)
+    std::shared_ptr<struct ReuseQueue> reuse;
 
     size_t nnodes() const { return mass.size(); }
-    // Incremental moments (tree reuse across steps) are not implemented on the GPU path: these
-    // throw std::runtime_error.
+    // Incremental moments (tree reuse across steps, tree.cc:211-329).  The events are queued and
+    // applied on the device before the next walk, refresh or node query (gt_tree_events); the host
+    // copies kept current are vmax (the engine reads vmax[root]) and xpad.  The incremental arrays
+    // dp/dq/dmass are allocated like the reference's (their emptiness says whether the build had
+    // node velocities) but their values live on the device: read node state through node_mass,
+    // node_com and node_vel.  raise_hmax / init_hmax belong to the neighbour search and throw.
     void raise_vmax(int leaf_node, float speed);
     void raise_hmax(int leaf_node, double h);
     void init_hmax(const std::vector<double>& h, size_t n_gas);
@@ -153,12 +159,10 @@ struct Tree {
     void kick_node(int leaf_node, const Vec3d& dp, double tau);
     void mass_event(int leaf_node, double dm, const Vec3d& x, const Vec3d& v, double tau, double box);
     void shift_node(int leaf_node, double m, const Vec3d& dx);
-    double node_mass(int no) const { return mass[no] + (dmass.empty() ? 0.0 : dmass[no]); }
+    double node_mass(int no) const;
     Vec3d node_com(int no, double tau) const;
     void refresh_walk_nodes(double tau);
-    Vec3d node_vel(int node_id) const {
-        return Vec3d{vcom_x[node_id], vcom_y[node_id], vcom_z[node_id]};
-    }
+    Vec3d node_vel(int node_id) const;
 };
 
 long long audit_tree(const Tree& T, const Particles& P, const double* h, size_t n_gas,

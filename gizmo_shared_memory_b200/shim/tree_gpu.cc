@@ -5,6 +5,8 @@
 #include <cfloat>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -92,6 +94,7 @@ Tree build(const Particles& P, BuildTimes* bt, const double* const* vel, bool wa
     T.nalloc = (int)nn;
     T.vmax.assign(nn, 0.0f);
     T.xpad.assign(nn, 0.0f);
+    T.reuse = std::make_shared<ReuseQueue>();
     if (vel) {
         // per-node speed bound, and with want_vcom the centre-of-mass velocity the jerk reads
         check(gt_tree_velocities(ctx, h, vel[0], vel[1], vel[2], 0, GT_MEM_HOST), "gt_tree_velocities");
@@ -102,6 +105,8 @@ Tree build(const Particles& P, BuildTimes* bt, const double* const* vel, bool wa
                                        want_vcom ? T.vcom_y.data() : nullptr,
                                        want_vcom ? T.vcom_z.data() : nullptr, T.vmax.data()),
               "gt_tree_velocity_moments");
+        if (want_vcom)  // the reference allocates the incremental arrays with vcom (tree.cc:449-452)
+            for (auto* v : {&T.dp_x, &T.dp_y, &T.dp_z, &T.dq_x, &T.dq_y, &T.dq_z, &T.dmass}) v->assign(nn, 0.0);
     }
     if (!P.type.empty()) {
         // sinks (type 5) under each node, for the engine's sink bookkeeping (tree.cc:168, 178)
@@ -135,8 +140,111 @@ Tree build(const Particles& P, BuildTimes* bt, const double* const* vel, bool wa
     return T;
 }
 
+// ---- tree reuse ----------------------------------------------------------------------------
+// Events are queued per host thread (the engine feeds kicks and speed bounds from OpenMP loops)
+// and applied on the device in one gt_tree_events call per kind.  Kicks, shifts and the speed and
+// softening bounds commute, so their per-thread queues merge in any order; mass events and pads
+// depend on order and the reference's callers are serial, so they flush the queues and go
+// straight to the device.
+struct ReuseQueue {
+    struct Buf {
+        std::vector<int32_t> kick_leaf, vmax_leaf, soft_leaf, shift_leaf;
+        std::vector<double> kick_dp, soft_val, shift_m, shift_dx;
+        std::vector<float> vmax_val;
+        double kick_tau = 0.0;
+    };
+    std::vector<Buf> bufs;
+    std::mutex mu;
+    bool moved = false;  // events or a refresh since the build: the walk needs current particles
+    ReuseQueue() : bufs((size_t)std::max(1, omp_get_max_threads())) {}
+    Buf& mine() {
+        const size_t t = (size_t)omp_get_thread_num();
+        if (t >= bufs.size()) throw std::runtime_error("shmem (GPU): more threads than at tree build");
+        return bufs[t];
+    }
+};
+
+namespace {
+
+ReuseQueue& queue_of(const Tree& T) {
+    if (!T.reuse) throw std::runtime_error("shmem (GPU): the Tree was not built by shmem::build");
+    return *T.reuse;
+}
+
+// Apply every queued commutative event on the device (kick runs grouped by their tau).
+void flush(const Tree& T) {
+    ReuseQueue& Q = queue_of(T);
+    std::lock_guard<std::mutex> lk(Q.mu);
+    gt_tree* h = T.gpu.get();
+    for (auto& b : Q.bufs) {
+        if (!b.kick_leaf.empty())
+            check(gt_tree_events(context(), h, GT_EVENT_KICK, (int64_t)b.kick_leaf.size(), b.kick_leaf.data(),
+                                 b.kick_dp.data(), nullptr, nullptr, nullptr, b.kick_tau, 0.0, GT_MEM_HOST),
+                  "gt_tree_events");
+        if (!b.vmax_leaf.empty())
+            check(gt_tree_events(context(), h, GT_EVENT_VMAX, (int64_t)b.vmax_leaf.size(), b.vmax_leaf.data(),
+                                 nullptr, nullptr, nullptr, b.vmax_val.data(), 0.0, 0.0, GT_MEM_HOST),
+                  "gt_tree_events");
+        if (!b.soft_leaf.empty())
+            check(gt_tree_events(context(), h, GT_EVENT_SOFT, (int64_t)b.soft_leaf.size(), b.soft_leaf.data(),
+                                 b.soft_val.data(), nullptr, nullptr, nullptr, 0.0, 0.0, GT_MEM_HOST),
+                  "gt_tree_events");
+        if (!b.shift_leaf.empty())
+            check(gt_tree_events(context(), h, GT_EVENT_SHIFT, (int64_t)b.shift_leaf.size(), b.shift_leaf.data(),
+                                 b.shift_m.data(), b.shift_dx.data(), nullptr, nullptr, 0.0, 0.0, GT_MEM_HOST),
+                  "gt_tree_events");
+        b = ReuseQueue::Buf{};
+    }
+}
+
+struct NodeState {
+    std::vector<double> com, vel, mass;
+};
+NodeState node_state(const Tree& T, double tau) {
+    flush(T);
+    const size_t nn = T.nnodes();
+    NodeState s;
+    s.com.resize(3 * nn); s.vel.resize(3 * nn); s.mass.resize(nn);
+    check(gt_tree_node_state(context(), T.gpu.get(), tau, s.com.data(), s.vel.data(), s.mass.data(), nullptr,
+                             nullptr), "gt_tree_node_state");
+    return s;
+}
+
+// climb with a float max that stops at the first ancestor already covering the value
+// (tree.cc:276-284); the host copy the engine reads
+void climb_max(std::vector<float>& arr, const std::vector<int>& parent, int leaf, float v) {
+    uint32_t want;
+    std::memcpy(&want, &v, 4);
+    for (int no = leaf; no >= 0; no = parent[no]) {
+        uint32_t* bits = reinterpret_cast<uint32_t*>(&arr[no]);
+        uint32_t seen = __atomic_load_n(bits, __ATOMIC_RELAXED);
+        if (seen >= want) return;
+        while (seen < want && !__atomic_compare_exchange_n(bits, &seen, want, true, __ATOMIC_RELAXED,
+                                                            __ATOMIC_RELAXED)) {
+        }
+    }
+}
+
+}  // namespace
+
 static void need_gpu(const Tree& T) {
     if (!T.gpu) throw std::runtime_error("shmem (GPU): the Tree was not built by shmem::build");
+}
+
+// Before a walk: queued tree events go to the device, and on a reused tree the device gets the
+// particles' current state, which the reference walk reads (tree.cc:786-789).  Lazy drift
+// (tree.cc:783-785) catches a particle up when the walk reaches it; the device walk reads all of
+// them, so every particle behind the target is caught up first.
+static void prepare_walk(const Tree& T, const Particles& P, const LazyDrift* lazy) {
+    flush(T);
+    const bool drift = lazy && lazy->catch_up && lazy->last;
+    if (drift)
+        for (uint32_t q : T.orderbuf)
+            if (lazy->last[q] < lazy->target) lazy->catch_up(lazy->ctx, q);
+    ReuseQueue& Q = queue_of(T);
+    if (Q.moved || drift)
+        check(gt_tree_particles(context(), T.gpu.get(), P.x.data(), P.y.data(), P.z.data(), P.m.data(),
+                                soft_or_null(P), GT_MEM_HOST), "gt_tree_particles");
 }
 
 void accel(const Tree& T, const Particles& P, const std::vector<uint32_t>& targets, double theta,
@@ -144,6 +252,7 @@ void accel(const Tree& T, const Particles& P, const std::vector<uint32_t>& targe
            const double* aold) {
     need_gpu(T);
     require_gravity_only(P);
+    prepare_walk(T, P, nullptr);
     const size_t nt = targets.size();
     ax.assign(nt, 0.0); ay.assign(nt, 0.0); az.assign(nt, 0.0);
     if (!nt) return;
@@ -166,8 +275,8 @@ void accel_grouped(const Tree& T, const Particles& P, const std::vector<uint32_t
                    std::vector<Vec3d>* jerk, const double* const* vel, double sink_direct_radius) {
     need_gpu(T);
     require_gravity_only(P);
-    if (lazy) unsupported("lazy drift");
     if (sink_direct_radius > 0 && !P.type.empty()) unsupported("sink-direct opening");
+    prepare_walk(T, P, lazy);
     // the jerk needs source velocities: the walk's `vel` for particles and the build's node
     // centre-of-mass velocities (tree.cc:638-640); without them it stays zero
     const bool want_jerk = jerk && vel && !T.vcom_x.empty();
@@ -198,7 +307,7 @@ void accel_grouped(const Tree& T, const Particles& P, const std::vector<uint32_t
 void potential(const Tree& T, const Particles& P, const std::vector<uint32_t>& targets,
                double theta, double G, std::vector<double>& phi, const double* aold) {
     need_gpu(T);
-    (void)P;
+    prepare_walk(T, P, nullptr);
     const size_t nt = targets.size();
     phi.assign(nt, 0.0);
     if (!nt) return;
@@ -223,19 +332,73 @@ int build_node(Tree&, const Particles&, const std::vector<uint32_t>&, const std:
 }
 void setup_walk(Tree&, int, int) { unsupported("setup_walk (threading is produced by the device build)"); }
 
-void Tree::raise_vmax(int, float) { unsupported("Tree::raise_vmax (tree reuse)"); }
-void Tree::raise_hmax(int, double) { unsupported("Tree::raise_hmax (tree reuse)"); }
-void Tree::init_hmax(const std::vector<double>&, size_t) { unsupported("Tree::init_hmax (tree reuse)"); }
-void Tree::raise_soft(int, double) { unsupported("Tree::raise_soft (tree reuse)"); }
-void Tree::raise_pad(int, double) { unsupported("Tree::raise_pad (tree reuse)"); }
-void Tree::kick_node(int, const Vec3d&, double) { unsupported("Tree::kick_node (tree reuse)"); }
-void Tree::mass_event(int, double, const Vec3d&, const Vec3d&, double, double) {
-    unsupported("Tree::mass_event (tree reuse)");
+
+void Tree::raise_vmax(int leaf_node, float speed) {
+    if (leaf_node < 0) return;
+    climb_max(vmax, parent, leaf_node, speed);
+    auto& b = queue_of(*this).mine();
+    b.vmax_leaf.push_back(leaf_node);
+    b.vmax_val.push_back(speed);
 }
-void Tree::shift_node(int, double, const Vec3d&) { unsupported("Tree::shift_node (tree reuse)"); }
-Vec3d Tree::node_com(int no, double) const { return Vec3d{cx[no], cy[no], cz[no]}; }
+void Tree::raise_hmax(int, double) { unsupported("Tree::raise_hmax (the neighbour search)"); }
+void Tree::init_hmax(const std::vector<double>&, size_t) { unsupported("Tree::init_hmax (the neighbour search)"); }
+void Tree::raise_soft(int leaf_node, double s) {
+    if (leaf_node < 0) return;
+    auto& b = queue_of(*this).mine();
+    b.soft_leaf.push_back(leaf_node);
+    b.soft_val.push_back(s);
+}
+void Tree::raise_pad(int leaf_node, double d) {
+    if (leaf_node < 0 || !(d > 0)) return;
+    flush(*this);
+    const int32_t lf = leaf_node;
+    check(gt_tree_events(context(), gpu.get(), GT_EVENT_PAD, 1, &lf, &d, nullptr, nullptr, nullptr, 0.0, 0.0,
+                         GT_MEM_HOST), "gt_tree_events");
+    // the host copy (the neighbour search reads it): the same serial climb (tree.cc:322-329)
+    float leaf_pad = (float)((double)xpad[leaf_node] + d);
+    if ((double)leaf_pad < (double)xpad[leaf_node] + d) leaf_pad = std::nextafter(leaf_pad, 1e30f);
+    for (int no = leaf_node; no >= 0 && xpad[no] < leaf_pad; no = parent[no]) xpad[no] = leaf_pad;
+    queue_of(*this).moved = true;
+}
+void Tree::kick_node(int leaf_node, const Vec3d& dp, double tau) {
+    if (dp_x.empty() || leaf_node < 0) return;  // no vcom, nothing to keep current (tree.cc:212)
+    auto& b = queue_of(*this).mine();
+    if (!b.kick_leaf.empty() && b.kick_tau != tau) flush(*this);
+    b.kick_tau = tau;
+    b.kick_leaf.push_back(leaf_node);
+    for (int k = 0; k < 3; ++k) b.kick_dp.push_back(dp[k]);
+    queue_of(*this).moved = true;
+}
+void Tree::mass_event(int leaf_node, double dm, const Vec3d& x, const Vec3d& v, double tau, double box) {
+    if (dp_x.empty() || leaf_node < 0 || dm == 0.0) return;
+    flush(*this);
+    const int32_t lf = leaf_node;
+    const double xx[3] = {x[0], x[1], x[2]}, vv[3] = {v[0], v[1], v[2]};
+    check(gt_tree_events(context(), gpu.get(), GT_EVENT_MASS, 1, &lf, &dm, xx, vv, nullptr, tau, box, GT_MEM_HOST),
+          "gt_tree_events");
+    queue_of(*this).moved = true;
+}
+void Tree::shift_node(int leaf_node, double m, const Vec3d& dx) {
+    if (dp_x.empty() || leaf_node < 0) return;
+    auto& b = queue_of(*this).mine();
+    b.shift_leaf.push_back(leaf_node);
+    b.shift_m.push_back(m);
+    for (int k = 0; k < 3; ++k) b.shift_dx.push_back(dx[k]);
+    queue_of(*this).moved = true;
+}
+double Tree::node_mass(int no) const { return node_state(*this, 0.0).mass[no]; }
+Vec3d Tree::node_com(int no, double tau) const {
+    const NodeState s = node_state(*this, tau);
+    return Vec3d{s.com[3 * no], s.com[3 * no + 1], s.com[3 * no + 2]};
+}
+Vec3d Tree::node_vel(int no) const {
+    const NodeState s = node_state(*this, 0.0);
+    return Vec3d{s.vel[3 * no], s.vel[3 * no + 1], s.vel[3 * no + 2]};
+}
 void Tree::refresh_walk_nodes(double tau) {
-    if (tau != 0.0) unsupported("Tree::refresh_walk_nodes with tau != 0 (tree reuse)");
+    flush(*this);
+    check(gt_tree_refresh(context(), gpu.get(), tau), "gt_tree_refresh");
+    if (tau != 0.0) queue_of(*this).moved = true;
 }
 
 // Structural audit of the downloaded tree (the topology and coverage parts of the reference's

@@ -218,6 +218,34 @@ GT_API int gt_tree_keys(gt_context* ctx, const gt_tree* tree, uint64_t* keys);
  * (tree.cc:793-797, 862-866). */
 GT_API int gt_tree_velocities(gt_context* ctx, gt_tree* tree, const double* vx, const double* vy,
                        const double* vz, int particles_only, int mem);
+/* ---- tree reuse between rebuilds (shmem/tree.cc:211-274, tree.h:286-341) -----------------
+ * Events of one kind on leaf nodes (the tree's own numbering, e.g. leaf_of of gt_tree_download),
+ * applied in array order where the result depends on it:
+ *   GT_EVENT_KICK   kick_node(leaf, dp = a[3e..3e+2], tau)         tree.cc:211-226 (no-op without node vcom)
+ *   GT_EVENT_SHIFT  shift_node(leaf, m = a[e], dx = x[3e..3e+2])   tree.cc:248-253 (no-op without node vcom)
+ *   GT_EVENT_VMAX   raise_vmax(leaf, speed = f[e])                 tree.cc:276-284
+ *   GT_EVENT_SOFT   raise_soft(leaf, soft = a[e])                  tree.cc:310-319
+ *   GT_EVENT_MASS   mass_event(leaf, dm = a[e], x[3e..], v[3e..], tau, box)  tree.cc:229-246 (serial; no-op without vcom)
+ *   GT_EVENT_PAD    raise_pad(leaf, d = a[e])                      tree.cc:322-329 (serial)
+ * Node vcom comes from gt_tree_velocities. */
+enum { GT_EVENT_KICK = 0, GT_EVENT_SHIFT = 1, GT_EVENT_VMAX = 2, GT_EVENT_SOFT = 3, GT_EVENT_MASS = 4,
+       GT_EVENT_PAD = 5 };
+GT_API int gt_tree_events(gt_context* ctx, gt_tree* tree, int kind, int64_t n, const int32_t* leaf,
+                   const double* a, const double* x, const double* v, const float* f, double tau,
+                   double box, int mem);
+/* refresh_walk_nodes(tau) (tree.cc:256-274): the walk nodes' centre of mass, mass, opening radius
+ * and side from the incremental moments (radius and side grow by 2 (vmax tau + xpad)).  Call
+ * before a walk on a reused tree. */
+GT_API int gt_tree_refresh(gt_context* ctx, gt_tree* tree, double tau);
+/* node_com(tau), node_vel and node_mass of every node (tree.h:326-341), with the speed and
+ * displacement bounds; host arrays (com, vel: 3 per node), any may be null. */
+GT_API int gt_tree_node_state(gt_context* ctx, gt_tree* tree, double tau, double* com, double* vel,
+                       double* mass, float* vmax, float* xpad);
+/* The particles' current positions, masses and softenings (indexed like the build input; a NULL
+ * group keeps its values) for walks on a reused tree: the reference walk reads the particles'
+ * current state (tree.cc:786-789), the structure stays the build's. */
+GT_API int gt_tree_particles(gt_context* ctx, gt_tree* tree, const double* x, const double* y,
+                      const double* z, const double* m, const double* soft, int mem);
 /* Per-node centre-of-mass velocity (n_nodes each) and speed bound; any pointer may be null. */
 GT_API int gt_tree_velocity_moments(gt_context* ctx, const gt_tree* tree, double* vcx, double* vcy,
                              double* vcz, float* vmax);

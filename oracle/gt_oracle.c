@@ -722,3 +722,18 @@ void or_walk_groups_ext(const or_tree* t, int64_t nt, const uint32_t* targets, i
         free(buf);
     }
 }
+
+/* Tree reuse: replace the walk's node fields with refreshed ones (refresh_walk_nodes writes the
+ * packed walk nodes, tree.cc:256-274) and point the tree at the particles' current positions (the
+ * walk reads them, tree.cc:786-789). */
+void or_set_walk_nodes(or_tree* t, const double* cx, const double* cy, const double* cz, const double* mass,
+                       const double* w_s, const float* w_len, const float* w_soft) {
+    const size_t nn = (size_t)t->nnodes;
+    memcpy(t->cx, cx, nn * 8); memcpy(t->cy, cy, nn * 8); memcpy(t->cz, cz, nn * 8);
+    memcpy(t->mass, mass, nn * 8); memcpy(t->w_s, w_s, nn * 8);
+    memcpy(t->w_len, w_len, nn * 4); memcpy(t->w_soft, w_soft, nn * 4);
+}
+
+void or_set_positions(or_tree* t, const double* x, const double* y, const double* z) {
+    t->x = x; t->y = y; t->z = z;
+}

@@ -74,6 +74,11 @@ void or_walk_groups_ext(const or_tree* t, int64_t nt, const uint32_t* targets, i
                         const double* vx, const double* vy, const double* vz, const double* vcx,
                         const double* vcy, const double* vcz, double* ax, double* ay, double* az,
                         double* tidal, double* jerk);
+/* Tree reuse: overwrite the walk's node fields (COM, mass, opening radius, side, softening) and
+ * re-point the particle positions (the caller keeps the arrays alive). */
+void or_set_walk_nodes(or_tree* t, const double* cx, const double* cy, const double* cz, const double* mass,
+                       const double* w_s, const float* w_len, const float* w_soft);
+void or_set_positions(or_tree* t, const double* x, const double* y, const double* z);
 /* accel_grouped (tree.cc:626-897), gravity only. */
 void or_accel_grouped(const or_tree* t, int64_t nt, const uint32_t* targets, double theta, double G,
                       int batch, const double* aold, double* ax, double* ay, double* az,

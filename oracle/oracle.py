@@ -99,6 +99,8 @@ class Restatement:
                                        C.c_int, _d, _d, _d, _d, _i64]
         L.or_accel.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, _d, _d, _d, _d]
         L.or_potential.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, _d, _d]
+        L.or_set_walk_nodes.argtypes = [C.c_void_p, _d, _d, _d, _d, _d, _f, _f]
+        L.or_set_positions.argtypes = [C.c_void_p, _d, _d, _d]
         L.or_spline_tidal_factor.restype = C.c_double
         L.or_spline_tidal_factor.argtypes = [C.c_double, C.c_double]
         L.or_velocity_moments.argtypes = [C.c_void_p, _d, _d, _d, _d, _d, _d, _f]
@@ -230,6 +232,19 @@ class OracleTree:
                                   _p(az, _d), _p(phi, _d), _p(cnt, _i64))
         return ax, ay, az, phi, cnt
 
+    def set_walk_nodes(self, st):
+        """Overwrite the walk's node fields with refreshed ones (oracle.reuse.Reuse.refresh)."""
+        self._walk_nodes = [np.ascontiguousarray(st["com"][:, k], np.float64) for k in range(3)] + [
+            _f64(st["mass"]), _f64(st["w_s"]), np.ascontiguousarray(st["w_len"], np.float32),
+            np.ascontiguousarray(st["w_soft"], np.float32)]
+        cx, cy, cz, m, s, ln, sf = self._walk_nodes
+        self.lib.L.or_set_walk_nodes(self.h, _p(cx, _d), _p(cy, _d), _p(cz, _d), _p(m, _d), _p(s, _d),
+                                     _p(ln, _f), _p(sf, _f))
+
+    def set_positions(self, x, y, z):
+        self._pos = [_f64(a) for a in (x, y, z)]
+        self.lib.L.or_set_positions(self.h, *[_p(a, _d) for a in self._pos])
+
     def velocity_moments(self, vel):
         """Node centre-of-mass velocity (3 arrays) and speed bound for velocities vel = (vx, vy, vz)."""
         v = [_f64(a) for a in vel]
@@ -330,6 +345,16 @@ class Reference:
         L.ref_tree_vel.argtypes = [C.c_void_p, _d, _d, _d, _f]
         L.ref_accel_grouped_ext.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double,
                                             C.c_int, _d, _d, _d, _d, _d, _d]
+        L.ref_reuse_begin.argtypes = [C.c_void_p]
+        L.ref_kick_node.argtypes = [C.c_void_p, C.c_int, _d, C.c_double]
+        L.ref_mass_event.argtypes = [C.c_void_p, C.c_int, C.c_double, _d, _d, C.c_double, C.c_double]
+        L.ref_shift_node.argtypes = [C.c_void_p, C.c_int, C.c_double, _d]
+        L.ref_raise_vmax.argtypes = [C.c_void_p, C.c_int, C.c_float]
+        L.ref_raise_pad.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.ref_raise_soft.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.ref_refresh_walk_nodes.argtypes = [C.c_void_p, C.c_double]
+        L.ref_node_state.argtypes = [C.c_void_p, C.c_double, _d, _d, _d, _f, _f, _d, _f, _f]
+        L.ref_set_positions.argtypes = [C.c_void_p, _d, _d, _d]
 
     def max_threads(self):
         return self.L.ref_max_threads()
@@ -449,6 +474,46 @@ class ReferenceTree:
         self.lib.L.ref_accel_grouped_ext(self.h, nt, _p(t, _u32), theta, G, batch, _p(ao, _d), _p(ax, _d),
                                          _p(ay, _d), _p(az, _d), _p(tt, _d), _p(jj, _d))
         return ax, ay, az, tt, jj
+
+    # ---- tree reuse (tree.cc:211-274): events on leaf nodes of this tree's numbering ----------
+    def reuse_begin(self):
+        self.lib.L.ref_reuse_begin(self.h)
+
+    def events(self, kind, leaf, a=None, x=None, v=None, f=None, tau=0.0, box=0.0):
+        """Apply events of one kind in order (kinds as GT_EVENT_*: 0 kick, 1 shift, 2 vmax, 3 soft,
+        4 mass, 5 pad), each with the reference's own per-event call."""
+        L = self.lib.L
+        for e, lf in enumerate(np.asarray(leaf)):
+            lf = int(lf)
+            if kind == 0:
+                L.ref_kick_node(self.h, lf, _p(_f64(a[e]), _d), tau)
+            elif kind == 1:
+                L.ref_shift_node(self.h, lf, float(a[e]), _p(_f64(x[e]), _d))
+            elif kind == 2:
+                L.ref_raise_vmax(self.h, lf, float(f[e]))
+            elif kind == 3:
+                L.ref_raise_soft(self.h, lf, float(a[e]))
+            elif kind == 4:
+                L.ref_mass_event(self.h, lf, float(a[e]), _p(_f64(x[e]), _d), _p(_f64(v[e]), _d), tau, box)
+            elif kind == 5:
+                L.ref_raise_pad(self.h, lf, float(a[e]))
+
+    def refresh(self, tau):
+        self.lib.L.ref_refresh_walk_nodes(self.h, tau)
+
+    def node_state(self, tau):
+        nn = self.nnodes
+        out = {"com": np.zeros((nn, 3)), "vel": np.zeros((nn, 3)), "mass": np.zeros(nn),
+               "vmax": np.zeros(nn, np.float32), "xpad": np.zeros(nn, np.float32), "w_s": np.zeros(nn),
+               "w_len": np.zeros(nn, np.float32), "w_soft": np.zeros(nn, np.float32)}
+        self.lib.L.ref_node_state(self.h, tau, _p(out["com"], _d), _p(out["vel"], _d), _p(out["mass"], _d),
+                                  _p(out["vmax"], _f), _p(out["xpad"], _f), _p(out["w_s"], _d),
+                                  _p(out["w_len"], _f), _p(out["w_soft"], _f))
+        return out
+
+    def set_positions(self, x, y, z):
+        x, y, z = (_f64(a) for a in (x, y, z))
+        self.lib.L.ref_set_positions(self.h, _p(x, _d), _p(y, _d), _p(z, _d))
 
     def vel_moments(self):
         nn = self.nnodes

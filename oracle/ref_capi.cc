@@ -105,6 +105,54 @@ void ref_accel_grouped_ext(void* p, int64_t nt, const uint32_t* targets, double 
         for (int k = 0; k < 3; ++k) jerk[3 * i + k] = jj[i][k];
 }
 
+// Tree reuse (tree.cc:211-274, tree.h:286-331): the incremental-moment events on leaf nodes of the
+// reference's own numbering, then refresh_walk_nodes.  The incremental arrays are allocated the
+// way the engine's rebuild does (mfm.cc:1408-1414): dp/dq/dmass sized to the nodes, zeroed.
+void ref_reuse_begin(void* p) {
+    Tree& T = static_cast<RefHandle*>(p)->T;
+    const size_t nn = T.nnodes();
+    for (auto* v : {&T.dp_x, &T.dp_y, &T.dp_z, &T.dq_x, &T.dq_y, &T.dq_z, &T.dmass}) v->assign(nn, 0.0);
+}
+void ref_kick_node(void* p, int leaf, const double* dp, double tau) {
+    static_cast<RefHandle*>(p)->T.kick_node(leaf, Vec3d{dp[0], dp[1], dp[2]}, tau);
+}
+void ref_mass_event(void* p, int leaf, double dm, const double* x, const double* v, double tau, double box) {
+    static_cast<RefHandle*>(p)->T.mass_event(leaf, dm, Vec3d{x[0], x[1], x[2]}, Vec3d{v[0], v[1], v[2]}, tau, box);
+}
+void ref_shift_node(void* p, int leaf, double m, const double* dx) {
+    static_cast<RefHandle*>(p)->T.shift_node(leaf, m, Vec3d{dx[0], dx[1], dx[2]});
+}
+void ref_raise_vmax(void* p, int leaf, float speed) { static_cast<RefHandle*>(p)->T.raise_vmax(leaf, speed); }
+void ref_raise_pad(void* p, int leaf, double d) { static_cast<RefHandle*>(p)->T.raise_pad(leaf, d); }
+void ref_raise_soft(void* p, int leaf, double s) { static_cast<RefHandle*>(p)->T.raise_soft(leaf, s); }
+void ref_refresh_walk_nodes(void* p, double tau) { static_cast<RefHandle*>(p)->T.refresh_walk_nodes(tau); }
+// Node state after the events: node_com(tau), node_vel, node_mass, vmax, xpad, and the packed walk
+// node's s and len (nnodes each, com/vel 3 per node; any pointer may be null).
+void ref_node_state(void* p, double tau, double* com, double* vel, double* mass, float* vmax, float* xpad,
+                    double* w_s, float* w_len, float* w_soft) {
+    const Tree& T = static_cast<RefHandle*>(p)->T;
+    for (size_t i = 0; i < T.nnodes(); ++i) {
+        const Vec3d c = T.node_com((int)i, tau);
+        if (com) for (int k = 0; k < 3; ++k) com[3 * i + k] = c[k];
+        if (vel && !T.vcom_x.empty()) {
+            const Vec3d v = T.node_vel((int)i);
+            for (int k = 0; k < 3; ++k) vel[3 * i + k] = v[k];
+        }
+        if (mass) mass[i] = T.node_mass((int)i);
+        if (vmax) vmax[i] = T.vmax[i];
+        if (xpad) xpad[i] = T.xpad[i];
+        if (w_s) w_s[i] = T.wn[i].s;
+        if (w_len) w_len[i] = T.wn[i].len;
+        if (w_soft) w_soft[i] = T.wn[i].soft;
+    }
+}
+// Replace the particles' positions (the walk reads P.x; a reused tree keeps its structure).
+void ref_set_positions(void* p, const double* x, const double* y, const double* z) {
+    RefHandle* h = static_cast<RefHandle*>(p);
+    const size_t n = h->P.x.size();
+    std::memcpy(h->P.x.data(), x, n * 8); std::memcpy(h->P.y.data(), y, n * 8); std::memcpy(h->P.z.data(), z, n * 8);
+}
+
 void ref_free(void* p) { delete static_cast<RefHandle*>(p); }
 
 int64_t ref_tree_nnodes(void* p) { return (int64_t)static_cast<RefHandle*>(p)->T.nnodes(); }

@@ -112,6 +112,25 @@ def main():
         out[f"plummer_{name}_tidal"] = tt
         out[f"plummer_{name}_jerk"] = jj
 
+    # ---- tree reuse: incremental moments, refresh and a walk on the reused tree (tree.cc:211-329)
+    sys.path.insert(0, HERE)
+    import reuse_scenario as RS
+
+    TR = R.build(P, vel=vel)
+    TR.reuse_begin()
+    leaf_r = TR.order()[2]
+    evs = RS.events(P, vel)
+    for kind, parts, arr, tau in evs:
+        TR.events(kind, leaf_r[parts], a=arr.get("a"), x=arr.get("x"), v=arr.get("v"), f=arr.get("f"), tau=tau)
+    TR.refresh(RS.TAU)
+    st = TR.node_state(RS.TAU)
+    for k, v in st.items():
+        out[f"reuse_{k}"] = v
+    xr, yr, zr = RS.positions_after(P, vel, evs)
+    TR.set_positions(xr, yr, zr)
+    rx, ry, rz = TR.accel_grouped(tg, 0.0, 1.0, 0, aold=aold)
+    out["reuse_ax"], out["reuse_ay"], out["reuse_az"] = rx, ry, rz
+
     # ---- collocated particles: the level-20 leaf (tree.cc:89) ----------------------------------
     Q = ics.plummer(n=600, seed=7, soft=0.02)
     Q["x"][:40] = Q["x"][0]

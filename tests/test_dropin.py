@@ -74,3 +74,37 @@ def test_reference_bench_treeforce_runs_on_the_gpu_tree(tmp_path):
     assert sums[2, 1] == pytest.approx(ref[2, 1], rel=1e-4)
     assert np.all(np.abs(sums[:, 0] - ref[:, 0]) < 5e-2)
     assert abs(sums[2, 2] - ref[2, 2]) < 5e-2 * max(1.0, abs(ref[2, 2]))
+
+
+@pytest.mark.gpu
+def test_tree_reuse_through_the_shim_matches_the_reference(tmp_path):
+    """tests/dropin/reuse_check.cc -- build with velocities, kicks, speed bounds, shifts, mass
+    events, pads, refresh_walk_nodes, a ballistic drift, and a walk for the acceleration, tidal
+    tensor and jerk on the reused tree -- compiled against the shim (GPU) and against the
+    reference's own tree (oracle/_ref, CPU): the two must agree to the walk bars (median 1e-5,
+    p99 2e-3 per target), and the root's incremental mass and centre of mass to 1e-12."""
+    from gizmo_shared_memory_b200 import ics
+
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "reuse_check")
+    if not os.path.exists(ref_bin):
+        pytest.skip("oracle/_ref/reuse_check not built (reference sources unavailable at build time)")
+    P, vel = ics.plummer_state(n=50000, seed=13)
+    state = tmp_path / "state.bin"
+    ics.write_state(str(state), P, vel)
+    outs = {}
+    for name, exe in (("gpu", binary("reuse_check")), ("ref", ref_bin)):
+        path = tmp_path / f"{name}.bin"
+        r = subprocess.run([exe, str(state), str(path)], capture_output=True, text=True, timeout=600,
+                           env=dict(os.environ, OMP_NUM_THREADS="4"))
+        assert r.returncode == 0, (name, r.stdout[-2000:], r.stderr[-2000:])
+        outs[name] = np.fromfile(path, np.float64)
+    n = 50000
+    g, r = outs["gpu"], outs["ref"]
+    assert g.size == r.size == 12 * n + 4
+    a_g, a_r = g[:3 * n].reshape(3, n).T, r[:3 * n].reshape(3, n).T
+    t_g, t_r = g[3 * n:9 * n].reshape(n, 6), r[3 * n:9 * n].reshape(n, 6)
+    j_g, j_r = g[9 * n:12 * n].reshape(n, 3), r[9 * n:12 * n].reshape(n, 3)
+    for what, x, y in (("accel", a_g, a_r), ("tidal", t_g, t_r), ("jerk", j_g, j_r)):
+        e = np.linalg.norm(x - y, axis=1) / np.linalg.norm(y, axis=1)
+        assert np.median(e) <= 1e-5 and np.quantile(e, 0.99) <= 2e-3, (what, np.median(e), np.quantile(e, 0.99))
+    np.testing.assert_allclose(g[12 * n:], r[12 * n:], rtol=1e-12)

@@ -198,3 +198,36 @@ def test_randomized_root_matches_reference(oracle, reference):
     tn, rn = T.nodes(), R.nodes()
     assert np.array_equal(tn["gcx"], rn["gcx"]) and np.array_equal(tn["size"], rn["size"])
     assert np.array_equal(T.order()[0], R.order()[0])
+
+
+def test_tree_reuse_matches_golden(oracle, golden):
+    """The restatement of the incremental node moments (oracle/reuse.py) and the oracle walk on
+    the refreshed tree, against the reference's own (tree.cc:211-329)."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import reuse_scenario as RS
+    from reuse import Reuse
+
+    P = particles(golden, "plummer")
+    vel = [golden[f"plummer_v{k}"] for k in "xyz"]
+    T = oracle.build(P)
+    vc, vmax = T.velocity_moments(vel)
+    R = Reuse(T.nodes(), vcom=vc, vmax=vmax)
+    leaf = golden["plummer_leaf_of"]
+    evs = RS.events(P, vel)
+    for kind, parts, arr, tau in evs:
+        R.events(kind, leaf[parts], a=arr.get("a"), x=arr.get("x"), v=arr.get("v"), f=arr.get("f"), tau=tau)
+    st = R.refresh(RS.TAU)
+    scale = np.abs(golden["reuse_com"]).max()
+    assert np.abs(st["com"] - golden["reuse_com"]).max() <= 1e-12 * scale
+    assert np.abs(st["vel"] - golden["reuse_vel"]).max() <= 1e-12 * np.abs(golden["reuse_vel"]).max()
+    np.testing.assert_allclose(st["mass"], golden["reuse_mass"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(st["w_s"], golden["reuse_w_s"], rtol=1e-12, atol=0)
+    for k in ("w_len", "w_soft", "vmax", "xpad"):
+        assert np.array_equal(st[k], golden[f"reuse_{k}"]), k
+    T.set_walk_nodes(st)
+    T.set_positions(*RS.positions_after(P, vel, evs))
+    ax, ay, az, _ = T.accel_grouped(golden["plummer_orderbuf"], 0.0, aold=golden["plummer_aold"])
+    assert relerr(ax, ay, az, golden["reuse_ax"], golden["reuse_ay"], golden["reuse_az"]).max() < 1e-12
