@@ -40,7 +40,7 @@ EXPORTS = [
     "gt_mac_train", "gt_mac_predict", "gt_mac_gradient", "gt_build_systems", "gt_tree_systems",
     "gt_plan_create", "gt_plan_launch", "gt_plan_destroy", "gt_tune_options_default", "gt_autotune",
     "gt_accel_grouped_ext", "gt_tree_velocities", "gt_tree_velocity_moments", "gt_tree_events",
-    "gt_tree_refresh", "gt_tree_node_state", "gt_tree_particles",
+    "gt_tree_refresh", "gt_tree_node_state", "gt_tree_particles", "gt_tree_gas",
 ]
 
 
@@ -61,7 +61,8 @@ class WalkOptions(C.Structure):
                 ("out_order", C.c_int), ("async_", C.c_int), ("count", C.c_int),
                 ("block_warps", C.c_int), ("list_capacity", C.c_int),
                 ("stack_capacity", C.c_int), ("dtype_out_f32", C.c_int),
-                ("mac_model", C.c_void_p), ("mac_kappa", C.c_double), ("mac_band", C.c_double * 2)]
+                ("mac_model", C.c_void_p), ("mac_kappa", C.c_double), ("mac_band", C.c_double * 2),
+                ("sink_direct_radius", C.c_double)]
 
 
 class TuneEntry(C.Structure):
@@ -149,6 +150,7 @@ def load_library(path: str = LIB_PATH):
     L.gt_tree_refresh.argtypes = [vp, vp, d]
     L.gt_tree_node_state.argtypes = [vp, vp, d, vp, vp, vp, vp, vp]
     L.gt_tree_particles.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int]
+    L.gt_tree_gas.argtypes = [vp, vp, vp, vp, C.c_int]
     L.gt_potential.argtypes = [vp, vp, i64, vp, d, d, vp, C.c_int, vp]
     L.gt_walk_stats_get.argtypes = [vp, C.POINTER(WalkStats)]
     L.gt_form_aold.argtypes = [vp, i64, vp, vp, vp, d, d, C.c_int, vp]
@@ -366,9 +368,10 @@ class Context:
     # ---- walks -----------------------------------------------------------------------------
     def _walk_opts(self, group_mode=GT_GROUP_LEAF, group_max=32, out_order=GT_OUT_TARGETS,
                    count=False, block_warps=0, async_=False, mac=GT_MAC_PLAIN, mac_model=None, list_capacity=0,
-                   mac_kappa=1.0, mac_band=(0.0, 0.0)):
+                   mac_kappa=1.0, mac_band=(0.0, 0.0), sink_direct_radius=0.0):
         o = WalkOptions()
         load_library().gt_walk_options_default(C.byref(o))
+        o.sink_direct_radius = sink_direct_radius
         o.group_mode = group_mode
         o.group_max = group_max
         o.out_order = out_order
@@ -576,6 +579,18 @@ class Context:
         x, y, z, m, soft = (cv(q) for q in (x, y, z, m, soft))
         self._check(load_library().gt_tree_particles(self.h, tree.h, _ptr(x), _ptr(y), _ptr(z), _ptr(m),
                                                      _ptr(soft), GT_MEM_HOST))
+
+    def tree_gas(self, tree: Tree, type=None, zeta=None):
+        """Attach particle types (uint8, GIZMO numbering: 0 gas, 5 sink; None = all gas) and the
+        adaptive-softening zeta (None = none), indexed like the build input: walks returning
+        accelerations then apply the zeta terms of gas-gas pairs, and sink_direct_radius > 0 in
+        the walk options turns on sink-direct opening.  Host arrays or device tensors."""
+        dev = _is_dev(type) or _is_dev(zeta)
+        if not dev:
+            type = None if type is None else np.ascontiguousarray(type, np.uint8)
+            zeta = None if zeta is None else np.ascontiguousarray(zeta, np.float64)
+        self._check(load_library().gt_tree_gas(self.h, tree.h, _ptr(type), _ptr(zeta),
+                                               GT_MEM_DEVICE if dev else GT_MEM_HOST))
 
     def velocity_moments(self, tree: Tree):
         nn = tree.info()["n_nodes"]

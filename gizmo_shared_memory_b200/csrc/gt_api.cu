@@ -4,6 +4,7 @@
 // gt_status plus a message on the context, never an exit() (the reference's CUDA entry exits on a
 // launch error, shmem/grav_cuda.cu:239-243).
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -122,7 +123,7 @@ void free_tree_arrays(gt_tree* t) {
     void* ptrs[] = {t->src, t->ssoft, t->smass, t->order, t->rank, t->leaf_of, t->sleaf, t->skey,
                     t->nodes, t->parent, t->next, t->level, t->size, t->delta, t->nsoft, t->gc,
                     t->nq2, t->sys_off_dev, t->geom_dev, t->svel, t->nvel, t->vcom, t->vmax,
-                    t->m0, t->c0, t->dp, t->dq, t->dmass, t->xpad};
+                    t->m0, t->c0, t->dp, t->dq, t->dmass, t->xpad, t->stype, t->szeta, t->nsink};
     // tree arrays came from the stream-ordered pool: hand them back to it (callers have synchronised)
     for (void* p : ptrs)
         if (p) cudaFreeAsync(p, 0);
@@ -166,6 +167,8 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
             if (!((GT_MAC_NODE_FEATURES >> i) & 1u) && o.mac_model[GT_MAC_FEATURES + i] != 0.0f)
                 throw Fail{GT_ERR_INVALID, "GT_MAC_NODE needs a model that reads node features only"};
     if (o.dtype_out_f32 != 0) throw Fail{GT_ERR_INVALID, "dtype_out_f32 is reserved"};
+    if (!(o.sink_direct_radius >= 0.0) || !std::isfinite(o.sink_direct_radius))
+        throw Fail{GT_ERR_INVALID, "sink_direct_radius must be finite and >= 0"};
     if (o.out_order == GT_OUT_ORIGINAL && targets) throw Fail{GT_ERR_INVALID, "GT_OUT_ORIGINAL needs targets == NULL"};
     DeviceGuard dg(ctx->device);
     const bool all = targets == nullptr;
@@ -215,6 +218,7 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     rq.stack_capacity = o.stack_capacity;
     rq.bufs = bufs;
     rq.capture = capture;
+    rq.sink_radius = o.sink_direct_radius;
     if ((ax == nullptr) != (ay == nullptr) || (ax == nullptr) != (az == nullptr))
         throw Fail{GT_ERR_INVALID, "ax, ay, az must all be given or all be null"};
     if (!ax && !phi && !tidal && !jerk) return;
@@ -660,6 +664,23 @@ int gt_tree_velocities(gt_context* ctx, gt_tree* tree, const double* vx, const d
         const double* dz = stage_in(ctx, kSlotIn2, vz, tree->n, mem);
         if (particles_only && !tree->svel) throw Fail{GT_ERR_INVALID, "no node velocities to keep yet"};
         tree_velocities(ctx, tree, dx, dy, dz, particles_only != 0);
+        finish(ctx, true);
+    });
+}
+
+int gt_tree_gas(gt_context* ctx, gt_tree* tree, const uint8_t* type, const double* zeta, int mem) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (!tree) throw Fail{GT_ERR_INVALID, "null tree"};
+        if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "tree and context are on different devices"};
+        if (mem == GT_MEM_HOST && zeta && tree->opt.validate)
+            for (int64_t i = 0; i < tree->n; ++i)
+                if (!std::isfinite(zeta[i])) throw Fail{GT_ERR_NONFINITE, "non-finite zeta"};
+        DeviceGuard dg(ctx->device);
+        const uint8_t* dt = stage_in(ctx, kSlotIn0, type, tree->n, mem);
+        const double* dz = stage_in(ctx, kSlotIn1, zeta, tree->n, mem);
+        tree_gas(ctx, tree, dt, dz);
         finish(ctx, true);
     });
 }

@@ -531,6 +531,30 @@ __global__ void gather_vel_kernel(const double* __restrict__ vx, const double* _
     }
 }
 
+// ---- gas and sinks: particle types and adaptive-softening zeta in tree order, sinks per node ----
+// (shmem::Particles::type / ::zeta, tree.h:38-49; the per-node sink count of tree.cc:155-187)
+__global__ void gather_gas_kernel(const uint8_t* __restrict__ type, const double* __restrict__ zeta,
+                                  const uint32_t* __restrict__ order, int64_t n, uint8_t* __restrict__ stype,
+                                  double* __restrict__ szeta) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = order[i];
+        stype[i] = type ? type[p] : (uint8_t)0;
+        szeta[i] = zeta ? zeta[p] : 0.0;
+    }
+}
+
+// Each live sink adds one to its leaf and every ancestor.  Integer atomics: the counts do not
+// depend on the order of the additions.
+__global__ void count_sinks_kernel(const uint8_t* __restrict__ stype, const int* __restrict__ sleaf,
+                                   const int* __restrict__ parent, int64_t n_live, uint32_t* __restrict__ nsink) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_live;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (stype[i] != 5) continue;
+        for (int no = sleaf[i]; no >= 0; no = parent[no]) atomicAdd(nsink + no, 1u);
+    }
+}
+
 __global__ void vel_moments_kernel(const GNode* __restrict__ nodes, const double* __restrict__ smass,
                                    const uint32_t* __restrict__ order, const double* __restrict__ vx,
                                    const double* __restrict__ vy, const double* __restrict__ vz, int64_t a,
@@ -827,6 +851,28 @@ void tree_velocities(gt_context* ctx, gt_tree* t, const double* vx, const double
                                                                        b, t->vcom, t->nvel, t->vmax);
         check_launch(ctx, "vel_moments_kernel");
     }
+}
+
+void tree_gas(gt_context* ctx, gt_tree* t, const uint8_t* type, const double* zeta) {
+    cudaStream_t st = ctx->stream;
+    const int64_t n = std::max<int64_t>(t->n, 1), nn = std::max<int64_t>(t->n_nodes, 1);
+    // allocated once: a plan captured after the first call keeps pointing at them
+    if (!t->stype) {
+        t->stype = dalloc<uint8_t>((size_t)n, st);
+        t->szeta = dalloc<double>((size_t)n, st);
+        t->nsink = dalloc<uint32_t>((size_t)nn, st);
+    }
+    if (t->n > 0) {
+        gather_gas_kernel<<<grid_for(ctx, t->n), kBlk, 0, st>>>(type, zeta, t->order, t->n, t->stype, t->szeta);
+        check_launch(ctx, "gather_gas_kernel");
+    }
+    check_cuda(cudaMemsetAsync(t->nsink, 0, (size_t)nn * sizeof(uint32_t), st), "memset");
+    if (t->n_live > 0 && type) {
+        count_sinks_kernel<<<grid_for(ctx, t->n_live), kBlk, 0, st>>>(t->stype, t->sleaf, t->parent, t->n_live,
+                                                                      t->nsink);
+        check_launch(ctx, "count_sinks_kernel");
+    }
+    t->gas_zeta = zeta != nullptr;
 }
 
 void run_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay,

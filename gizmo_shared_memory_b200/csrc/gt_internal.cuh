@@ -132,6 +132,12 @@ struct gt_tree {
     double* dq = nullptr;        // 3 * n_nodes
     double* dmass = nullptr;     // n_nodes
     float* xpad = nullptr;       // n_nodes
+    // gas and sinks (gt_tree_gas): particle type (GIZMO numbering) and adaptive-softening zeta in
+    // tree order, sinks (type 5) below each node; gas_zeta: zeta was given (the pair rule applies)
+    uint8_t* stype = nullptr;    // n
+    double* szeta = nullptr;     // n
+    uint32_t* nsink = nullptr;   // n_nodes
+    bool gas_zeta = false;
     // cached all-active group lists, keyed by (mode, param)
     struct GroupCache {
         int mode = -1, param = 0, kmax = 0;
@@ -214,6 +220,7 @@ struct WalkRequest {
     double *ax = nullptr, *ay = nullptr, *az = nullptr, *phi = nullptr;  // device outputs
     double* tidal = nullptr;  // 6 per target (xx yy zz xy yz xz), not times G
     double* jerk = nullptr;   // 3 per target, times G
+    double sink_radius = 0;   // > 0: sink-direct opening (grouped walks of a tree with types)
 };
 void run_walk(gt_context* ctx, const gt_tree* t, const WalkRequest& rq);
 
@@ -271,6 +278,9 @@ void tree_particles(gt_context* ctx, gt_tree* t, const double* x, const double* 
 // (gt_tree_velocities); vx, vy, vz are device arrays over the tree's input particles.
 void tree_velocities(gt_context* ctx, gt_tree* t, const double* vx, const double* vy, const double* vz,
                      bool particles_only = false);
+// Particle types (null: every particle gas) and zeta (null: none), device arrays over the tree's
+// input particles, gathered into tree order; the per-node sink count (gt_tree_gas).
+void tree_gas(gt_context* ctx, gt_tree* t, const uint8_t* type, const double* zeta);
 void run_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay,
                    const double* az, double alpha, double G, double* aold);
 

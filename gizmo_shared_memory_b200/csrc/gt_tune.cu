@@ -159,8 +159,8 @@ void run_autotune(gt_context* ctx, const gt_tree* t, const double* aold, double 
                 if (better(c, best)) best = c;
             }
     }
-    // 3. the learned criterion on the best configuration
-    if (tr.mac_model) {
+    // 3. the learned criterion on the best configuration (the gas pair rule takes the plain one)
+    if (tr.mac_model && !(t->szeta && t->gas_zeta)) {
         for (double kap : tr.kappa) {
             gt_tune_entry c = best;
             c.mac = tr.mac_mode;

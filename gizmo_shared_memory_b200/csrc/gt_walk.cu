@@ -69,6 +69,13 @@ struct WalkArgs {
     const float4* nvel;         // node centre-of-mass velocities (jerk)
     // forest: root node of each group (its system's root); null: node 0
     const int* group_root;
+    // gas and sinks (XT kernel): tree-order type and zeta, FP64 mass; null szeta: no zeta terms.
+    // nsink (per node) non-null with sink_r > 0: sink-direct opening.
+    const uint8_t* stype;
+    const double* szeta;
+    const double* smass;
+    const uint32_t* nsink;
+    double sink_r;
 };
 
 __device__ __forceinline__ int warp_incl_scan_i(int v) {
@@ -178,6 +185,35 @@ __device__ __noinline__ void spline_pair_tidal(float r2, float h, float m, float
     g2 = m * wk * hinv5;
 }
 
+// dW/dr / r of the 3-D cubic spline of support h at r < h (shmem/hydro.h:28-32, 46-54):
+// (8 / pi) fp(q) / (q h^5), with fp(q) / q = 18 q - 12 below q = 1/2 and -6 (1-q)^2 / q above.
+__device__ __forceinline__ float dwdr_over_r(float r, float h) {
+    const float hinv = 1.0f / h;
+    const float q = r * hinv;
+    const float hinv2 = hinv * hinv;
+    float g;
+    if (q < 0.5f) {
+        g = fmaf(18.0f, q, -12.0f);
+    } else {
+        const float u = 1.0f - q;
+        g = -6.0f * u * u / q;
+    }
+    return 2.5464790894703255f * g * (hinv2 * hinv2 * hinv);
+}
+
+// The adaptive-softening terms of a gas-gas pair (shmem/tree.cc:39-53), subtracted from the pair's
+// force factor: (zeta_t / m_t) dW/dr(r, h) / r inside h = max(h_t, h_s), plus (zeta_s / m_t)
+// dW/dr(r, h_s) / r inside h_s.  ztm = zeta_t / m_t and itm = 1 / m_t are 0 for a target that is not
+// gas or has no mass; zs is NaN for a source that is not gas.  r2 == 0 contributes nothing.
+__device__ __noinline__ float zeta_pair(float r2, float h, float hs, float zs, float ztm, float itm) {
+    if (!(r2 > 0.0f) || zs != zs) return 0.0f;
+    const float r = sqrtf(r2);
+    float c = 0.0f;
+    if (ztm != 0.0f && r < h) c = ztm * dwdr_over_r(r, h);
+    if (zs != 0.0f && itm != 0.0f && r < hs) c = fmaf(zs * itm, dwdr_over_r(r, hs), c);
+    return c;
+}
+
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
     const float y = x - comp;
     const float t = sum + y;
@@ -196,13 +232,16 @@ struct alignas(16) WarpHdr {
     double lo_x, lo_y, lo_z, hi_x, hi_y, hi_z, c_x, c_y, c_z, emax, amin;
 };
 
-// xt: the lists also carry each entry's velocity (float4), for the jerk.
+// xt: the lists also carry each entry's velocity (float4), for the jerk, and the particle list
+// each source's zeta (float), for the gas pair rule.
 __host__ __device__ constexpr int warp_smem_bytes(int pn_cap, int pp_cap, bool xt = false) {
-    return ((int)sizeof(WarpHdr) + pn_cap * 16 + pp_cap * 20 + (xt ? (pn_cap + pp_cap) * 16 : 0) + 15) & ~15;
+    return ((int)sizeof(WarpHdr) + pn_cap * 16 + pp_cap * 20 + (xt ? (pn_cap + pp_cap) * 16 + pp_cap * 4 : 0) + 15) &
+           ~15;
 }
 
 // MAC: 0 plain relative criterion, 1 network inside the walk (GT_MAC_LEARNED), 2 per-node
-// learned scale (GT_MAC_NODE).  XT: also the tidal tensor and/or the jerk (A.tidal, A.jerk).
+// learned scale (GT_MAC_NODE).  XT: also the tidal tensor and/or the jerk (A.tidal, A.jerk), the
+// zeta terms of gas-gas pairs (A.szeta) and sink-direct opening (A.nsink).
 template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT, int MAC, bool XT = false>
 __global__ void __launch_bounds__(kMaxWarps * 32, (TPL == 1 && !XT) ? 3 : 2)
 walk_kernel(const WalkArgs A) {
@@ -224,8 +263,11 @@ walk_kernel(const WalkArgs A) {
     float* __restrict__ ph = reinterpret_cast<float*>(pp + A.pp_cap);
     float4* __restrict__ pnv = reinterpret_cast<float4*>(ph + A.pp_cap);  // XT only
     float4* __restrict__ ppv = pnv + A.pn_cap;
+    float* __restrict__ pzs = reinterpret_cast<float*>(ppv + A.pp_cap);  // XT only: source zeta
     const bool want_tid = XT && A.tidal != nullptr;
     const bool want_jerk = XT && A.jerk != nullptr;
+    const bool want_zeta = XT && A.szeta != nullptr;
+    const bool sink_rule = XT && A.nsink != nullptr;
 
     unsigned long long c_nodes = 0, c_multi = 0, c_pairs = 0, c_zero = 0, c_flush = 0, c_steps = 0;
     int c_maxtop = 0;
@@ -306,22 +348,36 @@ walk_kernel(const WalkArgs A) {
                 pn[pos] = make_float4(x, y, z, m);
             }
         };
-        // tidal tensor and jerk: FP64 totals (xx yy zz xy yz xz, jx jy jz) and target velocities
+        // tidal tensor and jerk: FP64 totals (xx yy zz xy yz xz, jx jy jz) and target velocities;
+        // gas targets: zeta / m and 1 / m (0 for a target that is not gas or has no mass,
+        // tree.cc:46); a group holding a sink opens by the sink rule (tree.cc:691-698)
         double xt[9][TPL];
-        float tvx[TPL], tvy[TPL], tvz[TPL];
+        float tvx[TPL], tvy[TPL], tvz[TPL], tzm[TPL], tim[TPL];
+        bool has_sink = false;
         if (XT) {
+            bool sink = false;
 #pragma unroll
             for (int k = 0; k < TPL; ++k) {
 #pragma unroll
                 for (int c = 0; c < 9; ++c) xt[c][k] = 0.0;
                 tvx[k] = tvy[k] = tvz[k] = 0.0f;
+                tzm[k] = tim[k] = 0.0f;
                 const int i = ti + 32 * k;
+                const int p = i < nt ? (A.tpos ? (int)A.tpos[t0 + i] : t0 + i) : 0;
                 if (want_jerk && i < nt) {
-                    const int p = A.tpos ? (int)A.tpos[t0 + i] : t0 + i;
                     const float4 v = A.svel[p];
                     tvx[k] = v.x; tvy[k] = v.y; tvz[k] = v.z;
                 }
+                if (want_zeta && i < nt && A.stype[p] == 0) {
+                    const double mt = A.smass[p];
+                    if (mt > 0.0) {
+                        tzm[k] = (float)(A.szeta[p] / mt);
+                        tim[k] = (float)(1.0 / mt);
+                    }
+                }
+                if (sink_rule && i < nt) sink |= A.stype[p] == 5;
             }
+            has_sink = __any_sync(kFull, sink);
         }
         // one interaction's tidal and jerk terms: T += -g1 I + g2 d d, J += g1 dv - (dv.d) g2 d
         // (shmem/tree.cc:811-837, 845-872); d = source - target, dv = v_source - v_target
@@ -475,21 +531,25 @@ walk_kernel(const WalkArgs A) {
                         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                         const float hh = fmaxf(th[k], hj);
                         float f, p, g2 = 0.0f;
+                        float fa;  // the acceleration's factor: f less the gas pair's zeta terms
                         if (r2 >= hh * hh && r2 > 0.0f) {
                             const float ri = rsqrtf(r2);
                             const float mri = e.w * ri;
                             f = mri * ri * ri;
                             p = -mri;
                             if (XT) g2 = 3.0f * f * (ri * ri);
+                            fa = f;
                         } else if (XT) {
                             spline_pair_tidal(r2, hh, e.w, f, p, g2);
+                            fa = want_zeta ? f - zeta_pair(r2, hh, hj, pzs[j], tzm[k], tim[k]) : f;
                         } else {
                             spline_pair(r2, hh, e.w, f, p);
+                            fa = f;
                         }
                         if (COUNT) zero += (r2 == 0.0f);
-                        ax_[k] = fmaf(dx, f, ax_[k]);
-                        ay_[k] = fmaf(dy, f, ay_[k]);
-                        az_[k] = fmaf(dz, f, az_[k]);
+                        ax_[k] = fmaf(dx, fa, ax_[k]);
+                        ay_[k] = fmaf(dy, fa, ay_[k]);
+                        az_[k] = fmaf(dz, fa, az_[k]);
                         if (WANT_POT) ap_[k] += p;
                         if (XT) {
                             const float4 ev = want_jerk ? ppv[j] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -573,6 +633,11 @@ walk_kernel(const WalkArgs A) {
                         }
                     }
                 }
+                // sink-direct opening (tree.cc:772-778): only ever adds opening
+                if (sink_rule && has_sink && !open && __ldg(A.nsink + node) > 0u) {
+                    const double reach = A.sink_r + 0.6 * (double)nd.len;
+                    if (r2 < reach * reach) open = true;
+                }
                 if (!open) accept = true;
                 else if (leaf) expand = true;
                 else push = true;
@@ -654,6 +719,7 @@ walk_kernel(const WalkArgs A) {
                         pp[pos] = e;
                         ph[pos] = qh;
                         if (want_jerk) ppv[pos] = A.svel[qpos];
+                        if (want_zeta) pzs[pos] = A.stype[qpos] == 0 ? (float)A.szeta[qpos] : __int_as_float(0x7fc00000);
                     }
                     npn += nf;
                     npp += nn;
@@ -916,9 +982,13 @@ void dispatch_count(gt_context* ctx, const WalkArgs& a, int blocks, int warps, b
     else launch_walk<TPL, LA, POT, false, MAC>(ctx, a, blocks, warps);
 }
 
-// Tidal tensor / jerk: grouped walk, plain criterion, groups of at most 32 targets.
-void dispatch_xt(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool pot, bool cnt) {
-    if (pot) {
+// Tidal tensor / jerk / gas rules: plain criterion, groups of at most 32 targets.  The per-target
+// walk (no leaf acceptance) only for the gas rules of accelerations.
+void dispatch_xt(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la, bool pot, bool cnt) {
+    if (!la) {
+        if (cnt) launch_walk<1, false, false, true, 0, true>(ctx, a, blocks, warps);
+        else launch_walk<1, false, false, false, 0, true>(ctx, a, blocks, warps);
+    } else if (pot) {
         if (cnt) launch_walk<1, true, true, true, 0, true>(ctx, a, blocks, warps);
         else launch_walk<1, true, true, false, 0, true>(ctx, a, blocks, warps);
     } else {
@@ -971,8 +1041,11 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     int param = rq.group_param;
     if (mode == GT_GROUP_NODE && param <= 0) param = 32;
     if (mode == GT_GROUP_BATCH && param <= 0) mode = GT_GROUP_LEAF;
-    // a warp holds up to 32, 64 or 128 targets (1, 2 or 4 per lane); longer groups are chunked
-    const bool xt = rq.tidal != nullptr || rq.jerk != nullptr;
+    // a warp holds up to 32, 64 or 128 targets (1, 2 or 4 per lane); longer groups are chunked.
+    // The tidal tensor, the jerk and the gas rules run on the XT kernel.
+    const bool zeta_on = t->szeta && t->gas_zeta && rq.want_acc && rq.ax;
+    const bool sink_on = t->nsink && rq.sink_radius > 0.0 && rq.leaf_accept;
+    const bool xt = rq.tidal != nullptr || rq.jerk != nullptr || zeta_on || sink_on;
     int kmax = 32;
     if (!xt && (mode == GT_GROUP_NODE || mode == GT_GROUP_BATCH) && param > 32) kmax = param > 64 ? 128 : 64;
     const int tpl = kmax / 32;
@@ -1103,8 +1176,15 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     a.jerk = rq.jerk;
     a.svel = t->svel;
     a.nvel = t->nvel;
-    if (xt && (rq.mac != GT_MAC_PLAIN || !rq.leaf_accept))
-        throw Fail{GT_ERR_UNSUPPORTED, "the tidal tensor and the jerk come from the grouped walk with the plain criterion"};
+    if (xt && rq.mac != GT_MAC_PLAIN)
+        throw Fail{GT_ERR_UNSUPPORTED, "the tidal tensor, the jerk and the gas rules take the plain criterion"};
+    if (xt && !rq.leaf_accept && (rq.tidal || rq.jerk || (rq.want_phi && rq.phi)))
+        throw Fail{GT_ERR_UNSUPPORTED, "the tidal tensor and the jerk come from the grouped walk"};
+    a.stype = t->stype;
+    a.szeta = zeta_on ? t->szeta : nullptr;
+    a.smass = t->smass;
+    a.nsink = sink_on ? t->nsink : nullptr;
+    a.sink_r = rq.sink_radius;
     if (rq.jerk && !t->svel) throw Fail{GT_ERR_INVALID, "the jerk needs velocities (gt_tree_velocities)"};
     // a captured graph keeps its pointers: it runs on buffers its plan owns, not on the workspace
     WalkBuffers* wb = rq.bufs;
@@ -1161,7 +1241,7 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         a.stack_cap = stack_cap;
         check_cuda(cudaMemsetAsync(ctr, 0, 96, st), "memset counters");
         if (!rq.capture) check_cuda(cudaEventRecord(ctx->ev0, st), "event");
-        if (xt) dispatch_xt(ctx, a, blocks, warps, want_pot, rq.count);
+        if (xt) dispatch_xt(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count);
         else if (tpl == 1) dispatch<1>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
         else if (tpl == 2) dispatch<2>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
         else dispatch<4>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);

@@ -13,9 +13,12 @@
 //     consistent with it.
 //   * Equal keys keep particle-index order (the reference's parallel sort leaves them unordered).
 //   * Options the GPU path does not implement throw std::runtime_error naming the option: the
-//     adaptive-softening zeta terms, lazy drift, sink-direct opening, and the incremental-moment
-//     methods of Tree (tree reuse across steps).
-//   * The walk reads particle positions captured at build(): rebuild after moving particles.
+//     zeta terms in accel_brute (the FP64 direct sum has no gas rule) and the neighbour-search
+//     bounds Tree::raise_hmax / Tree::init_hmax.
+//   * Lazy drift catches up every particle behind the target before the walk (the device walk
+//     reads all of them), not only those the walk reaches.
+//   * After the first tree event or refresh, each walk uploads the particles' current positions,
+//     masses and softenings; types and zeta are uploaded before every walk that has them.
 #pragma once
 #include <omp.h>
 
@@ -34,7 +37,7 @@ namespace shmem {
 
 struct Particles {
     std::vector<double> x, y, z, m, soft;
-    std::vector<double> zeta;    // adaptive-softening corrections; must be empty or all zero here
+    std::vector<double> zeta;    // adaptive-softening corrections (gas-gas pairs); empty = none
     std::vector<uint8_t> type;   // GIZMO particle type (0 = gas); empty = all gas
     size_t size() const { return m.size(); }
     Vec3d pos(size_t i) const { return Vec3d{x[i], y[i], z[i]}; }

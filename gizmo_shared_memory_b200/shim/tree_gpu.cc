@@ -41,9 +41,10 @@ void check(int st, const char* what) {
     throw std::runtime_error(std::string("shmem (GPU): ") + what + " is not implemented on the GPU path");
 }
 
-void require_gravity_only(const Particles& P) {
+// The FP64 direct sum (gt_direct) has no gas pair rule.
+void require_no_zeta(const Particles& P) {
     for (double z : P.zeta)
-        if (z != 0.0) unsupported("the adaptive-softening zeta pair terms");
+        if (z != 0.0) unsupported("accel_brute with the adaptive-softening zeta pair terms");
 }
 
 const double* soft_or_null(const Particles& P) { return P.soft.empty() ? nullptr : P.soft.data(); }
@@ -245,13 +246,20 @@ static void prepare_walk(const Tree& T, const Particles& P, const LazyDrift* laz
     if (Q.moved || drift)
         check(gt_tree_particles(context(), T.gpu.get(), P.x.data(), P.y.data(), P.z.data(), P.m.data(),
                                 soft_or_null(P), GT_MEM_HOST), "gt_tree_particles");
+    // types and zeta as the walk reads them now (the engine updates zeta between steps): the gas
+    // pair rule and the per-node sink counts of sink-direct opening
+    if (!P.type.empty() || !P.zeta.empty()) {
+        if ((!P.type.empty() && P.type.size() != P.size()) || (!P.zeta.empty() && P.zeta.size() != P.size()))
+            throw std::runtime_error("shmem (GPU): Particles::type / ::zeta sizes differ from the particle count");
+        check(gt_tree_gas(context(), T.gpu.get(), P.type.empty() ? nullptr : P.type.data(),
+                          P.zeta.empty() ? nullptr : P.zeta.data(), GT_MEM_HOST), "gt_tree_gas");
+    }
 }
 
 void accel(const Tree& T, const Particles& P, const std::vector<uint32_t>& targets, double theta,
            double G, std::vector<double>& ax, std::vector<double>& ay, std::vector<double>& az,
            const double* aold) {
     need_gpu(T);
-    require_gravity_only(P);
     prepare_walk(T, P, nullptr);
     const size_t nt = targets.size();
     ax.assign(nt, 0.0); ay.assign(nt, 0.0); az.assign(nt, 0.0);
@@ -274,8 +282,6 @@ void accel_grouped(const Tree& T, const Particles& P, const std::vector<uint32_t
                    std::vector<SymTensor3d>* tidal, const double* aold, const LazyDrift* lazy,
                    std::vector<Vec3d>* jerk, const double* const* vel, double sink_direct_radius) {
     need_gpu(T);
-    require_gravity_only(P);
-    if (sink_direct_radius > 0 && !P.type.empty()) unsupported("sink-direct opening");
     prepare_walk(T, P, lazy);
     // the jerk needs source velocities: the walk's `vel` for particles and the build's node
     // centre-of-mass velocities (tree.cc:638-640); without them it stays zero
@@ -287,6 +293,8 @@ void accel_grouped(const Tree& T, const Particles& P, const std::vector<uint32_t
     if (!nt) return;
     gt_walk_options o;
     gt_walk_options_default(&o);
+    // live only with types (tree.cc:634-635): without them the tree counted no sinks
+    o.sink_direct_radius = (P.type.empty() || !(sink_direct_radius > 0.0)) ? 0.0 : sink_direct_radius;
     if (!tidal && !want_jerk) {
         check(gt_accel_grouped(context(), T.gpu.get(), (int64_t)nt, targets.data(), aold, theta, G, batch,
                                &o, GT_MEM_HOST, ax.data(), ay.data(), az.data(), nullptr), "gt_accel_grouped");
@@ -317,7 +325,7 @@ void potential(const Tree& T, const Particles& P, const std::vector<uint32_t>& t
 
 void accel_brute(const Particles& P, const std::vector<uint32_t>& targets, double G,
                  std::vector<double>& ax, std::vector<double>& ay, std::vector<double>& az) {
-    require_gravity_only(P);
+    require_no_zeta(P);
     const size_t nt = targets.size();
     ax.assign(nt, 0.0); ay.assign(nt, 0.0); az.assign(nt, 0.0);
     if (!nt) return;

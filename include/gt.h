@@ -20,9 +20,8 @@
  *    targets = orderbuf (what shmem/bench_treeforce.cc:41 passes).
  *  - One context per host thread; one CUDA stream per context.  Trees may be used by any context
  *    on the same device.
- *  - Options the GPU path does not implement (adaptive-softening zeta, tidal tensor, jerk, lazy
- *    drift, sink-direct opening, periodic boxes) are rejected with GT_ERR_UNSUPPORTED; there is
- *    no CPU fallback.
+ *  - Options the GPU path does not implement (lazy drift inside the walk, periodic boxes) are
+ *    rejected with GT_ERR_UNSUPPORTED; there is no CPU fallback.
  */
 #ifndef GT_H
 #define GT_H
@@ -119,6 +118,11 @@ typedef struct {
     const float* mac_model;
     double mac_kappa;
     double mac_band[2];
+    /* SINGLE_STAR_DIRECT_GRAVITY_RADIUS: > 0 turns on sink-direct opening in the grouped walks of a
+     * tree with particle types (gt_tree_gas): a group holding a sink opens every node the criterion
+     * accepted that holds a sink and comes within this radius + 0.6 side of the group's box
+     * (accel_grouped's sink_direct_radius, tree.h:435-440, tree.cc:691-698, 772-778).  Default 0. */
+    double sink_direct_radius;
 } gt_walk_options;
 
 typedef struct {
@@ -246,13 +250,24 @@ GT_API int gt_tree_node_state(gt_context* ctx, gt_tree* tree, double tau, double
  * current state (tree.cc:786-789), the structure stays the build's. */
 GT_API int gt_tree_particles(gt_context* ctx, gt_tree* tree, const double* x, const double* y,
                       const double* z, const double* m, const double* soft, int mem);
+/* Gas and sinks.  Attach particle types (GIZMO numbering: 0 gas, 5 sink; NULL = every particle
+ * gas) and the adaptive-softening zeta (NULL = none), indexed like the build's input, as
+ * shmem::Particles::type and ::zeta (tree.h:38-49); the tree counts the sinks below every node
+ * (tree.cc:155-187).  From then on every walk of the tree that returns accelerations applies the
+ * zeta terms of gas-gas pairs inside the kernel (pair_force_over_r, tree.cc:39-53) -- the
+ * potential, the tidal tensor and the jerk keep the zeta-free pair factor, as the reference's do --
+ * and gt_walk_options.sink_direct_radius > 0 turns on sink-direct opening.  Call again to update
+ * zeta between steps: the tree keeps the same buffers, so a plan created after the first call
+ * sees the new values.  A plan created before the first call does not apply the gas rules. */
+GT_API int gt_tree_gas(gt_context* ctx, gt_tree* tree, const uint8_t* type, const double* zeta, int mem);
 /* Per-node centre-of-mass velocity (n_nodes each) and speed bound; any pointer may be null. */
 GT_API int gt_tree_velocity_moments(gt_context* ctx, const gt_tree* tree, double* vcx, double* vcy,
                              double* vcz, float* vmax);
 
 /* ---- walks --------------------------------------------------------------------------------- */
-/* Grouped walk.  Replaces shmem::accel_grouped (shmem/tree.h:428-440, tree.cc:626-897) for the
- * gravity-only case (tidal = jerk = lazy = NULL, sink_direct_radius = 0).  batch <= 0 groups
+/* Grouped walk.  Replaces shmem::accel_grouped (shmem/tree.h:428-440, tree.cc:626-897) without
+ * the tidal tensor and the jerk (gt_accel_grouped_ext) and without lazy drift; the gas rules and
+ * sink-direct opening come from gt_tree_gas and gt_walk_options.sink_direct_radius.  batch <= 0 groups
  * targets by leaf, batch > 0 in fixed windows, unless opt->group_mode overrides it.
  * aold (may be NULL) is ErrTolForceAcc*|a_prev|/G per target (tree.h:389-391); theta > 0 adds the
  * Barnes-Hut test.  phi (may be NULL) receives the potential from the same walk. */

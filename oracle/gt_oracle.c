@@ -723,6 +723,145 @@ void or_walk_groups_ext(const or_tree* t, int64_t nt, const uint32_t* targets, i
     }
 }
 
+/* dW/dr of the 3-D cubic-spline kernel at fixed h (shmem/hydro.h:28-32, 46-54): norm 8/(pi h^3),
+ * fp(q) = -12 q + 18 q^2 below q = 1/2 and -6 (1-q)^2 above, zero from q = 1. */
+double or_kernel_dwdr(double r, double h) {
+    const double q = r / h;
+    if (q >= 1.0) return 0.0;
+    const double norm = 8.0 / (M_PI * h * h * h);
+    double fp;
+    if (q < 0.5) {
+        fp = -12.0 * q + 18.0 * q * q;
+    } else {
+        const double u = 1.0 - q;
+        fp = -6.0 * u * u;
+    }
+    return norm * fp / h;
+}
+
+/* Particle-particle force factor under adaptive gas softening (shmem/tree.cc:39-53): the spline
+ * of the larger softening, and for a gas-gas pair with a massive target the two zeta terms (the
+ * target's on the pair softening, the source's on its own), each only inside its kernel and
+ * divided by the target's mass. */
+static double or_pair_fac(double r, double qm, double te, double qs, double zt, double zq, double mt,
+                          int gas_gas) {
+    const double e = dmax(dmax(te, qs), 1e-300);
+    double fac = qm * or_spline_force_over_r(r, e);
+    if (!gas_gas || mt <= 0) return fac;
+    const double es = dmax(qs, 1e-300);
+    if (zt != 0.0 && r < e) fac -= (zt / mt) * or_kernel_dwdr(r, e) / r;
+    if (zq != 0.0 && r < es) fac -= (zq / mt) * or_kernel_dwdr(r, es) / r;
+    return fac;
+}
+
+/* Walk of explicit groups with the gas pair rule and sink-direct opening.  type (GIZMO numbering,
+ * 0 = gas, 5 = sink; null = every particle gas) and zeta (null = 0) are indexed like the build's
+ * particles.  leaf_accept = 1 is accel_grouped (tree.cc:626-897): a group holding a sink opens
+ * every node the criterion accepted that holds a sink and whose box comes within
+ * sink_radius + 0.6 len of the group's box (tree.cc:691-698, 772-778); leaf_accept = 0 is the
+ * per-target accel (tree.cc:528-582), with no sink rule. */
+void or_walk_groups_gas(const or_tree* t, int64_t nt, const uint32_t* targets, int64_t ngroups,
+                        const int64_t* starts, double theta, double G, const double* aold,
+                        const uint8_t* type, const double* zeta, double sink_radius, int leaf_accept,
+                        double* ax, double* ay, double* az) {
+    const double theta2 = theta * theta;
+    (void)nt;
+    /* sinks below each node: a prefix count over the tree order (a node owns [plo, phi)) */
+    int64_t* pre = (int64_t*)calloc((size_t)t->nlive + 1, sizeof(int64_t));
+    for (int64_t k = 0; k < t->nlive; ++k) pre[k + 1] = pre[k] + (type && type[t->order[k]] == 5);
+    const int sink_direct = sink_radius > 0.0 && type != NULL && leaf_accept;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t g = 0; g < ngroups; ++g) {
+        const int64_t lo = starts[g], hi = starts[g + 1];
+        const int nb = (int)(hi - lo);
+        double b0[3] = {1e300, 1e300, 1e300}, b1[3] = {-1e300, -1e300, -1e300}, emax = 0;
+        double amin = aold ? 1e300 : 0.0;
+        int has_sink = 0;
+        double* buf = (double*)calloc((size_t)nb * 9, 8);
+        double *tx = buf, *ty = buf + nb, *tz = buf + 2 * nb, *te = buf + 3 * nb;
+        double *tm = buf + 4 * nb, *tzeta = buf + 5 * nb;
+        double *oax = buf + 6 * nb, *oay = buf + 7 * nb, *oaz = buf + 8 * nb;
+        char* tgas = (char*)calloc((size_t)nb, 1);
+        for (int i = 0; i < nb; ++i) {
+            const uint32_t p = targets[lo + i];
+            tx[i] = t->x[p]; ty[i] = t->y[p]; tz[i] = t->z[p];
+            te[i] = t->soft ? t->soft[p] : 0.0;
+            tm[i] = t->m[p];
+            tzeta[i] = zeta ? zeta[p] : 0.0;
+            tgas[i] = type == NULL || type[p] == 0;
+            if (sink_direct && type[p] == 5) has_sink = 1;
+            b0[0] = dmin(b0[0], tx[i]); b1[0] = dmax(b1[0], tx[i]);
+            b0[1] = dmin(b0[1], ty[i]); b1[1] = dmax(b1[1], ty[i]);
+            b0[2] = dmin(b0[2], tz[i]); b1[2] = dmax(b1[2], tz[i]);
+            emax = dmax(emax, te[i]);
+            if (aold) amin = dmin(amin, aold[lo + i]);
+        }
+        int node = t->root;
+        while (node >= 0) {
+            const double ncx = t->cx[node], ncy = t->cy[node], ncz = t->cz[node];
+            const double dx = dmax(0.0, dmax(b0[0] - ncx, ncx - b1[0]));
+            const double dy = dmax(0.0, dmax(b0[1] - ncy, ncy - b1[1]));
+            const double dz = dmax(0.0, dmax(b0[2] - ncz, ncz - b1[2]));
+            const double r2n = dx * dx + dy * dy + dz * dz;
+            const int is_leaf = t->first[node] < 0;
+            int accept = 0;
+            if (leaf_accept || !is_leaf)
+                accept = !or_open_node(r2n, (double)t->w_len[node], t->w_s[node], t->mass[node],
+                                       (double)t->w_soft[node], emax, amin, theta2, dx, dy, dz);
+            if (accept && has_sink && pre[t->phi[node]] > pre[t->plo[node]]) {
+                const double reach = sink_radius + 0.6 * (double)t->w_len[node];
+                if (r2n < reach * reach) accept = 0;
+            }
+            if (accept || is_leaf) {
+                if (accept) {
+                    for (int i = 0; i < nb; ++i) {
+                        const double ox = ncx - tx[i], oy = ncy - ty[i], oz = ncz - tz[i];
+                        const double r2 = ox * ox + oy * oy + oz * oz;
+                        if (r2 <= 0) continue;
+                        const double f = t->mass[node] *
+                                         or_spline_force_over_r(sqrt(r2), dmax(dmax(te[i], (double)t->w_soft[node]), 1e-300));
+                        oax[i] += ox * f; oay[i] += oy * f; oaz[i] += oz * f;
+                    }
+                } else {
+                    for (int k = t->plo[node]; k < t->phi[node]; ++k) {
+                        const uint32_t q = t->order[k];
+                        const double qx = t->x[q], qy = t->y[q], qz = t->z[q], qm = t->m[q];
+                        const double qs = t->soft ? t->soft[q] : 0.0;
+                        const double zq = zeta ? zeta[q] : 0.0;
+                        const int qgas = type == NULL || type[q] == 0;
+                        for (int i = 0; i < nb; ++i) {
+                            if (targets[lo + i] == q) continue;
+                            const double ox = qx - tx[i], oy = qy - ty[i], oz = qz - tz[i];
+                            const double r2 = ox * ox + oy * oy + oz * oz;
+                            if (r2 <= 0) continue;
+                            const double f = or_pair_fac(sqrt(r2), qm, te[i], qs, tzeta[i], zq, tm[i], tgas[i] && qgas);
+                            oax[i] += ox * f; oay[i] += oy * f; oaz[i] += oz * f;
+                        }
+                    }
+                }
+                node = t->next[node];
+            } else {
+                node = t->first[node];
+            }
+        }
+        for (int i = 0; i < nb; ++i) {
+            ax[lo + i] = G * oax[i]; ay[lo + i] = G * oay[i]; az[lo + i] = G * oaz[i];
+        }
+        free(tgas);
+        free(buf);
+    }
+    free(pre);
+}
+
+/* Sinks (type 5) below every node (tree.cc:155-187); nsink has nnodes entries. */
+void or_node_sinks(const or_tree* t, const uint8_t* type, uint32_t* nsink) {
+    for (int64_t i = 0; i < t->nnodes; ++i) {
+        uint32_t c = 0;
+        for (int k = t->plo[i]; k < t->phi[i]; ++k) c += type[t->order[k]] == 5;
+        nsink[i] = c;
+    }
+}
+
 /* Tree reuse: replace the walk's node fields with refreshed ones (refresh_walk_nodes writes the
  * packed walk nodes, tree.cc:256-274) and point the tree at the particles' current positions (the
  * walk reads them, tree.cc:786-789). */

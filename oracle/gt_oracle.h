@@ -74,6 +74,18 @@ void or_walk_groups_ext(const or_tree* t, int64_t nt, const uint32_t* targets, i
                         const double* vx, const double* vy, const double* vz, const double* vcx,
                         const double* vcy, const double* vcz, double* ax, double* ay, double* az,
                         double* tidal, double* jerk);
+/* dW/dr of the 3-D cubic spline at fixed h (shmem/hydro.h:46-54). */
+double or_kernel_dwdr(double r, double h);
+/* Walk of explicit groups with the adaptive-softening pair rule (zeta terms for gas-gas pairs,
+ * tree.cc:39-53) and, with leaf_accept = 1, sink-direct opening within sink_radius
+ * (tree.cc:691-698, 772-778).  type (0 = gas, 5 = sink; null = all gas) and zeta (null = 0) are
+ * indexed like the build's particles.  leaf_accept = 0 is the per-target accel (tree.cc:528-582). */
+void or_walk_groups_gas(const or_tree* t, int64_t nt, const uint32_t* targets, int64_t ngroups,
+                        const int64_t* starts, double theta, double G, const double* aold,
+                        const uint8_t* type, const double* zeta, double sink_radius, int leaf_accept,
+                        double* ax, double* ay, double* az);
+/* Sinks below each node (tree.cc:155-187); nnodes entries. */
+void or_node_sinks(const or_tree* t, const uint8_t* type, uint32_t* nsink);
 /* Tree reuse: overwrite the walk's node fields (COM, mass, opening radius, side, softening) and
  * re-point the particle positions (the caller keeps the arrays alive). */
 void or_set_walk_nodes(or_tree* t, const double* cx, const double* cy, const double* cz, const double* mass,

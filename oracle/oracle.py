@@ -108,6 +108,11 @@ class Restatement:
                                          C.c_double, _d] + [_d] * 11
         L.or_direct.argtypes = [C.c_int64, _d, _d, _d, _d, _d, C.c_int64, _u32, C.c_double,
                                 _d, _d, _d, _d]
+        L.or_kernel_dwdr.restype = C.c_double
+        L.or_kernel_dwdr.argtypes = [C.c_double, C.c_double]
+        L.or_walk_groups_gas.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_int64, _i64, C.c_double,
+                                         C.c_double, _d, C.c_void_p, _d, C.c_double, C.c_int, _d, _d, _d]
+        L.or_node_sinks.argtypes = [C.c_void_p, C.c_void_p, _u32]
 
     # scalar helpers
     def spline_force_over_r(self, r, h):
@@ -274,6 +279,28 @@ class OracleTree:
                                       _p(az, _d), _p(tt, _d), _p(jj, _d))
         return ax, ay, az, tt, jj
 
+    def walk_groups_gas(self, targets, starts, theta, G=1.0, aold=None, type=None, zeta=None,
+                        sink_radius=0.0, leaf_accept=True):
+        """Walk with the gas pair rule (zeta terms for gas-gas pairs) and, grouped, sink-direct
+        opening; type (uint8, 0 gas, 5 sink) and zeta are indexed like the build's particles."""
+        t = _targets(targets)
+        nt = len(t)
+        st = np.ascontiguousarray(starts, np.int64)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        ty = None if type is None else np.ascontiguousarray(type, np.uint8)
+        ze = None if zeta is None else _f64(zeta)
+        ao = _f64(aold) if aold is not None else None
+        self.lib.L.or_walk_groups_gas(self.h, nt, _p(t, _u32), len(st) - 1, _p(st, _i64), theta, G, _p(ao, _d),
+                                      None if ty is None else ty.ctypes.data, _p(ze, _d), sink_radius,
+                                      int(leaf_accept), _p(ax, _d), _p(ay, _d), _p(az, _d))
+        return ax, ay, az
+
+    def node_sinks(self, type):
+        ty = np.ascontiguousarray(type, np.uint8)
+        out = np.zeros(self.nnodes, np.uint32)
+        self.lib.L.or_node_sinks(self.h, ty.ctypes.data, _p(out, _u32))
+        return out
+
     def accel_grouped(self, targets, theta, G=1.0, batch=0, aold=None):
         t = _targets(targets)
         nt = len(t)
@@ -345,6 +372,11 @@ class Reference:
         L.ref_tree_vel.argtypes = [C.c_void_p, _d, _d, _d, _f]
         L.ref_accel_grouped_ext.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double,
                                             C.c_int, _d, _d, _d, _d, _d, _d]
+        L.ref_build_gas.restype = C.c_void_p
+        L.ref_build_gas.argtypes = [C.c_int64] + [_d] * 6 + [C.c_void_p]
+        L.ref_accel_grouped_gas.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, C.c_int, _d,
+                                            C.c_double, _d, _d, _d]
+        L.ref_tree_nsink.argtypes = [C.c_void_p, _u32]
         L.ref_reuse_begin.argtypes = [C.c_void_p]
         L.ref_kick_node.argtypes = [C.c_void_p, C.c_int, _d, C.c_double]
         L.ref_mass_event.argtypes = [C.c_void_p, C.c_int, C.c_double, _d, _d, C.c_double, C.c_double]
@@ -397,16 +429,25 @@ class Reference:
         """vel = (vx, vy, vz): build with velocities (per-node vcom and vmax, for the jerk)."""
         return ReferenceTree(self, P, randomize_seed, vel)
 
+    def build_gas(self, P):
+        """Build with P["type"] (uint8, GIZMO numbering) and P["zeta"] (adaptive-softening terms)."""
+        return ReferenceTree(self, P, gas=True)
+
 
 class ReferenceTree:
-    def __init__(self, lib: Reference, P, randomize_seed=-1, vel=None):
+    def __init__(self, lib: Reference, P, randomize_seed=-1, vel=None, gas=False):
         self.lib = lib
         x, y, z, m = (_f64(P[k]) for k in ("x", "y", "z", "m"))
         soft = P.get("soft")
         soft = _f64(soft) if soft is not None else None
         self.n = len(m)
         self.build_times = np.zeros(7)
-        if vel is None:
+        if gas:
+            self._zeta = _f64(P["zeta"])
+            self._type = np.ascontiguousarray(P["type"], np.uint8)
+            self.h = lib.L.ref_build_gas(self.n, _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), _p(soft, _d),
+                                         _p(self._zeta, _d), self._type.ctypes.data)
+        elif vel is None:
             self.h = lib.L.ref_build(self.n, _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), _p(soft, _d),
                                      randomize_seed, _p(self.build_times, _d))
         else:
@@ -514,6 +555,20 @@ class ReferenceTree:
     def set_positions(self, x, y, z):
         x, y, z = (_f64(a) for a in (x, y, z))
         self.lib.L.ref_set_positions(self.h, _p(x, _d), _p(y, _d), _p(z, _d))
+
+    def accel_grouped_gas(self, targets, theta, G=1.0, batch=0, aold=None, sink_radius=0.0):
+        t = _targets(targets)
+        nt = len(t)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        ao = _f64(aold) if aold is not None else None
+        self.lib.L.ref_accel_grouped_gas(self.h, nt, _p(t, _u32), theta, G, batch, _p(ao, _d), sink_radius,
+                                         _p(ax, _d), _p(ay, _d), _p(az, _d))
+        return ax, ay, az
+
+    def nsink(self):
+        out = np.zeros(self.nnodes, np.uint32)
+        self.lib.L.ref_tree_nsink(self.h, _p(out, _u32))
+        return out
 
     def vel_moments(self):
         nn = self.nnodes

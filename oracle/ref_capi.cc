@@ -75,6 +75,38 @@ void* ref_build_vel(int64_t n, const double* x, const double* y, const double* z
     return h;
 }
 
+// shmem::build of particles with types and adaptive-softening zeta (Particles::type, ::zeta,
+// tree.h:38-49): the build counts sinks (type 5) per node for sink-direct opening (tree.cc:155-187).
+void* ref_build_gas(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                    const double* soft, const double* zeta, const uint8_t* type) {
+    RefHandle* h = new RefHandle();
+    h->P.x.assign(x, x + n); h->P.y.assign(y, y + n); h->P.z.assign(z, z + n);
+    h->P.m.assign(m, m + n);
+    if (soft) h->P.soft.assign(soft, soft + n);
+    if (zeta) h->P.zeta.assign(zeta, zeta + n);
+    if (type) h->P.type.assign(type, type + n);
+    h->T = build(h->P, nullptr, nullptr, false, -1);
+    return h;
+}
+
+// shmem::accel_grouped with the gas pair rule (zeta terms for gas-gas pairs, tree.cc:39-53) and
+// sink-direct opening within sink_direct_radius (tree.cc:773-778).
+void ref_accel_grouped_gas(void* p, int64_t nt, const uint32_t* targets, double theta, double G, int batch,
+                           const double* aold, double sink_direct_radius, double* ax, double* ay, double* az) {
+    RefHandle* h = static_cast<RefHandle*>(p);
+    std::vector<uint32_t> tg(targets, targets + nt);
+    std::vector<double> vx, vy, vz;
+    accel_grouped(h->T, h->P, tg, theta, G, batch, vx, vy, vz, nullptr, aold, nullptr, nullptr, nullptr,
+                  sink_direct_radius);
+    std::memcpy(ax, vx.data(), nt * 8); std::memcpy(ay, vy.data(), nt * 8);
+    std::memcpy(az, vz.data(), nt * 8);
+}
+
+void ref_tree_nsink(void* p, uint32_t* nsink) {
+    const Tree& T = static_cast<RefHandle*>(p)->T;
+    if (!T.nsink.empty()) std::memcpy(nsink, T.nsink.data(), T.nnodes() * 4);
+}
+
 // Per-node centre-of-mass velocity and speed bound (nnodes each; any pointer may be null).
 void ref_tree_vel(void* p, double* vcx, double* vcy, double* vcz, float* vmax) {
     const Tree& T = static_cast<RefHandle*>(p)->T;

@@ -23,6 +23,43 @@ from oracle import Reference  # noqa: E402
 from gizmo_shared_memory_b200 import ics  # noqa: E402
 
 
+def gas_scenario(R):
+    """A Plummer sphere of gas (type 0), stars (type 4) and sinks (type 5).  Gas softenings are
+    the distance to the 32nd neighbour (the adaptive kernel's support) and zeta is of the size that
+    makes its terms a percent-level correction; stars and sinks keep a small fixed softening.
+    Every 97th particle is massless.  Returns the inputs and the reference's walks on them."""
+    from scipy.spatial import cKDTree
+
+    P = ics.plummer(n=4096, seed=42, soft=0.01)
+    rng = np.random.default_rng(5)
+    X = np.stack([P["x"], P["y"], P["z"]], 1)
+    dk, _ = cKDTree(X).query(X, k=33)
+    t = np.where(rng.uniform(size=4096) < 0.7, 0, 4).astype(np.uint8)
+    t[rng.choice(4096, 120, replace=False)] = 5
+    P["soft"] = np.where(t == 0, dk[:, -1], 0.01)
+    P["m"][::97] = 0.0
+    P["type"] = t
+    P["zeta"] = np.where(t == 0, 0.1 * (1.0 / 4096) ** 2 * P["soft"] ** 2 * rng.normal(0, 1, 4096), 0.0)
+    out = {k: P[k] for k in ("x", "y", "z", "m", "soft", "type", "zeta")}
+    T = R.build_gas(P)
+    ob = T.order()[0]
+    out["orderbuf"] = ob
+    out["nsink"] = T.nsink()
+    a0 = T.accel_grouped_gas(ob, 0.7, 1.0, 0)
+    aold = 0.005 * np.sqrt(a0[0] ** 2 + a0[1] ** 2 + a0[2] ** 2)
+    out["aold"] = aold
+    for name, theta, batch, ao, rs in (("bh", 0.7, 0, None, 0.0), ("bh_sink", 0.7, 0, None, 0.3),
+                                       ("rel_sink", 0.0, 0, aold, 0.3), ("b8_sink", 0.7, 8, None, 0.3)):
+        a = T.accel_grouped_gas(ob, theta, 1.0, batch, aold=ao, sink_radius=rs)
+        for k, v in zip(("ax", "ay", "az"), a):
+            out[f"{name}_{k}"] = v
+    sub = ob[::7].copy()
+    out["sub"] = sub
+    for k, v in zip(("ax", "ay", "az"), T.accel(sub, 0.5)):
+        out[f"acc_{k}"] = v
+    return out
+
+
 def main():
     R = Reference()
     R.set_threads(1)
@@ -130,6 +167,12 @@ def main():
     TR.set_positions(xr, yr, zr)
     rx, ry, rz = TR.accel_grouped(tg, 0.0, 1.0, 0, aold=aold)
     out["reuse_ax"], out["reuse_ay"], out["reuse_az"] = rx, ry, rz
+
+    # ---- gas, stars and sinks: the adaptive-softening zeta terms of gas-gas pairs (tree.cc:39-53)
+    #      and sink-direct opening (tree.cc:691-698, 772-778) ------------------------------------
+    G_ = gas_scenario(R)
+    for k, v in G_.items():
+        out[f"gas_{k}"] = v
 
     # ---- collocated particles: the level-20 leaf (tree.cc:89) ----------------------------------
     Q = ics.plummer(n=600, seed=7, soft=0.02)

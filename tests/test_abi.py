@@ -41,6 +41,7 @@ def test_option_defaults_match_reference_constants():
     w = _gt.WalkOptions()
     L.gt_walk_options_default(C.byref(w))
     assert w.group_mode == g.GT_GROUP_LEAF and w.mac == g.GT_MAC_PLAIN
+    assert w.sink_direct_radius == 0.0  # accel_grouped's default (tree.h:440)
 
 
 def test_null_arguments_are_rejected():

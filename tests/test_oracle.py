@@ -231,3 +231,52 @@ def test_tree_reuse_matches_golden(oracle, golden):
     T.set_positions(*RS.positions_after(P, vel, evs))
     ax, ay, az, _ = T.accel_grouped(golden["plummer_orderbuf"], 0.0, aold=golden["plummer_aold"])
     assert relerr(ax, ay, az, golden["reuse_ax"], golden["reuse_ay"], golden["reuse_az"]).max() < 1e-12
+
+
+def gas_particles(golden):
+    P = {k: golden[f"gas_{k}"] for k in ("x", "y", "z", "m", "soft")}
+    return P, golden["gas_type"], golden["gas_zeta"]
+
+
+def test_gas_and_sinks_match_golden(oracle, golden):
+    """The restatement of the adaptive-softening pair rule (zeta terms of gas-gas pairs,
+    tree.cc:39-53) and of sink-direct opening (tree.cc:691-698, 772-778) against the reference's
+    grouped walk (leaf groups, windows of 8, the relative criterion) and its per-target walk."""
+    P, ty, ze = gas_particles(golden)
+    T = oracle.build(P)
+    ob = golden["gas_orderbuf"]
+    assert np.array_equal(T.order()[0], ob)
+    assert np.array_equal(T.node_sinks(ty), golden["gas_nsink"])
+    for name, theta, batch, aold, rs in (("bh", 0.7, 0, None, 0.0), ("bh_sink", 0.7, 0, None, 0.3),
+                                         ("rel_sink", 0.0, 0, golden["gas_aold"], 0.3),
+                                         ("b8_sink", 0.7, 8, None, 0.3)):
+        st = T.groups(ob, batch)
+        ax, ay, az = T.walk_groups_gas(ob, st, theta, aold=aold, type=ty, zeta=ze, sink_radius=rs)
+        e = relerr(ax, ay, az, *(golden[f"gas_{name}_{c}"] for c in ("ax", "ay", "az")))
+        assert e.max() < 1e-12, name
+    sub = golden["gas_sub"]
+    ax, ay, az = T.walk_groups_gas(sub, np.arange(len(sub) + 1), 0.5, type=ty, zeta=ze, leaf_accept=False)
+    assert relerr(ax, ay, az, golden["gas_acc_ax"], golden["gas_acc_ay"], golden["gas_acc_az"]).max() < 1e-12
+
+
+def test_gas_terms_and_sink_rule_change_the_forces(oracle, golden):
+    """The fixtures exercise both rules: zeta moves the forces of gas particles with gas
+    neighbours inside their kernels, and the sink rule opens nodes the criterion accepted."""
+    P, ty, ze = gas_particles(golden)
+    T = oracle.build(P)
+    ob = golden["gas_orderbuf"]
+    st = T.groups(ob, 0)
+    plain = T.walk_groups_gas(ob, st, 0.7, type=ty, zeta=np.zeros_like(ze))
+    e_zeta = relerr(*plain, *(golden[f"gas_bh_{c}"] for c in ("ax", "ay", "az")))
+    assert (e_zeta > 1e-3).sum() > 100
+    # only gas targets feel zeta
+    withz = T.walk_groups_gas(ob, st, 0.7, type=ty, zeta=ze)
+    assert relerr(*withz, *plain)[ty[ob] != 0].max() == 0.0
+    e_sink = relerr(*(golden[f"gas_bh_sink_{c}"] for c in ("ax", "ay", "az")),
+                    *(golden[f"gas_bh_{c}"] for c in ("ax", "ay", "az")))
+    assert (e_sink > 1e-4).sum() > 50
+    # the kernel derivative: dW/dr at q = 0.25 and 0.75 of h, against the formula
+    h = 0.5
+    for q, fp in ((0.25, -12 * 0.25 + 18 * 0.0625), (0.75, -6 * 0.0625)):
+        assert oracle.L.or_kernel_dwdr(q * h, h) == pytest.approx(8 / (np.pi * h ** 3) * fp / h, rel=1e-14)
+    assert oracle.L.or_kernel_dwdr(h, h) == 0.0
