@@ -9,7 +9,7 @@ from . import ics  # noqa: F401
 from ._gt import (  # noqa: F401
     GT_DIRECT_FP32, GT_DIRECT_FP64, GT_GROUP_BATCH, GT_GROUP_LEAF, GT_GROUP_NODE, GT_GROUP_SINGLE,
     GT_KEY_MORTON, GT_KEY_PEANO, GT_MAC_LEARNED, GT_MAC_NODE, GT_MAC_NODE_FEATURES, GT_MAC_PLAIN,
-    GT_OUT_ORIGINAL, GT_OUT_TARGETS,
+    GT_NGB_GATHER, GT_NGB_PAIRS, GT_NGB_REVERSE, GT_OUT_ORIGINAL, GT_OUT_TARGETS,
     Context, GTError, Tree, load_library,
 )
 

@@ -24,6 +24,8 @@ GT_MAC_PLAIN, GT_MAC_LEARNED, GT_MAC_NODE = 0, 1, 2
 GT_MAC_NODE_FEATURES = (1 << 1) | (1 << 2) | (1 << 5)
 GT_DIRECT_FP64, GT_DIRECT_FP32 = 0, 1
 GT_OUT_TARGETS, GT_OUT_ORIGINAL = 0, 1
+GT_NGB_GATHER, GT_NGB_REVERSE, GT_NGB_PAIRS = 0, 1, 2
+GT_EVENT_HMAX = 6
 
 STATUS = {0: "GT_OK", 1: "GT_ERR_INVALID", 2: "GT_ERR_CUDA", 3: "GT_ERR_NOMEM",
           4: "GT_ERR_UNSUPPORTED", 5: "GT_ERR_OVERFLOW", 6: "GT_ERR_TIMEOUT",
@@ -41,6 +43,7 @@ EXPORTS = [
     "gt_plan_create", "gt_plan_launch", "gt_plan_destroy", "gt_tune_options_default", "gt_autotune",
     "gt_accel_grouped_ext", "gt_tree_velocities", "gt_tree_velocity_moments", "gt_tree_events",
     "gt_tree_refresh", "gt_tree_node_state", "gt_tree_particles", "gt_tree_gas",
+    "gt_ngb_options_default", "gt_tree_hmax", "gt_ngb_search", "gt_density_options_default", "gt_density",
 ]
 
 
@@ -76,6 +79,17 @@ class TuneOptions(C.Structure):
                 ("sample", C.c_void_p), ("ref_ax", C.c_void_p), ("ref_ay", C.c_void_p),
                 ("ref_az", C.c_void_p), ("mac_model", C.c_void_p), ("n_kappa", C.c_int),
                 ("kappa", C.c_void_p), ("mac_band", C.c_double * 2), ("mac_mode", C.c_int)]
+
+
+class NgbOptions(C.Structure):
+    _fields_ = [("mode", C.c_int), ("box", C.c_double), ("elapsed", C.c_double), ("n_gas", C.c_int64),
+                ("h", C.c_void_p)]
+
+
+class DensityOptions(C.Structure):
+    _fields_ = [("des_ngb", C.c_double), ("ngb_tol", C.c_double), ("box", C.c_double), ("elapsed", C.c_double),
+                ("n_dims", C.c_int), ("face_correction", C.c_int), ("h_start", C.c_void_p),
+                ("cond_prev", C.c_void_p)]
 
 
 class MacTrainOptions(C.Structure):
@@ -151,6 +165,13 @@ def load_library(path: str = LIB_PATH):
     L.gt_tree_node_state.argtypes = [vp, vp, d, vp, vp, vp, vp, vp]
     L.gt_tree_particles.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int]
     L.gt_tree_gas.argtypes = [vp, vp, vp, vp, C.c_int]
+    L.gt_ngb_options_default.restype = None
+    L.gt_ngb_options_default.argtypes = [vp]
+    L.gt_tree_hmax.argtypes = [vp, vp, vp, C.c_int64, C.c_int]
+    L.gt_ngb_search.argtypes = [vp, vp, C.c_int64, vp, vp, vp, vp, vp, C.c_int, vp, vp, C.c_int64, vp]
+    L.gt_density_options_default.restype = None
+    L.gt_density_options_default.argtypes = [vp]
+    L.gt_density.argtypes = [vp, vp, C.c_int64, vp, vp, C.c_int, vp, vp, vp, vp]
     L.gt_potential.argtypes = [vp, vp, i64, vp, d, d, vp, C.c_int, vp]
     L.gt_walk_stats_get.argtypes = [vp, C.POINTER(WalkStats)]
     L.gt_form_aold.argtypes = [vp, i64, vp, vp, vp, d, d, C.c_int, vp]
@@ -591,6 +612,54 @@ class Context:
             zeta = None if zeta is None else np.ascontiguousarray(zeta, np.float64)
         self._check(load_library().gt_tree_gas(self.h, tree.h, _ptr(type), _ptr(zeta),
                                                GT_MEM_DEVICE if dev else GT_MEM_HOST))
+
+    # ---- neighbour search and the density solve ------------------------------------------------
+    def tree_hmax(self, tree: Tree, h, n_gas):
+        """Tree::init_hmax: per-node largest support radius of the gas particles [0, n_gas)."""
+        dev = _is_dev(h)
+        if not dev:
+            h = np.ascontiguousarray(h, np.float64)
+        self._check(load_library().gt_tree_hmax(self.h, tree.h, _ptr(h), int(n_gas),
+                                                GT_MEM_DEVICE if dev else GT_MEM_HOST))
+
+    def ngb_search(self, tree: Tree, cx, cy, cz, radius, mode=GT_NGB_GATHER, h=None, n_gas=0, box=0.0,
+                   elapsed=0.0):
+        """Neighbour lists as CSR (start [n+1] int64, found uint32 particle indices), host arrays."""
+        cx, cy, cz, radius = (np.ascontiguousarray(a, np.float64) for a in (cx, cy, cz, radius))
+        o = NgbOptions()
+        L = load_library()
+        L.gt_ngb_options_default(C.byref(o))
+        o.mode, o.box, o.elapsed, o.n_gas = mode, box, elapsed, int(n_gas)
+        hh = None if h is None else np.ascontiguousarray(h, np.float64)
+        o.h = _ptr(hh)
+        n = len(cx)
+        start = np.zeros(n + 1, np.int64)
+        tot = C.c_int64(0)
+        self._check(L.gt_ngb_search(self.h, tree.h, n, _ptr(cx), _ptr(cy), _ptr(cz), _ptr(radius), C.byref(o),
+                                    GT_MEM_HOST, _ptr(start), None, 0, C.byref(tot)))
+        found = np.zeros(max(tot.value, 1), np.uint32)
+        self._check(L.gt_ngb_search(self.h, tree.h, n, _ptr(cx), _ptr(cy), _ptr(cz), _ptr(radius), C.byref(o),
+                                    GT_MEM_HOST, _ptr(start), _ptr(found), len(found), C.byref(tot)))
+        return start, found[: tot.value]
+
+    def density(self, tree: Tree, targets, des_ngb=32.0, ngb_tol=0.05, h_start=None, box=0.0, n_dims=3,
+                cond_prev=None, face_correction=True, elapsed=0.0):
+        """shmem::density on the GPU: dict of h, rho, nngb, iters per target (host arrays)."""
+        t = np.ascontiguousarray(targets, np.uint32)
+        nt = len(t)
+        o = DensityOptions()
+        L = load_library()
+        L.gt_density_options_default(C.byref(o))
+        o.des_ngb, o.ngb_tol, o.box, o.n_dims = des_ngb, ngb_tol, box, n_dims
+        o.face_correction, o.elapsed = int(face_correction), elapsed
+        hs = None if h_start is None else np.ascontiguousarray(h_start, np.float64)
+        cp = None if cond_prev is None else np.ascontiguousarray(cond_prev, np.float64)
+        o.h_start, o.cond_prev = _ptr(hs), _ptr(cp)
+        h, rho = np.zeros(nt), np.zeros(nt)
+        nngb, iters = np.zeros(nt, np.int32), np.zeros(nt, np.int32)
+        self._check(L.gt_density(self.h, tree.h, nt, _ptr(t), C.byref(o), GT_MEM_HOST, _ptr(h), _ptr(rho),
+                                 _ptr(nngb), _ptr(iters)))
+        return {"h": h, "rho": rho, "nngb": nngb, "iters": iters}
 
     def velocity_moments(self, tree: Tree):
         nn = tree.info()["n_nodes"]

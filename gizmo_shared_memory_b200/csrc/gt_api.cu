@@ -123,7 +123,8 @@ void free_tree_arrays(gt_tree* t) {
     void* ptrs[] = {t->src, t->ssoft, t->smass, t->order, t->rank, t->leaf_of, t->sleaf, t->skey,
                     t->nodes, t->parent, t->next, t->level, t->size, t->delta, t->nsoft, t->gc,
                     t->nq2, t->sys_off_dev, t->geom_dev, t->svel, t->nvel, t->vcom, t->vmax,
-                    t->m0, t->c0, t->dp, t->dq, t->dmass, t->xpad, t->stype, t->szeta, t->nsink};
+                    t->m0, t->c0, t->dp, t->dq, t->dmass, t->xpad, t->stype, t->szeta, t->nsink,
+                    t->snode, t->hmax};
     // tree arrays came from the stream-ordered pool: hand them back to it (callers have synchronised)
     for (void* p : ptrs)
         if (p) cudaFreeAsync(p, 0);
@@ -692,7 +693,7 @@ int gt_tree_events(gt_context* ctx, gt_tree* tree, int kind, int64_t n, const in
         check_mem(mem);
         if (!tree || n < 0) throw Fail{GT_ERR_INVALID, "null tree or negative count"};
         if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "tree and context are on different devices"};
-        if (kind < GT_EVENT_KICK || kind > GT_EVENT_PAD) throw Fail{GT_ERR_INVALID, "unknown event kind"};
+        if (kind < GT_EVENT_KICK || kind > GT_EVENT_HMAX) throw Fail{GT_ERR_INVALID, "unknown event kind"};
         if (n == 0) return;
         const bool need_a = kind != GT_EVENT_VMAX, need_x = kind == GT_EVENT_SHIFT || kind == GT_EVENT_MASS;
         if (!leaf || (need_a && !a) || (need_x && !x) || (kind == GT_EVENT_MASS && !v) ||
@@ -707,8 +708,122 @@ int gt_tree_events(gt_context* ctx, gt_tree* tree, int kind, int64_t n, const in
         const double* dx = need_x ? stage_in(ctx, kSlotIn2, x, 3 * n, mem) : nullptr;
         const double* dv = kind == GT_EVENT_MASS ? stage_in(ctx, kSlotIn3, v, 3 * n, mem) : nullptr;
         const float* df = kind == GT_EVENT_VMAX ? stage_in(ctx, kSlotIn4, f, n, mem) : nullptr;
-        reuse_events(ctx, tree, kind, n, dl, da, dx, dv, df, tau, box);
+        if (kind == GT_EVENT_HMAX) raise_hmax(ctx, tree, n, dl, da);
+        else reuse_events(ctx, tree, kind, n, dl, da, dx, dv, df, tau, box);
         finish(ctx, mem == GT_MEM_HOST);
+    });
+}
+
+void gt_ngb_options_default(gt_ngb_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->mode = GT_NGB_GATHER;
+}
+
+void gt_density_options_default(gt_density_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->des_ngb = 32.0;
+    o->ngb_tol = 0.05;
+    o->n_dims = 3;
+    o->face_correction = 1;
+}
+
+int gt_tree_hmax(gt_context* ctx, gt_tree* tree, const double* h, int64_t n_gas, int mem) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (!tree || n_gas < 0 || (n_gas > 0 && !h)) throw Fail{GT_ERR_INVALID, "null tree or h, or n_gas < 0"};
+        if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "tree and context are on different devices"};
+        DeviceGuard dg(ctx->device);
+        const int64_t n = std::min<int64_t>(n_gas, tree->n);
+        tree_hmax(ctx, tree, stage_in(ctx, kSlotIn0, h, n, mem), n);
+        finish(ctx, true);
+    });
+}
+
+int gt_ngb_search(gt_context* ctx, const gt_tree* tc, int64_t n, const double* cx, const double* cy,
+                  const double* cz, const double* radius, const gt_ngb_options* opt, int mem, int64_t* start,
+                  uint32_t* found, int64_t capacity, int64_t* total) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        gt_tree* tree = const_cast<gt_tree*>(tc);  // search nodes are made on first use
+        if (!tree || n < 0 || !start) throw Fail{GT_ERR_INVALID, "null tree or start, or n < 0"};
+        if (n > 0 && (!cx || !cy || !cz || !radius)) throw Fail{GT_ERR_INVALID, "null centre or radius"};
+        if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "tree and context are on different devices"};
+        gt_ngb_options o;
+        gt_ngb_options_default(&o);
+        if (opt) o = *opt;
+        if (o.mode < GT_NGB_GATHER || o.mode > GT_NGB_PAIRS) throw Fail{GT_ERR_INVALID, "unknown search mode"};
+        if (o.mode != GT_NGB_GATHER && o.n_gas > 0 && !o.h) throw Fail{GT_ERR_INVALID, "the reverse search needs h"};
+        if (!(o.box >= 0.0) || !(o.elapsed >= 0.0)) throw Fail{GT_ERR_INVALID, "box and elapsed must be >= 0"};
+        if (capacity < 0) throw Fail{GT_ERR_INVALID, "capacity < 0"};
+        DeviceGuard dg(ctx->device);
+        if (total) *total = 0;
+        if (n == 0) {
+            start[0] = 0;  // host or device: one int64
+            if (mem == GT_MEM_DEVICE) check_cuda(cudaMemsetAsync(start, 0, 8, ctx->stream), "memset");
+            finish(ctx, true);
+            return;
+        }
+        const double* dx = stage_in(ctx, kSlotIn0, cx, n, mem);
+        const double* dy = stage_in(ctx, kSlotIn1, cy, n, mem);
+        const double* dz = stage_in(ctx, kSlotIn2, cz, n, mem);
+        const double* dr = stage_in(ctx, kSlotIn3, radius, n, mem);
+        const int64_t ng = o.mode == GT_NGB_GATHER ? 0 : std::min<int64_t>(o.n_gas, tree->n);
+        const double* dh = stage_in(ctx, kSlotIn4, o.h, ng, mem);
+        int64_t* ds = out_buf(ctx, kSlotOut0, start, n + 1, mem);
+        // the host path sizes the device list from the count pass: capacity 0 in the call below
+        // means "count only", the lists follow once the total is known
+        uint32_t* df = mem == GT_MEM_DEVICE ? found : nullptr;
+        const int64_t tot = run_ngb(ctx, tree, n, dx, dy, dz, dr, o.mode, dh, ng, o.box, o.elapsed, ds, df,
+                                    mem == GT_MEM_DEVICE ? capacity : 0);
+        if (total) *total = tot;
+        copy_out(ctx, start, ds, n + 1, mem);
+        if (mem == GT_MEM_HOST && found && tot <= capacity && tot > 0) {
+            uint32_t* hf = (uint32_t*)scratch(ctx, kSlotOut1, (size_t)tot * 4);
+            run_ngb(ctx, tree, n, dx, dy, dz, dr, o.mode, dh, ng, o.box, o.elapsed, ds, hf, tot);
+            copy_out(ctx, found, hf, tot, mem);
+        }
+        finish(ctx, true);
+        if (found && tot > capacity) throw Fail{GT_ERR_OVERFLOW, "the neighbour lists need more room than capacity"};
+    });
+}
+
+int gt_density(gt_context* ctx, const gt_tree* tc, int64_t nt, const uint32_t* targets,
+               const gt_density_options* opt, int mem, double* h, double* rho, int32_t* nngb, int32_t* iters) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        gt_tree* tree = const_cast<gt_tree*>(tc);
+        if (!tree || nt < 0 || (nt > 0 && !targets)) throw Fail{GT_ERR_INVALID, "null tree or targets, or nt < 0"};
+        if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "tree and context are on different devices"};
+        gt_density_options o;
+        gt_density_options_default(&o);
+        if (opt) o = *opt;
+        if (o.n_dims < 1 || o.n_dims > 3) throw Fail{GT_ERR_INVALID, "n_dims must be 1, 2 or 3"};
+        if (!(o.des_ngb > 0.0) || !(o.ngb_tol > 0.0)) throw Fail{GT_ERR_INVALID, "des_ngb and ngb_tol must be > 0"};
+        if (!(o.box >= 0.0) || !(o.elapsed >= 0.0)) throw Fail{GT_ERR_INVALID, "box and elapsed must be >= 0"};
+        if (mem == GT_MEM_HOST)
+            for (int64_t k = 0; k < nt; ++k)
+                if ((int64_t)targets[k] >= tree->n) throw Fail{GT_ERR_INVALID, "target index out of range"};
+        DeviceGuard dg(ctx->device);
+        if (nt == 0) return;
+        const uint32_t* dt = stage_in(ctx, kSlotIn0, targets, nt, mem);
+        const double* dhs = stage_in(ctx, kSlotIn1, o.h_start, nt, mem);
+        const double* dcp = stage_in(ctx, kSlotIn2, o.cond_prev, tree->n, mem);
+        double* dh = (double*)(mem == GT_MEM_DEVICE && h ? (void*)h : scratch(ctx, kSlotOut0, (size_t)nt * 8));
+        double* dr = (double*)(mem == GT_MEM_DEVICE && rho ? (void*)rho : scratch(ctx, kSlotOut1, (size_t)nt * 8));
+        int* dn = (int*)(mem == GT_MEM_DEVICE && nngb ? (void*)nngb : scratch(ctx, kSlotOut2, (size_t)nt * 4));
+        int* di = (int*)(mem == GT_MEM_DEVICE && iters ? (void*)iters : scratch(ctx, kSlotOut3, (size_t)nt * 4));
+        run_density(ctx, tree, nt, dt, o.des_ngb, o.ngb_tol, dhs, o.box, o.n_dims, dcp, o.face_correction != 0,
+                    o.elapsed, dh, dr, dn, di);
+        copy_out(ctx, h, dh, nt, mem);
+        copy_out(ctx, rho, dr, nt, mem);
+        copy_out(ctx, nngb, (int32_t*)dn, nt, mem);
+        copy_out(ctx, iters, (int32_t*)di, nt, mem);
+        finish(ctx, true);
     });
 }
 

@@ -42,6 +42,15 @@ struct alignas(16) SrcP {
 };
 static_assert(sizeof(SrcP) == 32, "SrcP must be 32 bytes");
 
+// Search node of the neighbour search, 32 bytes: float geometric centre and conservative half side
+// (the reference's SNode, shmem/tree.h:206-226), first child / next in the reference's threading,
+// particle range.
+struct alignas(16) SNodeG {
+    float cx, cy, cz, half;
+    int first, next, plo, phi;
+};
+static_assert(sizeof(SNodeG) == 32, "SNodeG must be 32 bytes");
+
 // Root cell geometry computed on the device (bbox -> centre, side, scale).
 struct RootGeom {
     double cx, cy, cz, side, scale;
@@ -138,6 +147,10 @@ struct gt_tree {
     double* szeta = nullptr;     // n
     uint32_t* nsink = nullptr;   // n_nodes
     bool gas_zeta = false;
+    // neighbour search (gt_ngb_search, gt_density): search nodes made on first use, and the
+    // per-node largest gas support radius of the reverse search (gt_tree_hmax)
+    gt::SNodeG* snode = nullptr; // n_nodes
+    float* hmax = nullptr;       // n_nodes
     // cached all-active group lists, keyed by (mode, param)
     struct GroupCache {
         int mode = -1, param = 0, kmax = 0;
@@ -159,6 +172,7 @@ enum Slot {
     kSlotTargets, kSlotAold, kSlotGroupKey, kSlotGroupsA, kSlotGroupsB,
     kSlotOut0, kSlotOut1, kSlotOut2, kSlotOut3, kSlotOut4, kSlotOut5,
     kSlotStack, kSlotCounters, kSlotDirect, kSlotGroupRoot, kSlotMacL2,
+    kSlotNgb0, kSlotNgb1, kSlotNgb2,
     kSlotCount
 };
 
@@ -281,6 +295,18 @@ void tree_velocities(gt_context* ctx, gt_tree* t, const double* vx, const double
 // Particle types (null: every particle gas) and zeta (null: none), device arrays over the tree's
 // input particles, gathered into tree order; the per-node sink count (gt_tree_gas).
 void tree_gas(gt_context* ctx, gt_tree* t, const uint8_t* type, const double* zeta);
+// Neighbour search and the density solve (gt_ngb.cu); array arguments are device pointers.
+void ensure_snodes(gt_context* ctx, gt_tree* t);
+void tree_hmax(gt_context* ctx, gt_tree* t, const double* h, int64_t n_gas);
+void raise_hmax(gt_context* ctx, gt_tree* t, int64_t n, const int* leaf, const double* h);
+// Counts into start (n+1, exclusive prefix sums) and, when found is given and the total fits
+// capacity, the lists; returns the total.
+int64_t run_ngb(gt_context* ctx, gt_tree* t, int64_t n, const double* cx, const double* cy, const double* cz,
+                const double* radius, int mode, const double* h, int64_t n_gas, double box, double elapsed,
+                int64_t* start, uint32_t* found, int64_t capacity);
+void run_density(gt_context* ctx, gt_tree* t, int64_t nt, const uint32_t* targets, double des_ngb, double ngb_tol,
+                 const double* h_start, double box, int n_dims, const double* cond_prev, int face_corr,
+                 double elapsed, double* h, double* rho, int* nngb, int* iters);
 void run_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay,
                    const double* az, double alpha, double G, double* aold);
 

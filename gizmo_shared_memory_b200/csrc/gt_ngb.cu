@@ -1,0 +1,505 @@
+// Neighbour search and the density solve on the gravity tree: shmem::ngb_search,
+// ngb_search_reverse and density (shmem/hydro.h:65-117, hydro.cc:37-327), with the per-node hmax
+// of Tree::init_hmax / raise_hmax (tree.cc:287-338).
+//
+// The search prunes against each node's BOX, not its centre of mass: a 32-byte search node holds
+// the float geometric centre and a conservative half side (the build's half side plus 1e-6 of the
+// root side plus four float ulps of the largest centre coordinate, tree.cc:490-505), with the
+// reference's threading (first child / next).  One thread follows the threading for one centre,
+// as the reference's loop does, so every list comes out in tree order -- the reference's order --
+// and the density sums accumulate in the reference's order too.  Neighbouring centres (tree-ordered
+// targets) follow nearly the same path, so a warp's threads mostly read the same nodes.
+//
+// Lists are CSR: a counting pass, an exclusive scan, and a filling pass over the same traversal.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "gt_internal.cuh"
+
+namespace gt {
+namespace {
+
+constexpr int kBlk = 128;
+
+int grid_of(gt_context* ctx, int64_t n) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + kBlk - 1) / kBlk, (int64_t)ctx->num_sms * 16));
+}
+
+__device__ __forceinline__ double min_image(double s, double box) {
+    if (box > 0) {
+        if (s > 0.5 * box) s -= box;
+        else if (s < -0.5 * box) s += box;
+    }
+    return s;
+}
+
+__device__ __forceinline__ float up_float(double h) {  // rounded up to float (tree.cc:288-291)
+    const float f = (float)h;
+    return (double)f < h ? nextafterf(f, 1e30f) : f;
+}
+
+__global__ void pack_snode_kernel(const GNode* __restrict__ nodes, const int* __restrict__ next,
+                                  const double* __restrict__ gc, const double* __restrict__ size, int64_t nn,
+                                  double eps, SNodeG* __restrict__ sn) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (int64_t)gridDim.x * blockDim.x) {
+        const double x = gc[3 * i], y = gc[3 * i + 1], z = gc[3 * i + 2];
+        const double cm = fmax(fabs(x), fmax(fabs(y), fabs(z)));
+        SNodeG s;
+        s.cx = (float)x; s.cy = (float)y; s.cz = (float)z;
+        s.half = (float)(0.5 * size[i] + eps + 4.0 * (double)FLT_EPSILON * cm);
+        s.first = nodes[i].first;
+        s.next = next[i];
+        s.plo = nodes[i].plo;
+        s.phi = nodes[i].phi;
+        sn[i] = s;
+    }
+}
+
+// Tree::init_hmax: every gas particle i < n_gas with h > 0 raises its leaf and ancestors to h
+// rounded up to float; the climb stops at the first ancestor already covering it.  A float max
+// through its bit pattern (non-negative), so the result does not depend on the order.
+__global__ void hmax_kernel(const double* __restrict__ h, const int* __restrict__ leaf, int64_t n,
+                            const int* __restrict__ parent, bool by_particle, float* __restrict__ hmax) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double hi = h[i];
+        const int lf = leaf[i];
+        if ((by_particle && !(hi > 0)) || lf < 0) continue;
+        const unsigned int want = __float_as_uint(up_float(hi));
+        for (int no = lf; no >= 0; no = parent[no]) {
+            unsigned int* slot = reinterpret_cast<unsigned int*>(hmax + no);
+            if (*reinterpret_cast<volatile unsigned int*>(slot) >= want) break;
+            atomicMax(slot, want);
+        }
+    }
+}
+
+struct SearchGeom {
+    int root;            // 0, or -1 for a tree without nodes
+    const SNodeG* sn;
+    const SrcP* src;
+    const uint32_t* order;
+    const float* xpad;   // null: 0
+    const float* vmax;   // null: 0
+    const float* hmax;   // reverse search
+    double elapsed, box;
+};
+
+// One traversal for one centre in the reference's node order.  REVERSE: gas particles j < n_gas
+// with radius <= r < h[j] (ngb_search_reverse); otherwise r < radius (ngb_search).  emit(j, s)
+// receives the particle index and its tree position.
+template <bool REVERSE, typename F>
+__device__ __forceinline__ void search(const SearchGeom& g, double px, double py, double pz, double radius,
+                                       const double* __restrict__ h, int64_t n_gas, F&& emit) {
+    const double r2max = radius * radius;
+    int node = g.root;
+    while (node >= 0) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(g.sn + node));
+        const int4 b = __ldg(reinterpret_cast<const int4*>(g.sn + node) + 1);
+        const double half = (double)a.w;
+        double dist;
+        if (REVERSE) {
+            const double hm = (double)__ldg(g.hmax + node);
+            if (hm <= radius) { node = b.y; continue; }
+            dist = hm + half;
+        } else {
+            dist = radius + half;
+        }
+        if (g.xpad) dist += (double)__ldg(g.xpad + node);
+        if (g.elapsed > 0 && g.vmax) dist += (double)__ldg(g.vmax + node) * g.elapsed;
+        const double dx = min_image((double)a.x - px, g.box);
+        if (dx > dist || -dx > dist) { node = b.y; continue; }
+        const double dy = min_image((double)a.y - py, g.box);
+        if (dy > dist || -dy > dist) { node = b.y; continue; }
+        const double dz = min_image((double)a.z - pz, g.box);
+        if (dz > dist || -dz > dist) { node = b.y; continue; }
+        dist += 0.7320508075688772 * half;
+        if (dx * dx + dy * dy + dz * dz > dist * dist) { node = b.y; continue; }
+        if (b.x < 0) {
+            for (int s = b.z; s < b.w; ++s) {
+                const uint32_t j = __ldg(g.order + s);
+                if (REVERSE && (int64_t)j >= n_gas) continue;
+                const double2 xy = __ldg(reinterpret_cast<const double2*>(g.src + s));
+                const double zz = __ldg(reinterpret_cast<const double*>(g.src + s) + 2);
+                const double ox = min_image(xy.x - px, g.box), oy = min_image(xy.y - py, g.box),
+                             oz = min_image(zz - pz, g.box);
+                // |d|^2 as x*x + y*y + z*z without contraction (Vec3d::norm_sq)
+                const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)), __dmul_rn(oz, oz));
+                bool keep;
+                if (REVERSE) {
+                    const double hj = __ldg(h + j);
+                    keep = r2 >= r2max && r2 < hj * hj;
+                } else {
+                    keep = r2 < r2max;
+                }
+                if (keep) emit(j, s);
+            }
+            node = b.y;
+        } else {
+            node = b.x;
+        }
+    }
+}
+
+struct NgbArgs {
+    SearchGeom g;
+    const double *cx, *cy, *cz, *radius;
+    int64_t n;
+    int mode;
+    const double* h;
+    int64_t n_gas;
+    uint32_t* count;              // counting pass
+    unsigned long long* total;    // counting pass: sum of the counts
+    const int64_t* start;         // filling pass
+    uint32_t* found;
+};
+
+template <bool FILL>
+__global__ void __launch_bounds__(kBlk) ngb_kernel(const NgbArgs a) {
+    unsigned long long mine = 0;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.n; c += (int64_t)gridDim.x * blockDim.x) {
+        const double px = a.cx[c], py = a.cy[c], pz = a.cz[c], r = a.radius[c];
+        int64_t k = FILL ? a.start[c] : 0;
+        auto emit = [&](uint32_t j, int) {
+            if (FILL) a.found[k] = j;
+            ++k;
+        };
+        if (a.mode != GT_NGB_REVERSE) search<false>(a.g, px, py, pz, r, nullptr, 0, emit);
+        if (a.mode != GT_NGB_GATHER) search<true>(a.g, px, py, pz, r, a.h, a.n_gas, emit);
+        if (!FILL) {
+            a.count[c] = (uint32_t)k;
+            mine += (unsigned long long)k;
+        }
+    }
+    if (!FILL) {
+        for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+        if ((threadIdx.x & 31) == 0 && mine) atomicAdd(a.total, mine);
+    }
+}
+
+__global__ void widen_kernel(const uint32_t* __restrict__ ex, const uint32_t* __restrict__ cnt, int64_t n,
+                             int64_t* __restrict__ start) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        start[i] = (int64_t)ex[i];
+        if (i == n - 1) start[n] = (int64_t)ex[i] + (int64_t)cnt[i];
+    }
+}
+
+// ---- the density solve ------------------------------------------------------------------------
+// The cubic spline of support h in n_dims dimensions (shmem/hydro.h:25-63).
+__device__ __forceinline__ double kernel_norm(double h, int dim) {
+    if (dim == 1) return (4.0 / 3.0) / h;
+    if (dim == 2) return 40.0 / (7.0 * M_PI * h * h);
+    return 8.0 / (M_PI * h * h * h);
+}
+__device__ __forceinline__ double ball_vol(double h, int dim) {
+    if (dim == 1) return 2.0 * h;
+    if (dim == 2) return M_PI * h * h;
+    return 4.0 * M_PI / 3.0 * h * h * h;
+}
+
+struct DensSums {
+    double wsum, dwdh, rho, mom[6], face[3];
+    int inside;
+};
+
+struct DensArgs {
+    SearchGeom g;
+    const double* smass;
+    const uint8_t* stype;  // tree order; null: every particle gas
+    const uint32_t* rank;
+    const uint32_t* targets;
+    int64_t nt;
+    double des_ngb, ngb_tol, h_default;
+    const double* h_start;
+    const double* cond_prev;  // per particle index
+    int n_dims, face_corr;
+    double *h, *rho;
+    int *nngb, *iters;
+};
+
+// One evaluation at h: the sums over the GAS neighbours inside h, in tree order (hydro.cc:205-222).
+__device__ void dens_eval(const DensArgs& a, double px, double py, double pz, double h, DensSums& s) {
+    s.wsum = s.dwdh = s.rho = 0.0;
+    for (int c = 0; c < 6; ++c) s.mom[c] = 0.0;
+    s.face[0] = s.face[1] = s.face[2] = 0.0;
+    s.inside = 0;
+    const int dim = a.n_dims;
+    const double norm = kernel_norm(h, dim);
+    search<false>(a.g, px, py, pz, h, nullptr, 0, [&](uint32_t, int sp) {
+        if (a.stype && __ldg(a.stype + sp) != 0) return;
+        const double2 xy = __ldg(reinterpret_cast<const double2*>(a.g.src + sp));
+        const double zz = __ldg(reinterpret_cast<const double*>(a.g.src + sp) + 2);
+        const double dx = min_image(xy.x - px, a.g.box), dy = min_image(xy.y - py, a.g.box),
+                     dz = min_image(zz - pz, a.g.box);
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double q = r / h;
+        double w = 0.0, dh = 0.0;
+        if (q < 1.0) {
+            double f, fp;
+            if (q < 0.5) {
+                f = 1.0 - 6.0 * q * q + 6.0 * q * q * q;
+                fp = -12.0 * q + 18.0 * q * q;
+            } else {
+                const double u = 1.0 - q;
+                f = 2.0 * u * u * u;
+                fp = -6.0 * u * u;
+            }
+            w = norm * f;
+            dh = -((double)dim / h) * norm * f - (q / h) * norm * fp;
+        }
+        s.wsum += w;
+        s.dwdh += dh;
+        s.rho += __ldg(a.smass + sp) * w;
+        s.mom[0] += dx * dx * w; s.mom[1] += dy * dy * w; s.mom[2] += dz * dz * w;
+        s.mom[3] += dx * dy * w; s.mom[4] += dy * dz * w; s.mom[5] += dx * dz * w;
+        s.face[0] += dx * w; s.face[1] += dy * w; s.face[2] += dz * w;
+        if (r < h) ++s.inside;
+    });
+}
+
+// Rank-d inverse of the symmetric moments (xx yy zz xy yz xz), row-major, zero when degenerate
+// (shmem/vec.h:43-66; 3-D: cofactors over the determinant).
+__device__ bool invert_moments(const double* m, double* B, int n_dims) {
+    for (int i = 0; i < 9; ++i) B[i] = 0.0;
+    if (n_dims == 1) {
+        if (fabs(m[0]) < 1e-300) return false;
+        B[0] = 1.0 / m[0];
+        return true;
+    }
+    if (n_dims == 2) {
+        const double det = m[0] * m[1] - m[3] * m[3];
+        if (fabs(det) < 1e-300) return false;
+        B[0] = m[1] / det; B[1] = -m[3] / det;
+        B[3] = -m[3] / det; B[4] = m[0] / det;
+        return true;
+    }
+    const double a00 = m[0], a01 = m[3], a02 = m[5], a11 = m[1], a12 = m[4], a22 = m[2];
+    const double a10 = a01, a20 = a02, a21 = a12;
+    const double d = a00 * (a11 * a22 - a12 * a21) - a01 * (a10 * a22 - a12 * a20) + a02 * (a10 * a21 - a11 * a20);
+    if (d == 0.0 || d != d) return false;
+    const double id = 1.0 / d;
+    B[0] = (a11 * a22 - a12 * a21) * id; B[1] = (a02 * a21 - a01 * a22) * id; B[2] = (a01 * a12 - a02 * a11) * id;
+    B[3] = (a12 * a20 - a10 * a22) * id; B[4] = (a00 * a22 - a02 * a20) * id; B[5] = (a02 * a10 - a00 * a12) * id;
+    B[6] = (a10 * a21 - a11 * a20) * id; B[7] = (a01 * a20 - a00 * a21) * id; B[8] = (a00 * a11 - a01 * a10) * id;
+    return true;
+}
+
+// One thread per target: bisection-guarded Newton on N_eff(h) = des_ngb with the face-closure and
+// condition-number corrections and the growing tolerance (hydro.cc:189-297).
+__global__ void __launch_bounds__(kBlk) density_kernel(const DensArgs a) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.nt; t += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = a.targets[t];
+        const uint32_t sp = a.rank[p];
+        const double px = a.g.src[sp].x, py = a.g.src[sp].y, pz = a.g.src[sp].z;
+        const int dim = a.n_dims;
+        double h = a.h_start ? a.h_start[t] : a.h_default, h_lo = 0.0, h_hi = 0.0;
+        int iter = 0;
+        bool converged = false;
+        DensSums s;
+        for (; iter < 100; ++iter) {
+            dens_eval(a, px, py, pz, h, s);
+            const double n_eff = ball_vol(h, dim) * s.wsum;
+            double ncorr = 1.0;
+            if (a.cond_prev) {
+                const double cn = a.cond_prev[p];
+                if (cn > 100.0) ncorr = fmin(sqrt(1.0 + (cn - 100.0) / 1000.0), 2.0);
+            }
+            double des_eff = a.des_ngb * ncorr, tol_eff = a.ngb_tol * ncorr;
+            if (a.face_corr && s.wsum > 0) {
+                double B[9];
+                if (invert_moments(s.mom, B, dim)) {
+                    const double vol = 1.0 / s.wsum;
+                    const double dx_i = sqrt(vol * (s.mom[0] + s.mom[1] + s.mom[2]));
+                    double sum_abs = 0.0;
+                    for (int r = 0; r < 3; ++r) {
+                        const double leak =
+                            (B[3 * r] * s.face[0] + B[3 * r + 1] * s.face[1] + B[3 * r + 2] * s.face[2]) * (2.0 * vol);
+                        sum_abs += fabs(leak) / dim;
+                    }
+                    const double denom = 2.0 * dim * pow(dx_i, dim - 1);
+                    if (denom > 0) {
+                        const double fce = sum_abs / denom;
+                        if (fce > 0.35) ncorr = fmax(ncorr, fmin(fce / 0.35, 2.0));
+                        des_eff = a.des_ngb * ncorr;
+                        tol_eff = a.ngb_tol * ncorr;
+                    }
+                }
+            }
+            if (iter > 1) tol_eff = fmin(0.25 * des_eff, tol_eff * exp(0.1 * log(des_eff / (16.0 * tol_eff)) * iter));
+            const double res = n_eff - des_eff;
+            if (fabs(res) < tol_eff) { converged = true; break; }
+            if (res > 0) h_hi = h; else h_lo = h;
+            const double dn = ball_vol(h, dim) * ((double)dim / h * s.wsum + s.dwdh);
+            double hn = dn > 0 ? h - res / dn : 0.0;
+            if (hn <= h_lo || (h_hi > 0 && hn >= h_hi) || hn <= 0) {
+                if (h_hi > 0) hn = h_lo > 0 ? sqrt(h_lo * h_hi) : 0.5 * h_hi;
+                else hn = h * (res > 0 ? 0.7 : 1.6);
+            }
+            h = hn;
+        }
+        if (!converged) dens_eval(a, px, py, pz, h, s);  // rho of the final h (hydro.cc:281-293)
+        a.h[t] = h;
+        a.rho[t] = s.rho;
+        a.nngb[t] = s.inside;
+        a.iters[t] = iter;
+    }
+}
+
+// bounding box of every particle (massless too), for the density solve's default h
+__global__ void bbox_all_kernel(const SrcP* __restrict__ src, int64_t n, double* __restrict__ part) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v[3] = {src[i].x, src[i].y, src[i].z};
+        for (int k = 0; k < 3; ++k) { lo[k] = fmin(lo[k], v[k]); hi[k] = fmax(hi[k], v[k]); }
+    }
+    __shared__ double sh[6][kBlk];
+    for (int k = 0; k < 3; ++k) { sh[k][threadIdx.x] = lo[k]; sh[3 + k][threadIdx.x] = hi[k]; }
+    __syncthreads();
+    for (int o = kBlk / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o)
+            for (int k = 0; k < 3; ++k) {
+                sh[k][threadIdx.x] = fmin(sh[k][threadIdx.x], sh[k][threadIdx.x + o]);
+                sh[3 + k][threadIdx.x] = fmax(sh[3 + k][threadIdx.x], sh[3 + k][threadIdx.x + o]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 6; ++k) part[6 * blockIdx.x + k] = sh[k][0];
+}
+
+SearchGeom geom_of(gt_context* ctx, gt_tree* t, double elapsed, double box) {
+    ensure_snodes(ctx, t);
+    SearchGeom g;
+    g.root = t->n_nodes > 0 ? 0 : -1;
+    g.sn = t->snode;
+    g.src = t->src;
+    g.order = t->order;
+    g.xpad = t->xpad;
+    g.vmax = t->vmax;
+    g.hmax = t->hmax;
+    g.elapsed = elapsed;
+    g.box = box;
+    return g;
+}
+
+}  // namespace
+
+void ensure_snodes(gt_context* ctx, gt_tree* t) {
+    if (t->snode || t->n_nodes <= 0) return;
+    if (t->n_systems > 1) throw Fail{GT_ERR_UNSUPPORTED, "the neighbour search works on single-system trees"};
+    SNodeG* p = nullptr;
+    check_cuda(cudaMallocAsync((void**)&p, (size_t)t->n_nodes * sizeof(SNodeG), ctx->stream), "cudaMallocAsync");
+    t->snode = p;
+    double root_size = 0.0;
+    check_cuda(cudaMemcpyAsync(&root_size, t->size, 8, cudaMemcpyDeviceToHost, ctx->stream), "d2h");
+    check_cuda(cudaStreamSynchronize(ctx->stream), "sync");
+    pack_snode_kernel<<<grid_of(ctx, t->n_nodes), kBlk, 0, ctx->stream>>>(t->nodes, t->next, t->gc, t->size,
+                                                                          t->n_nodes, 1e-6 * root_size, p);
+    check_launch(ctx, "pack_snode_kernel");
+}
+
+void tree_hmax(gt_context* ctx, gt_tree* t, const double* h, int64_t n_gas) {
+    const int64_t nn = std::max<int64_t>(t->n_nodes, 1);
+    if (!t->hmax) check_cuda(cudaMallocAsync((void**)&t->hmax, (size_t)nn * 4, ctx->stream), "cudaMallocAsync");
+    check_cuda(cudaMemsetAsync(t->hmax, 0, (size_t)nn * 4, ctx->stream), "memset");
+    const int64_t n = std::min<int64_t>(n_gas, t->n);
+    if (n > 0) {
+        hmax_kernel<<<grid_of(ctx, n), kBlk, 0, ctx->stream>>>(h, t->leaf_of, n, t->parent, true, t->hmax);
+        check_launch(ctx, "hmax_kernel");
+    }
+}
+
+void raise_hmax(gt_context* ctx, gt_tree* t, int64_t n, const int* leaf, const double* h) {
+    if (!t->hmax || n <= 0) return;  // Tree::raise_hmax is a no-op before init_hmax
+    hmax_kernel<<<grid_of(ctx, n), kBlk, 0, ctx->stream>>>(h, leaf, n, t->parent, false, t->hmax);
+    check_launch(ctx, "hmax_kernel");
+}
+
+int64_t run_ngb(gt_context* ctx, gt_tree* t, int64_t n, const double* cx, const double* cy, const double* cz,
+                const double* radius, int mode, const double* h, int64_t n_gas, double box, double elapsed,
+                int64_t* start, uint32_t* found, int64_t capacity) {
+    if (mode != GT_NGB_GATHER && !t->hmax) throw Fail{GT_ERR_INVALID, "the reverse search needs gt_tree_hmax first"};
+    cudaStream_t st = ctx->stream;
+    NgbArgs a;
+    a.g = geom_of(ctx, t, elapsed, box);
+    a.cx = cx; a.cy = cy; a.cz = cz; a.radius = radius;
+    a.n = n;
+    a.mode = mode;
+    a.h = h;
+    a.n_gas = n_gas;
+    uint32_t* cnt = (uint32_t*)scratch(ctx, kSlotNgb0, (size_t)std::max<int64_t>(n, 1) * 4);
+    uint32_t* ex = (uint32_t*)scratch(ctx, kSlotNgb1, (size_t)std::max<int64_t>(n, 1) * 4);
+    unsigned long long* tot = (unsigned long long*)scratch(ctx, kSlotNgb2, 8);
+    check_cuda(cudaMemsetAsync(tot, 0, 8, st), "memset");
+    a.count = cnt;
+    a.total = tot;
+    a.start = nullptr;
+    a.found = nullptr;
+    ngb_kernel<false><<<grid_of(ctx, n), kBlk, 0, st>>>(a);
+    check_launch(ctx, "ngb_kernel");
+    unsigned long long total = 0;
+    check_cuda(cudaMemcpyAsync(ctx->pinned, tot, 8, cudaMemcpyDeviceToHost, st), "d2h");
+    check_cuda(cudaStreamSynchronize(st), "sync");
+    std::memcpy(&total, ctx->pinned, 8);
+    if (total >= (1ull << 32)) throw Fail{GT_ERR_OVERFLOW, "more than 2^32 neighbours in one call"};
+    scan_exclusive_u32(ctx, cnt, ex, n, nullptr);
+    widen_kernel<<<grid_of(ctx, n), kBlk, 0, st>>>(ex, cnt, n, start);
+    check_launch(ctx, "widen_kernel");
+    if (found && (int64_t)total <= capacity && total > 0) {
+        a.start = start;
+        a.found = found;
+        ngb_kernel<true><<<grid_of(ctx, n), kBlk, 0, st>>>(a);
+        check_launch(ctx, "ngb_kernel");
+    }
+    return (int64_t)total;
+}
+
+void run_density(gt_context* ctx, gt_tree* t, int64_t nt, const uint32_t* targets, double des_ngb, double ngb_tol,
+                 const double* h_start, double box, int n_dims, const double* cond_prev, int face_corr,
+                 double elapsed, double* h, double* rho, int* nngb, int* iters) {
+    cudaStream_t st = ctx->stream;
+    DensArgs a;
+    a.g = geom_of(ctx, t, elapsed, box);
+    a.smass = t->smass;
+    a.stype = t->stype;
+    a.rank = t->rank;
+    a.targets = targets;
+    a.nt = nt;
+    a.des_ngb = des_ngb;
+    a.ngb_tol = ngb_tol;
+    a.h_start = h_start;
+    a.cond_prev = cond_prev;
+    a.n_dims = n_dims;
+    a.face_corr = face_corr;
+    a.h = h; a.rho = rho; a.nngb = nngb; a.iters = iters;
+    a.h_default = 0.0;
+    if (!h_start) {
+        // des_ngb particles at the mean number density of the bounding box of all particles
+        const int nb = std::max(1, std::min(grid_of(ctx, t->n), ctx->num_sms * 2));
+        double* part = (double*)scratch(ctx, kSlotNgb2, (size_t)nb * 6 * 8);
+        bbox_all_kernel<<<nb, kBlk, 0, st>>>(t->src, t->n, part);
+        check_launch(ctx, "bbox_all_kernel");
+        std::vector<double> hp((size_t)nb * 6);
+        check_cuda(cudaMemcpyAsync(hp.data(), part, hp.size() * 8, cudaMemcpyDeviceToHost, st), "d2h");
+        check_cuda(cudaStreamSynchronize(st), "sync");
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int b = 0; b < nb; ++b)
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = std::min(lo[k], hp[6 * b + k]);
+                hi[k] = std::max(hi[k], hp[6 * b + 3 + k]);
+            }
+        const double vol = (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
+        const double n = (double)t->n;
+        a.h_default = std::cbrt(3.0 * des_ngb * vol / (4.0 * M_PI * n));
+        if (n_dims == 1) a.h_default = 0.5 * des_ngb * (hi[0] - lo[0]) / n;
+        if (n_dims == 2) a.h_default = std::sqrt(des_ngb * (hi[0] - lo[0]) * (hi[1] - lo[1]) / (M_PI * n));
+    }
+    if (nt <= 0) return;
+    density_kernel<<<grid_of(ctx, nt), kBlk, 0, st>>>(a);
+    check_launch(ctx, "density_kernel");
+}
+
+}  // namespace gt

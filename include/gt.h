@@ -231,9 +231,10 @@ GT_API int gt_tree_velocities(gt_context* ctx, gt_tree* tree, const double* vx, 
  *   GT_EVENT_SOFT   raise_soft(leaf, soft = a[e])                  tree.cc:310-319
  *   GT_EVENT_MASS   mass_event(leaf, dm = a[e], x[3e..], v[3e..], tau, box)  tree.cc:229-246 (serial; no-op without vcom)
  *   GT_EVENT_PAD    raise_pad(leaf, d = a[e])                      tree.cc:322-329 (serial)
+ *   GT_EVENT_HMAX   raise_hmax(leaf, h = a[e])                     tree.cc:293-302 (no-op before gt_tree_hmax)
  * Node vcom comes from gt_tree_velocities. */
 enum { GT_EVENT_KICK = 0, GT_EVENT_SHIFT = 1, GT_EVENT_VMAX = 2, GT_EVENT_SOFT = 3, GT_EVENT_MASS = 4,
-       GT_EVENT_PAD = 5 };
+       GT_EVENT_PAD = 5, GT_EVENT_HMAX = 6 };
 GT_API int gt_tree_events(gt_context* ctx, gt_tree* tree, int kind, int64_t n, const int32_t* leaf,
                    const double* a, const double* x, const double* v, const float* f, double tau,
                    double box, int mem);
@@ -308,6 +309,54 @@ GT_API int gt_potential(gt_context* ctx, const gt_tree* tree, int64_t n_targets,
                  double theta, double G, const double* aold, int mem, double* phi);
 /* Counts and device time of the last walk on this context (SHMEM_COUNT_WALK, tree.cc:671-677). */
 GT_API int gt_walk_stats_get(const gt_context* ctx, gt_walk_stats* stats);
+
+/* ---- neighbour search and the density solve (shmem/hydro.h:65-117, hydro.cc:37-327) --------
+ * On the gravity tree (single-system trees), through search nodes that hold each node's box
+ * (shmem::SNode, tree.h:206-226), made on first use.  Lists are in tree order, which is the
+ * reference's order for a tree built with GT_KEY_MORTON. */
+enum {
+    GT_NGB_GATHER = 0,  /* ngb_search (hydro.cc:37-108): particles with r < radius */
+    GT_NGB_REVERSE = 1, /* ngb_search_reverse (hydro.cc:110-148): gas particles j < n_gas with radius <= r < h[j] */
+    GT_NGB_PAIRS = 2    /* the gather list followed by the reverse list: every pair with r < max(h_i, h_j) */
+};
+typedef struct {
+    int mode;          /* GT_NGB_* (default GT_NGB_GATHER) */
+    double box;        /* periodic box side, minimum-image separations (vec.h:25-31); 0 = open */
+    double elapsed;    /* Tree::t_since_build: node boxes widen by vmax * elapsed (and always by xpad) */
+    int64_t n_gas;     /* reverse: particles [0, n_gas) are gas */
+    const double* h;   /* reverse: support radius of each gas particle (n_gas), located like the other arrays */
+} gt_ngb_options;
+GT_API void gt_ngb_options_default(gt_ngb_options* opt);
+/* Tree::init_hmax (tree.cc:332-338): per node the largest h, rounded up to float, of the gas
+ * particles [0, n_gas) below it.  The reverse search needs it; GT_EVENT_HMAX raises it later. */
+GT_API int gt_tree_hmax(gt_context* ctx, gt_tree* tree, const double* h, int64_t n_gas, int mem);
+/* Neighbour lists of n_centres centres (cx, cy, cz, radius: n_centres each) as CSR: start
+ * (n_centres + 1 int64) always; found (particle indices) when it is not NULL and the total fits
+ * `capacity`, else GT_ERR_OVERFLOW with start and *total filled (call again with room).  *total
+ * (may be NULL) receives the number of entries. */
+GT_API int gt_ngb_search(gt_context* ctx, const gt_tree* tree, int64_t n_centres, const double* cx,
+                  const double* cy, const double* cz, const double* radius, const gt_ngb_options* opt,
+                  int mem, int64_t* start, uint32_t* found, int64_t capacity, int64_t* total);
+typedef struct {
+    double des_ngb;        /* DesNumNgb (default 32) */
+    double ngb_tol;        /* tolerance on N_eff (default 0.05, as shmem/bench_density.cc) */
+    double box;            /* periodic box side; 0 = open */
+    double elapsed;        /* Tree::t_since_build (search prune pad) */
+    int n_dims;            /* 1, 2 or 3 (default 3) */
+    int face_correction;   /* 1 (default): the face-closure correction; 0: SHMEM_NO_FACECORR */
+    const double* h_start; /* per target initial h; NULL: DesNumNgb at the mean density of the box */
+    const double* cond_prev; /* per particle condition number of the last evaluation, or NULL */
+} gt_density_options;
+GT_API void gt_density_options_default(gt_density_options* opt);
+/* shmem::density (hydro.cc:150-327): per target, bisection-guarded Newton on the effective
+ * neighbour number N_eff(h) = DesNumNgb over GAS neighbours (types of gt_tree_gas; all gas without
+ * them), with the face-closure and condition-number corrections.  Outputs per target: the
+ * converged support radius h, rho = sum m_j W(r_ij, h), the neighbours inside h and the
+ * iterations (100 = not converged).  One thread per target follows the tree in the reference's
+ * order, so the sums accumulate in its order.  Any output pointer may be NULL. */
+GT_API int gt_density(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
+               const gt_density_options* opt, int mem, double* h, double* rho, int32_t* nngb,
+               int32_t* iters);
 
 /* ---- autotuner ----------------------------------------------------------------------------- */
 /* One candidate launch configuration of the all-active grouped walk and what it measured. */

@@ -8,6 +8,7 @@
 #define _GNU_SOURCE
 #include "gt_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -875,4 +876,312 @@ void or_set_walk_nodes(or_tree* t, const double* cx, const double* cy, const dou
 
 void or_set_positions(or_tree* t, const double* x, const double* y, const double* z) {
     t->x = x; t->y = y; t->z = z;
+}
+
+/* ---- neighbour search and the density solve (shmem/hydro.h:25-117, hydro.cc:37-327) ---------- */
+
+/* Minimum-image separation, box <= 0 = open (shmem/vec.h:25-31). */
+static inline double or_min_image(double s, double box) {
+    if (box > 0) {
+        if (s > 0.5 * box) s -= box;
+        else if (s < -0.5 * box) s += box;
+    }
+    return s;
+}
+
+/* The search node's conservative half side: float centre, so widened by 1e-6 of the root side plus
+ * four float ulps of the centre's largest coordinate (tree.cc:490-505).  Only the prune uses it. */
+static float or_snode_half(const or_tree* t, int i) {
+    const double eps = 1e-6 * (t->nnodes ? t->size[t->root] : 1.0);
+    const double cm = dmax(fabs(t->gcx[i]), dmax(fabs(t->gcy[i]), fabs(t->gcz[i])));
+    return (float)(0.5 * t->size[i] + eps + 4.0 * (double)FLT_EPSILON * cm);
+}
+
+/* Tree::init_hmax (tree.cc:287-302, 332-338): per node the largest h, rounded up to float, of the
+ * gas particles [0, n_gas) below it with h > 0. */
+void or_init_hmax(const or_tree* t, const double* h, int64_t n_gas, float* hmax) {
+    for (int64_t i = 0; i < t->nnodes; ++i) hmax[i] = 0.0f;
+    const int64_t n = n_gas < t->n ? n_gas : t->n;
+    for (int64_t i = 0; i < n; ++i) {
+        if (!(h[i] > 0) || t->leaf_of[i] < 0) continue;
+        float f = (float)h[i];
+        if ((double)f < h[i]) f = nextafterf(f, 1e30f);
+        for (int no = t->leaf_of[i]; no >= 0; no = t->parent[no]) {
+            if (hmax[no] >= f) break;
+            hmax[no] = f;
+        }
+    }
+}
+
+/* One centre's search, appending particle indices to out (capacity cap; returns the count, which
+ * may exceed cap).  mode 0: ngb_search, r < radius (hydro.cc:37-108); mode 1: ngb_search_reverse,
+ * gas j < n_gas with radius <= r < h[j] (hydro.cc:110-148), pruned by hmax.  Nodes in the
+ * reference's threading order, so the lists come out in tree order. */
+static int64_t or_ngb_one(const or_tree* t, const float* half, const float* hmax, double cx, double cy, double cz,
+                          double radius, int mode, const double* h, int64_t n_gas, double box, uint32_t* out,
+                          int64_t cap) {
+    int64_t k = 0;
+    const double r2max = radius * radius;
+    int node = t->root;
+    while (node >= 0) {
+        const double hn = (double)half[node];
+        double dist;
+        if (mode == 0) {
+            dist = radius + hn;
+        } else {
+            const double hm = (double)hmax[node];
+            if (hm <= radius) { node = t->next[node]; continue; }
+            dist = hm + hn;
+        }
+        const double dx = or_min_image((double)(float)t->gcx[node] - cx, box);
+        if (dx > dist || -dx > dist) { node = t->next[node]; continue; }
+        const double dy = or_min_image((double)(float)t->gcy[node] - cy, box);
+        if (dy > dist || -dy > dist) { node = t->next[node]; continue; }
+        const double dz = or_min_image((double)(float)t->gcz[node] - cz, box);
+        if (dz > dist || -dz > dist) { node = t->next[node]; continue; }
+        dist += 0.7320508075688772 * hn;
+        if (dx * dx + dy * dy + dz * dz > dist * dist) { node = t->next[node]; continue; }
+        if (t->first[node] < 0) {
+            for (int s = t->plo[node]; s < t->phi[node]; ++s) {
+                const uint32_t j = t->order[s];
+                if (mode == 1 && (int64_t)j >= n_gas) continue;
+                const double ox = or_min_image(t->x[j] - cx, box), oy = or_min_image(t->y[j] - cy, box),
+                             oz = or_min_image(t->z[j] - cz, box);
+                const double r2 = ox * ox + oy * oy + oz * oz;
+                const int keep = mode == 0 ? r2 < r2max : (r2 >= r2max && r2 < h[j] * h[j]);
+                if (keep) {
+                    if (k < cap) out[k] = j;
+                    ++k;
+                }
+            }
+            node = t->next[node];
+        } else {
+            node = t->first[node];
+        }
+    }
+    return k;
+}
+
+/* Searches for n centres as CSR: mode 0 gather, 1 reverse (h, n_gas), 2 gather then reverse.
+ * start has n+1 entries; found (may be null) receives start[n] entries if cap suffices. */
+void or_ngb_search(const or_tree* t, int64_t n, const double* cx, const double* cy, const double* cz,
+                   const double* radius, int mode, const double* h, int64_t n_gas, double box, int64_t* start,
+                   uint32_t* found, int64_t cap) {
+    float* half = (float*)malloc((size_t)(t->nnodes > 0 ? t->nnodes : 1) * 4);
+    float* hmax = (float*)calloc((size_t)(t->nnodes > 0 ? t->nnodes : 1), 4);
+    for (int64_t i = 0; i < t->nnodes; ++i) half[i] = or_snode_half(t, (int)i);
+    if (mode != 0) or_init_hmax(t, h, n_gas, hmax);
+    int64_t* cnt = (int64_t*)calloc((size_t)n + 1, 8);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t c = 0; c < n; ++c) {
+        int64_t k = 0;
+        if (mode != 1) k += or_ngb_one(t, half, hmax, cx[c], cy[c], cz[c], radius[c], 0, h, n_gas, box, NULL, 0);
+        if (mode != 0) k += or_ngb_one(t, half, hmax, cx[c], cy[c], cz[c], radius[c], 1, h, n_gas, box, NULL, 0);
+        cnt[c] = k;
+    }
+    start[0] = 0;
+    for (int64_t c = 0; c < n; ++c) start[c + 1] = start[c] + cnt[c];
+    if (found && start[n] <= cap) {
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t c = 0; c < n; ++c) {
+            int64_t k = 0;
+            uint32_t* o = found + start[c];
+            if (mode != 1) k += or_ngb_one(t, half, hmax, cx[c], cy[c], cz[c], radius[c], 0, h, n_gas, box, o, cnt[c]);
+            if (mode != 0)
+                or_ngb_one(t, half, hmax, cx[c], cy[c], cz[c], radius[c], 1, h, n_gas, box, o + k, cnt[c] - k);
+        }
+    }
+    free(cnt);
+    free(hmax);
+    free(half);
+}
+
+/* The cubic spline of support h in n_dims dimensions (shmem/hydro.h:25-63): norm, W, dW/dh and the
+ * unit ball volume. */
+static double or_kernel_norm(double h, int dim) {
+    if (dim == 1) return (4.0 / 3.0) / h;
+    if (dim == 2) return 40.0 / (7.0 * M_PI * h * h);
+    return 8.0 / (M_PI * h * h * h);
+}
+static double or_ball_vol(double h, int dim) {
+    if (dim == 1) return 2.0 * h;
+    if (dim == 2) return M_PI * h * h;
+    return 4.0 * M_PI / 3.0 * h * h * h;
+}
+static double or_kernel_w(double r, double h, int dim) {
+    const double q = r / h;
+    if (q >= 1.0) return 0.0;
+    const double norm = or_kernel_norm(h, dim);
+    if (q < 0.5) return norm * (1.0 - 6.0 * q * q + 6.0 * q * q * q);
+    const double u = 1.0 - q;
+    return norm * 2.0 * u * u * u;
+}
+static double or_kernel_dwdh(double r, double h, int dim) {
+    const double q = r / h;
+    if (q >= 1.0) return 0.0;
+    const double norm = or_kernel_norm(h, dim);
+    double f, fp;
+    if (q < 0.5) {
+        f = 1.0 - 6.0 * q * q + 6.0 * q * q * q;
+        fp = -12.0 * q + 18.0 * q * q;
+    } else {
+        const double u = 1.0 - q;
+        f = 2.0 * u * u * u;
+        fp = -6.0 * u * u;
+    }
+    return -((double)dim / h) * norm * f - (q / h) * norm * fp;
+}
+
+/* Rank-d inverse of the symmetric moments (xx yy zz xy yz xz) into a row-major 3x3, zero when
+ * degenerate (shmem/vec.h:43-66; the 3-D case is the cofactor inverse of math_types/mat3.h:41-67). */
+static int or_invert_moments(const double* m, double* B, int n_dims) {
+    for (int i = 0; i < 9; ++i) B[i] = 0.0;
+    if (n_dims == 1) {
+        if (fabs(m[0]) < 1e-300) return 0;
+        B[0] = 1.0 / m[0];
+        return 1;
+    }
+    if (n_dims == 2) {
+        const double det = m[0] * m[1] - m[3] * m[3];
+        if (fabs(det) < 1e-300) return 0;
+        B[0] = m[1] / det; B[1] = -m[3] / det;
+        B[3] = -m[3] / det; B[4] = m[0] / det;
+        return 1;
+    }
+    const double a00 = m[0], a01 = m[3], a02 = m[5], a10 = m[3], a11 = m[1], a12 = m[4], a20 = m[5], a21 = m[4],
+                 a22 = m[2];
+    const double d = a00 * (a11 * a22 - a12 * a21) - a01 * (a10 * a22 - a12 * a20) + a02 * (a10 * a21 - a11 * a20);
+    if (d == 0.0 || d != d) return 0;
+    const double id = 1.0 / d;
+    B[0] = (a11 * a22 - a12 * a21) * id; B[1] = (a02 * a21 - a01 * a22) * id; B[2] = (a01 * a12 - a02 * a11) * id;
+    B[3] = (a12 * a20 - a10 * a22) * id; B[4] = (a00 * a22 - a02 * a20) * id; B[5] = (a02 * a10 - a00 * a12) * id;
+    B[6] = (a10 * a21 - a11 * a20) * id; B[7] = (a01 * a20 - a00 * a21) * id; B[8] = (a00 * a11 - a01 * a10) * id;
+    return 1;
+}
+
+/* One density evaluation at h over the gather list of the target at (px,py,pz): the sums the
+ * solve reads (hydro.cc:205-222). */
+typedef struct {
+    double wsum, dwdh, rho, mom[6], face[3];
+    int inside;
+} or_dens_sums;
+static void or_dens_eval(const or_tree* t, const uint8_t* type, const uint32_t* ngb, int64_t nn, double px, double py,
+                         double pz, double h, double box, int n_dims, or_dens_sums* s) {
+    memset(s, 0, sizeof(*s));
+    for (int64_t k = 0; k < nn; ++k) {
+        const uint32_t j = ngb[k];
+        if (type && type[j] != 0) continue;
+        const double dx = or_min_image(t->x[j] - px, box), dy = or_min_image(t->y[j] - py, box),
+                     dz = or_min_image(t->z[j] - pz, box);
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double w = or_kernel_w(r, h, n_dims);
+        s->wsum += w;
+        s->dwdh += or_kernel_dwdh(r, h, n_dims);
+        s->rho += t->m[j] * w;
+        s->mom[0] += dx * dx * w; s->mom[1] += dy * dy * w; s->mom[2] += dz * dz * w;
+        s->mom[3] += dx * dy * w; s->mom[4] += dy * dz * w; s->mom[5] += dx * dz * w;
+        s->face[0] += dx * w; s->face[1] += dy * w; s->face[2] += dz * w;
+        if (r < h) ++s->inside;
+    }
+}
+
+/* density (hydro.cc:150-327) for nt targets: bisection-guarded Newton on N_eff(h) = des_ngb with
+ * the face-closure and condition-number corrections.  h_start (per target) and cond_prev (per
+ * particle) may be null; type (per particle, 0 = gas) may be null (all gas).  face_corr = 0 is
+ * SHMEM_NO_FACECORR. */
+void or_density(const or_tree* t, int64_t nt, const uint32_t* targets, double des_ngb, double ngb_tol,
+                const double* h_start, double box, int n_dims, const double* cond_prev, const uint8_t* type,
+                int face_corr, double* h_out, double* rho_out, int32_t* nngb_out, int32_t* iters_out) {
+    double h_default = 0.0;
+    if (!h_start) {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int64_t i = 0; i < t->n; ++i) {
+            lo[0] = dmin(lo[0], t->x[i]); hi[0] = dmax(hi[0], t->x[i]);
+            lo[1] = dmin(lo[1], t->y[i]); hi[1] = dmax(hi[1], t->y[i]);
+            lo[2] = dmin(lo[2], t->z[i]); hi[2] = dmax(hi[2], t->z[i]);
+        }
+        const double vol = (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
+        h_default = cbrt(3.0 * des_ngb * vol / (4.0 * M_PI * (double)t->n));
+        if (n_dims == 1) h_default = 0.5 * des_ngb * (hi[0] - lo[0]) / (double)t->n;
+        if (n_dims == 2) h_default = sqrt(des_ngb * (hi[0] - lo[0]) * (hi[1] - lo[1]) / (M_PI * (double)t->n));
+    }
+    float* half = (float*)malloc((size_t)(t->nnodes > 0 ? t->nnodes : 1) * 4);
+    for (int64_t i = 0; i < t->nnodes; ++i) half[i] = or_snode_half(t, (int)i);
+#pragma omp parallel
+    {
+        int64_t cap = 256;
+        uint32_t* ngb = (uint32_t*)malloc((size_t)cap * 4);
+#pragma omp for schedule(dynamic, 16)
+        for (int64_t c = 0; c < nt; ++c) {
+            const uint32_t p = targets[c];
+            const double px = t->x[p], py = t->y[p], pz = t->z[p];
+            double h = h_start ? h_start[c] : h_default, h_lo = 0.0, h_hi = 0.0;
+            int iter = 0, converged = 0;
+            or_dens_sums s;
+            memset(&s, 0, sizeof(s));
+            for (; iter < 100; ++iter) {
+                int64_t nn = or_ngb_one(t, half, NULL, px, py, pz, h, 0, NULL, 0, box, ngb, cap);
+                if (nn > cap) {
+                    cap = nn * 2;
+                    ngb = (uint32_t*)realloc(ngb, (size_t)cap * 4);
+                    nn = or_ngb_one(t, half, NULL, px, py, pz, h, 0, NULL, 0, box, ngb, cap);
+                }
+                or_dens_eval(t, type, ngb, nn, px, py, pz, h, box, n_dims, &s);
+                const double n_eff = or_ball_vol(h, n_dims) * s.wsum;
+                double ncorr = 1.0;
+                if (cond_prev) {
+                    const double cn = cond_prev[p];
+                    if (cn > 100.0) ncorr = dmin(sqrt(1.0 + (cn - 100.0) / 1000.0), 2.0);
+                }
+                double des_eff = des_ngb * ncorr, tol_eff = ngb_tol * ncorr;
+                if (face_corr && s.wsum > 0) {
+                    double B[9];
+                    if (or_invert_moments(s.mom, B, n_dims)) {
+                        const double vol = 1.0 / s.wsum;
+                        const double dx_i = sqrt(vol * (s.mom[0] + s.mom[1] + s.mom[2]));
+                        double sum_abs = 0.0;
+                        for (int r = 0; r < 3; ++r) {
+                            const double leak = (B[3 * r] * s.face[0] + B[3 * r + 1] * s.face[1] + B[3 * r + 2] * s.face[2]) *
+                                                (2.0 * vol);
+                            sum_abs += fabs(leak) / n_dims;
+                        }
+                        const double denom = 2.0 * n_dims * pow(dx_i, n_dims - 1);
+                        if (denom > 0) {
+                            const double fce = sum_abs / denom;
+                            if (fce > 0.35) ncorr = dmax(ncorr, dmin(fce / 0.35, 2.0));
+                            des_eff = des_ngb * ncorr;
+                            tol_eff = ngb_tol * ncorr;
+                        }
+                    }
+                }
+                if (iter > 1)
+                    tol_eff = dmin(0.25 * des_eff, tol_eff * exp(0.1 * log(des_eff / (16.0 * tol_eff)) * iter));
+                const double res = n_eff - des_eff;
+                if (fabs(res) < tol_eff) { converged = 1; break; }
+                if (res > 0) h_hi = h; else h_lo = h;
+                const double dn = or_ball_vol(h, n_dims) * ((double)n_dims / h * s.wsum + s.dwdh);
+                double hn = dn > 0 ? h - res / dn : 0.0;
+                if (hn <= h_lo || (h_hi > 0 && hn >= h_hi) || hn <= 0) {
+                    if (h_hi > 0) hn = h_lo > 0 ? sqrt(h_lo * h_hi) : 0.5 * h_hi;
+                    else hn = h * (res > 0 ? 0.7 : 1.6);
+                }
+                h = hn;
+            }
+            if (!converged) {
+                int64_t nn = or_ngb_one(t, half, NULL, px, py, pz, h, 0, NULL, 0, box, ngb, cap);
+                if (nn > cap) {
+                    cap = nn * 2;
+                    ngb = (uint32_t*)realloc(ngb, (size_t)cap * 4);
+                    nn = or_ngb_one(t, half, NULL, px, py, pz, h, 0, NULL, 0, box, ngb, cap);
+                }
+                or_dens_eval(t, type, ngb, nn, px, py, pz, h, box, n_dims, &s);
+            }
+            h_out[c] = h;
+            rho_out[c] = s.rho;
+            nngb_out[c] = s.inside;
+            iters_out[c] = iter;
+        }
+        free(ngb);
+    }
+    free(half);
 }

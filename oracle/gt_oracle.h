@@ -86,6 +86,19 @@ void or_walk_groups_gas(const or_tree* t, int64_t nt, const uint32_t* targets, i
                         double* ax, double* ay, double* az);
 /* Sinks below each node (tree.cc:155-187); nnodes entries. */
 void or_node_sinks(const or_tree* t, const uint8_t* type, uint32_t* nsink);
+/* Neighbour search (shmem/hydro.cc:37-148) for n centres as CSR, in tree order: mode 0 gather
+ * (r < radius), 1 reverse (gas j < n_gas with radius <= r < h[j]), 2 gather then reverse.  start
+ * has n+1 entries; found (may be null) receives start[n] entries when cap suffices. */
+void or_ngb_search(const or_tree* t, int64_t n, const double* cx, const double* cy, const double* cz,
+                   const double* radius, int mode, const double* h, int64_t n_gas, double box, int64_t* start,
+                   uint32_t* found, int64_t cap);
+/* Tree::init_hmax (tree.cc:332-338); hmax has nnodes entries. */
+void or_init_hmax(const or_tree* t, const double* h, int64_t n_gas, float* hmax);
+/* density (hydro.cc:150-327).  h_start (per target), cond_prev (per particle) and type (per
+ * particle, 0 = gas) may be null. */
+void or_density(const or_tree* t, int64_t nt, const uint32_t* targets, double des_ngb, double ngb_tol,
+                const double* h_start, double box, int n_dims, const double* cond_prev, const uint8_t* type,
+                int face_corr, double* h_out, double* rho_out, int32_t* nngb_out, int32_t* iters_out);
 /* Tree reuse: overwrite the walk's node fields (COM, mass, opening radius, side, softening) and
  * re-point the particle positions (the caller keeps the arrays alive). */
 void or_set_walk_nodes(or_tree* t, const double* cx, const double* cy, const double* cz, const double* mass,

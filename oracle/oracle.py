@@ -113,6 +113,11 @@ class Restatement:
         L.or_walk_groups_gas.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_int64, _i64, C.c_double,
                                          C.c_double, _d, C.c_void_p, _d, C.c_double, C.c_int, _d, _d, _d]
         L.or_node_sinks.argtypes = [C.c_void_p, C.c_void_p, _u32]
+        L.or_ngb_search.argtypes = [C.c_void_p, C.c_int64, _d, _d, _d, _d, C.c_int, _d, C.c_int64, C.c_double,
+                                    _i64, _u32, C.c_int64]
+        L.or_init_hmax.argtypes = [C.c_void_p, _d, C.c_int64, _f]
+        L.or_density.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, _d, C.c_double, C.c_int, _d,
+                                 C.c_void_p, C.c_int, _d, _d, C.c_void_p, C.c_void_p]
 
     # scalar helpers
     def spline_force_over_r(self, r, h):
@@ -295,6 +300,39 @@ class OracleTree:
                                       int(leaf_accept), _p(ax, _d), _p(ay, _d), _p(az, _d))
         return ax, ay, az
 
+    def ngb_search(self, cx, cy, cz, radius, mode=0, h=None, n_gas=0, box=0.0):
+        """Neighbour lists (start [n+1], found) in tree order: mode 0 gather, 1 reverse, 2 both."""
+        cx, cy, cz, r = (_f64(a) for a in (cx, cy, cz, radius))
+        n = len(cx)
+        hv = _f64(h) if h is not None else None
+        start = np.zeros(n + 1, np.int64)
+        self.lib.L.or_ngb_search(self.h, n, _p(cx, _d), _p(cy, _d), _p(cz, _d), _p(r, _d), mode, _p(hv, _d),
+                                 int(n_gas), box, _p(start, _i64), None, 0)
+        found = np.zeros(max(int(start[-1]), 1), np.uint32)
+        self.lib.L.or_ngb_search(self.h, n, _p(cx, _d), _p(cy, _d), _p(cz, _d), _p(r, _d), mode, _p(hv, _d),
+                                 int(n_gas), box, _p(start, _i64), _p(found, _u32), len(found))
+        return start, found[: start[-1]]
+
+    def init_hmax(self, h, n_gas):
+        hv = _f64(h)
+        out = np.zeros(self.nnodes, np.float32)
+        self.lib.L.or_init_hmax(self.h, _p(hv, _d), int(n_gas), _p(out, _f))
+        return out
+
+    def density(self, targets, des_ngb=32.0, ngb_tol=0.05, h_start=None, box=0.0, n_dims=3, cond_prev=None,
+                type=None, face_corr=True):
+        t = _targets(targets)
+        nt = len(t)
+        h, rho = np.zeros(nt), np.zeros(nt)
+        nngb, iters = np.zeros(nt, np.int32), np.zeros(nt, np.int32)
+        hs = _f64(h_start) if h_start is not None else None
+        cp = _f64(cond_prev) if cond_prev is not None else None
+        ty = None if type is None else np.ascontiguousarray(type, np.uint8)
+        self.lib.L.or_density(self.h, nt, _p(t, _u32), des_ngb, ngb_tol, _p(hs, _d), box, n_dims, _p(cp, _d),
+                              None if ty is None else ty.ctypes.data, int(face_corr), _p(h, _d), _p(rho, _d),
+                              nngb.ctypes.data, iters.ctypes.data)
+        return {"h": h, "rho": rho, "nngb": nngb, "iters": iters}
+
     def node_sinks(self, type):
         ty = np.ascontiguousarray(type, np.uint8)
         out = np.zeros(self.nnodes, np.uint32)
@@ -377,6 +415,13 @@ class Reference:
         L.ref_accel_grouped_gas.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, C.c_int, _d,
                                             C.c_double, _d, _d, _d]
         L.ref_tree_nsink.argtypes = [C.c_void_p, _u32]
+        L.ref_set_elapsed.argtypes = [C.c_void_p, C.c_double]
+        L.ref_init_hmax.argtypes = [C.c_void_p, _d, C.c_int64, _f]
+        L.ref_raise_hmax.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, _d]
+        L.ref_ngb_search.argtypes = [C.c_void_p, C.c_int64, _d, _d, _d, _d, C.c_int, _d, C.c_int64, C.c_double,
+                                     _i64, _u32, C.c_int64]
+        L.ref_density.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_double, C.c_double, _d, C.c_double, C.c_int, _d,
+                                  _d, _d, C.c_void_p, C.c_void_p, _i64, _u32, C.c_int64]
         L.ref_reuse_begin.argtypes = [C.c_void_p]
         L.ref_kick_node.argtypes = [C.c_void_p, C.c_int, _d, C.c_double]
         L.ref_mass_event.argtypes = [C.c_void_p, C.c_int, C.c_double, _d, _d, C.c_double, C.c_double]
@@ -568,6 +613,54 @@ class ReferenceTree:
     def nsink(self):
         out = np.zeros(self.nnodes, np.uint32)
         self.lib.L.ref_tree_nsink(self.h, _p(out, _u32))
+        return out
+
+    # ---- neighbour search and the density solve (shmem/hydro.cc) ----
+    def set_elapsed(self, elapsed):
+        self.lib.L.ref_set_elapsed(self.h, float(elapsed))
+
+    def init_hmax(self, h, n_gas):
+        self._hmax_h = _f64(h)
+        out = np.zeros(self.nnodes, np.float32)
+        self.lib.L.ref_init_hmax(self.h, _p(self._hmax_h, _d), int(n_gas), _p(out, _f))
+        return out
+
+    def raise_hmax(self, leaf, h):
+        lf = np.ascontiguousarray(leaf, np.int32)
+        hv = _f64(h)
+        self.lib.L.ref_raise_hmax(self.h, len(lf), lf.ctypes.data, _p(hv, _d))
+
+    def ngb_search(self, cx, cy, cz, radius, mode=0, h=None, n_gas=0, box=0.0):
+        """Neighbour lists (start [n+1], found) of ngb_search (mode 0), ngb_search_reverse
+        (mode 1, h_i = radius, needs init_hmax) or both (mode 2), in the reference's order."""
+        cx, cy, cz, r = (_f64(a) for a in (cx, cy, cz, radius))
+        n = len(cx)
+        hv = _f64(h) if h is not None else None
+        start = np.zeros(n + 1, np.int64)
+        self.lib.L.ref_ngb_search(self.h, n, _p(cx, _d), _p(cy, _d), _p(cz, _d), _p(r, _d), mode, _p(hv, _d),
+                                  int(n_gas), box, _p(start, _i64), None, 0)
+        found = np.zeros(max(int(start[-1]), 1), np.uint32)
+        self.lib.L.ref_ngb_search(self.h, n, _p(cx, _d), _p(cy, _d), _p(cz, _d), _p(r, _d), mode, _p(hv, _d),
+                                  int(n_gas), box, _p(start, _i64), _p(found, _u32), len(found))
+        return start, found[: start[-1]]
+
+    def density(self, targets, des_ngb=32.0, ngb_tol=0.05, h_start=None, box=0.0, n_dims=3, cond_prev=None,
+                cache=False):
+        t = _targets(targets)
+        nt = len(t)
+        h, rho = np.zeros(nt), np.zeros(nt)
+        nngb, iters = np.zeros(nt, np.int32), np.zeros(nt, np.int32)
+        hs = _f64(h_start) if h_start is not None else None
+        cp = _f64(cond_prev) if cond_prev is not None else None
+        cs = np.zeros(nt + 1, np.int64) if cache else None
+        args = [self.h, nt, _p(t, _u32), des_ngb, ngb_tol, _p(hs, _d), box, n_dims, _p(cp, _d), _p(h, _d),
+                _p(rho, _d), nngb.ctypes.data, iters.ctypes.data]
+        self.lib.L.ref_density(*args, _p(cs, _i64), None, 0)
+        out = {"h": h, "rho": rho, "nngb": nngb, "iters": iters}
+        if cache:
+            flat = np.zeros(max(int(cs[-1]), 1), np.uint32)
+            self.lib.L.ref_density(*args, _p(cs, _i64), _p(flat, _u32), len(flat))
+            out["cache_start"], out["cache_flat"] = cs, flat[: cs[-1]]
         return out
 
     def vel_moments(self):

@@ -288,3 +288,76 @@ int ref_open_node(double r_sq, double len, double l_open, double node_mass, doub
 }
 
 }  // extern "C"
+
+// ---- neighbour search and the density solve (shmem/hydro.h:65-117, hydro.cc:37-327) --------------
+#include "hydro.h"
+
+namespace {
+void to_csr(const std::vector<std::vector<uint32_t>>& lists, int64_t* start, uint32_t* found, int64_t cap) {
+    int64_t tot = 0;
+    start[0] = 0;
+    for (size_t c = 0; c < lists.size(); ++c) start[c + 1] = (tot += (int64_t)lists[c].size());
+    if (found && tot <= cap)
+        for (size_t c = 0; c < lists.size(); ++c)
+            if (!lists[c].empty()) std::memcpy(found + start[c], lists[c].data(), lists[c].size() * 4);
+}
+}  // namespace
+
+extern "C" {
+
+// Tree::t_since_build (the staleness pad of the search prune).
+void ref_set_elapsed(void* p, double elapsed) { static_cast<RefHandle*>(p)->T.t_since_build = elapsed; }
+
+// Tree::init_hmax (tree.cc:332-338) and a copy of the result (nnodes floats; may be null).
+void ref_init_hmax(void* p, const double* h, int64_t n_gas, float* hmax_out) {
+    RefHandle* H = static_cast<RefHandle*>(p);
+    std::vector<double> hv(h, h + n_gas);
+    H->T.init_hmax(hv, (size_t)n_gas);
+    if (hmax_out) std::memcpy(hmax_out, H->T.hmax.data(), H->T.nnodes() * 4);
+}
+
+// Tree::raise_hmax (tree.cc:293-302) for a list of (leaf, h).
+void ref_raise_hmax(void* p, int64_t n, const int* leaf, const double* h) {
+    RefHandle* H = static_cast<RefHandle*>(p);
+    for (int64_t e = 0; e < n; ++e) H->T.raise_hmax(leaf[e], h[e]);
+}
+
+// ngb_search for each centre (hydro.cc:37-108); the lists as CSR (start: n+1, found: start[n]
+// entries when cap suffices).  mode 0: gather (r < radius); 1: reverse, ngb_search_reverse
+// (hydro.cc:110-148) with h_i = radius and the particles' h (n_gas); 2: both, gather first.
+void ref_ngb_search(void* p, int64_t n, const double* cx, const double* cy, const double* cz, const double* radius,
+                    int mode, const double* h, int64_t n_gas, double box, int64_t* start, uint32_t* found,
+                    int64_t cap) {
+    RefHandle* H = static_cast<RefHandle*>(p);
+    std::vector<std::vector<uint32_t>> lists((size_t)n);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t c = 0; c < n; ++c) {
+        const Vec3d ce{cx[c], cy[c], cz[c]};
+        if (mode == 0 || mode == 2) ngb_search(H->T, H->P, ce, radius[c], lists[(size_t)c], box);
+        if (mode == 1 || mode == 2) ngb_search_reverse(H->T, H->P, h, (size_t)n_gas, ce, radius[c], lists[(size_t)c], box);
+    }
+    to_csr(lists, start, found, cap);
+}
+
+// density (hydro.cc:150-327) with its neighbour cache as CSR (cache_start may be null).
+void ref_density(void* p, int64_t nt, const uint32_t* targets, double des_ngb, double ngb_tol, const double* h_start,
+                 double box, int n_dims, const double* cond_prev, double* h, double* rho, int32_t* nngb,
+                 int32_t* iters, int64_t* cache_start, uint32_t* cache_flat, int64_t cache_cap) {
+    RefHandle* H = static_cast<RefHandle*>(p);
+    std::vector<uint32_t> tg(targets, targets + nt);
+    std::vector<double> hs;
+    if (h_start) hs.assign(h_start, h_start + nt);
+    NeighborCache cache;
+    DensityResult R = density(H->T, H->P, tg, des_ngb, ngb_tol, hs, box, n_dims, cache_start ? &cache : nullptr,
+                              nullptr, cond_prev);
+    std::memcpy(h, R.h.data(), nt * 8);
+    std::memcpy(rho, R.rho.data(), nt * 8);
+    for (int64_t t = 0; t < nt; ++t) { nngb[t] = R.nngb[(size_t)t]; iters[t] = R.iters[(size_t)t]; }
+    if (cache_start) {
+        for (int64_t t = 0; t <= nt; ++t) cache_start[t] = (int64_t)cache.start[(size_t)t];
+        if (cache_flat && (int64_t)cache.flat.size() <= cache_cap)
+            std::memcpy(cache_flat, cache.flat.data(), cache.flat.size() * 4);
+    }
+}
+
+}  // extern "C"

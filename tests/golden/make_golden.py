@@ -60,6 +60,67 @@ def gas_scenario(R):
     return out
 
 
+def ngb_scenario(R):
+    """Neighbour search and the density solve (shmem/hydro.cc) on a Plummer sphere whose first 6000
+    particles are gas (type 0) and the rest stars (type 4), every 53rd massless: the reference's
+    gather / reverse / pair lists for seeded centres and radii, its per-node hmax, and its density
+    solve from a cold start (with the neighbour cache), from a warm start, and with a condition-
+    number history; plus a periodic box."""
+    P = ics.plummer(n=8192, seed=21, soft=0.01)
+    P["m"][::53] = 0.0
+    n_gas = 6000
+    P["type"] = np.where(np.arange(8192) < n_gas, 0, 4).astype(np.uint8)
+    P["zeta"] = np.zeros(8192)
+    out = {k: P[k] for k in ("x", "y", "z", "m", "type")}
+    out["n_gas"] = np.array([n_gas])
+    T = R.build_gas(P)
+    ob = T.order()[0]
+    tg = ob[ob < n_gas].copy()
+    out["targets"] = tg
+    d = T.density(tg, 32.0, 0.05, cache=True)
+    for k in ("h", "rho", "nngb", "iters", "cache_start", "cache_flat"):
+        out[f"cold_{k}"] = d[k]
+    w = T.density(tg, 32.0, 0.05, h_start=1.1 * d["h"])
+    for k in ("h", "rho", "nngb", "iters"):
+        out[f"warm_{k}"] = w[k]
+    rng = np.random.default_rng(77)
+    cond = np.where(rng.uniform(size=8192) < 0.2, rng.uniform(100, 3000, 8192), 10.0)
+    out["cond"] = cond
+    c = T.density(tg, 32.0, 0.05, cond_prev=cond)
+    for k in ("h", "rho", "nngb", "iters"):
+        out[f"cond_{k}"] = c[k]
+    h = np.zeros(8192)
+    h[tg] = d["h"]
+    out["h_part"] = h
+    out["hmax"] = T.init_hmax(h[:n_gas], n_gas)
+    cen = [rng.uniform(-1.5, 1.5, 400) for _ in range(3)]
+    cen[0][:100], cen[1][:100], cen[2][:100] = P["x"][tg[:100]], P["y"][tg[:100]], P["z"][tg[:100]]
+    rad = rng.uniform(0.02, 0.6, 400)
+    rad[:100] = d["h"][:100]
+    for k, v in zip("xyz", cen):
+        out[f"c{k}"] = v
+    out["radius"] = rad
+    for mode, name in ((0, "gather"), (1, "reverse"), (2, "pairs")):
+        st, f = T.ngb_search(*cen, rad, mode=mode, h=h, n_gas=n_gas)
+        out[f"{name}_start"], out[f"{name}_found"] = st, f
+    # periodic box of side 2: the sphere folded into it
+    Q = ics.plummer(n=8192, seed=22, soft=0.01)
+    for k in "xyz":
+        Q[k] = np.mod(Q[k], 2.0)
+    for k in "xyz":
+        out[f"box_{k}"] = Q[k]
+    out["box_m"] = Q["m"]
+    TB = R.build(Q)
+    obb = TB.order()[0]
+    st, f = TB.ngb_search(*cen, 0.5 * rad, box=2.0)
+    out["box_gather_start"], out["box_gather_found"] = st, f
+    b = TB.density(obb[:3000], 32.0, 0.05, box=2.0)
+    out["box_targets"] = obb[:3000].copy()
+    for k in ("h", "rho", "nngb", "iters"):
+        out[f"box_{k}"] = b[k]
+    return out
+
+
 def main():
     R = Reference()
     R.set_threads(1)
@@ -173,6 +234,10 @@ def main():
     G_ = gas_scenario(R)
     for k, v in G_.items():
         out[f"gas_{k}"] = v
+
+    # ---- neighbour search and the density solve (shmem/hydro.cc:37-327) ------------------------
+    for k, v in ngb_scenario(R).items():
+        out[f"ngb_{k}"] = v
 
     # ---- collocated particles: the level-20 leaf (tree.cc:89) ----------------------------------
     Q = ics.plummer(n=600, seed=7, soft=0.02)

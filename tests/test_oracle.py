@@ -280,3 +280,54 @@ def test_gas_terms_and_sink_rule_change_the_forces(oracle, golden):
     for q, fp in ((0.25, -12 * 0.25 + 18 * 0.0625), (0.75, -6 * 0.0625)):
         assert oracle.L.or_kernel_dwdr(q * h, h) == pytest.approx(8 / (np.pi * h ** 3) * fp / h, rel=1e-14)
     assert oracle.L.or_kernel_dwdr(h, h) == 0.0
+
+
+def ngb_particles(golden, prefix="ngb"):
+    P = {k: golden[f"{prefix}_{k}"] for k in ("x", "y", "z", "m")}
+    P["soft"] = np.full_like(P["m"], 0.01)
+    return P
+
+
+def test_neighbour_search_matches_golden(oracle, golden):
+    """The restatement of ngb_search, ngb_search_reverse and init_hmax (hydro.cc:37-148,
+    tree.cc:287-338) against the reference's lists: bit-exact, same order (tree order)."""
+    P = ngb_particles(golden)
+    T = oracle.build(P)
+    n_gas = int(golden["ngb_n_gas"][0])
+    h = golden["ngb_h_part"]
+    assert np.array_equal(T.init_hmax(h[:n_gas], n_gas), golden["ngb_hmax"])
+    cen = [golden[f"ngb_c{k}"] for k in "xyz"]
+    for mode, name in ((0, "gather"), (1, "reverse"), (2, "pairs")):
+        st, f = T.ngb_search(*cen, golden["ngb_radius"], mode=mode, h=h, n_gas=n_gas)
+        assert np.array_equal(st, golden[f"ngb_{name}_start"]), name
+        assert np.array_equal(f, golden[f"ngb_{name}_found"]), name
+    Q = {k: golden[f"ngb_box_{k}"] for k in ("x", "y", "z", "m")}
+    Q["soft"] = np.full_like(Q["m"], 0.01)
+    TB = oracle.build(Q)
+    st, f = TB.ngb_search(*cen, 0.5 * golden["ngb_radius"], box=2.0)
+    assert np.array_equal(st, golden["ngb_box_gather_start"]) and np.array_equal(f, golden["ngb_box_gather_found"])
+
+
+@pytest.mark.parametrize("case", ["cold", "warm", "cond", "box"])
+def test_density_matches_golden(oracle, golden, case):
+    """The restatement of the density solve (hydro.cc:150-327): the same iteration counts and
+    neighbour counts, h and rho to 1e-12 (FP64 in the same order; the reference's compiler may
+    contract multiply-adds)."""
+    if case == "box":
+        P = ngb_particles(golden, "ngb_box")
+        T = oracle.build(P)
+        d = T.density(golden["ngb_box_targets"], 32.0, 0.05, box=2.0)
+    else:
+        P = ngb_particles(golden)
+        T = oracle.build(P)
+        tg = golden["ngb_targets"]
+        kw = {"type": golden["ngb_type"]}
+        if case == "warm":
+            kw["h_start"] = 1.1 * golden["ngb_cold_h"]
+        if case == "cond":
+            kw["cond_prev"] = golden["ngb_cond"]
+        d = T.density(tg, 32.0, 0.05, **kw)
+    assert np.array_equal(d["iters"], golden[f"ngb_{case}_iters"])
+    assert np.array_equal(d["nngb"], golden[f"ngb_{case}_nngb"])
+    np.testing.assert_allclose(d["h"], golden[f"ngb_{case}_h"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(d["rho"], golden[f"ngb_{case}_rho"], rtol=1e-12, atol=0)
