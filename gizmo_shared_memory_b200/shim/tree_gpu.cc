@@ -1,6 +1,7 @@
 // shmem:: tree functions implemented on libgt (include/gt.h).  See tree.h in this directory for
 // the differences a caller can observe.
 #include "tree.h"
+#include "hydro.h"
 
 #include <cfloat>
 #include <cstdio>
@@ -149,14 +150,17 @@ Tree build(const Particles& P, BuildTimes* bt, const double* const* vel, bool wa
 // straight to the device.
 struct ReuseQueue {
     struct Buf {
-        std::vector<int32_t> kick_leaf, vmax_leaf, soft_leaf, shift_leaf;
-        std::vector<double> kick_dp, soft_val, shift_m, shift_dx;
+        std::vector<int32_t> kick_leaf, vmax_leaf, soft_leaf, shift_leaf, hmax_leaf;
+        std::vector<double> kick_dp, soft_val, shift_m, shift_dx, hmax_val;
         std::vector<float> vmax_val;
         double kick_tau = 0.0;
     };
     std::vector<Buf> bufs;
     std::mutex mu;
     bool moved = false;  // events or a refresh since the build: the walk needs current particles
+    // the per-centre neighbour search uploads the particles once per change of the tree
+    uint64_t gen = 0, search_gen = 0;
+    std::mutex search_mu;
     ReuseQueue() : bufs((size_t)std::max(1, omp_get_max_threads())) {}
     Buf& mine() {
         const size_t t = (size_t)omp_get_thread_num();
@@ -194,6 +198,10 @@ void flush(const Tree& T) {
             check(gt_tree_events(context(), h, GT_EVENT_SHIFT, (int64_t)b.shift_leaf.size(), b.shift_leaf.data(),
                                  b.shift_m.data(), b.shift_dx.data(), nullptr, nullptr, 0.0, 0.0, GT_MEM_HOST),
                   "gt_tree_events");
+        if (!b.hmax_leaf.empty())
+            check(gt_tree_events(context(), h, GT_EVENT_HMAX, (int64_t)b.hmax_leaf.size(), b.hmax_leaf.data(),
+                                 b.hmax_val.data(), nullptr, nullptr, nullptr, 0.0, 0.0, GT_MEM_HOST),
+                  "gt_tree_events");
         b = ReuseQueue::Buf{};
     }
 }
@@ -228,6 +236,12 @@ void climb_max(std::vector<float>& arr, const std::vector<int>& parent, int leaf
 
 }  // namespace
 
+static void touch(const Tree& T) {
+    ReuseQueue& Q = queue_of(T);
+    Q.moved = true;
+    ++Q.gen;
+}
+
 static void need_gpu(const Tree& T) {
     if (!T.gpu) throw std::runtime_error("shmem (GPU): the Tree was not built by shmem::build");
 }
@@ -243,9 +257,11 @@ static void prepare_walk(const Tree& T, const Particles& P, const LazyDrift* laz
         for (uint32_t q : T.orderbuf)
             if (lazy->last[q] < lazy->target) lazy->catch_up(lazy->ctx, q);
     ReuseQueue& Q = queue_of(T);
-    if (Q.moved || drift)
+    if (Q.moved || drift) {
         check(gt_tree_particles(context(), T.gpu.get(), P.x.data(), P.y.data(), P.z.data(), P.m.data(),
                                 soft_or_null(P), GT_MEM_HOST), "gt_tree_particles");
+        Q.search_gen = Q.gen;
+    }
     // types and zeta as the walk reads them now (the engine updates zeta between steps): the gas
     // pair rule and the per-node sink counts of sink-direct opening
     if (!P.type.empty() || !P.zeta.empty()) {
@@ -348,8 +364,26 @@ void Tree::raise_vmax(int leaf_node, float speed) {
     b.vmax_leaf.push_back(leaf_node);
     b.vmax_val.push_back(speed);
 }
-void Tree::raise_hmax(int, double) { unsupported("Tree::raise_hmax (the neighbour search)"); }
-void Tree::init_hmax(const std::vector<double>&, size_t) { unsupported("Tree::init_hmax (the neighbour search)"); }
+// rounded up to float, so the prune stays one-sided (tree.cc:288-291)
+static float up_float(double h) {
+    const float f = (float)h;
+    return ((double)f < h) ? std::nextafter(f, 1e30f) : f;
+}
+void Tree::raise_hmax(int leaf_node, double h) {
+    if (hmax.empty() || leaf_node < 0) return;  // before init_hmax: nothing to raise (tree.cc:294)
+    climb_max(hmax, parent, leaf_node, up_float(h));
+    auto& b = queue_of(*this).mine();
+    b.hmax_leaf.push_back(leaf_node);
+    b.hmax_val.push_back(h);
+}
+void Tree::init_hmax(const std::vector<double>& h, size_t n_gas) {
+    flush(*this);
+    const size_t n = std::min(std::min(n_gas, h.size()), leaf_of.size());
+    hmax.assign(nnodes(), 0.0f);
+    for (size_t i = 0; i < n; ++i)
+        if (h[i] > 0 && leaf_of[i] >= 0) climb_max(hmax, parent, leaf_of[i], up_float(h[i]));
+    check(gt_tree_hmax(context(), gpu.get(), h.data(), (int64_t)n, GT_MEM_HOST), "gt_tree_hmax");
+}
 void Tree::raise_soft(int leaf_node, double s) {
     if (leaf_node < 0) return;
     auto& b = queue_of(*this).mine();
@@ -366,7 +400,7 @@ void Tree::raise_pad(int leaf_node, double d) {
     float leaf_pad = (float)((double)xpad[leaf_node] + d);
     if ((double)leaf_pad < (double)xpad[leaf_node] + d) leaf_pad = std::nextafter(leaf_pad, 1e30f);
     for (int no = leaf_node; no >= 0 && xpad[no] < leaf_pad; no = parent[no]) xpad[no] = leaf_pad;
-    queue_of(*this).moved = true;
+    touch(*this);
 }
 void Tree::kick_node(int leaf_node, const Vec3d& dp, double tau) {
     if (dp_x.empty() || leaf_node < 0) return;  // no vcom, nothing to keep current (tree.cc:212)
@@ -375,7 +409,7 @@ void Tree::kick_node(int leaf_node, const Vec3d& dp, double tau) {
     b.kick_tau = tau;
     b.kick_leaf.push_back(leaf_node);
     for (int k = 0; k < 3; ++k) b.kick_dp.push_back(dp[k]);
-    queue_of(*this).moved = true;
+    touch(*this);
 }
 void Tree::mass_event(int leaf_node, double dm, const Vec3d& x, const Vec3d& v, double tau, double box) {
     if (dp_x.empty() || leaf_node < 0 || dm == 0.0) return;
@@ -384,7 +418,7 @@ void Tree::mass_event(int leaf_node, double dm, const Vec3d& x, const Vec3d& v, 
     const double xx[3] = {x[0], x[1], x[2]}, vv[3] = {v[0], v[1], v[2]};
     check(gt_tree_events(context(), gpu.get(), GT_EVENT_MASS, 1, &lf, &dm, xx, vv, nullptr, tau, box, GT_MEM_HOST),
           "gt_tree_events");
-    queue_of(*this).moved = true;
+    touch(*this);
 }
 void Tree::shift_node(int leaf_node, double m, const Vec3d& dx) {
     if (dp_x.empty() || leaf_node < 0) return;
@@ -392,7 +426,7 @@ void Tree::shift_node(int leaf_node, double m, const Vec3d& dx) {
     b.shift_leaf.push_back(leaf_node);
     b.shift_m.push_back(m);
     for (int k = 0; k < 3; ++k) b.shift_dx.push_back(dx[k]);
-    queue_of(*this).moved = true;
+    touch(*this);
 }
 double Tree::node_mass(int no) const { return node_state(*this, 0.0).mass[no]; }
 Vec3d Tree::node_com(int no, double tau) const {
@@ -406,7 +440,7 @@ Vec3d Tree::node_vel(int no) const {
 void Tree::refresh_walk_nodes(double tau) {
     flush(*this);
     check(gt_tree_refresh(context(), gpu.get(), tau), "gt_tree_refresh");
-    if (tau != 0.0) queue_of(*this).moved = true;
+    if (tau != 0.0) touch(*this);
 }
 
 // Structural audit of the downloaded tree (the topology and coverage parts of the reference's
@@ -455,6 +489,131 @@ long long audit_tree(const Tree& T, const Particles& P, const double*, size_t, c
     for (size_t p = 0; p < N; ++p)
         if (!seen_part[p] && P.m[p] > 0) { fail("particle unreachable from the root", (long long)p, 0); break; }
     return bad;
+}
+
+// ---- neighbour search and the density solve (hydro.h) ------------------------------------------
+
+void ngb_counters(long long& calls, long long& nodes, long long& examined, long long& kept, long long& pad_nodes,
+                  bool) {
+    calls = nodes = examined = kept = pad_nodes = 0;
+}
+void hiter_counters(long long out[8], bool) {
+    for (int i = 0; i < 8; ++i) out[i] = 0;
+}
+
+// Before a per-centre search: queued events to the device, lazy catch-up of every particle behind
+// the target, and the particles' current state on the device once per change of the tree.
+static void prepare_search(const Tree& T, const Particles& P, const LazyDrift* lazy) {
+    flush(T);
+    ReuseQueue& Q = queue_of(T);
+    std::lock_guard<std::mutex> lk(Q.search_mu);
+    bool behind = false;
+    if (lazy && lazy->catch_up && lazy->last)
+        for (uint32_t q : T.orderbuf)
+            if (lazy->last[q] < lazy->target) {
+                lazy->catch_up(lazy->ctx, q);
+                behind = true;
+            }
+    if (behind || (Q.moved && Q.search_gen != Q.gen)) {
+        check(gt_tree_particles(context(), T.gpu.get(), P.x.data(), P.y.data(), P.z.data(), P.m.data(),
+                                soft_or_null(P), GT_MEM_HOST), "gt_tree_particles");
+        Q.search_gen = Q.gen;
+    }
+}
+
+// One centre through the batched search: a first call with the thread's buffer, a second with
+// room for the total when the first overflowed.
+static void search_one(const Tree& T, const gt_ngb_options& o, const Vec3d& c, double radius,
+                       std::vector<uint32_t>& found) {
+    thread_local std::vector<uint32_t> buf(512);
+    const double cx = c[0], cy = c[1], cz = c[2];
+    int64_t start[2] = {0, 0}, tot = 0;
+    int st = gt_ngb_search(context(), T.gpu.get(), 1, &cx, &cy, &cz, &radius, &o, GT_MEM_HOST, start, buf.data(),
+                           (int64_t)buf.size(), &tot);
+    if (st == GT_ERR_OVERFLOW) {
+        buf.resize((size_t)tot * 2);
+        st = gt_ngb_search(context(), T.gpu.get(), 1, &cx, &cy, &cz, &radius, &o, GT_MEM_HOST, start, buf.data(),
+                           (int64_t)buf.size(), &tot);
+    }
+    check(st, "gt_ngb_search");
+    found.insert(found.end(), buf.begin(), buf.begin() + tot);
+}
+
+void ngb_search(const Tree& T, const Particles& P, const Vec3d& centre, double radius, std::vector<uint32_t>& found,
+                double box, const LazyDrift* lazy) {
+    need_gpu(T);
+    prepare_search(T, P, lazy);
+    gt_ngb_options o;
+    gt_ngb_options_default(&o);
+    o.box = box;
+    o.elapsed = T.t_since_build;
+    search_one(T, o, centre, radius, found);
+}
+
+void ngb_search_reverse(const Tree& T, const Particles& P, const double* h, size_t n_gas, const Vec3d& centre,
+                        double h_i, std::vector<uint32_t>& found, double box, const LazyDrift* lazy) {
+    need_gpu(T);
+    if (T.hmax.empty()) throw std::runtime_error("shmem (GPU): ngb_search_reverse needs Tree::init_hmax first");
+    prepare_search(T, P, lazy);
+    gt_ngb_options o;
+    gt_ngb_options_default(&o);
+    o.mode = GT_NGB_REVERSE;
+    o.box = box;
+    o.elapsed = T.t_since_build;
+    o.n_gas = (int64_t)n_gas;
+    o.h = h;
+    search_one(T, o, centre, h_i, found);
+}
+
+DensityResult density(const Tree& T, const Particles& P, const std::vector<uint32_t>& targets, double des_ngb,
+                      double ngb_tol, const std::vector<double>& h_start, double box, int n_dims, NeighborCache* cache,
+                      const LazyDrift* lazy, const double* cond_prev) {
+    need_gpu(T);
+    prepare_walk(T, P, lazy);  // current particles and types (the solve counts gas neighbours only)
+    const size_t nt = targets.size();
+    DensityResult R;
+    R.h.assign(nt, 0.0); R.rho.assign(nt, 0.0); R.nngb.assign(nt, 0); R.iters.assign(nt, 0);
+    if (cache) { cache->clear(); cache->start.assign(nt + 1, 0); }
+    if (!h_start.empty() && h_start.size() < nt)
+        throw std::runtime_error("shmem (GPU): density h_start has fewer entries than targets");
+    if (nt) {
+        gt_density_options o;
+        gt_density_options_default(&o);
+        o.des_ngb = des_ngb;
+        o.ngb_tol = ngb_tol;
+        o.box = box;
+        o.elapsed = T.t_since_build;
+        o.n_dims = n_dims;
+        o.face_correction = getenv("SHMEM_NO_FACECORR") ? 0 : 1;  // the reference's A/B switch
+        o.h_start = h_start.empty() ? nullptr : h_start.data();
+        o.cond_prev = cond_prev;
+        std::vector<int32_t> nngb(nt), iters(nt);
+        check(gt_density(context(), T.gpu.get(), (int64_t)nt, targets.data(), &o, GT_MEM_HOST, R.h.data(),
+                         R.rho.data(), nngb.data(), iters.data()), "gt_density");
+        for (size_t t = 0; t < nt; ++t) { R.nngb[t] = nngb[t]; R.iters[t] = iters[t]; }
+    }
+    if (cache) {
+        // every target's list at its final h: one batched search
+        if (nt) {
+            std::vector<double> cx(nt), cy(nt), cz(nt);
+            for (size_t t = 0; t < nt; ++t) { cx[t] = P.x[targets[t]]; cy[t] = P.y[targets[t]]; cz[t] = P.z[targets[t]]; }
+            gt_ngb_options o;
+            gt_ngb_options_default(&o);
+            o.box = box;
+            o.elapsed = T.t_since_build;
+            std::vector<int64_t> start(nt + 1);
+            int64_t tot = 0;
+            const int st = gt_ngb_search(context(), T.gpu.get(), (int64_t)nt, cx.data(), cy.data(), cz.data(),
+                                         R.h.data(), &o, GT_MEM_HOST, start.data(), nullptr, 0, &tot);
+            check(st, "gt_ngb_search");
+            cache->flat.resize((size_t)tot);
+            check(gt_ngb_search(context(), T.gpu.get(), (int64_t)nt, cx.data(), cy.data(), cz.data(), R.h.data(), &o,
+                                GT_MEM_HOST, start.data(), cache->flat.data(), tot, &tot), "gt_ngb_search");
+            for (size_t t = 0; t <= nt; ++t) cache->start[t] = (size_t)start[t];
+        }
+        cache->valid = true;
+    }
+    return R;
 }
 
 }  // namespace shmem

@@ -138,3 +138,32 @@ def test_gas_and_sinks_through_the_shim_match_the_reference(tmp_path):
         x, y = g[lo:hi].reshape(3, k), r[lo:hi].reshape(3, k)
         e = np.sqrt(((x - y) ** 2).sum(0)) / np.sqrt((y ** 2).sum(0))
         assert np.median(e) <= 1e-5 and np.quantile(e, 0.99) <= 2e-3, (what, np.median(e), np.quantile(e, 0.99))
+
+
+@pytest.mark.gpu
+def test_bench_density_through_the_shim_matches_the_reference(tmp_path):
+    """shmem/bench_density.cc compiled unchanged against the shim (GPU density solve and neighbour
+    search) and against the reference (oracle/_ref): its checksums of h and rho agree to 1e-9, and
+    the neighbour statistics it prints from per-target searches at the converged h (kept per
+    target, leaf groups, the summed and union candidate counts) are identical."""
+    import re
+
+    from gizmo_shared_memory_b200 import ics
+
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "bench_density")
+    if not os.path.exists(ref_bin):
+        pytest.skip("oracle/_ref/bench_density not built (reference sources unavailable at build time)")
+    P, vel = ics.plummer_state(n=30000, seed=17)
+    state = tmp_path / "state.bin"
+    ics.write_state(str(state), P, vel)
+    txt = {}
+    for name, exe in (("gpu", binary("bench_density")), ("ref", ref_bin)):
+        r = subprocess.run([exe, str(state), "32", "0.05"], capture_output=True, text=True, timeout=900,
+                           env=dict(os.environ, OMP_NUM_THREADS="4"))
+        assert r.returncode == 0, (name, r.stdout[-2000:], r.stderr[-2000:])
+        txt[name] = r.stdout
+    sums = {k: [float(v) for v in re.search(r"sum_h=(\S+)\s+sum_rho=(\S+)", t).groups()] for k, t in txt.items()}
+    np.testing.assert_allclose(sums["gpu"], sums["ref"], rtol=1e-9)
+    for pat in (r"([0-9.]+) kept/target", r"(\d+) leaf groups, (\d+) singleton", r"sum\(examined\)=(\d+)\s+union\(examined\)=(\d+)"):
+        a, b = (re.search(pat, txt[k]).groups() for k in ("gpu", "ref"))
+        assert a == b, (pat, a, b)
