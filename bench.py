@@ -613,14 +613,110 @@ def run_batch_arm(args):
     plan.free()
 
 
+def run_density_arm(args):
+    """The density solve (shmem::density, hydro.cc:150-327) on the GPU tree: every particle a
+    target, warm-started from the converged h of a first solve (what every step after the first
+    does), DesNumNgb 32, tolerance 0.05.  value = targets / device time with everything resident;
+    e2e = the same call with host arrays (targets and h_start in, h, rho, counts out).  The CPU
+    baseline is the reference's own density on a bounded sample of the same targets."""
+    import torch
+
+    import gizmo_shared_memory_b200 as g
+
+    torch.cuda.set_device(0)
+    wl = args.workload[len("density_"):]
+    P = make_workload(wl)
+    n = len(P["m"])
+    dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
+    ctx = g.Context(0, torch_stream=True)
+    T = ctx.build(dev, key_mode=g.GT_KEY_MORTON)
+    dl = T.download()
+    ob = dl["orderbuf"]
+    nl = len(ob)
+    # first guess from each target's leaf: DesNumNgb at the leaf's density
+    leaf = dl["leaf_of"][ob]
+    cnt = (dl["phi"] - dl["plo"])[leaf]
+    h0 = 0.8 * dl["size"][leaf] * np.cbrt(16.0 / np.maximum(cnt, 1))
+    tg = torch.as_tensor(ob.view(np.int32), device="cuda")  # uint32 indices, passed as raw 32-bit words
+    first = ctx.density(T, tg, h_start=torch.as_tensor(h0, device="cuda"))
+    hconv = first["h"].clone()
+    for _ in range(max(args.warmup, 3)):
+        ctx.density(T, tg, h_start=hconv)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = ctx.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for _ in range(args.steps):
+        e0.record(stream)
+        r = ctx.density(T, tg, h_start=hconv)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    launches = (ctx.launches() - l0) // args.steps
+    clocks = sampler.stop()
+    t_step = float(np.mean(ms)) / 1e3
+    iters = r["iters"].float().mean().item()
+    # end to end with host arrays
+    hh = hconv.cpu().numpy()
+    ctx.density(T, ob, h_start=hh)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rh = ctx.density(T, ob, h_start=hh)
+    t_e2e = (time.perf_counter() - t0) / args.steps
+    cpu = None
+    if not args.no_cpu:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            from oracle import Reference, reference_available
+
+            if reference_available():
+                R = Reference()
+                TR = R.build(P)
+                k = min(200000, nl)
+                step = max(1, nl // k)
+                sel, hs = ob[::step][:k], hh[::step][:k]
+                TR.density(sel[:1000], 32.0, 0.05, h_start=hs[:1000])
+                c0 = time.perf_counter()
+                TR.density(sel, 32.0, 0.05, h_start=hs)
+                tc = time.perf_counter() - c0
+                cpu = {"value": k / tc, "unit": "targets/s", "cores": os.cpu_count(), "kind": "reference",
+                       "sample": f"{k} targets (every {step}th in tree order), warm start from the GPU's converged h, "
+                                 "shmem::density with every host thread"}
+        except Exception as e:  # the reference library is optional on the box
+            log("cpu baseline skipped:", e)
+    line = {
+        "metric": "density-solve targets/s (warm start)", "value": nl / t_step, "unit": "targets/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "n": n, "description": WORKLOADS[wl]["desc"],
+                   "des_ngb": 32, "ngb_tol": 0.05, "start": "warm: the converged h of a first solve",
+                   "l2": f"inputs larger than L2: {n * 32 / 2**20:.0f} MiB of particles"},
+        "iterations_mean": iters, "first_solve_iterations_mean": first["iters"].float().mean().item(),
+        "kept_mean": float(rh["nngb"].mean()),
+        "roofline": {"bound": "latency", "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None,
+                     "kernel": "density_kernel",
+                     "note": "one thread per target follows the tree: a dependent chain of node and particle loads"},
+        "e2e": {"value": nl / t_e2e, "unit": "targets/s", "h2d_bytes_per_step": nl * 12,
+                "d2h_bytes_per_step": nl * 24},
+        "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["plummer_batch_256"], default="clustered_16m",
-                    help="plummer_batch_256: the batched many-system case (forest + autotuner + graph)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["plummer_batch_256"] +
+                    ["density_" + w for w in ("galaxy_4m", "clustered_16m")], default="clustered_16m",
+                    help="plummer_batch_256: the batched many-system case (forest + autotuner + graph); "
+                         "density_*: the density solve on that workload")
     ap.add_argument("--alpha", type=float, default=None)
     ap.add_argument("--group", choices=["leaf", "node", "batch"], default="batch",
                     help="leaf: accel_grouped batch 0; batch: windows of --group-max consecutive "
@@ -639,6 +735,8 @@ def main():
         run_reference_arm(args)
     elif args.workload == "plummer_batch_256":
         run_batch_arm(args)
+    elif args.workload.startswith("density_"):
+        run_density_arm(args)
     else:
         run_gpu_arm(args)
 

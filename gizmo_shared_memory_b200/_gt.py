@@ -644,21 +644,33 @@ class Context:
 
     def density(self, tree: Tree, targets, des_ngb=32.0, ngb_tol=0.05, h_start=None, box=0.0, n_dims=3,
                 cond_prev=None, face_correction=True, elapsed=0.0):
-        """shmem::density on the GPU: dict of h, rho, nngb, iters per target (host arrays)."""
-        t = np.ascontiguousarray(targets, np.uint32)
-        nt = len(t)
+        """shmem::density on the GPU: dict of h, rho, nngb, iters per target.  Host arrays, or,
+        when targets is a CUDA tensor, device tensors throughout (h_start and cond_prev too)."""
+        dev = _is_dev(targets)
         o = DensityOptions()
         L = load_library()
         L.gt_density_options_default(C.byref(o))
         o.des_ngb, o.ngb_tol, o.box, o.n_dims = des_ngb, ngb_tol, box, n_dims
         o.face_correction, o.elapsed = int(face_correction), elapsed
-        hs = None if h_start is None else np.ascontiguousarray(h_start, np.float64)
-        cp = None if cond_prev is None else np.ascontiguousarray(cond_prev, np.float64)
+        if dev:
+            import torch
+
+            t, hs, cp = targets, h_start, cond_prev
+            nt = int(t.numel())
+            h = torch.empty(nt, dtype=torch.float64, device=t.device)
+            rho = torch.empty_like(h)
+            nngb = torch.empty(nt, dtype=torch.int32, device=t.device)
+            iters = torch.empty_like(nngb)
+        else:
+            t = np.ascontiguousarray(targets, np.uint32)
+            nt = len(t)
+            hs = None if h_start is None else np.ascontiguousarray(h_start, np.float64)
+            cp = None if cond_prev is None else np.ascontiguousarray(cond_prev, np.float64)
+            h, rho = np.zeros(nt), np.zeros(nt)
+            nngb, iters = np.zeros(nt, np.int32), np.zeros(nt, np.int32)
         o.h_start, o.cond_prev = _ptr(hs), _ptr(cp)
-        h, rho = np.zeros(nt), np.zeros(nt)
-        nngb, iters = np.zeros(nt, np.int32), np.zeros(nt, np.int32)
-        self._check(L.gt_density(self.h, tree.h, nt, _ptr(t), C.byref(o), GT_MEM_HOST, _ptr(h), _ptr(rho),
-                                 _ptr(nngb), _ptr(iters)))
+        self._check(L.gt_density(self.h, tree.h, nt, _ptr(t), C.byref(o), GT_MEM_DEVICE if dev else GT_MEM_HOST,
+                                 _ptr(h), _ptr(rho), _ptr(nngb), _ptr(iters)))
         return {"h": h, "rho": rho, "nngb": nngb, "iters": iters}
 
     def velocity_moments(self, tree: Tree):
