@@ -220,43 +220,53 @@ struct DensArgs {
     int *nngb, *iters;
 };
 
-// One evaluation at h: the sums over the GAS neighbours inside h, in tree order (hydro.cc:205-222).
-__device__ void dens_eval(const DensArgs& a, double px, double py, double pz, double h, DensSums& s) {
+__device__ __forceinline__ void dens_zero(DensSums& s) {
     s.wsum = s.dwdh = s.rho = 0.0;
     for (int c = 0; c < 6; ++c) s.mom[c] = 0.0;
     s.face[0] = s.face[1] = s.face[2] = 0.0;
     s.inside = 0;
+}
+
+// One gas neighbour at offset (dx, dy, dz) from the target, inside h: its kernel weight and the
+// sums the solve reads (hydro.cc:209-222).
+__device__ __forceinline__ void dens_add(double dx, double dy, double dz, double m, double h, double norm, int dim,
+                                         DensSums& s) {
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const double q = r / h;
+    double w = 0.0, dh = 0.0;
+    if (q < 1.0) {
+        double f, fp;
+        if (q < 0.5) {
+            f = 1.0 - 6.0 * q * q + 6.0 * q * q * q;
+            fp = -12.0 * q + 18.0 * q * q;
+        } else {
+            const double u = 1.0 - q;
+            f = 2.0 * u * u * u;
+            fp = -6.0 * u * u;
+        }
+        w = norm * f;
+        dh = -((double)dim / h) * norm * f - (q / h) * norm * fp;
+    }
+    s.wsum += w;
+    s.dwdh += dh;
+    s.rho += m * w;
+    s.mom[0] += dx * dx * w; s.mom[1] += dy * dy * w; s.mom[2] += dz * dz * w;
+    s.mom[3] += dx * dy * w; s.mom[4] += dy * dz * w; s.mom[5] += dx * dz * w;
+    s.face[0] += dx * w; s.face[1] += dy * w; s.face[2] += dz * w;
+    if (r < h) ++s.inside;
+}
+
+// One evaluation at h: the sums over the GAS neighbours inside h, in tree order (hydro.cc:205-222).
+__device__ void dens_eval(const DensArgs& a, double px, double py, double pz, double h, DensSums& s) {
+    dens_zero(s);
     const int dim = a.n_dims;
     const double norm = kernel_norm(h, dim);
     search<false>(a.g, px, py, pz, h, nullptr, 0, [&](uint32_t, int sp) {
         if (a.stype && __ldg(a.stype + sp) != 0) return;
         const double2 xy = __ldg(reinterpret_cast<const double2*>(a.g.src + sp));
         const double zz = __ldg(reinterpret_cast<const double*>(a.g.src + sp) + 2);
-        const double dx = min_image(xy.x - px, a.g.box), dy = min_image(xy.y - py, a.g.box),
-                     dz = min_image(zz - pz, a.g.box);
-        const double r = sqrt(dx * dx + dy * dy + dz * dz);
-        const double q = r / h;
-        double w = 0.0, dh = 0.0;
-        if (q < 1.0) {
-            double f, fp;
-            if (q < 0.5) {
-                f = 1.0 - 6.0 * q * q + 6.0 * q * q * q;
-                fp = -12.0 * q + 18.0 * q * q;
-            } else {
-                const double u = 1.0 - q;
-                f = 2.0 * u * u * u;
-                fp = -6.0 * u * u;
-            }
-            w = norm * f;
-            dh = -((double)dim / h) * norm * f - (q / h) * norm * fp;
-        }
-        s.wsum += w;
-        s.dwdh += dh;
-        s.rho += __ldg(a.smass + sp) * w;
-        s.mom[0] += dx * dx * w; s.mom[1] += dy * dy * w; s.mom[2] += dz * dz * w;
-        s.mom[3] += dx * dy * w; s.mom[4] += dy * dz * w; s.mom[5] += dx * dz * w;
-        s.face[0] += dx * w; s.face[1] += dy * w; s.face[2] += dz * w;
-        if (r < h) ++s.inside;
+        dens_add(min_image(xy.x - px, a.g.box), min_image(xy.y - py, a.g.box), min_image(zz - pz, a.g.box),
+                 __ldg(a.smass + sp), h, norm, dim, s);
     });
 }
 
@@ -287,58 +297,77 @@ __device__ bool invert_moments(const double* m, double* B, int n_dims) {
     return true;
 }
 
-// One thread per target: bisection-guarded Newton on N_eff(h) = des_ngb with the face-closure and
-// condition-number corrections and the growing tolerance (hydro.cc:189-297).
+// The convergence test and the bisection-guarded Newton step of one iteration with the
+// face-closure and condition-number corrections and the growing tolerance (hydro.cc:224-272) for
+// particle p after an evaluation at h: true when converged (h kept), else h moves.
+struct NewtonParams {
+    double des_ngb, ngb_tol;
+    const double* cond_prev;
+    int n_dims, face_corr;
+};
+
+__device__ __forceinline__ bool dens_newton(const NewtonParams a, uint32_t p, const DensSums& s, int iter, double& h,
+                                         double& h_lo, double& h_hi) {
+    const int dim = a.n_dims;
+    const double n_eff = ball_vol(h, dim) * s.wsum;
+    double ncorr = 1.0;
+    if (a.cond_prev) {
+        const double cn = a.cond_prev[p];
+        if (cn > 100.0) ncorr = fmin(sqrt(1.0 + (cn - 100.0) / 1000.0), 2.0);
+    }
+    double des_eff = a.des_ngb * ncorr, tol_eff = a.ngb_tol * ncorr;
+    if (a.face_corr && s.wsum > 0) {
+        double B[9];
+        if (invert_moments(s.mom, B, dim)) {
+            const double vol = 1.0 / s.wsum;
+            const double dx_i = sqrt(vol * (s.mom[0] + s.mom[1] + s.mom[2]));
+            double sum_abs = 0.0;
+            for (int r = 0; r < 3; ++r) {
+                const double leak =
+                    (B[3 * r] * s.face[0] + B[3 * r + 1] * s.face[1] + B[3 * r + 2] * s.face[2]) * (2.0 * vol);
+                sum_abs += fabs(leak) / dim;
+            }
+            const double denom = 2.0 * dim * pow(dx_i, dim - 1);
+            if (denom > 0) {
+                const double fce = sum_abs / denom;
+                if (fce > 0.35) ncorr = fmax(ncorr, fmin(fce / 0.35, 2.0));
+                des_eff = a.des_ngb * ncorr;
+                tol_eff = a.ngb_tol * ncorr;
+            }
+        }
+    }
+    if (iter > 1) tol_eff = fmin(0.25 * des_eff, tol_eff * exp(0.1 * log(des_eff / (16.0 * tol_eff)) * iter));
+    const double res = n_eff - des_eff;
+    if (fabs(res) < tol_eff) return true;
+    if (res > 0) h_hi = h; else h_lo = h;
+    const double dn = ball_vol(h, dim) * ((double)dim / h * s.wsum + s.dwdh);
+    double hn = dn > 0 ? h - res / dn : 0.0;
+    if (hn <= h_lo || (h_hi > 0 && hn >= h_hi) || hn <= 0) {
+        if (h_hi > 0) hn = h_lo > 0 ? sqrt(h_lo * h_hi) : 0.5 * h_hi;
+        else hn = h * (res > 0 ? 0.7 : 1.6);
+    }
+    h = hn;
+    return false;
+}
+
+__device__ __forceinline__ NewtonParams newton_params(const DensArgs& a) {
+    return NewtonParams{a.des_ngb, a.ngb_tol, a.cond_prev, a.n_dims, a.face_corr};
+}
+
+// One thread per target: up to 100 iterations of evaluation and Newton step, then, when the solve
+// did not converge, one more evaluation at the final h (hydro.cc:189-297).
 __global__ void __launch_bounds__(kBlk) density_kernel(const DensArgs a) {
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.nt; t += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t p = a.targets[t];
         const uint32_t sp = a.rank[p];
         const double px = a.g.src[sp].x, py = a.g.src[sp].y, pz = a.g.src[sp].z;
-        const int dim = a.n_dims;
         double h = a.h_start ? a.h_start[t] : a.h_default, h_lo = 0.0, h_hi = 0.0;
         int iter = 0;
         bool converged = false;
         DensSums s;
         for (; iter < 100; ++iter) {
             dens_eval(a, px, py, pz, h, s);
-            const double n_eff = ball_vol(h, dim) * s.wsum;
-            double ncorr = 1.0;
-            if (a.cond_prev) {
-                const double cn = a.cond_prev[p];
-                if (cn > 100.0) ncorr = fmin(sqrt(1.0 + (cn - 100.0) / 1000.0), 2.0);
-            }
-            double des_eff = a.des_ngb * ncorr, tol_eff = a.ngb_tol * ncorr;
-            if (a.face_corr && s.wsum > 0) {
-                double B[9];
-                if (invert_moments(s.mom, B, dim)) {
-                    const double vol = 1.0 / s.wsum;
-                    const double dx_i = sqrt(vol * (s.mom[0] + s.mom[1] + s.mom[2]));
-                    double sum_abs = 0.0;
-                    for (int r = 0; r < 3; ++r) {
-                        const double leak =
-                            (B[3 * r] * s.face[0] + B[3 * r + 1] * s.face[1] + B[3 * r + 2] * s.face[2]) * (2.0 * vol);
-                        sum_abs += fabs(leak) / dim;
-                    }
-                    const double denom = 2.0 * dim * pow(dx_i, dim - 1);
-                    if (denom > 0) {
-                        const double fce = sum_abs / denom;
-                        if (fce > 0.35) ncorr = fmax(ncorr, fmin(fce / 0.35, 2.0));
-                        des_eff = a.des_ngb * ncorr;
-                        tol_eff = a.ngb_tol * ncorr;
-                    }
-                }
-            }
-            if (iter > 1) tol_eff = fmin(0.25 * des_eff, tol_eff * exp(0.1 * log(des_eff / (16.0 * tol_eff)) * iter));
-            const double res = n_eff - des_eff;
-            if (fabs(res) < tol_eff) { converged = true; break; }
-            if (res > 0) h_hi = h; else h_lo = h;
-            const double dn = ball_vol(h, dim) * ((double)dim / h * s.wsum + s.dwdh);
-            double hn = dn > 0 ? h - res / dn : 0.0;
-            if (hn <= h_lo || (h_hi > 0 && hn >= h_hi) || hn <= 0) {
-                if (h_hi > 0) hn = h_lo > 0 ? sqrt(h_lo * h_hi) : 0.5 * h_hi;
-                else hn = h * (res > 0 ? 0.7 : 1.6);
-            }
-            h = hn;
+            if (dens_newton(newton_params(a), p, s, iter, h, h_lo, h_hi)) { converged = true; break; }
         }
         if (!converged) dens_eval(a, px, py, pz, h, s);  // rho of the final h (hydro.cc:281-293)
         a.h[t] = h;
