@@ -118,6 +118,34 @@ def ngb_scenario(R):
     out["box_targets"] = obb[:3000].copy()
     for k in ("h", "rho", "nngb", "iters"):
         out[f"box_{k}"] = b[k]
+    # a 2-D sheet (z = 0) and a 1-D line (y = z = 0), jittered lattices with a density gradient:
+    # the dimension-aware kernels and solve, on the targets away from the edges
+    for dim, name in ((2, "d2"), (1, "d1")):
+        r2 = np.random.default_rng(30 + dim)
+        if dim == 2:
+            g1 = (np.arange(64) + 0.5) / 64
+            x, y = (a.ravel() for a in np.meshgrid(g1, g1, indexing="ij"))
+            x = x + r2.uniform(-0.2, 0.2, x.size) / 64
+            y = y + r2.uniform(-0.2, 0.2, y.size) / 64
+        else:
+            x = (np.arange(4096) + 0.5) / 4096
+            x = x + r2.uniform(-0.2, 0.2, x.size) / 4096
+            y = np.zeros_like(x)
+        x = x ** 1.3  # a density gradient along x
+        n = x.size
+        Q = {"x": x, "y": y, "z": np.zeros(n), "m": np.full(n, 1.0 / n), "soft": np.full(n, 0.01)}
+        TD = R.build(Q)
+        obd = TD.order()[0]
+        inner = (Q["x"][obd] > 0.15) & (Q["x"][obd] < 0.85)
+        if dim == 2:
+            inner &= (Q["y"][obd] > 0.15) & (Q["y"][obd] < 0.85)
+        obd = obd[inner].copy()
+        for k in ("x", "y", "z", "m"):
+            out[f"{name}_{k}"] = Q[k]
+        dd = TD.density(obd, 12.0 if dim == 2 else 5.0, 0.05, n_dims=dim)
+        out[f"{name}_targets"] = obd
+        for k in ("h", "rho", "nngb", "iters"):
+            out[f"{name}_{k}"] = dd[k]
     return out
 
 

@@ -73,6 +73,14 @@ def test_density_matches_reference(gpu_ctx, golden, ngb_tree, case):
     check_density(d, golden, case)
 
 
+@pytest.mark.parametrize("case,dim", [("d2", 2), ("d1", 1)])
+def test_low_dimension_density_matches_reference(gpu_ctx, golden, case, dim):
+    """A sheet and a line with the 2-D and 1-D kernels (hydro.h:28-37, hydro.cc:172-177)."""
+    T = gpu_ctx.build(particles(golden, f"ngb_{case}"), key_mode=g.GT_KEY_MORTON)
+    d = gpu_ctx.density(T, golden[f"ngb_{case}_targets"], 12.0 if dim == 2 else 5.0, 0.05, n_dims=dim)
+    check_density(d, golden, case)
+
+
 def test_periodic_density_matches_reference(gpu_ctx, golden):
     T = gpu_ctx.build(particles(golden, "ngb_box"), key_mode=g.GT_KEY_MORTON)
     d = gpu_ctx.density(T, golden["ngb_box_targets"], 32.0, 0.05, box=2.0)

@@ -308,12 +308,17 @@ def test_neighbour_search_matches_golden(oracle, golden):
     assert np.array_equal(st, golden["ngb_box_gather_start"]) and np.array_equal(f, golden["ngb_box_gather_found"])
 
 
-@pytest.mark.parametrize("case", ["cold", "warm", "cond", "box"])
+@pytest.mark.parametrize("case", ["cold", "warm", "cond", "box", "d2", "d1"])
 def test_density_matches_golden(oracle, golden, case):
     """The restatement of the density solve (hydro.cc:150-327): the same iteration counts and
     neighbour counts, h and rho to 1e-12 (FP64 in the same order; the reference's compiler may
-    contract multiply-adds)."""
-    if case == "box":
+    contract multiply-adds).  d2 / d1: a sheet and a line with the 2-D and 1-D kernels."""
+    if case in ("d2", "d1"):
+        P = ngb_particles(golden, f"ngb_{case}")
+        T = oracle.build(P)
+        dim = 2 if case == "d2" else 1
+        d = T.density(golden[f"ngb_{case}_targets"], 12.0 if dim == 2 else 5.0, 0.05, n_dims=dim)
+    elif case == "box":
         P = ngb_particles(golden, "ngb_box")
         T = oracle.build(P)
         d = T.density(golden["ngb_box_targets"], 32.0, 0.05, box=2.0)
