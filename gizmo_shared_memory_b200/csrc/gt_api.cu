@@ -236,14 +236,21 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
         if (rq.tidal) check_cuda(cudaMemsetAsync(rq.tidal, 0, (size_t)nout * 48, ctx->stream), "memset");
         if (rq.jerk) check_cuda(cudaMemsetAsync(rq.jerk, 0, (size_t)nout * 24, ctx->stream), "memset");
     }
-    run_walk(ctx, tree, rq);
+    // host outputs in target order: the walk copies each chunk back while the next one runs
+    if (mem == GT_MEM_HOST && !rq.out_original && !capture) {
+        rq.host.ax = ax; rq.host.ay = ay; rq.host.az = az;
+        rq.host.phi = phi; rq.host.tidal = tidal; rq.host.jerk = jerk;
+    }
+    const bool copied = run_walk(ctx, tree, rq);
     if (capture) return;
-    copy_out(ctx, ax, rq.ax, nout, mem);
-    copy_out(ctx, ay, rq.ay, nout, mem);
-    copy_out(ctx, az, rq.az, nout, mem);
-    copy_out(ctx, phi, rq.phi, nout, mem);
-    copy_out(ctx, tidal, rq.tidal, nout * 6, mem);
-    copy_out(ctx, jerk, rq.jerk, nout * 3, mem);
+    if (!copied) {
+        copy_out(ctx, ax, rq.ax, nout, mem);
+        copy_out(ctx, ay, rq.ay, nout, mem);
+        copy_out(ctx, az, rq.az, nout, mem);
+        copy_out(ctx, phi, rq.phi, nout, mem);
+        copy_out(ctx, tidal, rq.tidal, nout * 6, mem);
+        copy_out(ctx, jerk, rq.jerk, nout * 3, mem);
+    }
     const bool sync = mem == GT_MEM_HOST || !o.async;
     finish(ctx, sync);
     if (sync) record_walk_time(ctx);
@@ -339,6 +346,13 @@ int gt_context_destroy(gt_context* ctx) {
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
+    for (cudaEvent_t e : ctx->chunk_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->copy_done) cudaEventDestroy(ctx->copy_done);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     cudaGetLastError();
     if (prev >= 0) cudaSetDevice(prev);

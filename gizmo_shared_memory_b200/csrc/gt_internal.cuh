@@ -92,6 +92,10 @@ struct gt_context {
     std::vector<gt::DevBuf> scratch;  // grow-only workspace slots, indexed by gt::Slot
     void* pinned = nullptr;           // small pinned host buffer for scalar read-backs
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // result copies overlapped with a walk split into chunks (made on first use)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t chunk_ev[8] = {};
+    cudaEvent_t copy_done = nullptr;
 };
 
 struct gt_tree {
@@ -235,8 +239,15 @@ struct WalkRequest {
     double* tidal = nullptr;  // 6 per target (xx yy zz xy yz xz), not times G
     double* jerk = nullptr;   // 3 per target, times G
     double sink_radius = 0;   // > 0: sink-direct opening (grouped walks of a tree with types)
+    // host destinations of the outputs (indexed like the device outputs): the walk copies each
+    // chunk's results while the next chunk runs; null: the caller copies
+    struct HostOut {
+        double *ax = nullptr, *ay = nullptr, *az = nullptr, *phi = nullptr, *tidal = nullptr, *jerk = nullptr;
+        bool any() const { return ax || ay || az || phi || tidal || jerk; }
+    } host;
 };
-void run_walk(gt_context* ctx, const gt_tree* t, const WalkRequest& rq);
+// true when the walk copied the outputs to rq.host itself (chunked, overlapped with the walk)
+bool run_walk(gt_context* ctx, const gt_tree* t, const WalkRequest& rq);
 
 // Autotuner (gt_tune.cu); aold and mac_model are device pointers, the sample arrays host ones
 // except `sample`, which is copied to the device by the tuner.

@@ -1016,6 +1016,21 @@ void dispatch(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la
     }
 }
 
+// Chunk boundaries of a group list for the copy-overlapped walk: chunk c starts at the first group
+// whose first target is at or after c * nt / K.  out: K+1 pairs (group index, first target).
+__global__ void chunk_bounds_kernel(const int2* __restrict__ groups, int ng, int nt, int K, int2* __restrict__ out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int c = 0; c <= K; ++c) {
+        const int64_t want = (int64_t)nt * c / K;
+        int lo = 0, hi = ng;  // first g with groups[g].x >= want
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (groups[mid].x < want) lo = mid + 1; else hi = mid;
+        }
+        out[c] = make_int2(lo, lo < ng ? groups[lo].x : nt);
+    }
+}
+
 template <int TPL, bool LA, bool POT, bool CNT, int MAC, bool XT = false>
 int occupancy_blocks(int warps, int pn_cap) {
     prepare_walk<TPL, LA, POT, CNT, MAC, XT>();
@@ -1025,16 +1040,22 @@ int occupancy_blocks(int warps, int pn_cap) {
     return std::max(1, nb);
 }
 
+struct OutputCopy {
+    const double* dev;
+    double* host;
+    int stride;
+};
+
 }  // namespace
 
-void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
+bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     gt_tree* t = const_cast<gt_tree*>(tc);  // only the group cache is mutated
     cudaStream_t st = ctx->stream;
     const bool all = rq.targets == nullptr;
     const int64_t nt = all ? t->n_live : rq.n_targets;
     ctx->stats = gt_walk_stats{};
     ctx->stats.targets = nt;
-    if (nt <= 0) return;
+    if (nt <= 0) return false;
     if (nt > (int64_t)INT32_MAX) throw Fail{GT_ERR_INVALID, "too many targets for one walk"};
 
     int mode = rq.group_mode;
@@ -1118,7 +1139,7 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         }
     }
     ctx->stats.groups = ng;
-    if (ng <= 0) return;
+    if (ng <= 0) return false;
 
     // ---- launch -------------------------------------------------------------------------------
     const int warps = (rq.block_warps > 0 && rq.block_warps <= kMaxWarps) ? rq.block_warps : kMaxWarps;
@@ -1230,6 +1251,66 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         a.mac_l2 = l2;
     }
 
+    // Host outputs of a large walk: split the groups into chunks of about equal target count, and
+    // copy each chunk's results to the host on a second stream while the next chunk runs.
+    constexpr int kChunks = 4;
+    const bool chunked = rq.host.any() && !rq.count && rq.stack_capacity == 0 && !rq.capture &&
+                         ng >= 64 * kChunks && nt >= (1 << 18);
+    if (chunked) {
+        if (!ctx->copy_stream) {
+            check_cuda(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            for (cudaEvent_t& e : ctx->chunk_ev) check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+            check_cuda(cudaEventCreateWithFlags(&ctx->copy_done, cudaEventDisableTiming), "event");
+        }
+        int2* bounds = (int2*)(ctr + 16);  // K+1 int2 after the counters
+        check_cuda(cudaMemsetAsync(ctr, 0, 256, st), "memset counters");
+        chunk_bounds_kernel<<<1, 1, 0, st>>>(groups, (int)ng, (int)nt, kChunks, bounds);
+        check_launch(ctx, "chunk_bounds_kernel");
+        int2 hb[kChunks + 1];
+        check_cuda(cudaMemcpyAsync(ctx->pinned, bounds, sizeof(hb), cudaMemcpyDeviceToHost, st), "d2h");
+        check_cuda(cudaStreamSynchronize(st), "sync");
+        std::memcpy(hb, ctx->pinned, sizeof(hb));
+        const size_t stack_bytes = (size_t)total_warps * stack_cap * 4;
+        if (wb) {
+            own((void**)&wb->stack, wb->stack_bytes, stack_bytes);
+            a.stack = wb->stack;
+        } else {
+            a.stack = (int*)scratch(ctx, kSlotStack, stack_bytes);
+        }
+        a.stack_cap = stack_cap;
+        const OutputCopy outs[6] = {{rq.ax, rq.host.ax, 1},  {rq.ay, rq.host.ay, 1},       {rq.az, rq.host.az, 1},
+                                    {rq.phi, rq.host.phi, 1}, {rq.tidal, rq.host.tidal, 6}, {rq.jerk, rq.host.jerk, 3}};
+        check_cuda(cudaEventRecord(ctx->ev0, st), "event");
+        for (int c = 0; c < kChunks; ++c) {
+            const int g0 = hb[c].x, g1 = hb[c + 1].x;
+            if (g1 > g0) {
+                WalkArgs ac = a;
+                ac.groups = groups + g0;
+                ac.n_groups = g1 - g0;
+                ac.group_root = roots ? roots + g0 : nullptr;
+                ac.next_group = (unsigned int*)(ctr + 10) + c;
+                const int cb = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, ((int64_t)(g1 - g0) + warps - 1) / warps));
+                if (xt) dispatch_xt(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false);
+                else if (tpl == 1) dispatch<1>(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false, rq.mac);
+                else if (tpl == 2) dispatch<2>(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false, rq.mac);
+                else dispatch<4>(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false, rq.mac);
+            }
+            // this chunk's targets [hb[c].y, hb[c+1].y) go back while the next chunk runs
+            check_cuda(cudaEventRecord(ctx->chunk_ev[c], st), "event");
+            check_cuda(cudaStreamWaitEvent(ctx->copy_stream, ctx->chunk_ev[c], 0), "wait");
+            const int64_t t0 = hb[c].y, t1 = hb[c + 1].y;
+            for (const auto& o : outs)
+                if (o.dev && o.host && t1 > t0)
+                    check_cuda(cudaMemcpyAsync(o.host + t0 * o.stride, o.dev + t0 * o.stride,
+                                               (size_t)(t1 - t0) * o.stride * sizeof(double), cudaMemcpyDeviceToHost,
+                                               ctx->copy_stream), "d2h chunk");
+        }
+        check_cuda(cudaEventRecord(ctx->ev1, st), "event");
+        check_cuda(cudaEventRecord(ctx->copy_done, ctx->copy_stream), "event");
+        check_cuda(cudaStreamWaitEvent(st, ctx->copy_done, 0), "wait");
+        return true;
+    }
+
     for (int attempt = 0; attempt < 3; ++attempt) {
         const size_t stack_bytes = (size_t)total_warps * stack_cap * 4;
         if (wb) {
@@ -1267,6 +1348,7 @@ void run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         if (attempt == 2) throw Fail{GT_ERR_OVERFLOW, "walk stack overflow"};
         stack_cap *= 2;
     }
+    return false;
 }
 
 }  // namespace gt
