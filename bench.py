@@ -613,6 +613,153 @@ def run_batch_arm(args):
     plan.free()
 
 
+def run_extras_arm(args):
+    """The reference's options beyond the plain walk, on the 4M galaxy with seeded velocities
+    (windows of 32, relative criterion alpha=0.0025 after a theta=0.7 bootstrap walk):
+      * the tidal tensor, and the tidal tensor with the jerk (shmem/bench_treeforce.cc's variants);
+      * the gas rules: 70 % gas with adaptive-softening zeta, 1 % sinks, sink-direct radius 0.02;
+      * tree reuse: a kick and a speed bound for every particle, refresh_walk_nodes, the drifted
+        positions and a walk on the reused tree, against a rebuild (with velocities) and a walk.
+    Device time per step with inputs resident.  The CPU baseline is the reference's own walk,
+    plain, with the tidal tensor, and with both, on a bounded sample of leaf groups."""
+    import torch
+
+    import gizmo_shared_memory_b200 as g
+
+    torch.cuda.set_device(0)
+    wl = "galaxy_4m"
+    cfg = WORKLOADS[wl]
+    alpha = args.alpha if args.alpha is not None else cfg["alpha"]
+    P = make_workload(wl)
+    n = len(P["m"])
+    rng = np.random.default_rng(11)
+    vel = [rng.normal(0.0, 0.3, n) for _ in range(3)]
+    dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
+    vdev = [torch.as_tensor(v, device="cuda") for v in vel]
+    ctx = g.Context(0, torch_stream=True)
+    T = ctx.build(dev)
+    ctx.tree_velocities(T, *vdev)
+    nl = T.info()["n_live"]
+    wopts = dict(group_mode=g.GT_GROUP_BATCH, group_max=32, batch=32)
+
+    def mk(*shape):
+        return torch.empty(*shape, dtype=torch.float64, device="cuda")
+
+    a3 = (mk(nl), mk(nl), mk(nl))
+    ctx.accel_grouped(T, None, theta=0.7, outs=a3 + (None,), **wopts)
+    aold = ctx.form_aold(*a3, alpha)
+    tid, jk = mk(nl, 6), mk(nl, 3)
+    stream = torch.cuda.current_stream()
+
+    def timed(step):
+        for _ in range(max(args.warmup, 3)):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    # the gas tree: the same particles, types and zeta attached
+    ty = np.where(rng.uniform(size=n) < 0.7, 0, 4).astype(np.uint8)
+    ty[rng.choice(n, n // 100, replace=False)] = 5
+    zeta = np.where(ty == 0, 0.1 * P["m"] ** 2 * P["soft"] ** 2 * rng.normal(0.0, 1.0, n), 0.0)
+    Tg = ctx.build(dev)
+    ctx.tree_gas(Tg, ty, zeta)
+    # the reused tree: every live particle's leaf, its kick (m a dt) and speed bound
+    Tr = ctx.build(dev)
+    ctx.tree_velocities(Tr, *vdev)
+    dl = Tr.download(nodes=False)
+    ob = dl["orderbuf"]
+    leaf_live = torch.as_tensor(dl["leaf_of"][ob].astype(np.int32), device="cuda")
+    obd = torch.as_tensor(ob.astype(np.int64), device="cuda")
+    dt = 1e-4
+    dp = torch.stack([dev["m"][obd] * a3[k] * dt for k in range(3)], 1).contiguous()
+    speed = torch.sqrt(sum(vdev[k][obd] ** 2 for k in range(3))).float().contiguous()
+    clock = {"tau": 0.0}
+
+    def reuse_step():
+        clock["tau"] += dt
+        tau = clock["tau"]
+        ctx.tree_events(Tr, 0, leaf_live, a=dp, tau=tau)
+        ctx.tree_events(Tr, 2, leaf_live, f=speed)
+        ctx.tree_refresh(Tr, tau)
+        ctx.tree_particles(Tr, x=dev["x"] + vdev[0] * tau, y=dev["y"] + vdev[1] * tau, z=dev["z"] + vdev[2] * tau)
+        ctx.accel_grouped(Tr, None, aold=aold, outs=a3 + (None,), async_=True, **wopts)
+
+    def rebuild_step():
+        clock["tau"] += dt
+        tau = clock["tau"]
+        moved = dict(dev, x=dev["x"] + vdev[0] * tau, y=dev["y"] + vdev[1] * tau, z=dev["z"] + vdev[2] * tau)
+        Tb = ctx.build(moved)
+        ctx.tree_velocities(Tb, *vdev)
+        ctx.accel_grouped(Tb, None, aold=aold, outs=a3 + (None,), async_=True, **wopts)
+        torch.cuda.synchronize()
+        Tb.free()
+
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = ctx.launches()
+    ms = {
+        "plain": timed(lambda: ctx.accel_grouped(T, None, aold=aold, outs=a3 + (None,), async_=True, **wopts)),
+        "tidal": timed(lambda: ctx.accel_grouped_ext(T, None, aold=aold, outs=a3 + (None, tid, None), async_=True,
+                                                     **wopts)),
+        "tidal_jerk": timed(lambda: ctx.accel_grouped_ext(T, None, aold=aold, outs=a3 + (None, tid, jk), async_=True,
+                                                          **wopts)),
+        "gas_sinks": timed(lambda: ctx.accel_grouped(Tg, None, aold=aold, outs=a3 + (None,), async_=True,
+                                                     sink_direct_radius=0.02, **wopts)),
+        "reuse_step": timed(reuse_step),
+        "rebuild_step": timed(rebuild_step),
+    }
+    launches = ctx.launches() - l0
+    clocks = sampler.stop()
+    rows = {k: {"ms_per_step": v, "particles_per_s": nl / (v / 1e3)} for k, v in ms.items()}
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from oracle import Reference, reference_available
+
+        if reference_available():
+            R = Reference()
+            R.set_threads(os.cpu_count() or 1)
+            TR = R.build(P, vel=vel)
+            obr, _, leafr = TR.order()
+            tg = leaf_group_sample(obr, leafr, 200000, np.random.default_rng(5))
+            a0 = TR.accel_grouped(tg, 0.7, 1.0, 0)
+            ao = alpha * np.sqrt(a0[0] ** 2 + a0[1] ** 2 + a0[2] ** 2)
+            cpu = {"cores": os.cpu_count(), "kind": "reference", "unit": "particles/s",
+                   "sample": f"{len(tg)} targets in whole leaf groups picked at random, leaf groups (batch 0), "
+                             "the tree built with velocities (not timed)"}
+            for name, kw in (("plain", None), ("tidal", dict(tidal=True, jerk=False)),
+                             ("tidal_jerk", dict(tidal=True, jerk=True))):
+                t0 = time.perf_counter()
+                if kw is None:
+                    TR.accel_grouped(tg, 0.0, 1.0, 0, aold=ao)
+                else:
+                    TR.accel_grouped_ext(tg, 0.0, 1.0, 0, aold=ao, **kw)
+                cpu[name] = len(tg) / (time.perf_counter() - t0)
+            for name in ("plain", "tidal", "tidal_jerk"):
+                rows[name]["vs_cpu_reference"] = rows[name]["particles_per_s"] / cpu[name]
+    line = {
+        "metric": "tree-force particles/s with the tidal tensor and jerk, the gas rules and tree reuse",
+        "value": rows["tidal_jerk"]["particles_per_s"], "unit": "particles/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms["tidal_jerk"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded galaxy, seeded velocities and gas fractions)",
+        "config": {"workload": "extras_galaxy_4m", "n": n, "description": cfg["desc"],
+                   "criterion": f"plain relative criterion alpha={alpha} after a theta=0.7 bootstrap walk",
+                   "grouping": "windows of 32 consecutive targets in Peano-Hilbert tree order",
+                   "gas": "70 % gas with zeta = 0.1 m^2 h^2 N(0,1), 1 % sinks, sink-direct radius 0.02",
+                   "reuse": "kick and speed bound for every live particle, refresh, drifted positions, walk",
+                   "l2": f"inputs larger than L2: {n * 32 / 2**20:.0f} MiB of particles"},
+        "rows": rows, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_density_arm(args):
     """The density solve (shmem::density, hydro.cc:150-327) on the GPU tree: every particle a
     target, warm-started from the converged h of a first solve (what every step after the first
@@ -713,7 +860,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["plummer_batch_256"] +
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["plummer_batch_256", "extras_galaxy_4m"] +
                     ["density_" + w for w in ("galaxy_4m", "clustered_16m")], default="clustered_16m",
                     help="plummer_batch_256: the batched many-system case (forest + autotuner + graph); "
                          "density_*: the density solve on that workload")
@@ -737,6 +884,8 @@ def main():
         run_batch_arm(args)
     elif args.workload.startswith("density_"):
         run_density_arm(args)
+    elif args.workload == "extras_galaxy_4m":
+        run_extras_arm(args)
     else:
         run_gpu_arm(args)
 

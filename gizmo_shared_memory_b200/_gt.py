@@ -549,9 +549,20 @@ class Context:
         return (ax, ay, az, phi) if want_phi else (ax, ay, az)
 
     def accel_grouped_ext(self, tree: Tree, targets=None, aold=None, theta=0.0, G=1.0, batch=0, tidal=True,
-                          jerk=False, want_phi=False, **opts):
+                          jerk=False, want_phi=False, outs=None, **opts):
         """Grouped walk with the tidal tensor ([nt, 6]: xx yy zz xy yz xz, not times G) and the
-        jerk ([nt, 3]); host arrays.  Returns (ax, ay, az, phi, tidal, jerk)."""
+        jerk ([nt, 3]); host arrays.  Returns (ax, ay, az, phi, tidal, jerk).  With outs =
+        (ax, ay, az, phi, tidal, jerk) device tensors (any may be None) the walk writes them on the
+        device; targets and aold are then device tensors or None."""
+        if outs is not None:
+            o = self._walk_opts(**opts)
+            t, nt = self._targets(targets)
+            if t is None:
+                nt = tree.info()["n_live"]
+            self._check(load_library().gt_accel_grouped_ext(
+                self.h, tree.h, nt if targets is not None else 0, _ptr(t), _ptr(aold), theta, G, batch, C.byref(o),
+                GT_MEM_DEVICE, *[_ptr(x) for x in outs]))
+            return outs
         t, nt = self._targets(targets)
         if t is None:
             nt = tree.info()["n_live"] if opts.get("out_order", 0) == GT_OUT_TARGETS else tree.info()["n"]
@@ -576,8 +587,13 @@ class Context:
 
     # ---- tree reuse ---------------------------------------------------------------------------
     def tree_events(self, tree: Tree, kind, leaf, a=None, x=None, v=None, f=None, tau=0.0, box=0.0):
-        """Events of one kind (GT_EVENT_*: 0 kick, 1 shift, 2 vmax, 3 soft, 4 mass, 5 pad) on
-        leaf nodes of this tree, host arrays."""
+        """Events of one kind (GT_EVENT_*: 0 kick, 1 shift, 2 vmax, 3 soft, 4 mass, 5 pad, 6 hmax) on
+        leaf nodes of this tree: host arrays, or device tensors (int32 leaves, float64 a, x, v,
+        float32 f)."""
+        if _is_dev(leaf):
+            self._check(load_library().gt_tree_events(self.h, tree.h, kind, int(leaf.numel()), _ptr(leaf), _ptr(a),
+                                                      _ptr(x), _ptr(v), _ptr(f), tau, box, GT_MEM_DEVICE))
+            return
         lf = np.ascontiguousarray(leaf, np.int32)
         cv = lambda q, dt: None if q is None else np.ascontiguousarray(q, dt)
         a, x, v, f = cv(a, np.float64), cv(x, np.float64), cv(v, np.float64), cv(f, np.float32)
@@ -596,6 +612,12 @@ class Context:
         return out
 
     def tree_particles(self, tree: Tree, x=None, y=None, z=None, m=None, soft=None):
+        """The particles' current state (indexed like the build input; None keeps a field): host
+        arrays or device tensors."""
+        if any(_is_dev(q) for q in (x, y, z, m, soft)):
+            self._check(load_library().gt_tree_particles(self.h, tree.h, _ptr(x), _ptr(y), _ptr(z), _ptr(m),
+                                                         _ptr(soft), GT_MEM_DEVICE))
+            return
         cv = lambda q: None if q is None else np.ascontiguousarray(q, np.float64)
         x, y, z, m, soft = (cv(q) for q in (x, y, z, m, soft))
         self._check(load_library().gt_tree_particles(self.h, tree.h, _ptr(x), _ptr(y), _ptr(z), _ptr(m),

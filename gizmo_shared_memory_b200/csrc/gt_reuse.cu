@@ -10,7 +10,8 @@
 // the walk node grow by 2 (vmax tau + xpad): every particle may have moved that far.
 //
 // Events arrive as arrays.  Kicks, shifts and the speed/softening bounds commute, so one thread
-// per event climbs the parent chain with atomics; mass events and displacement pads depend on the
+// per event climbs the parent chain with atomics (a call with many kicks or shifts sums them per
+// leaf and carries the sums up level by level instead); mass events and displacement pads depend on the
 // order of earlier events (the centre of mass they read, the pad they add to), so one thread
 // applies them in array order, as the reference's serial callers do.
 #include <algorithm>
@@ -22,6 +23,7 @@ namespace gt {
 namespace {
 
 constexpr int kBlk = 256;
+constexpr int64_t kLevelSumEvents = 1 << 16;  // kicks / shifts per call from which sums go up by level
 
 int grid_of(gt_context* ctx, int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((n + kBlk - 1) / kBlk, (int64_t)ctx->num_sms * 8));
@@ -87,6 +89,49 @@ __global__ void shift_kernel(const int* __restrict__ parent, const int* __restri
         const double a = m[e] * dx[3 * e], b = m[e] * dx[3 * e + 1], c = m[e] * dx[3 * e + 2];
         for (int no = leaf[e]; no >= 0; no = parent[no]) {
             atomicAdd(adq + 3 * no, -a); atomicAdd(adq + 3 * no + 1, -b); atomicAdd(adq + 3 * no + 2, -c);
+        }
+    }
+}
+
+// Many kicks or shifts at once: climbing the chain per event would send every event's six
+// atomics to the root and the other top nodes, where they serialise.  Instead the events are first
+// summed into their leaves (a few events per leaf), the sums are carried up one level at a time
+// (a node adds its contiguous children), and every node then takes its total once.  kind 0: kick
+// (a = dp, 3 per event); kind 1: shift (a = m, x = dx, 3 per event).
+__global__ void leaf_sum_kernel(const int* __restrict__ leaf, const double* __restrict__ a, const double* __restrict__ x,
+                                int64_t n, int kind, double* __restrict__ acc) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int lf = leaf[e];
+        if (lf < 0) continue;
+        for (int k = 0; k < 3; ++k) {
+            const double v = kind == 0 ? a[3 * e + k] : -a[e] * x[3 * e + k];
+            atomicAdd(acc + 3 * lf + k, v);
+        }
+    }
+}
+
+__global__ void level_sum_kernel(const GNode* __restrict__ nodes, int64_t lo, int64_t hi, double* __restrict__ acc) {
+    for (int64_t i = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < hi; i += (int64_t)gridDim.x * blockDim.x) {
+        const int f = nodes[i].first, nc = nodes[i].nchild;
+        if (f < 0) continue;
+        double s0 = acc[3 * i], s1 = acc[3 * i + 1], s2 = acc[3 * i + 2];
+        for (int c = f; c < f + nc; ++c) {
+            s0 += acc[3 * c]; s1 += acc[3 * c + 1]; s2 += acc[3 * c + 2];
+        }
+        acc[3 * i] = s0; acc[3 * i + 1] = s1; acc[3 * i + 2] = s2;
+    }
+}
+
+// kick: dp += sum, dq += sum tau; shift: dq += sum (the sum already carries -m dx)
+__global__ void apply_sum_kernel(int64_t nn, const double* __restrict__ acc, int kind, double tau,
+                                 double* __restrict__ adp, double* __restrict__ adq) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < 3 * nn; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = acc[i];
+        if (kind == 0) {
+            adp[i] += v;
+            adq[i] += v * tau;
+        } else {
+            adq[i] += v;
         }
     }
 }
@@ -264,14 +309,29 @@ void reuse_events(gt_context* ctx, gt_tree* t, int kind, int64_t n, const int* l
     const bool have_vcom = t->vcom != nullptr;  // the momentum arrays exist only with vcom (tree.cc:212)
     switch (kind) {
         case kReuseKick:
-            if (!have_vcom) return;
-            kick_kernel<<<grid_of(ctx, n), kBlk, 0, st>>>(t->parent, leaf, a, n, tau, t->dp, t->dq);
-            check_launch(ctx, "kick_kernel");
-            break;
         case kReuseShift:
             if (!have_vcom) return;
-            shift_kernel<<<grid_of(ctx, n), kBlk, 0, st>>>(t->parent, leaf, a, x, n, t->dq);
-            check_launch(ctx, "shift_kernel");
+            if (n >= kLevelSumEvents) {
+                const int k = kind == kReuseKick ? 0 : 1;
+                const int64_t nn = t->n_nodes;
+                double* acc = (double*)scratch(ctx, kSlotNodeTmp1, (size_t)std::max<int64_t>(nn, 1) * 24);
+                check_cuda(cudaMemsetAsync(acc, 0, (size_t)std::max<int64_t>(nn, 1) * 24, st), "memset");
+                leaf_sum_kernel<<<grid_of(ctx, n), kBlk, 0, st>>>(leaf, a, x, n, k, acc);
+                check_launch(ctx, "leaf_sum_kernel");
+                for (int L = t->n_levels - 1; L >= 0; --L) {
+                    const int64_t lo = t->lvl_off[L], hi = t->lvl_off[L + 1];
+                    level_sum_kernel<<<grid_of(ctx, hi - lo), kBlk, 0, st>>>(t->nodes, lo, hi, acc);
+                    check_launch(ctx, "level_sum_kernel");
+                }
+                apply_sum_kernel<<<grid_of(ctx, 3 * nn), kBlk, 0, st>>>(nn, acc, k, tau, t->dp, t->dq);
+                check_launch(ctx, "apply_sum_kernel");
+            } else if (kind == kReuseKick) {
+                kick_kernel<<<grid_of(ctx, n), kBlk, 0, st>>>(t->parent, leaf, a, n, tau, t->dp, t->dq);
+                check_launch(ctx, "kick_kernel");
+            } else {
+                shift_kernel<<<grid_of(ctx, n), kBlk, 0, st>>>(t->parent, leaf, a, x, n, t->dq);
+                check_launch(ctx, "shift_kernel");
+            }
             break;
         case kReuseVmax:
             raise_vmax_kernel<<<grid_of(ctx, n), kBlk, 0, st>>>(t->parent, leaf, f, n, t->vmax);

@@ -97,3 +97,34 @@ def test_reuse_errors(gpu_ctx, golden):
     with pytest.raises(g.GTError) as e:
         gpu_ctx.tree_events(T, 0, np.array([10 ** 8], np.int32), a=np.zeros((1, 3)))
     assert e.value.status == 1
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_many_events_sum_by_level(gpu_ctx, kind):
+    """A call with many kicks (kind 0) or shifts (kind 1) sums them per leaf and carries the sums up
+    one tree level at a time; the same events applied in calls small enough to climb the parent
+    chain per event give the same node state to 1e-12 (FP64, another summation order)."""
+    from gizmo_shared_memory_b200 import ics
+
+    P = ics.plummer(n=300000, seed=31, soft=0.01)
+    rng = np.random.default_rng(6)
+    vel = [rng.normal(0.0, 0.5, 300000) for _ in range(3)]
+    trees = []
+    for _ in range(2):
+        T = gpu_ctx.build(P)
+        gpu_ctx.tree_velocities(T, *vel)
+        trees.append(T)
+    leaf = trees[0].download(nodes=False)["leaf_of"]
+    live = np.nonzero(leaf >= 0)[0]
+    vec = rng.normal(0.0, 1e-3, (len(live), 3))
+    tau = 0.01
+    kw = dict(a=vec, tau=tau) if kind == 0 else dict(a=P["m"][live], x=vec)
+    gpu_ctx.tree_events(trees[0], kind, leaf[live], **kw)  # one call: sums by level
+    for s in range(0, len(live), 50000):  # small calls: per-event climbs
+        part = slice(s, s + 50000)
+        kw2 = dict(a=vec[part], tau=tau) if kind == 0 else dict(a=P["m"][live][part], x=vec[part])
+        gpu_ctx.tree_events(trees[1], kind, leaf[live][part], **kw2)
+    st = [gpu_ctx.tree_node_state(T, 0.02) for T in trees]
+    for k in ("com", "vel", "mass"):
+        scale = np.abs(st[1][k]).max()
+        assert np.abs(st[0][k] - st[1][k]).max() <= 1e-12 * scale, k
