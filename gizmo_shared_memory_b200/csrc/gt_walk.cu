@@ -232,18 +232,21 @@ struct alignas(16) WarpHdr {
     double lo_x, lo_y, lo_z, hi_x, hi_y, hi_z, c_x, c_y, c_z, emax, amin;
 };
 
-// xt: the lists also carry each entry's velocity (float4), for the jerk, and the particle list
-// each source's zeta (float), for the gas pair rule.
-__host__ __device__ constexpr int warp_smem_bytes(int pn_cap, int pp_cap, bool xt = false) {
-    return ((int)sizeof(WarpHdr) + pn_cap * 16 + pp_cap * 20 + (xt ? (pn_cap + pp_cap) * 16 + pp_cap * 4 : 0) + 15) &
+// ext 1 (tidal tensor / jerk): the lists also carry each entry's velocity (float4), for the jerk,
+// and the particle list each source's zeta (float), for the gas pair rule; ext 2 (gas rules only):
+// just the zeta.
+__host__ __device__ constexpr int warp_smem_bytes(int pn_cap, int pp_cap, int ext = 0) {
+    return ((int)sizeof(WarpHdr) + pn_cap * 16 + pp_cap * 20 +
+            (ext == 1 ? (pn_cap + pp_cap) * 16 + pp_cap * 4 : ext == 2 ? pp_cap * 4 : 0) + 15) &
            ~15;
 }
 
 // MAC: 0 plain relative criterion, 1 network inside the walk (GT_MAC_LEARNED), 2 per-node
-// learned scale (GT_MAC_NODE).  XT: also the tidal tensor and/or the jerk (A.tidal, A.jerk), the
-// zeta terms of gas-gas pairs (A.szeta) and sink-direct opening (A.nsink).
-template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT, int MAC, bool XT = false>
-__global__ void __launch_bounds__(kMaxWarps * 32, (TPL == 1 && !XT) ? 3 : 2)
+// learned scale (GT_MAC_NODE).  XT 1: also the tidal tensor and/or the jerk (A.tidal, A.jerk), the
+// zeta terms of gas-gas pairs (A.szeta) and sink-direct opening (A.nsink); XT 2: the gas rules
+// alone, with the packed monopole evaluation of the plain walk.
+template <int TPL, bool LEAF_ACCEPT, bool WANT_POT, bool COUNT, int MAC, int XT = 0>
+__global__ void __launch_bounds__(kMaxWarps * 32, (TPL == 1 && XT == 0) ? 3 : 2)
 walk_kernel(const WalkArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -261,13 +264,14 @@ walk_kernel(const WalkArgs A) {
     float4* __restrict__ pn = reinterpret_cast<float4*>(wbase + sizeof(WarpHdr));
     float4* __restrict__ pp = pn + A.pn_cap;
     float* __restrict__ ph = reinterpret_cast<float*>(pp + A.pp_cap);
-    float4* __restrict__ pnv = reinterpret_cast<float4*>(ph + A.pp_cap);  // XT only
+    float4* __restrict__ pnv = reinterpret_cast<float4*>(ph + A.pp_cap);  // XT 1 only
     float4* __restrict__ ppv = pnv + A.pn_cap;
-    float* __restrict__ pzs = reinterpret_cast<float*>(ppv + A.pp_cap);  // XT only: source zeta
-    const bool want_tid = XT && A.tidal != nullptr;
-    const bool want_jerk = XT && A.jerk != nullptr;
-    const bool want_zeta = XT && A.szeta != nullptr;
-    const bool sink_rule = XT && A.nsink != nullptr;
+    // source zeta of the particle list: after the velocities (XT 1) or after the softenings (XT 2)
+    float* __restrict__ pzs = XT == 1 ? reinterpret_cast<float*>(ppv + A.pp_cap) : ph + A.pp_cap;
+    const bool want_tid = XT == 1 && A.tidal != nullptr;
+    const bool want_jerk = XT == 1 && A.jerk != nullptr;
+    const bool want_zeta = XT != 0 && A.szeta != nullptr;
+    const bool sink_rule = XT != 0 && A.nsink != nullptr;
 
     unsigned long long c_nodes = 0, c_multi = 0, c_pairs = 0, c_zero = 0, c_flush = 0, c_steps = 0;
     int c_maxtop = 0;
@@ -339,7 +343,7 @@ walk_kernel(const WalkArgs A) {
         // monopole-list entry pos (paired layout, see flush_pn)
         // The monopole list is paired (see flush_pn) for the packed evaluation of full groups
         // and one float4 per entry otherwise (warp-uniform: the group size decides).
-        const bool paired = !XT && NS == 1;
+        const bool paired = XT != 1 && NS == 1;
         auto pn_put = [&](int pos, float x, float y, float z, float m) {
             if (paired) {
                 float* q = reinterpret_cast<float*>(pn + 2 * (pos >> 1)) + (pos & 1);
@@ -354,7 +358,7 @@ walk_kernel(const WalkArgs A) {
         double xt[9][TPL];
         float tvx[TPL], tvy[TPL], tvz[TPL], tzm[TPL], tim[TPL];
         bool has_sink = false;
-        if (XT) {
+        if (XT != 0) {
             bool sink = false;
 #pragma unroll
             for (int k = 0; k < TPL; ++k) {
@@ -422,7 +426,7 @@ walk_kernel(const WalkArgs A) {
             __syncwarp();
             const int np = (n + 1) >> 1;
             float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
-            float xq[XT ? TPL : 1][9];
+            float xq[XT == 1 ? TPL : 1][9];
 #pragma unroll
             for (int k = 0; k < TPL; ++k) ax_[k] = ay_[k] = az_[k] = ap_[k] = 0.0f;
             // packed for full groups; groups of <= 16 targets split the list over lane slices, where
@@ -468,11 +472,11 @@ walk_kernel(const WalkArgs A) {
                     ap_[k] = -(ap2[k].x + ap2[k].y);
                 }
             } else {
-                if (XT) {
+                if (XT == 1) {
 #pragma unroll
                     for (int k = 0; k < TPL; ++k)
 #pragma unroll
-                        for (int c = 0; c < 9; ++c) xq[XT ? k : 0][c] = 0.0f;
+                        for (int c = 0; c < 9; ++c) xq[XT == 1 ? k : 0][c] = 0.0f;
                 }
 #pragma unroll 4
                 for (int j = slice; j < n; j += NS) {
@@ -489,21 +493,21 @@ walk_kernel(const WalkArgs A) {
                             ay_[k] = fmaf(dy, f, ay_[k]);
                             az_[k] = fmaf(dz, f, az_[k]);
                             if (WANT_POT) ap_[k] -= mri;
-                            if (XT) {
+                            if (XT == 1) {
                                 // Newtonian: g2 = 3 m / r^5
                                 const float4 ev = want_jerk ? pnv[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-                                xt_add(xq[XT ? k : 0], dx, dy, dz, f, 3.0f * f * (ri * ri), ev, k);
+                                xt_add(xq[XT == 1 ? k : 0], dx, dy, dz, f, 3.0f * f * (ri * ri), ev, k);
                             }
                         }
                     }
                 }
             }
             accumulate(ax_, ay_, az_, ap_);
-            if (XT) {
+            if (XT == 1) {
 #pragma unroll
                 for (int k = 0; k < TPL; ++k)
 #pragma unroll
-                    for (int c = 0; c < 9; ++c) xt[c][k] += (double)xq[XT ? k : 0][c];
+                    for (int c = 0; c < 9; ++c) xt[c][k] += (double)xq[XT == 1 ? k : 0][c];
             }
             __syncwarp();
         };
@@ -511,14 +515,14 @@ walk_kernel(const WalkArgs A) {
         auto flush_pp = [&](int n) {
             __syncwarp();
             float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
-            float xq[XT ? TPL : 1][9];
+            float xq[XT == 1 ? TPL : 1][9];
 #pragma unroll
             for (int k = 0; k < TPL; ++k) ax_[k] = ay_[k] = az_[k] = ap_[k] = 0.0f;
-            if (XT) {
+            if (XT == 1) {
 #pragma unroll
                 for (int k = 0; k < TPL; ++k)
 #pragma unroll
-                    for (int c = 0; c < 9; ++c) xq[XT ? k : 0][c] = 0.0f;
+                    for (int c = 0; c < 9; ++c) xq[XT == 1 ? k : 0][c] = 0.0f;
             }
             unsigned zero = 0;
             for (int j = slice; j < n; j += NS) {
@@ -537,33 +541,33 @@ walk_kernel(const WalkArgs A) {
                             const float mri = e.w * ri;
                             f = mri * ri * ri;
                             p = -mri;
-                            if (XT) g2 = 3.0f * f * (ri * ri);
+                            if (XT == 1) g2 = 3.0f * f * (ri * ri);
                             fa = f;
-                        } else if (XT) {
+                        } else if (XT == 1) {
                             spline_pair_tidal(r2, hh, e.w, f, p, g2);
                             fa = want_zeta ? f - zeta_pair(r2, hh, hj, pzs[j], tzm[k], tim[k]) : f;
                         } else {
                             spline_pair(r2, hh, e.w, f, p);
-                            fa = f;
+                            fa = (XT == 2 && want_zeta) ? f - zeta_pair(r2, hh, hj, pzs[j], tzm[k], tim[k]) : f;
                         }
                         if (COUNT) zero += (r2 == 0.0f);
                         ax_[k] = fmaf(dx, fa, ax_[k]);
                         ay_[k] = fmaf(dy, fa, ay_[k]);
                         az_[k] = fmaf(dz, fa, az_[k]);
                         if (WANT_POT) ap_[k] += p;
-                        if (XT) {
+                        if (XT == 1) {
                             const float4 ev = want_jerk ? ppv[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-                            xt_add(xq[XT ? k : 0], dx, dy, dz, f, g2, ev, k);
+                            xt_add(xq[XT == 1 ? k : 0], dx, dy, dz, f, g2, ev, k);
                         }
                     }
                 }
             }
             accumulate(ax_, ay_, az_, ap_);
-            if (XT) {
+            if (XT == 1) {
 #pragma unroll
                 for (int k = 0; k < TPL; ++k)
 #pragma unroll
-                    for (int c = 0; c < 9; ++c) xt[c][k] += (double)xq[XT ? k : 0][c];
+                    for (int c = 0; c < 9; ++c) xt[c][k] += (double)xq[XT == 1 ? k : 0][c];
             }
             if (COUNT) c_zero += zero;
             __syncwarp();
@@ -747,7 +751,7 @@ walk_kernel(const WalkArgs A) {
                 vz += __shfl_xor_sync(kFull, vz, o);
                 if (WANT_POT) vp += __shfl_xor_sync(kFull, vp, o);
             }
-            if (XT) {
+            if (XT == 1) {
 #pragma unroll
                 for (int c = 0; c < 9; ++c)
                     for (int o = NT; o < 32; o <<= 1) xt[c][k] += __shfl_xor_sync(kFull, xt[c][k], o);
@@ -946,20 +950,20 @@ int64_t finish_groups(gt_context* ctx, const uint32_t* flag, int64_t n, int kmax
     return nc;
 }
 
-size_t walk_smem(int warps, bool mac, int pn_cap, bool xt = false) {
-    return (size_t)warps * warp_smem_bytes(pn_cap, pn_cap / 2, xt) + (mac ? kMacModel * sizeof(float) : 0);
+size_t walk_smem(int warps, bool mac, int pn_cap, int ext = 0) {
+    return (size_t)warps * warp_smem_bytes(pn_cap, pn_cap / 2, ext) + (mac ? kMacModel * sizeof(float) : 0);
 }
 
 // Dynamic shared memory above 48 KB needs a per-kernel opt-in, done once per instantiation.
-template <int TPL, bool LA, bool POT, bool CNT, int MAC, bool XT = false>
+template <int TPL, bool LA, bool POT, bool CNT, int MAC, int XT = 0>
 void prepare_walk() {
     static bool done = false;
     if (done) return;
-    // the largest request of this instantiation: 8 warps at the largest list capacity (XT lists
-    // carry velocities too, so XT stops at half the capacity)
+    // the largest request of this instantiation: 8 warps at the largest list capacity (XT 1 lists
+    // carry velocities too, so XT 1 stops at half the capacity)
     check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT, MAC, XT>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)walk_smem(kMaxWarps, MAC == 1, XT ? kPnCapMax / 2 : kPnCapMax, XT)),
+                                    (int)walk_smem(kMaxWarps, MAC == 1, XT == 1 ? kPnCapMax / 2 : kPnCapMax, XT)),
                "cudaFuncSetAttribute");
     // the lists need 3 blocks x 55 KB per SM: ask for the largest shared-memory carveout
     check_cuda(cudaFuncSetAttribute(walk_kernel<TPL, LA, POT, CNT, MAC, XT>,
@@ -968,7 +972,7 @@ void prepare_walk() {
     done = true;
 }
 
-template <int TPL, bool LA, bool POT, bool CNT, int MAC, bool XT = false>
+template <int TPL, bool LA, bool POT, bool CNT, int MAC, int XT = 0>
 void launch_walk(gt_context* ctx, const WalkArgs& a, int blocks, int warps) {
     prepare_walk<TPL, LA, POT, CNT, MAC, XT>();
     walk_kernel<TPL, LA, POT, CNT, MAC, XT><<<blocks, warps * 32, walk_smem(warps, MAC == 1, a.pn_cap, XT),
@@ -984,17 +988,24 @@ void dispatch_count(gt_context* ctx, const WalkArgs& a, int blocks, int warps, b
 
 // Tidal tensor / jerk / gas rules: plain criterion, groups of at most 32 targets.  The per-target
 // walk (no leaf acceptance) only for the gas rules of accelerations.
-void dispatch_xt(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la, bool pot, bool cnt) {
+template <int EXT>
+void dispatch_ext_level(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la, bool pot, bool cnt) {
     if (!la) {
-        if (cnt) launch_walk<1, false, false, true, 0, true>(ctx, a, blocks, warps);
-        else launch_walk<1, false, false, false, 0, true>(ctx, a, blocks, warps);
+        if (cnt) launch_walk<1, false, false, true, 0, EXT>(ctx, a, blocks, warps);
+        else launch_walk<1, false, false, false, 0, EXT>(ctx, a, blocks, warps);
     } else if (pot) {
-        if (cnt) launch_walk<1, true, true, true, 0, true>(ctx, a, blocks, warps);
-        else launch_walk<1, true, true, false, 0, true>(ctx, a, blocks, warps);
+        if (cnt) launch_walk<1, true, true, true, 0, EXT>(ctx, a, blocks, warps);
+        else launch_walk<1, true, true, false, 0, EXT>(ctx, a, blocks, warps);
     } else {
-        if (cnt) launch_walk<1, true, false, true, 0, true>(ctx, a, blocks, warps);
-        else launch_walk<1, true, false, false, 0, true>(ctx, a, blocks, warps);
+        if (cnt) launch_walk<1, true, false, true, 0, EXT>(ctx, a, blocks, warps);
+        else launch_walk<1, true, false, false, 0, EXT>(ctx, a, blocks, warps);
     }
+}
+
+// ext 1: the tidal-tensor / jerk kernel (the gas rules too); ext 2: the gas rules alone
+void dispatch_xt(gt_context* ctx, const WalkArgs& a, int blocks, int warps, int ext, bool la, bool pot, bool cnt) {
+    if (ext == 1) dispatch_ext_level<1>(ctx, a, blocks, warps, la, pot, cnt);
+    else dispatch_ext_level<2>(ctx, a, blocks, warps, la, pot, cnt);
 }
 
 // The learned criteria are grouped-walk options (leaves offered to the criterion).
@@ -1031,7 +1042,7 @@ __global__ void chunk_bounds_kernel(const int2* __restrict__ groups, int ng, int
     }
 }
 
-template <int TPL, bool LA, bool POT, bool CNT, int MAC, bool XT = false>
+template <int TPL, bool LA, bool POT, bool CNT, int MAC, int XT = 0>
 int occupancy_blocks(int warps, int pn_cap) {
     prepare_walk<TPL, LA, POT, CNT, MAC, XT>();
     int nb = 0;
@@ -1066,7 +1077,10 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     // The tidal tensor, the jerk and the gas rules run on the XT kernel.
     const bool zeta_on = t->szeta && t->gas_zeta && rq.want_acc && rq.ax;
     const bool sink_on = t->nsink && rq.sink_radius > 0.0 && rq.leaf_accept;
-    const bool xt = rq.tidal != nullptr || rq.jerk != nullptr || zeta_on || sink_on;
+    // ext 1: the tidal tensor or the jerk (with the gas rules if the tree has them); ext 2: the gas
+    // rules alone.  Both walk groups of at most 32 targets.
+    const int ext = (rq.tidal != nullptr || rq.jerk != nullptr) ? 1 : ((zeta_on || sink_on) ? 2 : 0);
+    const bool xt = ext != 0;
     int kmax = 32;
     if (!xt && (mode == GT_GROUP_NODE || mode == GT_GROUP_BATCH) && param > 32) kmax = param > 64 ? 128 : 64;
     const int tpl = kmax / 32;
@@ -1151,11 +1165,13 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
             throw Fail{GT_ERR_INVALID, "list_capacity must be a multiple of 32 in [64, 1024]"};
         pn_cap = rq.list_capacity;
     }
-    if (xt && pn_cap > kPnCapMax / 2)
+    if (ext == 1 && pn_cap > kPnCapMax / 2)
         throw Fail{GT_ERR_INVALID, "list_capacity must be at most 512 with the tidal tensor or the jerk"};
     int per_sm;
-    if (xt)
-        per_sm = occupancy_blocks<1, true, false, false, 0, true>(warps, pn_cap);
+    if (ext == 1)
+        per_sm = occupancy_blocks<1, true, false, false, 0, 1>(warps, pn_cap);
+    else if (ext == 2)
+        per_sm = occupancy_blocks<1, true, false, false, 0, 2>(warps, pn_cap);
     else if (tpl == 1)
         per_sm = mac ? occupancy_blocks<1, true, false, false, 1>(warps, pn_cap)
                : macn ? occupancy_blocks<1, true, false, false, 2>(warps, pn_cap)
@@ -1192,7 +1208,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     const int total_warps = blocks * warps;
     a.pn_cap = pn_cap;
     a.pp_cap = pn_cap / 2;
-    a.warp_bytes = warp_smem_bytes(a.pn_cap, a.pp_cap, xt);
+    a.warp_bytes = warp_smem_bytes(a.pn_cap, a.pp_cap, ext);
     a.tidal = rq.tidal;
     a.jerk = rq.jerk;
     a.svel = t->svel;
@@ -1290,7 +1306,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                 ac.group_root = roots ? roots + g0 : nullptr;
                 ac.next_group = (unsigned int*)(ctr + 10) + c;
                 const int cb = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, ((int64_t)(g1 - g0) + warps - 1) / warps));
-                if (xt) dispatch_xt(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false);
+                if (xt) dispatch_xt(ctx, ac, cb, warps, ext, rq.leaf_accept, want_pot, false);
                 else if (tpl == 1) dispatch<1>(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false, rq.mac);
                 else if (tpl == 2) dispatch<2>(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false, rq.mac);
                 else dispatch<4>(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false, rq.mac);
@@ -1322,7 +1338,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         a.stack_cap = stack_cap;
         check_cuda(cudaMemsetAsync(ctr, 0, 96, st), "memset counters");
         if (!rq.capture) check_cuda(cudaEventRecord(ctx->ev0, st), "event");
-        if (xt) dispatch_xt(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count);
+        if (xt) dispatch_xt(ctx, a, blocks, warps, ext, rq.leaf_accept, want_pot, rq.count);
         else if (tpl == 1) dispatch<1>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
         else if (tpl == 2) dispatch<2>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
         else dispatch<4>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
