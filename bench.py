@@ -15,6 +15,10 @@ measured against an FP64 direct sum on a seeded 4096-particle sample.
 the reference sources into oracle/_ref) on a bounded sample of whole leaf groups of the same
 workload, with every host thread.
 
+Other workloads: --workload plummer_batch_256 (256 systems in one forest, autotuned, one captured
+graph), --workload extras_galaxy_4m (the tidal tensor, the jerk, the gas rules and tree reuse on the
+4M galaxy), --workload density_galaxy_4m / density_clustered_16m (the density solve).
+
 Multi-GPU (--gpus N under torchrun): every rank walks its own independent system of the same
 size (seed + rank); there is no data-path collective, only the barrier and a max over ranks of the
 timed region ("scaling": "weak").
