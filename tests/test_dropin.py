@@ -167,3 +167,56 @@ def test_bench_density_through_the_shim_matches_the_reference(tmp_path):
     for pat in (r"([0-9.]+) kept/target", r"(\d+) leaf groups, (\d+) singleton", r"sum\(examined\)=(\d+)\s+union\(examined\)=(\d+)"):
         a, b = (re.search(pat, txt[k]).groups() for k in ("gpu", "ref"))
         assert a == b, (pat, a, b)
+
+
+def _blocks(path):
+    raw = np.fromfile(path, np.uint8)
+    out, off = [], 0
+    kinds = ["i", "i", "f", "f", "i", "i", "i", "i", "i", "i"]
+    for k in kinds:
+        n = int(np.frombuffer(raw[off:off + 8], np.int64)[0])
+        off += 8
+        out.append(np.frombuffer(raw[off:off + 8 * n], np.int64 if k == "i" else np.float64))
+        off += 8 * n
+    return out
+
+
+@pytest.mark.gpu
+def test_neighbour_search_through_the_shim_matches_the_reference(tmp_path):
+    """tests/dropin/ngb_check.cc -- the density solve with its neighbour cache, Tree::init_hmax,
+    and per-centre ngb_search / ngb_search_reverse -- compiled against the shim (GPU) and against
+    the reference's own hydro (oracle/_ref, CPU).  The solve agrees to 1e-10 with identical
+    iteration and neighbour counts on at least 99.5 % of targets; wherever the iterations agree,
+    the cached lists and both searches return the same particles in the same order."""
+    from gizmo_shared_memory_b200 import ics
+
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "ngb_check")
+    if not os.path.exists(ref_bin):
+        pytest.skip("oracle/_ref/ngb_check not built (reference sources unavailable at build time)")
+    P, vel = ics.plummer_state(n=40000, seed=19)
+    state = tmp_path / "state.bin"
+    ics.write_state(str(state), P, vel)
+    outs = {}
+    for name, exe in (("gpu", binary("ngb_check")), ("ref", ref_bin)):
+        path = tmp_path / f"{name}.bin"
+        r = subprocess.run([exe, str(state), str(path)], capture_output=True, text=True, timeout=900,
+                           env=dict(os.environ, OMP_NUM_THREADS="4"))
+        assert r.returncode == 0, (name, r.stdout[-2000:], r.stderr[-2000:])
+        outs[name] = _blocks(path)
+    g_, r_ = outs["gpu"], outs["ref"]
+    same = g_[1] == r_[1]
+    assert same.mean() >= 0.995
+    assert np.array_equal(g_[0][same], r_[0][same])
+    for k in (2, 3):
+        e = np.abs(g_[k] - r_[k]) / np.abs(r_[k])
+        assert e[same].max() <= 1e-10, (k, e[same].max())
+    # the cache: per target, the same list wherever the iterations agree
+    cs_g, cf_g, cs_r, cf_r = g_[4], g_[5], r_[4], r_[5]
+    for t in np.nonzero(same)[0]:
+        assert np.array_equal(cf_g[cs_g[t]:cs_g[t + 1]], cf_r[cs_r[t]:cs_r[t + 1]]), t
+    # the searches of every 50th target
+    sub = same[::50]
+    for s_g, f_g, s_r, f_r in ((g_[6], g_[7], r_[6], r_[7]), (g_[8], g_[9], r_[8], r_[9])):
+        assert len(s_g) == len(s_r)
+        for i in np.nonzero(sub)[0]:
+            assert np.array_equal(f_g[s_g[i]:s_g[i + 1]], f_r[s_r[i]:s_r[i + 1]]), i
