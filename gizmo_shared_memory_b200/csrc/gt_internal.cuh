@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -163,6 +164,9 @@ struct gt_tree {
         int64_t n_groups = 0;
     };
     std::vector<GroupCache> group_cache;
+    // guards the state made on first use (the group cache, the search nodes): trees may be used by
+    // contexts on several threads
+    std::mutex lazy_mu;
 };
 
 namespace gt {

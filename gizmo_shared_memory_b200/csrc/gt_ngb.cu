@@ -416,18 +416,23 @@ SearchGeom geom_of(gt_context* ctx, gt_tree* t, double elapsed, double box) {
 
 }  // namespace
 
+// Made once per tree, under the tree's lock: contexts on other threads and streams may search the
+// same tree, so the nodes are complete on the device before the pointer is published.
 void ensure_snodes(gt_context* ctx, gt_tree* t) {
-    if (t->snode || t->n_nodes <= 0) return;
+    if (t->n_nodes <= 0) return;
     if (t->n_systems > 1) throw Fail{GT_ERR_UNSUPPORTED, "the neighbour search works on single-system trees"};
+    std::lock_guard<std::mutex> lk(t->lazy_mu);
+    if (t->snode) return;
     SNodeG* p = nullptr;
     check_cuda(cudaMallocAsync((void**)&p, (size_t)t->n_nodes * sizeof(SNodeG), ctx->stream), "cudaMallocAsync");
-    t->snode = p;
     double root_size = 0.0;
     check_cuda(cudaMemcpyAsync(&root_size, t->size, 8, cudaMemcpyDeviceToHost, ctx->stream), "d2h");
     check_cuda(cudaStreamSynchronize(ctx->stream), "sync");
     pack_snode_kernel<<<grid_of(ctx, t->n_nodes), kBlk, 0, ctx->stream>>>(t->nodes, t->next, t->gc, t->size,
                                                                           t->n_nodes, 1e-6 * root_size, p);
     check_launch(ctx, "pack_snode_kernel");
+    check_cuda(cudaStreamSynchronize(ctx->stream), "sync");
+    t->snode = p;
 }
 
 void tree_hmax(gt_context* ctx, gt_tree* t, const double* h, int64_t n_gas) {

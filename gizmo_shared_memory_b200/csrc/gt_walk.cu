@@ -1091,6 +1091,9 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     int64_t ng = 0;
     const uint32_t* tpos = nullptr;
     if (all) {
+        // the cache is shared by every context that walks this tree: look up and fill it under
+        // the tree's lock, and publish a new list only once it is complete on the device
+        std::lock_guard<std::mutex> lk(t->lazy_mu);
         for (auto& c : t->group_cache)
             if (c.mode == mode && c.param == param && c.kmax == kmax) {
                 groups = c.groups; roots = c.roots; ng = c.n_groups;
@@ -1124,6 +1127,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                                                                    t->n_systems, roots);
                 check_launch(ctx, "group_root_kernel");
             }
+            if (!rq.capture) check_cuda(cudaStreamSynchronize(st), "sync");
             gt_tree::GroupCache c;
             c.mode = mode; c.param = param; c.kmax = kmax; c.groups = groups; c.roots = roots; c.n_groups = ng;
             t->group_cache.push_back(c);

@@ -19,7 +19,10 @@
  *    (shmem/tree.h:389-394).  targets == NULL means "every live particle in tree order", i.e.
  *    targets = orderbuf (what shmem/bench_treeforce.cc:41 passes).
  *  - One context per host thread; one CUDA stream per context.  Trees may be used by any context
- *    on the same device.
+ *    on the same device, and walks and searches of one tree may run from several contexts at
+ *    once (what a tree builds on first use is made under a lock).  Calls that change a tree
+ *    (gt_tree_events, _refresh, _particles, _velocities, _gas, _hmax) must not overlap other calls
+ *    on that tree: the caller orders them.
  *  - Options the GPU path does not implement (lazy drift inside the walk, periodic boxes) are
  *    rejected with GT_ERR_UNSUPPORTED; there is no CPU fallback.
  */

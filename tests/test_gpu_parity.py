@@ -437,3 +437,32 @@ def test_host_outputs_copied_in_chunks_are_identical(gpu_ctx):
     b_dev = gpu_ctx.accel_grouped(T, torch.as_tensor(tg.view(np.int32), device="cuda"), theta=0.6)
     for d, h in zip(b_dev, b_host):
         assert np.array_equal(d.cpu().numpy(), h)
+
+
+def test_walks_and_searches_from_several_threads(gpu_ctx):
+    """Four host threads, each with its own context, walk and search one fresh tree at the same
+    time: the group list and the search nodes it builds on first use are made once, under the
+    tree's lock, and every thread gets the single-thread results."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    P = ics.plummer(n=300000, seed=14, soft=0.01)
+    rng = np.random.default_rng(2)
+    cen = [rng.normal(0.0, 0.5, 5000) for _ in range(3)]
+    rad = np.full(5000, 0.05)
+    ref_tree = gpu_ctx.build(P)
+    ref_w = gpu_ctx.accel_grouped(ref_tree, None, theta=0.6, group_mode=g.GT_GROUP_BATCH, batch=32)
+    ref_s = gpu_ctx.ngb_search(ref_tree, *cen, rad)
+    T = gpu_ctx.build(P)
+
+    def work(_):
+        ctx = g.Context(0)
+        w = ctx.accel_grouped(T, None, theta=0.6, group_mode=g.GT_GROUP_BATCH, batch=32)
+        s = ctx.ngb_search(T, *cen, rad)
+        ctx.close()
+        return w, s
+
+    with ThreadPoolExecutor(4) as ex:
+        for w, s in ex.map(work, range(4)):
+            for a, b in zip(w, ref_w):
+                assert np.array_equal(a, b)
+            assert np.array_equal(s[0], ref_s[0]) and np.array_equal(s[1], ref_s[1])
