@@ -44,6 +44,7 @@ EXPORTS = [
     "gt_accel_grouped_ext", "gt_tree_velocities", "gt_tree_velocity_moments", "gt_tree_events",
     "gt_tree_refresh", "gt_tree_node_state", "gt_tree_particles", "gt_tree_gas",
     "gt_ngb_options_default", "gt_tree_hmax", "gt_ngb_search", "gt_density_options_default", "gt_density",
+    "gt_direct_gas",
 ]
 
 
@@ -165,6 +166,7 @@ def load_library(path: str = LIB_PATH):
     L.gt_tree_node_state.argtypes = [vp, vp, d, vp, vp, vp, vp, vp]
     L.gt_tree_particles.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int]
     L.gt_tree_gas.argtypes = [vp, vp, vp, vp, C.c_int]
+    L.gt_direct_gas.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp, vp, i64, vp, d, C.c_int, vp, vp, vp]
     L.gt_ngb_options_default.restype = None
     L.gt_ngb_options_default.argtypes = [vp]
     L.gt_tree_hmax.argtypes = [vp, vp, vp, C.c_int64, C.c_int]
@@ -742,6 +744,21 @@ class Context:
         self._check(load_library().gt_form_aold(self.h, n, _ptr(ax), _ptr(ay), _ptr(az), alpha, G,
                                                 GT_MEM_DEVICE if dev else GT_MEM_HOST, _ptr(out)))
         return out if dev else out[:n]
+
+    def direct_gas(self, P, targets, type=None, zeta=None, G=1.0):
+        """FP64 direct sum with the zeta terms of gas-gas pairs (accel_brute on particles with
+        types and zeta); host arrays.  Returns (ax, ay, az)."""
+        x, y, z, m = (np.ascontiguousarray(P[k], np.float64) for k in ("x", "y", "z", "m"))
+        soft = P.get("soft")
+        soft = None if soft is None else np.ascontiguousarray(soft, np.float64)
+        ty = None if type is None else np.ascontiguousarray(type, np.uint8)
+        ze = None if zeta is None else np.ascontiguousarray(zeta, np.float64)
+        t = np.ascontiguousarray(targets, np.uint32)
+        ax, ay, az = np.empty(max(len(t), 1)), np.empty(max(len(t), 1)), np.empty(max(len(t), 1))
+        self._check(load_library().gt_direct_gas(self.h, len(m), _ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(soft),
+                                                 _ptr(ty), _ptr(ze), len(t), _ptr(t), G, GT_MEM_HOST, _ptr(ax),
+                                                 _ptr(ay), _ptr(az)))
+        return ax[:len(t)], ay[:len(t)], az[:len(t)]
 
     def direct(self, P, targets, G=1.0, precision=GT_DIRECT_FP64, want_phi=True):
         x, y, z, m = P["x"], P["y"], P["z"], P["m"]

@@ -1039,6 +1039,38 @@ int gt_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay,
     });
 }
 
+int gt_direct_gas(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z, const double* m,
+                  const double* soft, const uint8_t* type, const double* zeta, int64_t n_targets,
+                  const uint32_t* targets, double G, int mem, double* ax, double* ay, double* az) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        check_mem(mem);
+        if (n < 0 || n_targets < 0) throw Fail{GT_ERR_INVALID, "negative size"};
+        if (n > 0 && (!x || !y || !z || !m)) throw Fail{GT_ERR_INVALID, "null source array"};
+        if (n_targets > 0 && (!targets || !ax || !ay || !az)) throw Fail{GT_ERR_INVALID, "null targets or output"};
+        if (mem == GT_MEM_HOST)
+            for (int64_t k = 0; k < n_targets; ++k)
+                if ((int64_t)targets[k] >= n) throw Fail{GT_ERR_INVALID, "target index out of range"};
+        DeviceGuard dg(ctx->device);
+        const double* dx = stage_in(ctx, kSlotIn0, x, n, mem);
+        const double* dy = stage_in(ctx, kSlotIn1, y, n, mem);
+        const double* dz = stage_in(ctx, kSlotIn2, z, n, mem);
+        const double* dm = stage_in(ctx, kSlotIn3, m, n, mem);
+        const double* ds = stage_in(ctx, kSlotIn4, soft, n, mem);
+        const uint8_t* dty = stage_in(ctx, kSlotNodeTmp2, type, n, mem);
+        const double* dze = stage_in(ctx, kSlotNodeTmp0, zeta, n, mem);
+        const uint32_t* dt = stage_in(ctx, kSlotTargets, targets, n_targets, mem);
+        double* oax = out_buf(ctx, kSlotOut0, ax, n_targets, mem);
+        double* oay = out_buf(ctx, kSlotOut1, ay, n_targets, mem);
+        double* oaz = out_buf(ctx, kSlotOut2, az, n_targets, mem);
+        run_direct_gas(ctx, n, dx, dy, dz, dm, ds, dty, dze, n_targets, dt, G, oax, oay, oaz);
+        copy_out(ctx, ax, (const double*)oax, n_targets, mem);
+        copy_out(ctx, ay, (const double*)oay, n_targets, mem);
+        copy_out(ctx, az, (const double*)oaz, n_targets, mem);
+        finish(ctx, true);
+    });
+}
+
 int gt_direct(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
               const double* m, const double* soft, int64_t n_targets, const uint32_t* targets,
               double G, int precision, int mem, double* ax, double* ay, double* az, double* phi) {

@@ -10,6 +10,7 @@
 //   FP32: the pair offset is differenced in double and narrowed, everything after it is float
 //         (grav_cuda.cu:108-134 without zeta terms or a periodic wrap).
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 
 #include "gt_internal.cuh"
@@ -68,18 +69,47 @@ __device__ __forceinline__ void spline_f(float r, float h, float& f, float& p) {
     }
 }
 
-template <bool FP64>
+// dW/dr of the 3-D cubic spline of support h (shmem/hydro.h:46-54), FP64, zero from r = h.
+__device__ __forceinline__ double kernel_dwdr_d(double r, double h) {
+    const double q = r / h;
+    if (q >= 1.0) return 0.0;
+    const double norm = 8.0 / (M_PI * h * h * h);
+    double fp;
+    if (q < 0.5) {
+        fp = -12.0 * q + 18.0 * q * q;
+    } else {
+        const double u = 1.0 - q;
+        fp = -6.0 * u * u;
+    }
+    return norm * fp / h;
+}
+
+// GAS (FP64 only): the adaptive-softening zeta terms of gas-gas pairs (tree.cc:39-53); type
+// (0 = gas; null = every particle gas) and zeta (null = none) are indexed like the particles.
+template <bool FP64, bool GAS = false>
 __global__ void __launch_bounds__(kDirThreads)
 direct_kernel(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
               const double* __restrict__ m, const double* __restrict__ soft, int64_t n,
               const uint32_t* __restrict__ targets, int64_t nt, int64_t chunk,
-              double* __restrict__ partial) {
+              double* __restrict__ partial, const uint8_t* __restrict__ type = nullptr,
+              const double* __restrict__ zeta = nullptr) {
     __shared__ double shx[kDirTile], shy[kDirTile], shz[kDirTile], shm[kDirTile], shs[kDirTile];
+    __shared__ double shzeta[GAS ? kDirTile : 1];
+    __shared__ unsigned char shgas[GAS ? kDirTile : 1];
     const int64_t t = (int64_t)blockIdx.x * kDirThreads + threadIdx.x;
     const bool live = t < nt;
     const int64_t self = live ? (int64_t)targets[t] : -1;
     const double px = live ? x[self] : 0.0, py = live ? y[self] : 0.0, pz = live ? z[self] : 0.0;
     const double ps = (live && soft) ? soft[self] : 0.0;
+    // a gas target with mass: zeta_t / m_t and 1 / m_t of its pair terms
+    double tzm = 0.0, tm = 0.0, tzeta = 0.0;
+    bool tgas = false;
+    if (GAS && live) {
+        tgas = !type || type[self] == 0;
+        tzeta = zeta ? zeta[self] : 0.0;
+        tm = m[self];
+        if (tm > 0) tzm = tzeta / tm;
+    }
     const int64_t s0 = (int64_t)blockIdx.y * chunk, s1 = min(n, s0 + chunk);
     double ax = 0, ay = 0, az = 0, ap = 0;
     float fx = 0, fy = 0, fz = 0, fp = 0;
@@ -89,6 +119,10 @@ direct_kernel(const double* __restrict__ x, const double* __restrict__ y, const 
             shx[threadIdx.x] = x[q]; shy[threadIdx.x] = y[q]; shz[threadIdx.x] = z[q];
             shm[threadIdx.x] = m[q];
             shs[threadIdx.x] = soft ? soft[q] : 0.0;
+            if (GAS) {
+                shzeta[threadIdx.x] = zeta ? zeta[q] : 0.0;
+                shgas[threadIdx.x] = (!type || type[q] == 0) ? 1 : 0;
+            }
         }
         __syncthreads();
         const int nq = (int)min((int64_t)kDirTile, s1 - base);
@@ -102,7 +136,12 @@ direct_kernel(const double* __restrict__ x, const double* __restrict__ y, const 
                     const double e = fmax(fmax(ps, shs[k]), 1e-300);
                     double f, p;
                     spline_d(r, e, f, p);
-                    const double mf = shm[k] * f;
+                    double mf = shm[k] * f;
+                    if (GAS && tgas && shgas[k] && tm > 0.0) {
+                        const double es = fmax(shs[k], 1e-300);
+                        if (tzeta != 0.0 && r < e) mf -= tzm * kernel_dwdr_d(r, e) / r;
+                        if (shzeta[k] != 0.0 && r < es) mf -= (shzeta[k] / tm) * kernel_dwdr_d(r, es) / r;
+                    }
                     ax += ox * mf; ay += oy * mf; az += oz * mf;
                     ap += shm[k] * p;
                 } else {
@@ -172,6 +211,22 @@ void launch_direct(cudaStream_t st, int num_sms, int64_t n, const double* x, con
 }
 
 }  // namespace
+
+void run_direct_gas(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z, const double* m,
+                    const double* soft, const uint8_t* type, const double* zeta, int64_t nt, const uint32_t* targets,
+                    double G, double* ax, double* ay, double* az) {
+    if (nt <= 0) return;
+    int nchunk = 1;
+    const int64_t chunk = plan_chunks(n, nt, ctx->num_sms, 65535, nchunk);
+    double* partial = (double*)scratch(ctx, kSlotDirect, (size_t)nchunk * 4 * nt * 8);
+    const dim3 grid(div_up(nt, kDirThreads), nchunk);
+    direct_kernel<true, true><<<grid, kDirThreads, 0, ctx->stream>>>(x, y, z, m, soft, n, targets, nt, chunk, partial,
+                                                                     type, zeta);
+    direct_reduce_kernel<<<std::max(1, std::min(div_up(nt, 256), ctx->num_sms * 4)), 256, 0, ctx->stream>>>(
+        partial, nt, nchunk, G, ax, ay, az, nullptr);
+    ctx->launches += 2;
+    check_cuda(cudaGetLastError(), "direct_kernel");
+}
 
 void run_direct(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
                 const double* m, const double* soft, int64_t nt, const uint32_t* targets, double G,

@@ -274,6 +274,11 @@ void run_direct(gt_context* ctx, int64_t n, const double* x, const double* y, co
                 const double* m, const double* soft, int64_t nt, const uint32_t* targets, double G,
                 int precision, double* ax, double* ay, double* az, double* phi);
 
+// The FP64 direct sum with the zeta terms of gas-gas pairs; type / zeta may be null.
+void run_direct_gas(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z, const double* m,
+                    const double* soft, const uint8_t* type, const double* zeta, int64_t nt, const uint32_t* targets,
+                    double G, double* ax, double* ay, double* az);
+
 // Keys (gt_build.cu)
 void run_peano_keys(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
                     const double corner[3], double len, int bits, uint64_t* ph_hi, uint64_t* ph_lo,

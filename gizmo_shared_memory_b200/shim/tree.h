@@ -12,9 +12,8 @@
 //     depth-first allocation order; first/next threading, plo/phi, parent and leaf_of are
 //     consistent with it.
 //   * Equal keys keep particle-index order (the reference's parallel sort leaves them unordered).
-//   * Options the GPU path does not implement throw std::runtime_error naming the option: the
-//     zeta terms in accel_brute (the FP64 direct sum has no gas rule) and the neighbour-search
-//     bounds Tree::raise_hmax / Tree::init_hmax.
+//   * Options the GPU path does not implement throw std::runtime_error naming the option:
+//     build_node and setup_walk (the device build makes the whole tree in one call).
 //   * Lazy drift catches up every particle behind the target before the walk (the device walk
 //     reads all of them), not only those the walk reaches.
 //   * After the first tree event or refresh, each walk uploads the particles' current positions,

@@ -42,11 +42,6 @@ void check(int st, const char* what) {
     throw std::runtime_error(std::string("shmem (GPU): ") + what + " is not implemented on the GPU path");
 }
 
-// The FP64 direct sum (gt_direct) has no gas pair rule.
-void require_no_zeta(const Particles& P) {
-    for (double z : P.zeta)
-        if (z != 0.0) unsupported("accel_brute with the adaptive-softening zeta pair terms");
-}
 
 const double* soft_or_null(const Particles& P) { return P.soft.empty() ? nullptr : P.soft.data(); }
 
@@ -341,10 +336,17 @@ void potential(const Tree& T, const Particles& P, const std::vector<uint32_t>& t
 
 void accel_brute(const Particles& P, const std::vector<uint32_t>& targets, double G,
                  std::vector<double>& ax, std::vector<double>& ay, std::vector<double>& az) {
-    require_no_zeta(P);
     const size_t nt = targets.size();
     ax.assign(nt, 0.0); ay.assign(nt, 0.0); az.assign(nt, 0.0);
     if (!nt) return;
+    if (!P.zeta.empty()) {
+        // gas particles with zeta: the pair rule's correction terms (tree.cc:39-53)
+        check(gt_direct_gas(context(), (int64_t)P.size(), P.x.data(), P.y.data(), P.z.data(), P.m.data(),
+                            soft_or_null(P), P.type.empty() ? nullptr : P.type.data(), P.zeta.data(),
+                            (int64_t)nt, targets.data(), G, GT_MEM_HOST, ax.data(), ay.data(), az.data()),
+              "gt_direct_gas");
+        return;
+    }
     check(gt_direct(context(), (int64_t)P.size(), P.x.data(), P.y.data(), P.z.data(), P.m.data(),
                     soft_or_null(P), (int64_t)nt, targets.data(), G, GT_DIRECT_FP64, GT_MEM_HOST,
                     ax.data(), ay.data(), az.data(), nullptr), "gt_direct");

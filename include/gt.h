@@ -421,6 +421,15 @@ GT_API int gt_direct(gt_context* ctx, int64_t n, const double* x, const double* 
               const double* m, const double* soft, int64_t n_targets, const uint32_t* targets,
               double G, int precision, int mem, double* ax, double* ay, double* az, double* phi);
 
+/* The FP64 direct sum with the adaptive-softening zeta terms of gas-gas pairs: shmem::accel_brute
+ * (tree.h:450-451, tree.cc:946-971) on particles with types and zeta (Particles::type, ::zeta;
+ * pair_force_over_r, tree.cc:39-53).  type (0 = gas; NULL = every particle gas) and zeta (NULL =
+ * none) are indexed like the particles.  Accelerations only, times G. */
+GT_API int gt_direct_gas(gt_context* ctx, int64_t n, const double* x, const double* y, const double* z,
+                  const double* m, const double* soft, const uint8_t* type, const double* zeta,
+                  int64_t n_targets, const uint32_t* targets, double G, int mem, double* ax, double* ay,
+                  double* az);
+
 /* Allocation-free direct sum.  No counterpart in the reference: it exists for callers that cannot
  * allocate device memory at the point of the call -- an application whose pool allocator already
  * owns all free device memory, or one that must not trigger the implicit device-wide

@@ -854,6 +854,30 @@ void or_walk_groups_gas(const or_tree* t, int64_t nt, const uint32_t* targets, i
     free(pre);
 }
 
+/* accel_brute with the gas pair rule (tree.cc:946-971, 39-53): FP64 direct sum over all n
+ * particles; type (null = all gas) and zeta (null = 0) indexed like the particles. */
+void or_direct_gas(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                   const double* soft, const uint8_t* type, const double* zeta, int64_t nt,
+                   const uint32_t* targets, double G, double* ax, double* ay, double* az) {
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < nt; ++t) {
+        const uint32_t p = targets[t];
+        const double te = soft ? soft[p] : 0.0, zt = zeta ? zeta[p] : 0.0;
+        const int tg = type == NULL || type[p] == 0;
+        double sx = 0, sy = 0, sz = 0;
+        for (int64_t q = 0; q < n; ++q) {
+            if (q == (int64_t)p) continue;
+            const double ox = x[q] - x[p], oy = y[q] - y[p], oz = z[q] - z[p];
+            const double r = sqrt(ox * ox + oy * oy + oz * oz);
+            if (r <= 0) continue;
+            const double f = or_pair_fac(r, m[q], te, soft ? soft[q] : 0.0, zt, zeta ? zeta[q] : 0.0, m[p],
+                                         tg && (type == NULL || type[q] == 0));
+            sx += ox * f; sy += oy * f; sz += oz * f;
+        }
+        ax[t] = G * sx; ay[t] = G * sy; az[t] = G * sz;
+    }
+}
+
 /* Sinks (type 5) below every node (tree.cc:155-187); nsink has nnodes entries. */
 void or_node_sinks(const or_tree* t, const uint8_t* type, uint32_t* nsink) {
     for (int64_t i = 0; i < t->nnodes; ++i) {

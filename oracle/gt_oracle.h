@@ -84,6 +84,10 @@ void or_walk_groups_gas(const or_tree* t, int64_t nt, const uint32_t* targets, i
                         const int64_t* starts, double theta, double G, const double* aold,
                         const uint8_t* type, const double* zeta, double sink_radius, int leaf_accept,
                         double* ax, double* ay, double* az);
+/* accel_brute with the gas pair rule (tree.cc:946-971, 39-53). */
+void or_direct_gas(int64_t n, const double* x, const double* y, const double* z, const double* m,
+                   const double* soft, const uint8_t* type, const double* zeta, int64_t nt,
+                   const uint32_t* targets, double G, double* ax, double* ay, double* az);
 /* Sinks below each node (tree.cc:155-187); nnodes entries. */
 void or_node_sinks(const or_tree* t, const uint8_t* type, uint32_t* nsink);
 /* Neighbour search (shmem/hydro.cc:37-148) for n centres as CSR, in tree order: mode 0 gather

@@ -113,6 +113,8 @@ class Restatement:
         L.or_walk_groups_gas.argtypes = [C.c_void_p, C.c_int64, _u32, C.c_int64, _i64, C.c_double,
                                          C.c_double, _d, C.c_void_p, _d, C.c_double, C.c_int, _d, _d, _d]
         L.or_node_sinks.argtypes = [C.c_void_p, C.c_void_p, _u32]
+        L.or_direct_gas.argtypes = [C.c_int64, _d, _d, _d, _d, _d, C.c_void_p, _d, C.c_int64, _u32, C.c_double,
+                                    _d, _d, _d]
         L.or_ngb_search.argtypes = [C.c_void_p, C.c_int64, _d, _d, _d, _d, C.c_int, _d, C.c_int64, C.c_double,
                                     _i64, _u32, C.c_int64]
         L.or_init_hmax.argtypes = [C.c_void_p, _d, C.c_int64, _f]
@@ -156,6 +158,20 @@ class Restatement:
 
     def build(self, P, randomize_seed=-1, nodelta=False):
         return OracleTree(self, P, randomize_seed, nodelta)
+
+    def direct_gas(self, P, targets, type=None, zeta=None, G=1.0):
+        """accel_brute with the gas pair rule: FP64 direct sum with the zeta terms."""
+        x, y, z, m = (_f64(P[k]) for k in ("x", "y", "z", "m"))
+        soft = _f64(P["soft"]) if P.get("soft") is not None else None
+        ty = None if type is None else np.ascontiguousarray(type, np.uint8)
+        ze = None if zeta is None else _f64(zeta)
+        t = _targets(targets)
+        nt = len(t)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        self.L.or_direct_gas(len(m), _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), _p(soft, _d),
+                             None if ty is None else ty.ctypes.data, _p(ze, _d), nt, _p(t, _u32), G,
+                             _p(ax, _d), _p(ay, _d), _p(az, _d))
+        return ax, ay, az
 
     def direct(self, P, targets, G=1.0, want_phi=True):
         t = _targets(targets)

@@ -57,6 +57,8 @@ def gas_scenario(R):
     out["sub"] = sub
     for k, v in zip(("ax", "ay", "az"), T.accel(sub, 0.5)):
         out[f"acc_{k}"] = v
+    for k, v in zip(("ax", "ay", "az"), T.accel_brute(sub)):
+        out[f"brute_{k}"] = v
     return out
 
 

@@ -131,3 +131,12 @@ def test_bad_inputs_are_rejected(gpu_ctx, golden, gas_tree):
         gpu_ctx.tree_gas(T, golden["gas_type"], z)
     with pytest.raises(g.GTError):
         gpu_ctx.accel_grouped(gas_tree, None, theta=0.7, sink_direct_radius=-1.0)
+
+
+def test_gas_direct_sum_matches_reference(gpu_ctx, golden):
+    """gt_direct_gas, the FP64 direct sum with the zeta terms, against the reference's accel_brute
+    on the same particles: relative 1e-12 (FP64 in another summation order)."""
+    P = {k: golden[f"gas_{k}"] for k in ("x", "y", "z", "m", "soft")}
+    ax, ay, az = gpu_ctx.direct_gas(P, golden["gas_sub"], type=golden["gas_type"], zeta=golden["gas_zeta"])
+    e = relerr((ax, ay, az), golden_acc(golden, "brute"))
+    assert e.max() <= 1e-12, e.max()

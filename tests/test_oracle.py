@@ -336,3 +336,12 @@ def test_density_matches_golden(oracle, golden, case):
     assert np.array_equal(d["nngb"], golden[f"ngb_{case}_nngb"])
     np.testing.assert_allclose(d["h"], golden[f"ngb_{case}_h"], rtol=1e-12, atol=0)
     np.testing.assert_allclose(d["rho"], golden[f"ngb_{case}_rho"], rtol=1e-12, atol=0)
+
+
+def test_gas_direct_sum_matches_golden(oracle, golden):
+    """accel_brute with the zeta terms (tree.cc:946-971, 39-53): the FP64 restatement against the
+    reference's, to 1e-12."""
+    P, ty, ze = gas_particles(golden)
+    sub = golden["gas_sub"]
+    ax, ay, az = oracle.direct_gas(P, sub, type=ty, zeta=ze)
+    assert relerr(ax, ay, az, golden["gas_brute_ax"], golden["gas_brute_ay"], golden["gas_brute_az"]).max() < 1e-12
