@@ -80,7 +80,11 @@ class ClockSampler:
     def __init__(self, device_index):
         self.dev = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+        # the raw samples; the JSON line carries their summary
+        import tempfile
+
+        out_dir = os.environ.get("GT_CLOCKS_DIR", tempfile.gettempdir())
+        self.path = os.path.join(out_dir, f"clocks_rank{device_index}.csv")
 
     def start(self):
         try:
