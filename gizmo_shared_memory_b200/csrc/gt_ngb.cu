@@ -257,17 +257,33 @@ __device__ __forceinline__ void dens_add(double dx, double dy, double dz, double
 }
 
 // One evaluation at h: the sums over the GAS neighbours inside h, in tree order (hydro.cc:205-222).
+// The neighbours found are buffered and their kernel sums evaluated in runs, in the order found:
+// interleaving the FP64 sums with the traversal made the lanes of a warp that were still walking
+// wait on every neighbour another lane had found.
+constexpr int kDensBuf = 64;
+
 __device__ void dens_eval(const DensArgs& a, double px, double py, double pz, double h, DensSums& s) {
     dens_zero(s);
     const int dim = a.n_dims;
     const double norm = kernel_norm(h, dim);
+    int buf[kDensBuf];
+    int nb = 0;
+    auto drain = [&]() {
+        for (int i = 0; i < nb; ++i) {
+            const int sp = buf[i];
+            if (a.stype && __ldg(a.stype + sp) != 0) continue;
+            const double2 xy = __ldg(reinterpret_cast<const double2*>(a.g.src + sp));
+            const double zz = __ldg(reinterpret_cast<const double*>(a.g.src + sp) + 2);
+            dens_add(min_image(xy.x - px, a.g.box), min_image(xy.y - py, a.g.box), min_image(zz - pz, a.g.box),
+                     __ldg(a.smass + sp), h, norm, dim, s);
+        }
+        nb = 0;
+    };
     search<false>(a.g, px, py, pz, h, nullptr, 0, [&](uint32_t, int sp) {
-        if (a.stype && __ldg(a.stype + sp) != 0) return;
-        const double2 xy = __ldg(reinterpret_cast<const double2*>(a.g.src + sp));
-        const double zz = __ldg(reinterpret_cast<const double*>(a.g.src + sp) + 2);
-        dens_add(min_image(xy.x - px, a.g.box), min_image(xy.y - py, a.g.box), min_image(zz - pz, a.g.box),
-                 __ldg(a.smass + sp), h, norm, dim, s);
+        if (nb == kDensBuf) drain();
+        buf[nb++] = sp;
     });
+    drain();
 }
 
 // Rank-d inverse of the symmetric moments (xx yy zz xy yz xz), row-major, zero when degenerate
