@@ -372,7 +372,7 @@ __device__ __forceinline__ NewtonParams newton_params(const DensArgs& a) {
 
 // One thread per target: up to 100 iterations of evaluation and Newton step, then, when the solve
 // did not converge, one more evaluation at the final h (hydro.cc:189-297).
-__global__ void __launch_bounds__(kBlk) density_kernel(const DensArgs a) {
+__global__ void __launch_bounds__(kBlk, 6) density_kernel(const DensArgs a) {
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.nt; t += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t p = a.targets[t];
         const uint32_t sp = a.rank[p];
