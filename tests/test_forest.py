@@ -152,3 +152,36 @@ def test_forest_bad_offsets(gpu_ctx, batch):
     # the context stays usable
     T = gpu_ctx.build(split(P, off, 0))
     assert T.info()["n_live"] > 0
+
+
+def test_forest_with_gas_rules_bit_identical(gpu_ctx, batch):
+    """Gas data on a forest (types with sinks, zeta): the zeta terms and the sink rule act per
+    system exactly as on each system's own tree -- the per-node sink counts climb to each
+    system's root -- so the accelerations are bit-identical to the separate gas walks."""
+    P, off = batch
+    n = len(P["m"])
+    rng = np.random.default_rng(12)
+    ty = np.where(rng.uniform(size=n) < 0.7, 0, 4).astype(np.uint8)
+    ty[rng.choice(n, n // 50, replace=False)] = 5
+    soft = P["soft"] * rng.uniform(1.0, 20.0, n)
+    zeta = np.where(ty == 0, 0.1 * P["m"] ** 2 * soft ** 2 * rng.normal(0.0, 1.0, n), 0.0)
+    Q = dict(P, soft=soft)
+    F = gpu_ctx.build(Q, key_mode=g.GT_KEY_MORTON, offsets=off)
+    gpu_ctx.tree_gas(F, ty, zeta)
+    kw = dict(group_mode=g.GT_GROUP_BATCH, batch=32, out_order=g.GT_OUT_ORIGINAL, sink_direct_radius=0.5)
+    fx, fy, fz = gpu_ctx.accel_grouped(F, None, theta=0.7, **kw)
+    acted = False
+    for s in range(len(off) - 1):
+        sl = slice(off[s], off[s + 1])
+        if not (P["m"][sl] > 0).any():
+            continue
+        t = gpu_ctx.build({k: v[sl] for k, v in Q.items()}, key_mode=g.GT_KEY_MORTON)
+        gpu_ctx.tree_gas(t, ty[sl], zeta[sl])
+        sx, sy, sz = gpu_ctx.accel_grouped(t, None, theta=0.7, **kw)
+        m = P["m"][sl] > 0
+        for a, b in ((fx, sx), (fy, sy), (fz, sz)):
+            assert np.array_equal(a[sl][m], b[m])
+        plain = gpu_ctx.build({k: v[sl] for k, v in Q.items()}, key_mode=g.GT_KEY_MORTON)
+        px, _, _ = gpu_ctx.accel_grouped(plain, None, theta=0.7, **kw)
+        acted |= not np.array_equal(px[m], sx[m])
+    assert acted  # the gas rules changed some forces
