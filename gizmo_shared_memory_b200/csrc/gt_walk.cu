@@ -214,6 +214,24 @@ __device__ __noinline__ float zeta_pair(float r2, float h, float hs, float zs, f
     return c;
 }
 
+// 1/sqrt(x) by the PTX approximate reciprocal square root with flush-to-zero.  The monopole loops
+// floor r^2 at 1e-30, far above the FP32 subnormal range, so the flush never acts there and the
+// result equals rsqrtf's; the non-FTZ form only adds subnormal-range scaling instructions.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// max(0, lo - c, c - hi): the gap between coordinate c and the interval [lo, hi] (0 inside).
+// Written with comparisons; fmax on doubles costs more instructions and gives the same value
+// for every non-NaN input (and 0 here for a NaN c, as fmax does).
+__device__ __forceinline__ double box_gap(double lo, double c, double hi) {
+    const double a = lo - c, b = c - hi;
+    const double m = a > b ? a : b;
+    return m > 0.0 ? m : 0.0;
+}
+
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
     const float y = x - comp;
     const float t = sum + y;
@@ -420,7 +438,10 @@ walk_kernel(const WalkArgs A) {
         // {z0, z1, m0, m1}, so two 16-byte loads put a pair straight into the register pairs of the
         // sm_100 packed FP32 instructions (FADD2 / FMUL2 / FFMA2): two interactions per
         // instruction, each with exactly the scalar rounding.  An odd list is padded with a
-        // massless entry, which the r^2 guard turns into an exact zero.
+        // massless entry, which contributes an exact zero.  r^2 is floored at 1e-30 by starting
+        // its FMA chain at 1e-30 instead of 0: no extra instruction, and below the rounding of any
+        // r^2 above 1e-22, so only a point closer than FP32 resolves is affected (it then adds 0
+        // along that axis instead of a NaN).
         auto flush_pn = [&](int n) {
             if (paired && (n & 1) && lane == 0) pn_put(n, 0.0f, 0.0f, 0.0f, 0.0f);
             __syncwarp();
@@ -434,6 +455,7 @@ walk_kernel(const WalkArgs A) {
             if (paired) {
                 float2 ax2[TPL], ay2[TPL], az2[TPL], ap2[TPL];
                 float2 ntx[TPL], nty[TPL], ntz[TPL];
+                const float2 r2_floor = make_float2(1e-30f, 1e-30f);
 #pragma unroll
                 for (int k = 0; k < TPL; ++k) {
                     ax2[k] = ay2[k] = az2[k] = ap2[k] = make_float2(0.0f, 0.0f);
@@ -451,10 +473,8 @@ walk_kernel(const WalkArgs A) {
                         if (k < nk) {
                             const float2 dx = __fadd2_rn(X, ntx[k]), dy = __fadd2_rn(Y, nty[k]);
                             const float2 dz = __fadd2_rn(Z, ntz[k]);
-                            float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-                            r2.x = fmaxf(r2.x, 1e-30f);
-                            r2.y = fmaxf(r2.y, 1e-30f);
-                            const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+                            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, r2_floor)));
+                            const float2 ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
                             const float2 mri = __fmul2_rn(M, ri);
                             const float2 f = __fmul2_rn(mri, __fmul2_rn(ri, ri));
                             ax2[k] = __ffma2_rn(dx, f, ax2[k]);
@@ -485,8 +505,8 @@ walk_kernel(const WalkArgs A) {
                     for (int k = 0; k < TPL; ++k) {
                         if (k < nk) {
                             const float dx = e.x - tx[k], dy = e.y - ty[k], dz = e.z - tz[k];
-                            const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-30f);
-                            const float ri = rsqrtf(r2);
+                            const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 1e-30f)));
+                            const float ri = rsqrt_ftz(r2);
                             const float mri = e.w * ri;
                             const float f = mri * (ri * ri);
                             ax_[k] = fmaf(dx, f, ax_[k]);
@@ -591,9 +611,9 @@ walk_kernel(const WalkArgs A) {
             if (node >= 0) {
                 nd = load_node(A.nodes + node);
                 const bool leaf = nd.first < 0;
-                const double dx = fmax(0.0, fmax(S.lo_x - nd.cx, nd.cx - S.hi_x));
-                const double dy = fmax(0.0, fmax(S.lo_y - nd.cy, nd.cy - S.hi_y));
-                const double dz = fmax(0.0, fmax(S.lo_z - nd.cz, nd.cz - S.hi_z));
+                const double dx = box_gap(S.lo_x, nd.cx, S.hi_x);
+                const double dy = box_gap(S.lo_y, nd.cy, S.hi_y);
+                const double dz = box_gap(S.lo_z, nd.cz, S.hi_z);
                 const double r2 = dx * dx + dy * dy + dz * dz;
                 bool open = true;
                 if (MAC != 1) {
@@ -703,10 +723,11 @@ walk_kernel(const WalkArgs A) {
                             if (S.pre[l + step] <= q) l += step;
                         qpos = S.lo[l] + (q - S.pre[l]);
                         load_src(A.src + qpos, qx, qy, qz, qm, qh);
-                        const double ex = fmax(0.0, fmax(S.lo_x - qx, qx - S.hi_x));
-                        const double ey = fmax(0.0, fmax(S.lo_y - qy, qy - S.hi_y));
-                        const double ez = fmax(0.0, fmax(S.lo_z - qz, qz - S.hi_z));
-                        const double reach = fmax(S.emax, (double)qh);
+                        const double ex = box_gap(S.lo_x, qx, S.hi_x);
+                        const double ey = box_gap(S.lo_y, qy, S.hi_y);
+                        const double ez = box_gap(S.lo_z, qz, S.hi_z);
+                        const double qhd = (double)qh;
+                        const double reach = S.emax > qhd ? S.emax : qhd;
                         far = ex * ex + ey * ey + ez * ez > reach * reach;
                     }
                     const unsigned fm = __ballot_sync(kFull, live && far);
