@@ -37,8 +37,10 @@ void* scratch(gt_context* ctx, Slot s, size_t bytes) {
     bytes = std::max<size_t>(bytes, 4096);
     if (b.bytes >= bytes) return b.ptr;
     if (b.ptr) {
-        // a smaller buffer may still be read by queued work: wait for the stream before freeing
+        // a smaller buffer may still be read by queued work, or written by a queued upload on the
+        // copy stream: wait for both streams before freeing
         cudaStreamSynchronize(ctx->stream);
+        if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
         cudaFree(b.ptr);
         b.ptr = nullptr;
         b.bytes = 0;
@@ -52,6 +54,21 @@ void* scratch(gt_context* ctx, Slot s, size_t bytes) {
     }
     b.bytes = want;
     return b.ptr;
+}
+
+void ensure_copy_stream(gt_context* ctx) {
+    if (ctx->copy_stream) return;
+    // the events first: the stream marks the set as complete
+    auto make = [](cudaEvent_t& e) {
+        if (!e) check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    };
+    for (cudaEvent_t& e : ctx->chunk_ev) make(e);
+    for (cudaEvent_t& e : ctx->up_ev) make(e);
+    make(ctx->copy_done);
+    make(ctx->main_ev);
+    cudaStream_t s = nullptr;
+    check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+    ctx->copy_stream = s;
 }
 
 }  // namespace gt
@@ -186,7 +203,13 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     WalkRequest rq;
     rq.targets = all ? nullptr : stage_in(ctx, kSlotIn0, targets, nt, mem);
     rq.n_targets = nt;
-    rq.aold = stage_in(ctx, kSlotIn1, aold, nt, mem);
+    if (mem == GT_MEM_HOST && aold && nt > 0 && !capture) {
+        // the walk uploads it: per chunk, ahead of each chunk, when it splits the groups
+        rq.aold = (const double*)scratch(ctx, kSlotIn1, (size_t)nt * sizeof(double));
+        rq.host_aold = aold;
+    } else {
+        rq.aold = stage_in(ctx, kSlotIn1, aold, nt, mem);
+    }
     rq.theta = theta;
     rq.G = G;
     rq.group_mode = group_mode;
@@ -352,7 +375,10 @@ int gt_context_destroy(gt_context* ctx) {
     }
     for (cudaEvent_t e : ctx->chunk_ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->up_ev)
+        if (e) cudaEventDestroy(e);
     if (ctx->copy_done) cudaEventDestroy(ctx->copy_done);
+    if (ctx->main_ev) cudaEventDestroy(ctx->main_ev);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     cudaGetLastError();
     if (prev >= 0) cudaSetDevice(prev);
@@ -427,12 +453,29 @@ int build_common(gt_context* ctx, int64_t n, int32_t n_systems, const int64_t* o
         const double* dy = stage_in(ctx, kSlotIn1, y, n, mem);
         const double* dz = stage_in(ctx, kSlotIn2, z, n, mem);
         const double* dm = stage_in(ctx, kSlotIn3, m, n, mem);
-        const double* ds = stage_in(ctx, kSlotIn4, soft, n, mem);
-        build_tree(ctx, t, dx, dy, dz, dm, ds, n_systems, offsets);
+        const double* ds = nullptr;
+        cudaEvent_t soft_ready = nullptr;
+        if (mem == GT_MEM_HOST && soft && n > 0) {
+            // the softenings are first read in the gather stage: upload them on the copy stream
+            // once x, y, z, m are across, while the bounding box, keys and sort run
+            ensure_copy_stream(ctx);
+            double* d = (double*)scratch(ctx, kSlotIn4, (size_t)n * sizeof(double));
+            check_cuda(cudaEventRecord(ctx->main_ev, ctx->stream), "event");
+            check_cuda(cudaStreamWaitEvent(ctx->copy_stream, ctx->main_ev, 0), "wait");
+            check_cuda(cudaMemcpyAsync(d, soft, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->copy_stream),
+                       "H2D");
+            check_cuda(cudaEventRecord(ctx->copy_done, ctx->copy_stream), "event");
+            soft_ready = ctx->copy_done;
+            ds = d;
+        } else {
+            ds = stage_in(ctx, kSlotIn4, soft, n, mem);
+        }
+        build_tree(ctx, t, dx, dy, dz, dm, ds, n_systems, offsets, soft_ready);
         finish(ctx, true);
     });
     if (st != GT_OK) {
         cudaStreamSynchronize(ctx->stream);  // queued build work may still use the arrays
+        if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);  // and the softenings' upload
         cudaGetLastError();
         free_tree_arrays(t);
         delete t;

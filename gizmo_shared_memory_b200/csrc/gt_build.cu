@@ -279,13 +279,15 @@ __global__ void gather_kernel(const double* __restrict__ x, const double* __rest
                               int64_t n, SrcP* __restrict__ src, double* __restrict__ ssoft,
                               double* __restrict__ smass, uint32_t* __restrict__ order,
                               uint32_t* __restrict__ rank, int* __restrict__ leaf_of,
-                              int* __restrict__ sleaf) {
+                              int* __restrict__ sleaf, unsigned long long* __restrict__ bad_soft) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t p = idx[i];
         SrcP r;
         r.x = x[p]; r.y = y[p]; r.z = z[p];
         const double sp = soft ? soft[p] : 0.0;
+        // softenings that arrived after the bounding-box pass are checked here
+        if (bad_soft && !isfinite(sp)) atomicAdd(bad_soft, 1ull);
         r.m = (float)m[p];
         r.soft = (float)sp;
         src[i] = r;
@@ -637,7 +639,10 @@ void grow_nodes(gt_tree* t, int64_t need, cudaStream_t stream) {
 }  // namespace
 
 void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, const double* z,
-                const double* m, const double* soft, int n_systems, const int64_t* in_off) {
+                const double* m, const double* soft, int n_systems, const int64_t* in_off,
+                cudaEvent_t soft_ready) {
+    // with the softenings still on their way, the bounding-box pass checks x, y, z, m alone
+    const double* bbox_soft = soft_ready ? nullptr : soft;
     cudaStream_t st = ctx->stream;
     const int64_t n = t->n;
     const gt_build_options& o = t->opt;
@@ -661,7 +666,7 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
         const int nbb = std::max(1, std::min(ctx->num_sms * 2, div_up(std::max<int64_t>(n, 1), kBlk)));
         double* part = (double*)scratch(ctx, kSlotPartials, (size_t)nbb * 6 * 8 + (size_t)nbb * 16 + 256);
         unsigned long long* cnt = (unsigned long long*)(part + (size_t)nbb * 6);
-        bbox_partial_kernel<<<nbb, kBlk, 0, st>>>(x, y, z, m, soft, n, part, cnt);
+        bbox_partial_kernel<<<nbb, kBlk, 0, st>>>(x, y, z, m, bbox_soft, n, part, cnt);
         check_launch(ctx, "bbox_partial_kernel");
         root_geom_kernel<<<1, 1, 0, st>>>(part, cnt, nbb, gdev, bad_dev, o.randomize_seed, o.shift[0],
                                           o.shift[1], o.shift[2], o.max_level);
@@ -680,7 +685,7 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
         check_cuda(cudaMemcpyAsync(in_off_dev, in_off, (size_t)(S + 1) * 8, cudaMemcpyHostToDevice, st),
                    "offsets h2d");
         check_cuda(cudaMemsetAsync(bad_dev, 0, 8, st), "memset");
-        bbox_systems_kernel<<<(int)nparts, kBlk, 0, st>>>(x, y, z, m, soft, in_off_dev, chunks, part, cnt);
+        bbox_systems_kernel<<<(int)nparts, kBlk, 0, st>>>(x, y, z, m, bbox_soft, in_off_dev, chunks, part, cnt);
         check_launch(ctx, "bbox_systems_kernel");
         root_systems_kernel<<<div_up(S, 128), 128, 0, st>>>(part, cnt, S, chunks, gdev, bad_dev, o.randomize_seed,
                                                             o.shift[0], o.shift[1], o.shift[2], o.max_level);
@@ -756,9 +761,26 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
     t->sleaf = dalloc<int>(nalloc, st);
     t->skey = dalloc<uint64_t>(nalloc, st);
     if (n > 0) {
+        unsigned long long* bad_soft = nullptr;
+        if (soft_ready) {
+            check_cuda(cudaStreamWaitEvent(st, soft_ready, 0), "wait");
+            if (o.validate) {
+                bad_soft = bad_dev + 1;
+                check_cuda(cudaMemsetAsync(bad_soft, 0, 8, st), "memset");
+            }
+        }
         gather_kernel<<<grid_for(ctx, n), kBlk, 0, st>>>(x, y, z, m, soft, idx, n, t->src, t->ssoft,
-                                                         t->smass, t->order, t->rank, t->leaf_of, t->sleaf);
+                                                         t->smass, t->order, t->rank, t->leaf_of, t->sleaf,
+                                                         bad_soft);
         check_launch(ctx, "gather_kernel");
+        if (bad_soft) {
+            unsigned long long bad = 0;
+            check_cuda(cudaMemcpyAsync(ctx->pinned, bad_soft, 8, cudaMemcpyDeviceToHost, st), "d2h");
+            check_cuda(cudaStreamSynchronize(st), "sync");
+            std::memcpy(&bad, ctx->pinned, 8);
+            if (bad > 0)
+                throw Fail{GT_ERR_NONFINITE, "gt_build: " + std::to_string(bad) + " particle(s) with non-finite input"};
+        }
         check_cuda(cudaMemcpyAsync(t->skey, keys, (size_t)n * 8, cudaMemcpyDeviceToDevice, st), "skey");
     }
 

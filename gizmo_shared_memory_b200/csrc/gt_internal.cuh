@@ -93,10 +93,14 @@ struct gt_context {
     std::vector<gt::DevBuf> scratch;  // grow-only workspace slots, indexed by gt::Slot
     void* pinned = nullptr;           // small pinned host buffer for scalar read-backs
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // result copies overlapped with a walk split into chunks (made on first use)
+    // host copies overlapped with the main stream's work (made on first use): a walk split into
+    // chunks uploads each chunk's aold and copies its results back there; a build from host
+    // arrays uploads the softenings there while the bounding box, keys and sort run
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t chunk_ev[8] = {};
+    cudaEvent_t up_ev[8] = {};
     cudaEvent_t copy_done = nullptr;
+    cudaEvent_t main_ev = nullptr;
 };
 
 struct gt_tree {
@@ -208,8 +212,15 @@ void radix_sort_pairs(gt_context* ctx, uint64_t* keys, uint32_t* vals, int64_t n
 // Build (gt_build.cu)
 // n_systems > 1 builds a forest: particles of system s are the input range [in_off[s], in_off[s+1])
 // (host array of n_systems + 1), each system gets its own root cell and tree.
+// soft_ready (may be null): an event that the softenings' upload records; the build reads them
+// first in the gather stage and waits for it there, and it then checks them for non-finite values
+// in that stage instead of in the bounding-box pass.
 void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, const double* z,
-                const double* m, const double* soft, int n_systems = 1, const int64_t* in_off = nullptr);
+                const double* m, const double* soft, int n_systems = 1, const int64_t* in_off = nullptr,
+                cudaEvent_t soft_ready = nullptr);
+// The context's second stream (and its events), made on first use: host copies that overlap work
+// on the main stream.
+void ensure_copy_stream(gt_context* ctx);
 
 // Walk (gt_walk.cu)
 // Stack and counters owned by a walk plan (a captured graph must not point into the workspace).
@@ -249,6 +260,9 @@ struct WalkRequest {
         double *ax = nullptr, *ay = nullptr, *az = nullptr, *phi = nullptr, *tidal = nullptr, *jerk = nullptr;
         bool any() const { return ax || ay || az || phi || tidal || jerk; }
     } host;
+    // host source of aold not yet copied into the device buffer `aold`: the walk uploads it, per
+    // chunk ahead of each chunk when it splits the groups, else whole before its first kernel
+    const double* host_aold = nullptr;
 };
 // true when the walk copied the outputs to rq.host itself (chunked, overlapped with the walk)
 bool run_walk(gt_context* ctx, const gt_tree* t, const WalkRequest& rq);

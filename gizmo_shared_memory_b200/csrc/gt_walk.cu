@@ -605,11 +605,9 @@ walk_kernel(const WalkArgs A) {
             const int node = lane < npop ? stk[top + lane] : -1;
             __syncwarp();
             bool accept = false, expand = false, push = false;
-            NodeV nd;
-            nd.first = -1; nd.nchild = 0; nd.plo = nd.phi = 0;
-            nd.cx = nd.cy = nd.cz = nd.mass = nd.s = 0.0; nd.len = nd.soft = 0.0f;
+            // idle lanes read node 0 and decide nothing (cheaper than defaulting every field)
+            const NodeV nd = load_node(A.nodes + (node >= 0 ? node : 0));
             if (node >= 0) {
-                nd = load_node(A.nodes + node);
                 const bool leaf = nd.first < 0;
                 const double dx = box_gap(S.lo_x, nd.cx, S.hi_x);
                 const double dy = box_gap(S.lo_y, nd.cy, S.hi_y);
@@ -669,11 +667,30 @@ walk_kernel(const WalkArgs A) {
             if (COUNT && lane == 0) { c_nodes += npop; ++c_steps; }
 
             // children of opened interior nodes
+            // One scan gives both the children's stack slots and the expanded leaves' particle
+            // slots, packed as nch + (cnt << 10): nch <= 8, so the children's total stays below
+            // 1024, and the particles' total fits the upper 21 bits while every leaf holds fewer
+            // than 2^16 particles (else two scans).
             const int nch = push ? nd.nchild : 0;
-            const int incl = warp_incl_scan_i(nch);
+            const int cnt = expand ? nd.phi - nd.plo : 0;
+            int incl, inc2;
+            if (!__any_sync(kFull, cnt >= (1 << 16))) {
+                const int both = warp_incl_scan_i(nch | (cnt << 10));
+                incl = both & 1023;
+                inc2 = both >> 10;
+            } else {
+                incl = warp_incl_scan_i(nch);
+                inc2 = warp_incl_scan_i(cnt);
+            }
             const int tot = __shfl_sync(kFull, incl, 31);
             if (top + tot > A.stack_cap) { overflow = true; break; }
-            for (int c = 0; c < nch; ++c) stk[top + incl - nch + c] = nd.first + c;
+            {
+                // an octree node has at most 8 children: a fixed, predicated loop
+                int* dst = stk + (top + incl - nch);
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    if (c < nch) dst[c] = nd.first + c;
+            }
             top += tot;
             __syncwarp();  // pushes are visible to the lanes that pop them
             if (COUNT) c_maxtop = max(c_maxtop, top);
@@ -696,8 +713,6 @@ walk_kernel(const WalkArgs A) {
             // expanded leaves: their particles
             const unsigned em = __ballot_sync(kFull, expand);
             if (em) {
-                const int cnt = expand ? nd.phi - nd.plo : 0;
-                const int inc2 = warp_incl_scan_i(cnt);
                 const int tot2 = __shfl_sync(kFull, inc2, 31);
                 S.lo[lane] = nd.plo;
                 S.pre[lane] = inc2 - cnt;
@@ -1297,12 +1312,11 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     constexpr int kChunks = 4;
     const bool chunked = rq.host.any() && !rq.count && rq.stack_capacity == 0 && !rq.capture &&
                          ng >= 64 * kChunks && nt >= (1 << 18);
+    if (rq.host_aold && !chunked)
+        check_cuda(cudaMemcpyAsync((void*)rq.aold, rq.host_aold, (size_t)nt * sizeof(double), cudaMemcpyHostToDevice, st),
+                   "aold h2d");
     if (chunked) {
-        if (!ctx->copy_stream) {
-            check_cuda(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
-            for (cudaEvent_t& e : ctx->chunk_ev) check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-            check_cuda(cudaEventCreateWithFlags(&ctx->copy_done, cudaEventDisableTiming), "event");
-        }
+        ensure_copy_stream(ctx);
         int2* bounds = (int2*)(ctr + 16);  // K+1 int2 after the counters
         check_cuda(cudaMemsetAsync(ctr, 0, 256, st), "memset counters");
         chunk_bounds_kernel<<<1, 1, 0, st>>>(groups, (int)ng, (int)nt, kChunks, bounds);
@@ -1321,9 +1335,24 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         a.stack_cap = stack_cap;
         const OutputCopy outs[6] = {{rq.ax, rq.host.ax, 1},  {rq.ay, rq.host.ay, 1},       {rq.az, rq.host.az, 1},
                                     {rq.phi, rq.host.phi, 1}, {rq.tidal, rq.host.tidal, 6}, {rq.jerk, rq.host.jerk, 3}};
+        if (rq.host_aold) {
+            // every chunk's aold ahead of the results on the copy stream, after the work queued
+            // before this walk (which may still read the buffer); chunk c reads only the aold of
+            // its own targets [hb[c].y, hb[c+1].y), so it waits for that piece alone
+            check_cuda(cudaEventRecord(ctx->main_ev, st), "event");
+            check_cuda(cudaStreamWaitEvent(ctx->copy_stream, ctx->main_ev, 0), "wait");
+            for (int c = 0; c < kChunks; ++c) {
+                const int64_t t0 = hb[c].y, t1 = hb[c + 1].y;
+                if (t1 > t0)
+                    check_cuda(cudaMemcpyAsync((void*)(rq.aold + t0), rq.host_aold + t0, (size_t)(t1 - t0) * sizeof(double),
+                                               cudaMemcpyHostToDevice, ctx->copy_stream), "aold h2d chunk");
+                check_cuda(cudaEventRecord(ctx->up_ev[c], ctx->copy_stream), "event");
+            }
+        }
         check_cuda(cudaEventRecord(ctx->ev0, st), "event");
         for (int c = 0; c < kChunks; ++c) {
             const int g0 = hb[c].x, g1 = hb[c + 1].x;
+            if (rq.host_aold) check_cuda(cudaStreamWaitEvent(st, ctx->up_ev[c], 0), "wait");
             if (g1 > g0) {
                 WalkArgs ac = a;
                 ac.groups = groups + g0;

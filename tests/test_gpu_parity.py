@@ -394,6 +394,34 @@ def test_errors_leave_context_usable(gpu_ctx, plummer):
     assert np.isfinite(a[0]).all()
 
 
+def test_nonfinite_softening_rejected(gpu_ctx, plummer):
+    """A build from host arrays uploads the softenings while the bounding box, keys and sort run
+    and checks them in the gather stage; a non-finite softening is still GT_ERR_NONFINITE, with the
+    same count as a device build gives, and the context stays usable (the next build matches one
+    from device arrays bit for bit)."""
+    import torch
+
+    for bad in (np.nan, np.inf):
+        P = dict(plummer)
+        P["soft"] = P["soft"].copy()
+        P["soft"][[5, 77]] = bad
+        with pytest.raises(g.GTError) as e:
+            gpu_ctx.build(P)
+        assert e.value.status == 7
+        assert "2 particle(s)" in str(e.value)
+        dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
+        with pytest.raises(g.GTError) as e:
+            gpu_ctx.build(dev)
+        assert e.value.status == 7
+        assert "2 particle(s)" in str(e.value)
+    T = gpu_ctx.build(plummer)
+    Td = gpu_ctx.build({k: torch.as_tensor(v, device="cuda") for k, v in plummer.items()})
+    a = gpu_ctx.accel_grouped(T, None, theta=0.7)
+    b = gpu_ctx.accel_grouped(Td, None, theta=0.7)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
+
+
 # ---- size-independent properties at a large size ----------------------------------------------
 
 def test_properties_galaxy_4m(gpu_ctx):
