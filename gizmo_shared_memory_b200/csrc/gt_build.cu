@@ -15,8 +15,8 @@
 //                 max_level, tree.cc:89); a scan over child counts places every node's children
 //                 contiguously in the next level (BFS order).  Child centres are parent +-
 //                 side/4 by the child's octant bits, as tree.cc:116-118.
-//   6. moments    deepest level first, one warp per node: a leaf reduces its particles, an
-//                 interior node its children, with warp shuffles (mass, mass-weighted position,
+//   6. moments    deepest level first, eight lanes per node: a leaf reduces its particles, an
+//                 interior node its children, with shuffles (mass, mass-weighted position,
 //                 max softening), then COM, delta = |COM - centre| and the packed walk node
 //                 (tree.cc:145-196, 507-523).
 // The next/first threading of the reference (tree.cc:340-348) is produced alongside for the host
@@ -34,11 +34,6 @@ namespace {
 
 constexpr int kBlk = 256;
 
-__device__ __forceinline__ double warp_sum_d(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 __device__ __forceinline__ double warp_max_d(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -379,7 +374,23 @@ __global__ void emit_kernel(GNode* __restrict__ nodes, const SrcP* __restrict__ 
     }
 }
 
-// ---- 6. moments, one warp per node, deepest level first ---------------------------------------
+// ---- 6. moments, eight lanes per node, deepest level first ------------------------------------
+// An interior node has at most 8 children and a leaf usually at most leaf_max (16) particles, so
+// a node gets 8 lanes of a warp (4 nodes per warp) and 3-level shuffle reductions.
+constexpr int kMomLanes = 8;
+constexpr int kMomNodesPerBlock = kBlk / kMomLanes;
+
+__device__ __forceinline__ double group_sum_d(double v) {
+#pragma unroll
+    for (int o = kMomLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double group_max_d(double v) {
+#pragma unroll
+    for (int o = kMomLanes / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
 __global__ void moments_kernel(GNode* __restrict__ nodes, const SrcP* __restrict__ src,
                                const double* __restrict__ smass, const double* __restrict__ ssoft,
                                const uint32_t* __restrict__ order, int64_t a, int64_t b,
@@ -387,14 +398,19 @@ __global__ void moments_kernel(GNode* __restrict__ nodes, const SrcP* __restrict
                                double* __restrict__ delta, double* __restrict__ nsoft,
                                float* __restrict__ nq2, int* __restrict__ leaf_of,
                                int* __restrict__ sleaf, int nodelta) {
-    const int lane = threadIdx.x & 31;
-    const int64_t i = a + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
-    if (i >= b) return;
-    const int first = nodes[i].first, nc = nodes[i].nchild;
-    const int lo = nodes[i].plo, hi = nodes[i].phi;
+    const int sub = threadIdx.x & (kMomLanes - 1);
+    const int64_t i = a + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kMomLanes;
+    // every lane takes part in the group shuffles; lanes past the level's last node add nothing
+    const bool valid = i < b;
+    int first = 0, nc = 0, lo = 0, hi = 0;
+    if (valid) {
+        first = nodes[i].first; nc = nodes[i].nchild;
+        lo = nodes[i].plo; hi = nodes[i].phi;
+    }
+    const bool leaf = valid && first < 0;
     double M = 0, mx = 0, my = 0, mz = 0, smax = 0;
-    if (first < 0) {
-        for (int j = lo + lane; j < hi; j += 32) {
+    if (leaf) {
+        for (int j = lo + sub; j < hi; j += kMomLanes) {
             const double mj = smass[j];
             const SrcP s = src[j];
             M += mj; mx += mj * s.x; my += mj * s.y; mz += mj * s.z;
@@ -402,34 +418,34 @@ __global__ void moments_kernel(GNode* __restrict__ nodes, const SrcP* __restrict
             leaf_of[order[j]] = (int)i;
             sleaf[j] = (int)i;
         }
-    } else if (lane < nc) {
-        const GNode& ch = nodes[first + lane];
+    } else if (valid && sub < nc) {
+        const GNode& ch = nodes[first + sub];
         M = ch.mass; mx = M * ch.cx; my = M * ch.cy; mz = M * ch.cz;
-        smax = nsoft[first + lane];
+        smax = nsoft[first + sub];
     }
-    M = warp_sum_d(M); mx = warp_sum_d(mx); my = warp_sum_d(my); mz = warp_sum_d(mz);
-    smax = warp_max_d(smax);
+    M = group_sum_d(M); mx = group_sum_d(mx); my = group_sum_d(my); mz = group_sum_d(mz);
+    smax = group_max_d(smax);
     // Second mass moment about the COM, sum m |x - com|^2: from the particles in a leaf, from the
     // children by the parallel-axis rule otherwise.  Not used by the plain criterion; it is an input
     // of the learned one (the quadrupole error a monopole makes scales with it).
     {
         const double ox = M > 0 ? mx / M : 0.0, oy = M > 0 ? my / M : 0.0, oz = M > 0 ? mz / M : 0.0;
         double q = 0;
-        if (first < 0) {
-            for (int j = lo + lane; j < hi; j += 32) {
+        if (leaf) {
+            for (int j = lo + sub; j < hi; j += kMomLanes) {
                 const SrcP s = src[j];
                 const double ex = s.x - ox, ey = s.y - oy, ez = s.z - oz;
                 q += smass[j] * (ex * ex + ey * ey + ez * ez);
             }
-        } else if (lane < nc) {
-            const GNode& ch = nodes[first + lane];
+        } else if (valid && sub < nc) {
+            const GNode& ch = nodes[first + sub];
             const double ex = ch.cx - ox, ey = ch.cy - oy, ez = ch.cz - oz;
-            q = (double)nq2[first + lane] + ch.mass * (ex * ex + ey * ey + ez * ez);
+            q = (double)nq2[first + sub] + ch.mass * (ex * ex + ey * ey + ez * ez);
         }
-        q = warp_sum_d(q);
-        if (lane == 0) nq2[i] = (float)q;
+        q = group_sum_d(q);
+        if (valid && sub == 0) nq2[i] = (float)q;
     }
-    if (lane == 0) {
+    if (valid && sub == 0) {
         if (M > 0) { mx /= M; my /= M; mz /= M; }
         const double dx = mx - gc[3 * i], dy = my - gc[3 * i + 1], dz = mz - gc[3 * i + 2];
         const double dl = sqrt(dx * dx + dy * dy + dz * dz);
@@ -562,27 +578,28 @@ __global__ void vel_moments_kernel(const GNode* __restrict__ nodes, const double
                                    const double* __restrict__ vy, const double* __restrict__ vz, int64_t a,
                                    int64_t b, double* __restrict__ vcom, float4* __restrict__ nvel,
                                    float* __restrict__ vmax) {
-    const int lane = threadIdx.x & 31;
-    const int64_t i = a + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
-    if (i >= b) return;
-    const GNode nd = nodes[i];
+    const int sub = threadIdx.x & (kMomLanes - 1);
+    const int64_t i = a + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kMomLanes;
+    const bool valid = i < b;  // all lanes take part in the group shuffles
+    GNode nd{};
+    if (valid) nd = nodes[i];
     double px = 0, py = 0, pz = 0, vm = 0;
-    if (nd.first < 0) {
-        for (int j = nd.plo + lane; j < nd.phi; j += 32) {
+    if (valid && nd.first < 0) {
+        for (int j = nd.plo + sub; j < nd.phi; j += kMomLanes) {
             const uint32_t p = order[j];
             const double m = smass[j], ux = vx[p], uy = vy[p], uz = vz[p];
             px += m * ux; py += m * uy; pz += m * uz;
             vm = fmax(vm, sqrt(ux * ux + uy * uy + uz * uz));
         }
-    } else if (lane < nd.nchild) {
-        const int c = nd.first + lane;
+    } else if (valid && sub < nd.nchild) {
+        const int c = nd.first + sub;
         const double m = nodes[c].mass;
         px = m * vcom[3 * c]; py = m * vcom[3 * c + 1]; pz = m * vcom[3 * c + 2];
         vm = (double)vmax[c];
     }
-    px = warp_sum_d(px); py = warp_sum_d(py); pz = warp_sum_d(pz);
-    vm = warp_max_d(vm);
-    if (lane == 0) {
+    px = group_sum_d(px); py = group_sum_d(py); pz = group_sum_d(pz);
+    vm = group_max_d(vm);
+    if (valid && sub == 0) {
         const double M = nd.mass;
         const double ux = M > 0 ? px / M : 0.0, uy = M > 0 ? py / M : 0.0, uz = M > 0 ? pz / M : 0.0;
         vcom[3 * i] = ux; vcom[3 * i + 1] = uy; vcom[3 * i + 2] = uz;
@@ -826,7 +843,7 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
     for (int L = t->n_levels - 1; L >= 0; --L) {
         const int64_t a = t->lvl_off[L], b = t->lvl_off[L + 1];
         const int64_t warps = b - a;
-        moments_kernel<<<div_up(warps * 32, kBlk), kBlk, 0, st>>>(
+        moments_kernel<<<div_up(warps, kMomNodesPerBlock), kBlk, 0, st>>>(
             t->nodes, t->src, t->smass, t->ssoft, t->order, a, b, t->size, t->gc, t->delta,
             t->nsoft, t->nq2, t->leaf_of, t->sleaf, o.nodelta);
         check_launch(ctx, "moments_kernel");
@@ -869,7 +886,7 @@ void tree_velocities(gt_context* ctx, gt_tree* t, const double* vx, const double
     }
     for (int L = t->n_levels - 1; L >= 0 && !particles_only; --L) {
         const int64_t a = t->lvl_off[L], b = t->lvl_off[L + 1];
-        vel_moments_kernel<<<div_up((b - a) * 32, kBlk), kBlk, 0, st>>>(t->nodes, t->smass, t->order, vx, vy, vz, a,
+        vel_moments_kernel<<<div_up(b - a, kMomNodesPerBlock), kBlk, 0, st>>>(t->nodes, t->smass, t->order, vx, vy, vz, a,
                                                                        b, t->vcom, t->nvel, t->vmax);
         check_launch(ctx, "vel_moments_kernel");
     }

@@ -1063,12 +1063,24 @@ void dispatch(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la
     }
 }
 
+// Chunks of the copy-overlapped walk, as cumulative percentages of the targets.  The first chunk is
+// small, so the walk starts once a tenth of the host aold is across, and so is the last, so that
+// little of the results' download is left when the last kernel ends; the chunks between are large
+// enough that each one's download hides under the next one's walk.
+constexpr int kChunks = 5;
+struct ChunkEdges {
+    int pct[kChunks + 1];
+};
+constexpr ChunkEdges kChunkEdge{{0, 10, 45, 80, 93, 100}};
+
 // Chunk boundaries of a group list for the copy-overlapped walk: chunk c starts at the first group
-// whose first target is at or after c * nt / K.  out: K+1 pairs (group index, first target).
-__global__ void chunk_bounds_kernel(const int2* __restrict__ groups, int ng, int nt, int K, int2* __restrict__ out) {
+// whose first target is at or after nt * edges.pct[c] / 100.  out: kChunks+1 pairs (group index,
+// first target).
+__global__ void chunk_bounds_kernel(const int2* __restrict__ groups, int ng, int nt, ChunkEdges edges,
+                                    int2* __restrict__ out) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    for (int c = 0; c <= K; ++c) {
-        const int64_t want = (int64_t)nt * c / K;
+    for (int c = 0; c <= kChunks; ++c) {
+        const int64_t want = (int64_t)nt * edges.pct[c] / 100;
         int lo = 0, hi = ng;  // first g with groups[g].x >= want
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
@@ -1307,9 +1319,8 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         a.mac_l2 = l2;
     }
 
-    // Host outputs of a large walk: split the groups into chunks of about equal target count, and
-    // copy each chunk's results to the host on a second stream while the next chunk runs.
-    constexpr int kChunks = 4;
+    // Host outputs of a large walk: split the groups into chunks (kChunkEdge), and copy each chunk's
+    // results to the host on a second stream while the next chunk runs.
     const bool chunked = rq.host.any() && !rq.count && rq.stack_capacity == 0 && !rq.capture &&
                          ng >= 64 * kChunks && nt >= (1 << 18);
     if (rq.host_aold && !chunked)
@@ -1319,7 +1330,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         ensure_copy_stream(ctx);
         int2* bounds = (int2*)(ctr + 16);  // K+1 int2 after the counters
         check_cuda(cudaMemsetAsync(ctr, 0, 256, st), "memset counters");
-        chunk_bounds_kernel<<<1, 1, 0, st>>>(groups, (int)ng, (int)nt, kChunks, bounds);
+        chunk_bounds_kernel<<<1, 1, 0, st>>>(groups, (int)ng, (int)nt, kChunkEdge, bounds);
         check_launch(ctx, "chunk_bounds_kernel");
         int2 hb[kChunks + 1];
         check_cuda(cudaMemcpyAsync(ctx->pinned, bounds, sizeof(hb), cudaMemcpyDeviceToHost, st), "d2h");
