@@ -125,18 +125,26 @@ __global__ void radix_hist_kernel(const uint64_t* __restrict__ keys, int64_t n, 
 
 // Stable scatter of one 8-bit digit.  Warp w owns keys [w*256, w*256+256) of the tile and walks
 // them 32 at a time in index order; lanes with equal digits are ranked with __match_any_sync, so
-// the destination order equals the source order within every digit.
+// the destination order equals the source order within every digit.  The tile is first reordered
+// by digit in shared memory, and then written out in that order: consecutive threads store
+// consecutive positions of one digit's run, instead of every lane of a warp storing to its own
+// digit's bucket.
 __global__ void __launch_bounds__(kSortThreads)
 radix_scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                      uint64_t* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n, int shift,
                      const uint32_t* __restrict__ offsets, int nblocks) {
     __shared__ uint32_t wh[kSortWarps][kRadix];
     __shared__ uint32_t boff[kRadix];
+    __shared__ uint32_t bstart[kRadix];   // first tile position of each digit
+    __shared__ uint32_t wsum[kSortWarps];
+    __shared__ uint64_t tkey[kSortTile];
+    __shared__ uint32_t tval[kSortTile];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int d = threadIdx.x; d < kSortWarps * kRadix; d += kSortThreads) (&wh[0][0])[d] = 0;
     boff[threadIdx.x] = offsets[(int64_t)threadIdx.x * nblocks + blockIdx.x];
     __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * kSortTile + (int64_t)w * kWarpSpan;
+    const int64_t tile0 = (int64_t)blockIdx.x * kSortTile;
+    const int64_t base = tile0 + (int64_t)w * kWarpSpan;
     const uint32_t lt = (1u << lane) - 1u;
     uint64_t key[kSortItems];
     uint32_t val[kSortItems], rnk[kSortItems];
@@ -156,24 +164,46 @@ radix_scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restric
         __syncwarp();
     }
     __syncthreads();
+    uint32_t total = 0;  // this block's count of digit threadIdx.x
     {   // exclusive scan over warps for each digit: warp w's keys follow warps 0..w-1
         const int d = threadIdx.x;
-        uint32_t run = 0;
 #pragma unroll
         for (int ww = 0; ww < kSortWarps; ++ww) {
             const uint32_t c = wh[ww][d];
-            wh[ww][d] = run;
-            run += c;
+            wh[ww][d] = total;
+            total += c;
         }
+    }
+    {   // exclusive scan over digits of the block's counts: where each digit's run starts in the tile
+        uint32_t v = total;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += t;
+        }
+        if (lane == 31) wsum[w] = v;
+        __syncthreads();
+        uint32_t before = 0;
+        for (int ww = 0; ww < w; ++ww) before += wsum[ww];
+        bstart[threadIdx.x] = before + v - total;
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         if (dig[k] < kRadix) {
-            const uint32_t pos = boff[dig[k]] + wh[w][dig[k]] + rnk[k];
-            kout[pos] = key[k];
-            vout[pos] = val[k];
+            const uint32_t pos = bstart[dig[k]] + wh[w][dig[k]] + rnk[k];
+            tkey[pos] = key[k];
+            tval[pos] = val[k];
         }
+    }
+    __syncthreads();
+    const int nvalid = n - tile0 < kSortTile ? (int)(n - tile0) : kSortTile;
+    for (int j = threadIdx.x; j < nvalid; j += kSortThreads) {
+        const uint64_t kk = tkey[j];
+        const int d = (int)((kk >> shift) & 0xffu);
+        const uint32_t pos = boff[d] + (uint32_t)j - bstart[d];
+        kout[pos] = kk;
+        vout[pos] = tval[j];
     }
 }
 
