@@ -463,7 +463,8 @@ walk_kernel(const WalkArgs A) {
                     nty[k] = make_float2(-ty[k], -ty[k]);
                     ntz[k] = make_float2(-tz[k], -tz[k]);
                 }
-#pragma unroll 4
+                // 8 pairs in flight per lane (unroll 2 and 4 measured 1.9 % and 0.6 % slower)
+#pragma unroll 8
                 for (int jp = slice; jp < np; jp += NS) {
                     const float4 A = pn[2 * jp], B = pn[2 * jp + 1];
                     const float2 X = make_float2(A.x, A.y), Y = make_float2(A.z, A.w);
