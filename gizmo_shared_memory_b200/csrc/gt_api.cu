@@ -146,7 +146,10 @@ void free_tree_arrays(gt_tree* t) {
     for (void* p : ptrs)
         if (p) cudaFreeAsync(p, 0);
     for (auto& c : t->group_cache) {
-        if (c.groups) cudaFree(c.groups);
+        if (c.groups) {
+            if (c.pooled) cudaFreeAsync(c.groups, 0);
+            else cudaFree(c.groups);
+        }
         if (c.roots) cudaFree(c.roots);
     }
     t->group_cache.clear();

@@ -166,6 +166,7 @@ struct gt_tree {
         int2* groups = nullptr;
         int* roots = nullptr;  // forest: root node of each group
         int64_t n_groups = 0;
+        bool pooled = false;   // groups came from the stream-ordered pool (cudaMallocAsync)
     };
     std::vector<GroupCache> group_cache;
     // guards the state made on first use (the group cache, the search nodes): trees may be used by

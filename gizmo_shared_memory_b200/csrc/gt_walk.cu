@@ -910,6 +910,13 @@ __global__ void compact_starts_kernel(const uint32_t* __restrict__ flag, const u
         if (flag[i]) starts[pos[i]] = i;
 }
 
+// Fixed windows of `w` consecutive targets over all n live particles of one system.
+__global__ void window_groups_kernel(int2* __restrict__ groups, int64_t ng, int64_t n, int w) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ng;
+         g += (int64_t)gridDim.x * blockDim.x)
+        groups[g] = make_int2((int)(g * w), (int)std::min<int64_t>((g + 1) * w, n));
+}
+
 // Split groups longer than kmax into consecutive chunks (each walks with its own, tighter box).
 __global__ void chunk_count_kernel(const int64_t* __restrict__ starts, int64_t ng, int64_t n_end,
                                    int kmax, uint32_t* __restrict__ nchunk) {
@@ -1147,6 +1154,25 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
             if (c.mode == mode && c.param == param && c.kmax == kmax) {
                 groups = c.groups; roots = c.roots; ng = c.n_groups;
             }
+        if (!groups && !rq.capture && mode == GT_GROUP_BATCH && t->n_systems == 1 && param <= kmax &&
+            t->n_live > 0) {
+            // fixed windows over the tree order of one system: [param*g, param*(g+1)), the same
+            // list the flags below give, without their scans and read-backs
+            const int64_t n = t->n_live;
+            ng = (n + param - 1) / param;
+            void* p = nullptr;
+            if (cudaMallocAsync(&p, (size_t)ng * sizeof(int2), st) != cudaSuccess) {
+                cudaGetLastError();
+                throw Fail{GT_ERR_NOMEM, "cudaMallocAsync for the group list failed"};
+            }
+            groups = (int2*)p;
+            window_groups_kernel<<<grid1d(ctx, ng), 256, 0, st>>>(groups, ng, n, param);
+            check_launch(ctx, "window_groups_kernel");
+            check_cuda(cudaStreamSynchronize(st), "sync");  // complete before other contexts see it
+            gt_tree::GroupCache c;
+            c.mode = mode; c.param = param; c.kmax = kmax; c.groups = groups; c.n_groups = ng; c.pooled = true;
+            t->group_cache.push_back(c);
+        }
         if (!groups) {
             const int64_t n = t->n_live;
             uint32_t* flag = (uint32_t*)scratch(ctx, kSlotTargets, (size_t)n * 4);
