@@ -435,6 +435,7 @@ def run_gpu_arm(args):
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             te = float(tt[0])
         e2e = {"value": nl * world / te, "unit": "particles/s", "ms_per_step": 1e3 * te,
+               "ms_per_step_median": 1e3 * float(np.median(ttimes)), "ms_per_step_max": 1e3 * float(np.max(ttimes)),
                "h2d_bytes_per_step": int(5 * 8 * n + 8 * nl), "d2h_bytes_per_step": int(3 * 8 * nl),
                "includes": "H2D of x,y,z,m,soft,aold from pinned memory + tree build + walk + D2H of ax,ay,az"}
         hctx.close()
