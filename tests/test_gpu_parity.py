@@ -467,6 +467,40 @@ def test_host_outputs_copied_in_chunks_are_identical(gpu_ctx):
         assert np.array_equal(d.cpu().numpy(), h)
 
 
+def test_host_aold_uploaded_in_chunks_is_identical(gpu_ctx):
+    """A walk given a host aold and host outputs uploads aold piece by piece on the copy stream,
+    each chunk waiting only for its own targets' piece, and downloads each chunk's results while the
+    next one runs.  The results are bit-identical to the same walk with aold and the outputs on the
+    device: grouped windows, the tidal tensor, and the per-target walk (explicit targets)."""
+    import torch
+
+    P = ics.plummer(n=400000, seed=15, soft=0.01)
+    T = gpu_ctx.build(P)
+    nl = T.info()["n_live"]
+    kw = dict(group_mode=g.GT_GROUP_BATCH, batch=32)
+    aold = gpu_ctx.form_aold(*gpu_ctx.accel_grouped(T, None, theta=0.7, **kw), 0.0025)
+    aold_d = torch.as_tensor(aold, device="cuda")
+    dev = tuple(torch.empty(nl, dtype=torch.float64, device="cuda") for _ in range(3))
+    gpu_ctx.accel_grouped(T, None, aold=aold_d, outs=dev + (None,), **kw)
+    host = gpu_ctx.accel_grouped(T, None, aold=aold, **kw)
+    for d, h in zip(dev, host):
+        assert np.array_equal(d.cpu().numpy(), h)
+
+    tid = torch.empty((nl, 6), dtype=torch.float64, device="cuda")
+    gpu_ctx.accel_grouped_ext(T, None, aold=aold_d, outs=dev + (None, tid, None), **kw)
+    hx = gpu_ctx.accel_grouped_ext(T, None, aold=aold, **kw)
+    for d, h in zip(dev + (tid,), hx[:3] + (hx[4],)):
+        assert np.array_equal(d.cpu().numpy(), h)
+
+    tg = np.arange(len(P["m"]), dtype=np.uint32)
+    aold_t = gpu_ctx.form_aold(*gpu_ctx.accel(T, tg, theta=0.7), 0.0025)
+    h1 = gpu_ctx.accel(T, tg, aold=aold_t)
+    d1 = gpu_ctx.accel(T, torch.as_tensor(tg.view(np.int32), device="cuda"),
+                       aold=torch.as_tensor(aold_t, device="cuda"))
+    for d, h in zip(d1, h1):
+        assert np.array_equal(d.cpu().numpy(), h)
+
+
 def test_walks_and_searches_from_several_threads(gpu_ctx):
     """Four host threads, each with its own context, walk and search one fresh tree at the same
     time: the group list and the search nodes it builds on first use are made once, under the
