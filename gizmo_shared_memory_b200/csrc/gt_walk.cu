@@ -402,15 +402,20 @@ walk_kernel(const WalkArgs A) {
             has_sink = __any_sync(kFull, sink);
         }
         // one interaction's tidal and jerk terms: T += -g1 I + g2 d d, J += g1 dv - (dv.d) g2 d
-        // (shmem/tree.cc:811-837, 845-872); d = source - target, dv = v_source - v_target
-        auto xt_add = [&](float (&q)[9], float dx, float dy, float dz, float g1, float g2, float4 ev, int k) {
+        // (shmem/tree.cc:811-837, 845-872); d = source - target, dv = v_source - v_target.  The
+        // list's g2 d d and its sum of g1 (q[9]) are kept apart and the diagonal's -g1 is taken off
+        // in FP64 when the list is added to the totals: 10 FP32 operations per interaction instead
+        // of 15, and the diagonal's cancellation happens in FP64.
+        auto xt_add = [&](float (&q)[10], float dx, float dy, float dz, float g1, float g2, float4 ev, int k) {
             if (want_tid) {
-                q[0] += fmaf(dx * dx, g2, -g1);
-                q[1] += fmaf(dy * dy, g2, -g1);
-                q[2] += fmaf(dz * dz, g2, -g1);
-                q[3] = fmaf(dx * dy, g2, q[3]);
-                q[4] = fmaf(dy * dz, g2, q[4]);
-                q[5] = fmaf(dx * dz, g2, q[5]);
+                const float gx = g2 * dx, gy = g2 * dy, gz = g2 * dz;
+                q[0] = fmaf(gx, dx, q[0]);
+                q[1] = fmaf(gy, dy, q[1]);
+                q[2] = fmaf(gz, dz, q[2]);
+                q[3] = fmaf(gx, dy, q[3]);
+                q[4] = fmaf(gy, dz, q[4]);
+                q[5] = fmaf(gx, dz, q[5]);
+                q[9] += g1;
             }
             if (want_jerk) {
                 const float dvx = ev.x - tvx[k], dvy = ev.y - tvy[k], dvz = ev.z - tvz[k];
@@ -447,7 +452,7 @@ walk_kernel(const WalkArgs A) {
             __syncwarp();
             const int np = (n + 1) >> 1;
             float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
-            float xq[XT == 1 ? TPL : 1][9];
+            float xq[XT == 1 ? TPL : 1][10];
 #pragma unroll
             for (int k = 0; k < TPL; ++k) ax_[k] = ay_[k] = az_[k] = ap_[k] = 0.0f;
             // packed for full groups; groups of <= 16 targets split the list over lane slices, where
@@ -497,7 +502,7 @@ walk_kernel(const WalkArgs A) {
 #pragma unroll
                     for (int k = 0; k < TPL; ++k)
 #pragma unroll
-                        for (int c = 0; c < 9; ++c) xq[XT == 1 ? k : 0][c] = 0.0f;
+                        for (int c = 0; c < 10; ++c) xq[XT == 1 ? k : 0][c] = 0.0f;
                 }
 #pragma unroll 4
                 for (int j = slice; j < n; j += NS) {
@@ -526,9 +531,11 @@ walk_kernel(const WalkArgs A) {
             accumulate(ax_, ay_, az_, ap_);
             if (XT == 1) {
 #pragma unroll
-                for (int k = 0; k < TPL; ++k)
+                for (int k = 0; k < TPL; ++k) {
+                    const double sg = (double)xq[XT == 1 ? k : 0][9];  // the diagonal's -g1 terms
 #pragma unroll
-                    for (int c = 0; c < 9; ++c) xt[c][k] += (double)xq[XT == 1 ? k : 0][c];
+                    for (int c = 0; c < 9; ++c) xt[c][k] += (double)xq[XT == 1 ? k : 0][c] - (c < 3 ? sg : 0.0);
+                }
             }
             __syncwarp();
         };
@@ -536,14 +543,14 @@ walk_kernel(const WalkArgs A) {
         auto flush_pp = [&](int n) {
             __syncwarp();
             float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
-            float xq[XT == 1 ? TPL : 1][9];
+            float xq[XT == 1 ? TPL : 1][10];
 #pragma unroll
             for (int k = 0; k < TPL; ++k) ax_[k] = ay_[k] = az_[k] = ap_[k] = 0.0f;
             if (XT == 1) {
 #pragma unroll
                 for (int k = 0; k < TPL; ++k)
 #pragma unroll
-                    for (int c = 0; c < 9; ++c) xq[XT == 1 ? k : 0][c] = 0.0f;
+                    for (int c = 0; c < 10; ++c) xq[XT == 1 ? k : 0][c] = 0.0f;
             }
             unsigned zero = 0;
             for (int j = slice; j < n; j += NS) {
@@ -586,9 +593,11 @@ walk_kernel(const WalkArgs A) {
             accumulate(ax_, ay_, az_, ap_);
             if (XT == 1) {
 #pragma unroll
-                for (int k = 0; k < TPL; ++k)
+                for (int k = 0; k < TPL; ++k) {
+                    const double sg = (double)xq[XT == 1 ? k : 0][9];  // the diagonal's -g1 terms
 #pragma unroll
-                    for (int c = 0; c < 9; ++c) xt[c][k] += (double)xq[XT == 1 ? k : 0][c];
+                    for (int c = 0; c < 9; ++c) xt[c][k] += (double)xq[XT == 1 ? k : 0][c] - (c < 3 ? sg : 0.0);
+                }
             }
             if (COUNT) c_zero += zero;
             __syncwarp();
