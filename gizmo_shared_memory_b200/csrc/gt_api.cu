@@ -77,6 +77,12 @@ using namespace gt;
 
 namespace {
 
+// A failed call returns only once the copy stream has drained: no upload from, or download into,
+// the caller's host arrays is left running after the error is reported.
+void drain_copies(gt_context* ctx) {
+    if (ctx && ctx->copy_stream && cudaStreamSynchronize(ctx->copy_stream) != cudaSuccess) cudaGetLastError();
+}
+
 template <typename F>
 int guarded(gt_context* ctx, F&& body) {
     try {
@@ -84,12 +90,15 @@ int guarded(gt_context* ctx, F&& body) {
         if (ctx) ctx->last_error.clear();
         return GT_OK;
     } catch (const Fail& f) {
+        drain_copies(ctx);
         set_error(ctx, f.status, f.msg);
         return f.status;
     } catch (const std::bad_alloc&) {
+        drain_copies(ctx);
         set_error(ctx, GT_ERR_NOMEM, "host allocation failed");
         return GT_ERR_NOMEM;
     } catch (...) {
+        drain_copies(ctx);
         set_error(ctx, GT_ERR_CUDA, "unexpected exception");
         return GT_ERR_CUDA;
     }
