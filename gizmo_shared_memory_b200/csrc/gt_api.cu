@@ -66,6 +66,13 @@ void ensure_copy_stream(gt_context* ctx) {
     for (cudaEvent_t& e : ctx->up_ev) make(e);
     make(ctx->copy_done);
     make(ctx->main_ev);
+    make(ctx->walk2_start);
+    make(ctx->walk2_done);
+    if (!ctx->walk2) {
+        cudaStream_t w = nullptr;
+        check_cuda(cudaStreamCreateWithFlags(&w, cudaStreamNonBlocking), "cudaStreamCreate");
+        ctx->walk2 = w;
+    }
     cudaStream_t s = nullptr;
     check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
     ctx->copy_stream = s;
@@ -77,9 +84,11 @@ using namespace gt;
 
 namespace {
 
-// A failed call returns only once the copy stream has drained: no upload from, or download into,
-// the caller's host arrays is left running after the error is reported.
+// A failed call returns only once the second compute stream and the copy stream have drained: no
+// upload from, or download into, the caller's host arrays is left running after the error is
+// reported.
 void drain_copies(gt_context* ctx) {
+    if (ctx && ctx->walk2 && cudaStreamSynchronize(ctx->walk2) != cudaSuccess) cudaGetLastError();
     if (ctx && ctx->copy_stream && cudaStreamSynchronize(ctx->copy_stream) != cudaSuccess) cudaGetLastError();
 }
 
@@ -391,6 +400,12 @@ int gt_context_destroy(gt_context* ctx) {
         if (e) cudaEventDestroy(e);
     if (ctx->copy_done) cudaEventDestroy(ctx->copy_done);
     if (ctx->main_ev) cudaEventDestroy(ctx->main_ev);
+    if (ctx->walk2) {
+        cudaStreamSynchronize(ctx->walk2);
+        cudaStreamDestroy(ctx->walk2);
+    }
+    if (ctx->walk2_start) cudaEventDestroy(ctx->walk2_start);
+    if (ctx->walk2_done) cudaEventDestroy(ctx->walk2_done);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     cudaGetLastError();
     if (prev >= 0) cudaSetDevice(prev);

@@ -101,6 +101,9 @@ struct gt_context {
     cudaEvent_t up_ev[8] = {};
     cudaEvent_t copy_done = nullptr;
     cudaEvent_t main_ev = nullptr;
+    // second compute stream: the chunks of a chunked walk alternate between it and `stream`
+    cudaStream_t walk2 = nullptr;
+    cudaEvent_t walk2_start = nullptr, walk2_done = nullptr;
 };
 
 struct gt_tree {
@@ -186,6 +189,7 @@ enum Slot {
     kSlotOut0, kSlotOut1, kSlotOut2, kSlotOut3, kSlotOut4, kSlotOut5,
     kSlotStack, kSlotCounters, kSlotDirect, kSlotGroupRoot, kSlotMacL2,
     kSlotNgb0, kSlotNgb1, kSlotNgb2,
+    kSlotStack2,  // traversal stacks of the second compute stream (chunked walks)
     kSlotCount
 };
 

@@ -1398,12 +1398,31 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                 check_cuda(cudaEventRecord(ctx->up_ev[c], ctx->copy_stream), "event");
             }
         }
+        // The chunks alternate between the context stream and a second compute stream, so a chunk
+        // fills the SMs that the previous one's last groups leave idle.  The warps of two chunks in
+        // flight need their own traversal stacks; a plan's own buffers keep one stream.
+        const bool two = wb == nullptr;
+        cudaStream_t cs[2] = {st, two ? ctx->walk2 : st};
+        int* stacks[2] = {a.stack, two ? (int*)scratch(ctx, kSlotStack2, stack_bytes) : a.stack};
         check_cuda(cudaEventRecord(ctx->ev0, st), "event");
+        if (two) {
+            check_cuda(cudaEventRecord(ctx->walk2_start, st), "event");
+            check_cuda(cudaStreamWaitEvent(ctx->walk2, ctx->walk2_start, 0), "wait");
+        }
         for (int c = 0; c < kChunks; ++c) {
             const int g0 = hb[c].x, g1 = hb[c + 1].x;
-            if (rq.host_aold) check_cuda(cudaStreamWaitEvent(st, ctx->up_ev[c], 0), "wait");
+            cudaStream_t s = cs[c & 1];
+            if (rq.host_aold) check_cuda(cudaStreamWaitEvent(s, ctx->up_ev[c], 0), "wait");
             if (g1 > g0) {
+                // the dispatch launches on ctx->stream: point it at this chunk's stream meanwhile
+                struct OnStream {
+                    gt_context* c;
+                    cudaStream_t old;
+                    ~OnStream() { c->stream = old; }
+                } on{ctx, ctx->stream};
+                ctx->stream = s;
                 WalkArgs ac = a;
+                ac.stack = stacks[c & 1];
                 ac.groups = groups + g0;
                 ac.n_groups = g1 - g0;
                 ac.group_root = roots ? roots + g0 : nullptr;
@@ -1415,7 +1434,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                 else dispatch<4>(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false, rq.mac);
             }
             // this chunk's targets [hb[c].y, hb[c+1].y) go back while the next chunk runs
-            check_cuda(cudaEventRecord(ctx->chunk_ev[c], st), "event");
+            check_cuda(cudaEventRecord(ctx->chunk_ev[c], s), "event");
             check_cuda(cudaStreamWaitEvent(ctx->copy_stream, ctx->chunk_ev[c], 0), "wait");
             const int64_t t0 = hb[c].y, t1 = hb[c + 1].y;
             for (const auto& o : outs)
@@ -1423,6 +1442,10 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                     check_cuda(cudaMemcpyAsync(o.host + t0 * o.stride, o.dev + t0 * o.stride,
                                                (size_t)(t1 - t0) * o.stride * sizeof(double), cudaMemcpyDeviceToHost,
                                                ctx->copy_stream), "d2h chunk");
+        }
+        if (two) {
+            check_cuda(cudaEventRecord(ctx->walk2_done, ctx->walk2), "event");
+            check_cuda(cudaStreamWaitEvent(st, ctx->walk2_done, 0), "wait");
         }
         check_cuda(cudaEventRecord(ctx->ev1, st), "event");
         check_cuda(cudaEventRecord(ctx->copy_done, ctx->copy_stream), "event");
