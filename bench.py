@@ -129,6 +129,18 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------------
 # CPU reference walk on a bounded sample
 # ---------------------------------------------------------------------------------------------
+def window_sample(orderbuf, batch, want, rng):
+    """Whole windows of `batch` consecutive targets of orderbuf (the windows accel_grouped forms
+    over targets = orderbuf, shmem/tree.cc:668-670), picked at random until the sample holds at
+    least `want` targets; returned in tree order, so the reference's windows over the sample are
+    the same windows."""
+    nw = len(orderbuf) // batch
+    k = int(min(nw, max(1, -(-want // batch))))
+    w = np.sort(rng.choice(nw, size=k, replace=False))
+    pos = (w[:, None] * batch + np.arange(batch)[None, :]).ravel()
+    return orderbuf[pos].astype(np.uint32)
+
+
 def leaf_group_sample(orderbuf, leaf_of, want, rng):
     """Whole leaf groups (consecutive orderbuf runs with one leaf), picked at random until the
     sample holds at least `want` targets; returned in tree order."""
@@ -162,29 +174,118 @@ class CpuReference:
         T = self.lib.build(P)
         return T, time.perf_counter() - t0
 
-    def walk(self, T, targets, aold, theta=0.0):
+    def walk(self, T, targets, aold, theta=0.0, batch=0):
         if self.kind == "reference":
-            return T.accel_grouped(targets, theta, 1.0, 0, aold=aold)
-        return T.accel_grouped(targets, theta, 1.0, 0, aold=aold)[:3]
+            return T.accel_grouped(targets, theta, 1.0, batch, aold=aold)
+        return T.accel_grouped(targets, theta, 1.0, batch, aold=aold)[:3]
+
+    def direct(self, T, P, targets):
+        """FP64 direct sum: the reference's own accel_brute (shmem/tree.cc:946-971)."""
+        if self.kind == "reference":
+            return T.accel_brute(targets, 1.0)
+        return self.lib.direct(P, targets)[:3]
 
 
-def cpu_sample_walk(cpu, T, aold_orig, seconds, rng, alpha=None):
-    """Time one walk over a sample of whole leaf groups sized to about `seconds` of CPU work."""
+def ph_order(P):
+    """Live particles in Peano-Hilbert order of shmem::build's 20-bit cells, ties in index order:
+    the GPU tree's order.  The keys come from the oracle's key function, which is pinned bit-exact
+    to the reference's peano_hilbert_key (system/peano.cc:297-313)."""
+    from oracle import Restatement
+
+    keys, _ = Restatement().keys20(P, key_mode=1)
+    live = np.nonzero(np.asarray(P["m"]) > 0)[0]
+    return live[np.argsort(keys[live], kind="stable")].astype(np.uint32)
+
+
+def sample_groups(T, batch, want, rng, order=None):
     ob, _, leaf = T.order()
-    tg = leaf_group_sample(ob, leaf, 4096, rng)
+    if batch > 0:
+        return window_sample(ob if order is None else order, batch, want, rng)
+    return leaf_group_sample(ob, leaf, want, rng)
+
+
+def cpu_sample_walk(cpu, T, aold_orig, seconds, rng, alpha=None, batch=0, order=None):
+    """Time one walk over a sample of whole groups (windows of `batch` consecutive targets of
+    `order` -- the reference's own tree order by default -- or leaf groups for batch 0) sized to
+    about `seconds` of CPU work."""
+    tg = sample_groups(T, batch, 4096, rng, order)
 
     def aold_for(t):
         if aold_orig is not None:
             return aold_orig[t]
-        a = cpu.walk(T, t, None, theta=0.7)
+        a = cpu.walk(T, t, None, theta=0.7, batch=batch)
         return alpha * np.sqrt(a[0] ** 2 + a[1] ** 2 + a[2] ** 2)
 
     t0 = time.perf_counter()
-    cpu.walk(T, tg, aold_for(tg))
+    cpu.walk(T, tg, aold_for(tg), batch=batch)
     dt = time.perf_counter() - t0
-    want = int(min(len(ob), max(4096, len(tg) * seconds / max(dt, 1e-4))))
-    tg = leaf_group_sample(ob, leaf, want, rng)
+    want = int(min(T.nlive, max(4096, len(tg) * seconds / max(dt, 1e-4))))
+    tg = sample_groups(T, batch, want, rng, order)
     return tg, aold_for(tg)
+
+
+def error_sample(n, rank=0):
+    """The seeded 4096-particle sample both arms score against the FP64 direct sum."""
+    rng = np.random.default_rng(77 + rank)
+    return np.sort(rng.choice(n, size=min(4096, n), replace=False)).astype(np.uint32)
+
+
+def reference_error(cpu, T, P, alpha, batch, order=None):
+    """The reference walk's force error on the seeded sample: the groups holding the sampled
+    particles (whole windows of `order`, or whole leaf groups) are walked as in the timed steps --
+    bootstrap theta = 0.7, aold = alpha |a|, then the relative criterion -- and scored against the
+    reference's own FP64 direct sum (the recipe of shmem/mfm.cc:2713-2789)."""
+    n = len(P["m"])
+    sample = error_sample(n)
+    ob, rank, leaf = T.order()
+    if order is not None:
+        ob = order
+        rank = np.zeros(n, np.int64)
+        rank[ob] = np.arange(len(ob))
+    if batch > 0:
+        w = np.unique(rank[sample] // batch)
+        pos = (w[:, None] * batch + np.arange(batch)[None, :]).ravel()
+        pos = pos[pos < len(ob)]
+    else:
+        lv = leaf[ob]
+        keep = np.isin(lv, np.unique(leaf[sample]))
+        pos = np.nonzero(keep)[0]
+    tg = ob[pos].astype(np.uint32)
+    a = cpu.walk(T, tg, None, theta=0.7, batch=batch)
+    aold = alpha * np.sqrt(a[0] ** 2 + a[1] ** 2 + a[2] ** 2)
+    a = cpu.walk(T, tg, aold, batch=batch)
+    at = np.full(n, -1, np.int64)
+    at[tg] = np.arange(len(tg))
+    k = at[sample]
+    t0 = time.perf_counter()
+    ref = cpu.direct(T, P, sample)
+    td = time.perf_counter() - t0
+    err = relerr([a[c][k] for c in range(3)], ref)
+    return {"vs": "FP64 direct sum (the reference's accel_brute)", "sample": int(len(sample)),
+            "median": float(np.median(err)), "p99": float(np.quantile(err, 0.99)),
+            "walked_targets": int(len(tg)), "direct_s": td}
+
+
+def grouping_of(args):
+    """accel_grouped's batch for the --group choice, and its description."""
+    order = "Morton" if args.key == "morton" else "Peano-Hilbert"
+    if args.group == "batch":
+        return args.group_max, (f"windows of {args.group_max} consecutive targets in {order} tree order "
+                                f"(accel_grouped batch {args.group_max})")
+    if args.group == "leaf":
+        return 0, "leaf groups (accel_grouped batch 0)"
+    return None, f"tree nodes of at most {args.group_max} particles"
+
+
+def workload_config(args, n):
+    """The `config` object, identical in both arms for the same arguments."""
+    cfg = WORKLOADS[args.workload]
+    alpha = args.alpha if args.alpha is not None else cfg["alpha"]
+    return {"workload": args.workload, "description": cfg["desc"], "n": int(n),
+            "criterion": f"plain relative criterion alpha={alpha} after a theta=0.7 bootstrap walk",
+            "mac": "plain", "grouping": grouping_of(args)[1],
+            "l2": (f"inputs larger than L2: {n * 32 / 2**20:.0f} MiB of particles per walk" if n * 32 > 126 * 2**20
+                   else f"{n * 32 / 2**20:.0f} MiB of particles per walk: fits in L2")}
 
 
 def run_reference_arm(args):
@@ -192,31 +293,42 @@ def run_reference_arm(args):
     if rank != 0:
         return
     cfg = WORKLOADS[args.workload]
+    alpha = args.alpha if args.alpha is not None else cfg["alpha"]
+    batch, _ = grouping_of(args)
+    if batch is None:
+        print(json.dumps({"impl": "reference", "unavailable": "node groups are not a reference grouping"}))
+        return
     P = make_workload(args.workload)
+    n = len(P["m"])
     cpu = CpuReference()
     T, tbuild = cpu.build(P)
+    # windows over the same order as the GPU arm's: Peano-Hilbert (the targets' order is the
+    # caller's choice in accel_grouped), or the reference's own Morton orderbuf with --key morton
+    order = ph_order(P) if (batch > 0 and args.key == "peano") else None
     rng = np.random.default_rng(123)
-    tg, aold = cpu_sample_walk(cpu, T, None, args.sample_seconds, rng, alpha=cfg["alpha"])
+    tg, aold = cpu_sample_walk(cpu, T, None, args.sample_seconds, rng, alpha=alpha, batch=batch, order=order)
     for _ in range(args.warmup):
-        cpu.walk(T, tg, aold)
+        cpu.walk(T, tg, aold, batch=batch)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        cpu.walk(T, tg, aold)
+        cpu.walk(T, tg, aold, batch=batch)
         times.append(time.perf_counter() - t0)
     t = float(np.mean(times))
     value = len(tg) / t
+    error = reference_error(cpu, T, P, alpha, batch, order)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "particles/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": args.workload, "description": cfg["desc"],
-                                        "n": int(len(P["m"])), "criterion": f"relative alpha={cfg['alpha']}",
-                                        "grouping": "leaf groups (batch 0)"},
+        "data": "synthetic (seeded; see config.description)", "config": workload_config(args, n),
         "cpu_baseline": {"value": value, "unit": "particles/s", "cores": cpu.cores, "kind": cpu.kind,
-                         "sample": f"{len(tg)} targets in whole leaf groups picked at random; "
-                                   f"tree prebuilt ({tbuild:.1f} s build, not timed)"},
+                         "sample": f"{len(tg)} of {n} targets in whole groups picked at random, "
+                                   f"walked per step; particles/s over "
+                                   f"the sample stands for the whole job; tree prebuilt ({tbuild:.1f} s "
+                                   f"build, not timed)"},
         "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "error": error,
     }
     print(json.dumps(line), flush=True)
 
@@ -239,13 +351,30 @@ def read_profile_traffic(workload):
         return None
 
 
-def warm_build_ms(ctx, dev, offsets=None, reps=3):
+def window_parity(cpu, Tc, ob_gpu, aold_tree, full, batch, n_windows=256, seed=9):
+    """This walk against the reference's accel_grouped on whole windows of this walk's own groups:
+    the windows are passed in this tree's order with the same batch, so the reference forms exactly
+    these windows (shmem/tree.cc:668-670), with the same aold.  `full` holds this walk's
+    accelerations by particle index."""
+    rng = np.random.default_rng(seed)
+    nw = len(ob_gpu) // batch
+    w = np.sort(rng.choice(nw, size=min(n_windows, nw), replace=False))
+    pos = (w[:, None] * batch + np.arange(batch)[None, :]).ravel()
+    tg = ob_gpu[pos].astype(np.uint32)
+    r = cpu.walk(Tc, tg, aold_tree[pos], batch=batch)
+    e = relerr([full[c][tg] for c in range(3)], r)
+    return {"vs": f"the reference's accel_grouped ({cpu.kind}) on the same windows and aold",
+            "targets": int(len(tg)), "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99)),
+            "max": float(e.max())}
+
+
+def warm_build_ms(ctx, dev, offsets=None, reps=3, key_mode=0):
     """Device time of the tree build once the kernels are loaded and the memory pool holds the
     tree's arrays (the steady state of a rebuild every step); the first call also pays module
     loading and pool growth.  Median of `reps` rebuilds, per stage."""
     runs = []
     for _ in range(reps):
-        T2 = ctx.build(dev, offsets=offsets)
+        T2 = ctx.build(dev, offsets=offsets, key_mode=key_mode)
         runs.append(T2.info()["build_ms"])
         T2.free()
     return {k: float(np.median([r[k] for r in runs])) for k in runs[0]}
@@ -345,11 +474,12 @@ def run_gpu_arm(args):
     dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
     ctx = g.Context(local, torch_stream=True)
     peak32, peak64 = ctx.measure_peaks()
-    T = ctx.build(dev)
+    key_mode = g.GT_KEY_MORTON if args.key == "morton" else g.GT_KEY_PEANO
+    T = ctx.build(dev, key_mode=key_mode)
     info = T.info()
     nl = info["n_live"]
     build_cold = info["build_ms"]
-    info["build_ms"] = warm_build_ms(ctx, dev)
+    info["build_ms"] = warm_build_ms(ctx, dev, key_mode=key_mode)
     out = tuple(torch.empty(nl, dtype=torch.float64, device="cuda") for _ in range(3))
     # bootstrap walk (theta = 0.7, aold = 0), then aold = alpha |a| / G
     ctx.accel_grouped(T, None, theta=0.7, outs=out + (None,), **wopts)
@@ -396,8 +526,7 @@ def run_gpu_arm(args):
     value = nl * world / t_step
 
     # accuracy: FP64 direct sum on a seeded 4096-particle sample
-    rng = np.random.default_rng(77 + rank)
-    sample = np.sort(rng.choice(n, size=min(4096, n), replace=False)).astype(np.uint32)
+    sample = error_sample(n, rank)
     full = ctx.accel_grouped(T, None, aold=aold, theta=0.0, out_order=g.GT_OUT_ORIGINAL, **wopts)
     full = [f.cpu().numpy() for f in full]
     dref = ctx.direct(P, sample)
@@ -423,7 +552,7 @@ def run_gpu_arm(args):
         for it in range(args.warmup + args.steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            T2 = hctx.build(pin)
+            T2 = hctx.build(pin, key_mode=key_mode)
             hctx.accel_grouped(T2, None, aold=aold_h, theta=0.0, outs=tuple(ho) + (None,), **wopts)
             t1 = time.perf_counter()
             T2.free()
@@ -440,20 +569,29 @@ def run_gpu_arm(args):
                "includes": "H2D of x,y,z,m,soft,aold from pinned memory + tree build + walk + D2H of ax,ay,az"}
         hctx.close()
 
-    # CPU baseline (rank 0 only, N=1 only): the reference walk on a bounded sample
+    # CPU baseline (rank 0 only, N=1 only): the reference walk on a bounded sample, and the
+    # parity of this walk with the reference's on whole windows of this walk's own groups
     cpu_line = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = CpuReference()
         Tc, tbuild = cpu.build(P)
+        ob_gpu = T.download(nodes=False)["orderbuf"]
+        aold_tree = aold.cpu().numpy()
         aold_orig = np.zeros(n)
-        aold_orig[T.download(nodes=False)["orderbuf"]] = aold.cpu().numpy()
-        tg, ao = cpu_sample_walk(cpu, Tc, aold_orig, args.sample_seconds, np.random.default_rng(123))
+        aold_orig[ob_gpu] = aold_tree
+        batch, _ = grouping_of(args)
+        batch = 0 if batch is None else batch
+        tg, ao = cpu_sample_walk(cpu, Tc, aold_orig, args.sample_seconds, np.random.default_rng(123),
+                                 batch=batch, order=ob_gpu if batch > 0 else None)
         t0 = time.perf_counter()
-        cpu.walk(Tc, tg, ao)
+        cpu.walk(Tc, tg, ao, batch=batch)
         tc = time.perf_counter() - t0
         cpu_line = {"value": len(tg) / tc, "unit": "particles/s", "cores": cpu.cores, "kind": cpu.kind,
-                    "sample": f"{len(tg)} targets in whole leaf groups picked at random, the same aold; "
-                              f"tree prebuilt ({tbuild:.1f} s CPU build, not timed)"}
+                    "sample": f"{len(tg)} targets in whole groups of this walk's grouping picked at "
+                              f"random, the same aold; tree prebuilt ({tbuild:.1f} s CPU build, not timed)"}
+        if args.group == "batch":
+            parity = window_parity(cpu, Tc, ob_gpu, aold_tree, full, args.group_max, n_windows=256)
 
     achieved = FLOPS_PER_INTERACTION * inter / t_kernel / 1e12
     if learned and "value" in learned:
@@ -463,15 +601,12 @@ def run_gpu_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded; see config.description)",
-        "config": {"workload": args.workload, "description": cfg["desc"], "n": n,
-                   "criterion": f"plain relative criterion alpha={alpha} after a theta=0.7 bootstrap walk",
-                   "mac": "plain", "grouping": {"leaf": "leaf groups (accel_grouped batch 0)",
-                                "batch": f"windows of {args.group_max} consecutive targets in Peano-Hilbert tree order (accel_grouped batch {args.group_max})",
-                                "node": f"tree nodes of at most {args.group_max} particles"}[args.group],
-                   "l2": f"inputs larger than L2: {n * 32 / 2**20:.0f} MiB of particles + "
-                         f"{info['n_nodes'] * 64 / 2**20:.0f} MiB of nodes per walk",
-                   "precision": "FP64 positions and group-relative offsets, FP32 interactions, "
-                                "Kahan-compensated FP32 acceleration sums, FP64 potential/final sums"},
+        "config": workload_config(args, n),
+        "precision": "FP64 positions and group-relative offsets, FP32 interactions; FP32 partial sums "
+                     "per interaction-list flush, Kahan-compensated across flushes; FP64 potential and "
+                     "final sums",
+        "tree_bytes": int(info["n_nodes"]) * 64,
+        "parity": parity,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
                      "frac": achieved / peak32, "traffic": read_profile_traffic(args.workload),
                      "peak_source": "measured FP32 FMA-chain probe on this GPU (gt_measure_peaks), "
@@ -879,6 +1014,8 @@ def main():
                          "targets in tree order (accel_grouped batch > 0); node: tree nodes of at "
                          "most --group-max particles")
     ap.add_argument("--group-max", type=int, default=32)
+    ap.add_argument("--key", choices=["peano", "morton"], default="peano",
+                    help="sort key of the tree: the window order of --group batch")
     ap.add_argument("--sample-seconds", type=float, default=8.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

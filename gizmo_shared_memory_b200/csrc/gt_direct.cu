@@ -97,8 +97,11 @@ direct_kernel(const double* __restrict__ x, const double* __restrict__ y, const 
     __shared__ double shzeta[GAS ? kDirTile : 1];
     __shared__ unsigned char shgas[GAS ? kDirTile : 1];
     const int64_t t = (int64_t)blockIdx.x * kDirThreads + threadIdx.x;
-    const bool live = t < nt;
-    const int64_t self = live ? (int64_t)targets[t] : -1;
+    // a target index at or beyond n (device target arrays are not checked on the host) reads
+    // nothing and sums nothing: its outputs are zero
+    const bool slot = t < nt;
+    const int64_t self = slot ? (int64_t)targets[t] : -1;
+    const bool live = slot && self < n;
     const double px = live ? x[self] : 0.0, py = live ? y[self] : 0.0, pz = live ? z[self] : 0.0;
     const double ps = (live && soft) ? soft[self] : 0.0;
     // a gas target with mass: zeta_t / m_t and 1 / m_t of its pair terms
@@ -161,7 +164,7 @@ direct_kernel(const double* __restrict__ x, const double* __restrict__ y, const 
         }
         __syncthreads();
     }
-    if (live) {
+    if (slot) {
         double* P = partial + (int64_t)blockIdx.y * 4 * nt;
         P[t] = FP64 ? ax : (double)fx;
         P[nt + t] = FP64 ? ay : (double)fy;
@@ -289,6 +292,7 @@ extern "C" int gt_direct_noalloc(int64_t n, const double* x, const double* y, co
     if (precision != GT_DIRECT_FP64 && precision != GT_DIRECT_FP32) return GT_ERR_INVALID;
     if (n_targets > GT_DIRECT_NOALLOC_MAX_TARGETS) return GT_ERR_OVERFLOW;
     if (n_targets == 0) return GT_OK;
+    if (n == 0) return GT_ERR_INVALID;  // no particle can be a target
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
         cudaGetLastError();

@@ -205,6 +205,215 @@ __global__ void __launch_bounds__(256) mac_sample_kernel(const SampleArgs A) {
     }
 }
 
+// ---- the exact-label criterion: what a perfect learned predictor could reach ------------------
+//
+// ceiling_kernel walks chosen windows of consecutive targets as the grouped walk does (nearest
+// point of the window's box, largest target softening, leaves offered to the criterion first;
+// shmem/tree.cc:682-702, 744-779) and sums the forces in FP64.  Its acceptance rule is either
+//   mode 0: the plain relative criterion, M L^2 <= r^4 alpha min|a| (shmem/tree.h:134-135), or
+//   mode 1: exact labels -- inside the band rho_lo < rho <= rho_hi the warp sums the node's
+//           particles for every target of the window and accepts the node only when the monopole's
+//           worst error over the window, |a_mono - a_exact|_t / |a_t|, is at most eps; below the
+//           band it accepts, above it it opens.
+// Both modes share the softening-overlap and inside-node arms.  Mode 1 is the rule a learned
+// criterion that predicted every (window, node) error exactly would apply, so its interactions and
+// node visits at a given force error bound what any learned acceptance rule over the monopole walk
+// can save.  Mode 0 reproduces the production walk's decisions (the test checks its counts).
+struct CeilArgs {
+    const GNode* nodes;
+    const SrcP* src;
+    const double* ssoft;
+    const int64_t* wins;  // window indices: targets [w * window, min((w + 1) * window, n_live))
+    int n_win, window;
+    int64_t n_live;
+    const double* amag;   // |a| per live particle in tree order
+    double alpha, eps, rho_lo, rho_hi;
+    int mode;
+    int* stack;
+    int stack_cap;
+    unsigned* next;
+    double *ax, *ay, *az;          // n_win * window, slot w * window + lane
+    unsigned long long* counts;    // per window: visits, multipole, pairs, labelled nodes, label sum
+    int* error;
+};
+
+// FP64 force factor of the cubic spline of support h (shmem/tree.h:59-67): 1/r^3 outside.
+__device__ __forceinline__ double spline_force_d(double r2, double h) {
+    const double r = sqrt(r2);
+    if (r >= h) return 1.0 / (r2 * r);
+    const double hi = 1.0 / h, u = r * hi, hi3 = hi * hi * hi;
+    if (u < 0.5) return hi3 * (10.666666666666667 + u * u * (32.0 * u - 38.4));
+    return hi3 * (21.333333333333332 - 48.0 * u + 38.4 * u * u - 10.666666666666667 * u * u * u -
+                  0.06666666666666667 / (u * u * u));
+}
+
+__global__ void __launch_bounds__(256) ceiling_kernel(const CeilArgs A) {
+    __shared__ SrcP tile[8][32];
+    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + wi;
+    int* stk = A.stack + (size_t)gw * A.stack_cap;
+    for (;;) {
+        int g = 0;
+        if (lane == 0) g = (int)atomicAdd(A.next, 1u);
+        g = __shfl_sync(kFull, g, 0);
+        if (g >= A.n_win) break;
+        const int64_t t0 = A.wins[g] * A.window;
+        const int nt = (int)min((int64_t)A.window, A.n_live - t0);
+        const bool tv = lane < nt;
+        double px = 0, py = 0, pz = 0, ps = 0, am = 1e300;
+        if (tv) {
+            const SrcP s = A.src[t0 + lane];
+            px = s.x; py = s.y; pz = s.z;
+            ps = A.ssoft[t0 + lane];
+            am = A.amag[t0 + lane];
+        }
+        const double lx = wmin(tv ? px : 1e300), hx = wmax(tv ? px : -1e300);
+        const double ly = wmin(tv ? py : 1e300), hy = wmax(tv ? py : -1e300);
+        const double lz = wmin(tv ? pz : 1e300), hz = wmax(tv ? pz : -1e300);
+        const double emax = wmax(tv ? ps : 0.0);
+        const double aold = A.alpha * wmin(am);
+        const double inv_a = tv && am > 0.0 ? 1.0 / am : 0.0;  // 0: a target without |a| never accepts
+        double sx = 0, sy = 0, sz = 0;
+        unsigned long long c_vis = 0, c_mul = 0, c_pair = 0, c_lab = 0, c_labsum = 0;
+        unsigned c_self = 0;  // pairs at r = 0 (the target itself), which count as no interaction
+
+        int top = 1;
+        if (lane == 0) stk[0] = 0;
+        __syncwarp();
+        bool overflow = false;
+        while (top > 0) {
+            const int npop = min(top, 32);
+            top -= npop;
+            const int node = lane < npop ? stk[top + lane] : -1;
+            __syncwarp();
+            GNode nd;
+            nd.first = -1; nd.nchild = 0; nd.plo = nd.phi = 0; nd.cx = nd.cy = nd.cz = nd.mass = 0.0;
+            bool open = false, label = false;
+            if (node >= 0) {
+                nd = A.nodes[node];
+                const double len = (double)nd.len;
+                const double dx = fmax(0.0, fmax(lx - nd.cx, nd.cx - hx));
+                const double dy = fmax(0.0, fmax(ly - nd.cy, nd.cy - hy));
+                const double dz = fmax(0.0, fmax(lz - nd.cz, nd.cz - hz));
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                const double rt = emax + 0.6 * len, rn = (double)nd.soft + 0.6 * len;
+                const double lim = 0.6 * len;
+                const bool hard = (r2 < rt * rt) | (r2 < rn * rn) | ((dx < lim) & (dy < lim) & (dz < lim));
+                if (hard || !(aold > 0)) {
+                    open = true;
+                } else {
+                    const double rho = nd.mass * len * len / (r2 * r2 * aold);
+                    if (A.mode == 0) open = rho > 1.0;
+                    else if (rho <= A.rho_lo) open = false;
+                    else if (rho > A.rho_hi) open = true;
+                    else label = true;
+                }
+            }
+            // exact labels, one node at a time across the window's targets; the node's particles
+            // are staged 32 at a time in shared memory
+            unsigned lm = __ballot_sync(kFull, label);
+            while (lm) {
+                const int l = __ffs(lm) - 1;
+                lm &= lm - 1;
+                const int plo = __shfl_sync(kFull, nd.plo, l), phi = __shfl_sync(kFull, nd.phi, l);
+                const double ncx = __shfl_sync(kFull, nd.cx, l), ncy = __shfl_sync(kFull, nd.cy, l);
+                const double ncz = __shfl_sync(kFull, nd.cz, l), nm = __shfl_sync(kFull, nd.mass, l);
+                double ex = 0, ey = 0, ez = 0;
+                for (int base = plo; base < phi; base += 32) {
+                    if (base + lane < phi) tile[wi][lane] = A.src[base + lane];
+                    __syncwarp();
+                    const int k = min(32, phi - base);
+                    for (int j = 0; j < k; ++j) {
+                        const SrcP q = tile[wi][j];
+                        const double dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+                        const double r2 = dx * dx + dy * dy + dz * dz;
+                        if (r2 > 0.0) {
+                            const double f = (double)q.m * spline_force_d(r2, fmax(ps, (double)q.soft));
+                            ex += dx * f; ey += dy * f; ez += dz * f;
+                        }
+                    }
+                    __syncwarp();
+                }
+                const double mdx = ncx - px, mdy = ncy - py, mdz = ncz - pz;
+                const double mr2 = mdx * mdx + mdy * mdy + mdz * mdz;
+                const double mf = nm / (mr2 * sqrt(mr2));
+                const double ddx = mdx * mf - ex, ddy = mdy * mf - ey, ddz = mdz * mf - ez;
+                const double e = tv ? (inv_a > 0.0 ? sqrt(ddx * ddx + ddy * ddy + ddz * ddz) * inv_a : 1e300) : 0.0;
+                const double worst = wmax(e);
+                if (lane == l) open = worst > A.eps;
+                if (lane == 0) { ++c_lab; c_labsum += (unsigned long long)(phi - plo); }
+            }
+            const bool leaf = nd.first < 0;
+            const bool accept = node >= 0 && !open;
+            const bool expand = node >= 0 && open && leaf;
+            const bool push = node >= 0 && open && !leaf;
+            if (lane == 0) c_vis += npop;
+            // accepted nodes: Newtonian monopoles for every target
+            unsigned am_ = __ballot_sync(kFull, accept);
+            if (lane == 0) c_mul += (unsigned long long)__popc(am_) * nt;
+            while (am_) {
+                const int l = __ffs(am_) - 1;
+                am_ &= am_ - 1;
+                const double ncx = __shfl_sync(kFull, nd.cx, l), ncy = __shfl_sync(kFull, nd.cy, l);
+                const double ncz = __shfl_sync(kFull, nd.cz, l), nm = __shfl_sync(kFull, nd.mass, l);
+                const double dx = ncx - px, dy = ncy - py, dz = ncz - pz;
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                if (tv && r2 > 0.0) {
+                    const double f = nm / (r2 * sqrt(r2));
+                    sx += dx * f; sy += dy * f; sz += dz * f;
+                }
+            }
+            // expanded leaves: their particles with the pair rule (kernel of the larger softening)
+            unsigned em = __ballot_sync(kFull, expand);
+            while (em) {
+                const int l = __ffs(em) - 1;
+                em &= em - 1;
+                const int plo = __shfl_sync(kFull, nd.plo, l), phi = __shfl_sync(kFull, nd.phi, l);
+                if (lane == 0) c_pair += (unsigned long long)(phi - plo) * nt;
+                for (int base = plo; base < phi; base += 32) {
+                    if (base + lane < phi) tile[wi][lane] = A.src[base + lane];
+                    __syncwarp();
+                    const int k = min(32, phi - base);
+                    for (int j = 0; j < k; ++j) {
+                        const SrcP q = tile[wi][j];
+                        const double dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+                        const double r2 = dx * dx + dy * dy + dz * dz;
+                        if (tv && r2 > 0.0) {
+                            const double f = (double)q.m * spline_force_d(r2, fmax(ps, (double)q.soft));
+                            sx += dx * f; sy += dy * f; sz += dz * f;
+                        }
+                        c_self += (tv && r2 == 0.0);
+                    }
+                    __syncwarp();
+                }
+            }
+            const int nch = push ? nd.nchild : 0;
+            const int incl = warp_incl_scan_i(nch);
+            const int tot = __shfl_sync(kFull, incl, 31);
+            if (top + tot > A.stack_cap) { overflow = true; break; }
+            for (int c = 0; c < nch; ++c) stk[top + incl - nch + c] = nd.first + c;
+            top += tot;
+            __syncwarp();
+        }
+        if (overflow) {
+            if (lane == 0) atomicExch(A.error, 1);
+            continue;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c_self += __shfl_xor_sync(kFull, c_self, o);
+        const int64_t slot = (int64_t)g * A.window + lane;
+        if (lane < A.window) {
+            A.ax[slot] = tv ? sx : 0.0;
+            A.ay[slot] = tv ? sy : 0.0;
+            A.az[slot] = tv ? sz : 0.0;
+        }
+        if (lane == 0) {
+            unsigned long long* c = A.counts + (size_t)g * 5;
+            c[0] = c_vis; c[1] = c_mul; c[2] = c_pair - c_self; c[3] = c_lab; c[4] = c_labsum;
+        }
+    }
+}
+
 // ---- training --------------------------------------------------------------------------------
 constexpr int kActStride = kMacIn + 4 * kMacHidden + 1;  // xn, h1, h2, d2, d1, dy
 
@@ -362,6 +571,34 @@ void init_params(float* model, uint64_t seed, float bias_out) {
 }
 
 }  // namespace
+
+void run_mac_ceiling(gt_context* ctx, const gt_tree* t, const double* amag, double alpha, int window,
+                     int64_t n_win, const int64_t* wins, int mode, double eps, double rho_lo, double rho_hi,
+                     double* ax, double* ay, double* az, unsigned long long* counts) {
+    cudaStream_t st = ctx->stream;
+    if (n_win <= 0) return;
+    const int warps = 8;
+    const int blocks = std::max(1, std::min<int>((int)((n_win + warps - 1) / warps), ctx->num_sms * 4));
+    const int stack_cap = 256 * std::max(1, t->n_levels) + 32;
+    CeilArgs a;
+    a.nodes = t->nodes; a.src = t->src; a.ssoft = t->ssoft;
+    a.wins = wins; a.n_win = (int)n_win; a.window = window; a.n_live = t->n_live;
+    a.amag = amag; a.alpha = alpha; a.eps = eps; a.rho_lo = rho_lo; a.rho_hi = rho_hi; a.mode = mode;
+    a.stack = (int*)scratch(ctx, kSlotStack, (size_t)blocks * warps * stack_cap * 4);
+    a.stack_cap = stack_cap;
+    unsigned long long* ctr = (unsigned long long*)scratch(ctx, kSlotCounters, 256);
+    a.next = (unsigned*)ctr;
+    a.error = (int*)(ctr + 1);
+    a.ax = ax; a.ay = ay; a.az = az; a.counts = counts;
+    check_cuda(cudaMemsetAsync(ctr, 0, 16, st), "memset");
+    ceiling_kernel<<<blocks, warps * 32, 0, st>>>(a);
+    check_launch(ctx, "ceiling_kernel");
+    int err = 0;
+    check_cuda(cudaMemcpyAsync(ctx->pinned, ctr + 1, 4, cudaMemcpyDeviceToHost, st), "D2H");
+    check_cuda(cudaStreamSynchronize(st), "sync");
+    std::memcpy(&err, ctx->pinned, 4);
+    if (err) throw Fail{GT_ERR_OVERFLOW, "exact-label walk stack overflow"};
+}
 
 void run_mac_sample(gt_context* ctx, const gt_tree* t, const double* amag, double alpha, int window,
                     int64_t stride, double rho_lo, double rho_hi, int64_t cap, float* feat,

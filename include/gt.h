@@ -440,9 +440,13 @@ GT_API int gt_direct_gas(gt_context* ctx, int64_t n, const double* x, const doub
  * until the process exits).  The call never calls cudaMalloc or cudaFree.  It enqueues its two
  * kernels on `stream` (NULL: the default stream) and returns without synchronising.
  *  - n_targets above GT_DIRECT_NOALLOC_MAX_TARGETS is rejected with GT_ERR_OVERFLOW, before
- *    anything is launched.
+ *    anything is launched; n == 0 with n_targets > 0 is rejected with GT_ERR_INVALID.
+ *  - Every targets[k] must be < n.  The device array is not read on the host, so an index at or
+ *    beyond n is not reported: the kernel reads nothing for it and its outputs are zero.
  *  - The first call on a device looks up the array's device address with cudaGetSymbolAddress
  *    (once per device, with that device current); make that first call before any stream capture.
+ *    The address is kept for the life of the process: do not call this entry point after
+ *    cudaDeviceReset on that device (the reset unloads the module and the kept address is stale).
  *  - Every call shares the one array, which keeps the last call's contents (each call overwrites
  *    every partial it reads, so nothing needs clearing).  Calls that overlap on the GPU -- on
  *    different streams, or from different host threads -- race on it and give wrong results;
@@ -479,6 +483,22 @@ GT_API int gt_mac_sample(gt_context* ctx, const gt_tree* tree, const double* ama
                          int window, int64_t group_stride, double rho_lo, double rho_hi,
                          int64_t capacity, int mem, float* features, float* labels, float* rho,
                          int64_t* n_samples);
+/* The exact-label walk: what a perfect learned criterion could reach.  Walks the windows
+ * windows[k] (targets [w * window, min((w + 1) * window, n_live)) in tree order, window <= 32) as
+ * the grouped walk does -- nearest point of the window's box, largest target softening, leaves
+ * offered to the criterion (shmem/tree.cc:682-779) -- with FP64 sums.  mode 0 accepts by the plain
+ * relative criterion M L^2 <= r^4 alpha min|a| (shmem/tree.h:134-135) and reproduces the grouped
+ * walk's decisions; mode 1 sums, for every node whose rho = M L^2 / (r^4 alpha min|a|) lies in
+ * (rho_lo, rho_hi], the node's particles for every target of the window and accepts the node only
+ * if the monopole's worst error over the window, |a_mono - a_exact| / |a_t|, is at most eps
+ * (below the band it accepts, above it it opens).  amag = |a| per live particle in tree order.
+ * Outputs: ax/ay/az (n_windows * window; slot k * window + i is target i of window k, 0 past
+ * n_live) and counts (n_windows * 5: node visits, monopole and pair interactions counted as
+ * SHMEM_COUNT_WALK counts them, labelled nodes, particles summed for labels).  No reference
+ * counterpart: measurement of the learned criterion's ceiling. */
+GT_API int gt_mac_ceiling(gt_context* ctx, const gt_tree* tree, const double* amag, double alpha, int window,
+                          int64_t n_windows, const int64_t* windows, int mode, double eps, double rho_lo,
+                          double rho_hi, int mem, double* ax, double* ay, double* az, int64_t* counts);
 /* Train a model on (features, labels) with the pinball loss at quantile tau, Adam, on the GPU.
  * model (host, GT_MAC_MODEL_FLOATS) receives the trained network; loss the final epoch's mean. */
 GT_API int gt_mac_train(gt_context* ctx, int64_t n, const float* features, const float* labels,

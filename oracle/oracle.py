@@ -564,6 +564,14 @@ class ReferenceTree:
                                      _p(ax, _d), _p(ay, _d), _p(az, _d))
         return ax, ay, az
 
+    def accel_brute(self, targets, G=1.0):
+        """shmem::accel_brute (tree.cc:946-971): the FP64 direct sum over the tree's particles."""
+        t = _targets(targets)
+        nt = len(t)
+        ax, ay, az = np.empty(nt), np.empty(nt), np.empty(nt)
+        self.lib.L.ref_accel_brute(self.h, nt, _p(t, _u32), G, _p(ax, _d), _p(ay, _d), _p(az, _d))
+        return ax, ay, az
+
     def accel_grouped_ext(self, targets, theta, G=1.0, batch=0, aold=None, tidal=True, jerk=False):
         """accel_grouped with the tidal tensor ([nt, 6]: xx yy zz xy yz xz, not times G) and the
         jerk ([nt, 3], times G; the tree must have been built with velocities)."""

@@ -131,3 +131,62 @@ def test_what_the_trained_network_gains(gpu_ctx):
     learned = [e for e in entries if e["mac"] == g.GT_MAC_NODE]
     print(f"autotuner: plain best {plain_best:.3f} ms, learned {learned[0]['ms']:.3f} ms "
           f"(p99 {learned[0]['p99']:.3e}); chose mac={opts.get('mac', 0)}")
+
+
+@pytest.mark.gpu
+def test_exact_label_walk_plain_mode_is_the_grouped_walk(gpu_ctx):
+    """gt_mac_ceiling in mode 0 makes the grouped walk's decisions: on whole windows of 32 its node
+    visits and interactions equal the production walk's counts on the same windows and aold, and its
+    FP64 sums match the walk's FP32 ones to the walk parity bar (median 1e-5)."""
+    import gizmo_shared_memory_b200 as g
+    from gizmo_shared_memory_b200 import ics
+
+    P = ics.soneira_peebles(levels=9, seed=21)
+    T = gpu_ctx.build(P)
+    nl = T.info()["n_live"]
+    ob = T.download(nodes=False)["orderbuf"]
+    W = dict(group_mode=g.GT_GROUP_BATCH, batch=32)
+    boot = gpu_ctx.accel_grouped(T, None, theta=0.7, **W)
+    amag = np.sqrt(boot[0] ** 2 + boot[1] ** 2 + boot[2] ** 2)
+    alpha = 0.0025
+    rng = np.random.default_rng(3)
+    wins = np.sort(rng.choice(nl // 32, 300, replace=False))
+    pos = (wins[:, None] * 32 + np.arange(32)[None, :]).ravel()
+    (cx, cy, cz), cnt = gpu_ctx.mac_ceiling(T, amag, alpha, wins, window=32, mode=0)
+    tg = ob[pos]
+    a = gpu_ctx.accel_grouped(T, tg, aold=alpha * amag[pos], count=True, **W)
+    st = gpu_ctx.stats()
+    assert cnt[:, 0].sum() == st["nodes_visited"]
+    assert cnt[:, 1].sum() == st["multipole"]
+    assert cnt[:, 2].sum() == pytest.approx(st["pairs"], rel=1e-5)
+    e = np.sqrt((cx - a[0]) ** 2 + (cy - a[1]) ** 2 + (cz - a[2]) ** 2) / np.sqrt(a[0] ** 2 + a[1] ** 2 + a[2] ** 2)
+    assert np.median(e) <= 1e-5 and np.quantile(e, 0.99) <= 1e-4
+
+
+@pytest.mark.gpu
+def test_exact_label_walk_limits(gpu_ctx):
+    """Mode 1 with eps = 0 over an unbounded band opens every node whose monopole is not exact: the
+    FP64 direct sum to 1e-10.  Raising eps never adds interactions (a node accepted at some eps is
+    accepted at every larger one)."""
+    from gizmo_shared_memory_b200 import ics
+
+    P = ics.plummer(n=4096, seed=5, soft=0.01)
+    T = gpu_ctx.build(P)
+    nl = T.info()["n_live"]
+    ob = T.download(nodes=False)["orderbuf"]
+    W = dict(group_mode=1, batch=32)
+    boot = gpu_ctx.accel_grouped(T, None, theta=0.7, **W)
+    amag = np.sqrt(boot[0] ** 2 + boot[1] ** 2 + boot[2] ** 2)
+    wins = np.arange(0, nl // 32, 7)
+    pos = (wins[:, None] * 32 + np.arange(32)[None, :]).ravel()
+    (cx, cy, cz), cnt = gpu_ctx.mac_ceiling(T, amag, 0.0025, wins, mode=1, eps=0.0, band=(0.0, 1e300))
+    d = gpu_ctx.direct(P, ob[pos], want_phi=False)
+    e = np.sqrt((cx - d[0]) ** 2 + (cy - d[1]) ** 2 + (cz - d[2]) ** 2) / np.sqrt(d[0] ** 2 + d[1] ** 2 + d[2] ** 2)
+    assert e.max() <= 1e-10
+    prev = None
+    for eps in (1e-6, 1e-5, 1e-4, 1e-3, 1e-2):
+        _, c = gpu_ctx.mac_ceiling(T, amag, 0.0025, wins, mode=1, eps=eps, band=(0.0, 1e300))
+        inter = int(c[:, 1].sum() + c[:, 2].sum())
+        if prev is not None:
+            assert inter <= prev
+        prev = inter

@@ -1,0 +1,109 @@
+"""GPU parity at the sizes the throughput metric is quoted on.
+
+The workloads are the 16M clustered box, the 4M isolated galaxy and the 67M merger (generators in
+gizmo_shared_memory_b200/ics.py).  Each is walked as bench.py walks it:
+  * the GPU tree (Peano-Hilbert order, 20-bit cells as shmem::build), a bootstrap walk with
+    Barnes-Hut theta = 0.7 and aold = 0, aold = alpha |a| / G (shmem/mfm.cc:743-751);
+  * then the relative criterion alone, windows of 32 consecutive targets in the GPU's tree order.
+
+The checker is the reference's own shmem::accel_grouped (shmem/tree.cc:626-897), compiled from its
+sources into oracle/_ref (the pinned restatement oracle/gt_oracle.c where that is absent), on its
+own tree of the same particles.  It walks a random sample of whole GPU windows, passed in GPU tree
+order with batch = 32, so its fixed windows (tree.cc:668-670) are exactly the GPU's windows: the
+same group boxes, the same smallest aold, the same nodes offered to the criterion.  Both get the
+same aold.
+
+Bars: median relative error <= 1e-5 (FP32 interaction arithmetic on FP64 group-relative offsets);
+p99 <= 2e-3, for the rare target whose group sees an opening decision flip at the threshold (the
+node moments are summed in a different order).
+"""
+import numpy as np
+import pytest
+
+import gizmo_shared_memory_b200 as g
+from gizmo_shared_memory_b200 import ics
+
+pytestmark = pytest.mark.gpu
+
+MEDIAN_TOL = 1e-5
+P99_TOL = 2e-3
+WINDOW = 32
+
+
+def relerr(a, b):
+    d = np.sqrt(sum((x - y) ** 2 for x, y in zip(a, b)))
+    n = np.sqrt(sum(y ** 2 for y in b))
+    return d / np.where(n > 0, n, 1.0)
+
+
+def checker(P):
+    """The compiled reference when present, else the pinned restatement; a tree of P."""
+    from oracle import Reference, Restatement, reference_available
+
+    if reference_available():
+        R = Reference()
+        R.set_threads(R.max_threads())
+        return "reference", R.build(P)
+    return "restatement", Restatement().build(P)
+
+
+def walk_windows(kind, tree, targets, theta, aold):
+    if kind == "reference":
+        return tree.accel_grouped(targets, theta, 1.0, WINDOW, aold=aold)
+    return tree.accel_grouped(targets, theta, 1.0, WINDOW, aold=aold)[:3]
+
+
+def headline_parity(P, alpha, n_windows, seed):
+    import torch
+
+    ctx = g.Context(0)
+    dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
+    T = ctx.build(dev)
+    nl = T.info()["n_live"]
+    ob = T.download(nodes=False)["orderbuf"]
+    del dev
+    out = tuple(torch.empty(nl, dtype=torch.float64, device="cuda") for _ in range(3))
+    ctx.accel_grouped(T, None, theta=0.7, batch=WINDOW, outs=out + (None,), group_mode=g.GT_GROUP_BATCH)
+    boot = [o.cpu().numpy() for o in out]
+    aold = ctx.form_aold(*out, alpha)
+    ctx.accel_grouped(T, None, aold=aold, theta=0.0, batch=WINDOW, outs=out + (None,),
+                      group_mode=g.GT_GROUP_BATCH)
+    walk = [o.cpu().numpy() for o in out]
+    aold = aold.cpu().numpy()
+    T.free()
+    ctx.close()
+
+    rng = np.random.default_rng(seed)
+    w = np.sort(rng.choice(nl // WINDOW, size=n_windows, replace=False))
+    pos = (w[:, None] * WINDOW + np.arange(WINDOW)[None, :]).ravel()
+    kind, R = checker(P)
+    rb = walk_windows(kind, R, ob[pos], 0.7, None)
+    rw = walk_windows(kind, R, ob[pos], 0.0, aold[pos])
+    eb = relerr([a[pos] for a in boot], rb)
+    ew = relerr([a[pos] for a in walk], rw)
+    return kind, len(pos), eb, ew
+
+
+def report(name, kind, nt, eb, ew):
+    print(f"{name}: {nt} targets in whole windows of {WINDOW}, checker {kind}: "
+          f"bootstrap median {np.median(eb):.2e} p99 {np.quantile(eb, 0.99):.2e}; "
+          f"relative criterion median {np.median(ew):.2e} p99 {np.quantile(ew, 0.99):.2e}")
+    for e in (eb, ew):
+        assert np.isfinite(e).all()
+        assert np.median(e) <= MEDIAN_TOL, np.median(e)
+        assert np.quantile(e, 0.99) <= P99_TOL, np.quantile(e, 0.99)
+
+
+def test_parity_clustered_16m():
+    P = ics.soneira_peebles(seed=3)
+    report("clustered_16m", *headline_parity(P, 0.0025, 384, 11))
+
+
+def test_parity_galaxy_4m():
+    P = ics.galaxy(seed=2)
+    report("galaxy_4m", *headline_parity(P, 0.0025, 384, 12))
+
+
+def test_parity_merger_67m():
+    P = ics.merger(seed=5)
+    report("merger_67m", *headline_parity(P, 0.0025, 256, 13))
