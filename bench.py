@@ -19,9 +19,16 @@ Other workloads: --workload plummer_batch_256 (256 systems in one forest, autotu
 graph), --workload extras_galaxy_4m (the tidal tensor, the jerk, the gas rules and tree reuse on the
 4M galaxy), --workload density_galaxy_4m / density_clustered_16m (the density solve).
 
-Multi-GPU (--gpus N under torchrun): every rank walks its own independent system of the same
-size (seed + rank); there is no data-path collective, only the barrier and a max over ranks of the
-timed region ("scaling": "weak").
+Multi-GPU (--gpus N under torchrun): by default (--split targets) the ranks share one system:
+every rank builds the same tree and walks its window-aligned slice of the tree order
+(gizmo_shared_memory_b200/sharding.py), and ``value`` is the system's particles over the max-over-ranks
+step time ("scaling": "strong").  --split systems walks one independent system per rank (seed +
+rank, "scaling": "weak").  There is no data-path collective in either: only the barrier and the max
+over ranks of the timed region.
+
+--workload activeset_galaxy_4m / activeset_clustered_16m: sparse active sets (one call's latency
+at 0.01-10 % actives, scattered and compact, leaf groups and windows), next to the reference's
+CPU walk on the same targets.
 """
 from __future__ import annotations
 
@@ -285,7 +292,10 @@ def workload_config(args, n):
             "criterion": f"plain relative criterion alpha={alpha} after a theta=0.7 bootstrap walk",
             "mac": "plain", "grouping": grouping_of(args)[1],
             "l2": (f"inputs larger than L2: {n * 32 / 2**20:.0f} MiB of particles per walk" if n * 32 > 126 * 2**20
-                   else f"{n * 32 / 2**20:.0f} MiB of particles per walk: fits in L2")}
+                   else f"{n * 32 / 2**20:.0f} MiB of particles per walk: fits in L2"),
+            "parallelism": (f"{args.gpus} GPUs: one system, targets split by tree-order slice"
+                            if args.split == "targets" else f"{args.gpus} GPUs: one system per GPU")
+            if args.gpus > 1 else "1 GPU"}
 
 
 def run_reference_arm(args):
@@ -469,7 +479,11 @@ def run_gpu_arm(args):
     wopts = dict(group_mode=group_mode, group_max=args.group_max,
                  batch=args.group_max if args.group == "batch" else 0)
 
-    P = make_workload(args.workload, seed_offset=rank)
+    # --split targets (N > 1): one system, every rank builds the same tree and walks its
+    # window-aligned slice of the tree order (sharding.walk_shard); --split systems: one
+    # independent system per rank
+    split = world > 1 and args.split == "targets"
+    P = make_workload(args.workload, seed_offset=0 if split else rank)
     n = len(P["m"])
     dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
     ctx = g.Context(local, torch_stream=True)
@@ -484,13 +498,35 @@ def run_gpu_arm(args):
     # bootstrap walk (theta = 0.7, aold = 0), then aold = alpha |a| / G
     ctx.accel_grouped(T, None, theta=0.7, outs=out + (None,), **wopts)
     aold = ctx.form_aold(*out, alpha)
-    # counted walk: interactions as the reference counts them (SHMEM_COUNT_WALK)
-    ctx.accel_grouped(T, None, aold=aold, theta=0.0, outs=out + (None,), count=True, **wopts)
-    st = ctx.stats()
-    inter = st["multipole"] + st["pairs"]
+    if split:
+        from gizmo_shared_memory_b200.sharding import shard_ranges, walk_shard
 
-    def step():
-        ctx.accel_grouped(T, None, aold=aold, theta=0.0, outs=out + (None,), async_=True, **wopts)
+        ob_dev = torch.as_tensor(T.download(nodes=False)["orderbuf"].view(np.int32), device="cuda")
+        sa, sb = shard_ranges(nl, world, args.group_max)[rank]
+        out_s = tuple(torch.empty(max(sb - sa, 1), dtype=torch.float64, device="cuda") for _ in range(3))
+
+        def shard_walk(**kw):
+            walk = lambda tg, ao: ctx.accel_grouped(T, tg, aold=ao, theta=0.0, outs=out_s + (None,), **wopts, **kw)
+            return walk_shard(walk, ob_dev, aold, rank, world, args.group_max)
+
+        # counted walk: interactions as the reference counts them (SHMEM_COUNT_WALK)
+        shard_walk(count=True)
+        st = ctx.stats()
+
+        def step():
+            shard_walk(async_=True)
+    else:
+        ctx.accel_grouped(T, None, aold=aold, theta=0.0, outs=out + (None,), count=True, **wopts)
+        st = ctx.stats()
+
+        def step():
+            ctx.accel_grouped(T, None, aold=aold, theta=0.0, outs=out + (None,), async_=True, **wopts)
+    inter_rank = st["multipole"] + st["pairs"]
+    inter = inter_rank
+    if dist:
+        it = torch.tensor([inter_rank], device="cuda", dtype=torch.float64)
+        dist.all_reduce(it)
+        inter = float(it[0])
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -523,7 +559,8 @@ def run_gpu_arm(args):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_total, t_kernel = float(tt[0]), float(tt[1])
     t_step = t_total / args.steps
-    value = nl * world / t_step
+    jobs = 1 if split else world  # systems walked per step, all ranks together
+    value = nl * jobs / t_step
 
     # accuracy: FP64 direct sum on a seeded 4096-particle sample
     sample = error_sample(n, rank)
@@ -535,8 +572,8 @@ def run_gpu_arm(args):
 
     # the learned criterion at the same sampled p99 (the metric's comparison)
     learned = None
-    if not args.no_learned:
-        learned = learned_at_equal_p99(args, ctx, g, T, aold, wopts, sample, dref, err_p99, nl, world, dist)
+    if not args.no_learned and world == 1:
+        learned = learned_at_equal_p99(args, ctx, g, T, aold, wopts, sample, dref, err_p99, nl, jobs, dist)
 
     # end to end through the C ABI with host buffers (pinned), build + walk every step
     e2e = None
@@ -548,12 +585,20 @@ def run_gpu_arm(args):
         aold_h = aold_h.numpy()
         ho = [torch.empty(nl, dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
         hctx = g.Context(local)
+        if split:
+            ob_h = T.download(nodes=False)["orderbuf"]
+            sh = [o[sa:sb] for o in ho]
         ttimes = []
         for it in range(args.warmup + args.steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             T2 = hctx.build(pin, key_mode=key_mode)
-            hctx.accel_grouped(T2, None, aold=aold_h, theta=0.0, outs=tuple(ho) + (None,), **wopts)
+            if split:
+                # this rank's slice, host arrays in and out
+                walk_shard(lambda tg, ao: hctx.accel_grouped(T2, tg, aold=ao, theta=0.0, outs=tuple(sh) + (None,),
+                                                             **wopts), ob_h, aold_h, rank, world, args.group_max)
+            else:
+                hctx.accel_grouped(T2, None, aold=aold_h, theta=0.0, outs=tuple(ho) + (None,), **wopts)
             t1 = time.perf_counter()
             T2.free()
             if it >= args.warmup:
@@ -563,9 +608,10 @@ def run_gpu_arm(args):
             tt = torch.tensor([te], device="cuda", dtype=torch.float64)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             te = float(tt[0])
-        e2e = {"value": nl * world / te, "unit": "particles/s", "ms_per_step": 1e3 * te,
+        nw = (sb - sa) if split else nl  # targets this rank walks
+        e2e = {"value": nl * jobs / te, "unit": "particles/s", "ms_per_step": 1e3 * te,
                "ms_per_step_median": 1e3 * float(np.median(ttimes)), "ms_per_step_max": 1e3 * float(np.max(ttimes)),
-               "h2d_bytes_per_step": int(5 * 8 * n + 8 * nl), "d2h_bytes_per_step": int(3 * 8 * nl),
+               "h2d_bytes_per_step": int(5 * 8 * n + 8 * nw), "d2h_bytes_per_step": int(3 * 8 * nw),
                "includes": "H2D of x,y,z,m,soft,aold from pinned memory + tree build + walk + D2H of ax,ay,az"}
         hctx.close()
 
@@ -593,13 +639,13 @@ def run_gpu_arm(args):
         if args.group == "batch":
             parity = window_parity(cpu, Tc, ob_gpu, aold_tree, full, args.group_max, n_windows=256)
 
-    achieved = FLOPS_PER_INTERACTION * inter / t_kernel / 1e12
+    achieved = FLOPS_PER_INTERACTION * inter_rank / t_kernel / 1e12  # this GPU's walk kernel
     if learned and "value" in learned:
         learned["speedup_vs_plain"] = learned["value"] / value
     line = {
         "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_step,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": True, "scaling": "strong" if split else "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded; see config.description)",
         "config": workload_config(args, n),
         "precision": "FP64 positions and group-relative offsets, FP32 interactions; FP32 partial sums "
@@ -618,8 +664,8 @@ def run_gpu_arm(args):
         "gpu_launches": launches,
         "clocks": clocks,
         "error": {"vs": "FP64 direct sum", "sample": int(len(sample)), "median": err_med, "p99": err_p99},
-        "interactions_per_particle": inter / nl,
-        "interactions_per_s": inter * world / t_step,
+        "interactions_per_particle": inter / (nl * jobs),
+        "interactions_per_s": inter / t_step,
         "walk_stats": {k: st[k] for k in ("groups", "nodes_visited", "multipole", "pairs", "max_stack")},
         "build_ms": info["build_ms"],
         "build_ms_first_call": build_cold,
@@ -998,6 +1044,113 @@ def run_density_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def run_activeset_arm(args):
+    """Sparse active sets: the engine's deep-timebin steps, where only a scattered fraction of the
+    particles needs a force (shmem/bench_activeset.cc:1-16; compute_gravity hands the walk the
+    active targets in tree order, shmem/mfm.cc:698-732).  For each active fraction, scattered
+    (random particles) and compact (one run of the tree order), and for leaf groups (batch 0, the
+    engine's grouping) and windows of 32, this times one call:
+      * device: targets, aold and outputs resident on the device (CUDA events, median of steps);
+      * host: the same call through the C ABI with host arrays (wall clock, copies included);
+      * cpu: the reference's own accel_grouped on the same targets and aold (every host thread).
+    Also the parity of the GPU walk with the reference's on the scattered 1 % subset."""
+    import torch
+
+    import gizmo_shared_memory_b200 as g
+
+    torch.cuda.set_device(0)
+    wl = args.workload.replace("activeset_", "")
+    cfg = WORKLOADS[wl]
+    alpha = args.alpha if args.alpha is not None else cfg["alpha"]
+    P = make_workload(wl)
+    n = len(P["m"])
+    dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
+    ctx = g.Context(0, torch_stream=True)
+    T = ctx.build(dev)
+    nl = T.info()["n_live"]
+    ob = T.download(nodes=False)["orderbuf"]
+    out = tuple(torch.empty(nl, dtype=torch.float64, device="cuda") for _ in range(3))
+    ctx.accel_grouped(T, None, theta=0.7, outs=out + (None,), group_mode=g.GT_GROUP_BATCH, batch=32)
+    aold_tree = ctx.form_aold(*out, alpha).cpu().numpy()
+    aold_p = np.zeros(n)
+    aold_p[ob] = aold_tree
+    cpu = None if args.no_cpu else CpuReference()
+    Tc = cpu.build(P)[0] if cpu else None
+    rng = np.random.default_rng(41)
+    stream = torch.cuda.current_stream()
+    rows = []
+    parity = None
+    sampler = ClockSampler(0)
+    sampler.start()
+    l0 = ctx.launches()
+    for frac in (1e-4, 1e-3, 1e-2, 1e-1):
+        k = max(1, int(round(frac * nl)))
+        for layout in ("scattered", "compact"):
+            if layout == "scattered":
+                pos = np.sort(rng.choice(nl, size=k, replace=False))
+            else:
+                s0 = int(rng.integers(0, nl - k + 1))
+                pos = np.arange(s0, s0 + k)
+            tg = ob[pos].astype(np.uint32)
+            ao = aold_tree[pos]
+            tg_d = torch.as_tensor(tg.view(np.int32), device="cuda")
+            ao_d = torch.as_tensor(ao, device="cuda")
+            o_d = tuple(torch.empty(k, dtype=torch.float64, device="cuda") for _ in range(3))
+            for grouping, kw in (("leaf", dict(group_mode=g.GT_GROUP_LEAF, batch=0)),
+                                 ("window32", dict(group_mode=g.GT_GROUP_BATCH, batch=32))):
+                ctx.accel_grouped(T, tg_d, aold=ao_d, outs=o_d + (None,), count=True, **kw)
+                st = ctx.stats()
+                for _ in range(3):
+                    ctx.accel_grouped(T, tg_d, aold=ao_d, outs=o_d + (None,), async_=True, **kw)
+                torch.cuda.synchronize()
+                dts = []
+                for _ in range(max(args.steps, 5)):
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    ctx.accel_grouped(T, tg_d, aold=ao_d, outs=o_d + (None,), async_=True, **kw)
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    dts.append(e0.elapsed_time(e1))
+                hts = []
+                for _ in range(max(args.steps, 5)):
+                    t0 = time.perf_counter()
+                    res = ctx.accel_grouped(T, tg, aold=ao, **kw)
+                    hts.append(1e3 * (time.perf_counter() - t0))
+                row = {"fraction": frac, "targets": k, "layout": layout, "grouping": grouping,
+                       "groups": st["groups"], "device_ms": float(np.median(dts)),
+                       "host_ms": float(np.median(hts)),
+                       "interactions_per_target": (st["multipole"] + st["pairs"]) / k}
+                if cpu:
+                    b = 0 if grouping == "leaf" else 32
+                    cts = []
+                    for _ in range(3):
+                        t0 = time.perf_counter()
+                        r = cpu.walk(Tc, tg, ao, batch=b)
+                        cts.append(1e3 * (time.perf_counter() - t0))
+                    row["cpu_ms"] = float(min(cts))
+                    row["cpu_cores"] = cpu.cores
+                    if frac == 1e-2 and layout == "scattered":
+                        e = relerr(res, r)
+                        pr = {"targets": k, "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99))}
+                        parity = dict(parity or {}, **{grouping: pr})
+                rows.append(row)
+                log(json.dumps(row))
+    launches = ctx.launches() - l0
+    clocks = sampler.stop()
+    head = [r for r in rows if r["fraction"] == 1e-3 and r["layout"] == "scattered" and r["grouping"] == "leaf"][0]
+    line = {"metric": "active-set walk latency (one call)", "value": head["device_ms"], "unit": "ms",
+            "n_gpus": 1, "steps": args.steps, "warmup": 3, "ms_per_step": head["device_ms"],
+            "higher_is_better": False, "scaling": "none", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded; see config.description)",
+            "config": {"workload": args.workload, "description": cfg["desc"], "n": n,
+                       "criterion": f"plain relative criterion alpha={alpha}",
+                       "headline": "0.1 % scattered actives, leaf groups"},
+            "rows": rows, "parity": parity, "gpu_launches": launches, "clocks": clocks,
+            "e2e": {"value": head["host_ms"], "unit": "ms", "h2d_bytes_per_step": head["targets"] * 12,
+                    "d2h_bytes_per_step": head["targets"] * 24}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -1005,7 +1158,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["plummer_batch_256", "extras_galaxy_4m"] +
-                    ["density_" + w for w in ("galaxy_4m", "clustered_16m")], default="clustered_16m",
+                    ["density_" + w for w in ("galaxy_4m", "clustered_16m")] +
+                    ["activeset_" + w for w in ("galaxy_4m", "clustered_16m")], default="clustered_16m",
                     help="plummer_batch_256: the batched many-system case (forest + autotuner + graph); "
                          "density_*: the density solve on that workload")
     ap.add_argument("--alpha", type=float, default=None)
@@ -1014,6 +1168,9 @@ def main():
                          "targets in tree order (accel_grouped batch > 0); node: tree nodes of at "
                          "most --group-max particles")
     ap.add_argument("--group-max", type=int, default=32)
+    ap.add_argument("--split", choices=["targets", "systems"], default="targets",
+                    help="N > 1: targets = one system, every rank walks a window-aligned slice of its "
+                         "tree order; systems = one independent system per rank")
     ap.add_argument("--key", choices=["peano", "morton"], default="peano",
                     help="sort key of the tree: the window order of --group batch")
     ap.add_argument("--sample-seconds", type=float, default=8.0)
@@ -1028,6 +1185,8 @@ def main():
         run_reference_arm(args)
     elif args.workload == "plummer_batch_256":
         run_batch_arm(args)
+    elif args.workload.startswith("activeset_"):
+        run_activeset_arm(args)
     elif args.workload.startswith("density_"):
         run_density_arm(args)
     elif args.workload == "extras_galaxy_4m":

@@ -184,7 +184,7 @@ def load_library(path: str = LIB_PATH):
     L.gt_mac_train_options_default.argtypes = [C.POINTER(MacTrainOptions)]
     L.gt_mac_sample.argtypes = [vp, vp, vp, d, C.c_int, i64, d, d, i64, C.c_int, vp, vp, vp,
                                 C.POINTER(i64)]
-    L.gt_mac_ceiling.argtypes = [vp, vp, vp, d, C.c_int, i64, vp, C.c_int, d, d, d, C.c_int, vp, vp, vp, vp]
+    L.gt_mac_ceiling.argtypes = [vp, vp, vp, d, C.c_int, i64, vp, C.c_int, d, d, d, d, C.c_int, vp, vp, vp, vp]
     L.gt_mac_train.argtypes = [vp, i64, vp, vp, C.POINTER(MacTrainOptions), C.c_int, vp, C.POINTER(d)]
     L.gt_mac_predict.argtypes = [vp, vp, i64, vp, C.c_int, vp]
     L.gt_mac_gradient.argtypes = [vp, vp, i64, vp, vp, d, C.c_int, vp, C.POINTER(d)]
@@ -479,7 +479,8 @@ class Context:
         k = min(ns.value, capacity)
         return f[:k], lab[:k], rho[:k], ns.value
 
-    def mac_ceiling(self, tree: "Tree", amag, alpha, windows, window=32, mode=0, eps=0.0, band=(0.0, 0.0)):
+    def mac_ceiling(self, tree: "Tree", amag, alpha, windows, window=32, mode=0, eps=0.0, band=(0.0, 0.0),
+                    cost_exp=0.0):
         """The exact-label walk (gt_mac_ceiling) over the given window indices; amag = |a| per live
         particle in tree order.  Returns ((ax, ay, az), counts) with counts [n_windows, 5]: node
         visits, monopole and pair interactions, labelled nodes, particles summed for labels."""
@@ -489,7 +490,7 @@ class Context:
         ax, ay, az = np.empty(ns), np.empty(ns), np.empty(ns)
         cnt = np.empty((max(len(w), 1), 5), np.int64)
         self._check(load_library().gt_mac_ceiling(self.h, tree.h, _ptr(amag), alpha, window, len(w), _ptr(w),
-                                                  mode, eps, band[0], band[1], GT_MEM_HOST, _ptr(ax), _ptr(ay),
+                                                  mode, eps, cost_exp, band[0], band[1], GT_MEM_HOST, _ptr(ax), _ptr(ay),
                                                   _ptr(az), _ptr(cnt)))
         k = len(w) * window
         return (ax[:k], ay[:k], az[:k]), cnt[:len(w)]

@@ -1237,8 +1237,9 @@ int gt_mac_sample(gt_context* ctx, const gt_tree* tree, const double* amag, doub
 }
 
 int gt_mac_ceiling(gt_context* ctx, const gt_tree* tree, const double* amag, double alpha, int window,
-                   int64_t n_windows, const int64_t* windows, int mode, double eps, double rho_lo,
-                   double rho_hi, int mem, double* ax, double* ay, double* az, int64_t* counts) {
+                   int64_t n_windows, const int64_t* windows, int mode, double eps, double cost_exp,
+                   double rho_lo, double rho_hi, int mem, double* ax, double* ay, double* az,
+                   int64_t* counts) {
     if (!ctx) return GT_ERR_INVALID;
     return guarded(ctx, [&] {
         check_mem(mem);
@@ -1246,7 +1247,8 @@ int gt_mac_ceiling(gt_context* ctx, const gt_tree* tree, const double* amag, dou
             throw Fail{GT_ERR_INVALID, "bad arguments"};
         if (window < 1 || window > 32) throw Fail{GT_ERR_INVALID, "window must be in [1, 32]"};
         if (mode != 0 && mode != 1) throw Fail{GT_ERR_INVALID, "mode must be 0 (plain) or 1 (exact labels)"};
-        if (!(alpha > 0) || !(eps >= 0) || !(rho_hi >= rho_lo)) throw Fail{GT_ERR_INVALID, "bad alpha, eps or band"};
+        if (!(alpha > 0) || !(eps >= 0) || !(rho_hi >= rho_lo) || !(cost_exp >= 0.0 && cost_exp <= 4.0))
+            throw Fail{GT_ERR_INVALID, "bad alpha, eps, cost exponent or band"};
         if (tree->n_systems > 1) throw Fail{GT_ERR_UNSUPPORTED, "gt_mac_ceiling takes a single-system tree"};
         if (n_windows > (int64_t)INT32_MAX / 32) throw Fail{GT_ERR_INVALID, "too many windows"};
         const int64_t nwin_all = (tree->n_live + window - 1) / window;
@@ -1261,7 +1263,7 @@ int gt_mac_ceiling(gt_context* ctx, const gt_tree* tree, const double* amag, dou
         double* oy = out_buf(ctx, kSlotOut1, ay, ns, mem);
         double* oz = out_buf(ctx, kSlotOut2, az, ns, mem);
         int64_t* oc = out_buf(ctx, kSlotOut3, counts, n_windows * 5, mem);
-        run_mac_ceiling(ctx, tree, da, alpha, window, n_windows, dw, mode, eps, rho_lo, rho_hi, ox, oy, oz,
+        run_mac_ceiling(ctx, tree, da, alpha, window, n_windows, dw, mode, eps, cost_exp, rho_lo, rho_hi, ox, oy, oz,
                         (unsigned long long*)oc);
         copy_out(ctx, ax, (const double*)ox, ns, mem);
         copy_out(ctx, ay, (const double*)oy, ns, mem);

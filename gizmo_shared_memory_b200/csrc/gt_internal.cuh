@@ -190,6 +190,7 @@ enum Slot {
     kSlotStack, kSlotCounters, kSlotDirect, kSlotGroupRoot, kSlotMacL2,
     kSlotNgb0, kSlotNgb1, kSlotNgb2,
     kSlotStack2,  // traversal stacks of the second compute stream (chunked walks)
+    kSlotGroupCount,  // device-side group and chunk counts of an explicit-target walk
     kSlotCount
 };
 
@@ -307,8 +308,8 @@ void run_mac_sample(gt_context* ctx, const gt_tree* t, const double* amag, doubl
                     int64_t stride, double rho_lo, double rho_hi, int64_t cap, float* feat,
                     float* label, float* rho, int64_t* n_samples);
 void run_mac_ceiling(gt_context* ctx, const gt_tree* t, const double* amag, double alpha, int window,
-                     int64_t n_win, const int64_t* wins, int mode, double eps, double rho_lo, double rho_hi,
-                     double* ax, double* ay, double* az, unsigned long long* counts);
+                     int64_t n_win, const int64_t* wins, int mode, double eps, double cost_exp, double rho_lo,
+                     double rho_hi, double* ax, double* ay, double* az, unsigned long long* counts);
 void run_mac_train(gt_context* ctx, int64_t n, const float* X, const float* Y,
                    const gt_mac_train_options& o, float* model_host, double* loss);
 void run_mac_grad(gt_context* ctx, const float* dmodel, const float* X, const float* Y, const int* perm,

@@ -213,8 +213,11 @@ __global__ void __launch_bounds__(256) mac_sample_kernel(const SampleArgs A) {
 //   mode 0: the plain relative criterion, M L^2 <= r^4 alpha min|a| (shmem/tree.h:134-135), or
 //   mode 1: exact labels -- inside the band rho_lo < rho <= rho_hi the warp sums the node's
 //           particles for every target of the window and accepts the node only when the monopole's
-//           worst error over the window, |a_mono - a_exact|_t / |a_t|, is at most eps; below the
-//           band it accepts, above it it opens.
+//           worst error over the window, |a_mono - a_exact|_t / |a_t|, is at most
+//           eps * ((c - 1) / 7)^cost_exp, c the interactions opening it costs one step ahead (its
+//           children, or a leaf's particles; c - 1 floored at 1); below the band it accepts, above
+//           it it opens.  cost_exp = 0 is a constant threshold; cost_exp > 0 spends more of the
+//           error budget where opening is dearer.
 // Both modes share the softening-overlap and inside-node arms.  Mode 1 is the rule a learned
 // criterion that predicted every (window, node) error exactly would apply, so its interactions and
 // node visits at a given force error bound what any learned acceptance rule over the monopole walk
@@ -227,7 +230,7 @@ struct CeilArgs {
     int n_win, window;
     int64_t n_live;
     const double* amag;   // |a| per live particle in tree order
-    double alpha, eps, rho_lo, rho_hi;
+    double alpha, eps, cost_exp, rho_lo, rho_hi;
     int mode;
     int* stack;
     int stack_cap;
@@ -340,7 +343,12 @@ __global__ void __launch_bounds__(256) ceiling_kernel(const CeilArgs A) {
                 const double ddx = mdx * mf - ex, ddy = mdy * mf - ey, ddz = mdz * mf - ez;
                 const double e = tv ? (inv_a > 0.0 ? sqrt(ddx * ddx + ddy * ddy + ddz * ddz) * inv_a : 1e300) : 0.0;
                 const double worst = wmax(e);
-                if (lane == l) open = worst > A.eps;
+                if (lane == l) {
+                    const int cost = nd.first < 0 ? nd.phi - nd.plo : nd.nchild;
+                    const double thr = A.cost_exp == 0.0 ? A.eps
+                                                         : A.eps * pow(fmax((double)(cost - 1), 1.0) / 7.0, A.cost_exp);
+                    open = worst > thr;
+                }
                 if (lane == 0) { ++c_lab; c_labsum += (unsigned long long)(phi - plo); }
             }
             const bool leaf = nd.first < 0;
@@ -573,8 +581,8 @@ void init_params(float* model, uint64_t seed, float bias_out) {
 }  // namespace
 
 void run_mac_ceiling(gt_context* ctx, const gt_tree* t, const double* amag, double alpha, int window,
-                     int64_t n_win, const int64_t* wins, int mode, double eps, double rho_lo, double rho_hi,
-                     double* ax, double* ay, double* az, unsigned long long* counts) {
+                     int64_t n_win, const int64_t* wins, int mode, double eps, double cost_exp, double rho_lo,
+                     double rho_hi, double* ax, double* ay, double* az, unsigned long long* counts) {
     cudaStream_t st = ctx->stream;
     if (n_win <= 0) return;
     const int warps = 8;
@@ -583,7 +591,7 @@ void run_mac_ceiling(gt_context* ctx, const gt_tree* t, const double* amag, doub
     CeilArgs a;
     a.nodes = t->nodes; a.src = t->src; a.ssoft = t->ssoft;
     a.wins = wins; a.n_win = (int)n_win; a.window = window; a.n_live = t->n_live;
-    a.amag = amag; a.alpha = alpha; a.eps = eps; a.rho_lo = rho_lo; a.rho_hi = rho_hi; a.mode = mode;
+    a.amag = amag; a.alpha = alpha; a.eps = eps; a.cost_exp = cost_exp; a.rho_lo = rho_lo; a.rho_hi = rho_hi; a.mode = mode;
     a.stack = (int*)scratch(ctx, kSlotStack, (size_t)blocks * warps * stack_cap * 4);
     a.stack_cap = stack_cap;
     unsigned long long* ctr = (unsigned long long*)scratch(ctx, kSlotCounters, 256);

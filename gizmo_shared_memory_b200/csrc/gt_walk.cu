@@ -47,6 +47,7 @@ struct WalkArgs {
     const double* aold;         // per target; null: 0 everywhere
     const int2* groups;         // [start, end) in target index space
     int n_groups;
+    const uint32_t* n_groups_dev;  // non-null: the group count, on the device (overrides n_groups)
     double theta2, G;
     double *ax, *ay, *az, *phi;
     const uint32_t* out_map;    // null: write at the target index
@@ -295,12 +296,13 @@ walk_kernel(const WalkArgs A) {
 
     unsigned long long c_nodes = 0, c_multi = 0, c_pairs = 0, c_zero = 0, c_flush = 0, c_steps = 0;
     int c_maxtop = 0;
+    const int n_groups = A.n_groups_dev ? (int)*A.n_groups_dev : A.n_groups;
 
     for (;;) {
         int g = 0;
         if (lane == 0) g = (int)atomicAdd(A.next_group, 1u);
         g = __shfl_sync(kFull, g, 0);
-        if (g >= A.n_groups) break;
+        if (g >= n_groups) break;
         const int2 gr = A.groups[g];
         const int t0 = gr.x, nt = gr.y - gr.x;
         const int nk = TPL > 1 ? min(TPL, (nt + 31) >> 5) : 1;  // targets per lane in use (warp-uniform)
@@ -951,7 +953,9 @@ __global__ void chunk_emit_kernel(const int64_t* __restrict__ starts, int64_t ng
 // Forest: the root of each group is the root of the system of its first target (roots are
 // nodes 0 .. n_systems-1, groups never span two systems).
 __global__ void group_root_kernel(const int2* __restrict__ groups, int64_t ng, const uint32_t* __restrict__ tpos,
-                                  const int* __restrict__ sys_off, int n_systems, int* __restrict__ root) {
+                                  const int* __restrict__ sys_off, int n_systems, int* __restrict__ root,
+                                  const uint32_t* __restrict__ ng_dev = nullptr) {
+    if (ng_dev) ng = min(ng, (int64_t)*ng_dev);
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ng;
          g += (int64_t)gridDim.x * blockDim.x) {
         const int t0 = groups[g].x;
@@ -1003,6 +1007,54 @@ int64_t finish_groups(gt_context* ctx, const uint32_t* flag, int64_t n, int kmax
     check_launch(ctx, "chunk_emit_kernel");
     *out = groups;
     return nc;
+}
+
+// The same chunking with the group count on the device (gc[0]): no host read-back.  Threads past
+// the count write no chunks.
+__global__ void chunk_count_dev_kernel(const int64_t* __restrict__ starts, const uint32_t* __restrict__ gc,
+                                       int64_t cap, int64_t n_end, int kmax, uint32_t* __restrict__ nchunk) {
+    const int64_t ng = min(cap, (int64_t)gc[0]);
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < cap;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        if (g >= ng) { nchunk[g] = 0; continue; }
+        const int64_t s = starts[g], e = (g + 1 < ng) ? starts[g + 1] : n_end;
+        nchunk[g] = (uint32_t)((e - s + kmax - 1) / kmax);
+    }
+}
+
+__global__ void chunk_emit_dev_kernel(const int64_t* __restrict__ starts, const uint32_t* __restrict__ gc,
+                                      int64_t cap, int64_t n_end, int kmax, const uint32_t* __restrict__ coff,
+                                      int2* __restrict__ groups) {
+    const int64_t ng = min(cap, (int64_t)gc[0]);
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ng;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = starts[g], e = (g + 1 < ng) ? starts[g + 1] : n_end;
+        int64_t o = coff[g];
+        for (int64_t a = s; a < e; a += kmax, ++o) groups[o] = make_int2((int)a, (int)std::min<int64_t>(a + kmax, e));
+    }
+}
+
+// Group starts (flag over n items) to chunked [start, end) pairs without a host read-back: the
+// number of chunks stays on the device (*count_dev), at most n.  For explicit target lists, where
+// a read-back per call is most of the cost of a small walk.
+int2* finish_groups_dev(gt_context* ctx, const uint32_t* flag, int64_t n, int kmax, const uint32_t** count_dev) {
+    cudaStream_t st = ctx->stream;
+    uint32_t* gc = (uint32_t*)scratch(ctx, kSlotGroupCount, 64);  // [0] groups, [1] chunks
+    uint32_t* pos = (uint32_t*)scratch(ctx, kSlotScanA, (size_t)n * 4);
+    scan_exclusive_u32(ctx, flag, pos, n, gc);
+    int64_t* starts = (int64_t*)scratch(ctx, kSlotGroupsA, (size_t)(n + 1) * 8);
+    compact_starts_kernel<<<grid1d(ctx, n), 256, 0, st>>>(flag, pos, n, starts);
+    check_launch(ctx, "compact_starts_kernel");
+    uint32_t* nchunk = (uint32_t*)scratch(ctx, kSlotNodeTmp1, (size_t)n * 4);
+    uint32_t* coff = (uint32_t*)scratch(ctx, kSlotNodeTmp2, (size_t)n * 4);
+    chunk_count_dev_kernel<<<grid1d(ctx, n), 256, 0, st>>>(starts, gc, n, n, kmax, nchunk);
+    check_launch(ctx, "chunk_count_dev_kernel");
+    scan_exclusive_u32(ctx, nchunk, coff, n, gc + 1);
+    int2* groups = (int2*)scratch(ctx, kSlotGroupsB, (size_t)n * sizeof(int2));
+    chunk_emit_dev_kernel<<<grid1d(ctx, n), 256, 0, st>>>(starts, gc, n, n, kmax, coff, groups);
+    check_launch(ctx, "chunk_emit_dev_kernel");
+    *count_dev = gc + 1;
+    return groups;
 }
 
 size_t walk_smem(int warps, bool mac, int pn_cap, int ext = 0) {
@@ -1096,8 +1148,9 @@ constexpr ChunkEdges kChunkEdge{{0, 10, 45, 80, 93, 100}};
 // whose first target is at or after nt * edges.pct[c] / 100.  out: kChunks+1 pairs (group index,
 // first target).
 __global__ void chunk_bounds_kernel(const int2* __restrict__ groups, int ng, int nt, ChunkEdges edges,
-                                    int2* __restrict__ out) {
+                                    int2* __restrict__ out, const uint32_t* __restrict__ ng_dev) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    if (ng_dev) ng = min(ng, (int)*ng_dev);
     for (int c = 0; c <= kChunks; ++c) {
         const int64_t want = (int64_t)nt * edges.pct[c] / 100;
         int lo = 0, hi = ng;  // first g with groups[g].x >= want
@@ -1157,6 +1210,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     int* roots = nullptr;
     int64_t ng = 0;
     const uint32_t* tpos = nullptr;
+    const uint32_t* ng_dev = nullptr;  // explicit targets: the group count stays on the device
     if (all) {
         // the cache is shared by every context that walks this tree: look up and fill it under
         // the tree's lock, and publish a new list only once it is complete on the device
@@ -1233,12 +1287,15 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                                                              t->leaf_of, gid, tp, flag, t->sys_off_dev,
                                                              t->n_systems, 0);
         check_launch(ctx, "target_flags_kernel");
-        ng = finish_groups(ctx, flag, nt, kmax, &groups, false);
+        // every chunk holds at least one target: nt bounds the count, which the walk reads on the
+        // device, so the call needs no read-back before the walk
+        groups = finish_groups_dev(ctx, flag, nt, kmax, &ng_dev);
+        ng = nt;
         tpos = tp;
-        if (t->n_systems > 1 && ng > 0) {
+        if (t->n_systems > 1) {
             roots = (int*)scratch(ctx, kSlotGroupRoot, (size_t)ng * sizeof(int));
             group_root_kernel<<<grid1d(ctx, ng), 256, 0, st>>>(groups, ng, tpos, t->sys_off_dev, t->n_systems,
-                                                               roots);
+                                                               roots, ng_dev);
             check_launch(ctx, "group_root_kernel");
         }
     }
@@ -1288,6 +1345,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     a.aold = rq.aold;
     a.groups = groups;
     a.n_groups = (int)ng;
+    a.n_groups_dev = ng_dev;
     a.theta2 = rq.theta * rq.theta;
     a.G = rq.G;
     a.ax = rq.want_acc ? rq.ax : nullptr;
@@ -1368,7 +1426,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         ensure_copy_stream(ctx);
         int2* bounds = (int2*)(ctr + 16);  // K+1 int2 after the counters
         check_cuda(cudaMemsetAsync(ctr, 0, 256, st), "memset counters");
-        chunk_bounds_kernel<<<1, 1, 0, st>>>(groups, (int)ng, (int)nt, kChunkEdge, bounds);
+        chunk_bounds_kernel<<<1, 1, 0, st>>>(groups, (int)ng, (int)nt, kChunkEdge, bounds, ng_dev);
         check_launch(ctx, "chunk_bounds_kernel");
         int2 hb[kChunks + 1];
         check_cuda(cudaMemcpyAsync(ctx->pinned, bounds, sizeof(hb), cudaMemcpyDeviceToHost, st), "d2h");
@@ -1425,6 +1483,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                 ac.stack = stacks[c & 1];
                 ac.groups = groups + g0;
                 ac.n_groups = g1 - g0;
+                ac.n_groups_dev = nullptr;
                 ac.group_root = roots ? roots + g0 : nullptr;
                 ac.next_group = (unsigned int*)(ctr + 10) + c;
                 const int cb = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, ((int64_t)(g1 - g0) + warps - 1) / warps));
@@ -1479,6 +1538,11 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         unsigned long long h[10];
         std::memcpy(h, ctx->pinned, 80);
         if ((int)h[9] == 0) {
+            if (ng_dev) {
+                uint32_t hg = 0;
+                check_cuda(cudaMemcpy(&hg, ng_dev, 4, cudaMemcpyDeviceToHost), "group count d2h");
+                ctx->stats.groups = hg;
+            }
             ctx->stats.nodes_visited = (int64_t)h[0];
             ctx->stats.multipole = (int64_t)h[1];
             ctx->stats.pairs = (int64_t)h[2] - (int64_t)h[3];

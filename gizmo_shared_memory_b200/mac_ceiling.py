@@ -68,12 +68,14 @@ def main(argv=None):
     ap.add_argument("--alphas", default="0.001,0.0015,0.0025,0.0035,0.005,0.007,0.01,0.014")
     ap.add_argument("--eps", default="3e-5,1e-4,2e-4,4e-4,7e-4,1e-3,1.5e-3,2.5e-3,4e-3,7e-3")
     ap.add_argument("--band", default="0.001,1000", help="rho band of the exact labels")
+    ap.add_argument("--cost-exp", default="0", help="exponents of the cost-aware threshold to sweep")
     ap.add_argument("--alpha", type=float, default=0.0025, help="the headline plain criterion")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
     alphas = [float(a) for a in args.alphas.split(",")]
     epss = [float(e) for e in args.eps.split(",")]
+    cexps = [float(c) for c in args.cost_exp.split(",")]
     band = tuple(float(b) for b in args.band.split(","))
 
     P = make(args.workload)
@@ -125,10 +127,14 @@ def main(argv=None):
                      "full_ms": float(np.median(times))})
         print(json.dumps(rows[-1]), file=sys.stderr)
 
-    # cost model t = a V + b I over the plain runs (whole workload)
+    # cost model t = a V + b I over the plain runs (whole workload), non-negative coefficients:
+    # across alpha the visits and the interactions move together, so the split between them is
+    # poorly determined; the ratios below hold for either attribution
+    from scipy.optimize import nnls
+
     A = np.array([[r["full_visits"], r["full_inter"]] for r in rows], float)
     y = np.array([r["full_ms"] for r in rows])
-    coef, *_ = np.linalg.lstsq(A, y, rcond=None)
+    coef, _ = nnls(A, y)
     fit = A @ coef
     model = {"ms_per_visit": float(coef[0]), "ms_per_interaction": float(coef[1]),
              "max_rel_residual": float(np.max(np.abs(fit - y) / y))}
@@ -136,13 +142,14 @@ def main(argv=None):
     scale = nl / ns  # sampled windows -> whole workload
     groups = nl / 32
 
-    for eps in epss:
+    for cexp, eps in [(c, e) for c in cexps for e in epss]:
         t0 = time.time()
-        (cx, cy, cz), c = ctx.mac_ceiling(T, amag, args.alpha, wins, mode=1, eps=eps, band=band)
+        (cx, cy, cz), c = ctx.mac_ceiling(T, amag, args.alpha, wins, mode=1, eps=eps, band=band, cost_exp=cexp)
         e = relerr((cx, cy, cz), ref)
         V = c[:, 0].mean() * groups
         inter = (c[:, 1].sum() + c[:, 2].sum()) * scale
-        rows.append({"rule": "exact", "eps": eps, "p99": float(np.quantile(e, 0.99)), "median": float(np.median(e)),
+        rows.append({"rule": "exact", "cost_exp": cexp, "eps": eps, "p99": float(np.quantile(e, 0.99)),
+                     "median": float(np.median(e)),
                      "visits_per_window": float(c[:, 0].mean()), "ipp": float((c[:, 1].sum() + c[:, 2].sum()) / ns),
                      "labelled_per_window": float(c[:, 3].mean()), "label_particles_per_window": float(c[:, 4].mean()),
                      "model_ms": float(coef[0] * V + coef[1] * inter), "walk_s": time.time() - t0})
@@ -152,11 +159,11 @@ def main(argv=None):
             r["model_ms"] = float(coef[0] * r["visits_per_window"] * groups + coef[1] * r["ipp"] * nl)
 
     plain = [r for r in rows if r["rule"] == "plain"]
-    exact = [r for r in rows if r["rule"] == "exact"]
     head = min(plain, key=lambda r: abs(r["alpha"] - args.alpha))
     targets = sorted({head["p99"], 5e-3})
     compare = []
-    for tp in targets:
+    for cexp, tp in [(c, t) for c in cexps for t in targets]:
+        exact = [r for r in rows if r["rule"] == "exact" and r["cost_exp"] == cexp]
         t_plain = interp_at([r["p99"] for r in plain], [r["full_ms"] for r in plain], tp)
         m_plain = interp_at([r["p99"] for r in plain], [r["model_ms"] for r in plain], tp)
         m_exact = interp_at([r["p99"] for r in exact], [r["model_ms"] for r in exact], tp)
@@ -164,10 +171,13 @@ def main(argv=None):
         i_exact = interp_at([r["p99"] for r in exact], [r["ipp"] for r in exact], tp)
         v_plain = interp_at([r["p99"] for r in plain], [r["visits_per_window"] for r in plain], tp)
         v_exact = interp_at([r["p99"] for r in exact], [r["visits_per_window"] for r in exact], tp)
-        compare.append({"p99": tp, "plain_ms_measured": t_plain, "plain_ms_model": m_plain,
+        compare.append({"cost_exp": cexp, "p99": tp, "plain_ms_measured": t_plain, "plain_ms_model": m_plain,
                         "exact_ms_model": m_exact, "plain_ipp": i_plain, "exact_ipp": i_exact,
                         "plain_visits_per_window": v_plain, "exact_visits_per_window": v_exact,
-                        "ceiling_speedup": (m_plain / m_exact) if (m_plain and m_exact) else None})
+                        "ceiling_speedup": (m_plain / m_exact) if (m_plain and m_exact) else None,
+                        "interaction_ratio": (i_plain / i_exact) if (i_plain and i_exact) else None,
+                        "visit_ratio": (v_plain / v_exact) if (v_plain and v_exact) else None})
+        print(json.dumps(compare[-1]), file=sys.stderr)
     res = {"workload": args.workload, "n": n, "windows": int(len(wins)), "targets": int(ns), "band": band,
            "cost_model": model, "rows": rows, "at_equal_p99": compare}
     print(json.dumps(res))

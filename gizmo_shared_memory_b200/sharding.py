@@ -38,3 +38,18 @@ def gather_slices(parts, n_targets: int, world: int, window: int = 32) -> np.nda
     for (a, b), p in zip(shard_ranges(n_targets, world, window), parts):
         out[a:b] = p
     return out
+
+
+def walk_shard(walk, orderbuf, aold_tree, rank: int, world: int, window: int = 32):
+    """This rank's part of an all-active walk of one system.
+
+    orderbuf holds the tree order (particle indices) and aold_tree the per-target aold in the same
+    order (or None).  The rank walks targets orderbuf[a:b] with aold_tree[a:b], where [a, b) is its
+    window-aligned slice, so its windows are exactly the single-rank walk's windows over that
+    range.  walk(targets, aold) does the walking (the GPU context, or the oracle in the CPU tests)
+    and returns the results parallel to targets.  Returns (a, b, results)."""
+    a, b = shard_ranges(len(orderbuf), world, window)[rank]
+    tg = orderbuf[a:b]
+    ao = None if aold_tree is None else aold_tree[a:b]
+    return a, b, walk(tg, ao)
+

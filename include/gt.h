@@ -490,15 +490,18 @@ GT_API int gt_mac_sample(gt_context* ctx, const gt_tree* tree, const double* ama
  * relative criterion M L^2 <= r^4 alpha min|a| (shmem/tree.h:134-135) and reproduces the grouped
  * walk's decisions; mode 1 sums, for every node whose rho = M L^2 / (r^4 alpha min|a|) lies in
  * (rho_lo, rho_hi], the node's particles for every target of the window and accepts the node only
- * if the monopole's worst error over the window, |a_mono - a_exact| / |a_t|, is at most eps
- * (below the band it accepts, above it it opens).  amag = |a| per live particle in tree order.
+ * if the monopole's worst error over the window, |a_mono - a_exact| / |a_t|, is at most
+ * eps * ((c - 1) / 7)^cost_exp, c the interactions opening the node costs one step ahead (its
+ * children, or a leaf's particles; c - 1 floored at 1; cost_exp in [0, 4], 0 = a constant
+ * threshold).  Below the band it accepts, above it it opens.  amag = |a| per live particle in tree order.
  * Outputs: ax/ay/az (n_windows * window; slot k * window + i is target i of window k, 0 past
  * n_live) and counts (n_windows * 5: node visits, monopole and pair interactions counted as
  * SHMEM_COUNT_WALK counts them, labelled nodes, particles summed for labels).  No reference
  * counterpart: measurement of the learned criterion's ceiling. */
 GT_API int gt_mac_ceiling(gt_context* ctx, const gt_tree* tree, const double* amag, double alpha, int window,
-                          int64_t n_windows, const int64_t* windows, int mode, double eps, double rho_lo,
-                          double rho_hi, int mem, double* ax, double* ay, double* az, int64_t* counts);
+                          int64_t n_windows, const int64_t* windows, int mode, double eps, double cost_exp,
+                          double rho_lo, double rho_hi, int mem, double* ax, double* ay, double* az,
+                          int64_t* counts);
 /* Train a model on (features, labels) with the pinball loss at quantile tau, Adam, on the GPU.
  * model (host, GT_MAC_MODEL_FLOATS) receives the trained network; loss the final epoch's mean. */
 GT_API int gt_mac_train(gt_context* ctx, int64_t n, const float* features, const float* labels,

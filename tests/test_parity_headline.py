@@ -107,3 +107,41 @@ def test_parity_galaxy_4m():
 def test_parity_merger_67m():
     P = ics.merger(seed=5)
     report("merger_67m", *headline_parity(P, 0.0025, 256, 13))
+
+
+def test_parity_sparse_active_galaxy_4m():
+    """A scattered 1 % active set in tree order -- the engine's deep-timebin steps hand the walk
+    their active targets in tree order (shmem/mfm.cc:698-732) -- grouped by leaf (batch 0, the
+    engine's grouping) and in windows of 32, against the reference on the same targets and aold.
+    The group count of such a call stays on the device; the counted walk reports it."""
+    import torch
+
+    P = ics.galaxy(seed=2)
+    ctx = g.Context(0)
+    dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
+    T = ctx.build(dev)
+    nl = T.info()["n_live"]
+    ob = T.download(nodes=False)["orderbuf"]
+    out = tuple(torch.empty(nl, dtype=torch.float64, device="cuda") for _ in range(3))
+    ctx.accel_grouped(T, None, theta=0.7, batch=WINDOW, outs=out + (None,), group_mode=g.GT_GROUP_BATCH)
+    aold = ctx.form_aold(*out, 0.0025).cpu().numpy()
+    rng = np.random.default_rng(14)
+    pos = np.sort(rng.choice(nl, size=nl // 100, replace=False))
+    tg = ob[pos].astype(np.uint32)
+    kind, R = checker(P)
+    leaf = R.order()[2]
+    for batch, mode in ((0, g.GT_GROUP_LEAF), (WINDOW, g.GT_GROUP_BATCH)):
+        a = ctx.accel_grouped(T, tg, aold=aold[pos], batch=batch, group_mode=mode, count=True)
+        st = ctx.stats()
+        if batch == 0:
+            lv = leaf[tg]
+            assert st["groups"] == 1 + int(np.count_nonzero(lv[1:] != lv[:-1]))
+        else:
+            assert st["groups"] == -(-len(tg) // WINDOW)
+        r = walk_windows(kind, R, tg, 0.0, aold[pos]) if batch else (
+            R.accel_grouped(tg, 0.0, 1.0, 0, aold=aold[pos])[:3])
+        e = relerr(a, r)
+        print(f"galaxy_4m scattered 1 %: {len(tg)} targets, batch {batch}: median {np.median(e):.2e} "
+              f"p99 {np.quantile(e, 0.99):.2e}")
+        assert np.median(e) <= MEDIAN_TOL and np.quantile(e, 0.99) <= P99_TOL
+    ctx.close()

@@ -1,9 +1,9 @@
 """Multi-rank target sharding, on CPU with the gloo backend (world size 2).
 
-Each rank builds the tree from the full particle set, walks its slice of the targets with the
-oracle walk (the GPU walk's host-side logic is the same: a contiguous tree-order slice on window
-edges), and the slices are all-gathered only to check that together they equal the single-rank
-walk exactly.
+Each rank builds the tree from the full particle set and walks its slice of the targets through
+sharding.walk_shard -- the same host function bench.py --split targets uses on the GPU -- with the
+oracle walk as the walker.  The slices are all-gathered only to check that together they equal the
+single-rank walk exactly, for the bootstrap walk and for the relative criterion with aold.
 """
 import os
 import socket
@@ -14,7 +14,7 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 from gizmo_shared_memory_b200 import ics
-from gizmo_shared_memory_b200.sharding import gather_slices, rank_targets, shard_ranges
+from gizmo_shared_memory_b200.sharding import gather_slices, shard_ranges, walk_shard
 
 
 def test_shard_ranges_cover_and_align():
@@ -52,20 +52,28 @@ def _worker(rank, world, port, q):
         P = ics.plummer(n=12000, seed=5, soft=0.01)
         T = Restatement().build(P)           # every rank builds the same tree
         ob = T.order()[0]
-        mine = rank_targets(ob, rank, world, 32)
-        starts = np.arange(0, len(mine) + 1, 32, dtype=np.int64)
-        if starts[-1] != len(mine):
-            starts = np.append(starts, len(mine))
-        ax, ay, az, _, _ = T.walk_groups(mine, starts, 0.7)
+
+        def windows(t):
+            s = np.arange(0, len(t) + 1, 32, dtype=np.int64)
+            return s if s[-1] == len(t) else np.append(s, len(t))
+
+        def walker(theta):
+            return lambda tg, ao: np.stack(T.walk_groups(tg, windows(tg), theta, aold=ao)[:3])
+
+        ok = True
+        _, _, boot = walk_shard(walker(0.7), ob, None, rank, world, 32)
         parts = [None] * world
-        dist.all_gather_object(parts, np.stack([ax, ay, az]))   # check only
+        dist.all_gather_object(parts, boot)   # check only
+        full = np.stack([gather_slices([p[k] for p in parts], len(ob), world, 32) for k in range(3)])
+        aold = 0.005 * np.sqrt((full ** 2).sum(axis=0))
+        _, _, rel = walk_shard(walker(0.0), ob, aold, rank, world, 32)
+        parts2 = [None] * world
+        dist.all_gather_object(parts2, rel)
         if rank == 0:
-            full = np.stack([gather_slices([p[k] for p in parts], len(ob), world, 32) for k in range(3)])
-            starts_all = np.arange(0, len(ob) + 1, 32, dtype=np.int64)
-            if starts_all[-1] != len(ob):
-                starts_all = np.append(starts_all, len(ob))
-            bx, by, bz, _, _ = T.walk_groups(ob, starts_all, 0.7)
-            q.put(bool(np.array_equal(full, np.stack([bx, by, bz]))))
+            ok &= bool(np.array_equal(full, walker(0.7)(ob, None)))
+            full2 = np.stack([gather_slices([p[k] for p in parts2], len(ob), world, 32) for k in range(3)])
+            ok &= bool(np.array_equal(full2, walker(0.0)(ob, aold)))
+            q.put(ok)
     finally:
         dist.barrier()
         dist.destroy_process_group()
