@@ -361,6 +361,15 @@ def read_profile_traffic(workload):
         return None
 
 
+def nominal_fp32(clocks, sms=148, lanes=128):
+    """The FP32 CUDA-core peak from the data sheet arithmetic: SMs x FMA lanes x 2 flops x clock,
+    at the maximum SM clock and at the median clock sampled during the timed steps."""
+    mx = (clocks or {}).get("sm_max_mhz") or 1965.0
+    med = (clocks or {}).get("sm_mhz") or mx
+    return {"at_max_clock": sms * lanes * 2 * mx * 1e6 / 1e12, "at_sampled_clock": sms * lanes * 2 * med * 1e6 / 1e12,
+            "sm_max_mhz": mx, "sm_mhz_sampled": med}
+
+
 def window_parity(cpu, Tc, ob_gpu, aold_tree, full, batch, n_windows=256, seed=9):
     """This walk against the reference's accel_grouped on whole windows of this walk's own groups:
     the windows are passed in this tree's order with the same batch, so the reference forms exactly
@@ -657,6 +666,8 @@ def run_gpu_arm(args):
                      "frac": achieved / peak32, "traffic": read_profile_traffic(args.workload),
                      "peak_source": "measured FP32 FMA-chain probe on this GPU (gt_measure_peaks), "
                                     "not in MEASURED_PEAKS.json",
+                     "nominal_fp32_tflops": nominal_fp32(clocks),
+                     "frac_of_nominal": achieved / nominal_fp32(clocks)["at_max_clock"],
                      "flops_per_interaction": FLOPS_PER_INTERACTION, "kernel": "walk_kernel",
                      "kernel_ms": 1e3 * t_kernel, "fp64_peak_tflops": peak64},
         "cpu_baseline": cpu_line,

@@ -1246,7 +1246,7 @@ int gt_mac_ceiling(gt_context* ctx, const gt_tree* tree, const double* amag, dou
         if (!tree || !amag || n_windows < 0 || (n_windows > 0 && (!windows || !ax || !ay || !az || !counts)))
             throw Fail{GT_ERR_INVALID, "bad arguments"};
         if (window < 1 || window > 32) throw Fail{GT_ERR_INVALID, "window must be in [1, 32]"};
-        if (mode != 0 && mode != 1) throw Fail{GT_ERR_INVALID, "mode must be 0 (plain) or 1 (exact labels)"};
+        if (mode < 0 || mode > 5) throw Fail{GT_ERR_INVALID, "mode must be in [0, 5]"};
         if (!(alpha > 0) || !(eps >= 0) || !(rho_hi >= rho_lo) || !(cost_exp >= 0.0 && cost_exp <= 4.0))
             throw Fail{GT_ERR_INVALID, "bad alpha, eps, cost exponent or band"};
         if (tree->n_systems > 1) throw Fail{GT_ERR_UNSUPPORTED, "gt_mac_ceiling takes a single-system tree"};

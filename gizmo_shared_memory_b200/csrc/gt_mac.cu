@@ -218,7 +218,16 @@ __global__ void __launch_bounds__(256) mac_sample_kernel(const SampleArgs A) {
 //           children, or a leaf's particles; c - 1 floored at 1); below the band it accepts, above
 //           it it opens.  cost_exp = 0 is a constant threshold; cost_exp > 0 spends more of the
 //           error budget where opening is dearer.
-// Both modes share the softening-overlap and inside-node arms.  Mode 1 is the rule a learned
+// Modes 2-5 keep the form of the relative criterion, X / r^4 <= alpha |a|, with one ingredient of
+// the exact rule each, to show which of them carry the exact rule's savings:
+//   mode 2: r = the larger of the distances to the window's box and to its enclosing sphere (about
+//           the box centre): both are lower bounds of the distance to every target;
+//   mode 3: per target, r_t = its own distance to the node's centre of mass and its own |a_t|;
+//           the node opens if any target's ratio exceeds alpha;
+//   mode 4: mode 3 with X = 4 q2, q2 the node's second mass moment about its centre of mass,
+//           in place of M L^2 (4 q2 = M L^2 for a uniform cube);
+//   mode 5: mode 0 (the box's nearest point, min |a|) with X = 4 q2.
+// All modes share the softening-overlap and inside-node arms.  Mode 1 is the rule a learned
 // criterion that predicted every (window, node) error exactly would apply, so its interactions and
 // node visits at a given force error bound what any learned acceptance rule over the monopole walk
 // can save.  Mode 0 reproduces the production walk's decisions (the test checks its counts).
@@ -230,6 +239,7 @@ struct CeilArgs {
     int n_win, window;
     int64_t n_live;
     const double* amag;   // |a| per live particle in tree order
+    const float* nq2;     // per node second mass moment about the centre of mass (modes 4, 5)
     double alpha, eps, cost_exp, rho_lo, rho_hi;
     int mode;
     int* stack;
@@ -252,6 +262,7 @@ __device__ __forceinline__ double spline_force_d(double r2, double h) {
 
 __global__ void __launch_bounds__(256) ceiling_kernel(const CeilArgs A) {
     __shared__ SrcP tile[8][32];
+    __shared__ double tq[8][32][4];  // the window's targets: position and 1 / |a| (modes 3, 4)
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
     const int gw = blockIdx.x * (blockDim.x >> 5) + wi;
     int* stk = A.stack + (size_t)gw * A.stack_cap;
@@ -276,6 +287,12 @@ __global__ void __launch_bounds__(256) ceiling_kernel(const CeilArgs A) {
         const double emax = wmax(tv ? ps : 0.0);
         const double aold = A.alpha * wmin(am);
         const double inv_a = tv && am > 0.0 ? 1.0 / am : 0.0;  // 0: a target without |a| never accepts
+        const double gcx = 0.5 * (lx + hx), gcy = 0.5 * (ly + hy), gcz = 0.5 * (lz + hz);
+        // enclosing sphere about the box centre (mode 2)
+        const double rsph = sqrt(wmax(tv ? (px - gcx) * (px - gcx) + (py - gcy) * (py - gcy) + (pz - gcz) * (pz - gcz) : 0.0));
+        tq[wi][lane][0] = px; tq[wi][lane][1] = py; tq[wi][lane][2] = pz;
+        tq[wi][lane][3] = tv ? (am > 0.0 ? 1.0 / am : 1e300) : 0.0;
+        __syncwarp();
         double sx = 0, sy = 0, sz = 0;
         unsigned long long c_vis = 0, c_mul = 0, c_pair = 0, c_lab = 0, c_labsum = 0;
         unsigned c_self = 0;  // pairs at r = 0 (the target itself), which count as no interaction
@@ -306,7 +323,23 @@ __global__ void __launch_bounds__(256) ceiling_kernel(const CeilArgs A) {
                     open = true;
                 } else {
                     const double rho = nd.mass * len * len / (r2 * r2 * aold);
+                    const double X = (A.mode == 4 || A.mode == 5) ? 4.0 * (double)A.nq2[node] : nd.mass * len * len;
                     if (A.mode == 0) open = rho > 1.0;
+                    else if (A.mode == 5) open = X > r2 * r2 * aold;
+                    else if (A.mode == 2) {
+                        const double cx = nd.cx - gcx, cy = nd.cy - gcy, cz = nd.cz - gcz;
+                        const double rb = sqrt(r2), rs = sqrt(cx * cx + cy * cy + cz * cz) - rsph;
+                        const double r = rs > rb ? rs : rb;
+                        open = X > r * r * r * r * aold;
+                    } else if (A.mode == 3 || A.mode == 4) {
+                        double worst = 0.0;
+                        for (int k = 0; k < nt; ++k) {
+                            const double ex = nd.cx - tq[wi][k][0], ey = nd.cy - tq[wi][k][1], ez = nd.cz - tq[wi][k][2];
+                            const double q = ex * ex + ey * ey + ez * ez;
+                            worst = fmax(worst, X * tq[wi][k][3] / (q * q));
+                        }
+                        open = worst > A.alpha;
+                    }
                     else if (rho <= A.rho_lo) open = false;
                     else if (rho > A.rho_hi) open = true;
                     else label = true;
@@ -591,7 +624,7 @@ void run_mac_ceiling(gt_context* ctx, const gt_tree* t, const double* amag, doub
     CeilArgs a;
     a.nodes = t->nodes; a.src = t->src; a.ssoft = t->ssoft;
     a.wins = wins; a.n_win = (int)n_win; a.window = window; a.n_live = t->n_live;
-    a.amag = amag; a.alpha = alpha; a.eps = eps; a.cost_exp = cost_exp; a.rho_lo = rho_lo; a.rho_hi = rho_hi; a.mode = mode;
+    a.amag = amag; a.nq2 = t->nq2; a.alpha = alpha; a.eps = eps; a.cost_exp = cost_exp; a.rho_lo = rho_lo; a.rho_hi = rho_hi; a.mode = mode;
     a.stack = (int*)scratch(ctx, kSlotStack, (size_t)blocks * warps * stack_cap * 4);
     a.stack_cap = stack_cap;
     unsigned long long* ctr = (unsigned long long*)scratch(ctx, kSlotCounters, 256);

@@ -69,6 +69,8 @@ def main(argv=None):
     ap.add_argument("--eps", default="3e-5,1e-4,2e-4,4e-4,7e-4,1e-3,1.5e-3,2.5e-3,4e-3,7e-3")
     ap.add_argument("--band", default="0.001,1000", help="rho band of the exact labels")
     ap.add_argument("--cost-exp", default="0", help="exponents of the cost-aware threshold to sweep")
+    ap.add_argument("--modes", default="", help="modes 2-5 (one ingredient of the exact rule each) to sweep "
+                                                "over the alphas of the plain criterion")
     ap.add_argument("--alpha", type=float, default=0.0025, help="the headline plain criterion")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--out", default=None)
@@ -154,6 +156,16 @@ def main(argv=None):
                      "labelled_per_window": float(c[:, 3].mean()), "label_particles_per_window": float(c[:, 4].mean()),
                      "model_ms": float(coef[0] * V + coef[1] * inter), "walk_s": time.time() - t0})
         print(json.dumps(rows[-1]), file=sys.stderr)
+    for mode, a in [(int(m), a) for m in filter(None, args.modes.split(",")) for a in alphas]:
+        (cx, cy, cz), c = ctx.mac_ceiling(T, amag, a, wins, mode=mode)
+        e = relerr((cx, cy, cz), ref)
+        V = c[:, 0].mean() * groups
+        inter = (c[:, 1].sum() + c[:, 2].sum()) * scale
+        rows.append({"rule": f"mode{mode}", "alpha": a, "p99": float(np.quantile(e, 0.99)),
+                     "median": float(np.median(e)), "visits_per_window": float(c[:, 0].mean()),
+                     "ipp": float((c[:, 1].sum() + c[:, 2].sum()) / ns),
+                     "model_ms": float(coef[0] * V + coef[1] * inter)})
+        print(json.dumps(rows[-1]), file=sys.stderr)
     for r in rows:
         if r["rule"] == "plain":
             r["model_ms"] = float(coef[0] * r["visits_per_window"] * groups + coef[1] * r["ipp"] * nl)
@@ -162,8 +174,9 @@ def main(argv=None):
     head = min(plain, key=lambda r: abs(r["alpha"] - args.alpha))
     targets = sorted({head["p99"], 5e-3})
     compare = []
-    for cexp, tp in [(c, t) for c in cexps for t in targets]:
-        exact = [r for r in rows if r["rule"] == "exact" and r["cost_exp"] == cexp]
+    families = [("exact", c) for c in cexps] + [(f"mode{m}", None) for m in filter(None, args.modes.split(","))]
+    for (rule, cexp), tp in [(f, t) for f in families for t in targets]:
+        exact = [r for r in rows if r["rule"] == rule and (cexp is None or r["cost_exp"] == cexp)]
         t_plain = interp_at([r["p99"] for r in plain], [r["full_ms"] for r in plain], tp)
         m_plain = interp_at([r["p99"] for r in plain], [r["model_ms"] for r in plain], tp)
         m_exact = interp_at([r["p99"] for r in exact], [r["model_ms"] for r in exact], tp)
@@ -171,7 +184,7 @@ def main(argv=None):
         i_exact = interp_at([r["p99"] for r in exact], [r["ipp"] for r in exact], tp)
         v_plain = interp_at([r["p99"] for r in plain], [r["visits_per_window"] for r in plain], tp)
         v_exact = interp_at([r["p99"] for r in exact], [r["visits_per_window"] for r in exact], tp)
-        compare.append({"cost_exp": cexp, "p99": tp, "plain_ms_measured": t_plain, "plain_ms_model": m_plain,
+        compare.append({"rule": rule, "cost_exp": cexp, "p99": tp, "plain_ms_measured": t_plain, "plain_ms_model": m_plain,
                         "exact_ms_model": m_exact, "plain_ipp": i_plain, "exact_ipp": i_exact,
                         "plain_visits_per_window": v_plain, "exact_visits_per_window": v_exact,
                         "ceiling_speedup": (m_plain / m_exact) if (m_plain and m_exact) else None,

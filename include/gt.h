@@ -493,7 +493,11 @@ GT_API int gt_mac_sample(gt_context* ctx, const gt_tree* tree, const double* ama
  * if the monopole's worst error over the window, |a_mono - a_exact| / |a_t|, is at most
  * eps * ((c - 1) / 7)^cost_exp, c the interactions opening the node costs one step ahead (its
  * children, or a leaf's particles; c - 1 floored at 1; cost_exp in [0, 4], 0 = a constant
- * threshold).  Below the band it accepts, above it it opens.  amag = |a| per live particle in tree order.
+ * threshold).  Below the band it accepts, above it it opens.  Modes 2-5 keep the plain form
+ * X / r^4 <= alpha |a| with one ingredient of the exact rule each: 2 = r from the larger of the
+ * window box's and its enclosing sphere's distances; 3 = each target's own r_t and |a_t| (the node
+ * opens if any target's ratio exceeds alpha); 4 = mode 3 with X = 4 q2 (the node's second mass
+ * moment about its centre of mass) in place of M L^2; 5 = mode 0 with X = 4 q2.  amag = |a| per live particle in tree order.
  * Outputs: ax/ay/az (n_windows * window; slot k * window + i is target i of window k, 0 past
  * n_live) and counts (n_windows * 5: node visits, monopole and pair interactions counted as
  * SHMEM_COUNT_WALK counts them, labelled nodes, particles summed for labels).  No reference
