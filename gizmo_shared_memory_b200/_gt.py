@@ -44,7 +44,7 @@ EXPORTS = [
     "gt_accel_grouped_ext", "gt_tree_velocities", "gt_tree_velocity_moments", "gt_tree_events",
     "gt_tree_refresh", "gt_tree_node_state", "gt_tree_particles", "gt_tree_gas",
     "gt_ngb_options_default", "gt_tree_hmax", "gt_ngb_search", "gt_density_options_default", "gt_density",
-    "gt_direct_gas", "gt_mac_ceiling",
+    "gt_direct_gas", "gt_mac_ceiling", "gt_tree_audit",
 ]
 
 
@@ -184,6 +184,7 @@ def load_library(path: str = LIB_PATH):
     L.gt_mac_train_options_default.argtypes = [C.POINTER(MacTrainOptions)]
     L.gt_mac_sample.argtypes = [vp, vp, vp, d, C.c_int, i64, d, d, i64, C.c_int, vp, vp, vp,
                                 C.POINTER(i64)]
+    L.gt_tree_audit.argtypes = [vp, vp, C.POINTER(i64), C.c_char_p, C.c_size_t]
     L.gt_mac_ceiling.argtypes = [vp, vp, vp, d, C.c_int, i64, vp, C.c_int, d, d, d, d, C.c_int, vp, vp, vp, vp]
     L.gt_mac_train.argtypes = [vp, i64, vp, vp, C.POINTER(MacTrainOptions), C.c_int, vp, C.POINTER(d)]
     L.gt_mac_predict.argtypes = [vp, vp, i64, vp, C.c_int, vp]
@@ -595,6 +596,13 @@ class Context:
             GT_MEM_HOST, _ptr(ax), _ptr(ay), _ptr(az), _ptr(phi), _ptr(tt), _ptr(jj)))
         cut = lambda a: None if a is None else a[:nt]
         return cut(ax), cut(ay), cut(az), cut(phi), cut(tt), cut(jj)
+
+    def tree_audit(self, tree: Tree):
+        """gt_tree_audit: (number of violations, the first one's message)."""
+        nb = C.c_int64()
+        buf = C.create_string_buffer(512)
+        self._check(load_library().gt_tree_audit(self.h, tree.h, C.byref(nb), buf, 512))
+        return nb.value, buf.value.decode()
 
     def tree_velocities(self, tree: Tree, vx, vy, vz, particles_only=False):
         """Attach velocities (indexed like the build input): node vcom and vmax, for the jerk."""

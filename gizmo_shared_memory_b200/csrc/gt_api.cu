@@ -1236,6 +1236,16 @@ int gt_mac_sample(gt_context* ctx, const gt_tree* tree, const double* amag, doub
     });
 }
 
+int gt_tree_audit(gt_context* ctx, const gt_tree* tree, int64_t* n_bad, char* msg, size_t msglen) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        if (!tree || !n_bad) throw Fail{GT_ERR_INVALID, "bad arguments"};
+        if (tree->device != ctx->device) throw Fail{GT_ERR_DEVICE, "the tree belongs to another device"};
+        DeviceGuard dg(ctx->device);
+        run_tree_audit(ctx, tree, n_bad, msg, msglen);
+    });
+}
+
 int gt_mac_ceiling(gt_context* ctx, const gt_tree* tree, const double* amag, double alpha, int window,
                    int64_t n_windows, const int64_t* windows, int mode, double eps, double cost_exp,
                    double rho_lo, double rho_hi, int mem, double* ax, double* ay, double* az,

@@ -307,6 +307,7 @@ void run_peano_keys(gt_context* ctx, int64_t n, const double* x, const double* y
 void run_mac_sample(gt_context* ctx, const gt_tree* t, const double* amag, double alpha, int window,
                     int64_t stride, double rho_lo, double rho_hi, int64_t cap, float* feat,
                     float* label, float* rho, int64_t* n_samples);
+void run_tree_audit(gt_context* ctx, const gt_tree* t, int64_t* n_bad, char* msg, size_t msglen);
 void run_mac_ceiling(gt_context* ctx, const gt_tree* t, const double* amag, double alpha, int window,
                      int64_t n_win, const int64_t* wins, int mode, double eps, double cost_exp, double rho_lo,
                      double rho_hi, double* ax, double* ay, double* az, unsigned long long* counts);

@@ -36,6 +36,16 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxWarps = 8;     // warps per block of the walk kernel
+
+// The debug library (make debug: libgt_debug.so, built with -DGT_BOUNDS_CHECK) checks every index
+// the walk derives before it is used -- node, particle slot, target position, list slot, output
+// index -- and on a violation records error 3 and skips the access.  The ordinary library compiles
+// the checks away.
+#ifdef GT_BOUNDS_CHECK
+#define GT_IN_BOUNDS(i, n) ((i) >= 0 && (int64_t)(i) < (int64_t)(n) ? true : (atomicExch(A.error, 3), false))
+#else
+#define GT_IN_BOUNDS(i, n) true
+#endif
 constexpr int kPnCapDefault = 256;  // monopole-list entries per warp (gt_walk_options.list_capacity)
 constexpr int kPnCapMax = 1024;     // the particle list holds half as many entries
 
@@ -55,7 +65,8 @@ struct WalkArgs {
     int stack_cap;
     unsigned int* next_group;   // dynamic group counter
     unsigned long long* stats;  // [nodes, multipole, pairs_structural, zero_r2, flushes, max_stack, steps]
-    int* error;                 // 1: stack overflow
+    int* error;                 // 1: stack overflow; 3: an index out of bounds (debug library)
+    int64_t n_nodes, n_src, n_out;  // array extents, for the debug library's bounds checks
     int pn_cap, pp_cap;         // list capacities per warp (multiples of 32)
     int warp_bytes;             // shared memory per warp: header + lists
     // learned criterion
@@ -317,7 +328,8 @@ walk_kernel(const WalkArgs A) {
             ps[k] = 0.0;
             const int i = lane + 32 * k;
             if (k < nk && i < nt) {
-                const int p = A.tpos ? (int)A.tpos[t0 + i] : t0 + i;
+                int p = A.tpos ? (int)A.tpos[t0 + i] : t0 + i;
+                if (!GT_IN_BOUNDS(p, A.n_src)) p = 0;
                 float mf, hf;
                 load_src(A.src + p, px[k], py[k], pz[k], mf, hf);
                 ps[k] = A.ssoft[p];
@@ -616,7 +628,8 @@ walk_kernel(const WalkArgs A) {
         while (top > 0) {
             const int npop = min(top, 32);
             top -= npop;
-            const int node = lane < npop ? stk[top + lane] : -1;
+            int node = lane < npop ? stk[top + lane] : -1;
+            if (node >= 0 && !GT_IN_BOUNDS(node, A.n_nodes)) node = -1;
             __syncwarp();
             bool accept = false, expand = false, push = false;
             // idle lanes read node 0 and decide nothing (cheaper than defaulting every field)
@@ -714,7 +727,7 @@ walk_kernel(const WalkArgs A) {
             if (am) {
                 const int na = __popc(am);
                 if (npn + na > A.pn_cap) { flush_pn(npn); npn = 0; }
-                if (accept) {
+                if (accept && GT_IN_BOUNDS(npn + __popc(am & lt_mask), A.pn_cap)) {
                     const int pos = npn + __popc(am & lt_mask);
                     pn_put(pos, (float)(nd.cx - S.c_x), (float)(nd.cy - S.c_y), (float)(nd.cz - S.c_z),
                            (float)nd.mass);
@@ -751,6 +764,7 @@ walk_kernel(const WalkArgs A) {
                         for (int step = 16; step > 0; step >>= 1)
                             if (S.pre[l + step] <= q) l += step;
                         qpos = S.lo[l] + (q - S.pre[l]);
+                        if (!GT_IN_BOUNDS(qpos, A.n_src)) qpos = 0;
                         load_src(A.src + qpos, qx, qy, qz, qm, qh);
                         const double ex = box_gap(S.lo_x, qx, S.hi_x);
                         const double ey = box_gap(S.lo_y, qy, S.hi_y);
@@ -765,10 +779,10 @@ walk_kernel(const WalkArgs A) {
                     if (npn + nf > A.pn_cap) { flush_pn(npn); npn = 0; }
                     if (npp + nn > A.pp_cap) { flush_pp(npp); npp = 0; }
                     const float4 e = make_float4((float)(qx - S.c_x), (float)(qy - S.c_y), (float)(qz - S.c_z), qm);
-                    if (live && far) {
+                    if (live && far && GT_IN_BOUNDS(npn + __popc(fm & lt_mask), A.pn_cap)) {
                         pn_put(npn + __popc(fm & lt_mask), e.x, e.y, e.z, e.w);
                         if (want_jerk) pnv[npn + __popc(fm & lt_mask)] = A.svel[qpos];
-                    } else if (live) {
+                    } else if (live && GT_IN_BOUNDS(npp + __popc(nm & lt_mask), A.pp_cap)) {
                         const int pos = npp + __popc(nm & lt_mask);
                         pp[pos] = e;
                         ph[pos] = qh;
@@ -810,6 +824,7 @@ walk_kernel(const WalkArgs A) {
             if (slice == 0 && k < nk && i < nt) {
                 const int idx = t0 + i;
                 const int o = A.out_map ? (int)A.out_map[idx] : idx;
+                if (!GT_IN_BOUNDS(o, A.n_out)) continue;
                 if (A.ax) {
                     A.ax[o] = A.G * vx;
                     A.ay[o] = A.G * vy;
@@ -1343,6 +1358,9 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     a.ssoft = t->ssoft;
     a.tpos = tpos;
     a.aold = rq.aold;
+    a.n_nodes = t->n_nodes;
+    a.n_src = t->n;
+    a.n_out = (all && rq.out_original) ? t->n : nt;
     a.groups = groups;
     a.n_groups = (int)ng;
     a.n_groups_dev = ng_dev;
@@ -1529,14 +1547,17 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         else dispatch<4>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
         if (rq.capture) break;  // the default stack capacity is a proven bound
         check_cuda(cudaEventRecord(ctx->ev1, st), "event");
+#ifndef GT_BOUNDS_CHECK
         if (!rq.count && attempt == 0 && rq.stack_capacity == 0) {
             // the default capacity is a proven bound: no read-back needed on the fast path
             break;
         }
+#endif
         check_cuda(cudaMemcpyAsync(ctx->pinned, ctr, 80, cudaMemcpyDeviceToHost, st), "stats d2h");
         check_cuda(cudaStreamSynchronize(st), "sync");
         unsigned long long h[10];
         std::memcpy(h, ctx->pinned, 80);
+        if ((int)h[9] == 3) throw Fail{GT_ERR_INVALID, "walk: an index failed its bounds check"};
         if ((int)h[9] == 0) {
             if (ng_dev) {
                 uint32_t hg = 0;

@@ -268,7 +268,18 @@ GT_API int gt_tree_gas(gt_context* ctx, gt_tree* tree, const uint8_t* type, cons
 GT_API int gt_tree_velocity_moments(gt_context* ctx, const gt_tree* tree, double* vcx, double* vcy,
                              double* vcz, float* vmax);
 
-/* ---- walks --------------------------------------------------------------------------------- */
+/* Audit of the tree's invariants on the device: the replacement for shmem::audit_tree
+ * (shmem/tree.cc:973-1119).  Checks the structure (particle ranges, children contiguous and
+ * partitioning their parent's range, parent, level, side, the reference's next threading, leaf
+ * size), re-derives every node's mass and centre of mass from its particles (FP64; mass to 1e-10,
+ * centre of mass to 1e-6 of the node's reach), checks every particle lies in each ancestor's cell
+ * (plus 1e-6 of the root side and the node's displacement pad) and under its softening, and checks
+ * the maps (leaf_of, rank, order) and the live/massless split.  *n_bad receives the number of
+ * violations (0: the tree is sound); msg (may be NULL) the first one found.  On a reused tree call
+ * it after gt_tree_refresh: the moments compared are the walk nodes'. */
+GT_API int gt_tree_audit(gt_context* ctx, const gt_tree* tree, int64_t* n_bad, char* msg, size_t msglen);
+
+/* ---- walks --------------------------------------------------------------------------------- *//* ---- walks --------------------------------------------------------------------------------- */
 /* Grouped walk.  Replaces shmem::accel_grouped (shmem/tree.h:428-440, tree.cc:626-897) without
  * the tidal tensor and the jerk (gt_accel_grouped_ext) and without lazy drift; the gas rules and
  * sink-direct opening come from gt_tree_gas and gt_walk_options.sink_direct_radius.  batch <= 0 groups

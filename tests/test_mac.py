@@ -64,11 +64,11 @@ def test_what_the_trained_network_gains(gpu_ctx):
     the Plummer and galaxy workloads by train_mac.py) against the plain relative criterion it
     corrects, on a held-out clustered box (Soneira-Peebles, 10 levels, 1M particles).
 
-    Prints the interactions per particle and the walk time of both criteria at equal sampled
-    p99: on the workloads measured so far the network saves a few per cent of interactions at
-    best and no wall-clock time, so what is asserted is what must hold either way --
+    Asserts, with the interactions per particle and the walk time of both criteria printed:
       * the zero network is the plain criterion exactly (the correction is what the network adds);
-      * the trained network changes the decisions (it is not a no-op);
+      * at the kappa that matches the plain walk's sampled p99, the trained network takes fewer
+        interactions than the zero network (measured 1.057x on this box; the exact-label ceiling
+        of any acceptance rule is about 1.3x on the 16M box);
       * the autotuner, offered both, returns a configuration that meets the p99 target and is
         no slower than the plain one it measured (the plain criterion stays the fallback)."""
     import json
@@ -118,7 +118,7 @@ def test_what_the_trained_network_gains(gpu_ctx):
     print(f"\nplain: {ipp_plain:.1f} interactions/particle, p99 {p99_plain:.3e}; "
           f"trained per-node network (kappa {kappa:.3g}): {ipp_l:.1f}, p99 {p99_l:.3e}; "
           f"gain {ipp_plain / ipp_l:.3f}x in interactions at equal p99")
-    assert abs(ipp_l - ipp_plain) > 1e-3 * ipp_plain  # the network changes the decisions
+    assert ipp_plain / ipp_l >= 1.03  # the trained network's gain over the zero network
     opts, entries = gpu_ctx.autotune(T, aold, sample=sample, ref=list(ref), p99_max=p99_plain, reps=3,
                                      mac_model=model, kappas=[kappa], mac=g.GT_MAC_NODE)
     plain_best = min(e["ms"] for e in entries if e["mac"] == g.GT_MAC_PLAIN and e["accepted"])
