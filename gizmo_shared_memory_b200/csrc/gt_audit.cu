@@ -162,12 +162,13 @@ __global__ void __launch_bounds__(256) audit_nodes_kernel(const AuditArgs A) {
     }
 }
 
-// Tree positions past the live range hold the massless particles: no leaf, no tree position.
+// Tree positions past the live range hold the massless particles, in no leaf (the device keeps
+// their tree positions in rank; gt_tree_download marks them UINT32_MAX as the reference does).
 __global__ void audit_dead_kernel(const AuditArgs A) {
     for (int64_t s = A.n_live + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < A.n;
          s += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t pi = A.order[s];
-        if (A.smass[s] > 0.0 || pi >= A.n || A.leaf_of[pi] != -1 || A.rank[pi] != 0xffffffffu)
+        if (A.smass[s] > 0.0 || pi >= A.n || A.leaf_of[pi] != -1 || A.rank[pi] != (uint32_t)s || A.sleaf[s] != -1)
             report(A, kAuditDead, -1, s, A.smass[s], pi < A.n ? (double)A.leaf_of[pi] : -2.0);
     }
 }

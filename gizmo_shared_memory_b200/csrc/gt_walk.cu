@@ -894,41 +894,115 @@ __global__ void fill_group_id_kernel(const GNode* __restrict__ nodes, const int*
     }
 }
 
-// Group starts over explicit targets: a new group where the key changes or is negative.
+// Whether target k starts a group (a new group where the key changes or is negative); also
+// records its tree position.
+__device__ __forceinline__ bool target_starts(const uint32_t* __restrict__ targets, int64_t k, int mode,
+                                              int param, const uint32_t* __restrict__ rank,
+                                              const int* __restrict__ leaf_of, const int* __restrict__ gid,
+                                              uint32_t* __restrict__ tpos, const int* __restrict__ sys_off,
+                                              int n_systems, int all_live) {
+    const uint32_t p = targets[k];
+    const uint32_t pos = rank[p];
+    tpos[k] = pos;
+    if (k == 0) return true;
+    if (mode == GT_GROUP_LEAF) {
+        const int a = leaf_of[p], b = leaf_of[targets[k - 1]];
+        return a != b || a < 0;
+    }
+    if (mode == GT_GROUP_NODE) {
+        const int a = gid[pos], b = gid[rank[targets[k - 1]]];
+        return a != b || a < 0;
+    }
+    if (mode == GT_GROUP_BATCH) {
+        if (n_systems > 1) {
+            // a window never spans two systems of a forest; over all live targets the windows of
+            // each system start at its first particle, as in its own tree
+            const int s = system_of(sys_off, n_systems, pos);
+            return s != system_of(sys_off, n_systems, rank[targets[k - 1]]) ||
+                   (all_live ? ((int64_t)pos - sys_off[s]) % param == 0 : (k % param) == 0);
+        }
+        return (k % param) == 0;
+    }
+    return true;
+}
+
 __global__ void target_flags_kernel(const uint32_t* __restrict__ targets, int64_t nt, int mode,
                                     int param, const uint32_t* __restrict__ rank,
                                     const int* __restrict__ leaf_of, const int* __restrict__ gid,
                                     uint32_t* __restrict__ tpos, uint32_t* __restrict__ flag,
                                     const int* __restrict__ sys_off, int n_systems, int all_live) {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nt;
-         k += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t p = targets[k];
-        const uint32_t pos = rank[p];
-        tpos[k] = pos;
-        bool start = (k == 0);
-        if (!start) {
-            if (mode == GT_GROUP_LEAF) {
-                const int a = leaf_of[p], b = leaf_of[targets[k - 1]];
-                start = a != b || a < 0;
-            } else if (mode == GT_GROUP_NODE) {
-                const int a = gid[pos], b = gid[rank[targets[k - 1]]];
-                start = a != b || a < 0;
-            } else if (mode == GT_GROUP_BATCH) {
-                if (n_systems > 1) {
-                    // a window never spans two systems of a forest; over all live targets the
-                    // windows of each system start at its first particle, as in its own tree
-                    const int s = system_of(sys_off, n_systems, pos);
-                    start = s != system_of(sys_off, n_systems, rank[targets[k - 1]]) ||
-                            (all_live ? ((int64_t)pos - sys_off[s]) % param == 0 : (k % param) == 0);
-                } else {
-                    start = (k % param) == 0;
-                }
-            } else {
-                start = true;
-            }
-        }
-        flag[k] = start ? 1u : 0u;
+         k += (int64_t)gridDim.x * blockDim.x)
+        flag[k] = target_starts(targets, k, mode, param, rank, leaf_of, gid, tpos, sys_off, n_systems, all_live)
+                      ? 1u : 0u;
+}
+
+// Small explicit target lists (the sparse active sets of deep time bins) form their groups in one
+// block, in one launch: flags, an ordered compaction of the group starts into shared memory, then
+// the chunking of groups longer than kmax.  count[0] = groups, count[1] = chunks, as
+// finish_groups_dev leaves them; the walk reads count[1].
+constexpr int kSmallTargets = 8192;
+constexpr int kSmallThreads = 1024;
+
+// Exclusive scan of one value per thread over the 1024-thread block; *total gets the sum.
+__device__ __forceinline__ int block_excl_scan_1024(int v, int* wsum, int* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += t;
     }
+    if (lane == 31) wsum[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        const int x = wsum[lane];
+        int y = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(kFull, y, o);
+            if (lane >= o) y += t;
+        }
+        wsum[lane] = y - x;
+        if (lane == 31) *total = y;
+    }
+    __syncthreads();
+    const int r = inc - v + wsum[w];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kSmallThreads)
+small_groups_kernel(const uint32_t* __restrict__ targets, int nt, int mode, int param,
+                    const uint32_t* __restrict__ rank, const int* __restrict__ leaf_of,
+                    const int* __restrict__ gid, uint32_t* __restrict__ tpos,
+                    const int* __restrict__ sys_off, int n_systems, int kmax,
+                    int2* __restrict__ groups, uint32_t* __restrict__ count) {
+    __shared__ int starts[kSmallTargets + 1];
+    __shared__ int wsum[32];
+    __shared__ int total;
+    int ng = 0;
+    for (int base = 0; base < nt; base += kSmallThreads) {
+        const int k = base + (int)threadIdx.x;
+        const bool st = k < nt && target_starts(targets, k, mode, param, rank, leaf_of, gid, tpos, sys_off,
+                                                n_systems, 0);
+        const int at = block_excl_scan_1024(st ? 1 : 0, wsum, &total);
+        if (st) starts[ng + at] = k;
+        ng += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) starts[ng] = nt;
+    __syncthreads();
+    int nc = 0;
+    for (int base = 0; base < ng; base += kSmallThreads) {
+        const int gi = base + (int)threadIdx.x;
+        const int s = gi < ng ? starts[gi] : 0, e = gi < ng ? starts[gi + 1] : 0;
+        const int c = gi < ng ? (e - s + kmax - 1) / kmax : 0;
+        int o = nc + block_excl_scan_1024(c, wsum, &total);
+        for (int a = s; a < e; a += kmax, ++o) groups[o] = make_int2(a, min(a + kmax, e));
+        nc += total;
+    }
+    if (threadIdx.x == 0) { count[0] = (uint32_t)ng; count[1] = (uint32_t)nc; }
 }
 
 __global__ void compact_starts_kernel(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos,
@@ -1298,13 +1372,22 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                                                                           param, gid);
             check_launch(ctx, "fill_group_id_kernel");
         }
-        target_flags_kernel<<<grid1d(ctx, nt), 256, 0, st>>>(rq.targets, nt, mode, param, t->rank,
-                                                             t->leaf_of, gid, tp, flag, t->sys_off_dev,
-                                                             t->n_systems, 0);
-        check_launch(ctx, "target_flags_kernel");
         // every chunk holds at least one target: nt bounds the count, which the walk reads on the
         // device, so the call needs no read-back before the walk
-        groups = finish_groups_dev(ctx, flag, nt, kmax, &ng_dev);
+        if (nt <= kSmallTargets) {
+            uint32_t* gc = (uint32_t*)scratch(ctx, kSlotGroupCount, 64);
+            groups = (int2*)scratch(ctx, kSlotGroupsB, (size_t)nt * sizeof(int2));
+            small_groups_kernel<<<1, kSmallThreads, 0, st>>>(rq.targets, (int)nt, mode, param, t->rank, t->leaf_of,
+                                                             gid, tp, t->sys_off_dev, t->n_systems, kmax, groups, gc);
+            check_launch(ctx, "small_groups_kernel");
+            ng_dev = gc + 1;
+        } else {
+            target_flags_kernel<<<grid1d(ctx, nt), 256, 0, st>>>(rq.targets, nt, mode, param, t->rank,
+                                                                 t->leaf_of, gid, tp, flag, t->sys_off_dev,
+                                                                 t->n_systems, 0);
+            check_launch(ctx, "target_flags_kernel");
+            groups = finish_groups_dev(ctx, flag, nt, kmax, &ng_dev);
+        }
         ng = nt;
         tpos = tp;
         if (t->n_systems > 1) {

@@ -528,3 +528,26 @@ def test_walks_and_searches_from_several_threads(gpu_ctx):
             for a, b in zip(w, ref_w):
                 assert np.array_equal(a, b)
             assert np.array_equal(s[0], ref_s[0]) and np.array_equal(s[1], ref_s[1])
+
+
+def test_small_target_lists_group_in_one_launch(gpu_ctx, plummer_trees):
+    """Up to 8192 explicit targets form their groups in one block (the sparse active sets of deep
+    time bins); longer lists take the multi-kernel path.  Across the threshold the groups and the
+    forces are the same: the first 8192 targets walked alone (one launch) and as the head of 8193
+    targets (the scan path) agree bit for bit, for windows of 32 and for leaf groups (all groups
+    but the last, which the 8193rd target may extend)."""
+    T, O = plummer_trees
+    ob = O.order()[0]
+    aold = 0.0025 * np.ones(len(ob))
+    a = gpu_ctx.accel_grouped(T, ob[:8192], aold=aold[:8192], batch=32, group_mode=g.GT_GROUP_BATCH)
+    b = gpu_ctx.accel_grouped(T, ob[:8193], aold=aold[:8193], batch=32, group_mode=g.GT_GROUP_BATCH)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v[:8192])
+    leaf = O.order()[2][ob]
+    head = int(np.nonzero(leaf[:8192] != leaf[8191])[0][-1]) + 1  # first target of the last group
+    a = gpu_ctx.accel_grouped(T, ob[:8192], aold=aold[:8192], batch=0, count=True)
+    ga = gpu_ctx.stats()["groups"]
+    b = gpu_ctx.accel_grouped(T, ob[:8193], aold=aold[:8193], batch=0)
+    for u, v in zip(a, b):
+        assert np.array_equal(u[:head], v[:head])
+    assert ga == 1 + int(np.count_nonzero(leaf[1:8192] != leaf[:8191]))

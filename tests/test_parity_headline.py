@@ -145,3 +145,46 @@ def test_parity_sparse_active_galaxy_4m():
               f"p99 {np.quantile(e, 0.99):.2e}")
         assert np.median(e) <= MEDIAN_TOL and np.quantile(e, 0.99) <= P99_TOL
     ctx.close()
+
+
+def test_parity_tidal_jerk_galaxy_4m():
+    """The tidal tensor and the jerk (shmem::accel_grouped's `tidal` and `jerk`, tree.cc:811-880)
+    at full size: the 4M galaxy with seeded velocities, windows of 32 in GPU tree order, against the
+    reference's own extended walk on a tree built with the same velocities (tree.cc:149-190).
+    Per target, the Frobenius norm of the difference over the reference's norm: median <= 1e-5."""
+    import torch
+    from oracle import Reference, reference_available
+
+    if not reference_available():
+        pytest.skip("oracle/_ref not built")
+    P = ics.galaxy(seed=2)
+    rng = np.random.default_rng(21)
+    vel = [0.1 * rng.standard_normal(len(P["m"])) for _ in range(3)]
+    ctx = g.Context(0)
+    dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
+    T = ctx.build(dev)
+    ctx.tree_velocities(T, *vel)
+    nl = T.info()["n_live"]
+    ob = T.download(nodes=False)["orderbuf"]
+    out = tuple(torch.empty(nl, dtype=torch.float64, device="cuda") for _ in range(3))
+    ctx.accel_grouped(T, None, theta=0.7, batch=WINDOW, outs=out + (None,), group_mode=g.GT_GROUP_BATCH)
+    aold = ctx.form_aold(*out, 0.0025).cpu().numpy()
+    w = np.sort(np.random.default_rng(22).choice(nl // WINDOW, size=256, replace=False))
+    pos = (w[:, None] * WINDOW + np.arange(WINDOW)[None, :]).ravel()
+    tg = ob[pos].astype(np.uint32)
+    ax, ay, az, _, tt, jj = ctx.accel_grouped_ext(T, tg, aold=aold[pos], batch=WINDOW, tidal=True, jerk=True,
+                                                  group_mode=g.GT_GROUP_BATCH)
+    ctx.close()
+    R = Reference()
+    R.set_threads(R.max_threads())
+    RT = R.build(P, vel=vel)
+    rx, ry, rz, rt, rj = RT.accel_grouped_ext(tg, 0.0, 1.0, WINDOW, aold=aold[pos], tidal=True, jerk=True)
+    ea = relerr((ax, ay, az), (rx, ry, rz))
+    et = np.linalg.norm(tt - rt, axis=1) / np.linalg.norm(rt, axis=1)
+    ej = np.linalg.norm(jj - rj, axis=1) / np.linalg.norm(rj, axis=1)
+    print(f"galaxy_4m tidal/jerk, {len(tg)} targets: acceleration median {np.median(ea):.2e}; tidal median "
+          f"{np.median(et):.2e} p99 {np.quantile(et, 0.99):.2e}; jerk median {np.median(ej):.2e} "
+          f"p99 {np.quantile(ej, 0.99):.2e}")
+    for e in (ea, et, ej):
+        assert np.isfinite(e).all()
+        assert np.median(e) <= MEDIAN_TOL and np.quantile(e, 0.99) <= P99_TOL
