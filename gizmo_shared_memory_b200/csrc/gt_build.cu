@@ -306,23 +306,85 @@ __device__ __forceinline__ int lower_bound_digit(const uint64_t* __restrict__ ke
     return lo;
 }
 
-__global__ void split_kernel(GNode* __restrict__ nodes, const uint64_t* __restrict__ skey,
-                             int64_t a, int64_t b, int level, int max_level, int leaf_max,
-                             int* __restrict__ bnd, uint32_t* __restrict__ nchild) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= b - a) return;
-    const GNode& nd = nodes[a + t];
-    const int lo = nd.plo, hi = nd.phi;
-    int cnt = 0;
-    int* B = bnd + t * 9;
-    if (!(hi - lo <= leaf_max || level >= max_level)) {
-        const int shift = 3 * (max_level - level - 1);
-        B[0] = lo;
-        for (unsigned v = 1; v < 8; ++v) B[v] = lower_bound_digit(skey, B[v - 1], hi, shift, v);
-        B[8] = hi;
-        for (int v = 0; v < 8; ++v) cnt += (B[v + 1] > B[v]);
+// The level array of the structure stage on the device: level starts lv[L], level counts
+// lv[kLvCount + L], and the overflow flag lv[2 * kLvCount].
+constexpr int kLvCount = 32;
+
+// Deepest level at which the build splits a cell, from the sorted keys alone: particles i and
+// i + leaf_max share their top d digits exactly when they share a level-d cell, which then holds
+// more than leaf_max particles and splits (below max_level).  So the deepest split level is the
+// largest such d over i, capped at max_level - 1; -1 when nothing splits.  A forest's keys are
+// compared across system boundaries too, which can only deepen the estimate (the extra levels are
+// then empty).
+__global__ void split_depth_kernel(const uint64_t* __restrict__ skey, int64_t n_live, int leaf_max,
+                                   int max_level, int* __restrict__ depth) {
+    int d = -1;
+    const int pad = 64 - 3 * max_level;  // key bits above the 3 * max_level used ones
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i + leaf_max < n_live;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t x = skey[i] ^ skey[i + leaf_max];
+        const int common = x == 0 ? max_level : (__clzll((long long)x) - pad) / 3;
+        d = max(d, min(common, max_level - 1));
     }
-    nchild[t] = (uint32_t)cnt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d = max(d, __shfl_xor_sync(0xffffffffu, d, o));
+    if ((threadIdx.x & 31) == 0 && d >= 0) atomicMax(depth, d);
+}
+
+// Child boundaries of a level's nodes, eight lanes per node: lane v finds where digit v starts in
+// the node's sorted keys (one binary search each, in parallel, where a single thread would run
+// seven in sequence), the eight lanes count the non-empty octants.  bnd holds nine boundaries per
+// node (the octant ranges [B[v], B[v+1])), nchild the count (0 for a node that stays a leaf).  The
+// level's range comes from lv when given (device-side levels), else from [a, b).
+__global__ void split_kernel(const GNode* __restrict__ nodes, const uint64_t* __restrict__ skey,
+                             int64_t a, int64_t b, int level, int max_level, int leaf_max,
+                             int* __restrict__ bnd, uint32_t* __restrict__ nchild,
+                             const int64_t* __restrict__ lv = nullptr) {
+    if (lv) { a = lv[level]; b = a + lv[kLvCount + level]; }
+    const int lane = threadIdx.x & 31, sub = lane & 7;
+    const int64_t cnt = b - a;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4; base < cnt;
+         base += warps * 4) {
+        const int64_t t = base + (lane >> 3);
+        const bool live = t < cnt;
+        int lo = 0, hi = 0;
+        if (live) { lo = nodes[a + t].plo; hi = nodes[a + t].phi; }
+        const bool split = live && !(hi - lo <= leaf_max || level >= max_level);
+        int bv = lo;
+        if (split && sub > 0) bv = lower_bound_digit(skey, lo, hi, 3 * (max_level - level - 1), (unsigned)sub);
+        int nx = __shfl_down_sync(0xffffffffu, bv, 1, 8);
+        if (sub == 7) nx = hi;
+        int c = (split && nx > bv) ? 1 : 0;
+        c += __shfl_xor_sync(0xffffffffu, c, 1, 8);
+        c += __shfl_xor_sync(0xffffffffu, c, 2, 8);
+        c += __shfl_xor_sync(0xffffffffu, c, 4, 8);
+        if (split) {
+            int* B = bnd + t * 9;
+            B[sub] = bv;
+            if (sub == 7) B[8] = hi;
+        }
+        if (live && sub == 0) nchild[t] = (uint32_t)c;
+    }
+}
+
+// After the scan of level L's child counts: level L+1 starts where L ends and holds `total` nodes,
+// unless that overruns the node arrays; then the overflow flag is set, nothing more is emitted and
+// the host redoes the stage one level at a time, growing the arrays.
+__global__ void advance_level_kernel(int64_t* __restrict__ lv, int level, const uint32_t* __restrict__ total,
+                                     int64_t node_cap) {
+    int64_t* cnt = lv + kLvCount;
+    int64_t* ovf = lv + 2 * kLvCount;
+    const int64_t b = lv[level] + cnt[level];
+    int64_t tot = *ovf ? 0 : (int64_t)*total;
+    if (b + tot > node_cap) { *ovf = 1; tot = 0; }
+    lv[level + 1] = b;
+    cnt[level + 1] = tot;
+}
+
+__global__ void init_levels_kernel(int64_t* __restrict__ lv, int64_t n_roots) {
+    for (int i = 0; i <= 2 * kLvCount; ++i) lv[i] = 0;
+    lv[kLvCount] = n_roots;  // level 0: the roots [0, n_roots)
 }
 
 __global__ void emit_kernel(GNode* __restrict__ nodes, const SrcP* __restrict__ src,
@@ -331,46 +393,53 @@ __global__ void emit_kernel(GNode* __restrict__ nodes, const SrcP* __restrict__ 
                             const uint32_t* __restrict__ nchild, const uint32_t* __restrict__ coff,
                             int* __restrict__ parent, int* __restrict__ next, int* __restrict__ lvl,
                             double* __restrict__ size, double* __restrict__ gc,
-                            const int* __restrict__ sys_off, int n_systems) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= b - a) return;
-    const int64_t i = a + t;
-    const int nc = (int)nchild[t];
-    if (nc == 0) {
-        nodes[i].first = -1;
-        nodes[i].nchild = 0;
-        return;
+                            const int* __restrict__ sys_off, int n_systems,
+                            const int64_t* __restrict__ lv = nullptr) {
+    if (lv) {
+        if (lv[2 * kLvCount] != 0) return;  // the node arrays overflowed: the host redoes the stage
+        a = lv[level];
+        b = a + lv[kLvCount + level];
     }
-    const RootGeom g = gp[n_systems > 1 ? system_of(sys_off, n_systems, nodes[i].plo) : 0];
-    const int first = (int)(b + coff[t]);
-    nodes[i].first = first;
-    nodes[i].nchild = nc;
-    const int* B = bnd + t * 9;
-    const double sz = size[i], half = sz * 0.5, quarter = sz * 0.25;
-    const double pcx = gc[3 * i], pcy = gc[3 * i + 1], pcz = gc[3 * i + 2];
-    const int pnext = next[i];
     const int bit = max_level - 1 - level;  // coordinate bit that selects the octant at this level
-    int k = 0;
-    for (int v = 0; v < 8; ++v) {
-        if (B[v + 1] <= B[v]) continue;
-        const int c = first + k;
-        const SrcP& s0 = src[B[v]];
-        uint32_t qa, qb, qc;
-        quantise(g, s0.x, s0.y, s0.z, qa, qb, qc);
-        const int oct = (int)((qa >> bit) & 1u) | (int)(((qb >> bit) & 1u) << 1) | (int)(((qc >> bit) & 1u) << 2);
-        GNode& ch = nodes[c];
-        ch.plo = B[v];
-        ch.phi = B[v + 1];
-        ch.first = -1;
-        ch.nchild = 0;
-        parent[c] = (int)i;
-        lvl[c] = level + 1;
-        size[c] = half;
-        gc[3 * c] = pcx + ((oct & 1) ? quarter : -quarter);
-        gc[3 * c + 1] = pcy + ((oct & 2) ? quarter : -quarter);
-        gc[3 * c + 2] = pcz + ((oct & 4) ? quarter : -quarter);
-        next[c] = (k + 1 < nc) ? c + 1 : pnext;
-        ++k;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < b - a;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = a + t;
+        const int nc = (int)nchild[t];
+        if (nc == 0) {
+            nodes[i].first = -1;
+            nodes[i].nchild = 0;
+            continue;
+        }
+        const RootGeom g = gp[n_systems > 1 ? system_of(sys_off, n_systems, nodes[i].plo) : 0];
+        const int first = (int)(b + coff[t]);
+        nodes[i].first = first;
+        nodes[i].nchild = nc;
+        const int* B = bnd + t * 9;
+        const double sz = size[i], half = sz * 0.5, quarter = sz * 0.25;
+        const double pcx = gc[3 * i], pcy = gc[3 * i + 1], pcz = gc[3 * i + 2];
+        const int pnext = next[i];
+        int k = 0;
+        for (int v = 0; v < 8; ++v) {
+            if (B[v + 1] <= B[v]) continue;
+            const int c = first + k;
+            const SrcP& s0 = src[B[v]];
+            uint32_t qa, qb, qc;
+            quantise(g, s0.x, s0.y, s0.z, qa, qb, qc);
+            const int oct = (int)((qa >> bit) & 1u) | (int)(((qb >> bit) & 1u) << 1) | (int)(((qc >> bit) & 1u) << 2);
+            GNode& ch = nodes[c];
+            ch.plo = B[v];
+            ch.phi = B[v + 1];
+            ch.first = -1;
+            ch.nchild = 0;
+            parent[c] = (int)i;
+            lvl[c] = level + 1;
+            size[c] = half;
+            gc[3 * c] = pcx + ((oct & 1) ? quarter : -quarter);
+            gc[3 * c + 1] = pcy + ((oct & 2) ? quarter : -quarter);
+            gc[3 * c + 2] = pcz + ((oct & 4) ? quarter : -quarter);
+            next[c] = (k + 1 < nc) ? c + 1 : pnext;
+            ++k;
+        }
     }
 }
 
@@ -810,7 +879,62 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
     t->lvl_off.assign(1, 0);
     t->lvl_off.push_back(S);
     uint32_t* total_dev = (uint32_t*)(bad_dev + 2);
-    for (int L = 0;; ++L) {
+    // The tree's depth comes from the sorted keys (one read-back); then every level runs on the
+    // device with its offsets and counts in a small device array, each kernel reading its level's
+    // range from it and sized for the widest level the node arrays hold, and one read-back at the
+    // end.  If the levels outgrow the node arrays the kernels stop emitting and the stage is redone
+    // below one level at a time, growing the arrays as it goes.
+    bool structured = false;
+    if (nl > 0 && o.max_level + 2 < kLvCount) {
+        int* depth = (int*)(bad_dev + 3);
+        check_cuda(cudaMemsetAsync(depth, 0xff, 4, st), "memset");  // -1: nothing splits
+        split_depth_kernel<<<grid_for(ctx, nl), kBlk, 0, st>>>(t->skey, nl, o.leaf_max, o.max_level, depth);
+        check_launch(ctx, "split_depth_kernel");
+        int dmax = -1;
+        check_cuda(cudaMemcpyAsync(ctx->pinned, depth, 4, cudaMemcpyDeviceToHost, st), "depth d2h");
+        check_cuda(cudaStreamSynchronize(st), "sync");
+        std::memcpy(&dmax, ctx->pinned, 4);
+        const int64_t cap = t->node_cap;
+        int64_t* lv = (int64_t*)scratch(ctx, kSlotLevels, (2 * kLvCount + 1) * sizeof(int64_t));
+        int* bnd = (int*)scratch(ctx, kSlotNodeTmp0, (size_t)cap * 9 * 4);
+        uint32_t* nch = (uint32_t*)scratch(ctx, kSlotNodeTmp1, (size_t)cap * 4);
+        uint32_t* coff = (uint32_t*)scratch(ctx, kSlotNodeTmp2, (size_t)cap * 4);
+        init_levels_kernel<<<1, 1, 0, st>>>(lv, S);
+        check_launch(ctx, "init_levels_kernel");
+        const int g_split = grid_for(ctx, cap * 8), g_emit = grid_for(ctx, cap);
+        for (int L = 0; L <= dmax; ++L) {
+            split_kernel<<<g_split, kBlk, 0, st>>>(t->nodes, t->skey, 0, 0, L, o.max_level, o.leaf_max, bnd, nch, lv);
+            check_launch(ctx, "split_kernel");
+            scan_exclusive_u32(ctx, nch, coff, cap, total_dev, lv + kLvCount + L);
+            advance_level_kernel<<<1, 1, 0, st>>>(lv, L, total_dev, cap);
+            check_launch(ctx, "advance_level_kernel");
+            emit_kernel<<<g_emit, kBlk, 0, st>>>(t->nodes, t->src, gdev, 0, 0, L, o.max_level, bnd, nch, coff,
+                                                 t->parent, t->next, t->level, t->size, t->gc, t->sys_off_dev, S, lv);
+            check_launch(ctx, "emit_kernel");
+        }
+        // the deepest level's nodes are all leaves: mark them (emit writes first/nchild of its level)
+        const int Lz = dmax + 1;
+        if (Lz + 1 < kLvCount) {
+            split_kernel<<<g_split, kBlk, 0, st>>>(t->nodes, t->skey, 0, 0, Lz, o.max_level, o.leaf_max, bnd, nch, lv);
+            check_launch(ctx, "split_kernel");
+            scan_exclusive_u32(ctx, nch, coff, cap, total_dev, lv + kLvCount + Lz);
+            advance_level_kernel<<<1, 1, 0, st>>>(lv, Lz, total_dev, cap);
+            check_launch(ctx, "advance_level_kernel");
+            emit_kernel<<<g_emit, kBlk, 0, st>>>(t->nodes, t->src, gdev, 0, 0, Lz, o.max_level, bnd, nch, coff,
+                                                 t->parent, t->next, t->level, t->size, t->gc, t->sys_off_dev, S, lv);
+            check_launch(ctx, "emit_kernel");
+        }
+        int64_t h[2 * kLvCount + 1];
+        check_cuda(cudaMemcpyAsync(ctx->pinned, lv, sizeof(h), cudaMemcpyDeviceToHost, st), "levels d2h");
+        check_cuda(cudaStreamSynchronize(st), "sync");
+        std::memcpy(h, ctx->pinned, sizeof(h));
+        // sound only if nothing overflowed and the level after the last one run is empty
+        if (h[2 * kLvCount] == 0 && (Lz + 1 >= kLvCount || h[kLvCount + Lz + 1] == 0)) {
+            for (int L = 1; L < kLvCount && h[kLvCount + L] > 0; ++L) t->lvl_off.push_back(h[L] + h[kLvCount + L]);
+            structured = true;
+        }
+    }
+    for (int L = 0; !structured; ++L) {
         const int64_t a = t->lvl_off[L], b = t->lvl_off[L + 1];
         const int64_t cnt_l = b - a;
         if (cnt_l <= 0) break;
@@ -819,8 +943,8 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
         int* bnd = (int*)scratch(ctx, kSlotNodeTmp0, (size_t)wmax * 9 * 4);
         uint32_t* nch = (uint32_t*)scratch(ctx, kSlotNodeTmp1, (size_t)wmax * 4);
         uint32_t* coff = (uint32_t*)scratch(ctx, kSlotNodeTmp2, (size_t)wmax * 4);
-        split_kernel<<<div_up(cnt_l, kBlk), kBlk, 0, st>>>(t->nodes, t->skey, a, b, L, o.max_level,
-                                                           o.leaf_max, bnd, nch);
+        split_kernel<<<div_up(cnt_l * 8, kBlk), kBlk, 0, st>>>(t->nodes, t->skey, a, b, L, o.max_level,
+                                                               o.leaf_max, bnd, nch);
         check_launch(ctx, "split_kernel");
         scan_exclusive_u32(ctx, nch, coff, cnt_l, total_dev);
         uint32_t total = 0;

@@ -191,6 +191,7 @@ enum Slot {
     kSlotNgb0, kSlotNgb1, kSlotNgb2,
     kSlotStack2,  // traversal stacks of the second compute stream (chunked walks)
     kSlotGroupCount,  // device-side group and chunk counts of an explicit-target walk
+    kSlotLevels,      // device-side level offsets and counts of the build's structure stage
     kSlotCount
 };
 
@@ -210,8 +211,10 @@ inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 // Device-wide helpers (gt_scan.cu).
 // Exclusive scan of n uint32 values into out (may alias in); returns nothing, total written to
 // total_dev[0] when total_dev is non-null.
+// n_dev (optional): the number of items, on the device, at most n; the launch is sized by n, so
+// the host needs no read-back of the count.
 void scan_exclusive_u32(gt_context* ctx, const uint32_t* in, uint32_t* out, int64_t n,
-                        uint32_t* total_dev);
+                        uint32_t* total_dev, const int64_t* n_dev = nullptr);
 // Stable LSD radix sort of (key, value) pairs over the low `bits` bits of the key.
 void radix_sort_pairs(gt_context* ctx, uint64_t* keys, uint32_t* vals, int64_t n, int bits);
 

@@ -46,7 +46,10 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* total)
     return res;
 }
 
-__global__ void tile_sum_kernel(const uint32_t* __restrict__ in, int64_t n, uint32_t* __restrict__ sums) {
+// n_dev (optional): the number of items, on the device, at most n (the launch is sized by n).
+__global__ void tile_sum_kernel(const uint32_t* __restrict__ in, int64_t n, uint32_t* __restrict__ sums,
+                                const int64_t* __restrict__ n_dev) {
+    if (n_dev) n = min(n, *n_dev);
     const int64_t base = (int64_t)blockIdx.x * kScanTile;
     uint32_t s = 0;
 #pragma unroll
@@ -60,7 +63,9 @@ __global__ void tile_sum_kernel(const uint32_t* __restrict__ in, int64_t n, uint
 }
 
 // One block scans all tile totals in place (exclusive); total to total_out.
-__global__ void scan_sums_kernel(uint32_t* __restrict__ sums, int nb, uint32_t* __restrict__ total_out) {
+__global__ void scan_sums_kernel(uint32_t* __restrict__ sums, int nb, uint32_t* __restrict__ total_out,
+                                 const int64_t* __restrict__ n_dev) {
+    if (n_dev) nb = (int)min((int64_t)nb, (*n_dev + kScanTile - 1) / kScanTile);
     const int per = (nb + blockDim.x - 1) / blockDim.x;
     const int lo = threadIdx.x * per, hi = min(nb, lo + per);
     uint32_t s = 0;
@@ -78,7 +83,9 @@ __global__ void scan_sums_kernel(uint32_t* __restrict__ sums, int nb, uint32_t* 
 // Blocked arrangement inside the tile: thread t owns items [t*8, t*8+8) so the scan order is the
 // index order.
 __global__ void tile_scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int64_t n,
-                                 const uint32_t* __restrict__ sums) {
+                                 const uint32_t* __restrict__ sums, const int64_t* __restrict__ n_dev) {
+    if (n_dev) n = min(n, *n_dev);
+    if ((int64_t)blockIdx.x * kScanTile >= n) return;  // the whole block lies past the items
     const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
     uint32_t s = 0;
@@ -210,18 +217,18 @@ radix_scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restric
 }  // namespace
 
 void scan_exclusive_u32(gt_context* ctx, const uint32_t* in, uint32_t* out, int64_t n,
-                        uint32_t* total_dev) {
+                        uint32_t* total_dev, const int64_t* n_dev) {
     if (n <= 0) {
         if (total_dev) check_cuda(cudaMemsetAsync(total_dev, 0, 4, ctx->stream), "memset");
         return;
     }
     const int nb = div_up(n, kScanTile);
     uint32_t* sums = (uint32_t*)scratch(ctx, kSlotScanB, (size_t)nb * 4);
-    tile_sum_kernel<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, sums);
+    tile_sum_kernel<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, sums, n_dev);
     check_launch(ctx, "tile_sum_kernel");
-    scan_sums_kernel<<<1, 1024, 0, ctx->stream>>>(sums, nb, total_dev);
+    scan_sums_kernel<<<1, 1024, 0, ctx->stream>>>(sums, nb, total_dev, n_dev);
     check_launch(ctx, "scan_sums_kernel");
-    tile_scan_kernel<<<nb, kScanThreads, 0, ctx->stream>>>(in, out, n, sums);
+    tile_scan_kernel<<<nb, kScanThreads, 0, ctx->stream>>>(in, out, n, sums, n_dev);
     check_launch(ctx, "tile_scan_kernel");
 }
 

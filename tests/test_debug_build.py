@@ -15,6 +15,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 CHILD = r"""
 import os, sys
+ROOT = sys.argv[1]
 import numpy as np
 sys.path.insert(0, ROOT)
 import gizmo_shared_memory_b200 as g
@@ -55,8 +56,7 @@ def test_bounds_checked_library_runs_clean_and_identical():
     dbg = os.path.join(ROOT, "gizmo_shared_memory_b200", "lib", "libgt_debug.so")
     if not os.path.exists(dbg):
         pytest.fail("libgt_debug.so not built (make -C gizmo_shared_memory_b200/csrc debug)")
-    r = subprocess.run([sys.executable, "-c", CHILD.replace("ROOT", repr(ROOT), 1)], capture_output=True,
-                       text=True, timeout=600)
+    r = subprocess.run([sys.executable, "-c", CHILD, ROOT], capture_output=True, text=True, timeout=600)
     print(r.stdout, r.stderr[-2000:])
     assert r.returncode == 0
     assert "identical" in r.stdout
