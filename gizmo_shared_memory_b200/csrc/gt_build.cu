@@ -124,12 +124,18 @@ __device__ void finish_root(const double* lo, const double* hi, unsigned long lo
     g->n_live = (long long)live;
 }
 
-__global__ void root_geom_kernel(const double* __restrict__ part, const unsigned long long* __restrict__ cnt,
-                                 int nb, RootGeom* __restrict__ g, unsigned long long* __restrict__ bad_out,
-                                 long long seed, double fx, double fy, double fz, int max_level) {
+// One block combines the partial boxes and counts (minimum, maximum and integer sums are exact in
+// any order, so the root cell does not depend on the block shape), then thread 0 finishes the root.
+constexpr int kRootThreads = 256;
+__global__ void __launch_bounds__(kRootThreads)
+root_geom_kernel(const double* __restrict__ part, const unsigned long long* __restrict__ cnt,
+                 int nb, RootGeom* __restrict__ g, unsigned long long* __restrict__ bad_out,
+                 long long seed, double fx, double fy, double fz, int max_level) {
+    __shared__ double sh[6][kRootThreads];
+    __shared__ unsigned long long sc[2][kRootThreads];
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     unsigned long long live = 0, bad = 0;
-    for (int b = 0; b < nb; ++b) {
+    for (int b = threadIdx.x; b < nb; b += kRootThreads) {
         for (int c = 0; c < 3; ++c) {
             lo[c] = fmin(lo[c], part[b * 6 + c]);
             hi[c] = fmax(hi[c], part[b * 6 + 3 + c]);
@@ -137,8 +143,26 @@ __global__ void root_geom_kernel(const double* __restrict__ part, const unsigned
         live += cnt[b * 2];
         bad += cnt[b * 2 + 1];
     }
-    finish_root(lo, hi, live, g, seed, fx, fy, fz, max_level);
-    *bad_out = bad;
+    for (int c = 0; c < 3; ++c) { sh[c][threadIdx.x] = lo[c]; sh[3 + c][threadIdx.x] = hi[c]; }
+    sc[0][threadIdx.x] = live;
+    sc[1][threadIdx.x] = bad;
+    __syncthreads();
+    for (int o = kRootThreads / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            for (int c = 0; c < 3; ++c) {
+                sh[c][threadIdx.x] = fmin(sh[c][threadIdx.x], sh[c][threadIdx.x + o]);
+                sh[3 + c][threadIdx.x] = fmax(sh[3 + c][threadIdx.x], sh[3 + c][threadIdx.x + o]);
+            }
+            sc[0][threadIdx.x] += sc[0][threadIdx.x + o];
+            sc[1][threadIdx.x] += sc[1][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < 3; ++c) { lo[c] = sh[c][0]; hi[c] = sh[3 + c][0]; }
+        finish_root(lo, hi, sc[0][0], g, seed, fx, fy, fz, max_level);
+        *bad_out = sc[1][0];
+    }
 }
 
 // Forest: `chunks` blocks per system each reduce a slice of that system's input range into a
@@ -754,7 +778,7 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
         unsigned long long* cnt = (unsigned long long*)(part + (size_t)nbb * 6);
         bbox_partial_kernel<<<nbb, kBlk, 0, st>>>(x, y, z, m, bbox_soft, n, part, cnt);
         check_launch(ctx, "bbox_partial_kernel");
-        root_geom_kernel<<<1, 1, 0, st>>>(part, cnt, nbb, gdev, bad_dev, o.randomize_seed, o.shift[0],
+        root_geom_kernel<<<1, kRootThreads, 0, st>>>(part, cnt, nbb, gdev, bad_dev, o.randomize_seed, o.shift[0],
                                           o.shift[1], o.shift[2], o.max_level);
         check_launch(ctx, "root_geom_kernel");
     } else {
