@@ -491,7 +491,7 @@ def run_gpu_arm(args):
     # --split targets (N > 1): one system, every rank builds the same tree and walks its
     # window-aligned slice of the tree order (sharding.walk_shard); --split systems: one
     # independent system per rank
-    split = world > 1 and args.split == "targets"
+    split = args.split == "targets" and (world > 1 or args.shard_check)
     P = make_workload(args.workload, seed_offset=0 if split else rank)
     n = len(P["m"])
     dev = {k: torch.as_tensor(v, device="cuda") for k, v in P.items()}
@@ -1182,6 +1182,9 @@ def main():
     ap.add_argument("--split", choices=["targets", "systems"], default="targets",
                     help="N > 1: targets = one system, every rank walks a window-aligned slice of its "
                          "tree order; systems = one independent system per rank")
+    ap.add_argument("--shard-check", action="store_true",
+                    help="run the --split targets path at N = 1 too (one slice holding every target), to "
+                         "check it against the ordinary walk on one GPU")
     ap.add_argument("--key", choices=["peano", "morton"], default="peano",
                     help="sort key of the tree: the window order of --group batch")
     ap.add_argument("--sample-seconds", type=float, default=8.0)
