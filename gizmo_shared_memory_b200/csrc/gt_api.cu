@@ -214,13 +214,8 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     const int64_t nt = all ? tree->n_live : n_targets;
     const int64_t nout = (all && o.out_order == GT_OUT_ORIGINAL) ? tree->n : nt;
     if (!all && nt > 0 && !targets) throw Fail{GT_ERR_INVALID, "targets is null"};
-    if (!all) {
-        // host-side range check of target indices: a bad index would read out of bounds
-        if (mem == GT_MEM_HOST) {
-            for (int64_t k = 0; k < nt; ++k)
-                if ((int64_t)targets[k] >= tree->n) throw Fail{GT_ERR_INVALID, "target index out of range"};
-        }
-    }
+    // Target indices are range-checked on the device as the walk groups them (an index at or
+    // beyond the particle count is never dereferenced); a synchronising call reports it below.
     WalkRequest rq;
     rq.targets = all ? nullptr : stage_in(ctx, kSlotIn0, targets, nt, mem);
     rq.n_targets = nt;
@@ -287,6 +282,13 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     }
     const bool copied = run_walk(ctx, tree, rq);
     if (capture) return;
+    const bool sync_call = mem == GT_MEM_HOST || !o.async;
+    uint32_t* bad_host = reinterpret_cast<uint32_t*>(static_cast<char*>(ctx->pinned) + kPinnedTargetCheck);
+    if (!all && nt > 0 && sync_call) {
+        *bad_host = 0;
+        check_cuda(cudaMemcpyAsync(bad_host, (uint32_t*)scratch(ctx, kSlotGroupCount, 64) + 2, 4,
+                                   cudaMemcpyDeviceToHost, ctx->stream), "target check d2h");
+    }
     if (!copied) {
         copy_out(ctx, ax, rq.ax, nout, mem);
         copy_out(ctx, ay, rq.ay, nout, mem);
@@ -295,9 +297,10 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
         copy_out(ctx, tidal, rq.tidal, nout * 6, mem);
         copy_out(ctx, jerk, rq.jerk, nout * 3, mem);
     }
-    const bool sync = mem == GT_MEM_HOST || !o.async;
+    const bool sync = sync_call;
     finish(ctx, sync);
     if (sync) record_walk_time(ctx);
+    if (!all && nt > 0 && sync && *bad_host) throw Fail{GT_ERR_INVALID, "target index out of range"};
 }
 
 }  // namespace

@@ -91,7 +91,7 @@ struct gt_context {
     uint64_t launches = 0;
     gt_walk_stats stats{};
     std::vector<gt::DevBuf> scratch;  // grow-only workspace slots, indexed by gt::Slot
-    void* pinned = nullptr;           // small pinned host buffer for scalar read-backs
+    void* pinned = nullptr;           // small pinned host buffer for scalar read-backs (4096 B)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // host copies overlapped with the main stream's work (made on first use): a walk split into
     // chunks uploads each chunk's aold and copies its results back there; a build from host
@@ -178,6 +178,10 @@ struct gt_tree {
 };
 
 namespace gt {
+
+// Byte offset in gt_context::pinned of the out-of-range-target flag a walk reads back; the other
+// read-backs use the start of the buffer.
+constexpr size_t kPinnedTargetCheck = 4000;
 
 // Scratch slots of the context workspace.
 enum Slot {

@@ -894,23 +894,35 @@ __global__ void fill_group_id_kernel(const GNode* __restrict__ nodes, const int*
     }
 }
 
+// A target index as the grouping reads it: an index at or beyond the particle count sets *bad
+// (the call then fails with GT_ERR_INVALID) and reads particle 0 instead, so nothing is read out of
+// bounds; the check costs nothing on the host, which does not walk the target list.
+__device__ __forceinline__ uint32_t checked_target(const uint32_t* __restrict__ targets, int64_t k, int64_t n,
+                                                   unsigned* __restrict__ bad) {
+    const uint32_t p = targets[k];
+    if ((int64_t)p < n) return p;
+    if (bad) atomicOr(bad, 1u);
+    return 0u;
+}
+
 // Whether target k starts a group (a new group where the key changes or is negative); also
 // records its tree position.
 __device__ __forceinline__ bool target_starts(const uint32_t* __restrict__ targets, int64_t k, int mode,
                                               int param, const uint32_t* __restrict__ rank,
                                               const int* __restrict__ leaf_of, const int* __restrict__ gid,
                                               uint32_t* __restrict__ tpos, const int* __restrict__ sys_off,
-                                              int n_systems, int all_live) {
-    const uint32_t p = targets[k];
+                                              int n_systems, int all_live, int64_t n, unsigned* __restrict__ bad) {
+    const uint32_t p = checked_target(targets, k, n, bad);
     const uint32_t pos = rank[p];
     tpos[k] = pos;
     if (k == 0) return true;
+    const uint32_t q = checked_target(targets, k - 1, n, nullptr);  // reported at its own k
     if (mode == GT_GROUP_LEAF) {
-        const int a = leaf_of[p], b = leaf_of[targets[k - 1]];
+        const int a = leaf_of[p], b = leaf_of[q];
         return a != b || a < 0;
     }
     if (mode == GT_GROUP_NODE) {
-        const int a = gid[pos], b = gid[rank[targets[k - 1]]];
+        const int a = gid[pos], b = gid[rank[q]];
         return a != b || a < 0;
     }
     if (mode == GT_GROUP_BATCH) {
@@ -918,7 +930,7 @@ __device__ __forceinline__ bool target_starts(const uint32_t* __restrict__ targe
             // a window never spans two systems of a forest; over all live targets the windows of
             // each system start at its first particle, as in its own tree
             const int s = system_of(sys_off, n_systems, pos);
-            return s != system_of(sys_off, n_systems, rank[targets[k - 1]]) ||
+            return s != system_of(sys_off, n_systems, rank[q]) ||
                    (all_live ? ((int64_t)pos - sys_off[s]) % param == 0 : (k % param) == 0);
         }
         return (k % param) == 0;
@@ -930,11 +942,12 @@ __global__ void target_flags_kernel(const uint32_t* __restrict__ targets, int64_
                                     int param, const uint32_t* __restrict__ rank,
                                     const int* __restrict__ leaf_of, const int* __restrict__ gid,
                                     uint32_t* __restrict__ tpos, uint32_t* __restrict__ flag,
-                                    const int* __restrict__ sys_off, int n_systems, int all_live) {
+                                    const int* __restrict__ sys_off, int n_systems, int all_live,
+                                    int64_t n = INT64_MAX, unsigned* __restrict__ bad = nullptr) {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nt;
          k += (int64_t)gridDim.x * blockDim.x)
-        flag[k] = target_starts(targets, k, mode, param, rank, leaf_of, gid, tpos, sys_off, n_systems, all_live)
-                      ? 1u : 0u;
+        flag[k] = target_starts(targets, k, mode, param, rank, leaf_of, gid, tpos, sys_off, n_systems, all_live,
+                                n, bad) ? 1u : 0u;
 }
 
 // Small explicit target lists (the sparse active sets of deep time bins) form their groups in one
@@ -977,7 +990,8 @@ small_groups_kernel(const uint32_t* __restrict__ targets, int nt, int mode, int 
                     const uint32_t* __restrict__ rank, const int* __restrict__ leaf_of,
                     const int* __restrict__ gid, uint32_t* __restrict__ tpos,
                     const int* __restrict__ sys_off, int n_systems, int kmax,
-                    int2* __restrict__ groups, uint32_t* __restrict__ count) {
+                    int2* __restrict__ groups, uint32_t* __restrict__ count, int64_t n,
+                    unsigned* __restrict__ bad) {
     __shared__ int starts[kSmallTargets + 1];
     __shared__ int wsum[32];
     __shared__ int total;
@@ -985,7 +999,7 @@ small_groups_kernel(const uint32_t* __restrict__ targets, int nt, int mode, int 
     for (int base = 0; base < nt; base += kSmallThreads) {
         const int k = base + (int)threadIdx.x;
         const bool st = k < nt && target_starts(targets, k, mode, param, rank, leaf_of, gid, tpos, sys_off,
-                                                n_systems, 0);
+                                                n_systems, 0, n, bad);
         const int at = block_excl_scan_1024(st ? 1 : 0, wsum, &total);
         if (st) starts[ng + at] = k;
         ng += total;
@@ -1374,17 +1388,21 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         }
         // every chunk holds at least one target: nt bounds the count, which the walk reads on the
         // device, so the call needs no read-back before the walk
+        // gc[2]: set when a target index is out of range (read by the caller after the walk)
+        uint32_t* gc = (uint32_t*)scratch(ctx, kSlotGroupCount, 64);
+        check_cuda(cudaMemsetAsync(gc + 2, 0, 4, st), "memset");
+        unsigned* bad = gc + 2;
         if (nt <= kSmallTargets) {
-            uint32_t* gc = (uint32_t*)scratch(ctx, kSlotGroupCount, 64);
             groups = (int2*)scratch(ctx, kSlotGroupsB, (size_t)nt * sizeof(int2));
             small_groups_kernel<<<1, kSmallThreads, 0, st>>>(rq.targets, (int)nt, mode, param, t->rank, t->leaf_of,
-                                                             gid, tp, t->sys_off_dev, t->n_systems, kmax, groups, gc);
+                                                             gid, tp, t->sys_off_dev, t->n_systems, kmax, groups, gc,
+                                                             t->n, bad);
             check_launch(ctx, "small_groups_kernel");
             ng_dev = gc + 1;
         } else {
             target_flags_kernel<<<grid1d(ctx, nt), 256, 0, st>>>(rq.targets, nt, mode, param, t->rank,
                                                                  t->leaf_of, gid, tp, flag, t->sys_off_dev,
-                                                                 t->n_systems, 0);
+                                                                 t->n_systems, 0, t->n, bad);
             check_launch(ctx, "target_flags_kernel");
             groups = finish_groups_dev(ctx, flag, nt, kmax, &ng_dev);
         }

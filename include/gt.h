@@ -285,7 +285,11 @@ GT_API int gt_tree_audit(gt_context* ctx, const gt_tree* tree, int64_t* n_bad, c
  * sink-direct opening come from gt_tree_gas and gt_walk_options.sink_direct_radius.  batch <= 0 groups
  * targets by leaf, batch > 0 in fixed windows, unless opt->group_mode overrides it.
  * aold (may be NULL) is ErrTolForceAcc*|a_prev|/G per target (tree.h:389-391); theta > 0 adds the
- * Barnes-Hut test.  phi (may be NULL) receives the potential from the same walk. */
+ * Barnes-Hut test.  phi (may be NULL) receives the potential from the same walk.  Every targets[k]
+ * must be < n: the walk checks the indices on the device as it groups them and never reads past
+ * the particles; a call that synchronises (host arrays, or gt_walk_options.async = 0) then fails with
+ * GT_ERR_INVALID, while an asynchronous call cannot report it and leaves that target's outputs
+ * undefined. */
 GT_API int gt_accel_grouped(gt_context* ctx, const gt_tree* tree, int64_t n_targets,
                      const uint32_t* targets, const double* aold, double theta, double G, int batch,
                      const gt_walk_options* opt, int mem, double* ax, double* ay, double* az,

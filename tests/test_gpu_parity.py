@@ -387,6 +387,20 @@ def test_errors_leave_context_usable(gpu_ctx, plummer):
     with pytest.raises(g.GTError) as e:
         gpu_ctx.accel_grouped(T, np.array([10 ** 7], np.uint32), theta=0.7)
     assert e.value.status == 1  # GT_ERR_INVALID
+    # target indices are checked on the device while the walk groups them: a bad index in a long
+    # list (the multi-kernel grouping), from host and from device arrays, reads nothing out of
+    # bounds and fails the synchronising call
+    import torch
+
+    long = np.arange(20000, dtype=np.uint32)
+    long[12345] = len(P["m"]) + 3
+    with pytest.raises(g.GTError) as e:
+        gpu_ctx.accel_grouped(T, long, theta=0.7)
+    assert e.value.status == 1
+    with pytest.raises(g.GTError) as e:
+        gpu_ctx.accel_grouped(T, torch.as_tensor(long.view(np.int32), device="cuda"), theta=0.7, batch=32,
+                              group_mode=g.GT_GROUP_BATCH)
+    assert e.value.status == 1
     with pytest.raises(g.GTError) as e:
         gpu_ctx.accel_grouped(T, None, theta=0.7, mac=g.GT_MAC_LEARNED)
     assert e.value.status == 1  # GT_ERR_INVALID: the learned criterion without a model
