@@ -919,6 +919,17 @@ def run_extras_arm(args):
     launches = ctx.launches() - l0
     clocks = sampler.stop()
     rows = {k: {"ms_per_step": v, "particles_per_s": nl / (v / 1e3)} for k, v in ms.items()}
+    # force error against the FP64 direct sum on the seeded 4096-particle sample: the plain walk,
+    # and the gas-rules walk against the direct sum with the same zeta terms
+    sample = error_sample(n)
+    full = [f.cpu().numpy() for f in ctx.accel_grouped(T, None, aold=aold, out_order=g.GT_OUT_ORIGINAL, **wopts)]
+    e = relerr([full[k][sample] for k in range(3)], ctx.direct(P, sample, want_phi=False)[:3])
+    fg = [f.cpu().numpy() for f in ctx.accel_grouped(Tg, None, aold=aold, out_order=g.GT_OUT_ORIGINAL,
+                                                     sink_direct_radius=0.02, **wopts)]
+    eg = relerr([fg[k][sample] for k in range(3)], ctx.direct_gas(P, sample, type=ty, zeta=zeta))
+    error = {"vs": "FP64 direct sum (with the zeta terms for the gas walk)", "sample": int(len(sample)),
+             "plain": {"median": float(np.median(e)), "p99": float(np.quantile(e, 0.99))},
+             "gas": {"median": float(np.median(eg)), "p99": float(np.quantile(eg, 0.99))}}
     cpu = None
     if not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -956,7 +967,7 @@ def run_extras_arm(args):
                    "gas": "70 % gas with zeta = 0.1 m^2 h^2 N(0,1), 1 % sinks, sink-direct radius 0.02",
                    "reuse": "kick and speed bound for every live particle, refresh, drifted positions, walk",
                    "l2": f"inputs larger than L2: {n * 32 / 2**20:.0f} MiB of particles"},
-        "rows": rows, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+        "rows": rows, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks, "error": error,
     }
     print(json.dumps(line), flush=True)
 
@@ -1091,6 +1102,7 @@ def run_activeset_arm(args):
     stream = torch.cuda.current_stream()
     rows = []
     parity = None
+    error = None
     sampler = ClockSampler(0)
     sampler.start()
     l0 = ctx.launches()
@@ -1144,6 +1156,12 @@ def run_activeset_arm(args):
                         e = relerr(res, r)
                         pr = {"targets": k, "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99))}
                         parity = dict(parity or {}, **{grouping: pr})
+                if frac == 1e-2 and layout == "scattered" and grouping == "leaf":
+                    sub = np.arange(0, k, max(1, k // 4096))[:4096]
+                    d = ctx.direct(P, tg[sub], want_phi=False)
+                    e = relerr([res[c][sub] for c in range(3)], d[:3])
+                    error = {"vs": "FP64 direct sum", "walk": "1 % scattered, leaf groups", "sample": int(len(sub)),
+                             "median": float(np.median(e)), "p99": float(np.quantile(e, 0.99))}
                 rows.append(row)
                 log(json.dumps(row))
     launches = ctx.launches() - l0
@@ -1156,7 +1174,7 @@ def run_activeset_arm(args):
             "config": {"workload": args.workload, "description": cfg["desc"], "n": n,
                        "criterion": f"plain relative criterion alpha={alpha}",
                        "headline": "0.1 % scattered actives, leaf groups"},
-            "rows": rows, "parity": parity, "gpu_launches": launches, "clocks": clocks,
+            "rows": rows, "parity": parity, "error": error, "gpu_launches": launches, "clocks": clocks,
             "e2e": {"value": head["host_ms"], "unit": "ms", "h2d_bytes_per_step": head["targets"] * 12,
                     "d2h_bytes_per_step": head["targets"] * 24}}
     print(json.dumps(line), flush=True)
