@@ -595,7 +595,8 @@ def run_gpu_arm(args):
         ho = [torch.empty(nl, dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
         hctx = g.Context(local)
         if split:
-            ob_h = T.download(nodes=False)["orderbuf"]
+            # the target list sits in pinned memory like the other host arrays of the step
+            ob_h = torch.from_numpy(T.download(nodes=False)["orderbuf"].view(np.int32)).pin_memory().numpy().view(np.uint32)
             sh = [o[sa:sb] for o in ho]
         ttimes = []
         for it in range(args.warmup + args.steps):
@@ -620,7 +621,8 @@ def run_gpu_arm(args):
         nw = (sb - sa) if split else nl  # targets this rank walks
         e2e = {"value": nl * jobs / te, "unit": "particles/s", "ms_per_step": 1e3 * te,
                "ms_per_step_median": 1e3 * float(np.median(ttimes)), "ms_per_step_max": 1e3 * float(np.max(ttimes)),
-               "h2d_bytes_per_step": int(5 * 8 * n + 8 * nw), "d2h_bytes_per_step": int(3 * 8 * nw),
+               "h2d_bytes_per_step": int(5 * 8 * n + 8 * nw + (4 * nw if split else 0)),
+               "d2h_bytes_per_step": int(3 * 8 * nw),
                "includes": "H2D of x,y,z,m,soft,aold from pinned memory + tree build + walk + D2H of ax,ay,az"}
         hctx.close()
 
