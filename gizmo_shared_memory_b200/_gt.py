@@ -44,8 +44,10 @@ EXPORTS = [
     "gt_accel_grouped_ext", "gt_tree_velocities", "gt_tree_velocity_moments", "gt_tree_events",
     "gt_tree_refresh", "gt_tree_node_state", "gt_tree_particles", "gt_tree_gas",
     "gt_ngb_options_default", "gt_tree_hmax", "gt_ngb_search", "gt_density_options_default", "gt_density",
-    "gt_direct_gas", "gt_mac_ceiling", "gt_tree_audit",
+    "gt_direct_gas", "gt_mac_ceiling", "gt_tree_audit", "gt_ngb_count", "gt_ngb_counters_get",
 ]
+
+GT_NGB_COUNTERS = 13
 
 
 class GTError(RuntimeError):
@@ -84,7 +86,7 @@ class TuneOptions(C.Structure):
 
 class NgbOptions(C.Structure):
     _fields_ = [("mode", C.c_int), ("box", C.c_double), ("elapsed", C.c_double), ("n_gas", C.c_int64),
-                ("h", C.c_void_p)]
+                ("h", C.c_void_p), ("systems", C.c_void_p)]
 
 
 class DensityOptions(C.Structure):
@@ -185,6 +187,8 @@ def load_library(path: str = LIB_PATH):
     L.gt_mac_sample.argtypes = [vp, vp, vp, d, C.c_int, i64, d, d, i64, C.c_int, vp, vp, vp,
                                 C.POINTER(i64)]
     L.gt_tree_audit.argtypes = [vp, vp, C.POINTER(i64), C.c_char_p, C.c_size_t]
+    L.gt_ngb_count.argtypes = [vp, C.c_int]
+    L.gt_ngb_counters_get.argtypes = [vp, vp, C.c_int]
     L.gt_mac_ceiling.argtypes = [vp, vp, vp, d, C.c_int, i64, vp, C.c_int, d, d, d, d, C.c_int, vp, vp, vp, vp]
     L.gt_mac_train.argtypes = [vp, i64, vp, vp, C.POINTER(MacTrainOptions), C.c_int, vp, C.POINTER(d)]
     L.gt_mac_predict.argtypes = [vp, vp, i64, vp, C.c_int, vp]
@@ -672,8 +676,9 @@ class Context:
                                                 GT_MEM_DEVICE if dev else GT_MEM_HOST))
 
     def ngb_search(self, tree: Tree, cx, cy, cz, radius, mode=GT_NGB_GATHER, h=None, n_gas=0, box=0.0,
-                   elapsed=0.0):
-        """Neighbour lists as CSR (start [n+1] int64, found uint32 particle indices), host arrays."""
+                   elapsed=0.0, systems=None):
+        """Neighbour lists as CSR (start [n+1] int64, found uint32 particle indices), host arrays.
+        On a forest, systems (per centre) names the one system each centre searches; None: all."""
         cx, cy, cz, radius = (np.ascontiguousarray(a, np.float64) for a in (cx, cy, cz, radius))
         o = NgbOptions()
         L = load_library()
@@ -681,6 +686,8 @@ class Context:
         o.mode, o.box, o.elapsed, o.n_gas = mode, box, elapsed, int(n_gas)
         hh = None if h is None else np.ascontiguousarray(h, np.float64)
         o.h = _ptr(hh)
+        ss = None if systems is None else np.ascontiguousarray(systems, np.int32)
+        o.systems = _ptr(ss)
         n = len(cx)
         start = np.zeros(n + 1, np.int64)
         tot = C.c_int64(0)
@@ -721,6 +728,20 @@ class Context:
         self._check(L.gt_density(self.h, tree.h, nt, _ptr(t), C.byref(o), GT_MEM_DEVICE if dev else GT_MEM_HOST,
                                  _ptr(h), _ptr(rho), _ptr(nngb), _ptr(iters)))
         return {"h": h, "rho": rho, "nngb": nngb, "iters": iters}
+
+    def ngb_count(self, enable=True):
+        """SHMEM_NGB_COUNT on this context: tally the gather searches and density solves."""
+        self._check(load_library().gt_ngb_count(self.h, int(bool(enable))))
+
+    def ngb_counters(self, reset=False):
+        """The tallies: dict of calls, nodes, examined, kept, pad_nodes and the iteration histogram
+        hiter[8] (slot i: targets that took i + 1 iterations; the last, 8 or more)."""
+        v = np.zeros(GT_NGB_COUNTERS, np.int64)
+        self._check(load_library().gt_ngb_counters_get(self.h, _ptr(v), int(bool(reset))))
+        names = ("calls", "nodes", "examined", "kept", "pad_nodes")
+        out = {k: int(v[i]) for i, k in enumerate(names)}
+        out["hiter"] = v[5:].copy()
+        return out
 
     def velocity_moments(self, tree: Tree):
         nn = tree.info()["n_nodes"]

@@ -157,7 +157,7 @@ void check_mem(int mem) {
 void free_tree_arrays(gt_tree* t) {
     void* ptrs[] = {t->src, t->ssoft, t->smass, t->order, t->rank, t->leaf_of, t->sleaf, t->skey,
                     t->nodes, t->parent, t->next, t->level, t->size, t->delta, t->nsoft, t->gc,
-                    t->nq2, t->sys_off_dev, t->geom_dev, t->svel, t->nvel, t->vcom, t->vmax,
+                    t->nq2, t->sys_off_dev, t->in_off_dev, t->geom_dev, t->svel, t->nvel, t->vcom, t->vmax,
                     t->m0, t->c0, t->dp, t->dq, t->dmass, t->xpad, t->stype, t->szeta, t->nsink,
                     t->snode, t->hmax};
     // tree arrays came from the stream-ordered pool: hand them back to it (callers have synchronised)
@@ -408,6 +408,7 @@ int gt_context_destroy(gt_context* ctx) {
         cudaStreamDestroy(ctx->walk2);
     }
     if (ctx->walk2_start) cudaEventDestroy(ctx->walk2_start);
+    if (ctx->tally_dev) cudaFree(ctx->tally_dev);
     if (ctx->walk2_done) cudaEventDestroy(ctx->walk2_done);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     cudaGetLastError();
@@ -860,21 +861,28 @@ int gt_ngb_search(gt_context* ctx, const gt_tree* tc, int64_t n, const double* c
         const double* dr = stage_in(ctx, kSlotIn3, radius, n, mem);
         const int64_t ng = o.mode == GT_NGB_GATHER ? 0 : std::min<int64_t>(o.n_gas, tree->n);
         const double* dh = stage_in(ctx, kSlotIn4, o.h, ng, mem);
+        const int* dsys = (const int*)stage_in(ctx, kSlotIn5, o.systems, n, mem);
         int64_t* ds = out_buf(ctx, kSlotOut0, start, n + 1, mem);
         // the host path sizes the device list from the count pass: capacity 0 in the call below
-        // means "count only", the lists follow once the total is known
+        // means "count only", the lists follow once the total is known.  SHMEM_NGB_COUNT: a call
+        // counts its searches once, when it delivers the lists; a count-only call or one that
+        // overflows counts nothing, so counting then filling counts each search once
         uint32_t* df = mem == GT_MEM_DEVICE ? found : nullptr;
-        const int64_t tot = run_ngb(ctx, tree, n, dx, dy, dz, dr, o.mode, dh, ng, o.box, o.elapsed, ds, df,
-                                    mem == GT_MEM_DEVICE ? capacity : 0);
+        int64_t tl[5] = {0, 0, 0, 0, 0};
+        const bool counted = ctx->ngb_count && found;
+        const int64_t tot = run_ngb(ctx, tree, n, dx, dy, dz, dr, dsys, o.mode, dh, ng, o.box, o.elapsed, ds, df,
+                                    mem == GT_MEM_DEVICE ? capacity : 0, counted ? tl : nullptr);
         if (total) *total = tot;
         copy_out(ctx, start, ds, n + 1, mem);
         if (mem == GT_MEM_HOST && found && tot <= capacity && tot > 0) {
             uint32_t* hf = (uint32_t*)scratch(ctx, kSlotOut1, (size_t)tot * 4);
-            run_ngb(ctx, tree, n, dx, dy, dz, dr, o.mode, dh, ng, o.box, o.elapsed, ds, hf, tot);
+            run_ngb(ctx, tree, n, dx, dy, dz, dr, dsys, o.mode, dh, ng, o.box, o.elapsed, ds, hf, tot, nullptr);
             copy_out(ctx, found, hf, tot, mem);
         }
         finish(ctx, true);
         if (found && tot > capacity) throw Fail{GT_ERR_OVERFLOW, "the neighbour lists need more room than capacity"};
+        if (counted)
+            for (int k = 0; k < 5; ++k) ctx->ngb_totals[k] += tl[k];
     });
 }
 
@@ -904,13 +912,33 @@ int gt_density(gt_context* ctx, const gt_tree* tc, int64_t nt, const uint32_t* t
         double* dr = (double*)(mem == GT_MEM_DEVICE && rho ? (void*)rho : scratch(ctx, kSlotOut1, (size_t)nt * 8));
         int* dn = (int*)(mem == GT_MEM_DEVICE && nngb ? (void*)nngb : scratch(ctx, kSlotOut2, (size_t)nt * 4));
         int* di = (int*)(mem == GT_MEM_DEVICE && iters ? (void*)iters : scratch(ctx, kSlotOut3, (size_t)nt * 4));
+        int64_t tl[GT_NGB_COUNTERS] = {};
         run_density(ctx, tree, nt, dt, o.des_ngb, o.ngb_tol, dhs, o.box, o.n_dims, dcp, o.face_correction != 0,
-                    o.elapsed, dh, dr, dn, di);
+                    o.elapsed, dh, dr, dn, di, ctx->ngb_count ? tl : nullptr);
         copy_out(ctx, h, dh, nt, mem);
         copy_out(ctx, rho, dr, nt, mem);
         copy_out(ctx, nngb, (int32_t*)dn, nt, mem);
         copy_out(ctx, iters, (int32_t*)di, nt, mem);
         finish(ctx, true);
+        if (ctx->ngb_count)
+            for (int k = 0; k < GT_NGB_COUNTERS; ++k) ctx->ngb_totals[k] += tl[k];
+    });
+}
+
+int gt_ngb_count(gt_context* ctx, int enable) {
+    if (!ctx) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        ctx->ngb_count = enable != 0;
+    });
+}
+
+int gt_ngb_counters_get(gt_context* ctx, int64_t* counts, int reset) {
+    if (!ctx || !counts) return GT_ERR_INVALID;
+    return guarded(ctx, [&] {
+        for (int k = 0; k < GT_NGB_COUNTERS; ++k) {
+            counts[k] = ctx->ngb_totals[k];
+            if (reset) ctx->ngb_totals[k] = 0;
+        }
     });
 }
 

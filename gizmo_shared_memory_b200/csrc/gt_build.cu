@@ -787,11 +787,14 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
         for (int s = 0; s < S; ++s) nmax = std::max<int64_t>(nmax, in_off[s + 1] - in_off[s]);
         const int chunks = (int)std::min<int64_t>(64, std::max<int64_t>(1, (nmax + 8191) / 8192));
         const size_t nparts = (size_t)S * chunks;
-        char* ws = (char*)scratch(ctx, kSlotPartials, (size_t)(S + 1) * 8 + nparts * 64 + 256);
-        in_off_dev = (int64_t*)ws;
-        double* part = (double*)(ws + (((size_t)(S + 1) * 8 + 15) & ~(size_t)15));
+        double* part = (double*)scratch(ctx, kSlotPartials, nparts * 64 + 256);
         unsigned long long* cnt = (unsigned long long*)(part + nparts * 6);
-        // pageable source: the copy is staged before the call returns, in_off may go away after
+        // kept with the tree: the neighbour search, the density solve and explicit-target walks
+        // find a particle's system from its index.  Pageable source: the copy is staged before
+        // the call returns, in_off may go away after
+        t->in_off.assign(in_off, in_off + S + 1);
+        t->in_off_dev = dalloc<int64_t>((size_t)S + 1, st);
+        in_off_dev = t->in_off_dev;
         check_cuda(cudaMemcpyAsync(in_off_dev, in_off, (size_t)(S + 1) * 8, cudaMemcpyHostToDevice, st),
                    "offsets h2d");
         check_cuda(cudaMemsetAsync(bad_dev, 0, 8, st), "memset");

@@ -104,6 +104,12 @@ struct gt_context {
     // second compute stream: the chunks of a chunked walk alternate between it and `stream`
     cudaStream_t walk2 = nullptr;
     cudaEvent_t walk2_start = nullptr, walk2_done = nullptr;
+    // SHMEM_NGB_COUNT (gt_ngb_count): while ngb_count is set, a counted call tallies on the
+    // device into tally_dev (GT_NGB_COUNTERS, made on first use, zeroed per call) and adds the
+    // tally to the host totals ngb_totals once the call has delivered its results
+    bool ngb_count = false;
+    unsigned long long* tally_dev = nullptr;
+    int64_t ngb_totals[GT_NGB_COUNTERS] = {};
 };
 
 struct gt_tree {
@@ -118,6 +124,10 @@ struct gt_tree {
     std::vector<gt::RootGeom> sys_geom;  // per-system root cells
     std::vector<int64_t> sys_off;        // n_systems + 1
     int* sys_off_dev = nullptr;          // device copy (int32), n_systems + 1
+    // forest: device copy of the input offsets (n_systems + 1): system s owns the particle indices
+    // [in_off_dev[s], in_off_dev[s+1]), massless ones included (null for one system)
+    int64_t* in_off_dev = nullptr;
+    std::vector<int64_t> in_off;         // host copy (forest only)
     gt::RootGeom* geom_dev = nullptr;    // device copy of sys_geom
     std::vector<int64_t> lvl_off;  // node index range of each level: [lvl_off[L], lvl_off[L+1])
     double build_ms[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -196,6 +206,7 @@ enum Slot {
     kSlotStack2,  // traversal stacks of the second compute stream (chunked walks)
     kSlotGroupCount,  // device-side group and chunk counts of an explicit-target walk
     kSlotLevels,      // device-side level offsets and counts of the build's structure stage
+    kSlotIn5,         // a sixth staged input (the neighbour search's per-centre systems)
     kSlotCount
 };
 
@@ -352,12 +363,15 @@ void tree_hmax(gt_context* ctx, gt_tree* t, const double* h, int64_t n_gas);
 void raise_hmax(gt_context* ctx, gt_tree* t, int64_t n, const int* leaf, const double* h);
 // Counts into start (n+1, exclusive prefix sums) and, when found is given and the total fits
 // capacity, the lists; returns the total.
+// systems: per centre, the one system searched (null: every system).  tally (host, 5 values, or
+// null): the SHMEM_NGB_COUNT tally of the gather searches of the counting pass.
 int64_t run_ngb(gt_context* ctx, gt_tree* t, int64_t n, const double* cx, const double* cy, const double* cz,
-                const double* radius, int mode, const double* h, int64_t n_gas, double box, double elapsed,
-                int64_t* start, uint32_t* found, int64_t capacity);
+                const double* radius, const int* systems, int mode, const double* h, int64_t n_gas, double box,
+                double elapsed, int64_t* start, uint32_t* found, int64_t capacity, int64_t* tally);
+// tally (host, GT_NGB_COUNTERS values, or null): the solve's SHMEM_NGB_COUNT tally (synchronises).
 void run_density(gt_context* ctx, gt_tree* t, int64_t nt, const uint32_t* targets, double des_ngb, double ngb_tol,
                  const double* h_start, double box, int n_dims, const double* cond_prev, int face_corr,
-                 double elapsed, double* h, double* rho, int* nngb, int* iters);
+                 double elapsed, double* h, double* rho, int* nngb, int* iters, int64_t* tally);
 void run_form_aold(gt_context* ctx, int64_t n, const double* ax, const double* ay,
                    const double* az, double alpha, double G, double* aold);
 

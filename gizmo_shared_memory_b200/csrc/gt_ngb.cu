@@ -11,6 +11,16 @@
 // targets) follow nearly the same path, so a warp's threads mostly read the same nodes.
 //
 // Lists are CSR: a counting pass, an exclusive scan, and a filling pass over the same traversal.
+//
+// Forests (gt_build_systems): roots 0 .. n_systems-1 each stand alone in the threading.  A centre
+// searches every system in turn, or the one system its caller names; a density target searches the
+// system that owns its particle index.  Each system's search nodes are padded by its own root side,
+// so a system searched in a forest finds what it finds in a tree of its own.
+//
+// SHMEM_NGB_COUNT (hydro.cc:7-35): a context with counting on tallies, per gather search, the nodes
+// visited, the particles examined, the neighbours kept and the nodes admitted only by the staleness
+// pad, and per density target the iterations it took; the counting variants of the kernels are
+// separate instantiations, so the plain ones keep their code.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -41,12 +51,16 @@ __device__ __forceinline__ float up_float(double h) {  // rounded up to float (t
     return (double)f < h ? nextafterf(f, 1e30f) : f;
 }
 
+// The pad 1e-6 of the root side is that of the node's own system: root s is node s, and a deeper
+// node belongs to the system whose live tree positions hold its first particle.
 __global__ void pack_snode_kernel(const GNode* __restrict__ nodes, const int* __restrict__ next,
                                   const double* __restrict__ gc, const double* __restrict__ size, int64_t nn,
-                                  double eps, SNodeG* __restrict__ sn) {
+                                  const int* __restrict__ sys_off, int n_systems, SNodeG* __restrict__ sn) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (int64_t)gridDim.x * blockDim.x) {
         const double x = gc[3 * i], y = gc[3 * i + 1], z = gc[3 * i + 2];
         const double cm = fmax(fabs(x), fmax(fabs(y), fabs(z)));
+        const int sys = n_systems > 1 ? (i < n_systems ? (int)i : system_of(sys_off, n_systems, nodes[i].plo)) : 0;
+        const double eps = 1e-6 * size[sys];
         SNodeG s;
         s.cx = (float)x; s.cy = (float)y; s.cz = (float)z;
         s.half = (float)(0.5 * size[i] + eps + 4.0 * (double)FLT_EPSILON * cm);
@@ -77,7 +91,9 @@ __global__ void hmax_kernel(const double* __restrict__ h, const int* __restrict_
 }
 
 struct SearchGeom {
-    int root;            // 0, or -1 for a tree without nodes
+    int n_roots;         // roots 0 .. n_roots-1: 1, n_systems in a forest, 0 for a tree without nodes
+    int n_systems;
+    const int64_t* in_off;  // forest: system s owns the particle indices [in_off[s], in_off[s+1])
     const SNodeG* sn;
     const SrcP* src;
     const uint32_t* order;
@@ -87,15 +103,24 @@ struct SearchGeom {
     double elapsed, box;
 };
 
-// One traversal for one centre in the reference's node order.  REVERSE: gas particles j < n_gas
-// with radius <= r < h[j] (ngb_search_reverse); otherwise r < radius (ngb_search).  emit(j, s)
-// receives the particle index and its tree position.
-template <bool REVERSE, typename F>
-__device__ __forceinline__ void search(const SearchGeom& g, double px, double py, double pz, double radius,
-                                       const double* __restrict__ h, int64_t n_gas, F&& emit) {
+// What a gather search tallies under SHMEM_NGB_COUNT (hydro.cc:51-106): nodes visited, particles
+// examined in the leaves opened, nodes admitted only by the vmax * elapsed and xpad pads.
+struct NgbTally {
+    unsigned long long nodes = 0, examined = 0, pad = 0;
+};
+
+// One traversal for one centre in the reference's node order, from roots r0 .. r1-1 in turn.
+// REVERSE: gas particles j < n_gas with radius <= r < h[j] (ngb_search_reverse); otherwise
+// r < radius (ngb_search).  emit(j, s) receives the particle index and its tree position.  COUNT
+// (gather only, as the reference counts): the tally.
+template <bool REVERSE, bool COUNT = false, typename F>
+__device__ __forceinline__ void search(const SearchGeom& g, int r0, int r1, double px, double py, double pz,
+                                       double radius, const double* __restrict__ h, int64_t n_gas, F&& emit,
+                                       NgbTally* tally = nullptr) {
     const double r2max = radius * radius;
-    int node = g.root;
-    while (node >= 0) {
+    for (int root = r0; root < r1; ++root)
+    for (int node = root; node >= 0;) {
+        if (COUNT) ++tally->nodes;
         const float4 a = __ldg(reinterpret_cast<const float4*>(g.sn + node));
         const int4 b = __ldg(reinterpret_cast<const int4*>(g.sn + node) + 1);
         const double half = (double)a.w;
@@ -117,7 +142,12 @@ __device__ __forceinline__ void search(const SearchGeom& g, double px, double py
         if (dz > dist || -dz > dist) { node = b.y; continue; }
         dist += 0.7320508075688772 * half;
         if (dx * dx + dy * dy + dz * dz > dist * dist) { node = b.y; continue; }
+        if (COUNT && g.elapsed > 0) {
+            const double nopad = radius + 1.7320508075688772 * half;
+            if (dx * dx + dy * dy + dz * dz > nopad * nopad) ++tally->pad;
+        }
         if (b.x < 0) {
+            if (COUNT) tally->examined += (unsigned long long)(b.w - b.z);
             for (int s = b.z; s < b.w; ++s) {
                 const uint32_t j = __ldg(g.order + s);
                 if (REVERSE && (int64_t)j >= n_gas) continue;
@@ -146,36 +176,74 @@ __device__ __forceinline__ void search(const SearchGeom& g, double px, double py
 struct NgbArgs {
     SearchGeom g;
     const double *cx, *cy, *cz, *radius;
+    const int* systems;           // per centre, the one system searched; null: every system
     int64_t n;
     int mode;
     const double* h;
     int64_t n_gas;
     uint32_t* count;              // counting pass
-    unsigned long long* total;    // counting pass: sum of the counts
+    unsigned long long* total;    // counting pass: [0] sum of the counts, [1] centres naming no system
     const int64_t* start;         // filling pass
     uint32_t* found;
+    unsigned long long* tally;    // SHMEM_NGB_COUNT totals (calls, nodes, examined, kept, pad)
 };
 
-template <bool FILL>
+// Sums v over the warp and adds it to *dst from lane 0; every lane of the warp calls it.
+__device__ __forceinline__ void warp_flush(unsigned long long v, unsigned long long* dst) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
+}
+
+// The roots a centre searches: every system's, or those of the system it names (checked: a
+// system outside [0, n_systems) searches nothing and is counted in *bad).
+__device__ __forceinline__ void roots_of(const SearchGeom& g, const int* systems, int64_t c, int& r0, int& r1,
+                                         unsigned long long* bad) {
+    r0 = 0;
+    r1 = g.n_roots;
+    if (!systems) return;
+    const int s = systems[c];
+    if (s < 0 || s >= g.n_systems) {
+        if (bad) atomicAdd(bad, 1ull);
+        r1 = 0;
+        return;
+    }
+    r0 = s;
+    r1 = min(s + 1, g.n_roots);
+}
+
+template <bool FILL, bool COUNT>
 __global__ void __launch_bounds__(kBlk) ngb_kernel(const NgbArgs a) {
-    unsigned long long mine = 0;
+    unsigned long long mine = 0, calls = 0, kept = 0;
+    NgbTally tl;
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.n; c += (int64_t)gridDim.x * blockDim.x) {
         const double px = a.cx[c], py = a.cy[c], pz = a.cz[c], r = a.radius[c];
+        int r0, r1;
+        roots_of(a.g, a.systems, c, r0, r1, FILL ? nullptr : a.total + 1);
         int64_t k = FILL ? a.start[c] : 0;
         auto emit = [&](uint32_t j, int) {
             if (FILL) a.found[k] = j;
             ++k;
         };
-        if (a.mode != GT_NGB_REVERSE) search<false>(a.g, px, py, pz, r, nullptr, 0, emit);
-        if (a.mode != GT_NGB_GATHER) search<true>(a.g, px, py, pz, r, a.h, a.n_gas, emit);
+        if (a.mode != GT_NGB_REVERSE) {
+            search<false, COUNT>(a.g, r0, r1, px, py, pz, r, nullptr, 0, emit, &tl);
+            if (COUNT) {
+                ++calls;
+                kept += (unsigned long long)k;
+            }
+        }
+        if (a.mode != GT_NGB_GATHER) search<true>(a.g, r0, r1, px, py, pz, r, a.h, a.n_gas, emit);
         if (!FILL) {
             a.count[c] = (uint32_t)k;
             mine += (unsigned long long)k;
         }
     }
-    if (!FILL) {
-        for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
-        if ((threadIdx.x & 31) == 0 && mine) atomicAdd(a.total, mine);
+    if (!FILL) warp_flush(mine, a.total);
+    if (COUNT) {
+        warp_flush(calls, a.tally + 0);
+        warp_flush(tl.nodes, a.tally + 1);
+        warp_flush(tl.examined, a.tally + 2);
+        warp_flush(kept, a.tally + 3);
+        warp_flush(tl.pad, a.tally + 4);
     }
 }
 
@@ -213,11 +281,13 @@ struct DensArgs {
     const uint32_t* targets;
     int64_t nt;
     double des_ngb, ngb_tol, h_default;
+    const double* h_default_sys;  // forest without h_start: the default h of each system
     const double* h_start;
     const double* cond_prev;  // per particle index
     int n_dims, face_corr;
     double *h, *rho;
     int *nngb, *iters;
+    unsigned long long* tally;  // SHMEM_NGB_COUNT: calls, nodes, examined, kept, pad, iterations [8]
 };
 
 __device__ __forceinline__ void dens_zero(DensSums& s) {
@@ -262,7 +332,9 @@ __device__ __forceinline__ void dens_add(double dx, double dy, double dz, double
 // wait on every neighbour another lane had found.
 constexpr int kDensBuf = 64;
 
-__device__ void dens_eval(const DensArgs& a, double px, double py, double pz, double h, DensSums& s) {
+template <bool COUNT>
+__device__ void dens_eval(const DensArgs& a, int r0, int r1, double px, double py, double pz, double h, DensSums& s,
+                          NgbTally& tl, unsigned long long& kept) {
     dens_zero(s);
     const int dim = a.n_dims;
     const double norm = kernel_norm(h, dim);
@@ -279,10 +351,11 @@ __device__ void dens_eval(const DensArgs& a, double px, double py, double pz, do
         }
         nb = 0;
     };
-    search<false>(a.g, px, py, pz, h, nullptr, 0, [&](uint32_t, int sp) {
+    search<false, COUNT>(a.g, r0, r1, px, py, pz, h, nullptr, 0, [&](uint32_t, int sp) {
+        if (COUNT) ++kept;
         if (nb == kDensBuf) drain();
         buf[nb++] = sp;
-    });
+    }, &tl);
     drain();
 }
 
@@ -371,26 +444,80 @@ __device__ __forceinline__ NewtonParams newton_params(const DensArgs& a) {
 }
 
 // One thread per target: up to 100 iterations of evaluation and Newton step, then, when the solve
-// did not converge, one more evaluation at the final h (hydro.cc:189-297).
+// did not converge, one more evaluation at the final h (hydro.cc:189-297).  In a forest the target
+// searches the system that owns its particle index.  COUNT: every evaluation is one gather search
+// of the tally, and the target's iterations go to the histogram (hydro.cc:293-296).  ONE_ROOT: a
+// single-system tree with nodes, whose one root (node 0) the compiler then knows, which keeps the
+// traversal's registers those of a plain tree walk.
+template <bool COUNT, bool ONE_ROOT>
 __global__ void __launch_bounds__(kBlk, 6) density_kernel(const DensArgs a) {
+    NgbTally tl;
+    unsigned long long calls = 0, kept = 0, hist[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.nt; t += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t p = a.targets[t];
         const uint32_t sp = a.rank[p];
         const double px = a.g.src[sp].x, py = a.g.src[sp].y, pz = a.g.src[sp].z;
-        double h = a.h_start ? a.h_start[t] : a.h_default, h_lo = 0.0, h_hi = 0.0;
+        int r0 = 0, r1 = ONE_ROOT ? 1 : a.g.n_roots;
+        if (!ONE_ROOT && a.g.in_off) {
+            r0 = system_of(a.g.in_off, a.g.n_systems, (int64_t)p);
+            r1 = r0 + 1;
+        }
+        double h = a.h_start ? a.h_start[t] : (a.h_default_sys ? a.h_default_sys[r0] : a.h_default);
+        double h_lo = 0.0, h_hi = 0.0;
         int iter = 0;
         bool converged = false;
         DensSums s;
         for (; iter < 100; ++iter) {
-            dens_eval(a, px, py, pz, h, s);
+            dens_eval<COUNT>(a, r0, r1, px, py, pz, h, s, tl, kept);
+            if (COUNT) ++calls;
             if (dens_newton(newton_params(a), p, s, iter, h, h_lo, h_hi)) { converged = true; break; }
         }
-        if (!converged) dens_eval(a, px, py, pz, h, s);  // rho of the final h (hydro.cc:281-293)
+        if (!converged) {  // rho of the final h (hydro.cc:281-293)
+            dens_eval<COUNT>(a, r0, r1, px, py, pz, h, s, tl, kept);
+            if (COUNT) ++calls;
+        }
+        if (COUNT) ++hist[min(converged ? iter + 1 : 100, 8) - 1];
         a.h[t] = h;
         a.rho[t] = s.rho;
         a.nngb[t] = s.inside;
         a.iters[t] = iter;
     }
+    if (COUNT) {
+        warp_flush(calls, a.tally + 0);
+        warp_flush(tl.nodes, a.tally + 1);
+        warp_flush(tl.examined, a.tally + 2);
+        warp_flush(kept, a.tally + 3);
+        warp_flush(tl.pad, a.tally + 4);
+        for (int k = 0; k < 8; ++k) warp_flush(hist[k], a.tally + 5 + k);
+    }
+}
+
+// Per system of a forest, the bounding box of all its particles (massless too) for its default h:
+// block b reduces chunk b % chunks of system b / chunks, through the particles' tree positions.
+__global__ void density_bbox_kernel(const SrcP* __restrict__ src, const uint32_t* __restrict__ rank,
+                                    const int64_t* __restrict__ in_off, int chunks, double* __restrict__ part) {
+    const int s = blockIdx.x / chunks, c = blockIdx.x % chunks;
+    const int64_t lo0 = in_off[s], len = in_off[s + 1] - lo0;
+    const int64_t b = lo0 + len * c / chunks, e = lo0 + len * (c + 1) / chunks;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+        const SrcP q = src[rank[i]];
+        const double v[3] = {q.x, q.y, q.z};
+        for (int k = 0; k < 3; ++k) { lo[k] = fmin(lo[k], v[k]); hi[k] = fmax(hi[k], v[k]); }
+    }
+    __shared__ double sh[6][kBlk];
+    for (int k = 0; k < 3; ++k) { sh[k][threadIdx.x] = lo[k]; sh[3 + k][threadIdx.x] = hi[k]; }
+    __syncthreads();
+    for (int o = kBlk / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o)
+            for (int k = 0; k < 3; ++k) {
+                sh[k][threadIdx.x] = fmin(sh[k][threadIdx.x], sh[k][threadIdx.x + o]);
+                sh[3 + k][threadIdx.x] = fmax(sh[3 + k][threadIdx.x], sh[3 + k][threadIdx.x + o]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 6; ++k) part[6 * (int64_t)blockIdx.x + k] = sh[k][0];
 }
 
 // bounding box of every particle (massless too), for the density solve's default h
@@ -418,7 +545,9 @@ __global__ void bbox_all_kernel(const SrcP* __restrict__ src, int64_t n, double*
 SearchGeom geom_of(gt_context* ctx, gt_tree* t, double elapsed, double box) {
     ensure_snodes(ctx, t);
     SearchGeom g;
-    g.root = t->n_nodes > 0 ? 0 : -1;
+    g.n_roots = t->n_nodes > 0 ? t->n_systems : 0;
+    g.n_systems = t->n_systems;
+    g.in_off = t->n_systems > 1 ? t->in_off_dev : nullptr;
     g.sn = t->snode;
     g.src = t->src;
     g.order = t->order;
@@ -436,20 +565,30 @@ SearchGeom geom_of(gt_context* ctx, gt_tree* t, double elapsed, double box) {
 // same tree, so the nodes are complete on the device before the pointer is published.
 void ensure_snodes(gt_context* ctx, gt_tree* t) {
     if (t->n_nodes <= 0) return;
-    if (t->n_systems > 1) throw Fail{GT_ERR_UNSUPPORTED, "the neighbour search works on single-system trees"};
     std::lock_guard<std::mutex> lk(t->lazy_mu);
     if (t->snode) return;
     SNodeG* p = nullptr;
     check_cuda(cudaMallocAsync((void**)&p, (size_t)t->n_nodes * sizeof(SNodeG), ctx->stream), "cudaMallocAsync");
-    double root_size = 0.0;
-    check_cuda(cudaMemcpyAsync(&root_size, t->size, 8, cudaMemcpyDeviceToHost, ctx->stream), "d2h");
-    check_cuda(cudaStreamSynchronize(ctx->stream), "sync");
     pack_snode_kernel<<<grid_of(ctx, t->n_nodes), kBlk, 0, ctx->stream>>>(t->nodes, t->next, t->gc, t->size,
-                                                                          t->n_nodes, 1e-6 * root_size, p);
+                                                                          t->n_nodes, t->sys_off_dev, t->n_systems, p);
     check_launch(ctx, "pack_snode_kernel");
     check_cuda(cudaStreamSynchronize(ctx->stream), "sync");
     t->snode = p;
 }
+
+namespace {
+// The context's device tally, zeroed for one call (allocated on first use).
+unsigned long long* fresh_tally(gt_context* ctx) {
+    if (!ctx->tally_dev) {
+        unsigned long long* p = nullptr;
+        check_cuda(cudaMalloc((void**)&p, GT_NGB_COUNTERS * sizeof(unsigned long long)), "cudaMalloc");
+        ctx->tally_dev = p;
+    }
+    check_cuda(cudaMemsetAsync(ctx->tally_dev, 0, GT_NGB_COUNTERS * sizeof(unsigned long long), ctx->stream),
+               "memset");
+    return ctx->tally_dev;
+}
+}  // namespace
 
 void tree_hmax(gt_context* ctx, gt_tree* t, const double* h, int64_t n_gas) {
     const int64_t nn = std::max<int64_t>(t->n_nodes, 1);
@@ -469,47 +608,65 @@ void raise_hmax(gt_context* ctx, gt_tree* t, int64_t n, const int* leaf, const d
 }
 
 int64_t run_ngb(gt_context* ctx, gt_tree* t, int64_t n, const double* cx, const double* cy, const double* cz,
-                const double* radius, int mode, const double* h, int64_t n_gas, double box, double elapsed,
-                int64_t* start, uint32_t* found, int64_t capacity) {
+                const double* radius, const int* systems, int mode, const double* h, int64_t n_gas, double box,
+                double elapsed, int64_t* start, uint32_t* found, int64_t capacity, int64_t* tally) {
     if (mode != GT_NGB_GATHER && !t->hmax) throw Fail{GT_ERR_INVALID, "the reverse search needs gt_tree_hmax first"};
     cudaStream_t st = ctx->stream;
     NgbArgs a;
     a.g = geom_of(ctx, t, elapsed, box);
     a.cx = cx; a.cy = cy; a.cz = cz; a.radius = radius;
+    a.systems = systems;
+    a.tally = tally ? fresh_tally(ctx) : nullptr;
     a.n = n;
     a.mode = mode;
     a.h = h;
     a.n_gas = n_gas;
     uint32_t* cnt = (uint32_t*)scratch(ctx, kSlotNgb0, (size_t)std::max<int64_t>(n, 1) * 4);
     uint32_t* ex = (uint32_t*)scratch(ctx, kSlotNgb1, (size_t)std::max<int64_t>(n, 1) * 4);
-    unsigned long long* tot = (unsigned long long*)scratch(ctx, kSlotNgb2, 8);
-    check_cuda(cudaMemsetAsync(tot, 0, 8, st), "memset");
+    unsigned long long* tot = (unsigned long long*)scratch(ctx, kSlotNgb2, 16);
+    check_cuda(cudaMemsetAsync(tot, 0, 16, st), "memset");
     a.count = cnt;
     a.total = tot;
     a.start = nullptr;
     a.found = nullptr;
-    ngb_kernel<false><<<grid_of(ctx, n), kBlk, 0, st>>>(a);
+    if (a.tally) ngb_kernel<false, true><<<grid_of(ctx, n), kBlk, 0, st>>>(a);
+    else ngb_kernel<false, false><<<grid_of(ctx, n), kBlk, 0, st>>>(a);
     check_launch(ctx, "ngb_kernel");
-    unsigned long long total = 0;
-    check_cuda(cudaMemcpyAsync(ctx->pinned, tot, 8, cudaMemcpyDeviceToHost, st), "d2h");
+    unsigned long long total[2] = {0, 0};
+    check_cuda(cudaMemcpyAsync(ctx->pinned, tot, 16, cudaMemcpyDeviceToHost, st), "d2h");
+    if (a.tally)
+        check_cuda(cudaMemcpyAsync((char*)ctx->pinned + 64, a.tally, 5 * 8, cudaMemcpyDeviceToHost, st), "d2h");
     check_cuda(cudaStreamSynchronize(st), "sync");
-    std::memcpy(&total, ctx->pinned, 8);
-    if (total >= (1ull << 32)) throw Fail{GT_ERR_OVERFLOW, "more than 2^32 neighbours in one call"};
+    std::memcpy(total, ctx->pinned, 16);
+    if (a.tally) std::memcpy(tally, (char*)ctx->pinned + 64, 5 * 8);
+    if (total[1] > 0) throw Fail{GT_ERR_INVALID, "a centre names a system outside [0, n_systems)"};
+    if (total[0] >= (1ull << 32)) throw Fail{GT_ERR_OVERFLOW, "more than 2^32 neighbours in one call"};
     scan_exclusive_u32(ctx, cnt, ex, n, nullptr);
     widen_kernel<<<grid_of(ctx, n), kBlk, 0, st>>>(ex, cnt, n, start);
     check_launch(ctx, "widen_kernel");
-    if (found && (int64_t)total <= capacity && total > 0) {
+    if (found && (int64_t)total[0] <= capacity && total[0] > 0) {
         a.start = start;
         a.found = found;
-        ngb_kernel<true><<<grid_of(ctx, n), kBlk, 0, st>>>(a);
+        a.tally = nullptr;
+        ngb_kernel<true, false><<<grid_of(ctx, n), kBlk, 0, st>>>(a);
         check_launch(ctx, "ngb_kernel");
     }
-    return (int64_t)total;
+    return (int64_t)total[0];
+}
+
+// The default h of a particle set: des_ngb particles at the mean number density of its bounding
+// box (lo, hi) over n particles (hydro.cc:169-183).
+double default_h(const double* lo, const double* hi, double n, double des_ngb, int n_dims) {
+    const double vol = (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
+    double hd = std::cbrt(3.0 * des_ngb * vol / (4.0 * M_PI * n));
+    if (n_dims == 1) hd = 0.5 * des_ngb * (hi[0] - lo[0]) / n;
+    if (n_dims == 2) hd = std::sqrt(des_ngb * (hi[0] - lo[0]) * (hi[1] - lo[1]) / (M_PI * n));
+    return hd;
 }
 
 void run_density(gt_context* ctx, gt_tree* t, int64_t nt, const uint32_t* targets, double des_ngb, double ngb_tol,
                  const double* h_start, double box, int n_dims, const double* cond_prev, int face_corr,
-                 double elapsed, double* h, double* rho, int* nngb, int* iters) {
+                 double elapsed, double* h, double* rho, int* nngb, int* iters, int64_t* tally) {
     cudaStream_t st = ctx->stream;
     DensArgs a;
     a.g = geom_of(ctx, t, elapsed, box);
@@ -525,8 +682,38 @@ void run_density(gt_context* ctx, gt_tree* t, int64_t nt, const uint32_t* target
     a.n_dims = n_dims;
     a.face_corr = face_corr;
     a.h = h; a.rho = rho; a.nngb = nngb; a.iters = iters;
+    a.tally = tally && nt > 0 ? fresh_tally(ctx) : nullptr;
     a.h_default = 0.0;
-    if (!h_start) {
+    a.h_default_sys = nullptr;
+    if (!h_start && t->n_systems > 1) {
+        // each system's own default, from its own particles (all of them, massless too)
+        const int S = t->n_systems;
+        int64_t nmax = 0;
+        for (int s = 0; s < S; ++s) nmax = std::max<int64_t>(nmax, t->in_off[s + 1] - t->in_off[s]);
+        const int chunks = (int)std::min<int64_t>(64, std::max<int64_t>(1, (nmax + 8191) / 8192));
+        const size_t nparts = (size_t)S * chunks;
+        double* part = (double*)scratch(ctx, kSlotNgb2, nparts * 6 * 8);
+        density_bbox_kernel<<<(int)nparts, kBlk, 0, st>>>(t->src, t->rank, t->in_off_dev, chunks, part);
+        check_launch(ctx, "density_bbox_kernel");
+        std::vector<double> hp(nparts * 6), hd(S, 0.0);
+        check_cuda(cudaMemcpyAsync(hp.data(), part, hp.size() * 8, cudaMemcpyDeviceToHost, st), "d2h");
+        check_cuda(cudaStreamSynchronize(st), "sync");
+        for (int s = 0; s < S; ++s) {
+            const int64_t ns = t->in_off[s + 1] - t->in_off[s];
+            if (ns == 0) continue;  // an empty system owns no target
+            double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+            for (int c = 0; c < chunks; ++c)
+                for (int k = 0; k < 3; ++k) {
+                    lo[k] = std::min(lo[k], hp[6 * ((size_t)s * chunks + c) + k]);
+                    hi[k] = std::max(hi[k], hp[6 * ((size_t)s * chunks + c) + 3 + k]);
+                }
+            hd[s] = default_h(lo, hi, (double)ns, des_ngb, n_dims);
+        }
+        double* dhd = (double*)scratch(ctx, kSlotNgb1, (size_t)S * 8);
+        check_cuda(cudaMemcpyAsync(dhd, hd.data(), (size_t)S * 8, cudaMemcpyHostToDevice, st), "h2d");
+        check_cuda(cudaStreamSynchronize(st), "sync");  // hd is pageable and goes out of scope
+        a.h_default_sys = dhd;
+    } else if (!h_start) {
         // des_ngb particles at the mean number density of the bounding box of all particles
         const int nb = std::max(1, std::min(grid_of(ctx, t->n), ctx->num_sms * 2));
         double* part = (double*)scratch(ctx, kSlotNgb2, (size_t)nb * 6 * 8);
@@ -541,15 +728,19 @@ void run_density(gt_context* ctx, gt_tree* t, int64_t nt, const uint32_t* target
                 lo[k] = std::min(lo[k], hp[6 * b + k]);
                 hi[k] = std::max(hi[k], hp[6 * b + 3 + k]);
             }
-        const double vol = (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
-        const double n = (double)t->n;
-        a.h_default = std::cbrt(3.0 * des_ngb * vol / (4.0 * M_PI * n));
-        if (n_dims == 1) a.h_default = 0.5 * des_ngb * (hi[0] - lo[0]) / n;
-        if (n_dims == 2) a.h_default = std::sqrt(des_ngb * (hi[0] - lo[0]) * (hi[1] - lo[1]) / (M_PI * n));
+        a.h_default = default_h(lo, hi, (double)t->n, des_ngb, n_dims);
     }
     if (nt <= 0) return;
-    density_kernel<<<grid_of(ctx, nt), kBlk, 0, st>>>(a);
+    const bool one = a.g.n_roots == 1;
+    if (a.tally) density_kernel<true, false><<<grid_of(ctx, nt), kBlk, 0, st>>>(a);
+    else if (one) density_kernel<false, true><<<grid_of(ctx, nt), kBlk, 0, st>>>(a);
+    else density_kernel<false, false><<<grid_of(ctx, nt), kBlk, 0, st>>>(a);
     check_launch(ctx, "density_kernel");
+    if (a.tally) {
+        check_cuda(cudaMemcpyAsync(ctx->pinned, a.tally, GT_NGB_COUNTERS * 8, cudaMemcpyDeviceToHost, st), "d2h");
+        check_cuda(cudaStreamSynchronize(st), "sync");
+        std::memcpy(tally, ctx->pinned, GT_NGB_COUNTERS * 8);
+    }
 }
 
 }  // namespace gt

@@ -906,12 +906,14 @@ __device__ __forceinline__ uint32_t checked_target(const uint32_t* __restrict__ 
 }
 
 // Whether target k starts a group (a new group where the key changes or is negative); also
-// records its tree position.
+// records its tree position.  In a forest a target's system comes from its particle index
+// (in_off): massless particles sit after every live one in tree order, outside sys_off's ranges.
 __device__ __forceinline__ bool target_starts(const uint32_t* __restrict__ targets, int64_t k, int mode,
                                               int param, const uint32_t* __restrict__ rank,
                                               const int* __restrict__ leaf_of, const int* __restrict__ gid,
                                               uint32_t* __restrict__ tpos, const int* __restrict__ sys_off,
-                                              int n_systems, int all_live, int64_t n, unsigned* __restrict__ bad) {
+                                              const int64_t* __restrict__ in_off, int n_systems, int all_live,
+                                              int64_t n, unsigned* __restrict__ bad) {
     const uint32_t p = checked_target(targets, k, n, bad);
     const uint32_t pos = rank[p];
     tpos[k] = pos;
@@ -929,8 +931,8 @@ __device__ __forceinline__ bool target_starts(const uint32_t* __restrict__ targe
         if (n_systems > 1) {
             // a window never spans two systems of a forest; over all live targets the windows of
             // each system start at its first particle, as in its own tree
-            const int s = system_of(sys_off, n_systems, pos);
-            return s != system_of(sys_off, n_systems, rank[q]) ||
+            const int s = system_of(in_off, n_systems, p);
+            return s != system_of(in_off, n_systems, q) ||
                    (all_live ? ((int64_t)pos - sys_off[s]) % param == 0 : (k % param) == 0);
         }
         return (k % param) == 0;
@@ -942,12 +944,13 @@ __global__ void target_flags_kernel(const uint32_t* __restrict__ targets, int64_
                                     int param, const uint32_t* __restrict__ rank,
                                     const int* __restrict__ leaf_of, const int* __restrict__ gid,
                                     uint32_t* __restrict__ tpos, uint32_t* __restrict__ flag,
-                                    const int* __restrict__ sys_off, int n_systems, int all_live,
-                                    int64_t n = INT64_MAX, unsigned* __restrict__ bad = nullptr) {
+                                    const int* __restrict__ sys_off, const int64_t* __restrict__ in_off,
+                                    int n_systems, int all_live, int64_t n = INT64_MAX,
+                                    unsigned* __restrict__ bad = nullptr) {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nt;
          k += (int64_t)gridDim.x * blockDim.x)
-        flag[k] = target_starts(targets, k, mode, param, rank, leaf_of, gid, tpos, sys_off, n_systems, all_live,
-                                n, bad) ? 1u : 0u;
+        flag[k] = target_starts(targets, k, mode, param, rank, leaf_of, gid, tpos, sys_off, in_off, n_systems,
+                                all_live, n, bad) ? 1u : 0u;
 }
 
 // Small explicit target lists (the sparse active sets of deep time bins) form their groups in one
@@ -989,8 +992,8 @@ __global__ void __launch_bounds__(kSmallThreads)
 small_groups_kernel(const uint32_t* __restrict__ targets, int nt, int mode, int param,
                     const uint32_t* __restrict__ rank, const int* __restrict__ leaf_of,
                     const int* __restrict__ gid, uint32_t* __restrict__ tpos,
-                    const int* __restrict__ sys_off, int n_systems, int kmax,
-                    int2* __restrict__ groups, uint32_t* __restrict__ count, int64_t n,
+                    const int* __restrict__ sys_off, const int64_t* __restrict__ in_off, int n_systems,
+                    int kmax, int2* __restrict__ groups, uint32_t* __restrict__ count, int64_t n,
                     unsigned* __restrict__ bad) {
     __shared__ int starts[kSmallTargets + 1];
     __shared__ int wsum[32];
@@ -999,7 +1002,7 @@ small_groups_kernel(const uint32_t* __restrict__ targets, int nt, int mode, int 
     for (int base = 0; base < nt; base += kSmallThreads) {
         const int k = base + (int)threadIdx.x;
         const bool st = k < nt && target_starts(targets, k, mode, param, rank, leaf_of, gid, tpos, sys_off,
-                                                n_systems, 0, n, bad);
+                                                in_off, n_systems, 0, n, bad);
         const int at = block_excl_scan_1024(st ? 1 : 0, wsum, &total);
         if (st) starts[ng + at] = k;
         ng += total;
@@ -1054,15 +1057,22 @@ __global__ void chunk_emit_kernel(const int64_t* __restrict__ starts, int64_t ng
 }
 
 // Forest: the root of each group is the root of the system of its first target (roots are
-// nodes 0 .. n_systems-1, groups never span two systems).
-__global__ void group_root_kernel(const int2* __restrict__ groups, int64_t ng, const uint32_t* __restrict__ tpos,
-                                  const int* __restrict__ sys_off, int n_systems, int* __restrict__ root,
-                                  const uint32_t* __restrict__ ng_dev = nullptr) {
+// nodes 0 .. n_systems-1, groups never span two systems).  All live targets: group members are
+// live tree positions (sys_off); explicit targets: particle indices (in_off), below n as the
+// grouping has checked (an index beyond it has failed the call and reads system 0 here).
+__global__ void group_root_kernel(const int2* __restrict__ groups, int64_t ng, const uint32_t* __restrict__ targets,
+                                  int64_t n, const int* __restrict__ sys_off, const int64_t* __restrict__ in_off,
+                                  int n_systems, int* __restrict__ root, const uint32_t* __restrict__ ng_dev = nullptr) {
     if (ng_dev) ng = min(ng, (int64_t)*ng_dev);
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ng;
          g += (int64_t)gridDim.x * blockDim.x) {
         const int t0 = groups[g].x;
-        root[g] = system_of(sys_off, n_systems, tpos ? (int64_t)tpos[t0] : (int64_t)t0);
+        if (targets) {
+            const int64_t p = (int64_t)targets[t0];
+            root[g] = p < n ? system_of(in_off, n_systems, p) : 0;
+        } else {
+            root[g] = system_of(sys_off, n_systems, (int64_t)t0);
+        }
     }
 }
 
@@ -1354,7 +1364,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                 target_flags_kernel<<<grid1d(ctx, n), 256, 0, st>>>(
                     t->order, n, mode == GT_GROUP_BATCH ? GT_GROUP_BATCH : GT_GROUP_SINGLE, param,
                     t->rank, t->leaf_of, nullptr, (uint32_t*)scratch(ctx, kSlotGroupKey, (size_t)n * 4),
-                    flag, t->sys_off_dev, t->n_systems, 1);
+                    flag, t->sys_off_dev, t->in_off_dev, t->n_systems, 1);
                 check_launch(ctx, "target_flags_kernel");
             }
             ng = finish_groups(ctx, flag, n, kmax, &groups, true);
@@ -1366,8 +1376,8 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                     throw Fail{GT_ERR_NOMEM, "cudaMalloc for the group roots failed"};
                 }
                 roots = (int*)p;
-                group_root_kernel<<<grid1d(ctx, ng), 256, 0, st>>>(groups, ng, nullptr, t->sys_off_dev,
-                                                                   t->n_systems, roots);
+                group_root_kernel<<<grid1d(ctx, ng), 256, 0, st>>>(groups, ng, nullptr, 0, t->sys_off_dev,
+                                                                   t->in_off_dev, t->n_systems, roots);
                 check_launch(ctx, "group_root_kernel");
             }
             if (!rq.capture) check_cuda(cudaStreamSynchronize(st), "sync");
@@ -1395,14 +1405,14 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         if (nt <= kSmallTargets) {
             groups = (int2*)scratch(ctx, kSlotGroupsB, (size_t)nt * sizeof(int2));
             small_groups_kernel<<<1, kSmallThreads, 0, st>>>(rq.targets, (int)nt, mode, param, t->rank, t->leaf_of,
-                                                             gid, tp, t->sys_off_dev, t->n_systems, kmax, groups, gc,
-                                                             t->n, bad);
+                                                             gid, tp, t->sys_off_dev, t->in_off_dev, t->n_systems,
+                                                             kmax, groups, gc, t->n, bad);
             check_launch(ctx, "small_groups_kernel");
             ng_dev = gc + 1;
         } else {
             target_flags_kernel<<<grid1d(ctx, nt), 256, 0, st>>>(rq.targets, nt, mode, param, t->rank,
                                                                  t->leaf_of, gid, tp, flag, t->sys_off_dev,
-                                                                 t->n_systems, 0, t->n, bad);
+                                                                 t->in_off_dev, t->n_systems, 0, t->n, bad);
             check_launch(ctx, "target_flags_kernel");
             groups = finish_groups_dev(ctx, flag, nt, kmax, &ng_dev);
         }
@@ -1410,8 +1420,8 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         tpos = tp;
         if (t->n_systems > 1) {
             roots = (int*)scratch(ctx, kSlotGroupRoot, (size_t)ng * sizeof(int));
-            group_root_kernel<<<grid1d(ctx, ng), 256, 0, st>>>(groups, ng, tpos, t->sys_off_dev, t->n_systems,
-                                                               roots, ng_dev);
+            group_root_kernel<<<grid1d(ctx, ng), 256, 0, st>>>(groups, ng, rq.targets, t->n, t->sys_off_dev,
+                                                               t->in_off_dev, t->n_systems, roots, ng_dev);
             check_launch(ctx, "group_root_kernel");
         }
     }

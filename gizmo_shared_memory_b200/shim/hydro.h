@@ -13,7 +13,8 @@
 //   * The per-centre searches read the particle positions the device holds: those of the build,
 //     or, once the tree has seen an event or a refresh, those uploaded by the first search or walk
 //     after it.  Lazy drift catches up every particle behind the target first.
-//   * ngb_counters / hiter_counters return zeros (the SHMEM_NGB_COUNT diagnostics are not kept).
+//   * ngb_counters / hiter_counters (SHMEM_NGB_COUNT) total every host thread's library context;
+//     read them between searches, as the reference's callers do.
 #pragma once
 #include <cmath>
 

@@ -10,11 +10,22 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "gt.h"
 
 namespace shmem {
 namespace {
+
+// SHMEM_NGB_COUNT (hydro.cc:24-27): every context counts its searches from creation.
+bool ngb_counting() {
+    static const bool v = getenv("SHMEM_NGB_COUNT") != nullptr;
+    return v;
+}
+
+// Every context of the process, for the process-wide counter totals the reference keeps.
+std::mutex g_contexts_mu;
+std::vector<gt_context*> g_contexts;
 
 // One library context per host thread, on device $GT_DEVICE (default 0), created on first use.
 // It is deliberately never destroyed: a destructor running at thread or process exit could call
@@ -24,11 +35,14 @@ gt_context* context() {
     thread_local gt_context* ctx = nullptr;
     if (!ctx) {
         const char* d = getenv("GT_DEVICE");
-        const int st = gt_context_create(d ? atoi(d) : 0, &ctx);
-        if (st != GT_OK) {
-            ctx = nullptr;
-            throw std::runtime_error(std::string("gt_context_create: ") + gt_status_string(st));
-        }
+        gt_context* c = nullptr;
+        const int st = gt_context_create(d ? atoi(d) : 0, &c);
+        if (st != GT_OK) throw std::runtime_error(std::string("gt_context_create: ") + gt_status_string(st));
+        if (ngb_counting() && gt_ngb_count(c, 1) != GT_OK)
+            throw std::runtime_error(std::string("gt_ngb_count: ") + gt_last_error(c));
+        std::lock_guard<std::mutex> lk(g_contexts_mu);
+        g_contexts.push_back(c);
+        ctx = c;
     }
     return ctx;
 }
@@ -495,12 +509,34 @@ long long audit_tree(const Tree& T, const Particles& P, const double*, size_t, c
 
 // ---- neighbour search and the density solve (hydro.h) ------------------------------------------
 
-void ngb_counters(long long& calls, long long& nodes, long long& examined, long long& kept, long long& pad_nodes,
-                  bool) {
-    calls = nodes = examined = kept = pad_nodes = 0;
+// The counters (hydro.cc:28-35, 20-23) summed over every context: each read moves the contexts'
+// device totals into these host totals, which the two readers reset separately, as the
+// reference's do.  Read them where the reference does, between searches.
+static long long g_tally[GT_NGB_COUNTERS] = {};
+
+static void gather_tallies() {
+    std::lock_guard<std::mutex> lk(g_contexts_mu);
+    for (gt_context* c : g_contexts) {
+        int64_t v[GT_NGB_COUNTERS];
+        if (gt_ngb_counters_get(c, v, 1) != GT_OK)
+            throw std::runtime_error(std::string("gt_ngb_counters_get: ") + gt_last_error(c));
+        for (int k = 0; k < GT_NGB_COUNTERS; ++k) g_tally[k] += (long long)v[k];
+    }
 }
-void hiter_counters(long long out[8], bool) {
-    for (int i = 0; i < 8; ++i) out[i] = 0;
+
+void ngb_counters(long long& calls, long long& nodes, long long& examined, long long& kept, long long& pad_nodes,
+                  bool reset) {
+    gather_tallies();
+    calls = g_tally[0]; nodes = g_tally[1]; examined = g_tally[2]; kept = g_tally[3]; pad_nodes = g_tally[4];
+    if (reset)
+        for (int k = 0; k < 5; ++k) g_tally[k] = 0;
+}
+void hiter_counters(long long out[8], bool reset) {
+    gather_tallies();
+    for (int i = 0; i < 8; ++i) {
+        out[i] = g_tally[5 + i];
+        if (reset) g_tally[5 + i] = 0;
+    }
 }
 
 // Before a per-centre search: queued events to the device, lazy catch-up of every particle behind
@@ -532,7 +568,7 @@ static void search_one(const Tree& T, const gt_ngb_options& o, const Vec3d& c, d
     int64_t start[2] = {0, 0}, tot = 0;
     int st = gt_ngb_search(context(), T.gpu.get(), 1, &cx, &cy, &cz, &radius, &o, GT_MEM_HOST, start, buf.data(),
                            (int64_t)buf.size(), &tot);
-    if (st == GT_ERR_OVERFLOW) {
+    if (st == GT_ERR_OVERFLOW) {  // (an overflowed call counts nothing under SHMEM_NGB_COUNT)
         buf.resize((size_t)tot * 2);
         st = gt_ngb_search(context(), T.gpu.get(), 1, &cx, &cy, &cz, &radius, &o, GT_MEM_HOST, start, buf.data(),
                            (int64_t)buf.size(), &tot);
@@ -605,12 +641,16 @@ DensityResult density(const Tree& T, const Particles& P, const std::vector<uint3
             o.elapsed = T.t_since_build;
             std::vector<int64_t> start(nt + 1);
             int64_t tot = 0;
+            // the reference's cache holds the solve's own lists: these searches are not counted
+            if (ngb_counting()) check(gt_ngb_count(context(), 0), "gt_ngb_count");
             const int st = gt_ngb_search(context(), T.gpu.get(), (int64_t)nt, cx.data(), cy.data(), cz.data(),
                                          R.h.data(), &o, GT_MEM_HOST, start.data(), nullptr, 0, &tot);
             check(st, "gt_ngb_search");
             cache->flat.resize((size_t)tot);
-            check(gt_ngb_search(context(), T.gpu.get(), (int64_t)nt, cx.data(), cy.data(), cz.data(), R.h.data(), &o,
-                                GT_MEM_HOST, start.data(), cache->flat.data(), tot, &tot), "gt_ngb_search");
+            const int st2 = gt_ngb_search(context(), T.gpu.get(), (int64_t)nt, cx.data(), cy.data(), cz.data(),
+                                          R.h.data(), &o, GT_MEM_HOST, start.data(), cache->flat.data(), tot, &tot);
+            if (ngb_counting()) check(gt_ngb_count(context(), 1), "gt_ngb_count");
+            check(st2, "gt_ngb_search");
             for (size_t t = 0; t <= nt; ++t) cache->start[t] = (size_t)start[t];
         }
         cache->valid = true;

@@ -329,9 +329,13 @@ GT_API int gt_potential(gt_context* ctx, const gt_tree* tree, int64_t n_targets,
 GT_API int gt_walk_stats_get(const gt_context* ctx, gt_walk_stats* stats);
 
 /* ---- neighbour search and the density solve (shmem/hydro.h:65-117, hydro.cc:37-327) --------
- * On the gravity tree (single-system trees), through search nodes that hold each node's box
- * (shmem::SNode, tree.h:206-226), made on first use.  Lists are in tree order, which is the
- * reference's order for a tree built with GT_KEY_MORTON. */
+ * On the gravity tree, through search nodes that hold each node's box (shmem::SNode,
+ * tree.h:206-226), made on first use.  Lists are in tree order, which is the reference's order for
+ * a tree built with GT_KEY_MORTON.  On a forest (gt_build_systems) a centre searches every system
+ * in turn (system 0's tree order first), or the one system gt_ngb_options.systems names for it; a
+ * density target searches the system that owns its particle index, with that system's own default
+ * h.  Each system then finds exactly what it finds as a tree of its own (particle indices shifted
+ * by its offset).  No reference counterpart for forests: shmem::build makes one tree per call. */
 enum {
     GT_NGB_GATHER = 0,  /* ngb_search (hydro.cc:37-108): particles with r < radius */
     GT_NGB_REVERSE = 1, /* ngb_search_reverse (hydro.cc:110-148): gas particles j < n_gas with radius <= r < h[j] */
@@ -343,6 +347,8 @@ typedef struct {
     double elapsed;    /* Tree::t_since_build: node boxes widen by vmax * elapsed (and always by xpad) */
     int64_t n_gas;     /* reverse: particles [0, n_gas) are gas */
     const double* h;   /* reverse: support radius of each gas particle (n_gas), located like the other arrays */
+    const int32_t* systems; /* per centre, the one system searched (n_centres, in [0, n_systems), located
+                            * like the other arrays; GT_ERR_INVALID otherwise); NULL: every system */
 } gt_ngb_options;
 GT_API void gt_ngb_options_default(gt_ngb_options* opt);
 /* Tree::init_hmax (tree.cc:332-338): per node the largest h, rounded up to float, of the gas
@@ -375,6 +381,22 @@ GT_API void gt_density_options_default(gt_density_options* opt);
 GT_API int gt_density(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const uint32_t* targets,
                const gt_density_options* opt, int mem, double* h, double* rho, int32_t* nngb,
                int32_t* iters);
+/* SHMEM_NGB_COUNT diagnostics (hydro.cc:7-35, 51-106, 293-296; shmem::ngb_counters and
+ * hiter_counters).  While counting is on, this context's gather searches add to its totals:
+ *   [0] calls: gather searches, one per centre and per density evaluation;
+ *   [1] nodes visited;  [2] particles examined in the leaves opened;  [3] neighbours kept;
+ *   [4] nodes admitted only by the vmax * elapsed and xpad pads (elapsed > 0 only);
+ *   [5 + i] density targets that took i + 1 iterations (i = 7: 8 or more, the 100 of a solve that
+ *   did not converge included).
+ * gt_ngb_search counts the centres of the gather and pairs modes once the call has delivered its
+ * lists: a count-only call (found NULL) or one that overflows counts nothing, so counting and then
+ * filling counts each search once.  gt_density counts every evaluation.  Off by default; the
+ * counting variants of the kernels are separate instantiations, so the plain ones are unchanged.
+ * gt_ngb_counters_get copies the totals (GT_NGB_COUNTERS int64) and zeroes them when reset is
+ * non-zero. */
+#define GT_NGB_COUNTERS 13
+GT_API int gt_ngb_count(gt_context* ctx, int enable);
+GT_API int gt_ngb_counters_get(gt_context* ctx, int64_t* counts, int reset);
 
 /* ---- autotuner ----------------------------------------------------------------------------- */
 /* One candidate launch configuration of the all-active grouped walk and what it measured. */

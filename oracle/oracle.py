@@ -431,6 +431,7 @@ class Reference:
                                             C.c_double, _d, _d, _d]
         L.ref_tree_nsink.argtypes = [C.c_void_p, _u32]
         L.ref_set_elapsed.argtypes = [C.c_void_p, C.c_double]
+        L.ref_ngb_counters.argtypes = [_i64, C.c_int]
         L.ref_init_hmax.argtypes = [C.c_void_p, _d, C.c_int64, _f]
         L.ref_raise_hmax.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, _d]
         L.ref_ngb_search.argtypes = [C.c_void_p, C.c_int64, _d, _d, _d, _d, C.c_int, _d, C.c_int64, C.c_double,
@@ -488,6 +489,13 @@ class Reference:
     def build(self, P, randomize_seed=-1, vel=None):
         """vel = (vx, vy, vz): build with velocities (per-node vcom and vmax, for the jerk)."""
         return ReferenceTree(self, P, randomize_seed, vel)
+
+    def ngb_counters(self, reset=False):
+        """The reference's SHMEM_NGB_COUNT totals (13 int64: calls, nodes, examined, kept, pad
+        nodes, iteration histogram[8]); zeros unless SHMEM_NGB_COUNT was set before the first search."""
+        v = np.zeros(13, np.int64)
+        self.L.ref_ngb_counters(_p(v, _i64), int(bool(reset)))
+        return v
 
     def build_gas(self, P):
         """Build with P["type"] (uint8, GIZMO numbering) and P["zeta"] (adaptive-softening terms)."""

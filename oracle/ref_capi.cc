@@ -308,6 +308,16 @@ extern "C" {
 // Tree::t_since_build (the staleness pad of the search prune).
 void ref_set_elapsed(void* p, double elapsed) { static_cast<RefHandle*>(p)->T.t_since_build = elapsed; }
 
+// The SHMEM_NGB_COUNT totals (hydro.cc:20-35): calls, nodes, examined, kept, pad nodes, then the
+// iteration histogram (8).  Zero unless SHMEM_NGB_COUNT was in the environment at the first search.
+void ref_ngb_counters(int64_t* out, int reset) {
+    long long c[5], h[8];
+    ngb_counters(c[0], c[1], c[2], c[3], c[4], reset != 0);
+    hiter_counters(h, reset != 0);
+    for (int k = 0; k < 5; ++k) out[k] = c[k];
+    for (int k = 0; k < 8; ++k) out[5 + k] = h[k];
+}
+
 // Tree::init_hmax (tree.cc:332-338) and a copy of the result (nnodes floats; may be null).
 void ref_init_hmax(void* p, const double* h, int64_t n_gas, float* hmax_out) {
     RefHandle* H = static_cast<RefHandle*>(p);

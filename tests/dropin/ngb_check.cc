@@ -10,7 +10,9 @@
 // then searches, for every 50th gas particle, both ways: ngb_search at its h and
 // ngb_search_reverse (gas neighbours whose own kernel reaches it).  OUT receives, as int64 and
 // float64 blocks: the counts, the iteration numbers and the h and rho of the solve, the cache
-// (offsets and indices), and the gather and reverse lists (offsets and indices).
+// (offsets and indices), the gather and reverse lists (offsets and indices), and the
+// SHMEM_NGB_COUNT totals of all of it (ngb_counters then hiter_counters; zeros unless the
+// variable is set).
 #include "hydro.h"
 
 #include <cstdio>
@@ -74,6 +76,12 @@ int main(int argc, char** argv) {
     put64(cstart); putu(cache.flat);
     put64(gstart); putu(gather);
     put64(rstart); putu(reverse);
+    long long c[5], hh[8];
+    ngb_counters(c[0], c[1], c[2], c[3], c[4], true);
+    hiter_counters(hh, true);
+    std::vector<int64_t> counts(c, c + 5);
+    counts.insert(counts.end(), hh, hh + 8);
+    put64(counts);
     fclose(fo);
     printf("ngb_check: %zu targets, %zu gather, %zu reverse\n", targets.size(), gather.size(), reverse.size());
     return 0;

@@ -2,7 +2,8 @@
 one launch.  Each system must come out exactly as if it had been built and walked alone with
 gt_build: the same keys, order and cells, and bit-identical accelerations (the walk visits the same
 nodes in the same order, only the node numbering differs), for windowed, leaf and explicit-target
-walks.  Systems include an empty one and one with massless particles."""
+walks.  Systems include an empty one and one with massless particles.  The neighbour search and
+the density solve on the forest must likewise reproduce each system's own tree."""
 import numpy as np
 import pytest
 
@@ -185,3 +186,112 @@ def test_forest_with_gas_rules_bit_identical(gpu_ctx, batch):
         px, _, _ = gpu_ctx.accel_grouped(plain, None, theta=0.7, **kw)
         acted |= not np.array_equal(px[m], sx[m])
     assert acted  # the gas rules changed some forces
+
+
+def local_targets(P, off, S, rng, massless=True):
+    """Per system (visited in random order) a sorted random subset of its particle indices,
+    massless ones included when asked: the forest's global list and each system's local list."""
+    glob, loc = [], {}
+    for s in rng.permutation(S):
+        n = off[s + 1] - off[s]
+        if n == 0:
+            continue
+        pool = np.arange(n) if massless else np.nonzero(P["m"][off[s]:off[s + 1]] > 0)[0]
+        sub = np.sort(rng.choice(pool, size=max(1, len(pool) // 3), replace=False)).astype(np.uint32)
+        glob.append(sub + np.uint32(off[s]))
+        loc[s] = sub
+    return np.concatenate(glob), loc
+
+
+@pytest.mark.parametrize("mode", [g.GT_GROUP_LEAF, g.GT_GROUP_SINGLE])
+def test_forest_massless_targets_walk_their_own_system(gpu_ctx, batch, forest, mode):
+    """Massless particles sit after every live one in tree order, outside every system's live
+    range: an explicit target list holding massless particles must still walk each one in its own
+    system, bit-identical to the separate walks."""
+    P, off = batch
+    F, trees = forest
+    S = len(off) - 1
+    rng = np.random.default_rng(11)
+    tl, loc = local_targets(P, off, S, rng)
+    assert np.any(P["m"][tl] == 0)
+    got = np.stack(gpu_ctx.accel_grouped(F, tl, theta=0.7, group_mode=mode))
+    k = 0
+    for s in loc:
+        r = np.stack(gpu_ctx.accel_grouped(trees[s], loc[s], theta=0.7, group_mode=mode))
+        assert np.array_equal(got[:, k:k + len(loc[s])], r), s
+        k += len(loc[s])
+    assert k == len(tl)
+
+
+def test_forest_neighbour_search(gpu_ctx, batch, forest):
+    """A centre with no system named searches every system in turn: its gather (reverse) list is
+    the concatenation, in system order, of the separate trees' gather (reverse) lists, indices
+    shifted by the offsets, and its pair list all the gathers followed by all the reverses.  With a
+    system named, exactly that system's lists."""
+    P, off = batch
+    F, trees = forest
+    S = len(off) - 1
+    rng = np.random.default_rng(5)
+    n = len(P["m"])
+    # centres on particles of every system, plus points between the systems
+    pick = rng.choice(n, 300, replace=False)
+    cen = [np.concatenate([P[k][pick], rng.uniform(P[k].min(), P[k].max(), 100)]) for k in "xyz"]
+    rad = rng.uniform(0.05, 2.0, len(cen[0]))
+    nc = len(rad)
+    h = rng.uniform(0.05, 1.0, n)
+    gpu_ctx.tree_hmax(F, h, n)
+    for s, t in enumerate(trees):
+        gpu_ctx.tree_hmax(t, h[off[s]:off[s + 1]], off[s + 1] - off[s])
+
+    def lists(T, mode, hh, ng, shift, **kw):
+        st, f = gpu_ctx.ngb_search(T, *cen, rad, mode=mode, h=hh, n_gas=ng, **kw)
+        f = f.astype(np.int64) + shift
+        return [f[st[c]:st[c + 1]] for c in range(nc)]
+
+    per = {m: [lists(t, m, h[off[s]:off[s + 1]], off[s + 1] - off[s], off[s]) for s, t in enumerate(trees)]
+           for m in (g.GT_NGB_GATHER, g.GT_NGB_REVERSE)}
+    want = {m: [np.concatenate([per[m][s][c] for s in range(S)]) for c in range(nc)] for m in per}
+    want[g.GT_NGB_PAIRS] = [np.concatenate([want[g.GT_NGB_GATHER][c], want[g.GT_NGB_REVERSE][c]])
+                            for c in range(nc)]
+    sysid = rng.integers(0, S, nc).astype(np.int32)
+    for mode in (g.GT_NGB_GATHER, g.GT_NGB_REVERSE, g.GT_NGB_PAIRS):
+        got = lists(F, mode, h, n, 0)
+        for c in range(nc):
+            assert np.array_equal(got[c], want[mode][c]), (mode, c)
+        got = lists(F, mode, h, n, 0, systems=sysid)
+        for c in range(nc):
+            s = sysid[c]
+            w = {g.GT_NGB_GATHER: per[g.GT_NGB_GATHER][s][c], g.GT_NGB_REVERSE: per[g.GT_NGB_REVERSE][s][c]}
+            w[g.GT_NGB_PAIRS] = np.concatenate([w[g.GT_NGB_GATHER], w[g.GT_NGB_REVERSE]])
+            assert np.array_equal(got[c], w[mode]), (mode, c)
+    assert sum(len(x) for x in want[g.GT_NGB_GATHER]) > 10 * nc
+    with pytest.raises(g.GTError):
+        gpu_ctx.ngb_search(F, *cen, rad, systems=np.full(nc, S, np.int32))
+
+def test_forest_density(gpu_ctx, batch, forest):
+    """Each density target searches the system that owns it, from that system's own default h
+    (the mean density of its own particles): bit-identical to the separate solves, cold and warm,
+    massless targets included."""
+    P, off = batch
+    F, trees = forest
+    S = len(off) - 1
+    rng = np.random.default_rng(9)
+    tl, loc = local_targets(P, off, S, rng)
+    d = gpu_ctx.density(F, tl, des_ngb=32.0)
+    k = 0
+    hs = np.empty(len(tl))
+    for s in loc:
+        r = gpu_ctx.density(trees[s], loc[s], des_ngb=32.0)
+        seg = slice(k, k + len(loc[s]))
+        for key in ("h", "rho", "nngb", "iters"):
+            assert np.array_equal(d[key][seg], r[key]), (s, key)
+        hs[seg] = 1.2 * r["h"]
+        k += len(loc[s])
+    w = gpu_ctx.density(F, tl, des_ngb=32.0, h_start=hs)
+    k = 0
+    for s in loc:
+        seg = slice(k, k + len(loc[s]))
+        r = gpu_ctx.density(trees[s], loc[s], des_ngb=32.0, h_start=hs[seg])
+        for key in ("h", "rho", "nngb", "iters"):
+            assert np.array_equal(w[key][seg], r[key]), (s, key)
+        k += len(loc[s])

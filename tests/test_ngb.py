@@ -148,3 +148,65 @@ def test_errors(gpu_ctx, golden):
     assert st.tolist() == [0] and f.size == 0
     with pytest.raises(g.GTError):
         gpu_ctx.density(T, np.array([0], np.uint32), n_dims=4)
+
+
+@pytest.fixture(scope="module")
+def ngb_counts():
+    import os
+
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ngb_counts.npz")
+    return dict(np.load(here))
+
+
+def test_counters_match_reference(gpu_ctx, golden, ngb_tree, ngb_counts):
+    """SHMEM_NGB_COUNT (hydro.cc:7-35): the totals of the reference's own search and solve on the
+    same inputs (tests/golden/ngb_counts.npz).  The counts are integers over the same traversal in
+    the same node order: nodes visited, particles examined, neighbours kept and pad-only nodes are
+    identical, and so is the density's iteration histogram wherever every target took the
+    reference's number of iterations (else within the targets that did not)."""
+    cen = [golden[f"ngb_c{k}"] for k in "xyz"]
+    rad = golden["ngb_radius"]
+    n_gas = int(golden["ngb_n_gas"][0])
+    gpu_ctx.ngb_count(True)
+    try:
+        gpu_ctx.ngb_counters(reset=True)
+        gpu_ctx.ngb_search(ngb_tree, *cen, rad)
+        c = gpu_ctx.ngb_counters(reset=True)
+        ref = ngb_counts["gather"]
+        assert [c["calls"], c["nodes"], c["examined"], c["kept"], c["pad_nodes"]] == ref[:5].tolist()
+        assert not c["hiter"].any()
+        # the reverse search is not counted; a pair search counts its gather half
+        gpu_ctx.ngb_search(ngb_tree, *cen, rad, mode=g.GT_NGB_PAIRS, h=golden["ngb_h_part"][:n_gas], n_gas=n_gas)
+        c = gpu_ctx.ngb_counters(reset=True)
+        assert [c["calls"], c["nodes"], c["examined"], c["kept"], c["pad_nodes"]] == ref[:5].tolist()
+        # a stale tree: the vmax * elapsed pad admits nodes that only it admits
+        T = gpu_ctx.build(particles(golden), key_mode=g.GT_KEY_MORTON)
+        gpu_ctx.tree_velocities(T, ngb_counts["vx"], ngb_counts["vy"], ngb_counts["vz"])
+        el = float(ngb_counts["stale_elapsed"][0])
+        st, f = gpu_ctx.ngb_search(T, *cen, rad, elapsed=el)
+        assert np.array_equal(st, ngb_counts["stale_start"]) and np.array_equal(f, ngb_counts["stale_found"])
+        c = gpu_ctx.ngb_counters(reset=True)
+        ref = ngb_counts["stale"]
+        assert ref[4] > 0
+        assert [c["calls"], c["nodes"], c["examined"], c["kept"], c["pad_nodes"]] == ref[:5].tolist()
+        # the density solve: one gather search per evaluation, and the iteration histogram
+        d = gpu_ctx.density(ngb_tree, golden["ngb_targets"], 32.0, 0.05)
+        c = gpu_ctx.ngb_counters(reset=False)
+        ref = ngb_counts["density"]
+        it = d["iters"]
+        assert c["calls"] == int((it + 1).sum())
+        used = np.where(it < 100, it + 1, 100)
+        assert np.array_equal(c["hiter"], np.bincount(np.minimum(used, 8) - 1, minlength=8))
+        if np.array_equal(it, golden["ngb_cold_iters"]):
+            assert [c["calls"], c["nodes"], c["examined"], c["kept"], c["pad_nodes"]] == ref[:5].tolist()
+            assert np.array_equal(c["hiter"], ref[5:])
+        else:
+            for k, i in (("calls", 0), ("nodes", 1), ("examined", 2), ("kept", 3)):
+                assert abs(c[k] - ref[i]) <= 0.01 * ref[i], k
+        # reading without reset keeps the totals; counting off adds nothing
+        assert gpu_ctx.ngb_counters(reset=True)["calls"] == c["calls"]
+        gpu_ctx.ngb_count(False)
+        gpu_ctx.ngb_search(ngb_tree, *cen, rad)
+        assert gpu_ctx.ngb_counters()["calls"] == 0
+    finally:
+        gpu_ctx.ngb_count(False)

@@ -345,3 +345,24 @@ def test_gas_direct_sum_matches_golden(oracle, golden):
     sub = golden["gas_sub"]
     ax, ay, az = oracle.direct_gas(P, sub, type=ty, zeta=ze)
     assert relerr(ax, ay, az, golden["gas_brute_ax"], golden["gas_brute_ay"], golden["gas_brute_az"]).max() < 1e-12
+
+
+def test_ngb_count_fixture_consistent_with_golden(golden):
+    """The reference's SHMEM_NGB_COUNT totals (tests/golden/ngb_counts.npz, hydro.cc:7-35) agree with
+    its own lists and solve in golden.npz: one call per centre and per density evaluation, the
+    neighbours kept equal the gather lists, the iteration histogram is that of the cold solve's
+    iteration counts, and the stale tree keeps the fresh tree's neighbours."""
+    import os
+
+    c = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ngb_counts.npz")))
+    nc = len(golden["ngb_radius"])
+    for k in ("gather", "stale"):
+        assert c[k][0] == nc and c[k][3] == len(golden["ngb_gather_found"])
+        assert c[k][2] >= c[k][3] and not c[k][5:].any()
+    assert c["gather"][4] == 0 and c["stale"][4] > 0 and c["stale"][1] > c["gather"][1]
+    assert np.array_equal(c["stale_start"], golden["ngb_gather_start"])
+    assert np.array_equal(c["stale_found"], golden["ngb_gather_found"])
+    it = golden["ngb_cold_iters"]
+    assert c["density"][0] == int((it + 1).sum())
+    used = np.where(it < 100, it + 1, 100)
+    assert np.array_equal(c["density"][5:], np.bincount(np.minimum(used, 8) - 1, minlength=8))
