@@ -258,13 +258,18 @@ __global__ void keys_kernel(const double* __restrict__ x, const double* __restri
                             const double* __restrict__ z, const double* __restrict__ m, int64_t n,
                             const RootGeom* __restrict__ gp, int key_mode, int levels,
                             uint64_t* __restrict__ keys, uint32_t* __restrict__ idx,
-                            const int64_t* __restrict__ sys_in, int n_systems, uint64_t* __restrict__ sys_key) {
+                            const int64_t* __restrict__ sys_in, int n_systems, uint64_t* __restrict__ sys_key,
+                            double2* __restrict__ pk) {
     __shared__ uint16_t tab[48 * 8];
     for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x) tab[k] = kPhStep[k];
     __syncthreads();
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         idx[i] = (uint32_t)i;
+        // x, y, z, m packed in one 32-byte sector per particle: the gather into tree order then
+        // reads one sector per particle through the permutation instead of four
+        pk[2 * i] = make_double2(x[i], y[i]);
+        pk[2 * i + 1] = make_double2(z[i], m[i]);
         // forest: the particle's own system's root cell; the second sort key is the system
         // (massless particles of every system go last)
         const int s = n_systems > 1 ? system_of(sys_in, n_systems, i) : 0;
@@ -292,29 +297,29 @@ __global__ void keys_kernel(const double* __restrict__ x, const double* __restri
 }
 
 // ---- 4. gather into tree order ---------------------------------------------------------------
-__global__ void gather_kernel(const double* __restrict__ x, const double* __restrict__ y,
-                              const double* __restrict__ z, const double* __restrict__ m,
-                              const double* __restrict__ soft, const uint32_t* __restrict__ idx,
-                              int64_t n, SrcP* __restrict__ src, double* __restrict__ ssoft,
-                              double* __restrict__ smass, uint32_t* __restrict__ order,
-                              uint32_t* __restrict__ rank, int* __restrict__ leaf_of,
-                              int* __restrict__ sleaf, unsigned long long* __restrict__ bad_soft) {
+// Tree order: x, y, z, m from the packed copy the keys pass wrote (pk), the softening from its own
+// array.  leaf_of is preset to -1 by a memset (the moments pass sets the live particles' leaves).
+__global__ void gather_kernel(const double2* __restrict__ pk, const double* __restrict__ soft,
+                              const uint32_t* __restrict__ idx, int64_t n, SrcP* __restrict__ src,
+                              double* __restrict__ ssoft, double* __restrict__ smass, uint32_t* __restrict__ order,
+                              uint32_t* __restrict__ rank, int* __restrict__ sleaf,
+                              unsigned long long* __restrict__ bad_soft) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t p = idx[i];
+        const double2 a = __ldg(pk + 2 * (int64_t)p), b = __ldg(pk + 2 * (int64_t)p + 1);
         SrcP r;
-        r.x = x[p]; r.y = y[p]; r.z = z[p];
+        r.x = a.x; r.y = a.y; r.z = b.x;
         const double sp = soft ? soft[p] : 0.0;
         // softenings that arrived after the bounding-box pass are checked here
         if (bad_soft && !isfinite(sp)) atomicAdd(bad_soft, 1ull);
-        r.m = (float)m[p];
+        r.m = (float)b.y;
         r.soft = (float)sp;
         src[i] = r;
         ssoft[i] = sp;
-        smass[i] = m[p];
+        smass[i] = b.y;
         order[i] = p;
         rank[p] = (uint32_t)i;
-        leaf_of[p] = -1;
         sleaf[i] = -1;
     }
 }
@@ -832,9 +837,12 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
     uint32_t* idx = (uint32_t*)scratch(ctx, kSlotValsA, (size_t)std::max<int64_t>(n, 1) * 4);
     uint64_t* sys_key = nullptr;
     if (S > 1) sys_key = dalloc<uint64_t>((size_t)std::max<int64_t>(n, 1), st);
+    // the packed x, y, z, m (32 bytes per particle) until the gather; the structure stage reuses
+    // the slot afterwards
+    double2* pk = (double2*)scratch(ctx, kSlotNodeTmp0, (size_t)std::max<int64_t>(n, 1) * 32);
     if (n > 0) {
         keys_kernel<<<grid_for(ctx, n), kBlk, 0, st>>>(x, y, z, m, n, gdev, o.key_mode, o.max_level, keys, idx,
-                                                       in_off_dev, S, sys_key);
+                                                       in_off_dev, S, sys_key, pk);
         check_launch(ctx, "keys_kernel");
     }
     check_cuda(cudaEventRecord(ev[2], st), "event");
@@ -882,9 +890,9 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
                 check_cuda(cudaMemsetAsync(bad_soft, 0, 8, st), "memset");
             }
         }
-        gather_kernel<<<grid_for(ctx, n), kBlk, 0, st>>>(x, y, z, m, soft, idx, n, t->src, t->ssoft,
-                                                         t->smass, t->order, t->rank, t->leaf_of, t->sleaf,
-                                                         bad_soft);
+        check_cuda(cudaMemsetAsync(t->leaf_of, 0xff, (size_t)n * sizeof(int), st), "memset");
+        gather_kernel<<<grid_for(ctx, n), kBlk, 0, st>>>(pk, soft, idx, n, t->src, t->ssoft, t->smass, t->order,
+                                                         t->rank, t->sleaf, bad_soft);
         check_launch(ctx, "gather_kernel");
         if (bad_soft) {
             unsigned long long bad = 0;
