@@ -68,7 +68,7 @@ class WalkOptions(C.Structure):
                 ("block_warps", C.c_int), ("list_capacity", C.c_int),
                 ("stack_capacity", C.c_int), ("dtype_out_f32", C.c_int),
                 ("mac_model", C.c_void_p), ("mac_kappa", C.c_double), ("mac_band", C.c_double * 2),
-                ("sink_direct_radius", C.c_double)]
+                ("sink_direct_radius", C.c_double), ("no_window_pairs", C.c_int)]
 
 
 class TuneEntry(C.Structure):
@@ -397,10 +397,11 @@ class Context:
     # ---- walks -----------------------------------------------------------------------------
     def _walk_opts(self, group_mode=GT_GROUP_LEAF, group_max=32, out_order=GT_OUT_TARGETS,
                    count=False, block_warps=0, async_=False, mac=GT_MAC_PLAIN, mac_model=None, list_capacity=0,
-                   mac_kappa=1.0, mac_band=(0.0, 0.0), sink_direct_radius=0.0):
+                   mac_kappa=1.0, mac_band=(0.0, 0.0), sink_direct_radius=0.0, window_pairs=True):
         o = WalkOptions()
         load_library().gt_walk_options_default(C.byref(o))
         o.sink_direct_radius = sink_direct_radius
+        o.no_window_pairs = 0 if window_pairs else 1
         o.group_mode = group_mode
         o.group_max = group_max
         o.out_order = out_order

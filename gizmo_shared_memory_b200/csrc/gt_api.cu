@@ -256,6 +256,7 @@ void walk_common(gt_context* ctx, const gt_tree* tree, int64_t n_targets, const 
     rq.block_warps = o.block_warps;
     rq.list_capacity = o.list_capacity;
     rq.stack_capacity = o.stack_capacity;
+    rq.pair_windows = o.no_window_pairs == 0;
     rq.bufs = bufs;
     rq.capture = capture;
     rq.sink_radius = o.sink_direct_radius;

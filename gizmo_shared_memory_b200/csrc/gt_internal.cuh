@@ -272,6 +272,7 @@ struct WalkRequest {
     double mac_kappa = 1.0, mac_band_lo = 0.0, mac_band_hi = 0.0;
     bool count = false;
     int block_warps = 0, list_capacity = 0, stack_capacity = 0;
+    bool pair_windows = true;     // windows of 17-32 targets: two per warp (walk_pair_kernel)
     WalkBuffers* bufs = nullptr;  // plan-owned buffers; null: the context workspace
     bool capture = false;         // being captured into a graph: no events, no read-back
     double *ax = nullptr, *ay = nullptr, *az = nullptr, *phi = nullptr;  // device outputs

@@ -27,6 +27,7 @@
 //     the factor G are FP64.
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 #include "gt_internal.cuh"
 #include "gt_mac.cuh"
@@ -856,6 +857,387 @@ walk_kernel(const WalkArgs A) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Paired windows
+// ---------------------------------------------------------------------------------------------
+// Two consecutive windows of a batch walk (groups 2p and 2p+1 of the list, up to 32 targets each)
+// share one traversal.  Each stack entry carries, in its two low bits, the windows for which its
+// parent was opened, and a popped node is tested against the boxes of those windows only.  So each
+// window tests exactly the nodes its own walk tests, makes the same decisions and collects the
+// same monopoles and particles, into its own lists.  The pop, the node load, the child pushes and
+// the expanded leaves' particle loads are shared: windows adjacent in Peano-Hilbert order open
+// mostly the same nodes.  Lane l holds target l of each window; the lists are evaluated window by
+// window with walk_kernel's packed monopole loop.  A window's nodes can join its list in another
+// order than in its own walk (the other window's nodes interleave on the stack), so the sums agree
+// with walk_kernel's to FP32 rounding, not bit for bit.  One target per lane, the grouped walk,
+// the plain or per-node learned criterion, one system.
+
+struct alignas(16) PairHdr {
+    int lo[32];   // leaf-expansion scratch: first slot, exclusive prefix and windows of each leaf
+    int pre[32];
+    int msk[32];
+    // per window: box corners, centre, largest target softening, smallest aold
+    double lo_x[2], lo_y[2], lo_z[2], hi_x[2], hi_y[2], hi_z[2], c_x[2], c_y[2], c_z[2], emax[2], amin[2];
+};
+
+__host__ __device__ constexpr int pair_list_bytes(int pn_cap, int pp_cap) { return pn_cap * 16 + pp_cap * 20; }
+__host__ __device__ constexpr int pair_smem_bytes(int pn_cap, int pp_cap) {
+    return ((int)sizeof(PairHdr) + 2 * pair_list_bytes(pn_cap, pp_cap) + 15) & ~15;
+}
+
+template <bool WANT_POT, bool COUNT, int MAC>
+__global__ void __launch_bounds__(kMaxWarps * 32, 3) walk_pair_kernel(const WalkArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + w;
+    int* __restrict__ stk = A.stack + (size_t)gw * A.stack_cap;
+    unsigned char* wbase = smem_raw + (size_t)w * A.warp_bytes;
+    PairHdr& S = *reinterpret_cast<PairHdr*>(wbase);
+    const int list_bytes = pair_list_bytes(A.pn_cap, A.pp_cap);
+    // window v's lists: monopoles (pn_cap float4, paired layout), particles (pp_cap float4) and
+    // their softenings (pp_cap float)
+    auto pn_of = [&](int v) { return reinterpret_cast<float4*>(wbase + sizeof(PairHdr) + (size_t)v * list_bytes); };
+    auto pp_of = [&](int v) { return pn_of(v) + A.pn_cap; };
+    auto ph_of = [&](int v) { return reinterpret_cast<float*>(pp_of(v) + A.pp_cap); };
+    const int n_groups = A.n_groups_dev ? (int)*A.n_groups_dev : A.n_groups;
+    const int n_pairs = (n_groups + 1) >> 1;
+    // SHMEM_COUNT_WALK: per window, as walk_kernel counts them (node tests, monopoles and
+    // particles times the window's targets, r = 0 pairs), so a paired walk counts what the two
+    // one-window walks count
+    unsigned long long c_nodes = 0, c_multi = 0, c_pairs = 0, c_zero = 0, c_flush = 0, c_steps = 0;
+    int c_maxtop = 0;
+
+    for (;;) {
+        int pr = 0;
+        if (lane == 0) pr = (int)atomicAdd(A.next_group, 1u);
+        pr = __shfl_sync(kFull, pr, 0);
+        if (pr >= n_pairs) break;
+        int t0[2], nt[2];
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            const int g = 2 * pr + v;
+            const int2 gr = g < n_groups ? A.groups[g] : make_int2(0, 0);
+            t0[v] = gr.x;
+            nt[v] = gr.y - gr.x;
+        }
+
+        // ---- targets: lane l holds target l of each window ---------------------------------
+        float tx[2], ty[2], tz[2], th[2];
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            double px = 0.0, py = 0.0, pz = 0.0, ps = 0.0;
+            double lx = 1e300, ly = 1e300, lz = 1e300, hx = -1e300, hy = -1e300, hz = -1e300;
+            double amin = A.aold ? 1e300 : 0.0;
+            if (lane < nt[v]) {
+                int p = A.tpos ? (int)A.tpos[t0[v] + lane] : t0[v] + lane;
+                if (!GT_IN_BOUNDS(p, A.n_src)) p = 0;
+                float mf, hf;
+                load_src(A.src + p, px, py, pz, mf, hf);
+                ps = A.ssoft[p];
+                lx = hx = px;
+                ly = hy = py;
+                lz = hz = pz;
+                if (A.aold) amin = A.aold[t0[v] + lane];
+            }
+            lx = wmin(lx); ly = wmin(ly); lz = wmin(lz);
+            hx = wmax(hx); hy = wmax(hy); hz = wmax(hz);
+            const double emax = wmax(ps);
+            if (A.aold) amin = wmin(amin);
+            const double cx = 0.5 * (lx + hx), cy = 0.5 * (ly + hy), cz = 0.5 * (lz + hz);
+            if (lane == 0) {
+                S.lo_x[v] = lx; S.lo_y[v] = ly; S.lo_z[v] = lz;
+                S.hi_x[v] = hx; S.hi_y[v] = hy; S.hi_z[v] = hz;
+                S.c_x[v] = cx; S.c_y[v] = cy; S.c_z[v] = cz;
+                S.emax[v] = emax; S.amin[v] = amin;
+            }
+            tx[v] = (float)(px - cx);
+            ty[v] = (float)(py - cy);
+            tz[v] = (float)(pz - cz);
+            th[v] = (float)ps;
+        }
+        __syncwarp();
+        float sx0 = 0.0f, sy0 = 0.0f, sz0 = 0.0f, cx0 = 0.0f, cy0 = 0.0f, cz0 = 0.0f;
+        float sx1 = 0.0f, sy1 = 0.0f, sz1 = 0.0f, cx1 = 0.0f, cy1 = 0.0f, cz1 = 0.0f;
+        double pot0 = 0.0, pot1 = 0.0;
+        // one window's partial sums into its Kahan-compensated totals (v at run time: the
+        // evaluation loops below exist once in the code, for both windows)
+        auto add_partial = [&](int v, float ax, float ay, float az, float ap) {
+            if (v == 0) {
+                kahan_add(sx0, cx0, ax); kahan_add(sy0, cy0, ay); kahan_add(sz0, cz0, az);
+                if (WANT_POT) pot0 += (double)ap;
+            } else {
+                kahan_add(sx1, cx1, ax); kahan_add(sy1, cy1, ay); kahan_add(sz1, cz1, az);
+                if (WANT_POT) pot1 += (double)ap;
+            }
+        };
+        // monopole-list entry pos of window v, in walk_kernel's paired layout (see flush_pn there)
+        auto pn_put = [&](int v, int pos, float x, float y, float z, float m) {
+            float* q = reinterpret_cast<float*>(pn_of(v) + 2 * (pos >> 1)) + (pos & 1);
+            q[0] = x; q[2] = y; q[4] = z; q[6] = m;
+        };
+        // window v's monopoles against its targets: walk_kernel's packed loop
+        auto flush_pn = [&](int v, int n) {
+            if ((n & 1) && lane == 0) pn_put(v, n, 0.0f, 0.0f, 0.0f, 0.0f);
+            __syncwarp();
+            const int np = (n + 1) >> 1;
+            float2 ax2 = make_float2(0.0f, 0.0f), ay2 = ax2, az2 = ax2, ap2 = ax2;
+            const float qx = v ? tx[1] : tx[0], qy = v ? ty[1] : ty[0], qz = v ? tz[1] : tz[0];
+            const float2 ntx = make_float2(-qx, -qx), nty = make_float2(-qy, -qy), ntz = make_float2(-qz, -qz);
+            const float2 r2_floor = make_float2(1e-30f, 1e-30f);
+            const float4* __restrict__ L = pn_of(v);
+#pragma unroll 8
+            for (int jp = 0; jp < np; ++jp) {
+                const float4 P = L[2 * jp], Q = L[2 * jp + 1];
+                const float2 X = make_float2(P.x, P.y), Y = make_float2(P.z, P.w);
+                const float2 Z = make_float2(Q.x, Q.y), M = make_float2(Q.z, Q.w);
+                const float2 dx = __fadd2_rn(X, ntx), dy = __fadd2_rn(Y, nty), dz = __fadd2_rn(Z, ntz);
+                const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, r2_floor)));
+                const float2 ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+                const float2 mri = __fmul2_rn(M, ri);
+                const float2 f = __fmul2_rn(mri, __fmul2_rn(ri, ri));
+                ax2 = __ffma2_rn(dx, f, ax2);
+                ay2 = __ffma2_rn(dy, f, ay2);
+                az2 = __ffma2_rn(dz, f, az2);
+                if (WANT_POT) ap2 = __fadd2_rn(ap2, mri);
+            }
+            add_partial(v, ax2.x + ax2.y, ay2.x + ay2.y, az2.x + az2.y, -(ap2.x + ap2.y));
+            if (COUNT) c_flush += (lane == 0);
+            __syncwarp();
+        };
+        // window v's particles: the kernel of the larger softening; r^2 == 0 contributes 0
+        auto flush_pp = [&](int v, int n) {
+            __syncwarp();
+            float ax = 0.0f, ay = 0.0f, az = 0.0f, ap = 0.0f;
+            const float qx = v ? tx[1] : tx[0], qy = v ? ty[1] : ty[0], qz = v ? tz[1] : tz[0];
+            const float qh = v ? th[1] : th[0];
+            const float4* __restrict__ L = pp_of(v);
+            const float* __restrict__ H = ph_of(v);
+            for (int j = 0; j < n; ++j) {
+                const float4 e = L[j];
+                const float hj = H[j];
+                const float dx = e.x - qx, dy = e.y - qy, dz = e.z - qz;
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const float hh = fmaxf(qh, hj);
+                float f, p;
+                if (r2 >= hh * hh && r2 > 0.0f) {
+                    const float ri = rsqrtf(r2);
+                    const float mri = e.w * ri;
+                    f = mri * ri * ri;
+                    p = -mri;
+                } else {
+                    spline_pair(r2, hh, e.w, f, p);
+                }
+                ax = fmaf(dx, f, ax);
+                ay = fmaf(dy, f, ay);
+                az = fmaf(dz, f, az);
+                if (WANT_POT) ap += p;
+                if (COUNT) c_zero += (r2 == 0.0f);
+            }
+            add_partial(v, ax, ay, az, ap);
+            if (COUNT) c_flush += (lane == 0);
+            __syncwarp();
+        };
+
+        // ---- traversal ----------------------------------------------------------------------
+        // One loop: each pass either walks one traversal step or places the next 32 particles of
+        // the leaves the last step expanded.  A pass adds at most 32 entries to each list, so the
+        // lists are flushed at the top of the loop, when the next pass could overflow them, and at
+        // the end: one flush site per list kind, which keeps the kernel's code small (instruction
+        // fetch, not arithmetic, limited the first version with a flush at every append site).
+        int top = 1;
+        if (lane == 0) stk[0] = 1 | (nt[1] > 0 ? 2 : 0);  // the root (node 0) for both windows
+        __syncwarp();
+        int npn0 = 0, npn1 = 0, npp0 = 0, npp1 = 0;
+        int base = 0, tot2 = 0;  // the expanded leaves' particles still to place: [base, tot2)
+        bool overflow = false;
+        for (;;) {
+            const bool done = top == 0 && base >= tot2;
+#pragma unroll 1
+            for (int v = 0; v < 2; ++v) {
+                const int n1 = v ? npn1 : npn0, n2 = v ? npp1 : npp0;
+                if (n1 > 0 && (done || n1 > A.pn_cap - 32)) {
+                    flush_pn(v, n1);
+                    if (v) npn1 = 0; else npn0 = 0;
+                }
+                if (n2 > 0 && (done || n2 > A.pp_cap - 32)) {
+                    flush_pp(v, n2);
+                    if (v) npp1 = 0; else npp0 = 0;
+                }
+            }
+            if (done) break;
+
+            if (base < tot2) {
+                // 32 expanded-leaf particles, one per lane, to the windows that opened their leaf:
+                // a particle farther from a window's box than max(its largest target softening,
+                // the particle's) is a monopole for that window, the rest need the softened pair
+                const int q = base + lane;
+                const bool live = q < tot2;
+                double qx = 0, qy = 0, qz = 0;
+                float qm = 0.0f, qh = 0.0f;
+                int wm = 0;
+                if (live) {
+                    int l = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1)
+                        if (S.pre[l + step] <= q) l += step;
+                    int qpos = S.lo[l] + (q - S.pre[l]);
+                    if (!GT_IN_BOUNDS(qpos, A.n_src)) qpos = 0;
+                    load_src(A.src + qpos, qx, qy, qz, qm, qh);
+                    wm = S.msk[l];
+                }
+#pragma unroll
+                for (int v = 0; v < 2; ++v) {
+                    const bool in = (wm >> v) & 1;
+                    bool far = false;
+                    if (in) {
+                        const double ex = box_gap(S.lo_x[v], qx, S.hi_x[v]);
+                        const double ey = box_gap(S.lo_y[v], qy, S.hi_y[v]);
+                        const double ez = box_gap(S.lo_z[v], qz, S.hi_z[v]);
+                        const double qhd = (double)qh;
+                        const double reach = S.emax[v] > qhd ? S.emax[v] : qhd;
+                        far = ex * ex + ey * ey + ez * ez > reach * reach;
+                    }
+                    const unsigned fm = __ballot_sync(kFull, in && far);
+                    const unsigned nm = __ballot_sync(kFull, in && !far);
+                    int& npn = v ? npn1 : npn0;
+                    int& npp = v ? npp1 : npp0;
+                    if (COUNT && lane == 0) c_pairs += (unsigned long long)__popc(fm | nm) * nt[v];
+                    const float ex = (float)(qx - S.c_x[v]), ey = (float)(qy - S.c_y[v]), ez = (float)(qz - S.c_z[v]);
+                    if (in && far && GT_IN_BOUNDS(npn + __popc(fm & lt_mask), A.pn_cap)) {
+                        pn_put(v, npn + __popc(fm & lt_mask), ex, ey, ez, qm);
+                    } else if (in && GT_IN_BOUNDS(npp + __popc(nm & lt_mask), A.pp_cap)) {
+                        const int pos = npp + __popc(nm & lt_mask);
+                        pp_of(v)[pos] = make_float4(ex, ey, ez, qm);
+                        ph_of(v)[pos] = qh;
+                    }
+                    npn += __popc(fm);
+                    npp += __popc(nm);
+                }
+                base += 32;
+                __syncwarp();
+                continue;
+            }
+
+            // one traversal step: pop up to 32 nodes, test each against its windows
+            const int npop = min(top, 32);
+            top -= npop;
+            const int ent = lane < npop ? stk[top + lane] : -1;
+            int node = ent >= 0 ? (ent >> 2) : -1;
+            if (node >= 0 && !GT_IN_BOUNDS(node, A.n_nodes)) node = -1;
+            const int mk = node >= 0 ? (ent & 3) : 0;
+            __syncwarp();
+            const NodeV nd = load_node(A.nodes + (node >= 0 ? node : 0));
+            const bool leaf = nd.first < 0;
+            if (COUNT) {
+                const unsigned tests = __reduce_add_sync(kFull, (unsigned)__popc(mk));
+                if (lane == 0) { c_nodes += tests; ++c_steps; }
+            }
+            bool acc[2], opn[2];
+#pragma unroll
+            for (int v = 0; v < 2; ++v) {
+                acc[v] = false;
+                opn[v] = false;
+                if ((mk >> v) & 1) {
+                    const double dx = box_gap(S.lo_x[v], nd.cx, S.hi_x[v]);
+                    const double dy = box_gap(S.lo_y[v], nd.cy, S.hi_y[v]);
+                    const double dz = box_gap(S.lo_z[v], nd.cz, S.hi_z[v]);
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    const double len = (double)nd.len;
+                    const double ml2 = MAC == 2 ? nd.mass * (double)__ldg(A.mac_l2 + node) : nd.mass * len * len;
+                    const bool o = open_node(r2, len, nd.s, ml2, (double)nd.soft, S.emax[v], S.amin[v], A.theta2,
+                                             dx, dy, dz);
+                    acc[v] = !o;
+                    opn[v] = o;
+                }
+            }
+            const int pm = (opn[0] ? 1 : 0) | (opn[1] ? 2 : 0);  // the windows that open this node
+            const bool push = pm != 0 && !leaf, expand = pm != 0 && leaf;
+
+            // children of opened interior nodes, with the windows that opened them; one scan for
+            // the children's stack slots and the expanded leaves' particle slots (walk_kernel)
+            const int nch = push ? nd.nchild : 0;
+            const int cnt = expand ? nd.phi - nd.plo : 0;
+            int incl, inc2;
+            if (!__any_sync(kFull, cnt >= (1 << 16))) {
+                const int both = warp_incl_scan_i(nch | (cnt << 10));
+                incl = both & 1023;
+                inc2 = both >> 10;
+            } else {
+                incl = warp_incl_scan_i(nch);
+                inc2 = warp_incl_scan_i(cnt);
+            }
+            const int tot = __shfl_sync(kFull, incl, 31);
+            if (top + tot > A.stack_cap) { overflow = true; break; }
+            {
+                int* dst = stk + (top + incl - nch);
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    if (c < nch) dst[c] = ((nd.first + c) << 2) | pm;
+            }
+            top += tot;
+            if (COUNT) c_maxtop = max(c_maxtop, top);
+
+            // accepted nodes: monopoles of the windows that accept them
+#pragma unroll
+            for (int v = 0; v < 2; ++v) {
+                const unsigned am = __ballot_sync(kFull, acc[v]);
+                int& npn = v ? npn1 : npn0;
+                if (COUNT && lane == 0) c_multi += (unsigned long long)__popc(am) * nt[v];
+                if (acc[v] && GT_IN_BOUNDS(npn + __popc(am & lt_mask), A.pn_cap))
+                    pn_put(v, npn + __popc(am & lt_mask), (float)(nd.cx - S.c_x[v]), (float)(nd.cy - S.c_y[v]),
+                           (float)(nd.cz - S.c_z[v]), (float)nd.mass);
+                npn += __popc(am);
+            }
+
+            // expanded leaves: their particles are placed by the next passes
+            tot2 = __shfl_sync(kFull, inc2, 31);
+            base = 0;
+            if (tot2 > 0) {
+                S.lo[lane] = nd.plo;
+                S.pre[lane] = inc2 - cnt;
+                S.msk[lane] = pm;
+            }
+            __syncwarp();
+        }
+        if (overflow) {
+            if (lane == 0) atomicExch(A.error, 1);
+            continue;
+        }
+
+        // ---- write --------------------------------------------------------------------------
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            if (lane < nt[v]) {
+                const int idx = t0[v] + lane;
+                const int o = A.out_map ? (int)A.out_map[idx] : idx;
+                if (!GT_IN_BOUNDS(o, A.n_out)) continue;
+                const float sx = v ? sx1 : sx0, sy = v ? sy1 : sy0, sz = v ? sz1 : sz0;
+                const float cx = v ? cx1 : cx0, cy = v ? cy1 : cy0, cz = v ? cz1 : cz0;
+                if (A.ax) {
+                    A.ax[o] = A.G * ((double)sx - (double)cx);
+                    A.ay[o] = A.G * ((double)sy - (double)cy);
+                    A.az[o] = A.G * ((double)sz - (double)cz);
+                }
+                if (WANT_POT && A.phi) A.phi[o] = A.G * (v ? pot1 : pot0);
+            }
+        }
+    }
+    if (COUNT) {
+        if (lane == 0) {
+            atomicAdd(&A.stats[0], c_nodes);
+            atomicAdd(&A.stats[1], c_multi);
+            atomicAdd(&A.stats[2], c_pairs);
+            atomicAdd(&A.stats[4], c_flush);
+            atomicMax(&A.stats[5], (unsigned long long)c_maxtop);
+            atomicAdd(&A.stats[6], c_steps);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c_zero += __shfl_xor_sync(kFull, c_zero, o);
+        if (lane == 0) atomicAdd(&A.stats[3], c_zero);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Groups
 // ---------------------------------------------------------------------------------------------
 
@@ -1247,6 +1629,58 @@ void dispatch(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la
     }
 }
 
+// The paired-window walk: at most 512 list entries per window (two windows' lists of 8 warps fit
+// the 227 KB of shared memory).
+constexpr int kPairCapMax = 512;
+constexpr int kPairCapDefault = 128;
+
+size_t pair_smem(int warps, int pn_cap) { return (size_t)warps * pair_smem_bytes(pn_cap, pn_cap / 2); }
+
+template <bool POT, bool CNT, int MAC>
+void prepare_pair() {
+    static bool done = false;
+    if (done) return;
+    check_cuda(cudaFuncSetAttribute(walk_pair_kernel<POT, CNT, MAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)pair_smem(kMaxWarps, kPairCapMax)),
+               "cudaFuncSetAttribute");
+    check_cuda(cudaFuncSetAttribute(walk_pair_kernel<POT, CNT, MAC>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    100),
+               "cudaFuncSetAttribute");
+    done = true;
+}
+
+template <bool POT, bool CNT, int MAC>
+int pair_occupancy(int warps, int pn_cap) {
+    prepare_pair<POT, CNT, MAC>();
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_pair_kernel<POT, CNT, MAC>, warps * 32,
+                                                  pair_smem(warps, pn_cap));
+    return std::max(1, nb);
+}
+
+template <bool POT, bool CNT, int MAC>
+void launch_pair(gt_context* ctx, const WalkArgs& a, int blocks, int warps) {
+    prepare_pair<POT, CNT, MAC>();
+    walk_pair_kernel<POT, CNT, MAC><<<blocks, warps * 32, pair_smem(warps, a.pn_cap), ctx->stream>>>(a);
+    check_launch(ctx, "walk_pair_kernel");
+}
+
+template <bool POT, bool CNT>
+void dispatch_pair_mac(gt_context* ctx, const WalkArgs& a, int blocks, int warps, int mac) {
+    if (mac == GT_MAC_NODE) launch_pair<POT, CNT, 2>(ctx, a, blocks, warps);
+    else launch_pair<POT, CNT, 0>(ctx, a, blocks, warps);
+}
+
+void dispatch_pair(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool pot, bool cnt, int mac) {
+    if (pot) {
+        if (cnt) dispatch_pair_mac<true, true>(ctx, a, blocks, warps, mac);
+        else dispatch_pair_mac<true, false>(ctx, a, blocks, warps, mac);
+    } else {
+        if (cnt) dispatch_pair_mac<false, true>(ctx, a, blocks, warps, mac);
+        else dispatch_pair_mac<false, false>(ctx, a, blocks, warps, mac);
+    }
+}
+
 // Chunks of the copy-overlapped walk, as cumulative percentages of the targets.  The first chunk is
 // small, so the walk starts once a tenth of the host aold is across, and so is the last, so that
 // little of the results' download is left when the last kernel ends; the chunks between are large
@@ -1258,10 +1692,11 @@ struct ChunkEdges {
 constexpr ChunkEdges kChunkEdge{{0, 10, 45, 80, 93, 100}};
 
 // Chunk boundaries of a group list for the copy-overlapped walk: chunk c starts at the first group
-// whose first target is at or after nt * edges.pct[c] / 100.  out: kChunks+1 pairs (group index,
-// first target).
+// whose first target is at or after nt * edges.pct[c] / 100 (rounded down to an even group when
+// the walk pairs windows, so that no pair straddles two chunks).  out: kChunks+1 pairs (group
+// index, first target).
 __global__ void chunk_bounds_kernel(const int2* __restrict__ groups, int ng, int nt, ChunkEdges edges,
-                                    int2* __restrict__ out, const uint32_t* __restrict__ ng_dev) {
+                                    int2* __restrict__ out, const uint32_t* __restrict__ ng_dev, int even) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     if (ng_dev) ng = min(ng, (int)*ng_dev);
     for (int c = 0; c <= kChunks; ++c) {
@@ -1271,6 +1706,7 @@ __global__ void chunk_bounds_kernel(const int2* __restrict__ groups, int ng, int
             const int mid = (lo + hi) >> 1;
             if (groups[mid].x < want) lo = mid + 1; else hi = mid;
         }
+        if (even && c > 0 && c < kChunks) lo &= ~1;
         out[c] = make_int2(lo, lo < ng ? groups[lo].x : nt);
     }
 }
@@ -1440,8 +1876,16 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     }
     if (ext == 1 && pn_cap > kPnCapMax / 2)
         throw Fail{GT_ERR_INVALID, "list_capacity must be at most 512 with the tidal tensor or the jerk"};
+    // two consecutive windows per warp (walk_pair_kernel) where it applies; its default lists hold
+    // 128 entries per window, so that three blocks of eight warps fit an SM
+    const bool paired = rq.pair_windows && !xt && tpl == 1 && mode == GT_GROUP_BATCH && param > 16 &&
+                        rq.leaf_accept && !mac && roots == nullptr && t->n_nodes < (1 << 29) &&
+                        pn_cap <= kPairCapMax;
+    if (paired && rq.list_capacity == 0) pn_cap = kPairCapDefault;
     int per_sm;
-    if (ext == 1)
+    if (paired)
+        per_sm = macn ? pair_occupancy<false, false, 2>(warps, pn_cap) : pair_occupancy<false, false, 0>(warps, pn_cap);
+    else if (ext == 1)
         per_sm = occupancy_blocks<1, true, false, false, 0, 1>(warps, pn_cap);
     else if (ext == 2)
         per_sm = occupancy_blocks<1, true, false, false, 0, 2>(warps, pn_cap);
@@ -1458,7 +1902,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         per_sm = mac ? occupancy_blocks<4, true, false, false, 1>(warps, pn_cap)
                : macn ? occupancy_blocks<4, true, false, false, 2>(warps, pn_cap)
                       : occupancy_blocks<4, true, false, false, 0>(warps, pn_cap);
-    const int64_t want_blocks = (ng + warps - 1) / warps;
+    const int64_t want_blocks = ((paired ? (ng + 1) / 2 : ng) + warps - 1) / warps;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want_blocks, (int64_t)per_sm * ctx->num_sms));
     int stack_cap = rq.stack_capacity > 0 ? rq.stack_capacity : 256 * std::max(1, t->n_levels) + 32;
     stack_cap = (stack_cap + 31) & ~31;
@@ -1485,7 +1929,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     const int total_warps = blocks * warps;
     a.pn_cap = pn_cap;
     a.pp_cap = pn_cap / 2;
-    a.warp_bytes = warp_smem_bytes(a.pn_cap, a.pp_cap, ext);
+    a.warp_bytes = paired ? pair_smem_bytes(a.pn_cap, a.pp_cap) : warp_smem_bytes(a.pn_cap, a.pp_cap, ext);
     a.tidal = rq.tidal;
     a.jerk = rq.jerk;
     a.svel = t->svel;
@@ -1555,7 +1999,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         ensure_copy_stream(ctx);
         int2* bounds = (int2*)(ctr + 16);  // K+1 int2 after the counters
         check_cuda(cudaMemsetAsync(ctr, 0, 256, st), "memset counters");
-        chunk_bounds_kernel<<<1, 1, 0, st>>>(groups, (int)ng, (int)nt, kChunkEdge, bounds, ng_dev);
+        chunk_bounds_kernel<<<1, 1, 0, st>>>(groups, (int)ng, (int)nt, kChunkEdge, bounds, ng_dev, paired ? 1 : 0);
         check_launch(ctx, "chunk_bounds_kernel");
         int2 hb[kChunks + 1];
         check_cuda(cudaMemcpyAsync(ctx->pinned, bounds, sizeof(hb), cudaMemcpyDeviceToHost, st), "d2h");
@@ -1615,8 +2059,10 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
                 ac.n_groups_dev = nullptr;
                 ac.group_root = roots ? roots + g0 : nullptr;
                 ac.next_group = (unsigned int*)(ctr + 10) + c;
-                const int cb = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, ((int64_t)(g1 - g0) + warps - 1) / warps));
-                if (xt) dispatch_xt(ctx, ac, cb, warps, ext, rq.leaf_accept, want_pot, false);
+                const int64_t units = paired ? ((int64_t)(g1 - g0) + 1) / 2 : (int64_t)(g1 - g0);
+                const int cb = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (units + warps - 1) / warps));
+                if (paired) dispatch_pair(ctx, ac, cb, warps, want_pot, false, rq.mac);
+                else if (xt) dispatch_xt(ctx, ac, cb, warps, ext, rq.leaf_accept, want_pot, false);
                 else if (tpl == 1) dispatch<1>(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false, rq.mac);
                 else if (tpl == 2) dispatch<2>(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false, rq.mac);
                 else dispatch<4>(ctx, ac, cb, warps, rq.leaf_accept, want_pot, false, rq.mac);
@@ -1652,7 +2098,8 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         a.stack_cap = stack_cap;
         check_cuda(cudaMemsetAsync(ctr, 0, 96, st), "memset counters");
         if (!rq.capture) check_cuda(cudaEventRecord(ctx->ev0, st), "event");
-        if (xt) dispatch_xt(ctx, a, blocks, warps, ext, rq.leaf_accept, want_pot, rq.count);
+        if (paired) dispatch_pair(ctx, a, blocks, warps, want_pot, rq.count, rq.mac);
+        else if (xt) dispatch_xt(ctx, a, blocks, warps, ext, rq.leaf_accept, want_pot, rq.count);
         else if (tpl == 1) dispatch<1>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
         else if (tpl == 2) dispatch<2>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);
         else dispatch<4>(ctx, a, blocks, warps, rq.leaf_accept, want_pot, rq.count, rq.mac);

@@ -126,6 +126,12 @@ typedef struct {
      * accepted that holds a sink and comes within this radius + 0.6 side of the group's box
      * (accel_grouped's sink_direct_radius, tree.h:435-440, tree.cc:691-698, 772-778).  Default 0. */
     double sink_direct_radius;
+    /* Grouped windows of 17-32 targets (GT_GROUP_BATCH) are walked two per warp by default: two
+     * consecutive windows share one traversal, each testing exactly its own nodes, so every
+     * window gets its own walk's decisions and interactions (sums equal to FP32 rounding, not bit
+     * for bit: the list order can differ).  Not for GT_MAC_LEARNED, the tidal tensor, the jerk,
+     * the gas rules, counting walks or forests.  1: one window per warp. */
+    int no_window_pairs;
 } gt_walk_options;
 
 typedef struct {

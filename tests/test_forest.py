@@ -74,7 +74,9 @@ def test_forest_walk_bit_identical(gpu_ctx, batch, forest, mode, batch_size):
     P, off = batch
     F, trees = forest
     live, _ = F.systems()
-    kw = dict(group_mode=mode, batch=batch_size, out_order=g.GT_OUT_ORIGINAL)
+    # one window per warp: a single tree's windows of 32 are otherwise walked two at a time,
+    # which matches the one-window walk to FP32 rounding only
+    kw = dict(group_mode=mode, batch=batch_size, out_order=g.GT_OUT_ORIGINAL, window_pairs=False)
     fx, fy, fz = gpu_ctx.accel_grouped(F, None, theta=0.7, **kw)
     for s, t in enumerate(trees):
         if live[s + 1] == live[s]:

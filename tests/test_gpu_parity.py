@@ -565,3 +565,38 @@ def test_small_target_lists_group_in_one_launch(gpu_ctx, plummer_trees):
     for u, v in zip(a, b):
         assert np.array_equal(u[:head], v[:head])
     assert ga == 1 + int(np.count_nonzero(leaf[1:8192] != leaf[:8191]))
+
+
+@pytest.mark.parametrize("nt", [None, 30001, 30000])
+def test_window_pairs_match_single_windows(gpu_ctx, plummer_trees, nt):
+    """Windows of 17-32 targets are walked two per warp by default (walk_pair_kernel): a node is
+    tested only against the windows whose own walk reaches it, so each window makes its own
+    walk's decisions.  The interaction counts therefore equal the one-window walk's exactly, and
+    the forces agree to FP32 summation order (a node accepted instead of opened would move a
+    force by ~1e-3).  All live targets, and explicit lists with an odd number of windows whose
+    last one holds 17 or 16 targets; with the relative criterion, Barnes-Hut and the potential."""
+    T, O = plummer_trees
+    ob = O.order()[0]
+    tg = None if nt is None else ob[:nt]
+    kw = dict(group_mode=g.GT_GROUP_BATCH, batch=32)
+    boot = gpu_ctx.accel_grouped(T, tg, theta=0.7, **kw)
+    aold = gpu_ctx.form_aold(*boot, 0.0025)
+    for crit in (dict(aold=aold, theta=0.0), dict(theta=0.6)):
+        for pot in (False, True):
+            runs = {}
+            for pairs in (True, False):
+                res = gpu_ctx.accel_grouped(T, tg, want_phi=pot, count=True, window_pairs=pairs, **crit, **kw)
+                runs[pairs] = (np.stack(res), gpu_ctx.stats())
+                plain = gpu_ctx.accel_grouped(T, tg, want_phi=pot, window_pairs=pairs, **crit, **kw)
+                assert np.array_equal(np.stack(plain), runs[pairs][0])  # counting changes nothing
+            (p, sp), (u, su) = runs[True], runs[False]
+            for k in ("nodes_visited", "multipole", "pairs"):
+                assert sp[k] == su[k], (k, sp[k], su[k])
+            # per target: |a_pair - a_single| / |a_single| (the potential on its own), floored at a
+            # thousandth of the median magnitude where the net force nearly cancels
+            for d, r in ((p[:3] - u[:3], u[:3]), (p[3:] - u[3:], u[3:])):
+                if len(r) == 0:
+                    continue
+                nd, nr = np.linalg.norm(d, axis=0), np.linalg.norm(r, axis=0)
+                e = nd / np.maximum(nr, 1e-3 * np.median(nr))
+                assert np.median(e) < 1e-6 and e.max() < 1e-4, (np.median(e), e.max())
