@@ -352,9 +352,15 @@ def relerr(a, b):
     return d / np.where(n > 0, n, 1.0)
 
 
-def read_profile_traffic(workload):
+def walk_kernel_name(args):
+    """The kernel a single-system walk of this grouping runs: windows of 17-32 targets are walked
+    two per warp (walk_pair_kernel), everything else by walk_kernel."""
+    return "walk_pair_kernel" if args.group == "batch" and 16 < args.group_max <= 32 else "walk_kernel"
+
+
+def read_profile_traffic(workload, kernel):
     """dram bytes per walk launch from the committed ncu summary, if one exists."""
-    p = os.path.join(ROOT, "profiles", f"walk_kernel_{workload}.json")
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.json")
     try:
         return json.load(open(p)).get("dram_bytes_per_launch")
     except Exception:
@@ -671,12 +677,12 @@ def run_gpu_arm(args):
         "tree_bytes": int(info["n_nodes"]) * 64,
         "parity": parity,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
-                     "frac": achieved / peak32, "traffic": read_profile_traffic(args.workload),
+                     "frac": achieved / peak32, "traffic": read_profile_traffic(args.workload, walk_kernel_name(args)),
                      "peak_source": "measured FP32 FMA-chain probe on this GPU (gt_measure_peaks), "
                                     "not in MEASURED_PEAKS.json",
                      "nominal_fp32_tflops": nominal_fp32(clocks),
                      "frac_of_nominal": achieved / nominal_fp32(clocks)["at_max_clock"],
-                     "flops_per_interaction": FLOPS_PER_INTERACTION, "kernel": "walk_kernel",
+                     "flops_per_interaction": FLOPS_PER_INTERACTION, "kernel": walk_kernel_name(args),
                      "kernel_ms": 1e3 * t_kernel, "fp64_peak_tflops": peak64},
         "cpu_baseline": cpu_line,
         "e2e": e2e,

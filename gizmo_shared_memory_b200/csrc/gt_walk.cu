@@ -1632,7 +1632,7 @@ void dispatch(gt_context* ctx, const WalkArgs& a, int blocks, int warps, bool la
 // The paired-window walk: at most 512 list entries per window (two windows' lists of 8 warps fit
 // the 227 KB of shared memory).
 constexpr int kPairCapMax = 512;
-constexpr int kPairCapDefault = 128;
+constexpr int kPairCapDefault = 160;
 
 size_t pair_smem(int warps, int pn_cap) { return (size_t)warps * pair_smem_bytes(pn_cap, pn_cap / 2); }
 
