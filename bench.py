@@ -810,7 +810,10 @@ def run_batch_arm(args):
                    "autotuned": {k: v for k, v in best.items() if k != "mac_model"},
                    "l2": f"inputs larger than L2: {n * 32 / 2**20:.0f} MiB of particles"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
-                     "frac": achieved / peak32, "traffic": None, "kernel": "walk_kernel"},
+                     "frac": achieved / peak32, "traffic": None,
+                     "kernel": ("walk_pair_kernel" if kw.get("group_mode") == g.GT_GROUP_BATCH and
+                                16 < kw.get("batch", 0) <= 32 and kw.get("mac", g.GT_MAC_PLAIN) != g.GT_MAC_LEARNED
+                                else "walk_kernel")},
         "gpu_launches": launches, "clocks": clocks,
         "error": {"vs": "FP64 direct sum per system, 16 targets each", "sample": int(len(sample)),
                   "median": float(np.median(err)), "p99": float(np.quantile(err, 0.99)),

@@ -869,7 +869,7 @@ walk_kernel(const WalkArgs A) {
 // window with walk_kernel's packed monopole loop.  A window's nodes can join its list in another
 // order than in its own walk (the other window's nodes interleave on the stack), so the sums agree
 // with walk_kernel's to FP32 rounding, not bit for bit.  One target per lane, the grouped walk,
-// the plain or per-node learned criterion, one system.
+// the plain or per-node learned criterion; in a forest the two windows may start from two roots.
 
 struct alignas(16) PairHdr {
     int lo[32];   // leaf-expansion scratch: first slot, exclusive prefix and windows of each leaf
@@ -1044,8 +1044,19 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 3) walk_pair_kernel(const Walk
         // lists are flushed at the top of the loop, when the next pass could overflow them, and at
         // the end: one flush site per list kind, which keeps the kernel's code small (instruction
         // fetch, not arithmetic, limited the first version with a flush at every append site).
+        // the root of each window: node 0, or in a forest its system's root; windows of one
+        // system share a root entry, windows of two systems start from one entry each
         int top = 1;
-        if (lane == 0) stk[0] = 1 | (nt[1] > 0 ? 2 : 0);  // the root (node 0) for both windows
+        {
+            const int ra = A.group_root ? A.group_root[2 * pr] : 0;
+            const int rb = (A.group_root && nt[1] > 0) ? A.group_root[2 * pr + 1] : ra;
+            if (ra == rb) {
+                if (lane == 0) stk[0] = (ra << 2) | 1 | (nt[1] > 0 ? 2 : 0);
+            } else {
+                if (lane == 0) { stk[0] = (ra << 2) | 1; stk[1] = (rb << 2) | 2; }
+                top = 2;
+            }
+        }
         __syncwarp();
         int npn0 = 0, npn1 = 0, npp0 = 0, npp1 = 0;
         int base = 0, tot2 = 0;  // the expanded leaves' particles still to place: [base, tot2)
@@ -1879,8 +1890,7 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
     // two consecutive windows per warp (walk_pair_kernel) where it applies; its default lists hold
     // 128 entries per window, so that three blocks of eight warps fit an SM
     const bool paired = rq.pair_windows && !xt && tpl == 1 && mode == GT_GROUP_BATCH && param > 16 &&
-                        rq.leaf_accept && !mac && roots == nullptr && t->n_nodes < (1 << 29) &&
-                        pn_cap <= kPairCapMax;
+                        rq.leaf_accept && !mac && t->n_nodes < (1 << 29) && pn_cap <= kPairCapMax;
     if (paired && rq.list_capacity == 0) pn_cap = kPairCapDefault;
     int per_sm;
     if (paired)

@@ -1,7 +1,8 @@
 """The bounds-checked library (libgt_debug.so: the same kernels built with -DGT_BOUNDS_CHECK, the
 build's stand-in for a memory checker) runs the walks clean and gives the ordinary library's
 results.  It runs in a child process, since a process loads one libgt at a time: the child walks a
-Plummer sphere with leaf groups, windows, explicit targets and node groups, and a forest, on both
+Plummer sphere with leaf groups, windows (two per warp), explicit targets in leaf groups and in
+windows, node groups, and a forest, on both
 libraries in turn (fresh contexts each), and every call must return GT_OK with identical forces."""
 import os
 import subprocess
@@ -36,6 +37,7 @@ def run(lib):
     out += list(ctx.accel_grouped(T, None, aold=aold, group_mode=g.GT_GROUP_NODE, group_max=64))
     sub = ob[::7].copy()
     out += list(ctx.accel_grouped(T, sub, aold=aold[::7].copy(), batch=0))
+    out += list(ctx.accel_grouped(T, sub, aold=aold[::7].copy(), batch=32, group_mode=g.GT_GROUP_BATCH))
     F = ctx.build({k: np.concatenate([v[:10000], v[10000:] + (30.0 if k == "x" else 0.0)]) for k, v in P.items()},
                   offsets=np.array([0, 10000, 30000], np.int64))
     out += list(ctx.accel_grouped(F, None, theta=0.7, batch=32, group_mode=g.GT_GROUP_BATCH))

@@ -297,3 +297,30 @@ def test_forest_density(gpu_ctx, batch, forest):
         for key in ("h", "rho", "nngb", "iters"):
             assert np.array_equal(w[key][seg], r[key]), (s, key)
         k += len(loc[s])
+
+
+def test_forest_window_pairs_match_single_windows(gpu_ctx, batch, forest):
+    """A forest's windows are walked two per warp like a single tree's; two windows of different
+    systems start from their own roots.  Each window still tests exactly its own nodes: the
+    counts equal the one-window walk's, the forces agree to FP32 summation order.  All live
+    targets and an explicit list that visits the systems out of order."""
+    P, off = batch
+    F, _ = forest
+    S = len(off) - 1
+    kw = dict(group_mode=g.GT_GROUP_BATCH, batch=32)
+    boot = gpu_ctx.accel_grouped(F, None, theta=0.7, window_pairs=False, out_order=g.GT_OUT_ORIGINAL, **kw)
+    aold = gpu_ctx.form_aold(*boot, 0.0025)  # per particle index
+    ob = F.download(nodes=False)["orderbuf"][:F.info()["n_live"]]
+    tl, _ = local_targets(P, off, S, np.random.default_rng(21), massless=False)
+    for tg in (None, tl):
+        a = aold[ob] if tg is None else aold[tl]  # per target, in the order walked
+        runs = {}
+        for pairs in (True, False):
+            res = gpu_ctx.accel_grouped(F, tg, aold=a, count=True, window_pairs=pairs, **kw)
+            runs[pairs] = (np.stack(res), gpu_ctx.stats())
+        (p, sp), (u, su) = runs[True], runs[False]
+        for k in ("nodes_visited", "multipole", "pairs"):
+            assert sp[k] == su[k], (k, sp[k], su[k])
+        nd, nr = np.linalg.norm(p - u, axis=0), np.linalg.norm(u, axis=0)
+        e = nd / np.maximum(nr, 1e-3 * np.median(nr))
+        assert np.median(e) < 1e-6 and e.max() < 1e-4, (np.median(e), e.max())
