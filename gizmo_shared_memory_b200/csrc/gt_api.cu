@@ -64,6 +64,7 @@ void ensure_copy_stream(gt_context* ctx) {
     };
     for (cudaEvent_t& e : ctx->chunk_ev) make(e);
     for (cudaEvent_t& e : ctx->up_ev) make(e);
+    for (cudaEvent_t& e : ctx->down_ev) make(e);
     make(ctx->copy_done);
     make(ctx->main_ev);
     make(ctx->walk2_start);
@@ -76,6 +77,27 @@ void ensure_copy_stream(gt_context* ctx) {
     cudaStream_t s = nullptr;
     check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
     ctx->copy_stream = s;
+}
+
+void* host_stage(gt_context* ctx, size_t bytes) {
+    if (ctx->stage_bytes >= bytes) return ctx->stage;
+    if (ctx->stage) {
+        // queued copies may still use the smaller buffer
+        cudaStreamSynchronize(ctx->stream);
+        if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+        cudaFreeHost(ctx->stage);
+        ctx->stage = nullptr;
+        ctx->stage_bytes = 0;
+    }
+    const size_t want = bytes + bytes / 8;
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, want, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        throw Fail{GT_ERR_NOMEM, "pinned staging allocation of " + std::to_string(want) + " bytes failed"};
+    }
+    ctx->stage = p;
+    ctx->stage_bytes = want;
+    return p;
 }
 
 }  // namespace gt
@@ -402,6 +424,9 @@ int gt_context_destroy(gt_context* ctx) {
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->up_ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->down_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stage) cudaFreeHost(ctx->stage);
     if (ctx->copy_done) cudaEventDestroy(ctx->copy_done);
     if (ctx->main_ev) cudaEventDestroy(ctx->main_ev);
     if (ctx->walk2) {

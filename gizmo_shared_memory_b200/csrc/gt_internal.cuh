@@ -99,6 +99,12 @@ struct gt_context {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t chunk_ev[8] = {};
     cudaEvent_t up_ev[8] = {};
+    cudaEvent_t down_ev[8] = {};      // a chunk's results are in the pinned staging buffer
+    // pinned staging for pageable host outputs of a chunked walk (grow-only, made on first use):
+    // a copy to pageable memory blocks the host thread until it is done, which would serialise
+    // the chunks with their copies
+    void* stage = nullptr;
+    size_t stage_bytes = 0;
     cudaEvent_t copy_done = nullptr;
     cudaEvent_t main_ev = nullptr;
     // second compute stream: the chunks of a chunked walk alternate between it and `stream`
@@ -245,6 +251,8 @@ void build_tree(gt_context* ctx, gt_tree* t, const double* x, const double* y, c
 // The context's second stream (and its events), made on first use: host copies that overlap work
 // on the main stream.
 void ensure_copy_stream(gt_context* ctx);
+// The context's pinned staging buffer of at least `bytes` (grow-only; throws Fail).
+void* host_stage(gt_context* ctx, size_t bytes);
 
 // Walk (gt_walk.cu)
 // Stack and counters owned by a walk plan (a captured graph must not point into the workspace).

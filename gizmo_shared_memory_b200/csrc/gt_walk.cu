@@ -2025,6 +2025,25 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
         a.stack_cap = stack_cap;
         const OutputCopy outs[6] = {{rq.ax, rq.host.ax, 1},  {rq.ay, rq.host.ay, 1},       {rq.az, rq.host.az, 1},
                                     {rq.phi, rq.host.phi, 1}, {rq.tidal, rq.host.tidal, 6}, {rq.jerk, rq.host.jerk, 3}};
+        // pageable host outputs (std::vector, numpy) are copied into the context's pinned staging
+        // buffer and from there, chunk by chunk, into the caller's arrays while later chunks run:
+        // a device-to-host copy into pageable memory would block this thread until its chunk is
+        // done, and so hold back the launch of the next one
+        size_t stage_off[6] = {0, 0, 0, 0, 0, 0};
+        bool staged[6] = {false, false, false, false, false, false};
+        size_t stage_need = 0;
+        for (int i = 0; i < 6; ++i) {
+            if (!outs[i].dev || !outs[i].host) continue;
+            cudaPointerAttributes at;
+            const bool pageable = cudaPointerGetAttributes(&at, outs[i].host) != cudaSuccess ||
+                                  at.type == cudaMemoryTypeUnregistered;
+            cudaGetLastError();
+            if (!pageable) continue;
+            staged[i] = true;
+            stage_off[i] = stage_need;
+            stage_need += (size_t)nt * outs[i].stride * sizeof(double);
+        }
+        char* stage = stage_need ? static_cast<char*>(host_stage(ctx, stage_need)) : nullptr;
         if (rq.host_aold) {
             // every chunk's aold ahead of the results on the copy stream, after the work queued
             // before this walk (which may still read the buffer); chunk c reads only the aold of
@@ -2081,11 +2100,28 @@ bool run_walk(gt_context* ctx, const gt_tree* tc, const WalkRequest& rq) {
             check_cuda(cudaEventRecord(ctx->chunk_ev[c], s), "event");
             check_cuda(cudaStreamWaitEvent(ctx->copy_stream, ctx->chunk_ev[c], 0), "wait");
             const int64_t t0 = hb[c].y, t1 = hb[c + 1].y;
-            for (const auto& o : outs)
-                if (o.dev && o.host && t1 > t0)
-                    check_cuda(cudaMemcpyAsync(o.host + t0 * o.stride, o.dev + t0 * o.stride,
-                                               (size_t)(t1 - t0) * o.stride * sizeof(double), cudaMemcpyDeviceToHost,
-                                               ctx->copy_stream), "d2h chunk");
+            for (int i = 0; i < 6; ++i) {
+                const OutputCopy& o = outs[i];
+                if (!o.dev || !o.host || t1 <= t0) continue;
+                double* dst = staged[i] ? reinterpret_cast<double*>(stage + stage_off[i]) + t0 * o.stride
+                                        : o.host + t0 * o.stride;
+                check_cuda(cudaMemcpyAsync(dst, o.dev + t0 * o.stride, (size_t)(t1 - t0) * o.stride * sizeof(double),
+                                           cudaMemcpyDeviceToHost, ctx->copy_stream), "d2h chunk");
+            }
+            check_cuda(cudaEventRecord(ctx->down_ev[c], ctx->copy_stream), "event");
+        }
+        if (stage) {
+            // every chunk is queued: move each one's results into the caller's arrays as they land
+            for (int c = 0; c < kChunks; ++c) {
+                const int64_t t0 = hb[c].y, t1 = hb[c + 1].y;
+                if (t1 <= t0) continue;
+                check_cuda(cudaEventSynchronize(ctx->down_ev[c]), "sync");
+                for (int i = 0; i < 6; ++i)
+                    if (staged[i])
+                        std::memcpy(outs[i].host + t0 * outs[i].stride,
+                                    reinterpret_cast<const double*>(stage + stage_off[i]) + t0 * outs[i].stride,
+                                    (size_t)(t1 - t0) * outs[i].stride * sizeof(double));
+            }
         }
         if (two) {
             check_cuda(cudaEventRecord(ctx->walk2_done, ctx->walk2), "event");
