@@ -287,7 +287,7 @@ void accel(const Tree& T, const Particles& P, const std::vector<uint32_t>& targe
     need_gpu(T);
     prepare_walk(T, P, nullptr);
     const size_t nt = targets.size();
-    ax.assign(nt, 0.0); ay.assign(nt, 0.0); az.assign(nt, 0.0);
+    ax.resize(nt); ay.resize(nt); az.resize(nt);  // every target's outputs are written
     if (!nt) return;
     check(gt_accel(context(), T.gpu.get(), (int64_t)nt, targets.data(), theta, G, aold, GT_MEM_HOST,
                    ax.data(), ay.data(), az.data()), "gt_accel");
@@ -312,9 +312,14 @@ void accel_grouped(const Tree& T, const Particles& P, const std::vector<uint32_t
     // centre-of-mass velocities (tree.cc:638-640); without them it stays zero
     const bool want_jerk = jerk && vel && !T.vcom_x.empty();
     const size_t nt = targets.size();
-    ax.assign(nt, 0.0); ay.assign(nt, 0.0); az.assign(nt, 0.0);
-    if (tidal) tidal->assign(nt, SymTensor3d{0, 0, 0, 0, 0, 0});
-    if (jerk) jerk->assign(nt, Vec3d{0, 0, 0});
+    // every target's outputs are written by the walk: size the vectors without clearing them
+    // (a jerk without velocities stays zero)
+    ax.resize(nt); ay.resize(nt); az.resize(nt);
+    if (tidal) tidal->resize(nt);
+    if (jerk) {
+        if (want_jerk) jerk->resize(nt);
+        else jerk->assign(nt, Vec3d{0, 0, 0});
+    }
     if (!nt) return;
     gt_walk_options o;
     gt_walk_options_default(&o);
