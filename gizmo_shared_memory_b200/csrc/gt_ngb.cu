@@ -288,6 +288,11 @@ struct DensArgs {
     double *h, *rho;
     int *nngb, *iters;
     unsigned long long* tally;  // SHMEM_NGB_COUNT: calls, nodes, examined, kept, pad, iterations [8]
+    // candidate cache: per thread of the grid, cand_cap tree positions, interleaved (entry k of
+    // thread i at cand[k * n_threads + i])
+    uint32_t* cand;
+    int cand_cap;
+    int64_t n_threads;
 };
 
 __device__ __forceinline__ void dens_zero(DensSums& s) {
@@ -331,6 +336,11 @@ __device__ __forceinline__ void dens_add(double dx, double dy, double dz, double
 // interleaving the FP64 sums with the traversal made the lanes of a warp that were still walking
 // wait on every neighbour another lane had found.
 constexpr int kDensBuf = 64;
+// The candidate cache (below): capacity per thread, and the radius of a refill relative to the h
+// that outgrew the cache.
+constexpr int kCandCap = 160;
+constexpr double kCacheFirst = 1.1;
+constexpr double kCacheGrow = 1.4;
 
 template <bool COUNT>
 __device__ void dens_eval(const DensArgs& a, int r0, int r1, double px, double py, double pz, double h, DensSums& s,
@@ -357,6 +367,43 @@ __device__ void dens_eval(const DensArgs& a, int r0, int r1, double px, double p
         buf[nb++] = sp;
     }, &tl);
     drain();
+}
+
+// The candidate cache of the Newton iterations.  One search at radius R stores the GAS particles it
+// finds (their tree positions, in the search's order) in the thread's slice of a global array; an
+// evaluation at any h <= R then scans them and keeps those with r^2 < h^2, with the search's own
+// r^2 expression.  That is the set a search at h would keep, in the same order (a larger radius
+// only adds particles between them: the order is the threading's), so the sums are bit-identical,
+// and an iteration that shrinks h costs a scan of a few dozen candidates instead of a traversal.
+// A search that finds more than cand_cap gas particles leaves the cache empty.
+__device__ __forceinline__ int cache_fill(const DensArgs& a, int r0, int r1, double px, double py, double pz,
+                                          double R, uint32_t* __restrict__ slot, int64_t stride) {
+    int k = 0;
+    const int cap = a.cand_cap;
+    NgbTally none;
+    search<false>(a.g, r0, r1, px, py, pz, R, nullptr, 0, [&](uint32_t, int sp) {
+        if (a.stype && __ldg(a.stype + sp) != 0) return;
+        if (k < cap) slot[(int64_t)k * stride] = (uint32_t)sp;
+        ++k;
+    }, &none);
+    return k <= cap ? k : -1;
+}
+
+__device__ void cache_eval(const DensArgs& a, const uint32_t* __restrict__ slot, int64_t stride, int n, double px,
+                           double py, double pz, double h, DensSums& s) {
+    dens_zero(s);
+    const int dim = a.n_dims;
+    const double norm = kernel_norm(h, dim);
+    const double r2max = h * h;
+    for (int k = 0; k < n; ++k) {
+        const int sp = (int)slot[(int64_t)k * stride];
+        const double2 xy = __ldg(reinterpret_cast<const double2*>(a.g.src + sp));
+        const double zz = __ldg(reinterpret_cast<const double*>(a.g.src + sp) + 2);
+        const double ox = min_image(xy.x - px, a.g.box), oy = min_image(xy.y - py, a.g.box),
+                     oz = min_image(zz - pz, a.g.box);
+        const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)), __dmul_rn(oz, oz));
+        if (r2 < r2max) dens_add(ox, oy, oz, __ldg(a.smass + sp), h, norm, dim, s);
+    }
 }
 
 // Rank-d inverse of the symmetric moments (xx yy zz xy yz xz), row-major, zero when degenerate
@@ -467,13 +514,29 @@ __global__ void __launch_bounds__(kBlk, 6) density_kernel(const DensArgs a) {
         int iter = 0;
         bool converged = false;
         DensSums s;
+        // the candidate cache (not for the counting variant, whose tallies are per search):
+        // filled at the first h, refilled at kCacheGrow times h when h outgrows it
+        uint32_t* slot = a.cand + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+        double R = -1.0;   // radius of the cached search; < 0: nothing cached
+        int ncand = 0;
+        bool cache_ok = !COUNT && a.cand != nullptr;
+        auto evaluate = [&](double hh) {
+            if (cache_ok && !(R >= hh)) {
+                const double rad = (R < 0 ? kCacheFirst : kCacheGrow) * hh;
+                ncand = cache_fill(a, r0, r1, px, py, pz, rad, slot, a.n_threads);
+                if (ncand < 0) cache_ok = false;  // too many candidates: search directly from now on
+                else R = rad;
+            }
+            if (cache_ok) cache_eval(a, slot, a.n_threads, ncand, px, py, pz, hh, s);
+            else dens_eval<COUNT>(a, r0, r1, px, py, pz, hh, s, tl, kept);
+        };
         for (; iter < 100; ++iter) {
-            dens_eval<COUNT>(a, r0, r1, px, py, pz, h, s, tl, kept);
+            evaluate(h);
             if (COUNT) ++calls;
             if (dens_newton(newton_params(a), p, s, iter, h, h_lo, h_hi)) { converged = true; break; }
         }
         if (!converged) {  // rho of the final h (hydro.cc:281-293)
-            dens_eval<COUNT>(a, r0, r1, px, py, pz, h, s, tl, kept);
+            evaluate(h);
             if (COUNT) ++calls;
         }
         if (COUNT) ++hist[min(converged ? iter + 1 : 100, 8) - 1];
@@ -683,6 +746,13 @@ void run_density(gt_context* ctx, gt_tree* t, int64_t nt, const uint32_t* target
     a.face_corr = face_corr;
     a.h = h; a.rho = rho; a.nngb = nngb; a.iters = iters;
     a.tally = tally && nt > 0 ? fresh_tally(ctx) : nullptr;
+    a.cand = nullptr;
+    a.cand_cap = kCandCap;
+    a.n_threads = 0;
+    if (!a.tally && nt > 0) {
+        a.n_threads = (int64_t)grid_of(ctx, nt) * kBlk;
+        a.cand = (uint32_t*)scratch(ctx, kSlotNgb0, (size_t)a.n_threads * kCandCap * sizeof(uint32_t));
+    }
     a.h_default = 0.0;
     a.h_default_sys = nullptr;
     if (!h_start && t->n_systems > 1) {

@@ -210,3 +210,30 @@ def test_counters_match_reference(gpu_ctx, golden, ngb_tree, ngb_counts):
         assert gpu_ctx.ngb_counters()["calls"] == 0
     finally:
         gpu_ctx.ngb_count(False)
+
+
+@pytest.mark.parametrize("case", ["cold", "warm", "cond", "box"])
+def test_candidate_cache_is_bit_identical(gpu_ctx, golden, ngb_tree, case):
+    """The density solve scans a per-thread cache of one search's gas candidates when a Newton step
+    shrinks h below the cached radius.  It keeps the particles, the order and the r^2 test of a
+    search at h, so h, rho, the neighbour counts and the iterations are bit-identical to the
+    solve that searches at every evaluation (the counting variant, SHMEM_NGB_COUNT on)."""
+    kw = {}
+    T = ngb_tree
+    tg = golden["ngb_targets"]
+    if case == "warm":
+        kw["h_start"] = 1.1 * golden["ngb_cold_h"]
+    if case == "cond":
+        kw["cond_prev"] = golden["ngb_cond"]
+    if case == "box":
+        T = gpu_ctx.build(particles(golden, "ngb_box"), key_mode=g.GT_KEY_MORTON)
+        tg = golden["ngb_box_targets"]
+        kw["box"] = 2.0
+    cached = gpu_ctx.density(T, tg, 32.0, 0.05, **kw)
+    gpu_ctx.ngb_count(True)
+    try:
+        direct = gpu_ctx.density(T, tg, 32.0, 0.05, **kw)
+    finally:
+        gpu_ctx.ngb_count(False)
+    for k in ("h", "rho", "nngb", "iters"):
+        assert np.array_equal(cached[k], direct[k]), k
