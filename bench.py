@@ -161,10 +161,18 @@ def leaf_group_sample(orderbuf, leaf_of, want, rng):
     return np.concatenate([orderbuf[s:e] for s, e in zip(starts[sel], ends[sel])]).astype(np.uint32)
 
 
+def reference_omp_env():
+    """The reference's recommended OpenMP placement (shmem/README.md:47-51), set before its library,
+    and with it its OpenMP runtime, is loaded."""
+    os.environ.setdefault("OMP_PROC_BIND", "spread")
+    os.environ.setdefault("OMP_PLACES", "cores")
+
+
 class CpuReference:
     """oracle/_ref (the reference's own shmem tree) when built, else the oracle restatement."""
 
     def __init__(self):
+        reference_omp_env()
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         from oracle import Reference, Restatement, reference_available
 
@@ -949,6 +957,7 @@ def run_extras_arm(args):
              "gas": {"median": float(np.median(eg)), "p99": float(np.quantile(eg, 0.99))}}
     cpu = None
     if not args.no_cpu:
+        reference_omp_env()
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         from oracle import Reference, reference_available
 
@@ -1046,6 +1055,7 @@ def run_density_arm(args):
     cpu = None
     if not args.no_cpu:
         try:
+            reference_omp_env()
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
             from oracle import Reference, reference_available
 
