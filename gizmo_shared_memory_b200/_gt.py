@@ -692,11 +692,15 @@ class Context:
         n = len(cx)
         start = np.zeros(n + 1, np.int64)
         tot = C.c_int64(0)
-        self._check(L.gt_ngb_search(self.h, tree.h, n, _ptr(cx), _ptr(cy), _ptr(cz), _ptr(radius), C.byref(o),
-                                    GT_MEM_HOST, _ptr(start), None, 0, C.byref(tot)))
-        found = np.zeros(max(tot.value, 1), np.uint32)
-        self._check(L.gt_ngb_search(self.h, tree.h, n, _ptr(cx), _ptr(cy), _ptr(cz), _ptr(radius), C.byref(o),
-                                    GT_MEM_HOST, _ptr(start), _ptr(found), len(found), C.byref(tot)))
+        # one call with room for 48 neighbours per centre; a second, sized, call if that overflows
+        found = np.empty(max(48 * n, 1024), np.uint32)
+        st = L.gt_ngb_search(self.h, tree.h, n, _ptr(cx), _ptr(cy), _ptr(cz), _ptr(radius), C.byref(o),
+                             GT_MEM_HOST, _ptr(start), _ptr(found), len(found), C.byref(tot))
+        if st == 5:  # GT_ERR_OVERFLOW: start and the total are filled
+            found = np.empty(max(tot.value, 1), np.uint32)
+            st = L.gt_ngb_search(self.h, tree.h, n, _ptr(cx), _ptr(cy), _ptr(cz), _ptr(radius), C.byref(o),
+                                 GT_MEM_HOST, _ptr(start), _ptr(found), len(found), C.byref(tot))
+        self._check(st)
         return start, found[: tot.value]
 
     def density(self, tree: Tree, targets, des_ngb=32.0, ngb_tol=0.05, h_start=None, box=0.0, n_dims=3,

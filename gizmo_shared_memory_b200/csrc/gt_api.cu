@@ -889,22 +889,20 @@ int gt_ngb_search(gt_context* ctx, const gt_tree* tc, int64_t n, const double* c
         const double* dh = stage_in(ctx, kSlotIn4, o.h, ng, mem);
         const int* dsys = (const int*)stage_in(ctx, kSlotIn5, o.systems, n, mem);
         int64_t* ds = out_buf(ctx, kSlotOut0, start, n + 1, mem);
-        // the host path sizes the device list from the count pass: capacity 0 in the call below
-        // means "count only", the lists follow once the total is known.  SHMEM_NGB_COUNT: a call
-        // counts its searches once, when it delivers the lists; a count-only call or one that
-        // overflows counts nothing, so counting then filling counts each search once
+        // the host path makes the lists in a workspace buffer once the counting pass has sized
+        // them.  SHMEM_NGB_COUNT: a call counts its searches once, when it delivers the lists; a
+        // count-only call or one that overflows counts nothing, so counting then filling counts
+        // each search once
         uint32_t* df = mem == GT_MEM_DEVICE ? found : nullptr;
         int64_t tl[5] = {0, 0, 0, 0, 0};
         const bool counted = ctx->ngb_count && found;
+        uint32_t* hf = nullptr;  // host path: the lists, made on the device in one call
         const int64_t tot = run_ngb(ctx, tree, n, dx, dy, dz, dr, dsys, o.mode, dh, ng, o.box, o.elapsed, ds, df,
-                                    mem == GT_MEM_DEVICE ? capacity : 0, counted ? tl : nullptr);
+                                    found ? capacity : 0, counted ? tl : nullptr,
+                                    mem == GT_MEM_HOST && found ? &hf : nullptr);
         if (total) *total = tot;
         copy_out(ctx, start, ds, n + 1, mem);
-        if (mem == GT_MEM_HOST && found && tot <= capacity && tot > 0) {
-            uint32_t* hf = (uint32_t*)scratch(ctx, kSlotOut1, (size_t)tot * 4);
-            run_ngb(ctx, tree, n, dx, dy, dz, dr, dsys, o.mode, dh, ng, o.box, o.elapsed, ds, hf, tot, nullptr);
-            copy_out(ctx, found, hf, tot, mem);
-        }
+        if (hf) copy_out(ctx, found, hf, tot, mem);
         finish(ctx, true);
         if (found && tot > capacity) throw Fail{GT_ERR_OVERFLOW, "the neighbour lists need more room than capacity"};
         if (counted)

@@ -208,7 +208,7 @@ enum Slot {
     kSlotTargets, kSlotAold, kSlotGroupKey, kSlotGroupsA, kSlotGroupsB,
     kSlotOut0, kSlotOut1, kSlotOut2, kSlotOut3, kSlotOut4, kSlotOut5,
     kSlotStack, kSlotCounters, kSlotDirect, kSlotGroupRoot, kSlotMacL2,
-    kSlotNgb0, kSlotNgb1, kSlotNgb2,
+    kSlotNgb0, kSlotNgb1, kSlotNgb2, kSlotNgb3,
     kSlotStack2,  // traversal stacks of the second compute stream (chunked walks)
     kSlotGroupCount,  // device-side group and chunk counts of an explicit-target walk
     kSlotLevels,      // device-side level offsets and counts of the build's structure stage
@@ -373,10 +373,13 @@ void raise_hmax(gt_context* ctx, gt_tree* t, int64_t n, const int* leaf, const d
 // Counts into start (n+1, exclusive prefix sums) and, when found is given and the total fits
 // capacity, the lists; returns the total.
 // systems: per centre, the one system searched (null: every system).  tally (host, 5 values, or
-// null): the SHMEM_NGB_COUNT tally of the gather searches of the counting pass.
+// null): the SHMEM_NGB_COUNT tally of the gather searches of the counting pass.  list_out (with
+// found null): when the lists fit capacity, they are made in a workspace buffer whose device
+// pointer is returned there (null otherwise).
 int64_t run_ngb(gt_context* ctx, gt_tree* t, int64_t n, const double* cx, const double* cy, const double* cz,
                 const double* radius, const int* systems, int mode, const double* h, int64_t n_gas, double box,
-                double elapsed, int64_t* start, uint32_t* found, int64_t capacity, int64_t* tally);
+                double elapsed, int64_t* start, uint32_t* found, int64_t capacity, int64_t* tally,
+                uint32_t** list_out = nullptr);
 // tally (host, GT_NGB_COUNTERS values, or null): the solve's SHMEM_NGB_COUNT tally (synchronises).
 void run_density(gt_context* ctx, gt_tree* t, int64_t nt, const uint32_t* targets, double des_ngb, double ngb_tol,
                  const double* h_start, double box, int n_dims, const double* cond_prev, int face_corr,

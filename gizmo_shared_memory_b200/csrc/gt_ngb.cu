@@ -182,10 +182,16 @@ struct NgbArgs {
     const double* h;
     int64_t n_gas;
     uint32_t* count;              // counting pass
-    unsigned long long* total;    // counting pass: [0] sum of the counts, [1] centres naming no system
+    unsigned long long* total;    // counting pass: [0] sum of the counts, [1] centres naming no
+                                  // system, [2] centres with more than kcache entries
     const int64_t* start;         // filling pass
     uint32_t* found;
     unsigned long long* tally;    // SHMEM_NGB_COUNT totals (calls, nodes, examined, kept, pad)
+    // The counting pass keeps each centre's first kcache entries (entry k of centre c at
+    // cache[k * n + c]); the lists of centres with at most kcache entries are then copied from
+    // there, and only the others are searched again.  kcache 0: no cache.
+    uint32_t* cache;
+    int kcache;
 };
 
 // Sums v over the warp and adds it to *dst from lane 0; every lane of the warp calls it.
@@ -213,15 +219,17 @@ __device__ __forceinline__ void roots_of(const SearchGeom& g, const int* systems
 
 template <bool FILL, bool COUNT>
 __global__ void __launch_bounds__(kBlk) ngb_kernel(const NgbArgs a) {
-    unsigned long long mine = 0, calls = 0, kept = 0;
+    unsigned long long mine = 0, calls = 0, kept = 0, over = 0;
     NgbTally tl;
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < a.n; c += (int64_t)gridDim.x * blockDim.x) {
         const double px = a.cx[c], py = a.cy[c], pz = a.cz[c], r = a.radius[c];
         int r0, r1;
         roots_of(a.g, a.systems, c, r0, r1, FILL ? nullptr : a.total + 1);
+        if (FILL && a.kcache > 0 && a.count[c] <= (uint32_t)a.kcache) continue;  // copied from the cache
         int64_t k = FILL ? a.start[c] : 0;
         auto emit = [&](uint32_t j, int) {
             if (FILL) a.found[k] = j;
+            else if (k < a.kcache) a.cache[k * a.n + c] = j;
             ++k;
         };
         if (a.mode != GT_NGB_REVERSE) {
@@ -235,15 +243,30 @@ __global__ void __launch_bounds__(kBlk) ngb_kernel(const NgbArgs a) {
         if (!FILL) {
             a.count[c] = (uint32_t)k;
             mine += (unsigned long long)k;
+            over += k > a.kcache ? 1ull : 0ull;
         }
     }
-    if (!FILL) warp_flush(mine, a.total);
+    if (!FILL) {
+        warp_flush(mine, a.total);
+        warp_flush(over, a.total + 2);
+    }
     if (COUNT) {
         warp_flush(calls, a.tally + 0);
         warp_flush(tl.nodes, a.tally + 1);
         warp_flush(tl.examined, a.tally + 2);
         warp_flush(kept, a.tally + 3);
         warp_flush(tl.pad, a.tally + 4);
+    }
+}
+
+// The lists of the centres the counting pass kept whole in the cache, into their CSR slots.
+__global__ void ngb_copy_kernel(const uint32_t* __restrict__ cache, int kcache, const uint32_t* __restrict__ cnt,
+                                const int64_t* __restrict__ start, int64_t n, uint32_t* __restrict__ found) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t m = cnt[c];
+        if (m > (uint32_t)kcache) continue;
+        const int64_t s0 = start[c];
+        for (uint32_t k = 0; k < m; ++k) found[s0 + k] = cache[(int64_t)k * n + c];
     }
 }
 
@@ -672,7 +695,8 @@ void raise_hmax(gt_context* ctx, gt_tree* t, int64_t n, const int* leaf, const d
 
 int64_t run_ngb(gt_context* ctx, gt_tree* t, int64_t n, const double* cx, const double* cy, const double* cz,
                 const double* radius, const int* systems, int mode, const double* h, int64_t n_gas, double box,
-                double elapsed, int64_t* start, uint32_t* found, int64_t capacity, int64_t* tally) {
+                double elapsed, int64_t* start, uint32_t* found, int64_t capacity, int64_t* tally,
+                uint32_t** list_out) {
     if (mode != GT_NGB_GATHER && !t->hmax) throw Fail{GT_ERR_INVALID, "the reverse search needs gt_tree_hmax first"};
     cudaStream_t st = ctx->stream;
     NgbArgs a;
@@ -686,34 +710,52 @@ int64_t run_ngb(gt_context* ctx, gt_tree* t, int64_t n, const double* cx, const 
     a.n_gas = n_gas;
     uint32_t* cnt = (uint32_t*)scratch(ctx, kSlotNgb0, (size_t)std::max<int64_t>(n, 1) * 4);
     uint32_t* ex = (uint32_t*)scratch(ctx, kSlotNgb1, (size_t)std::max<int64_t>(n, 1) * 4);
-    unsigned long long* tot = (unsigned long long*)scratch(ctx, kSlotNgb2, 16);
-    check_cuda(cudaMemsetAsync(tot, 0, 16, st), "memset");
+    unsigned long long* tot = (unsigned long long*)scratch(ctx, kSlotNgb2, 24);
+    check_cuda(cudaMemsetAsync(tot, 0, 24, st), "memset");
     a.count = cnt;
     a.total = tot;
     a.start = nullptr;
     a.found = nullptr;
+    // the first entries of every centre, kept by the counting pass when the lists are wanted: up
+    // to 64 per centre within 2 GiB (none below 8)
+    const bool want = (found && capacity > 0) || list_out;
+    a.kcache = want ? (int)std::min<int64_t>(64, ((int64_t)1 << 31) / (4 * std::max<int64_t>(n, 1))) : 0;
+    if (a.kcache < 8) a.kcache = 0;
+    a.cache = a.kcache ? (uint32_t*)scratch(ctx, kSlotNgb3, (size_t)n * a.kcache * 4) : nullptr;
     if (a.tally) ngb_kernel<false, true><<<grid_of(ctx, n), kBlk, 0, st>>>(a);
     else ngb_kernel<false, false><<<grid_of(ctx, n), kBlk, 0, st>>>(a);
     check_launch(ctx, "ngb_kernel");
-    unsigned long long total[2] = {0, 0};
-    check_cuda(cudaMemcpyAsync(ctx->pinned, tot, 16, cudaMemcpyDeviceToHost, st), "d2h");
+    unsigned long long total[3] = {0, 0, 0};
+    check_cuda(cudaMemcpyAsync(ctx->pinned, tot, 24, cudaMemcpyDeviceToHost, st), "d2h");
     if (a.tally)
         check_cuda(cudaMemcpyAsync((char*)ctx->pinned + 64, a.tally, 5 * 8, cudaMemcpyDeviceToHost, st), "d2h");
     check_cuda(cudaStreamSynchronize(st), "sync");
-    std::memcpy(total, ctx->pinned, 16);
+    std::memcpy(total, ctx->pinned, 24);
     if (a.tally) std::memcpy(tally, (char*)ctx->pinned + 64, 5 * 8);
     if (total[1] > 0) throw Fail{GT_ERR_INVALID, "a centre names a system outside [0, n_systems)"};
     if (total[0] >= (1ull << 32)) throw Fail{GT_ERR_OVERFLOW, "more than 2^32 neighbours in one call"};
     scan_exclusive_u32(ctx, cnt, ex, n, nullptr);
     widen_kernel<<<grid_of(ctx, n), kBlk, 0, st>>>(ex, cnt, n, start);
     check_launch(ctx, "widen_kernel");
-    if (found && (int64_t)total[0] <= capacity && total[0] > 0) {
-        a.start = start;
-        a.found = found;
-        a.tally = nullptr;
-        ngb_kernel<true, false><<<grid_of(ctx, n), kBlk, 0, st>>>(a);
-        check_launch(ctx, "ngb_kernel");
+    uint32_t* dst = nullptr;
+    if ((int64_t)total[0] <= capacity && total[0] > 0) {
+        if (found) dst = found;
+        else if (list_out) dst = (uint32_t*)scratch(ctx, kSlotOut1, (size_t)total[0] * 4);
     }
+    if (dst) {
+        if (a.kcache) {
+            ngb_copy_kernel<<<grid_of(ctx, n), kBlk, 0, st>>>(a.cache, a.kcache, cnt, start, n, dst);
+            check_launch(ctx, "ngb_copy_kernel");
+        }
+        if (!a.kcache || total[2] > 0) {  // the centres the cache did not hold whole
+            a.start = start;
+            a.found = dst;
+            a.tally = nullptr;
+            ngb_kernel<true, false><<<grid_of(ctx, n), kBlk, 0, st>>>(a);
+            check_launch(ctx, "ngb_kernel");
+        }
+    }
+    if (list_out) *list_out = dst;
     return (int64_t)total[0];
 }
 

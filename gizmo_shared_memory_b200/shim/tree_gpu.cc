@@ -646,16 +646,20 @@ DensityResult density(const Tree& T, const Particles& P, const std::vector<uint3
             o.elapsed = T.t_since_build;
             std::vector<int64_t> start(nt + 1);
             int64_t tot = 0;
-            // the reference's cache holds the solve's own lists: these searches are not counted
+            // the reference's cache holds the solve's own lists: these searches are not counted.
+            // One call with room for 64 neighbours per target, a sized second one if that overflows.
             if (ngb_counting()) check(gt_ngb_count(context(), 0), "gt_ngb_count");
-            const int st = gt_ngb_search(context(), T.gpu.get(), (int64_t)nt, cx.data(), cy.data(), cz.data(),
-                                         R.h.data(), &o, GT_MEM_HOST, start.data(), nullptr, 0, &tot);
+            cache->flat.resize(nt * 64);
+            int st = gt_ngb_search(context(), T.gpu.get(), (int64_t)nt, cx.data(), cy.data(), cz.data(), R.h.data(),
+                                   &o, GT_MEM_HOST, start.data(), cache->flat.data(), (int64_t)cache->flat.size(), &tot);
+            if (st == GT_ERR_OVERFLOW) {
+                cache->flat.resize((size_t)tot);
+                st = gt_ngb_search(context(), T.gpu.get(), (int64_t)nt, cx.data(), cy.data(), cz.data(), R.h.data(),
+                                   &o, GT_MEM_HOST, start.data(), cache->flat.data(), tot, &tot);
+            }
+            if (ngb_counting()) check(gt_ngb_count(context(), 1), "gt_ngb_count");
             check(st, "gt_ngb_search");
             cache->flat.resize((size_t)tot);
-            const int st2 = gt_ngb_search(context(), T.gpu.get(), (int64_t)nt, cx.data(), cy.data(), cz.data(),
-                                          R.h.data(), &o, GT_MEM_HOST, start.data(), cache->flat.data(), tot, &tot);
-            if (ngb_counting()) check(gt_ngb_count(context(), 1), "gt_ngb_count");
-            check(st2, "gt_ngb_search");
             for (size_t t = 0; t <= nt; ++t) cache->start[t] = (size_t)start[t];
         }
         cache->valid = true;
