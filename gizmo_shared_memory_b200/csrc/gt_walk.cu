@@ -378,7 +378,7 @@ walk_kernel(const WalkArgs A) {
         // monopole-list entry pos (paired layout, see flush_pn)
         // The monopole list is paired (see flush_pn) for the packed evaluation of full groups
         // and one float4 per entry otherwise (warp-uniform: the group size decides).
-        const bool paired = XT != 1 && NS == 1;
+        const bool paired = NS == 1;
         auto pn_put = [&](int pos, float x, float y, float z, float m) {
             if (paired) {
                 float* q = reinterpret_cast<float*>(pn + 2 * (pos >> 1)) + (pos & 1);
@@ -465,7 +465,10 @@ walk_kernel(const WalkArgs A) {
         // r^2 above 1e-22, so only a point closer than FP32 resolves is affected (it then adds 0
         // along that axis instead of a NaN).
         auto flush_pn = [&](int n) {
-            if (paired && (n & 1) && lane == 0) pn_put(n, 0.0f, 0.0f, 0.0f, 0.0f);
+            if (paired && (n & 1) && lane == 0) {
+                pn_put(n, 0.0f, 0.0f, 0.0f, 0.0f);
+                if (want_jerk) pnv[n] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // the pad's velocity
+            }
             __syncwarp();
             const int np = (n + 1) >> 1;
             float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
@@ -477,6 +480,8 @@ walk_kernel(const WalkArgs A) {
             if (paired) {
                 float2 ax2[TPL], ay2[TPL], az2[TPL], ap2[TPL];
                 float2 ntx[TPL], nty[TPL], ntz[TPL];
+                // XT 1: the tidal and jerk sums of xt_add, two entries per instruction
+                float2 xq2[XT == 1 ? TPL : 1][10];
                 const float2 r2_floor = make_float2(1e-30f, 1e-30f);
 #pragma unroll
                 for (int k = 0; k < TPL; ++k) {
@@ -484,9 +489,13 @@ walk_kernel(const WalkArgs A) {
                     ntx[k] = make_float2(-tx[k], -tx[k]);
                     nty[k] = make_float2(-ty[k], -ty[k]);
                     ntz[k] = make_float2(-tz[k], -tz[k]);
+                    if (XT == 1)
+#pragma unroll
+                        for (int c = 0; c < 10; ++c) xq2[XT == 1 ? k : 0][c] = make_float2(0.0f, 0.0f);
                 }
-                // 8 pairs in flight per lane (unroll 2 and 4 measured 1.9 % and 0.6 % slower)
-#pragma unroll 8
+                // 8 pairs in flight per lane (unroll 2 and 4 measured 1.9 % and 0.6 % slower); the
+                // tidal and jerk body is three times longer, and unrolled it outgrows instruction fetch
+#pragma unroll (XT == 1 ? 1 : 8)
                 for (int jp = slice; jp < np; jp += NS) {
                     const float4 A = pn[2 * jp], B = pn[2 * jp + 1];
                     const float2 X = make_float2(A.x, A.y), Y = make_float2(A.z, A.w);
@@ -504,6 +513,33 @@ walk_kernel(const WalkArgs A) {
                             ay2[k] = __ffma2_rn(dy, f, ay2[k]);
                             az2[k] = __ffma2_rn(dz, f, az2[k]);
                             if (WANT_POT) ap2[k] = __fadd2_rn(ap2[k], mri);
+                            if (XT == 1) {
+                                // Newtonian: g1 = f, g2 = 3 f / r^2, each element rounded as xt_add
+                                float2(&q)[10] = xq2[XT == 1 ? k : 0];
+                                const float2 g2 = __fmul2_rn(__fmul2_rn(make_float2(3.0f, 3.0f), f), __fmul2_rn(ri, ri));
+                                if (want_tid) {
+                                    const float2 gx = __fmul2_rn(g2, dx), gy = __fmul2_rn(g2, dy), gz = __fmul2_rn(g2, dz);
+                                    q[0] = __ffma2_rn(gx, dx, q[0]);
+                                    q[1] = __ffma2_rn(gy, dy, q[1]);
+                                    q[2] = __ffma2_rn(gz, dz, q[2]);
+                                    q[3] = __ffma2_rn(gx, dy, q[3]);
+                                    q[4] = __ffma2_rn(gy, dz, q[4]);
+                                    q[5] = __ffma2_rn(gx, dz, q[5]);
+                                    q[9] = __fadd2_rn(q[9], f);
+                                }
+                                if (want_jerk) {
+                                    const float4 v0 = pnv[2 * jp], v1 = pnv[2 * jp + 1];
+                                    const float2 dvx = __fadd2_rn(make_float2(v0.x, v1.x), make_float2(-tvx[k], -tvx[k]));
+                                    const float2 dvy = __fadd2_rn(make_float2(v0.y, v1.y), make_float2(-tvy[k], -tvy[k]));
+                                    const float2 dvz = __fadd2_rn(make_float2(v0.z, v1.z), make_float2(-tvz[k], -tvz[k]));
+                                    const float2 vg =
+                                        __fmul2_rn(__ffma2_rn(dvx, dx, __ffma2_rn(dvy, dy, __fmul2_rn(dvz, dz))), g2);
+                                    const float2 nvg = make_float2(-vg.x, -vg.y);
+                                    q[6] = __fadd2_rn(q[6], __ffma2_rn(f, dvx, __fmul2_rn(nvg, dx)));
+                                    q[7] = __fadd2_rn(q[7], __ffma2_rn(f, dvy, __fmul2_rn(nvg, dy)));
+                                    q[8] = __fadd2_rn(q[8], __ffma2_rn(f, dvz, __fmul2_rn(nvg, dz)));
+                                }
+                            }
                         }
                     }
                 }
@@ -513,6 +549,10 @@ walk_kernel(const WalkArgs A) {
                     ay_[k] = ay2[k].x + ay2[k].y;
                     az_[k] = az2[k].x + az2[k].y;
                     ap_[k] = -(ap2[k].x + ap2[k].y);
+                    if (XT == 1)
+#pragma unroll
+                        for (int c = 0; c < 10; ++c)
+                            xq[XT == 1 ? k : 0][c] = xq2[XT == 1 ? k : 0][c].x + xq2[XT == 1 ? k : 0][c].y;
                 }
             } else {
                 if (XT == 1) {
