@@ -20,7 +20,7 @@ graph), --workload extras_galaxy_4m (the tidal tensor, the jerk, the gas rules a
 4M galaxy), --workload density_galaxy_4m / density_clustered_16m (the density solve).
 
 Multi-GPU (--gpus N under torchrun): by default (--split targets) the ranks share one system:
-every rank builds the same tree and walks its window-aligned slice of the tree order
+every rank builds the same tree and walks its slice of the tree order, aligned to window pairs
 (gizmo_shared_memory_b200/sharding.py), and ``value`` is the system's particles over the max-over-ranks
 step time ("scaling": "strong").  --split systems walks one independent system per rank (seed +
 rank, "scaling": "weak").  There is no data-path collective in either: only the barrier and the max
@@ -503,7 +503,7 @@ def run_gpu_arm(args):
                  batch=args.group_max if args.group == "batch" else 0)
 
     # --split targets (N > 1): one system, every rank builds the same tree and walks its
-    # window-aligned slice of the tree order (sharding.walk_shard); --split systems: one
+    # slice of the tree order, aligned to window pairs (sharding.walk_shard); --split systems: one
     # independent system per rank
     split = args.split == "targets" and (world > 1 or args.shard_check)
     P = make_workload(args.workload, seed_offset=0 if split else rank)
@@ -1225,7 +1225,7 @@ def main():
                          "most --group-max particles")
     ap.add_argument("--group-max", type=int, default=32)
     ap.add_argument("--split", choices=["targets", "systems"], default="targets",
-                    help="N > 1: targets = one system, every rank walks a window-aligned slice of its "
+                    help="N > 1: targets = one system, every rank walks a slice (aligned to window pairs) of its "
                          "tree order; systems = one independent system per rank")
     ap.add_argument("--shard-check", action="store_true",
                     help="run the --split targets path at N = 1 too (one slice holding every target), to "

@@ -4,7 +4,8 @@ Targets are independent once the tree exists, so N GPUs split one all-active wal
 every rank builds the same tree from the full particle set (the build is deterministic, so the
 trees are identical and nothing is exchanged), then walks a contiguous slice of the targets in
 tree order -- a Peano-Hilbert key range, hence a compact region of space -- with slice edges on
-group-window boundaries so that no window is split.  The results stay on the rank that computed
+boundaries of two group windows, so that no window is split and the walk pairs windows as the
+single-rank walk does.  The results stay on the rank that computed
 them, as the engine keeps forces where the targets live; there is no collective in the data path.
 Gathering the slices (for a check, or for a caller that wants all forces in one place) is a
 separate, optional all-gather.
@@ -16,11 +17,15 @@ import numpy as np
 
 def shard_ranges(n_targets: int, world: int, window: int = 32):
     """Contiguous [start, end) slices of n_targets tree-order targets, one per rank, with every
-    edge on a multiple of `window` and sizes differing by at most one window."""
+    edge on a multiple of two windows and sizes differing by at most two windows.  The walk takes
+    consecutive windows two per warp, pairing windows 2p and 2p + 1 of its target list; a slice
+    that starts on an even window pairs its windows as the single-rank walk does, so the ranks'
+    results are those of the single-rank walk bit for bit."""
     if world < 1:
         raise ValueError("world must be >= 1")
-    n_win = (n_targets + window - 1) // window
-    edges = [(r * n_win) // world * window for r in range(world + 1)]
+    unit = 2 * window
+    n_unit = (n_targets + unit - 1) // unit
+    edges = [(r * n_unit) // world * unit for r in range(world + 1)]
     edges = [min(e, n_targets) for e in edges]
     edges[-1] = n_targets
     return [(edges[r], edges[r + 1]) for r in range(world)]
@@ -45,8 +50,8 @@ def walk_shard(walk, orderbuf, aold_tree, rank: int, world: int, window: int = 3
 
     orderbuf holds the tree order (particle indices) and aold_tree the per-target aold in the same
     order (or None).  The rank walks targets orderbuf[a:b] with aold_tree[a:b], where [a, b) is its
-    window-aligned slice, so its windows are exactly the single-rank walk's windows over that
-    range.  walk(targets, aold) does the walking (the GPU context, or the oracle in the CPU tests)
+    slice (aligned to two windows), so its windows, and the pairs of windows its warps walk, are
+    exactly the single-rank walk's over that range.  walk(targets, aold) does the walking (the GPU context, or the oracle in the CPU tests)
     and returns the results parallel to targets.  Returns (a, b, results)."""
     a, b = shard_ranges(len(orderbuf), world, window)[rank]
     tg = orderbuf[a:b]
