@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(kBlk, 6) density_kernel(const DensArgs a) {
         DensSums s;
         // the candidate cache (not for the counting variant, whose tallies are per search):
         // filled at the first h, refilled at kCacheGrow times h when h outgrows it
-        uint32_t* slot = a.cand + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+        uint32_t* slot = a.cand ? a.cand + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) : nullptr;
         double R = -1.0;   // radius of the cached search; < 0: nothing cached
         int ncand = 0;
         bool cache_ok = !COUNT && a.cand != nullptr;
