@@ -129,8 +129,8 @@ typedef struct {
     /* Grouped windows of 17-32 targets (GT_GROUP_BATCH) are walked two per warp by default: two
      * consecutive windows share one traversal, each testing exactly its own nodes, so every
      * window gets its own walk's decisions and interactions (sums equal to FP32 rounding, not bit
-     * for bit: the list order can differ).  Not for GT_MAC_LEARNED, the tidal tensor, the jerk,
-     * the gas rules, counting walks or forests.  1: one window per warp. */
+     * for bit: the list order can differ).  Forests and counting walks included; not for
+     * GT_MAC_LEARNED, the tidal tensor, the jerk or the gas rules.  1: one window per warp. */
     int no_window_pairs;
 } gt_walk_options;
 
@@ -363,7 +363,8 @@ GT_API int gt_tree_hmax(gt_context* ctx, gt_tree* tree, const double* h, int64_t
 /* Neighbour lists of n_centres centres (cx, cy, cz, radius: n_centres each) as CSR: start
  * (n_centres + 1 int64) always; found (particle indices) when it is not NULL and the total fits
  * `capacity`, else GT_ERR_OVERFLOW with start and *total filled (call again with room).  *total
- * (may be NULL) receives the number of entries. */
+ * (may be NULL) receives the number of entries.  A call with room traverses the tree once: its
+ * counting pass keeps each centre's first entries and copies them into place. */
 GT_API int gt_ngb_search(gt_context* ctx, const gt_tree* tree, int64_t n_centres, const double* cx,
                   const double* cy, const double* cz, const double* radius, const gt_ngb_options* opt,
                   int mem, int64_t* start, uint32_t* found, int64_t capacity, int64_t* total);
