@@ -387,6 +387,13 @@ walk_kernel(const WalkArgs A) {
                 pn[pos] = make_float4(x, y, z, m);
             }
         };
+        // the particle list is paired the same way for full groups of the plain walk (the tidal
+        // tensor, the jerk and the gas rules read it one entry at a time)
+        const bool ppair = XT == 0 && paired;
+        auto pp_put = [&](int pos, float x, float y, float z, float m) {
+            float* q = reinterpret_cast<float*>(pp + 2 * (pos >> 1)) + (pos & 1);
+            q[0] = x; q[2] = y; q[4] = z; q[6] = m;
+        };
         // tidal tensor and jerk: FP64 totals (xx yy zz xy yz xz, jx jy jz) and target velocities;
         // gas targets: zeta / m and 1 / m (0 for a target that is not gas or has no mass,
         // tree.cc:46); a group holding a sink opens by the sink rule (tree.cc:691-698)
@@ -597,7 +604,16 @@ walk_kernel(const WalkArgs A) {
             __syncwarp();
         };
         // Particles: kernel of the larger softening; r^2 == 0 (the target itself) contributes 0.
+        // Full groups of the plain walk pair the list like the monopoles and evaluate two entries
+        // per packed instruction while both are outside the kernel or at r = 0; a pair with an
+        // entry inside the kernel takes the scalar spline for both, with the same terms, so the
+        // sums do not depend on which lanes diverge.  An odd list is padded with a massless entry
+        // far outside (1e18 on each axis), which adds exact zeros.
         auto flush_pp = [&](int n) {
+            if (ppair && (n & 1) && lane == 0) {
+                pp_put(n, 1e18f, 1e18f, 1e18f, 0.0f);
+                ph[n] = 0.0f;
+            }
             __syncwarp();
             float ax_[TPL], ay_[TPL], az_[TPL], ap_[TPL];
             float xq[XT == 1 ? TPL : 1][10];
@@ -610,39 +626,100 @@ walk_kernel(const WalkArgs A) {
                     for (int c = 0; c < 10; ++c) xq[XT == 1 ? k : 0][c] = 0.0f;
             }
             unsigned zero = 0;
-            for (int j = slice; j < n; j += NS) {
-                const float4 e = pp[j];
-                const float hj = ph[j];
+            if (ppair) {
+                float2 ax2[TPL], ay2[TPL], az2[TPL], np2[TPL];  // np2: minus the potential
+#pragma unroll
+                for (int k = 0; k < TPL; ++k) ax2[k] = ay2[k] = az2[k] = np2[k] = make_float2(0.0f, 0.0f);
+                const float2* __restrict__ H = reinterpret_cast<const float2*>(ph);
+                const int np = (n + 1) >> 1;
+                for (int jp = 0; jp < np; ++jp) {
+                    const float4 P = pp[2 * jp], Q = pp[2 * jp + 1];
+                    const float2 hj = H[jp];
+                    const float2 X = make_float2(P.x, P.y), Y = make_float2(P.z, P.w);
+                    const float2 Z = make_float2(Q.x, Q.y), M = make_float2(Q.z, Q.w);
+#pragma unroll
+                    for (int k = 0; k < TPL; ++k) {
+                        if (k < nk) {
+                            const float2 dx = __fadd2_rn(X, make_float2(-tx[k], -tx[k]));
+                            const float2 dy = __fadd2_rn(Y, make_float2(-ty[k], -ty[k]));
+                            const float2 dz = __fadd2_rn(Z, make_float2(-tz[k], -tz[k]));
+                            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+                            const float2 hh = make_float2(fmaxf(th[k], hj.x), fmaxf(th[k], hj.y));
+                            const float2 hh2 = __fmul2_rn(hh, hh);
+                            const bool z0 = r2.x == 0.0f, z1 = r2.y == 0.0f;
+                            if (COUNT) zero += (unsigned)z0 + (unsigned)z1;
+                            float2 f, mp;
+                            if ((r2.x >= hh2.x || z0) && (r2.y >= hh2.y || z1)) {
+                                const float2 ri = make_float2(z0 ? 0.0f : rsqrt_ftz(r2.x), z1 ? 0.0f : rsqrt_ftz(r2.y));
+                                mp = __fmul2_rn(M, ri);
+                                f = __fmul2_rn(mp, __fmul2_rn(ri, ri));
+                            } else {
+                                // the same terms one entry at a time, the spline where r < h
+                                const float r2s[2] = {r2.x, r2.y}, hs[2] = {hh.x, hh.y}, ms[2] = {M.x, M.y};
+                                float fs[2], ps[2];
+#pragma unroll
+                                for (int e = 0; e < 2; ++e) {
+                                    if (r2s[e] >= hs[e] * hs[e] && r2s[e] > 0.0f) {
+                                        const float ri = rsqrt_ftz(r2s[e]);
+                                        const float mri = ms[e] * ri;
+                                        fs[e] = mri * (ri * ri);
+                                        ps[e] = -mri;
+                                    } else {
+                                        spline_pair(r2s[e], hs[e], ms[e], fs[e], ps[e]);
+                                    }
+                                }
+                                f = make_float2(fs[0], fs[1]);
+                                mp = make_float2(-ps[0], -ps[1]);
+                            }
+                            ax2[k] = __ffma2_rn(dx, f, ax2[k]);
+                            ay2[k] = __ffma2_rn(dy, f, ay2[k]);
+                            az2[k] = __ffma2_rn(dz, f, az2[k]);
+                            if (WANT_POT) np2[k] = __fadd2_rn(np2[k], mp);
+                        }
+                    }
+                }
 #pragma unroll
                 for (int k = 0; k < TPL; ++k) {
-                    if (k < nk) {
-                        const float dx = e.x - tx[k], dy = e.y - ty[k], dz = e.z - tz[k];
-                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        const float hh = fmaxf(th[k], hj);
-                        float f, p, g2 = 0.0f;
-                        float fa;  // the acceleration's factor: f less the gas pair's zeta terms
-                        if (r2 >= hh * hh && r2 > 0.0f) {
-                            const float ri = rsqrtf(r2);
-                            const float mri = e.w * ri;
-                            f = mri * ri * ri;
-                            p = -mri;
-                            if (XT == 1) g2 = 3.0f * f * (ri * ri);
-                            fa = f;
-                        } else if (XT == 1) {
-                            spline_pair_tidal(r2, hh, e.w, f, p, g2);
-                            fa = want_zeta ? f - zeta_pair(r2, hh, hj, pzs[j], tzm[k], tim[k]) : f;
-                        } else {
-                            spline_pair(r2, hh, e.w, f, p);
-                            fa = (XT == 2 && want_zeta) ? f - zeta_pair(r2, hh, hj, pzs[j], tzm[k], tim[k]) : f;
-                        }
-                        if (COUNT) zero += (r2 == 0.0f);
-                        ax_[k] = fmaf(dx, fa, ax_[k]);
-                        ay_[k] = fmaf(dy, fa, ay_[k]);
-                        az_[k] = fmaf(dz, fa, az_[k]);
-                        if (WANT_POT) ap_[k] += p;
-                        if (XT == 1) {
-                            const float4 ev = want_jerk ? ppv[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-                            xt_add(xq[XT == 1 ? k : 0], dx, dy, dz, f, g2, ev, k);
+                    ax_[k] = ax2[k].x + ax2[k].y;
+                    ay_[k] = ay2[k].x + ay2[k].y;
+                    az_[k] = az2[k].x + az2[k].y;
+                    ap_[k] = -(np2[k].x + np2[k].y);
+                }
+            } else {
+                for (int j = slice; j < n; j += NS) {
+                    const float4 e = pp[j];
+                    const float hj = ph[j];
+#pragma unroll
+                    for (int k = 0; k < TPL; ++k) {
+                        if (k < nk) {
+                            const float dx = e.x - tx[k], dy = e.y - ty[k], dz = e.z - tz[k];
+                            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            const float hh = fmaxf(th[k], hj);
+                            float f, p, g2 = 0.0f;
+                            float fa;  // the acceleration's factor: f less the gas pair's zeta terms
+                            if (r2 >= hh * hh && r2 > 0.0f) {
+                                const float ri = rsqrtf(r2);
+                                const float mri = e.w * ri;
+                                f = mri * ri * ri;
+                                p = -mri;
+                                if (XT == 1) g2 = 3.0f * f * (ri * ri);
+                                fa = f;
+                            } else if (XT == 1) {
+                                spline_pair_tidal(r2, hh, e.w, f, p, g2);
+                                fa = want_zeta ? f - zeta_pair(r2, hh, hj, pzs[j], tzm[k], tim[k]) : f;
+                            } else {
+                                spline_pair(r2, hh, e.w, f, p);
+                                fa = (XT == 2 && want_zeta) ? f - zeta_pair(r2, hh, hj, pzs[j], tzm[k], tim[k]) : f;
+                            }
+                            if (COUNT) zero += (r2 == 0.0f);
+                            ax_[k] = fmaf(dx, fa, ax_[k]);
+                            ay_[k] = fmaf(dy, fa, ay_[k]);
+                            az_[k] = fmaf(dz, fa, az_[k]);
+                            if (WANT_POT) ap_[k] += p;
+                            if (XT == 1) {
+                                const float4 ev = want_jerk ? ppv[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                                xt_add(xq[XT == 1 ? k : 0], dx, dy, dz, f, g2, ev, k);
+                            }
                         }
                     }
                 }
@@ -825,7 +902,8 @@ walk_kernel(const WalkArgs A) {
                         if (want_jerk) pnv[npn + __popc(fm & lt_mask)] = A.svel[qpos];
                     } else if (live && GT_IN_BOUNDS(npp + __popc(nm & lt_mask), A.pp_cap)) {
                         const int pos = npp + __popc(nm & lt_mask);
-                        pp[pos] = e;
+                        if (ppair) pp_put(pos, e.x, e.y, e.z, e.w);
+                        else pp[pos] = e;
                         ph[pos] = qh;
                         if (want_jerk) ppv[pos] = A.svel[qpos];
                         if (want_zeta) pzs[pos] = A.stype[qpos] == 0 ? (float)A.szeta[qpos] : __int_as_float(0x7fc00000);
@@ -1015,6 +1093,11 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 3) walk_pair_kernel(const Walk
             float* q = reinterpret_cast<float*>(pn_of(v) + 2 * (pos >> 1)) + (pos & 1);
             q[0] = x; q[2] = y; q[4] = z; q[6] = m;
         };
+        // particle-list entry pos of window v, in the same paired layout
+        auto pp_put = [&](int v, int pos, float x, float y, float z, float m) {
+            float* q = reinterpret_cast<float*>(pp_of(v) + 2 * (pos >> 1)) + (pos & 1);
+            q[0] = x; q[2] = y; q[4] = z; q[6] = m;
+        };
         // window v's monopoles against its targets: walk_kernel's packed loop
         auto flush_pn = [&](int v, int n) {
             if ((n & 1) && lane == 0) pn_put(v, n, 0.0f, 0.0f, 0.0f, 0.0f);
@@ -1044,36 +1127,68 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 3) walk_pair_kernel(const Walk
             if (COUNT) c_flush += (lane == 0);
             __syncwarp();
         };
-        // window v's particles: the kernel of the larger softening; r^2 == 0 contributes 0
+        // window v's particles: the kernel of the larger softening; r^2 == 0 contributes 0.  The
+        // list is paired like the monopoles (pp_put), softenings side by side, and evaluated two
+        // entries per packed instruction while both are outside the kernel or at r = 0 (the
+        // window's own particles); a pair with an entry inside the kernel takes the scalar spline
+        // for both.  Each entry's terms are the same on either path, so the sums do not depend on
+        // which lanes diverge.  An odd list is padded with a massless entry far outside (1e18 on
+        // each axis, r^2 ~ 3e36 below the FP32 range's end), which adds exact zeros.
         auto flush_pp = [&](int v, int n) {
+            if ((n & 1) && lane == 0) {
+                pp_put(v, n, 1e18f, 1e18f, 1e18f, 0.0f);
+                ph_of(v)[n] = 0.0f;
+            }
             __syncwarp();
-            float ax = 0.0f, ay = 0.0f, az = 0.0f, ap = 0.0f;
+            const int np = (n + 1) >> 1;
+            float2 ax2 = make_float2(0.0f, 0.0f), ay2 = ax2, az2 = ax2, np2 = ax2;  // np2: minus the potential
             const float qx = v ? tx[1] : tx[0], qy = v ? ty[1] : ty[0], qz = v ? tz[1] : tz[0];
             const float qh = v ? th[1] : th[0];
+            const float2 ntx = make_float2(-qx, -qx), nty = make_float2(-qy, -qy), ntz = make_float2(-qz, -qz);
             const float4* __restrict__ L = pp_of(v);
-            const float* __restrict__ H = ph_of(v);
-            for (int j = 0; j < n; ++j) {
-                const float4 e = L[j];
-                const float hj = H[j];
-                const float dx = e.x - qx, dy = e.y - qy, dz = e.z - qz;
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const float hh = fmaxf(qh, hj);
-                float f, p;
-                if (r2 >= hh * hh && r2 > 0.0f) {
-                    const float ri = rsqrtf(r2);
-                    const float mri = e.w * ri;
-                    f = mri * ri * ri;
-                    p = -mri;
+            const float2* __restrict__ H = reinterpret_cast<const float2*>(ph_of(v));
+            for (int jp = 0; jp < np; ++jp) {
+                const float4 P = L[2 * jp], Q = L[2 * jp + 1];
+                const float2 hj = H[jp];
+                const float2 X = make_float2(P.x, P.y), Y = make_float2(P.z, P.w);
+                const float2 Z = make_float2(Q.x, Q.y), M = make_float2(Q.z, Q.w);
+                const float2 dx = __fadd2_rn(X, ntx), dy = __fadd2_rn(Y, nty), dz = __fadd2_rn(Z, ntz);
+                const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+                const float2 hh = make_float2(fmaxf(qh, hj.x), fmaxf(qh, hj.y));
+                const float2 hh2 = __fmul2_rn(hh, hh);
+                const bool z0 = r2.x == 0.0f, z1 = r2.y == 0.0f;
+                if (COUNT) c_zero += (unsigned long long)z0 + (unsigned long long)z1;
+                if ((r2.x >= hh2.x || z0) && (r2.y >= hh2.y || z1)) {
+                    const float2 ri = make_float2(z0 ? 0.0f : rsqrt_ftz(r2.x), z1 ? 0.0f : rsqrt_ftz(r2.y));
+                    const float2 mri = __fmul2_rn(M, ri);
+                    const float2 f = __fmul2_rn(mri, __fmul2_rn(ri, ri));
+                    ax2 = __ffma2_rn(dx, f, ax2);
+                    ay2 = __ffma2_rn(dy, f, ay2);
+                    az2 = __ffma2_rn(dz, f, az2);
+                    if (WANT_POT) np2 = __fadd2_rn(np2, mri);
                 } else {
-                    spline_pair(r2, hh, e.w, f, p);
+                    // the same terms one entry at a time, the spline where r < h
+                    const float r2s[2] = {r2.x, r2.y}, hs[2] = {hh.x, hh.y}, ms[2] = {M.x, M.y};
+                    float fs[2], ps[2];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        if (r2s[e] >= hs[e] * hs[e] && r2s[e] > 0.0f) {
+                            const float ri = rsqrt_ftz(r2s[e]);
+                            const float mri = ms[e] * ri;
+                            fs[e] = mri * (ri * ri);
+                            ps[e] = -mri;
+                        } else {
+                            spline_pair(r2s[e], hs[e], ms[e], fs[e], ps[e]);
+                        }
+                    }
+                    const float2 f = make_float2(fs[0], fs[1]);
+                    ax2 = __ffma2_rn(dx, f, ax2);
+                    ay2 = __ffma2_rn(dy, f, ay2);
+                    az2 = __ffma2_rn(dz, f, az2);
+                    if (WANT_POT) np2 = __fadd2_rn(np2, make_float2(-ps[0], -ps[1]));
                 }
-                ax = fmaf(dx, f, ax);
-                ay = fmaf(dy, f, ay);
-                az = fmaf(dz, f, az);
-                if (WANT_POT) ap += p;
-                if (COUNT) c_zero += (r2 == 0.0f);
             }
-            add_partial(v, ax, ay, az, ap);
+            add_partial(v, ax2.x + ax2.y, ay2.x + ay2.y, az2.x + az2.y, -(np2.x + np2.y));
             if (COUNT) c_flush += (lane == 0);
             __syncwarp();
         };
@@ -1158,7 +1273,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 3) walk_pair_kernel(const Walk
                         pn_put(v, npn + __popc(fm & lt_mask), ex, ey, ez, qm);
                     } else if (in && GT_IN_BOUNDS(npp + __popc(nm & lt_mask), A.pp_cap)) {
                         const int pos = npp + __popc(nm & lt_mask);
-                        pp_of(v)[pos] = make_float4(ex, ey, ez, qm);
+                        pp_put(v, pos, ex, ey, ez, qm);
                         ph_of(v)[pos] = qh;
                     }
                     npn += __popc(fm);
