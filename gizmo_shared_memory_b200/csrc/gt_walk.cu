@@ -19,9 +19,10 @@
 //     and softening.  When the list fills it is evaluated against the group's targets.
 //   * Evaluation (FP32): r^2, rsqrt, Newtonian force and potential; the cubic-spline branch only
 //     when r < max(h_target, h_source) (shmem/tree.h:59-80).  r^2 == 0 (the target itself, or a
-//     coincident particle) contributes nothing, as tree.cc:799-802 skips it.  Groups of <= 16
-//     targets split the list across the idle lanes (lane = slice * NT + target) and reduce the
-//     slices at the end.
+//     coincident particle) contributes nothing, as tree.cc:799-802 skips it.  Full groups store
+//     both lists in pairs of entries and evaluate two entries per sm_100 packed FP32 instruction.
+//     Groups of <= 16 targets split the list across the idle lanes (lane = slice * NT + target)
+//     and reduce the slices at the end.
 //   * Accumulation: each list evaluation sums into FP32 partials, which are added into FP32
 //     Kahan-compensated totals (acceleration) and an FP64 total (potential); the final sums and
 //     the factor G are FP64.
