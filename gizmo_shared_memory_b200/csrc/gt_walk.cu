@@ -229,8 +229,11 @@ __device__ __noinline__ float zeta_pair(float r2, float h, float hs, float zs, f
 }
 
 // 1/sqrt(x) by the PTX approximate reciprocal square root with flush-to-zero.  The monopole loops
-// floor r^2 at 1e-30, far above the FP32 subnormal range, so the flush never acts there and the
-// result equals rsqrtf's; the non-FTZ form only adds subnormal-range scaling instructions.
+// floor r^2 at 1e-30, far above the FP32 subnormal range, and the particle loops take it only for
+// r^2 > 0 and r^2 >= h^2 with h the larger softening, a normal number for any h above 1.1e-19.  So
+// the result equals rsqrtf's except for two particles closer than 1.1e-19 with softenings below
+// that, whose force overflows FP32 either way.  The non-FTZ form only adds subnormal-range scaling
+// instructions.
 __device__ __forceinline__ float rsqrt_ftz(float x) {
     float y;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -633,7 +636,7 @@ walk_kernel(const WalkArgs A) {
                 for (int k = 0; k < TPL; ++k) ax2[k] = ay2[k] = az2[k] = np2[k] = make_float2(0.0f, 0.0f);
                 const float2* __restrict__ H = reinterpret_cast<const float2*>(ph);
                 const int np = (n + 1) >> 1;
-                for (int jp = 0; jp < np; ++jp) {
+                for (int jp = slice; jp < np; jp += NS) {
                     const float4 P = pp[2 * jp], Q = pp[2 * jp + 1];
                     const float2 hj = H[jp];
                     const float2 X = make_float2(P.x, P.y), Y = make_float2(P.z, P.w);
@@ -698,8 +701,10 @@ walk_kernel(const WalkArgs A) {
                             const float hh = fmaxf(th[k], hj);
                             float f, p, g2 = 0.0f;
                             float fa;  // the acceleration's factor: f less the gas pair's zeta terms
-                            if (r2 >= hh * hh && r2 > 0.0f) {
-                                const float ri = rsqrtf(r2);
+                            // r = 0 (the target itself) takes this branch with 1/r = 0: every term
+                            // is then 0, as the spline branch gives it, without the call
+                            if (r2 >= hh * hh || r2 == 0.0f) {
+                                const float ri = r2 > 0.0f ? rsqrt_ftz(r2) : 0.0f;
                                 const float mri = e.w * ri;
                                 f = mri * ri * ri;
                                 p = -mri;
