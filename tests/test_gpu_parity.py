@@ -238,6 +238,30 @@ def test_grouped_potential_matches_oracle(gpu_ctx, plummer_trees):
     assert np.median(e) <= MEDIAN_TOL
 
 
+@pytest.mark.parametrize("pairs", [True, False])
+def test_packed_particle_lists_match_oracle(gpu_ctx, oracle, pairs):
+    """Windows of 32 evaluate their particle lists two entries per packed FP32x2 instruction; a
+    pair holding an entry inside the softening kernel takes the one-entry spline for both, and
+    r = 0 (each target's own entry) contributes nothing on either path.  Softenings drawn from
+    0.02-0.2 around a central spacing of about 0.05 put many pairs in that mixed case, with the
+    two entries' kernel radii max(h_target, h_source) differing.  Accelerations and potentials
+    against the oracle's windows of 32: two windows per warp and one."""
+    P = ics.plummer(n=32768, seed=77)
+    P["soft"] = np.random.default_rng(78).uniform(0.02, 0.2, len(P["m"]))
+    T, O = gpu_ctx.build(P, key_mode=g.GT_KEY_MORTON), oracle.build(P)
+    ob = O.order()[0]
+    n = len(ob)
+    starts = np.concatenate([np.arange(0, n, 32), [n]]).astype(np.int64)
+    bx, by, bz, _, _ = O.walk_groups(ob, starts, 0.7)
+    aold = 0.0025 * np.sqrt(bx ** 2 + by ** 2 + bz ** 2)
+    ax, ay, az, phi = gpu_ctx.accel_grouped(T, ob, aold=aold, theta=0.0, want_phi=True, batch=32,
+                                            group_mode=g.GT_GROUP_BATCH, window_pairs=pairs)
+    rx, ry, rz, rphi, _ = O.walk_groups(ob, starts, 0.0, aold=aold, want_phi=True)
+    check((ax, ay, az), (rx, ry, rz))
+    e = np.abs(phi - rphi) / np.abs(rphi)
+    assert np.median(e) <= MEDIAN_TOL and np.quantile(e, 0.99) <= 1e-4, (np.median(e), np.quantile(e, 0.99))
+
+
 def node_group_starts(O, gmax):
     """Group starts of GT_GROUP_NODE over the full tree order, from the oracle tree."""
     nd = O.nodes()
