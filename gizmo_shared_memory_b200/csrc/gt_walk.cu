@@ -1003,9 +1003,9 @@ struct alignas(16) PairHdr {
     int lo[32];   // leaf-expansion scratch: first slot, exclusive prefix and windows of each leaf
     int pre[32];
     int msk[32];
-    // per window: box corners, centre, largest target softening, smallest aold
-    double lo_x[2], lo_y[2], lo_z[2], hi_x[2], hi_y[2], hi_z[2], c_x[2], c_y[2], c_z[2], emax[2], amin[2];
-    double w_x[2], w_y[2], w_z[2];  // half widths of the boxes
+    // per window, in one 64-byte record: box centre and half width per axis side by side (one
+    // 16-byte shared-memory load per axis of a box gap), largest target softening, smallest aold
+    struct alignas(16) Win { double c_x, w_x, c_y, w_y, c_z, w_z, emax, amin; } wb[2];
 };
 
 __host__ __device__ constexpr int pair_list_bytes(int pn_cap, int pp_cap) { return pn_cap * 16 + pp_cap * 20; }
@@ -1074,11 +1074,9 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 3) walk_pair_kernel(const Walk
             if (A.aold) amin = wmin(amin);
             const double cx = 0.5 * (lx + hx), cy = 0.5 * (ly + hy), cz = 0.5 * (lz + hz);
             if (lane == 0) {
-                S.lo_x[v] = lx; S.lo_y[v] = ly; S.lo_z[v] = lz;
-                S.hi_x[v] = hx; S.hi_y[v] = hy; S.hi_z[v] = hz;
-                S.c_x[v] = cx; S.c_y[v] = cy; S.c_z[v] = cz;
-                S.w_x[v] = 0.5 * (hx - lx); S.w_y[v] = 0.5 * (hy - ly); S.w_z[v] = 0.5 * (hz - lz);
-                S.emax[v] = emax; S.amin[v] = amin;
+                S.wb[v].c_x = cx; S.wb[v].c_y = cy; S.wb[v].c_z = cz;
+                S.wb[v].w_x = 0.5 * (hx - lx); S.wb[v].w_y = 0.5 * (hy - ly); S.wb[v].w_z = 0.5 * (hz - lz);
+                S.wb[v].emax = emax; S.wb[v].amin = amin;
             }
             tx[v] = (float)(px - cx);
             ty[v] = (float)(py - cy);
@@ -1268,11 +1266,11 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 3) walk_pair_kernel(const Walk
                     const bool in = (wm >> v) & 1;
                     bool far = false;
                     if (in) {
-                        const double ex = box_gap(qx, S.c_x[v], S.w_x[v]);
-                        const double ey = box_gap(qy, S.c_y[v], S.w_y[v]);
-                        const double ez = box_gap(qz, S.c_z[v], S.w_z[v]);
+                        const double ex = box_gap(qx, S.wb[v].c_x, S.wb[v].w_x);
+                        const double ey = box_gap(qy, S.wb[v].c_y, S.wb[v].w_y);
+                        const double ez = box_gap(qz, S.wb[v].c_z, S.wb[v].w_z);
                         const double qhd = (double)qh;
-                        const double reach = S.emax[v] > qhd ? S.emax[v] : qhd;
+                        const double reach = S.wb[v].emax > qhd ? S.wb[v].emax : qhd;
                         far = ex * ex + ey * ey + ez * ez > reach * reach;
                     }
                     const unsigned fm = __ballot_sync(kFull, in && far);
@@ -1280,7 +1278,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 3) walk_pair_kernel(const Walk
                     int& npn = v ? npn1 : npn0;
                     int& npp = v ? npp1 : npp0;
                     if (COUNT && lane == 0) c_pairs += (unsigned long long)__popc(fm | nm) * nt[v];
-                    const float ex = (float)(qx - S.c_x[v]), ey = (float)(qy - S.c_y[v]), ez = (float)(qz - S.c_z[v]);
+                    const float ex = (float)(qx - S.wb[v].c_x), ey = (float)(qy - S.wb[v].c_y), ez = (float)(qz - S.wb[v].c_z);
                     if (in && far && GT_IN_BOUNDS(npn + __popc(fm & lt_mask), A.pn_cap)) {
                         pn_put(v, npn + __popc(fm & lt_mask), ex, ey, ez, qm);
                     } else if (in && GT_IN_BOUNDS(npp + __popc(nm & lt_mask), A.pp_cap)) {
@@ -1316,13 +1314,13 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 3) walk_pair_kernel(const Walk
                 acc[v] = false;
                 opn[v] = false;
                 if ((mk >> v) & 1) {
-                    const double dx = box_gap(nd.cx, S.c_x[v], S.w_x[v]);
-                    const double dy = box_gap(nd.cy, S.c_y[v], S.w_y[v]);
-                    const double dz = box_gap(nd.cz, S.c_z[v], S.w_z[v]);
+                    const double dx = box_gap(nd.cx, S.wb[v].c_x, S.wb[v].w_x);
+                    const double dy = box_gap(nd.cy, S.wb[v].c_y, S.wb[v].w_y);
+                    const double dz = box_gap(nd.cz, S.wb[v].c_z, S.wb[v].w_z);
                     const double r2 = dx * dx + dy * dy + dz * dz;
                     const double len = (double)nd.len;
                     const double ml2 = MAC == 2 ? nd.mass * (double)__ldg(A.mac_l2 + node) : nd.mass * len * len;
-                    const bool o = open_node(r2, len, nd.s, ml2, (double)nd.soft, S.emax[v], S.amin[v], A.theta2,
+                    const bool o = open_node(r2, len, nd.s, ml2, (double)nd.soft, S.wb[v].emax, S.wb[v].amin, A.theta2,
                                              dx, dy, dz);
                     acc[v] = !o;
                     opn[v] = o;
@@ -1362,8 +1360,8 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 3) walk_pair_kernel(const Walk
                 int& npn = v ? npn1 : npn0;
                 if (COUNT && lane == 0) c_multi += (unsigned long long)__popc(am) * nt[v];
                 if (acc[v] && GT_IN_BOUNDS(npn + __popc(am & lt_mask), A.pn_cap))
-                    pn_put(v, npn + __popc(am & lt_mask), (float)(nd.cx - S.c_x[v]), (float)(nd.cy - S.c_y[v]),
-                           (float)(nd.cz - S.c_z[v]), (float)nd.mass);
+                    pn_put(v, npn + __popc(am & lt_mask), (float)(nd.cx - S.wb[v].c_x), (float)(nd.cy - S.wb[v].c_y),
+                           (float)(nd.cz - S.wb[v].c_z), (float)nd.mass);
                 npn += __popc(am);
             }
 
